@@ -1,0 +1,551 @@
+/*
+ * CPU oracle for the standard-gridder imaging path.
+ *
+ * TEST INFRASTRUCTURE ONLY.  This file restates, in plain C and FP64, the
+ * arithmetic of astroviper's standard-gridder path so that the CUDA kernels
+ * of astroviper_b200 can be checked against it.  Only tests/, the smoke check
+ * and bench.py's CPU-baseline leg may load it.  The product never calls it.
+ *
+ * Every function keeps the reference's operation order (no FMA contraction:
+ * build with -ffp-contract=off) so that its results are bit-identical to the
+ * reference's Numba / C++ code; tests/golden pins that.
+ *
+ * Reference files (paths inside the astroviper project):
+ *   src/astroviper/core/imaging/imaging_utils/gcf_prolate_spheroidal.py
+ *   src/astroviper/core/imaging/imaging_utils/standard_grid.py
+ *   src/astroviper/core/imaging/imaging_utils/standard_degrid.py
+ *   src/astroviper/core/imaging/imaging_weighting/grid_imaging_weights.py
+ *   src/astroviper/core/imaging/deconvolvers/hogbom/src/hclean.cpp
+ */
+#include <math.h>
+#include <stdint.h>
+#include <stdlib.h>
+#include <string.h>
+#ifdef _OPENMP
+#include <omp.h>
+#endif
+
+typedef struct { double re, im; } cplx;
+
+/* ---------------------------------------------------------------------------
+ * PSWF rational approximation (Schwab), gcf_prolate_spheroidal.py:102-158.
+ * grdsf(u) = sum_k p[part][k] d^k / sum_k q[part][k] d^k, d = u^2 - uend^2,
+ * part 0 for |u| < 0.75 (uend 0.75), part 1 for 0.75 <= |u| <= 1 (uend 1),
+ * 0 for |u| > 1.  Returns grdsf and (1 - u^2) grdsf.
+ * ------------------------------------------------------------------------- */
+static const double PSWF_P[2][5] = {
+    {8.203343e-2, -3.644705e-1, 6.278660e-1, -5.335581e-1, 2.312756e-1},
+    {4.028559e-3, -3.697768e-2, 1.021332e-1, -1.201436e-1, 6.412774e-2}};
+static const double PSWF_Q[2][3] = {{1.0000000e0, 8.212018e-1, 2.078043e-1},
+                                    {1.0000000e0, 9.599102e-1, 2.918724e-1}};
+
+void orc_pswf(const double *u_in, int64_t n, double *grdsf_out, double *kern_out) {
+  for (int64_t i = 0; i < n; ++i) {
+    double u = fabs(u_in[i]);
+    int part = 0;
+    double uend = 0.0;
+    if (u >= 0.0 && u < 0.75) { part = 0; uend = 0.75; }
+    if (u >= 0.75 && u <= 1.0) { part = 1; uend = 1.0; }
+    double delusq = u * u - uend * uend;
+    double top = PSWF_P[part][0];
+    for (int k = 1; k < 5; ++k) top += PSWF_P[part][k] * pow(delusq, (double)k);
+    double bot = PSWF_Q[part][0];
+    for (int k = 1; k < 3; ++k) bot += PSWF_Q[part][k] * pow(delusq, (double)k);
+    double g = 0.0;
+    if (bot > 0.0) g = top / bot;
+    if (u > 1.0) g = 0.0;
+    if (grdsf_out) grdsf_out[i] = g;
+    if (kern_out) kern_out[i] = (1.0 - u * u) * g;
+  }
+}
+
+/* create_prolate_spheroidal_kernel_1D, gcf_prolate_spheroidal.py:87-99:
+ * out has oversampling*(support//2+1) entries; the first
+ * oversampling*(support//2) are (1-u^2) grdsf(u) at u = i/(sc*os), rest 0. */
+void orc_cgk_1d(int oversampling, int support, double *out) {
+  int sc = support / 2;
+  int64_t n = (int64_t)oversampling * sc;
+  int64_t ntot = (int64_t)oversampling * (sc + 1);
+  for (int64_t i = 0; i < ntot; ++i) out[i] = 0.0;
+  for (int64_t i = 0; i < n; ++i) {
+    double u = (double)i / (double)(sc * oversampling);
+    orc_pswf(&u, 1, NULL, &out[i]);
+  }
+}
+
+/* Grid-correction image of create_prolate_spheroidal_kernel,
+ * gcf_prolate_spheroidal.py:73-79 (coordinates() at :161). */
+void orc_corr_term(int64_t nx, int64_t ny, double *out) {
+  double *gx = (double *)malloc(sizeof(double) * nx);
+  double *gy = (double *)malloc(sizeof(double) * ny);
+  for (int64_t i = 0; i < nx; ++i) {
+    double c = (double)(i - nx / 2) / (double)nx;
+    double u = fabs(2.0 * c);
+    orc_pswf(&u, 1, &gx[i], NULL);
+  }
+  for (int64_t i = 0; i < ny; ++i) {
+    double c = (double)(i - ny / 2) / (double)ny;
+    double u = fabs(2.0 * c);
+    orc_pswf(&u, 1, &gy[i], NULL);
+  }
+  for (int64_t i = 0; i < nx; ++i)
+    for (int64_t j = 0; j < ny; ++j) out[i * ny + j] = gx[i] * gy[j];
+  free(gx);
+  free(gy);
+}
+
+/* Python int(x) of a finite double: truncation toward zero.  Values outside
+ * +-2^62 cannot be inside any grid; they map to a sentinel that fails every
+ * bounds test (Numba's fptosi gives INT64_MIN there). */
+static inline int64_t trunc_i64(double x) {
+  if (!(fabs(x) < 4.611686018427388e18)) return INT64_MIN / 2;
+  return (int64_t)x;
+}
+
+/* ---------------------------------------------------------------------------
+ * standard_grid_jit, standard_grid.py:246-432.
+ * grid: (n_img_chan, n_img_pol, n_u, n_v), complex (is_complex=1, interleaved)
+ *       or real (is_complex=0, only meaningful with do_psf).
+ * vis: (nt, nb, nchan, npol) complex; weight same shape, real.
+ * uvw: (nt, nb, 3).  chan_map (nchan), pol_map (npol).
+ * The (t, b) range [tb_lo, tb_hi) lets the CPU baseline split work.
+ * ------------------------------------------------------------------------- */
+static void grid_range(void *grid, int is_complex, double *sum_weight, int do_psf,
+                       int do_imaging_weight, const cplx *vis, const double *uvw,
+                       const double *freq, const int64_t *chan_map,
+                       const int64_t *pol_map, const double *weight, const double *cgk,
+                       int64_t n_u, int64_t n_v, double dl0, double dl1, int support,
+                       int oversampling, int64_t nt, int64_t nb, int64_t nchan,
+                       int64_t npol, int64_t n_img_pol, int64_t tb_lo, int64_t tb_hi) {
+  const double c = 299792458.0;
+  double *us0 = (double *)malloc(sizeof(double) * nchan);
+  double *us1 = (double *)malloc(sizeof(double) * nchan);
+  for (int64_t k = 0; k < nchan; ++k) {
+    us0[k] = -(freq[k] * dl0 * (double)n_u) / c;
+    us1[k] = -(freq[k] * dl1 * (double)n_v) / c;
+  }
+  const int64_t sc = support / 2;
+  const int64_t uc0 = n_u / 2, uc1 = n_v / 2;
+  const int64_t s0 = -sc, s1 = support - sc;
+  cplx *gc = (cplx *)grid;
+  double *gr = (double *)grid;
+  (void)nt;
+  for (int64_t tb = tb_lo; tb < tb_hi; ++tb) {
+    const double *p_uvw = uvw + tb * 3;
+    for (int64_t ic = 0; ic < nchan; ++ic) {
+      int64_t a_chan = chan_map[ic];
+      double u = p_uvw[0] * us0[ic];
+      double v = p_uvw[1] * us1[ic];
+      if (isnan(u) || isnan(v)) continue;
+      double u_pos = u + (double)uc0, v_pos = v + (double)uc1;
+      double u_pos_c = -u + (double)uc0, v_pos_c = -v + (double)uc1;
+      int64_t ui = trunc_i64(u_pos + 0.5), vi = trunc_i64(v_pos + 0.5);
+      int64_t uic = trunc_i64(u_pos_c + 0.5), vic = trunc_i64(v_pos_c + 0.5);
+      if (!((ui + sc < n_u) && (vi + sc < n_v) && (ui - sc >= 0) && (vi - sc >= 0)))
+        continue;
+      double u_off = (double)ui - u_pos;
+      int64_t uoi = (int64_t)floor(u_off * (double)oversampling + 0.5);
+      double v_off = (double)vi - v_pos;
+      int64_t voi = (int64_t)floor(v_off * (double)oversampling + 0.5);
+      for (int64_t ip = 0; ip < npol; ++ip) {
+        const int64_t idx = (tb * nchan + ic) * npol + ip;
+        double sel_weight;
+        cplx wd;
+        if (do_psf) {
+          if (npol >= 2 && do_imaging_weight) {
+            const int64_t i0 = (tb * nchan + ic) * npol;
+            wd.re = (weight[i0] + weight[i0 + 1]) / 2.0;
+            wd.im = 0.0;
+            sel_weight = wd.re;
+          } else {
+            sel_weight = weight[idx];
+            wd.re = weight[idx];
+            wd.im = 0.0;
+          }
+        } else {
+          sel_weight = weight[idx];
+          wd.re = vis[idx].re * weight[idx];
+          wd.im = vis[idx].im * weight[idx];
+        }
+        if (isnan(wd.re) || isnan(wd.im)) continue;
+        if (!(wd.re != 0.0 || wd.im != 0.0)) continue;
+        int64_t a_pol = pol_map[ip];
+        double norm = 0.0;
+        int64_t plane = (a_chan * n_img_pol + a_pol) * n_u * n_v;
+        for (int64_t iv = s0; iv < s1; ++iv) {
+          int64_t v_indx = vi + iv;
+          int64_t vo = oversampling * iv + voi;
+          double conv_v = cgk[vo < 0 ? -vo : vo];
+          int64_t v_indx_c = vic + iv;
+          for (int64_t iu = s0; iu < s1; ++iu) {
+            int64_t u_indx = ui + iu;
+            int64_t uo = oversampling * iu + uoi;
+            double conv_u = cgk[uo < 0 ? -uo : uo];
+            double conv = conv_u * conv_v;
+            int64_t g = plane + u_indx * n_v + v_indx;
+            if (is_complex) {
+              gc[g].re = gc[g].re + conv * wd.re;
+              gc[g].im = gc[g].im + conv * wd.im;
+            } else {
+              gr[g] = gr[g] + conv * wd.re;
+            }
+            norm = norm + conv;
+            if (do_imaging_weight) {
+              int64_t u_indx_c = uic + iu;
+              int64_t gg = plane + u_indx_c * n_v + v_indx_c;
+              if (is_complex) {
+                gc[gg].re = gc[gg].re + conv * wd.re;
+                gc[gg].im = gc[gg].im + conv * wd.im;
+              } else {
+                gr[gg] = gr[gg] + conv * wd.re;
+              }
+            }
+          }
+        }
+        int64_t sw = a_chan * n_img_pol + a_pol;
+        sum_weight[sw] = sum_weight[sw] + sel_weight * norm;
+        if (do_imaging_weight) sum_weight[sw] = sum_weight[sw] + sel_weight * norm;
+      }
+    }
+  }
+  free(us0);
+  free(us1);
+}
+
+void orc_standard_grid(void *grid, int is_complex, double *sum_weight, int do_psf,
+                       int do_imaging_weight, const cplx *vis, const double *uvw,
+                       const double *freq, const int64_t *chan_map, const int64_t *pol_map,
+                       const double *weight, const double *cgk, int64_t n_u, int64_t n_v,
+                       double dl0, double dl1, int support, int oversampling, int64_t nt,
+                       int64_t nb, int64_t nchan, int64_t npol, int64_t n_img_pol) {
+  grid_range(grid, is_complex, sum_weight, do_psf, do_imaging_weight, vis, uvw, freq,
+             chan_map, pol_map, weight, cgk, n_u, n_v, dl0, dl1, support, oversampling, nt,
+             nb, nchan, npol, n_img_pol, 0, nt * nb);
+}
+
+/* Multi-threaded baseline: (t, b) rows split across threads, each into a
+ * private complex grid, summed at the end.  Same per-sample arithmetic. */
+int orc_standard_grid_mt(cplx *grid, double *sum_weight, int do_psf, const cplx *vis,
+                         const double *uvw, const double *freq, const int64_t *chan_map,
+                         const int64_t *pol_map, const double *weight, const double *cgk,
+                         int64_t n_u, int64_t n_v, double dl0, double dl1, int support,
+                         int oversampling, int64_t nt, int64_t nb, int64_t nchan,
+                         int64_t npol, int64_t n_img_chan, int64_t n_img_pol, int nthreads) {
+#ifdef _OPENMP
+  if (nthreads < 1) nthreads = omp_get_max_threads();
+#else
+  nthreads = 1;
+#endif
+  const int64_t gsz = n_img_chan * n_img_pol * n_u * n_v;
+  const int64_t ssz = n_img_chan * n_img_pol;
+  cplx **priv = (cplx **)calloc(nthreads, sizeof(cplx *));
+  double **psw = (double **)calloc(nthreads, sizeof(double *));
+  for (int t = 0; t < nthreads; ++t) {
+    priv[t] = (cplx *)calloc(gsz, sizeof(cplx));
+    psw[t] = (double *)calloc(ssz, sizeof(double));
+    if (!priv[t] || !psw[t]) return -1;
+  }
+  const int64_t ntb = nt * nb;
+#pragma omp parallel num_threads(nthreads)
+  {
+    int t = 0, T = 1;
+#ifdef _OPENMP
+    t = omp_get_thread_num();
+    T = omp_get_num_threads();
+#endif
+    int64_t lo = ntb * t / T, hi = ntb * (t + 1) / T;
+    grid_range(priv[t], 1, psw[t], do_psf, 0, vis, uvw, freq, chan_map, pol_map, weight, cgk,
+               n_u, n_v, dl0, dl1, support, oversampling, nt, nb, nchan, npol, n_img_pol, lo,
+               hi);
+  }
+#pragma omp parallel for num_threads(nthreads) schedule(static)
+  for (int64_t g = 0; g < gsz; ++g) {
+    double re = grid[g].re, im = grid[g].im;
+    for (int t = 0; t < nthreads; ++t) { re += priv[t][g].re; im += priv[t][g].im; }
+    grid[g].re = re;
+    grid[g].im = im;
+  }
+  for (int64_t s = 0; s < ssz; ++s)
+    for (int t = 0; t < nthreads; ++t) sum_weight[s] += psw[t][s];
+  for (int t = 0; t < nthreads; ++t) { free(priv[t]); free(psw[t]); }
+  free(priv);
+  free(psw);
+  return nthreads;
+}
+
+/* ---------------------------------------------------------------------------
+ * dgrid_numba, standard_degrid.py:388-485.
+ * values (nt, nb, nvchan, nvpol) complex, += ; flag same shape (uint8).
+ * grid (nchan, npol, gx, gy) complex; the bounds test uses the reference's
+ * own nx = shape[3], ny = shape[2] (standard_degrid.py:407,457-462); a sample
+ * that passes it but would still index outside the array is skipped here.
+ * ------------------------------------------------------------------------- */
+static void dgrid_range(const double *uvw, const double *dphase, cplx *values,
+                        const uint8_t *flag, const double *scale, const double *offset,
+                        const cplx *grid, int64_t g_nchan, int64_t g_npol, int64_t g_n2,
+                        int64_t g_n3, const double *freq, double c, int support, int sampling,
+                        const double *convFunc, const int64_t *chanmap, const int64_t *polmap,
+                        int64_t nt, int64_t nb, int64_t nvchan, int64_t nvpol, int64_t t_lo,
+                        int64_t t_hi) {
+  const int64_t nx = g_n3, ny = g_n2; /* as named in the reference */
+  const int64_t supp_centre = support / 2;
+  const int64_t supp_beg = -supp_centre, supp_end = supp_beg + support;
+  for (int64_t t = t_lo; t < t_hi; ++t) {
+    for (int64_t b = 0; b < nb; ++b) {
+      const double *p_uvw = uvw + (t * nb + b) * 3;
+      for (int64_t ipol = 0; ipol < nvpol; ++ipol) {
+        int64_t apol = polmap[ipol];
+        if (!(0 <= apol && apol < g_npol)) continue;
+        for (int64_t ichan = 0; ichan < nvchan; ++ichan) {
+          int64_t achan = chanmap[ichan];
+          int64_t vidx = ((t * nb + b) * nvchan + ichan) * nvpol + ipol;
+          if (!(0 <= achan && achan < g_nchan) || flag[vidx]) continue;
+          double pos0 = scale[0] * p_uvw[0] * freq[ichan] / c + offset[0];
+          double pos1 = scale[1] * p_uvw[1] * freq[ichan] / c + offset[1];
+          double r0 = nearbyint(pos0), r1 = nearbyint(pos1);
+          /* loc and off are stored in int32 arrays by the reference
+           * (standard_degrid.py:413-414): keep its wrap-around. */
+          int64_t loc0 = (int32_t)(uint32_t)(uint64_t)trunc_i64(r0);
+          int64_t loc1 = (int32_t)(uint32_t)(uint64_t)trunc_i64(r1);
+          int64_t off0 = (int32_t)(uint32_t)(uint64_t)trunc_i64(
+              nearbyint(((double)loc0 - pos0) * (double)sampling));
+          int64_t off1 = (int32_t)(uint32_t)(uint64_t)trunc_i64(
+              nearbyint(((double)loc1 - pos1) * (double)sampling));
+          double phase = -2.0 * M_PI * dphase[t * nb + b] * freq[ichan] / c;
+          double ph_re = cos(phase), ph_im = sin(phase);
+          int64_t x0 = loc0, y0 = loc1;
+          if (!((x0 + supp_beg >= 0) && ((x0 + supp_end - 1) < nx) && (y0 + supp_beg >= 0) &&
+                ((y0 + supp_end - 1) < ny)))
+            continue;
+          if (x0 + supp_end - 1 >= g_n2 || y0 + supp_end - 1 >= g_n3) continue;
+          double nv_re = 0.0, nv_im = 0.0, norm = 0.0;
+          const cplx *plane = grid + (achan * g_npol + apol) * g_n2 * g_n3;
+          for (int64_t ix = supp_beg; ix < supp_end; ++ix) {
+            int64_t i1 = sampling * ix + off0;
+            double wtx = convFunc[i1 < 0 ? -i1 : i1];
+            for (int64_t iy = supp_beg; iy < supp_end; ++iy) {
+              int64_t i2 = sampling * iy + off1;
+              double wty = convFunc[i2 < 0 ? -i2 : i2];
+              double wt = wtx * wty;
+              norm += wt;
+              cplx gv = plane[(x0 + ix) * g_n3 + (y0 + iy)];
+              nv_re = nv_re + wt * gv.re;
+              nv_im = nv_im + wt * gv.im;
+            }
+          }
+          if (norm != 0.0) {
+            /* nvalue * conj(phasor), then / norm (component-wise for a real
+             * divisor, as the complex quotient reduces to it). */
+            double cr = ph_re, ci = -ph_im;
+            double pr = nv_re * cr - nv_im * ci;
+            double pi = nv_re * ci + nv_im * cr;
+            values[vidx].re = values[vidx].re + pr / norm;
+            values[vidx].im = values[vidx].im + pi / norm;
+          }
+        }
+      }
+    }
+  }
+}
+
+void orc_dgrid(const double *uvw, const double *dphase, cplx *values, const uint8_t *flag,
+               const double *scale, const double *offset, const cplx *grid, int64_t g_nchan,
+               int64_t g_npol, int64_t g_n2, int64_t g_n3, const double *freq, double c,
+               int support, int sampling, const double *convFunc, const int64_t *chanmap,
+               const int64_t *polmap, int64_t nt, int64_t nb, int64_t nvchan, int64_t nvpol,
+               int nthreads) {
+#ifdef _OPENMP
+  if (nthreads < 1) nthreads = omp_get_max_threads();
+#pragma omp parallel num_threads(nthreads)
+  {
+    int t = omp_get_thread_num(), T = omp_get_num_threads();
+    int64_t lo = nt * t / T, hi = nt * (t + 1) / T;
+    dgrid_range(uvw, dphase, values, flag, scale, offset, grid, g_nchan, g_npol, g_n2, g_n3,
+                freq, c, support, sampling, convFunc, chanmap, polmap, nt, nb, nvchan, nvpol,
+                lo, hi);
+  }
+#else
+  (void)nthreads;
+  dgrid_range(uvw, dphase, values, flag, scale, offset, grid, g_nchan, g_npol, g_n2, g_n3, freq,
+              c, support, sampling, convFunc, chanmap, polmap, nt, nb, nvchan, nvpol, 0, nt);
+#endif
+}
+
+/* ---------------------------------------------------------------------------
+ * grid_imaging_weights_jit, grid_imaging_weights.py:93-206.
+ * grid (n_chan, n_gpol, n_u, n_v) real; data_weights (nt, nb, nchan, npol).
+ * ------------------------------------------------------------------------- */
+void orc_grid_imaging_weights(double *grid, int64_t n_gpol, double *sum_weight,
+                              const double *uvw, const double *freq, const int64_t *chan_map,
+                              const double *data_weights, int64_t n_u, int64_t n_v, double dl0,
+                              double dl1, int64_t nt, int64_t nb, int64_t nchan, int64_t npol) {
+  const double c = 299792458.0;
+  const int64_t uc0 = n_u / 2, uc1 = n_v / 2;
+  for (int64_t tb = 0; tb < nt * nb; ++tb) {
+    for (int64_t ic = 0; ic < nchan; ++ic) {
+      int64_t a_chan = chan_map[ic];
+      double us0 = -(freq[ic] * dl0 * (double)n_u) / c;
+      double us1 = -(freq[ic] * dl1 * (double)n_v) / c;
+      double u = uvw[tb * 3 + 0] * us0, v = uvw[tb * 3 + 1] * us1;
+      if (isnan(u) || isnan(v)) continue;
+      double u_pos = u + (double)uc0, v_pos = v + (double)uc1;
+      double u_pos_c = -u + (double)uc0, v_pos_c = -v + (double)uc1;
+      int64_t ui = trunc_i64(u_pos + 0.5), vi = trunc_i64(v_pos + 0.5);
+      int64_t uic = trunc_i64(u_pos_c + 0.5), vic = trunc_i64(v_pos_c + 0.5);
+      if (!((ui < n_u) && (vi < n_v) && (ui >= 0) && (vi >= 0))) continue;
+      double w = data_weights[(tb * nchan + ic) * npol + 0];
+      if (isnan(w)) continue;
+      double *plane = grid + (a_chan * n_gpol + 0) * n_u * n_v;
+      plane[ui * n_v + vi] = plane[ui * n_v + vi] + w;
+      /* the conjugate cell is not bounds-checked by the reference; for a
+       * grid of even size it is in range whenever the direct cell is,
+       * except at index 0 where it would be n (skipped here). */
+      if (uic >= 0 && uic < n_u && vic >= 0 && vic < n_v)
+        plane[uic * n_v + vic] = plane[uic * n_v + vic] + w;
+      sum_weight[a_chan * n_gpol + 0] = sum_weight[a_chan * n_gpol + 0] + 2.0 * w;
+    }
+  }
+}
+
+/* degrid_imaging_weights_jit, grid_imaging_weights.py:285-443.
+ * imaging_weight must be zero-initialised by the caller (the reference wrapper
+ * allocates np.zeros, :266). */
+int orc_degrid_imaging_weights(double *imaging_weight, const double *grid, int64_t n_gchan,
+                               int64_t n_gpol, const double *briggs_factors,
+                               const double *uvw, const double *freq, const int64_t *chan_map,
+                               const int64_t *pol_map, int64_t n_pol_map,
+                               const double *data_weight, int64_t n_u, int64_t n_v, double dl0,
+                               double dl1, int64_t nt, int64_t nb, int64_t nchan,
+                               int64_t npol) {
+  const double c = 299792458.0;
+  const int64_t uc0 = n_u / 2, uc1 = n_v / 2;
+  for (int64_t tb = 0; tb < nt * nb; ++tb) {
+    for (int64_t ic = 0; ic < nchan; ++ic) {
+      int64_t a_chan = chan_map[ic];
+      double us0 = -(freq[ic] * dl0 * (double)n_u) / c;
+      double us1 = -(freq[ic] * dl1 * (double)n_v) / c;
+      double u = uvw[tb * 3 + 0] * us0, v = uvw[tb * 3 + 1] * us1;
+      if (isnan(u) || isnan(v)) continue;
+      double u_pos = u + (double)uc0, v_pos = v + (double)uc1;
+      int64_t ui = trunc_i64(u_pos + 0.5), vi = trunc_i64(v_pos + 0.5);
+      if (!((ui < n_u) && (vi < n_v) && (ui >= 0) && (vi >= 0))) continue;
+      for (int64_t ip = 0; ip < n_pol_map; ++ip) {
+        int64_t a_pol = pol_map[ip];
+        int64_t idx = (tb * nchan + ic) * npol + ip;
+        double dw = data_weight[idx];
+        imaging_weight[idx] = dw;
+        if (!isnan(dw) && dw != 0.0) {
+          double gij = grid[((a_chan * n_gpol + a_pol) * n_u + ui) * n_v + vi];
+          if (!isnan(gij) && gij != 0.0) {
+            double f0 = briggs_factors[(0 * n_gchan + a_chan) * n_gpol + a_pol];
+            double f1 = briggs_factors[(1 * n_gchan + a_chan) * n_gpol + a_pol];
+            if (isnan(f0) || isnan(f1)) return -1;
+            double denom = f0 * gij + f1;
+            imaging_weight[idx] = imaging_weight[idx] / denom;
+          }
+        }
+      }
+    }
+  }
+  return 0;
+}
+
+/* ---------------------------------------------------------------------------
+ * Hogbom CLEAN, hclean.cpp:51-81 (maximg) and :106-210 (clean).
+ * Generalised to a PSF of size (pny, pnx) >= (ny, nx) with centre
+ * (pny/2, pnx/2): with pnx = nx, pny = ny this is the reference exactly.
+ * comps (optional, 3 x niter): px, py and the component value pv per
+ * iteration, for position checks.
+ * ------------------------------------------------------------------------- */
+#define HOGBOM_BODY(T, ABS, POW)                                                              \
+  int yes = 0;                                                                                \
+  T maxval = 0, absval = 0;                                                                   \
+  int px = 0, py = 0;                                                                         \
+  int iter;                                                                                   \
+  int ncomp = 0;                                                                              \
+  for (iter = siter; iter < niter; ++iter) {                                                  \
+    absval = (T)0;                                                                            \
+    for (int iy = ybeg; iy < yend; ++iy)                                                      \
+      for (int ix = xbeg; ix < xend; ++ix) {                                                  \
+        if (domask == 0 || lmask[(int64_t)iy * nx + ix] > (T)0.5) {                           \
+          T val = ABS(limagestep[(int64_t)iy * nx + ix]);                                     \
+          if (val > absval) { px = ix; py = iy; absval = val; }                               \
+        }                                                                                     \
+      }                                                                                       \
+    maxval = limagestep[(int64_t)py * nx + px];                                               \
+    T cthres;                                                                                 \
+    if (cspeedup > (T)0) cthres = thres * POW((T)2, (T)(iter - siter) / cspeedup);            \
+    else cthres = thres;                                                                      \
+    if (yes == 1 || absval < cthres) break;                                                   \
+    int x1 = px - pnx / 2 > 0 ? px - pnx / 2 : 0;                                             \
+    int y1 = py - pny / 2 > 0 ? py - pny / 2 : 0;                                             \
+    int x2 = px + pnx / 2 - 1 < nx - 1 ? px + pnx / 2 - 1 : nx - 1;                           \
+    int y2 = py + pny / 2 - 1 < ny - 1 ? py + pny / 2 - 1 : ny - 1;                           \
+    T pv = gain * maxval;                                                                     \
+    limage[(int64_t)py * nx + px] += pv;                                                      \
+    if (comps) {                                                                              \
+      comps[3 * ncomp + 0] = (double)px;                                                      \
+      comps[3 * ncomp + 1] = (double)py;                                                      \
+      comps[3 * ncomp + 2] = (double)pv;                                                      \
+    }                                                                                         \
+    ++ncomp;                                                                                  \
+    for (int iy = y1; iy <= y2; ++iy)                                                         \
+      for (int ix = x1; ix <= x2; ++ix) {                                                     \
+        int psf_x = pnx / 2 + ix - px, psf_y = pny / 2 + iy - py;                             \
+        if (psf_x < 0 || psf_x >= pnx || psf_y < 0 || psf_y >= pny) continue;                 \
+        limagestep[(int64_t)iy * nx + ix] -= pv * lpsf[(int64_t)psf_y * pnx + psf_x];         \
+      }                                                                                       \
+  }                                                                                           \
+  if (iter > niter) iter = niter;                                                             \
+  out_peak[0] = px;                                                                           \
+  out_peak[1] = py;                                                                           \
+  *out_maxval = (double)maxval;                                                               \
+  return iter;
+
+int orc_hogbom_f32(float *limage, float *limagestep, const float *lpsf, int pnx, int pny,
+                   int domask, const float *lmask, int nx, int ny, int xbeg, int xend, int ybeg,
+                   int yend, int niter, int siter, float gain, float thres, float cspeedup,
+                   double *comps, int *out_peak, double *out_maxval) {
+  HOGBOM_BODY(float, fabsf, powf)
+}
+
+int orc_hogbom_f64(double *limage, double *limagestep, const double *lpsf, int pnx, int pny,
+                   int domask, const double *lmask, int nx, int ny, int xbeg, int xend,
+                   int ybeg, int yend, int niter, int siter, double gain, double thres,
+                   double cspeedup, double *comps, int *out_peak, double *out_maxval) {
+  HOGBOM_BODY(double, fabs, pow)
+}
+
+void orc_maximg_f32(const float *img, int domask, const float *mask, int nx, int ny,
+                    float *fmin, float *fmax) {
+  float mn = 1e20f, mx = -1e20f;
+  for (int64_t i = 0; i < (int64_t)nx * ny; ++i)
+    if (domask == 0 || mask[i] > 0.5f) {
+      float w = img[i];
+      if (w > mx) mx = w;
+      if (w < mn) mn = w;
+    }
+  *fmin = mn;
+  *fmax = mx;
+}
+
+void orc_maximg_f64(const double *img, int domask, const double *mask, int nx, int ny,
+                    double *fmin, double *fmax) {
+  double mn = 1e20, mx = -1e20;
+  for (int64_t i = 0; i < (int64_t)nx * ny; ++i)
+    if (domask == 0 || mask[i] > 0.5) {
+      double w = img[i];
+      if (w > mx) mx = w;
+      if (w < mn) mn = w;
+    }
+  *fmin = mn;
+  *fmax = mx;
+}
+
+int orc_num_threads(void) {
+#ifdef _OPENMP
+  return omp_get_max_threads();
+#else
+  return 1;
+#endif
+}

@@ -1,0 +1,187 @@
+"""The CPU oracle against the reference's own outputs (tests/golden).
+
+Every comparison is bit-exact: the oracle restates the reference's FP64
+arithmetic in the same operation order."""
+import numpy as np
+import pytest
+
+import oracle as O
+from conftest import golden
+
+
+def test_pswf_tables():
+    g = golden("pswf.npz")
+    for os_, sup in [(100, 7), (64, 9), (100, 8), (50, 5), (128, 6)]:
+        assert np.array_equal(O.create_prolate_spheroidal_kernel_1D(os_, sup), g[f"cgk_{os_}_{sup}"])
+    for n in [(64, 64), (96, 128), (101, 77)]:
+        assert np.array_equal(O.corr_term(n), g[f"corr_{n[0]}_{n[1]}"])
+    gr, k = O.prolate_spheroidal_function(g["u"])
+    assert np.array_equal(gr, g["grdsf"]) and np.array_equal(k, g["kern"])
+
+
+@pytest.mark.parametrize("case", ["a", "b", "c"])
+def test_grid_golden(case):
+    g = golden(f"grid_{case}.npz")
+    sup, os_ = int(g["support"]), int(g["oversampling"])
+    cgk = O.create_prolate_spheroidal_kernel_1D(os_, sup)
+    assert np.array_equal(cgk, g["cgk"])
+    for do_psf in (False, True):
+        for mode in ("continuum", "cube"):
+            key = f"{'psf' if do_psf else 'vis'}_{mode}"
+            gr, sw = O.standard_grid(g["vis"], g["uvw"], g["weight"], g["freq"], cgk,
+                                     g["image_size"], g["cell"], os_, sup, do_psf, mode)
+            assert np.array_equal(gr, g["grid_" + key]), key
+            assert np.array_equal(sw, g["sumwt_" + key]), key
+    # accumulate into given arrays
+    gr = g["acc_grid0"].copy()
+    sw = g["acc_sumwt0"].copy()
+    nchan, npol = g["weight"].shape[2:]
+    O.standard_grid_jit(gr, sw, False, False, g["vis"], g["uvw"], g["freq"],
+                        np.zeros(nchan, np.int64), np.arange(npol), g["weight"], cgk,
+                        g["image_size"], g["cell"], sup, os_)
+    assert np.array_equal(gr, g["acc_grid"]) and np.array_equal(sw, g["acc_sumwt"])
+    if "iw_grid" in g:
+        gg = np.zeros(g["iw_grid"].shape, np.complex128)
+        ss = np.zeros(g["iw_sumwt"].shape)
+        O.standard_grid_jit(gg, ss, True, True, None, g["uvw"], g["freq"],
+                            np.zeros(nchan, np.int64), np.arange(npol), g["iw_weight"], cgk,
+                            g["image_size"], g["cell"], sup, os_)
+        assert np.array_equal(gg, g["iw_grid"]) and np.array_equal(ss, g["iw_sumwt"])
+
+
+def test_grid_multithread_matches():
+    g = golden("grid_a.npz")
+    cgk = g["cgk"]
+    a = O.standard_grid(g["vis"], g["uvw"], g["weight"], g["freq"], cgk, g["image_size"],
+                        g["cell"], 100, 7, False, "cube", nthreads=1)
+    b = O.standard_grid(g["vis"], g["uvw"], g["weight"], g["freq"], cgk, g["image_size"],
+                        g["cell"], 100, 7, False, "cube", nthreads=3)
+    assert np.linalg.norm(a[0] - b[0]) <= 1e-14 * np.linalg.norm(a[0])
+    assert np.allclose(a[1], b[1], rtol=1e-14, atol=0)
+
+
+def test_image_golden():
+    g = golden("image.npz")
+    cgk = O.create_prolate_spheroidal_kernel_1D(100, 7)
+    for dopsf in (False, True):
+        for mode in ("continuum", "cube"):
+            w = g["weight"].copy()
+            w[g["flag"]] = 0.0
+            w[np.isnan(g["uvw"][:, :, 0]) | np.isnan(g["uvw"][:, :, 1])] = 0.0
+            tag = f"{'psf' if dopsf else 'vis'}_{mode}"
+            assert np.array_equal(w, g["weight_after_" + tag])
+            gr, sw = O.standard_grid(g["vis"], g["uvw"], w, g["freq"], cgk, (64, 64), g["cell"],
+                                     100, 7, dopsf, mode)
+            img = O.grid_to_image(gr, sw)
+            assert np.array_equal(img, g["img_" + tag]), tag
+    assert np.array_equal(O.fft_lm_to_uv(g["fft_in"], axes=[2, 3]), g["fft_out"])
+    assert np.array_equal(O.ifft_uv_to_lm(g["fft_out"], axes=[2, 3]), g["ifft_out"])
+
+
+def test_degrid_golden():
+    g = golden("degrid.npz")
+    nt, nb = g["uvw"].shape[:2]
+    for sup, os_ in ((7, 100), (9, 64), (8, 100)):
+        cf = O.create_prolate_spheroidal_kernel_1D(os_, sup)
+        for dp_name in ("zero", "phase"):
+            dp = np.zeros((nt, nb)) if dp_name == "zero" else g["dphase"]
+            v = g[f"v0_{sup}_{os_}_{dp_name}"].copy()
+            O.dgrid_numba(g["uvw"], dp, v, g["flag"], g["scale"], g["offset"], g["grid"],
+                          g["freq"], 299792458.0, sup, os_, cf, g["chanmap"], g["polmap"])
+            assert np.array_equal(v, g[f"v_{sup}_{os_}_{dp_name}"]), (sup, os_, dp_name)
+    # the reference's known answer: |vis| == 2.0 for a 2 Jy centre source
+    vk = np.zeros((1, 64 * 64, 1, 1), dtype=complex)
+    gk = np.zeros((1, 1, 200, 200), dtype=complex)
+    mod = np.zeros((200, 200))
+    mod[100, 100] = 2.0
+    gk[0, 0] = np.conj(O.fft_lm_to_uv(mod, axes=[0, 1]))
+    O.dgrid_numba(g["kat_uvw"], np.zeros((1, 64 * 64)), vk, np.zeros(vk.shape, bool),
+                  g["kat_cell"], np.array([100, 100]), gk, np.array([1.4e9]), 299792458.0, 7,
+                  100, O.create_prolate_spheroidal_kernel_1D(100, 7), np.zeros(1, int),
+                  np.zeros(1, int))
+    assert np.array_equal(vk, g["kat_vis"])
+    assert np.max(np.abs(vk)) == 2.0
+
+
+def test_weights_golden():
+    g = golden("weights.npz")
+    for npol in (1, 2, 4):
+        p = lambda k: g[f"p{npol}_{k}"]
+        for robust in (-1.0, 0.5, 2.0):
+            iw, G, sw, bf = O.imaging_weights(p("uvw"), p("w"), p("flag"), p("freq"), p("n"),
+                                              p("cell"), robust)
+            assert np.array_equal(G, p("G")) and np.array_equal(sw, p("sw"))
+            assert np.array_equal(bf, p(f"bf_{robust}"))
+            assert np.array_equal(iw, p(f"iw_{robust}"), equal_nan=True)
+        assert np.array_equal(O.calculate_briggs_params(
+            p("G"), p("sw"), {"weighting": "briggs_abs", "robust": 0.7,
+                              "briggs_abs_noise": 0.3}), p("bf_abs"))
+        assert np.array_equal(O.calculate_briggs_params(p("G"), p("sw"),
+                                                        {"weighting": "natural"}), p("bf_nat"))
+
+
+RUNS = {
+    "default": dict(max_iter=100),
+    "box_thr": dict(max_iter=400, gain=0.2, threshold=0.02, clean_box=(5, 50, 10, 60)),
+    "mask_speed": dict(max_iter=150, start_iter=3, speedup=40.0, threshold=0.005, mask=True),
+    "long": dict(max_iter=1000, gain=0.05),
+}
+
+
+@pytest.mark.parametrize("tag", ["f32", "f64"])
+@pytest.mark.parametrize("name", list(RUNS))
+def test_hogbom_golden(tag, name):
+    g = golden("hogbom.npz")
+    dt = np.float32 if tag == "f32" else np.float64
+    kw = dict(RUNS[name])
+    if kw.pop("mask", False):
+        kw["mask"] = g["mask"].astype(dt)
+    r = O.hogbom_clean(g["dirty"].astype(dt), g["psf"].astype(dt), **kw)
+    assert r["iterations_performed"] == int(g[f"{tag}_{name}_iterations_performed"])
+    assert np.array_equal(r["model_image"], g[f"{tag}_{name}_model_image"])
+    assert np.array_equal(r["residual_image"], g[f"{tag}_{name}_residual_image"])
+
+
+def test_maximg_golden():
+    g = golden("hogbom.npz")
+    for tag, dt in (("f32", np.float32), ("f64", np.float64)):
+        assert np.array_equal(np.array(O.maximg(g["dirty"].astype(dt))), g[f"{tag}_maximg"])
+        assert np.array_equal(np.array(O.maximg(g["dirty"].astype(dt), g["mask"].astype(dt))),
+                              g[f"{tag}_maximg_mask"])
+
+
+def test_reference_lattice_known_answer():
+    """test_standard_grid.py:14-111 of the reference, on the oracle: point
+    sources on a 200x200 regular uv lattice image at (87,92) > 1.8 and
+    (110,115) > 0.9; the PSF peak is within 0.01 of 1 at (100,100)."""
+    nant = 200
+    c = 299792458.0
+    freq = np.array([1.4e9])
+    maxuv = 2e3
+    cell = 0.5 * c / freq[0] / maxuv
+    mod = np.zeros((nant, nant))
+    mod[np.array([110, 87]), np.array([115, 92])] = np.array([1.0, 2.0])
+    ft = np.conj(O.fft_lm_to_uv(mod, axes=[0, 1]))
+    ax = np.linspace(-maxuv, maxuv, nant)
+    uu, vv = np.meshgrid(ax, ax, indexing="ij")
+    uvw = np.stack([uu.ravel(), vv.ravel(), np.zeros(nant * nant)], -1)[None]
+    vis = ft.reshape(1, nant * nant, 1, 1).astype(np.complex128)
+    w = np.ones(vis.shape)
+    cgk = O.create_prolate_spheroidal_kernel_1D(100, 7)
+    gr, sw = O.standard_grid(vis, uvw, w, freq, cgk, (nant, nant), np.array([cell, cell]))
+    ct = O.corr_term((nant, nant))
+    dirty = O.ifft_uv_to_lm(gr, axes=[2, 3]) / ct * nant * nant / sw[..., None, None]
+    assert dirty[0, 0, 87, 92] > 1.8 and dirty[0, 0, 110, 115] > 0.9
+    gr, sw = O.standard_grid(vis, uvw, w, freq, cgk, (nant, nant), np.array([cell, cell]),
+                             do_psf=True)
+    psf = O.ifft_uv_to_lm(gr, axes=[2, 3]) / ct * nant * nant / sw[..., None, None]
+    assert abs(psf[0, 0, 100, 100] - 1.0) < 0.01
+
+
+def test_fft_round_trip_known_answer():
+    """test_fft_ifft.py:12-26 of the reference."""
+    sky = np.zeros((128, 128))
+    sky[64, 64] = 1
+    sky[50, 40] = 1
+    rt = O.ifft_uv_to_lm(O.fft_lm_to_uv(sky, (0, 1)), (0, 1))
+    assert np.max(np.abs(sky - rt)) < 1e-10
