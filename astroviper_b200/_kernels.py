@@ -1,0 +1,357 @@
+"""Device-tensor front end of libav200: one function per C-ABI entry point.
+
+All tensors are CUDA tensors (C-contiguous); results stay on the device.  The
+numpy/xarray drop-in modules under ``astroviper_b200.core`` stage host arrays
+through these functions.  Scratch space comes from torch's caching allocator
+and is handed to the library as (pointer, bytes).
+"""
+import math
+
+import torch
+
+from . import _lib
+from ._lib import AV_C64, AV_C128, AV_F32, AV_F64, check, lib
+
+C_LIGHT = 299792458.0
+
+_DT = {torch.float32: AV_F32, torch.float64: AV_F64, torch.complex64: AV_C64,
+       torch.complex128: AV_C128}
+
+
+def require_gpu():
+    if not torch.cuda.is_available():
+        raise RuntimeError("astroviper_b200 needs a CUDA device (B200, sm_100a); none is visible")
+    lib()
+
+
+def device():
+    require_gpu()
+    return torch.device("cuda", torch.cuda.current_device())
+
+
+def stream_ptr():
+    return torch.cuda.current_stream().cuda_stream
+
+
+def dcode(t):
+    try:
+        return _DT[t.dtype]
+    except KeyError:
+        raise TypeError(f"unsupported dtype {t.dtype}") from None
+
+
+def p(t):
+    """Device pointer of a tensor (None passes NULL)."""
+    if t is None:
+        return None
+    assert t.is_cuda and t.is_contiguous(), "expected a contiguous CUDA tensor"
+    return t.data_ptr()
+
+
+def workspace(nbytes):
+    """Scratch buffer (256-byte aligned) from torch's caching allocator."""
+    n = int(max(nbytes, 256))
+    buf = torch.empty(n + 256, dtype=torch.uint8, device=device())
+    off = (-buf.data_ptr()) % 256
+    return buf, buf.data_ptr() + off, n
+
+
+def on_device(x, dtype=None):
+    """Contiguous CUDA tensor from a tensor or array-like."""
+    dev = device()
+    if isinstance(x, torch.Tensor):
+        t = x.to(device=dev, dtype=dtype or x.dtype, non_blocking=True)
+    else:
+        t = torch.as_tensor(x, dtype=dtype, device=dev)
+    return t.contiguous()
+
+
+# --------------------------------------------------------------------- PSWF --
+def pswf(u):
+    u = on_device(u, torch.float64)
+    g = torch.empty_like(u)
+    k = torch.empty_like(u)
+    check(lib().av_pswf(p(u), u.numel(), p(g), p(k), stream_ptr()), "av_pswf")
+    return g, k
+
+
+def pswf_table(oversampling, support):
+    out = torch.empty(oversampling * (support // 2 + 1), dtype=torch.float64, device=device())
+    check(lib().av_pswf_table(p(out), int(oversampling), int(support), stream_ptr()),
+          "av_pswf_table")
+    return out
+
+
+def corr_term(nx, ny):
+    out = torch.empty((int(nx), int(ny)), dtype=torch.float64, device=device())
+    check(lib().av_corr_term(p(out), int(nx), int(ny), stream_ptr()), "av_corr_term")
+    return out
+
+
+def pswf_kernel4d(oversampling, support):
+    n_os = oversampling + 1 if oversampling % 2 == 0 else oversampling
+    out = torch.empty((n_os, n_os, support, support), dtype=torch.float64, device=device())
+    check(lib().av_pswf_kernel4d(p(out), int(oversampling), int(support), stream_ptr()),
+          "av_pswf_kernel4d")
+    return out
+
+
+# ----------------------------------------------------------------- gridding --
+def grid(vis, weight, uvw, freq, chan_map, pol_map, cgk, n_uv, delta_lm, support,
+         oversampling, n_img_chan, n_img_pol, grid_out=None, sum_weight=None, do_psf=False,
+         do_imaging_weight=False, precision="fp32"):
+    """Accumulate samples into grid_out / sum_weight (allocated when None).
+
+    precision "fp32": the tiled kernel (reads complex64 visibilities and
+    float32 weights, accumulates in FP64; complex128 grid unless a complex64
+    grid is passed); "fp64": the plain FP64 kernel (FP64 inputs, every option
+    of the reference, complex128 grid)."""
+    dev = device()
+    nu, nv = int(n_uv[0]), int(n_uv[1])
+    nt, nb = int(uvw.shape[0]), int(uvw.shape[1])
+    nchan, npol = int(weight.shape[2]), int(weight.shape[3])
+    uvw = on_device(uvw, torch.float64)
+    freq = on_device(freq, torch.float64)
+    cm = on_device(chan_map, torch.int32)
+    pm = on_device(pol_map, torch.int32)
+    cgk = on_device(cgk, torch.float64)
+    fp64 = precision == "fp64" or do_imaging_weight or support > 9 or support < 3 \
+        or oversampling > 254 or npol > 4 or n_img_pol > 4
+    if grid_out is None:
+        grid_out = torch.zeros((n_img_chan, n_img_pol, nu, nv), dtype=torch.complex128,
+                               device=dev)
+    if sum_weight is None:
+        sum_weight = torch.zeros((n_img_chan, n_img_pol), dtype=torch.float64, device=dev)
+    assert grid_out.is_contiguous() and sum_weight.is_contiguous()
+    if fp64:
+        w = on_device(weight)
+        if w.dtype not in (torch.float32, torch.float64):
+            w = w.to(torch.float64)
+        v = None if do_psf else on_device(vis)
+        if v is not None and v.dtype not in (torch.complex64, torch.complex128):
+            v = v.to(torch.complex128)
+        rc = lib().av_grid_plain(
+            p(grid_out), dcode(grid_out), p(sum_weight), int(bool(do_psf)),
+            int(bool(do_imaging_weight)), p(v), dcode(v) if v is not None else AV_C128, p(w),
+            dcode(w), p(uvw), p(freq), p(cm), p(pm), p(cgk), nu, nv, float(delta_lm[0]),
+            float(delta_lm[1]), int(support), int(oversampling), nt, nb, nchan, npol,
+            int(n_img_chan), int(n_img_pol), stream_ptr())
+        check(rc, "av_grid_plain")
+        return grid_out, sum_weight
+    w = on_device(weight, torch.float32)
+    v = None if do_psf else on_device(vis, torch.complex64)
+    ws_bytes = lib().av_grid_tiled_workspace_size(nt, nb, nchan, nu, nv, int(n_img_chan),
+                                                  int(support))
+    _buf, wptr, wbytes = workspace(ws_bytes)
+    rc = lib().av_grid_tiled(
+        p(grid_out), dcode(grid_out), p(sum_weight), int(bool(do_psf)), p(v), AV_C64, p(w),
+        AV_F32, p(uvw), p(freq), p(cm), p(pm), p(cgk), nu, nv, float(delta_lm[0]),
+        float(delta_lm[1]), int(support), int(oversampling), nt, nb, nchan, npol,
+        int(n_img_chan), int(n_img_pol), wptr, wbytes, stream_ptr())
+    check(rc, "av_grid_tiled")
+    return grid_out, sum_weight
+
+
+def degrid(grid_t, uvw, freq, scale, offset, chanmap, polmap, cgk, support, sampling,
+           values=None, flag=None, dphase=None, c=C_LIGHT, nvchan=None, nvpol=None,
+           precision="fp32"):
+    """values (nt, nb, nvchan, nvpol) += degridded model (allocated as zeros of
+    complex64 / complex128 when None)."""
+    dev = device()
+    g = on_device(grid_t)
+    if g.dtype not in (torch.complex64, torch.complex128):
+        g = g.to(torch.complex128)
+    nt, nb = int(uvw.shape[0]), int(uvw.shape[1])
+    if values is not None:
+        nvchan, nvpol = int(values.shape[2]), int(values.shape[3])
+    uvw = on_device(uvw, torch.float64)
+    freq = on_device(freq, torch.float64)
+    cm = on_device(chanmap, torch.int32)
+    pm = on_device(polmap, torch.int32)
+    cgk = on_device(cgk, torch.float64)
+    fl = None if flag is None else on_device(flag).to(torch.uint8).contiguous()
+    dph = None if dphase is None else on_device(dphase, torch.float64)
+    g_nchan, g_npol, g_n2, g_n3 = (int(s) for s in g.shape)
+    tiled_ok = (precision != "fp64" and 3 <= support <= 9 and sampling <= 254 and g_npol <= 4
+                and float(c) == C_LIGHT)
+    if values is None:
+        vdt = torch.complex64 if tiled_ok else torch.complex128
+        values = torch.zeros((nt, nb, nvchan, nvpol), dtype=vdt, device=dev)
+    assert values.is_contiguous()
+    args_common = (p(uvw), p(dph), p(values), dcode(values), p(fl), float(scale[0]),
+                   float(scale[1]), float(offset[0]), float(offset[1]))
+    if not tiled_ok:
+        rc = lib().av_degrid_plain(*args_common, p(g), dcode(g), g_nchan, g_npol, g_n2, g_n3,
+                                   p(freq), float(c), int(support), int(sampling), p(cgk), p(cm),
+                                   p(pm), nt, nb, nvchan, nvpol, stream_ptr())
+        check(rc, "av_degrid_plain")
+        return values
+    if g.dtype == torch.complex128:
+        g = g.to(torch.complex64)
+    ws_bytes = lib().av_degrid_tiled_workspace_size(nt, nb, nvchan, g_n2, g_n3, g_nchan,
+                                                    int(support))
+    _buf, wptr, wbytes = workspace(ws_bytes)
+    rc = lib().av_degrid_tiled(*args_common, p(g), dcode(g), g_nchan, g_npol, g_n2, g_n3,
+                               p(freq), float(c), int(support), int(sampling), p(cgk), p(cm),
+                               p(pm), nt, nb, nvchan, nvpol, wptr, wbytes, stream_ptr())
+    check(rc, "av_degrid_tiled")
+    return values
+
+
+# ------------------------------------------------------------------- images --
+def grid_to_image(grid_t, sum_weight=None, apply_corr=True, out_dtype=None):
+    """Re(fftshift(ifft2(ifftshift(grid)))) / corrTerm * nx*ny / sum_weight per
+    plane of a (..., nx, ny) complex grid."""
+    g = on_device(grid_t)
+    if g.dtype not in (torch.complex64, torch.complex128):
+        g = g.to(torch.complex128)
+    nx, ny = int(g.shape[-2]), int(g.shape[-1])
+    npl = int(g.numel() // (nx * ny))
+    if out_dtype is None:
+        out_dtype = torch.float32 if g.dtype == torch.complex64 else torch.float64
+    img = torch.empty(g.shape, dtype=out_dtype, device=g.device)
+    sw = None
+    if sum_weight is not None:
+        sw = on_device(sum_weight, torch.float64).reshape(-1)
+        assert sw.numel() == npl
+    ws = lib().av_grid_to_image_workspace_size(npl, nx, ny)
+    _buf, wptr, wbytes = workspace(ws)
+    check(lib().av_grid_to_image(p(g), dcode(g), p(sw), p(img), dcode(img), npl, nx, ny,
+                                 int(bool(apply_corr)), wptr, wbytes, stream_ptr()),
+          "av_grid_to_image")
+    return img
+
+
+def fft_shifted(x, inverse):
+    """fftshift(fft2 / ifft2(ifftshift(x))) over the last two axes (complex)."""
+    t = on_device(x)
+    if not t.is_complex():
+        t = t.to(torch.complex128 if t.dtype == torch.float64 else torch.complex64)
+    nx, ny = int(t.shape[-2]), int(t.shape[-1])
+    npl = int(t.numel() // max(1, nx * ny))
+    out = torch.empty_like(t)
+    ws = lib().av_fft_workspace_size(npl, nx, ny, dcode(t))
+    _buf, wptr, wbytes = workspace(ws)
+    check(lib().av_fft_shifted(p(t), p(out), dcode(t), npl, nx, ny, int(bool(inverse)), wptr,
+                               wbytes, stream_ptr()), "av_fft_shifted")
+    return out
+
+
+# ------------------------------------------------------------------ weights --
+def weight_density(uvw, freq, weight, flag, n_uv, delta_lm, density=None, sum_weight=None):
+    """Nearest-cell weight-density grid (nchan, 1, nu, nv) and sum_weight."""
+    dev = device()
+    nt, nb, nchan, npol = (int(s) for s in weight.shape)
+    nu, nv = int(n_uv[0]), int(n_uv[1])
+    w = on_device(weight)
+    if w.dtype not in (torch.float32, torch.float64):
+        w = w.to(torch.float64)
+    fl = None if flag is None else on_device(flag).to(torch.uint8).contiguous()
+    if density is None:
+        density = torch.zeros((nchan, 1, nu, nv), dtype=torch.float64, device=dev)
+    if sum_weight is None:
+        sum_weight = torch.zeros((nchan, 1), dtype=torch.float64, device=dev)
+    # device copies are held in locals until the launch: a temporary freed
+    # right after taking its pointer could be handed to the next one
+    uvw_d = on_device(uvw, torch.float64)
+    freq_d = on_device(freq, torch.float64)
+    check(lib().av_weight_density(p(density), p(sum_weight), p(uvw_d),
+                                  p(freq_d), p(w), dcode(w), p(fl), nu,
+                                  nv, float(delta_lm[0]), float(delta_lm[1]), nt, nb, nchan,
+                                  npol, stream_ptr()), "av_weight_density")
+    return density, sum_weight
+
+
+def briggs_factors(density, sum_weight, robust):
+    d = on_device(density, torch.float64)
+    sw = on_device(sum_weight, torch.float64)
+    npl = int(d.shape[0] * d.shape[1])
+    nu, nv = int(d.shape[2]), int(d.shape[3])
+    out = torch.empty((2,) + tuple(sw.shape), dtype=torch.float64, device=d.device)
+    _buf, wptr, wbytes = workspace(lib().av_briggs_factors_workspace_size(npl))
+    check(lib().av_briggs_factors(p(d), p(sw), p(out), npl, nu, nv, float(robust), wptr, wbytes,
+                                  stream_ptr()), "av_briggs_factors")
+    return out
+
+
+def briggs_apply(density, factors, uvw, freq, weight, flag, n_uv, delta_lm,
+                 out_dtype=torch.float64):
+    nt, nb, nchan, npol = (int(s) for s in weight.shape)
+    w = on_device(weight)
+    if w.dtype not in (torch.float32, torch.float64):
+        w = w.to(torch.float64)
+    fl = None if flag is None else on_device(flag).to(torch.uint8).contiguous()
+    out = torch.empty((nt, nb, nchan, npol), dtype=out_dtype, device=w.device)
+    err = torch.zeros(1, dtype=torch.int32, device=w.device)
+    dens_d = on_device(density, torch.float64)
+    fac_d = on_device(factors, torch.float64)
+    uvw_d = on_device(uvw, torch.float64)
+    freq_d = on_device(freq, torch.float64)
+    check(lib().av_briggs_apply(p(out), dcode(out), p(dens_d), p(fac_d), p(uvw_d), p(freq_d),
+                                p(w), dcode(w), p(fl),
+                                int(n_uv[0]), int(n_uv[1]), float(delta_lm[0]),
+                                float(delta_lm[1]), nt, nb, nchan, npol, p(err), stream_ptr()),
+          "av_briggs_apply")
+    return out, err
+
+
+# ------------------------------------------------------------------- Hogbom --
+def maximg(image, mask=None):
+    im = on_device(image)
+    m = None if mask is None else on_device(mask, im.dtype)
+    out = torch.empty(2, dtype=im.dtype, device=im.device)
+    ny, nx = int(im.shape[0]), int(im.shape[1])
+    check(lib().av_maximg(p(im), p(m), dcode(im), nx, ny, p(out), stream_ptr()), "av_maximg")
+    return out
+
+
+def abs_sum_ordered(x):
+    t = on_device(x)
+    out = torch.empty(1, dtype=t.dtype, device=t.device)
+    n = t.numel()
+    _buf, wptr, wbytes = workspace(lib().av_abs_sum_workspace_size(n, dcode(t)))
+    check(lib().av_abs_sum_ordered(p(t), dcode(t), n, p(out), wptr, wbytes, stream_ptr()),
+          "av_abs_sum_ordered")
+    return out
+
+
+class HogbomRun:
+    """Device state of one Hogbom CLEAN run (residual, model, PSF)."""
+
+    def __init__(self, dirty, psf, mask=None, box=None, niter=100, siter=0, gain=0.1,
+                 threshold=0.0, speedup=0.0):
+        self.resid = on_device(dirty).clone()
+        self.dtype = self.resid.dtype
+        assert self.dtype in (torch.float32, torch.float64)
+        self.psf = on_device(psf, self.dtype)
+        self.mask = None if mask is None else on_device(mask, self.dtype)
+        self.model = torch.zeros_like(self.resid)
+        self.ny, self.nx = (int(s) for s in self.resid.shape)
+        self.pny, self.pnx = (int(s) for s in self.psf.shape)
+        self.box = box if box is not None else (0, self.nx, 0, self.ny)
+        self.niter, self.siter = int(niter), int(siter)
+        self.gain, self.threshold, self.speedup = float(gain), float(threshold), float(speedup)
+        self.state = torch.zeros(int(lib().av_hogbom_state_size()) // 8, dtype=torch.float64,
+                                 device=self.resid.device)
+        self._ws = workspace(lib().av_hogbom_workspace_size(self.nx, self.ny, dcode(self.resid)))
+        self.started = False
+
+    def run(self, iter_begin, iter_end):
+        xb, xe, yb, ye = self.box
+        init = 0 if self.started else 1
+        _buf, wptr, wbytes = self._ws
+        check(lib().av_hogbom_run(p(self.model), p(self.resid), p(self.psf), p(self.mask),
+                                  dcode(self.resid), self.nx, self.ny, self.pnx, self.pny, xb, xe,
+                                  yb, ye, self.niter, self.siter, int(iter_begin), int(iter_end),
+                                  self.gain, self.threshold, self.speedup, p(self.state), init,
+                                  wptr, wbytes, stream_ptr()), "av_hogbom_run")
+        self.started = True
+
+    def read_state(self):
+        import ctypes
+        oi = (ctypes.c_int32 * 5)()
+        od = (ctypes.c_double * 2)()
+        check(lib().av_hogbom_state_read(p(self.state), oi, od, stream_ptr()),
+              "av_hogbom_state_read")
+        return dict(iter=oi[0], px=oi[1], py=oi[2], stopped=oi[3], err=oi[4], peak=od[0],
+                    absval=od[1])

@@ -1,0 +1,158 @@
+// Error reporting, version, device queries and the PSWF tables.
+#include <stdarg.h>
+#include <string.h>
+
+#include <atomic>
+
+#include "common.cuh"
+
+namespace av {
+
+static thread_local char g_err[1024] = "";
+
+void set_error(const char *fmt, ...) {
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(g_err, sizeof(g_err), fmt, ap);
+  va_end(ap);
+}
+
+void clear_error() { g_err[0] = 0; }
+
+static std::atomic<unsigned long long> g_launches{0};
+void count_launch() { g_launches.fetch_add(1, std::memory_order_relaxed); }
+
+int sm_count() {
+  static int cache[64] = {0};
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess) return 148;
+  if (dev < 0 || dev >= 64) return 148;
+  if (cache[dev] == 0) {
+    int n = 0;
+    if (cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || n <= 0)
+      n = 148;
+    cache[dev] = n;
+  }
+  return cache[dev];
+}
+
+// grdsf and (1-u^2) grdsf of gcf_prolate_spheroidal.py:102-158.
+__global__ void k_pswf(const double *__restrict__ u, int64_t n, double *grdsf, double *kern) {
+  int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  double x = fabs(u[i]);
+  double g = pswf_grdsf(x);
+  if (grdsf) grdsf[i] = g;
+  if (kern) kern[i] = __dmul_rn(__dsub_rn(1.0, __dmul_rn(x, x)), g);
+}
+
+// create_prolate_spheroidal_kernel_1D (gcf_prolate_spheroidal.py:87-99).
+__global__ void k_pswf_table(double *out, int os, int sc) {
+  int64_t n = (int64_t)os * sc, ntot = (int64_t)os * (sc + 1);
+  int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (i >= ntot) return;
+  if (i >= n) {
+    out[i] = 0.0;
+    return;
+  }
+  double u = __ddiv_rn((double)i, (double)(sc * os));
+  double g = pswf_grdsf(u);
+  out[i] = __dmul_rn(__dsub_rn(1.0, __dmul_rn(u, u)), g);
+}
+
+// corrTerm of gcf_prolate_spheroidal.py:73-79 with coordinates() (:161).
+__global__ void k_corr_term(double *out, int64_t nx, int64_t ny) {
+  int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (k >= nx * ny) return;
+  int64_t i = k / ny, j = k - i * ny;
+  double cx = __ddiv_rn((double)(i - nx / 2), (double)nx);
+  double cy = __ddiv_rn((double)(j - ny / 2), (double)ny);
+  double gx = pswf_grdsf(fabs(__dmul_rn(2.0, cx)));
+  double gy = pswf_grdsf(fabs(__dmul_rn(2.0, cy)));
+  out[k] = __dmul_rn(gx, gy);
+}
+
+// The 4-D kernel of create_prolate_spheroidal_kernel (gcf:28-67):
+// kernel[x, y, :, :] = outer(k1[x, :], k1[y, :]) for x, y < oversampling with
+// k1[o, s] = (1-u^2) grdsf(u), u = ((s - sc) + (o - oc)/os) / sc; the last
+// row/column (index os, even oversampling only) stays zero as in the loop
+// bounds of the reference.
+__global__ void k_pswf_kernel4d(double *out, int os, int support, int n_os) {
+  int64_t total = (int64_t)n_os * n_os * support * support;
+  int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (k >= total) return;
+  int s2 = (int)(k % support);
+  int64_t r = k / support;
+  int s1 = (int)(r % support);
+  r /= support;
+  int y = (int)(r % n_os);
+  int x = (int)(r / n_os);
+  if (x >= os || y >= os) {
+    out[k] = 0.0;
+    return;
+  }
+  int sc = support / 2, oc = os / 2;
+  double ox = __ddiv_rn((double)(x - oc), (double)os);
+  double oy = __ddiv_rn((double)(y - oc), (double)os);
+  double ux = __ddiv_rn(__dadd_rn((double)(s1 - sc), ox), (double)sc);
+  double uy = __ddiv_rn(__dadd_rn((double)(s2 - sc), oy), (double)sc);
+  double kx = __dmul_rn(__dsub_rn(1.0, __dmul_rn(ux, ux)), pswf_grdsf(fabs(ux)));
+  double ky = __dmul_rn(__dsub_rn(1.0, __dmul_rn(uy, uy)), pswf_grdsf(fabs(uy)));
+  out[k] = __dmul_rn(kx, ky);
+}
+
+}  // namespace av
+
+using namespace av;
+
+extern "C" {
+
+int av_version(void) { return 100; }
+
+const char *av_last_error(void) { return g_err; }
+
+int av_device_sm_count(void) { return sm_count(); }
+
+unsigned long long av_launch_count(void) { return g_launches.load(); }
+
+int av_pswf(const double *u_in, int64_t n, double *grdsf, double *kern, void *stream) {
+  clear_error();
+  AV_CHECK_ARG(n >= 0 && (n == 0 || u_in), "av_pswf: bad input");
+  if (n == 0) return AV_OK;
+  k_pswf<<<(unsigned)((n + 255) / 256), 256, 0, as_stream(stream)>>>(u_in, n, grdsf, kern);
+  AV_LAUNCH_CHECK();
+  return AV_OK;
+}
+
+int av_pswf_table(double *out, int oversampling, int support, void *stream) {
+  clear_error();
+  AV_CHECK_ARG(out && oversampling > 0 && support >= 2, "av_pswf_table: bad arguments");
+  int sc = support / 2;
+  int64_t ntot = (int64_t)oversampling * (sc + 1);
+  k_pswf_table<<<(unsigned)((ntot + 255) / 256), 256, 0, as_stream(stream)>>>(out, oversampling,
+                                                                              sc);
+  AV_LAUNCH_CHECK();
+  return AV_OK;
+}
+
+int av_corr_term(double *out, int64_t nx, int64_t ny, void *stream) {
+  clear_error();
+  AV_CHECK_ARG(out && nx > 0 && ny > 0, "av_corr_term: bad arguments");
+  int64_t n = nx * ny;
+  k_corr_term<<<(unsigned)((n + 255) / 256), 256, 0, as_stream(stream)>>>(out, nx, ny);
+  AV_LAUNCH_CHECK();
+  return AV_OK;
+}
+
+int av_pswf_kernel4d(double *out, int oversampling, int support, void *stream) {
+  clear_error();
+  AV_CHECK_ARG(out && oversampling > 0 && support >= 2, "av_pswf_kernel4d: bad arguments");
+  int n_os = (oversampling % 2 == 0) ? oversampling + 1 : oversampling;
+  int64_t total = (int64_t)n_os * n_os * support * support;
+  k_pswf_kernel4d<<<(unsigned)((total + 255) / 256), 256, 0, as_stream(stream)>>>(
+      out, oversampling, support, n_os);
+  AV_LAUNCH_CHECK();
+  return AV_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,501 @@
+// Convolutional degridding (dgrid_numba, standard_degrid.py:388-485).
+//
+// av_degrid_plain: one thread per (sample, polarisation), FP64, the
+//   reference's tap order and summation order: bit-identical to it.
+// av_degrid_tiled: FP32 over a cell-sorted plan (plan.cuh).  Each CTA stages
+//   a tile's sub-grid (all image polarisations) in shared memory and gives
+//   one record to each thread; consecutive threads hold samples of the same
+//   cell, so the sub-grid reads are broadcasts.  The separable kernel is
+//   applied as row sums (sum_j cv_j G_ij, then sum_i cu_i row_i) with packed
+//   FP32 FMAs; the normalisation sum_k w_k is (sum_i cu_i)(sum_j cv_j) from
+//   FP64 per-offset row sums.
+#include "plan.cuh"
+
+namespace av {
+
+struct DegridArgs {
+  const double *uvw, *dphase;
+  void *values;
+  int values_c128;
+  const uint8_t *flag;
+  double scale0, scale1, offset0, offset1;
+  const void *grid;
+  int grid_c128;
+  int64_t g_nchan, g_npol, g_n2, g_n3;
+  const double *freq;
+  double c;
+  int support, sampling;
+  const double *cf;
+  const int32_t *chanmap, *polmap;
+  int64_t nt, nb, nvchan, nvpol;
+};
+
+// ---------------------------------------------------------------- plain ----
+__global__ void __launch_bounds__(256) k_degrid_plain(DegridArgs a) {
+  int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  int64_t total = a.nt * a.nb * a.nvchan * a.nvpol;
+  if (k >= total) return;
+  int64_t row = k / a.nvpol;
+  int ipol = (int)(k - row * a.nvpol);
+  int64_t tb = row / a.nvchan;
+  int ichan = (int)(row - tb * a.nvchan);
+  int apol = a.polmap[ipol];
+  if (!(0 <= apol && apol < a.g_npol)) return;
+  int achan = a.chanmap[ichan];
+  if (!(0 <= achan && achan < a.g_nchan)) return;
+  if (a.flag && a.flag[k]) return;
+  const double f = a.freq[ichan];
+  double p0 = __dadd_rn(__ddiv_rn(__dmul_rn(__dmul_rn(a.scale0, a.uvw[3 * tb]), f), a.c), a.offset0);
+  double p1 = __dadd_rn(__ddiv_rn(__dmul_rn(__dmul_rn(a.scale1, a.uvw[3 * tb + 1]), f), a.c), a.offset1);
+  int x0 = (int)(unsigned)(unsigned long long)trunc_ll(rint(p0));
+  int y0 = (int)(unsigned)(unsigned long long)trunc_ll(rint(p1));
+  int o0 = (int)(unsigned)(unsigned long long)trunc_ll(rint(__dmul_rn(__dsub_rn((double)x0, p0), (double)a.sampling)));
+  int o1 = (int)(unsigned)(unsigned long long)trunc_ll(rint(__dmul_rn(__dsub_rn((double)y0, p1), (double)a.sampling)));
+  const long long beg = -(a.support / 2), end = beg + a.support;
+  // the reference's nx = shape[3], ny = shape[2] (standard_degrid.py:407)
+  if (!(((long long)x0 + beg >= 0) && ((long long)x0 + end - 1 < a.g_n3) &&
+        ((long long)y0 + beg >= 0) && ((long long)y0 + end - 1 < a.g_n2)))
+    return;
+  if (!((long long)x0 + end - 1 < a.g_n2 && (long long)y0 + end - 1 < a.g_n3)) return;
+  double ph_re = 1.0, ph_im = 0.0;
+  double phase = 0.0;
+  if (a.dphase) {
+    phase = __ddiv_rn(__dmul_rn(__dmul_rn(-2.0 * 3.141592653589793, a.dphase[tb]), f), a.c);
+    sincos(phase, &ph_im, &ph_re);
+  } else {
+    phase = __ddiv_rn(__dmul_rn(__dmul_rn(-2.0 * 3.141592653589793, 0.0), f), a.c);
+    ph_re = 1.0;
+    ph_im = phase;  // sin(+-0) = +-0
+  }
+  double nv_re = 0.0, nv_im = 0.0, norm = 0.0;
+  const int64_t plane = ((int64_t)achan * a.g_npol + apol) * a.g_n2 * a.g_n3;
+  for (long long ix = beg; ix < end; ++ix) {
+    long long i1 = (long long)a.sampling * ix + o0;
+    double wtx = a.cf[i1 < 0 ? -i1 : i1];
+    for (long long iy = beg; iy < end; ++iy) {
+      long long i2 = (long long)a.sampling * iy + o1;
+      double wty = a.cf[i2 < 0 ? -i2 : i2];
+      double wt = __dmul_rn(wtx, wty);
+      norm = __dadd_rn(norm, wt);
+      int64_t gi = plane + ((int64_t)x0 + ix) * a.g_n3 + ((int64_t)y0 + iy);
+      double gr, gim;
+      if (a.grid_c128) {
+        double2 gv = ((const double2 *)a.grid)[gi];
+        gr = gv.x; gim = gv.y;
+      } else {
+        float2 gv = ((const float2 *)a.grid)[gi];
+        gr = gv.x; gim = gv.y;
+      }
+      nv_re = __dadd_rn(nv_re, __dmul_rn(wt, gr));
+      nv_im = __dadd_rn(nv_im, __dmul_rn(wt, gim));
+    }
+  }
+  if (norm != 0.0) {
+    double cr = ph_re, ci = -ph_im;
+    double pr = __dsub_rn(__dmul_rn(nv_re, cr), __dmul_rn(nv_im, ci));
+    double pi = __dadd_rn(__dmul_rn(nv_re, ci), __dmul_rn(nv_im, cr));
+    if (a.values_c128) {
+      double2 *o = (double2 *)a.values + k;
+      double2 cur = *o;
+      *o = make_double2(__dadd_rn(cur.x, __ddiv_rn(pr, norm)), __dadd_rn(cur.y, __ddiv_rn(pi, norm)));
+    } else {
+      float2 *o = (float2 *)a.values + k;
+      float2 cur = *o;
+      *o = make_float2((float)((double)cur.x + pr / norm), (float)((double)cur.y + pi / norm));
+    }
+  }
+}
+
+// ---------------------------------------------------------------- tiled ----
+constexpr int DT_THREADS = 256;
+
+struct TiledDegridArgs {
+  const Rec *recs;
+  const uint32_t *tile_start;
+  const uint32_t *n_rec;
+  int64_t n_tiles, ntu, ntv, chunk;
+  DegridArgs d;
+  int cgk_len;
+};
+
+template <int S, int NPG>
+struct DSmem {
+  static constexpr int W = TILE + S - 1;
+  static constexpr int RW = (S + 3) & ~3;  // tap-table row (floats)
+  static constexpr size_t tab_bytes = 256 * RW * sizeof(float);
+  static constexpr size_t rs_bytes = 256 * sizeof(double);
+  static constexpr size_t sub_bytes = (size_t)NPG * W * W * sizeof(float2);
+  static constexpr size_t total = tab_bytes + rs_bytes + sub_bytes;
+};
+
+template <int S, int RW>
+__device__ void build_tap_tables_d(float *tab, double *rs, const double *cgk, int cgk_len,
+                                   int os) {
+  for (int o = threadIdx.x; o < 256; o += blockDim.x) {
+    int off = o - 128;
+    double s = 0.0;
+#pragma unroll
+    for (int i = 0; i < RW; ++i) {
+      double v = 0.0;
+      if (i < S) {
+        int k = os * (i - S / 2) + off;
+        k = k < 0 ? -k : k;
+        v = (k < cgk_len) ? cgk[k] : 0.0;
+        s += v;
+      }
+      tab[o * RW + i] = (float)v;
+    }
+    rs[o] = s;
+  }
+}
+
+__device__ __forceinline__ int find_tile_d(const uint32_t *ts, int64_t n_tiles, uint32_t r) {
+  int64_t lo = 0, hi = n_tiles;
+  while (hi - lo > 1) {
+    int64_t mid = (lo + hi) >> 1;
+    if (ts[mid] <= r) lo = mid; else hi = mid;
+  }
+  return (int)lo;
+}
+
+template <int S, int NPG>
+__global__ void __launch_bounds__(DT_THREADS) k_degrid_tiled(TiledDegridArgs a) {
+  using M = DSmem<S, NPG>;
+  constexpr int W = M::W, RW = M::RW;
+  extern __shared__ __align__(16) unsigned char smem[];
+  float *tab = (float *)smem;
+  double *rs = (double *)(smem + M::tab_bytes);
+  float2 *sub = (float2 *)(smem + M::tab_bytes + M::rs_bytes);
+  const DegridArgs &d = a.d;
+
+  const uint32_t n_rec = *a.n_rec;
+  const uint32_t r0 = (uint32_t)(blockIdx.x * a.chunk);
+  if (r0 >= n_rec) return;
+  const uint32_t r1 = (uint32_t)min((int64_t)n_rec, (int64_t)r0 + a.chunk);
+  build_tap_tables_d<S, RW>(tab, rs, d.cf, a.cgk_len, d.sampling);
+
+  int t = find_tile_d(a.tile_start, a.n_tiles, r0);
+  uint32_t seg_lo = r0;
+  const int64_t gplane = d.g_n2 * d.g_n3;
+  while (seg_lo < r1) {
+    uint32_t t_end = a.tile_start[t + 1];
+    uint32_t seg_hi = min(r1, t_end);
+    if (seg_hi <= seg_lo) {
+      ++t;
+      continue;
+    }
+    const int64_t plane = t / (a.ntu * a.ntv);
+    const int64_t trem = t - plane * a.ntu * a.ntv;
+    const int tu = (int)(trem / a.ntv), tv = (int)(trem - (int64_t)tu * a.ntv);
+    __syncthreads();  // previous segment's readers are done with sub
+    // stage the sub-grid (zero outside the grid)
+    for (int i = threadIdx.x; i < NPG * W * W; i += DT_THREADS) {
+      int gp = i / (W * W);
+      int cell = i - gp * W * W;
+      int iu = cell / W, iv = cell - iu * W;
+      int64_t gu = (int64_t)tu * TILE + iu, gv = (int64_t)tv * TILE + iv;
+      float2 v = make_float2(0.f, 0.f);
+      if (gp < d.g_npol && gu < d.g_n2 && gv < d.g_n3) {
+        int64_t gi = (plane * d.g_npol + gp) * gplane + gu * d.g_n3 + gv;
+        if (d.grid_c128) {
+          double2 x = ((const double2 *)d.grid)[gi];
+          v = make_float2((float)x.x, (float)x.y);
+        } else {
+          v = ((const float2 *)d.grid)[gi];
+        }
+      }
+      sub[i] = v;
+    }
+    __syncthreads();
+    for (uint32_t r = seg_lo + threadIdx.x; r < seg_hi; r += DT_THREADS) {
+      Rec rc = a.recs[r];
+      float cu[RW], cv[RW];
+#pragma unroll
+      for (int k = 0; k < RW; k += 4) {
+        const float4 a4 = *(const float4 *)&tab[rc.ou * RW + k];
+        const float4 b4 = *(const float4 *)&tab[rc.ov * RW + k];
+        cu[k] = a4.x; cu[k + 1] = a4.y; cu[k + 2] = a4.z; cu[k + 3] = a4.w;
+        cv[k] = b4.x; cv[k + 1] = b4.y; cv[k + 2] = b4.z; cv[k + 3] = b4.w;
+      }
+      float2 acc[NPG];
+#pragma unroll
+      for (int gp = 0; gp < NPG; ++gp) acc[gp] = make_float2(0.f, 0.f);
+#pragma unroll
+      for (int i = 0; i < S; ++i) {
+        float2 rowacc[NPG];
+#pragma unroll
+        for (int gp = 0; gp < NPG; ++gp) rowacc[gp] = make_float2(0.f, 0.f);
+        const int base = (rc.du + i) * W + rc.dv;
+#pragma unroll
+        for (int j = 0; j < S; ++j)
+#pragma unroll
+          for (int gp = 0; gp < NPG; ++gp)
+            rowacc[gp] = __ffma2_rn(make_float2(cv[j], cv[j]), sub[gp * W * W + base + j], rowacc[gp]);
+#pragma unroll
+        for (int gp = 0; gp < NPG; ++gp)
+          acc[gp] = __ffma2_rn(make_float2(cu[i], cu[i]), rowacc[gp], acc[gp]);
+      }
+      const double norm = rs[rc.ou] * rs[rc.ov];
+      if (norm == 0.0) continue;
+      const int64_t row = rc.row;
+      const int64_t tb = row / d.nvchan;
+      const int ichan = (int)(row - tb * d.nvchan);
+      double ph_re = 1.0, ph_im = 0.0;
+      if (d.dphase) {
+        double phase = (-2.0 * 3.141592653589793 * d.dphase[tb]) * d.freq[ichan] / d.c;
+        sincos(phase, &ph_im, &ph_re);
+      }
+      const float inv = (float)(1.0 / norm);
+      for (int p = 0; p < d.nvpol; ++p) {
+        int apol = d.polmap[p];
+        if (apol < 0 || apol >= NPG || apol >= d.g_npol) continue;
+        int64_t k = row * d.nvpol + p;
+        if (d.flag && d.flag[k]) continue;
+        float2 v = acc[0];
+#pragma unroll
+        for (int gp = 1; gp < NPG; ++gp)
+          if (apol == gp) v = acc[gp];
+        double vr = v.x, vi = v.y;
+        if (d.dphase) {
+          double cr = ph_re, ci = -ph_im;
+          double pr = vr * cr - vi * ci, pi = vr * ci + vi * cr;
+          vr = pr;
+          vi = pi;
+        }
+        if (d.values_c128) {
+          double2 *o = (double2 *)d.values + k;
+          double2 cur = *o;
+          *o = make_double2(cur.x + vr / norm, cur.y + vi / norm);
+        } else {
+          float2 *o = (float2 *)d.values + k;
+          float2 cur = *o;
+          *o = make_float2(cur.x + (float)vr * inv, cur.y + (float)vi * inv);
+        }
+      }
+    }
+    seg_lo = seg_hi;
+    if (seg_hi == t_end) ++t;
+  }
+}
+
+template <int S, int NPG>
+static int launch_degrid_tiled(const TiledDegridArgs &a, int64_t nblocks, cudaStream_t st) {
+  size_t smem = DSmem<S, NPG>::total;
+  if (smem > 48 * 1024) {
+    static bool configured[64] = {false};
+    int dev = 0;
+    cudaGetDevice(&dev);
+    if (dev >= 0 && dev < 64 && !configured[dev]) {
+      AV_CUDA(cudaFuncSetAttribute(k_degrid_tiled<S, NPG>,
+                                   cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+      configured[dev] = true;
+    }
+  }
+  k_degrid_tiled<S, NPG><<<(unsigned)nblocks, DT_THREADS, smem, st>>>(a);
+  AV_LAUNCH_CHECK();
+  return AV_OK;
+}
+
+template <int S>
+static int degrid_dispatch_npg(const TiledDegridArgs &a, int npg, int64_t nb, cudaStream_t st) {
+  if (npg == 1) return launch_degrid_tiled<S, 1>(a, nb, st);
+  if (npg == 2) return launch_degrid_tiled<S, 2>(a, nb, st);
+  return launch_degrid_tiled<S, 4>(a, nb, st);
+}
+
+static int degrid_dispatch(const TiledDegridArgs &a, int support, int npg, int64_t nb,
+                           cudaStream_t st) {
+  switch (support) {
+    case 3: return degrid_dispatch_npg<3>(a, npg, nb, st);
+    case 4: return degrid_dispatch_npg<4>(a, npg, nb, st);
+    case 5: return degrid_dispatch_npg<5>(a, npg, nb, st);
+    case 6: return degrid_dispatch_npg<6>(a, npg, nb, st);
+    case 7: return degrid_dispatch_npg<7>(a, npg, nb, st);
+    case 8: return degrid_dispatch_npg<8>(a, npg, nb, st);
+    case 9: return degrid_dispatch_npg<9>(a, npg, nb, st);
+  }
+  set_error("av_degrid_tiled: support %d not in [3, 9]", support);
+  return AV_ERR_UNSUPPORTED;
+}
+
+static int fill_degrid_args(DegridArgs &a, const double *uvw, const double *dphase, void *values,
+                            int values_dtype, const uint8_t *flag, double scale_x, double scale_y,
+                            double offset_x, double offset_y, const void *grid, int grid_dtype,
+                            int64_t g_nchan, int64_t g_npol, int64_t g_n2, int64_t g_n3,
+                            const double *freq, double c, int support, int sampling,
+                            const double *convFunc, const int32_t *chanmap,
+                            const int32_t *polmap, int64_t nt, int64_t nb, int64_t nvchan,
+                            int64_t nvpol, const char *who) {
+  AV_CHECK_ARG(uvw && values && grid && freq && convFunc && chanmap && polmap,
+               "%s: null pointer", who);
+  AV_CHECK_ARG(values_dtype == AV_C64 || values_dtype == AV_C128, "%s: values dtype", who);
+  AV_CHECK_ARG(grid_dtype == AV_C64 || grid_dtype == AV_C128, "%s: grid dtype", who);
+  AV_CHECK_ARG(support >= 1 && sampling >= 1, "%s: bad kernel sizes", who);
+  AV_CHECK_ARG(nt >= 0 && nb >= 0 && nvchan >= 0 && nvpol >= 0 && g_nchan >= 0 && g_npol >= 0 &&
+                   g_n2 >= 0 && g_n3 >= 0, "%s: bad shape", who);
+  a.scale0 = scale_x; a.scale1 = scale_y; a.offset0 = offset_x; a.offset1 = offset_y;
+  a.uvw = uvw; a.dphase = dphase; a.values = values; a.values_c128 = values_dtype == AV_C128;
+  a.flag = flag;
+  a.grid = grid; a.grid_c128 = grid_dtype == AV_C128;
+  a.g_nchan = g_nchan; a.g_npol = g_npol; a.g_n2 = g_n2; a.g_n3 = g_n3;
+  a.freq = freq; a.c = c; a.support = support; a.sampling = sampling; a.cf = convFunc;
+  a.chanmap = chanmap; a.polmap = polmap; a.nt = nt; a.nb = nb; a.nvchan = nvchan; a.nvpol = nvpol;
+  return AV_OK;
+}
+
+}  // namespace av
+
+using namespace av;
+
+extern "C" {
+
+int av_degrid_plain(const double *uvw, const double *dphase, void *values, int values_dtype,
+                    const uint8_t *flag, double scale_x, double scale_y, double offset_x, double offset_y,
+                    const void *grid, int grid_dtype, int64_t g_nchan, int64_t g_npol,
+                    int64_t g_n2, int64_t g_n3, const double *freq, double c, int support,
+                    int sampling, const double *convFunc, const int32_t *chanmap,
+                    const int32_t *polmap, int64_t nt, int64_t nb, int64_t nvchan,
+                    int64_t nvpol, void *stream) {
+  clear_error();
+  DegridArgs a;
+  int rc = fill_degrid_args(a, uvw, dphase, values, values_dtype, flag, scale_x, scale_y, offset_x, offset_y, grid,
+                            grid_dtype, g_nchan, g_npol, g_n2, g_n3, freq, c, support, sampling,
+                            convFunc, chanmap, polmap, nt, nb, nvchan, nvpol, "av_degrid_plain");
+  if (rc) return rc;
+  cudaStream_t st = as_stream(stream);
+  int64_t total = nt * nb * nvchan * nvpol;
+  if (total == 0) return AV_OK;
+  k_degrid_plain<<<(unsigned)((total + 255) / 256), 256, 0, st>>>(a);
+  AV_LAUNCH_CHECK();
+  return AV_OK;
+}
+
+size_t av_degrid_tiled_workspace_size(int64_t nt, int64_t nb, int64_t nvchan, int64_t g_n2,
+                                      int64_t g_n3, int64_t g_nchan, int support) {
+  PlanGeom g;
+  plan_geometry(g, nt, nb, nvchan, g_nchan, g_n2, g_n3, support, 100);
+  return plan_workspace_bytes(g);
+}
+
+static int degrid_geom_checked(PlanGeom &g, Plan &p, double scale_x, double scale_y,
+                               double offset_x, double offset_y, int64_t g_nchan, int64_t g_n2,
+                               int64_t g_n3, int support, int sampling, int64_t nt, int64_t nb,
+                               int64_t nvchan, void *workspace, size_t workspace_bytes,
+                               const char *who) {
+  AV_CHECK_ARG(support >= 3 && support <= 9, "%s: support must be in [3, 9]", who);
+  AV_CHECK_ARG(sampling >= 1 && sampling <= 254, "%s: sampling must be in [1, 254]", who);
+  AV_CHECK_ARG(g_n2 >= support && g_n3 >= support && g_n2 < 131072 && g_n3 < 131072,
+               "%s: grid size out of range", who);
+  AV_CHECK_ARG(nt >= 0 && nb >= 0 && nvchan >= 0 && g_nchan >= 0, "%s: bad shape", who);
+  AV_CHECK_ARG(workspace && (((uintptr_t)workspace) & 255) == 0,
+               "%s: workspace must be 256-byte aligned", who);
+  plan_geometry(g, nt, nb, nvchan, g_nchan > 0 ? g_nchan : 1, g_n2, g_n3, support, sampling);
+  g.convention = 1;
+  g.chk_x = g_n3;
+  g.chk_y = g_n2;
+  g.scale0 = scale_x;
+  g.scale1 = scale_y;
+  g.offset0 = offset_x;
+  g.offset1 = offset_y;
+  size_t need = plan_workspace_bytes(g);
+  if (workspace_bytes < need) {
+    set_error("%s: workspace %zu bytes < %zu needed", who, workspace_bytes, need);
+    return AV_ERR_WORKSPACE;
+  }
+  Workspace ws(workspace, workspace_bytes);
+  if (!plan_carve(g, ws, p)) {
+    set_error("%s: workspace carve failed", who);
+    return AV_ERR_WORKSPACE;
+  }
+  return AV_OK;
+}
+
+int av_degrid_tiled_plan(const double *uvw, const double *freq, const int32_t *chanmap,
+                         double scale_x, double scale_y, double offset_x, double offset_y,
+                         int64_t g_nchan, int64_t g_n2, int64_t g_n3, int support, int sampling,
+                         int64_t nt, int64_t nb, int64_t nvchan, void *workspace,
+                         size_t workspace_bytes, void *stream) {
+  clear_error();
+  AV_CHECK_ARG(uvw && freq && chanmap, "av_degrid_tiled_plan: null pointer");
+  PlanGeom g;
+  Plan p;
+  int rc = degrid_geom_checked(g, p, scale_x, scale_y, offset_x, offset_y, g_nchan, g_n2, g_n3,
+                               support, sampling, nt, nb, nvchan, workspace, workspace_bytes,
+                               "av_degrid_tiled_plan");
+  if (rc) return rc;
+  return plan_build(g, p, uvw, freq, chanmap, 0.0, 0.0, as_stream(stream));
+}
+
+int av_degrid_tiled_execute(const double *dphase, void *values, int values_dtype,
+                            const uint8_t *flag, const void *grid, int grid_dtype,
+                            int64_t g_nchan, int64_t g_npol, int64_t g_n2, int64_t g_n3,
+                            const double *freq, int support, int sampling,
+                            const double *convFunc, const int32_t *polmap, int64_t nt,
+                            int64_t nb, int64_t nvchan, int64_t nvpol, void *workspace,
+                            size_t workspace_bytes, void *stream) {
+  clear_error();
+  AV_CHECK_ARG(values && grid && freq && convFunc && polmap,
+               "av_degrid_tiled_execute: null pointer");
+  AV_CHECK_ARG(values_dtype == AV_C64 || values_dtype == AV_C128,
+               "av_degrid_tiled_execute: values dtype");
+  AV_CHECK_ARG(grid_dtype == AV_C64 || grid_dtype == AV_C128,
+               "av_degrid_tiled_execute: grid dtype");
+  AV_CHECK_ARG(g_npol >= 1 && g_npol <= 4, "av_degrid_tiled_execute: grid pols must be in [1, 4]");
+  AV_CHECK_ARG(nvpol >= 0, "av_degrid_tiled_execute: bad shape");
+  PlanGeom g;
+  Plan p;
+  int rc = degrid_geom_checked(g, p, 0.0, 0.0, 0.0, 0.0, g_nchan, g_n2, g_n3, support, sampling,
+                               nt, nb, nvchan, workspace, workspace_bytes,
+                               "av_degrid_tiled_execute");
+  if (rc) return rc;
+  int64_t rows = nt * nb * nvchan;
+  if (rows == 0 || nvpol == 0 || g_nchan == 0) return AV_OK;
+  DegridArgs d;
+  d.uvw = nullptr;
+  d.dphase = dphase;
+  d.values = values;
+  d.values_c128 = values_dtype == AV_C128;
+  d.flag = flag;
+  d.scale0 = d.scale1 = d.offset0 = d.offset1 = 0.0;
+  d.grid = grid;
+  d.grid_c128 = grid_dtype == AV_C128;
+  d.g_nchan = g_nchan; d.g_npol = g_npol; d.g_n2 = g_n2; d.g_n3 = g_n3;
+  d.freq = freq; d.c = C_LIGHT; d.support = support; d.sampling = sampling; d.cf = convFunc;
+  d.chanmap = nullptr; d.polmap = polmap; d.nt = nt; d.nb = nb; d.nvchan = nvchan;
+  d.nvpol = nvpol;
+  TiledDegridArgs a;
+  a.recs = p.recs;
+  a.tile_start = p.tile_start;
+  a.n_rec = p.offs + g.n_keys();
+  a.n_tiles = g.n_tiles();
+  a.ntu = g.ntu;
+  a.ntv = g.ntv;
+  int sms = sm_count();
+  int64_t chunk = (rows + (int64_t)sms * 8 - 1) / ((int64_t)sms * 8);
+  if (chunk < 1024) chunk = 1024;
+  a.chunk = chunk;
+  a.d = d;
+  a.cgk_len = sampling * (support / 2 + 1);
+  int npg = g_npol <= 1 ? 1 : (g_npol <= 2 ? 2 : 4);
+  return degrid_dispatch(a, support, npg, (rows + chunk - 1) / chunk, as_stream(stream));
+}
+
+int av_degrid_tiled(const double *uvw, const double *dphase, void *values, int values_dtype,
+                    const uint8_t *flag, double scale_x, double scale_y, double offset_x, double offset_y,
+                    const void *grid, int grid_dtype, int64_t g_nchan, int64_t g_npol,
+                    int64_t g_n2, int64_t g_n3, const double *freq, double c, int support,
+                    int sampling, const double *convFunc, const int32_t *chanmap,
+                    const int32_t *polmap, int64_t nt, int64_t nb, int64_t nvchan,
+                    int64_t nvpol, void *workspace, size_t workspace_bytes, void *stream) {
+  clear_error();
+  AV_CHECK_ARG(c == C_LIGHT, "av_degrid_tiled: c must be 299792458.0 (use av_degrid_plain)");
+  int rc = av_degrid_tiled_plan(uvw, freq, chanmap, scale_x, scale_y, offset_x, offset_y, g_nchan,
+                                g_n2, g_n3, support, sampling, nt, nb, nvchan, workspace,
+                                workspace_bytes, stream);
+  if (rc) return rc;
+  return av_degrid_tiled_execute(dphase, values, values_dtype, flag, grid, grid_dtype, g_nchan,
+                                 g_npol, g_n2, g_n3, freq, support, sampling, convFunc, polmap, nt,
+                                 nb, nvchan, nvpol, workspace, workspace_bytes, stream);
+}
+
+}  // extern "C"

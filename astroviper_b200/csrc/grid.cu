@@ -1,0 +1,642 @@
+// Convolutional gridding (standard_grid_jit, standard_grid.py:246-432).
+//
+// av_grid_plain: one thread per (time, baseline, channel) sample, FP64, the
+//   reference's per-sample arithmetic and tap order, FP64 atomics.
+// av_grid_tiled: FP32 tiled gridder over a cell-sorted plan (plan.cuh).
+//   Each CTA walks a chunk of records; per tile it keeps a (T+S-1)^2 x npg
+//   complex sub-grid in shared memory.  Records are staged in batches; lanes
+//   form groups of S threads, lane g of a group owns footprint row g and
+//   keeps S x NPOL complex accumulators in registers for as long as the
+//   group's records stay in one cell (cell-sorted input makes that long),
+//   flushing to the sub-grid only on a cell change.  The tile is flushed to
+//   the global grid once.  Products use packed FP32 (fma.rn.f32x2).
+#include "plan.cuh"
+
+namespace av {
+
+// ---------------------------------------------------------------------------
+// plain kernel
+// ---------------------------------------------------------------------------
+struct GridArgs {
+  void *grid;
+  int grid_dtype;
+  double *sumw;
+  int do_psf, do_iw;
+  const void *vis;
+  int vis_dtype;
+  const void *wt;
+  int wt_dtype;
+  const double *uvw, *freq;
+  const int32_t *chan_map, *pol_map;
+  const double *cgk;
+  int64_t n_u, n_v;
+  double dl0, dl1;
+  int support, os;
+  int64_t nt, nb, nchan, npol, n_img_chan, n_img_pol;
+};
+
+__device__ __forceinline__ double load_real(const void *p, int dt, int64_t i) {
+  return dt == AV_F32 ? (double)((const float *)p)[i] : ((const double *)p)[i];
+}
+__device__ __forceinline__ double2 load_cplx(const void *p, int dt, int64_t i) {
+  if (dt == AV_C64) {
+    float2 v = ((const float2 *)p)[i];
+    return make_double2(v.x, v.y);
+  }
+  return ((const double2 *)p)[i];
+}
+__device__ __forceinline__ void grid_add(void *g, int dt, int64_t i, double re, double im) {
+  switch (dt) {
+    case AV_C128:
+      atomicAdd(&((double2 *)g)[i].x, re);
+      atomicAdd(&((double2 *)g)[i].y, im);
+      break;
+    case AV_C64:
+      atomicAdd(&((float2 *)g)[i].x, (float)re);
+      atomicAdd(&((float2 *)g)[i].y, (float)im);
+      break;
+    case AV_F64: atomicAdd(&((double *)g)[i], re); break;
+    default: atomicAdd(&((float *)g)[i], (float)re); break;
+  }
+}
+
+__global__ void __launch_bounds__(256) k_grid_plain(GridArgs a) {
+  int64_t row = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (row >= a.nt * a.nb * a.nchan) return;
+  int64_t tb = row / a.nchan;
+  int c = (int)(row - tb * a.nchan);
+  int a_chan = a.chan_map[c];
+  if (a_chan < 0 || a_chan >= a.n_img_chan) return;  // outside the image: dropped
+  double f = a.freq[c];
+  double us0 = __ddiv_rn(-__dmul_rn(__dmul_rn(f, a.dl0), (double)a.n_u), C_LIGHT);
+  double us1 = __ddiv_rn(-__dmul_rn(__dmul_rn(f, a.dl1), (double)a.n_v), C_LIGHT);
+  double u = __dmul_rn(a.uvw[3 * tb + 0], us0), v = __dmul_rn(a.uvw[3 * tb + 1], us1);
+  if (isnan(u) || isnan(v)) return;
+  double u_pos = __dadd_rn(u, (double)(a.n_u / 2)), v_pos = __dadd_rn(v, (double)(a.n_v / 2));
+  double u_pos_c = __dadd_rn(-u, (double)(a.n_u / 2)), v_pos_c = __dadd_rn(-v, (double)(a.n_v / 2));
+  long long ui = trunc_ll(__dadd_rn(u_pos, 0.5)), vi = trunc_ll(__dadd_rn(v_pos, 0.5));
+  long long uic = trunc_ll(__dadd_rn(u_pos_c, 0.5)), vic = trunc_ll(__dadd_rn(v_pos_c, 0.5));
+  const long long sc = a.support / 2;
+  if (!((ui + sc < a.n_u) && (vi + sc < a.n_v) && (ui - sc >= 0) && (vi - sc >= 0))) return;
+  long long uoi = (long long)floor(__dadd_rn(__dmul_rn(__dsub_rn((double)ui, u_pos), (double)a.os), 0.5));
+  long long voi = (long long)floor(__dadd_rn(__dmul_rn(__dsub_rn((double)vi, v_pos), (double)a.os), 0.5));
+  const long long s0 = -sc, s1 = a.support - sc;
+  const bool is_cplx = (a.grid_dtype == AV_C64 || a.grid_dtype == AV_C128);
+  for (int64_t ip = 0; ip < a.npol; ++ip) {
+    int64_t idx = row * a.npol + ip;
+    double sel_w, wr, wi;
+    if (a.do_psf) {
+      if (a.npol >= 2 && a.do_iw) {
+        wr = __ddiv_rn(__dadd_rn(load_real(a.wt, a.wt_dtype, row * a.npol),
+                                 load_real(a.wt, a.wt_dtype, row * a.npol + 1)), 2.0);
+        wi = 0.0;
+        sel_w = wr;
+      } else {
+        sel_w = load_real(a.wt, a.wt_dtype, idx);
+        wr = sel_w;
+        wi = 0.0;
+      }
+    } else {
+      sel_w = load_real(a.wt, a.wt_dtype, idx);
+      double2 vv = load_cplx(a.vis, a.vis_dtype, idx);
+      wr = __dmul_rn(vv.x, sel_w);
+      wi = __dmul_rn(vv.y, sel_w);
+    }
+    if (isnan(wr) || isnan(wi)) continue;
+    if (!(wr != 0.0 || wi != 0.0)) continue;
+    int a_pol = a.pol_map[ip];
+    if (a_pol < 0 || a_pol >= a.n_img_pol) continue;
+    int64_t plane = ((int64_t)a_chan * a.n_img_pol + a_pol) * a.n_u * a.n_v;
+    double norm = 0.0;
+    for (long long iv = s0; iv < s1; ++iv) {
+      long long vo = (long long)a.os * iv + voi;
+      double conv_v = a.cgk[vo < 0 ? -vo : vo];
+      long long v_indx = vi + iv, v_indx_c = vic + iv;
+      for (long long iu = s0; iu < s1; ++iu) {
+        long long uo = (long long)a.os * iu + uoi;
+        double conv_u = a.cgk[uo < 0 ? -uo : uo];
+        double conv = __dmul_rn(conv_u, conv_v);
+        long long u_indx = ui + iu;
+        grid_add(a.grid, a.grid_dtype, plane + u_indx * a.n_v + v_indx, __dmul_rn(conv, wr),
+                 is_cplx ? __dmul_rn(conv, wi) : 0.0);
+        norm = __dadd_rn(norm, conv);
+        if (a.do_iw) {
+          // standard_grid.py:407-421 indexes the conjugate cell without a
+          // bounds check: Numba wraps negative indices per axis and lets an
+          // index of n run into the next row / plane.  The same flat cell is
+          // used here while it lies inside the array; beyond the array the
+          // reference writes out of bounds and the sample is skipped.
+          long long uc = uic + iu, vc = v_indx_c;
+          if (uc < 0) uc += a.n_u;
+          if (vc < 0) vc += a.n_v;
+          long long flat = plane + uc * a.n_v + vc;
+          long long total = a.n_img_chan * a.n_img_pol * a.n_u * a.n_v;
+          if (uc >= 0 && vc >= 0 && flat < total)
+            grid_add(a.grid, a.grid_dtype, flat, __dmul_rn(conv, wr),
+                     is_cplx ? __dmul_rn(conv, wi) : 0.0);
+        }
+      }
+    }
+    double add = __dmul_rn(sel_w, norm);
+    atomicAdd(&a.sumw[(int64_t)a_chan * a.n_img_pol + a_pol], add);
+    if (a.do_iw) atomicAdd(&a.sumw[(int64_t)a_chan * a.n_img_pol + a_pol], add);
+  }
+}
+
+// ---------------------------------------------------------------------------
+// tiled kernel: FP32 data, FP64 accumulation
+// ---------------------------------------------------------------------------
+// Grid correction divides the image by the taper grdsf(x) grdsf(y), which is
+// ~4e-3 at the edges, so white errors in the uv plane are amplified ~500x in
+// the image (norm-wise).  Accumulating in FP32 (even in short runs) leaves
+// 3e-5 .. 2e-4 relative error in the dirty image; FP32 products summed in
+// FP64 leave ~4e-6.  The kernel therefore reads FP32 visibilities and
+// weights, forms tap weights from an FP64 table, and accumulates with DFMA
+// into FP64 registers and an FP64 shared-memory sub-grid.
+constexpr int GT_THREADS = 256;
+constexpr int GT_WARPS = GT_THREADS / 32;
+constexpr int GT_RPG = 32;  // records per group per batch
+
+struct TiledGridArgs {
+  const Rec *recs;
+  const uint32_t *tile_start;
+  const uint32_t *n_rec;  // device: total records (offs[n_keys])
+  int64_t n_tiles, ntu, ntv;
+  int64_t chunk;
+  const float2 *vis;
+  const float *wt;
+  int do_psf;
+  const double *cgk;
+  int cgk_len, os;
+  const int32_t *pol_map;  // device, npol entries
+  int npol, npg;
+  void *grid;
+  int grid_c128;
+  double *sumw;
+  int64_t n_u, n_v;
+};
+
+// S taps, NPOL visibility polarisations, PPT polarisations per thread.
+template <int S, int NPOL, int PPT>
+struct GCfg {
+  static constexpr int W = TILE + S - 1;         // sub-grid edge
+  static constexpr int RW = (S + 1) & ~1;        // tap-table row (doubles)
+  static constexpr int LPG = S * (NPOL / PPT);   // lanes per group
+  static constexpr int GPW = 32 / LPG;           // groups per warp
+  static constexpr int NG = GT_WARPS * GPW;      // groups per CTA
+  static constexpr int B = NG * GT_RPG;          // records per batch
+  // padded per-group strides keep the groups of a warp on different banks
+  static constexpr int WD_STRIDE = GT_RPG * NPOL + 2;  // float2
+  static constexpr int MT_STRIDE = GT_RPG + 1;         // int2
+  static constexpr size_t tab_bytes = 256 * RW * sizeof(double);
+  static constexpr size_t rs_bytes = 256 * sizeof(double);
+  static constexpr size_t wd_bytes = (size_t)NG * WD_STRIDE * sizeof(float2);
+  static constexpr size_t mt_bytes = (size_t)NG * MT_STRIDE * sizeof(int2);
+  static size_t sub_bytes(int npg) { return (size_t)npg * W * W * sizeof(double2); }
+  static size_t total(int npg) { return tab_bytes + rs_bytes + wd_bytes + mt_bytes + sub_bytes(npg); }
+};
+
+// Per-offset tap tables: tab[(o + 128) * RW + i] = cgk[|os * (i - S/2) + o|]
+// and rs[o + 128] = sum_i of the same (so sum_k w_k = rs[ou] * rs[ov]).
+template <int S, int RW>
+__device__ void build_tap_tables64(double *tab, double *rs, const double *cgk, int cgk_len,
+                                   int os) {
+  for (int o = threadIdx.x; o < 256; o += blockDim.x) {
+    int off = o - 128;
+    double s = 0.0;
+#pragma unroll
+    for (int i = 0; i < RW; ++i) {
+      double v = 0.0;
+      if (i < S) {
+        int k = os * (i - S / 2) + off;
+        k = k < 0 ? -k : k;
+        v = (k < cgk_len) ? cgk[k] : 0.0;
+        s += v;
+      }
+      tab[o * RW + i] = v;
+    }
+    rs[o] = s;
+  }
+}
+
+__device__ __forceinline__ int find_tile(const uint32_t *ts, int64_t n_tiles, uint32_t r) {
+  // largest t in [0, n_tiles) with ts[t] <= r (ts[n_tiles] = total > r)
+  int64_t lo = 0, hi = n_tiles;
+  while (hi - lo > 1) {
+    int64_t mid = (lo + hi) >> 1;
+    if (ts[mid] <= r) lo = mid; else hi = mid;
+  }
+  return (int)lo;
+}
+
+template <int S, int NPOL, int PPT>
+__global__ void __launch_bounds__(GT_THREADS, 1) k_grid_tiled(TiledGridArgs a) {
+  using C = GCfg<S, NPOL, PPT>;
+  constexpr int W = C::W, RW = C::RW;
+  extern __shared__ __align__(16) unsigned char smem[];
+  double *tab = (double *)smem;
+  double *rs = (double *)(smem + C::tab_bytes);
+  float2 *st_wd = (float2 *)(smem + C::tab_bytes + C::rs_bytes);
+  int2 *st_mt = (int2 *)(smem + C::tab_bytes + C::rs_bytes + C::wd_bytes);
+  double2 *sub = (double2 *)(smem + C::tab_bytes + C::rs_bytes + C::wd_bytes + C::mt_bytes);
+
+  const uint32_t n_rec = *a.n_rec;
+  const uint32_t r0 = (uint32_t)(blockIdx.x * a.chunk);
+  if (r0 >= n_rec) return;
+  const uint32_t r1 = (uint32_t)min((int64_t)n_rec, (int64_t)r0 + a.chunk);
+  const int npg = a.npg;
+  const int sub_n = npg * W * W;
+
+  build_tap_tables64<S, RW>(tab, rs, a.cgk, a.cgk_len, a.os);
+  for (int i = threadIdx.x; i < sub_n; i += GT_THREADS) sub[i] = make_double2(0.0, 0.0);
+
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int gq = lane / C::LPG, r = lane - gq * C::LPG;
+  const int g = r % S;        // footprint row owned by this lane
+  const int pg = r / S;       // polarisation group
+  const bool computes = gq < C::GPW;
+  const int q = warp * C::GPW + gq;  // group index in the CTA
+  // image polarisation of each of this lane's visibility polarisations (-1 drops)
+  int pm[PPT];
+#pragma unroll
+  for (int j = 0; j < PPT; ++j) {
+    int pp = pg * PPT + j;
+    int v = pp < a.npol ? a.pol_map[pp] : -1;
+    pm[j] = (v >= 0 && v < npg) ? v : -1;
+  }
+  // all polarisations, for sum_weight
+  int pmall[NPOL];
+#pragma unroll
+  for (int pp = 0; pp < NPOL; ++pp) {
+    int v = pp < a.npol ? a.pol_map[pp] : -1;
+    pmall[pp] = (v >= 0 && v < npg) ? v : -1;
+  }
+
+  int t = find_tile(a.tile_start, a.n_tiles, r0);
+  uint32_t seg_lo = r0;
+  __syncthreads();
+  while (seg_lo < r1) {
+    uint32_t t_end = a.tile_start[t + 1];
+    uint32_t seg_hi = min(r1, t_end);
+    if (seg_hi <= seg_lo) {  // empty tile (uniform across the CTA)
+      ++t;
+      continue;
+    }
+    const int64_t plane = t / (a.ntu * a.ntv);
+    const int64_t trem = t - plane * a.ntu * a.ntv;
+    const int tu = (int)(trem / a.ntv), tv = (int)(trem - (int64_t)tu * a.ntv);
+
+    double2 acc[PPT][S];
+#pragma unroll
+    for (int j = 0; j < PPT; ++j)
+#pragma unroll
+      for (int k = 0; k < S; ++k) acc[j][k] = make_double2(0.0, 0.0);
+    int cur = -1;
+    double sw[NPOL];
+#pragma unroll
+    for (int pp = 0; pp < NPOL; ++pp) sw[pp] = 0.0;
+
+    auto flush_acc = [&](int key) {
+      const int du = key & 255, dv = (key >> 8) & 255;
+      const int base = (du + g) * W + dv;
+#pragma unroll
+      for (int j = 0; j < PPT; ++j)
+#pragma unroll
+        for (int k = 0; k < S; ++k) {
+          double2 v = acc[j][k];
+          if (pm[j] >= 0 && (v.x != 0.0 || v.y != 0.0)) {
+            double2 *d = &sub[pm[j] * W * W + base + k];
+            atomicAdd(&d->x, v.x);
+            atomicAdd(&d->y, v.y);
+          }
+          acc[j][k] = make_double2(0.0, 0.0);
+        }
+    };
+
+    for (uint32_t b0 = seg_lo; b0 < seg_hi; b0 += C::B) {
+      const int nbat = (int)min((uint32_t)C::B, seg_hi - b0);
+      // ---- stage: one thread per record
+      for (int j = threadIdx.x; j < nbat; j += GT_THREADS) {
+        Rec rc = a.recs[b0 + j];
+        const int qq = j / GT_RPG, jj = j - qq * GT_RPG;
+        const int64_t vb = (int64_t)rc.row * a.npol;
+        const double nrm = rs[rc.ou] * rs[rc.ov];
+        float2 wdv[NPOL];
+        float wv[NPOL];
+        if (NPOL == 4 && a.npol == 4) {
+          float4 w4 = *(const float4 *)(a.wt + vb);
+          wv[0] = w4.x; wv[1 % NPOL] = w4.y; wv[2 % NPOL] = w4.z; wv[3 % NPOL] = w4.w;
+          if (!a.do_psf) {
+            float4 v01 = *(const float4 *)(a.vis + vb);
+            float4 v23 = *(const float4 *)(a.vis + vb + 2);
+            wdv[0] = make_float2(v01.x * wv[0], v01.y * wv[0]);
+            wdv[1 % NPOL] = make_float2(v01.z * wv[1 % NPOL], v01.w * wv[1 % NPOL]);
+            wdv[2 % NPOL] = make_float2(v23.x * wv[2 % NPOL], v23.y * wv[2 % NPOL]);
+            wdv[3 % NPOL] = make_float2(v23.z * wv[3 % NPOL], v23.w * wv[3 % NPOL]);
+          } else {
+#pragma unroll
+            for (int pp = 0; pp < NPOL; ++pp) wdv[pp] = make_float2(wv[pp], 0.f);
+          }
+        } else {
+#pragma unroll
+          for (int pp = 0; pp < NPOL; ++pp) {
+            wv[pp] = 0.f;
+            wdv[pp] = make_float2(0.f, 0.f);
+            if (pp < a.npol) {
+              wv[pp] = a.wt[vb + pp];
+              if (a.do_psf) {
+                wdv[pp] = make_float2(wv[pp], 0.f);
+              } else {
+                float2 v = a.vis[vb + pp];
+                wdv[pp] = make_float2(v.x * wv[pp], v.y * wv[pp]);
+              }
+            }
+          }
+        }
+        float2 *dst = st_wd + qq * C::WD_STRIDE + jj * NPOL;
+#pragma unroll
+        for (int pp = 0; pp < NPOL; ++pp) {
+          float2 d = wdv[pp];
+          // the reference skips NaN and exact-zero weighted data (standard_grid.py:378)
+          bool ok = pp < a.npol && !isnan(d.x) && !isnan(d.y) && (d.x != 0.f || d.y != 0.f);
+          dst[pp] = ok ? d : make_float2(0.f, 0.f);
+          if (ok) sw[pp] += (double)wv[pp] * nrm;
+        }
+        st_mt[qq * C::MT_STRIDE + jj] =
+            make_int2((int)rc.du | ((int)rc.dv << 8), (int)rc.ou | ((int)rc.ov << 8));
+      }
+      __syncthreads();
+      // ---- compute: group q takes its slice of the batch in order
+      if (computes) {
+        const int jn = min(GT_RPG, nbat - q * GT_RPG);
+        const float2 *wq = st_wd + q * C::WD_STRIDE;
+        const int2 *mq = st_mt + q * C::MT_STRIDE;
+        for (int jj = 0; jj < jn; ++jj) {
+          const int2 mt = mq[jj];
+          if (mt.x != cur) {
+            if (cur >= 0) flush_acc(cur);
+            cur = mt.x;
+          }
+          const double cu = tab[(mt.y & 255) * RW + g];
+          const double *cvp = &tab[((mt.y >> 8) & 255) * RW];
+          double cv[RW];
+#pragma unroll
+          for (int k = 0; k < RW; k += 2) {
+            double2 c2 = *(const double2 *)(cvp + k);
+            cv[k] = c2.x;
+            cv[k + 1] = c2.y;
+          }
+#pragma unroll
+          for (int j = 0; j < PPT; ++j) {
+            const float2 d = wq[jj * NPOL + pg * PPT + j];
+            const double tr = cu * (double)d.x, ti = cu * (double)d.y;
+#pragma unroll
+            for (int k = 0; k < S; ++k) {
+              acc[j][k].x = fma(cv[k], tr, acc[j][k].x);
+              acc[j][k].y = fma(cv[k], ti, acc[j][k].y);
+            }
+          }
+        }
+      }
+      __syncthreads();
+    }
+    if (computes && cur >= 0) flush_acc(cur);
+    // ---- sum_weight: warp reduction, one atomic per warp and polarisation
+#pragma unroll
+    for (int pp = 0; pp < NPOL; ++pp) {
+      double v = sw[pp];
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+      if (lane == 0 && pmall[pp] >= 0 && v != 0.0)
+        atomicAdd(&a.sumw[plane * npg + pmall[pp]], v);
+    }
+    __syncthreads();
+    // ---- flush the tile to the global grid and clear it
+    for (int i = threadIdx.x; i < sub_n; i += GT_THREADS) {
+      double2 v = sub[i];
+      if (v.x != 0.0 || v.y != 0.0) {
+        int gp = i / (W * W);
+        int cell = i - gp * W * W;
+        int iu = cell / W, iv = cell - iu * W;
+        int64_t gu = (int64_t)tu * TILE + iu, gv = (int64_t)tv * TILE + iv;
+        int64_t gi = ((plane * npg + gp) * a.n_u + gu) * a.n_v + gv;
+        if (a.grid_c128) {
+          double2 *gd = (double2 *)a.grid + gi;
+          atomicAdd(&gd->x, v.x);
+          atomicAdd(&gd->y, v.y);
+        } else {
+          atomicAdd((float2 *)a.grid + gi, make_float2((float)v.x, (float)v.y));
+        }
+        sub[i] = make_double2(0.0, 0.0);
+      }
+    }
+    __syncthreads();
+    seg_lo = seg_hi;
+    if (seg_hi == t_end) ++t;
+  }
+}
+
+template <int S, int NPOL, int PPT>
+static int launch_grid_tiled(const TiledGridArgs &a, int64_t nblocks, cudaStream_t st) {
+  using C = GCfg<S, NPOL, PPT>;
+  size_t smem = C::total(a.npg);
+  static bool configured[64] = {false};
+  int dev = 0;
+  AV_CUDA(cudaGetDevice(&dev));
+  if (dev >= 0 && dev < 64 && !configured[dev]) {
+    AV_CUDA(cudaFuncSetAttribute(k_grid_tiled<S, NPOL, PPT>,
+                                 cudaFuncAttributeMaxDynamicSharedMemorySize, (int)C::total(4)));
+    configured[dev] = true;
+  }
+  k_grid_tiled<S, NPOL, PPT><<<(unsigned)nblocks, GT_THREADS, smem, st>>>(a);
+  AV_LAUNCH_CHECK();
+  return AV_OK;
+}
+
+template <int S>
+static int dispatch_npol(const TiledGridArgs &a, int npol, int64_t nb, cudaStream_t st) {
+  if (npol == 1) return launch_grid_tiled<S, 1, 1>(a, nb, st);
+  if (npol == 2) return launch_grid_tiled<S, 2, 1>(a, nb, st);
+  // four polarisations: one per lane while 4*S lanes fit a warp, else two
+  constexpr int PPT = (4 * S <= 32) ? 1 : 2;
+  return launch_grid_tiled<S, 4, PPT>(a, nb, st);
+}
+
+static int dispatch_support(const TiledGridArgs &a, int support, int npol, int64_t nb,
+                            cudaStream_t st) {
+  switch (support) {
+    case 3: return dispatch_npol<3>(a, npol, nb, st);
+    case 4: return dispatch_npol<4>(a, npol, nb, st);
+    case 5: return dispatch_npol<5>(a, npol, nb, st);
+    case 6: return dispatch_npol<6>(a, npol, nb, st);
+    case 7: return dispatch_npol<7>(a, npol, nb, st);
+    case 8: return dispatch_npol<8>(a, npol, nb, st);
+    case 9: return dispatch_npol<9>(a, npol, nb, st);
+  }
+  set_error("av_grid_tiled: support %d not in [3, 9]", support);
+  return AV_ERR_UNSUPPORTED;
+}
+
+}  // namespace av
+
+using namespace av;
+
+extern "C" {
+
+int av_grid_plain(void *grid, int grid_dtype, double *sum_weight, int do_psf,
+                  int do_imaging_weight, const void *vis, int vis_dtype, const void *weight,
+                  int weight_dtype, const double *uvw, const double *freq,
+                  const int32_t *chan_map, const int32_t *pol_map, const double *cgk,
+                  int64_t n_u, int64_t n_v, double delta_l, double delta_m, int support,
+                  int oversampling, int64_t nt, int64_t nb, int64_t nchan, int64_t npol,
+                  int64_t n_img_chan, int64_t n_img_pol, void *stream) {
+  clear_error();
+  AV_CHECK_ARG(grid && sum_weight && weight && uvw && freq && chan_map && pol_map && cgk,
+               "av_grid_plain: null pointer");
+  AV_CHECK_ARG(do_psf || vis, "av_grid_plain: vis is required unless do_psf");
+  AV_CHECK_ARG(grid_dtype >= AV_F32 && grid_dtype <= AV_C128, "av_grid_plain: grid dtype");
+  AV_CHECK_ARG(do_psf || grid_dtype == AV_C64 || grid_dtype == AV_C128,
+               "av_grid_plain: a real grid needs do_psf");
+  AV_CHECK_ARG(vis_dtype == AV_C64 || vis_dtype == AV_C128 || do_psf, "av_grid_plain: vis dtype");
+  AV_CHECK_ARG(weight_dtype == AV_F32 || weight_dtype == AV_F64, "av_grid_plain: weight dtype");
+  AV_CHECK_ARG(n_u > 0 && n_v > 0 && support >= 1 && oversampling >= 1,
+               "av_grid_plain: bad grid/kernel sizes");
+  AV_CHECK_ARG(nt >= 0 && nb >= 0 && nchan >= 0 && npol >= 0, "av_grid_plain: bad shape");
+  int64_t rows = nt * nb * nchan;
+  if (rows == 0 || npol == 0) return AV_OK;
+  GridArgs a;
+  a.grid = grid; a.grid_dtype = grid_dtype; a.sumw = sum_weight;
+  a.do_psf = do_psf; a.do_iw = do_imaging_weight;
+  a.vis = vis; a.vis_dtype = vis_dtype; a.wt = weight; a.wt_dtype = weight_dtype;
+  a.uvw = uvw; a.freq = freq; a.chan_map = chan_map; a.pol_map = pol_map; a.cgk = cgk;
+  a.n_u = n_u; a.n_v = n_v; a.dl0 = delta_l; a.dl1 = delta_m;
+  a.support = support; a.os = oversampling;
+  a.nt = nt; a.nb = nb; a.nchan = nchan; a.npol = npol;
+  a.n_img_chan = n_img_chan; a.n_img_pol = n_img_pol;
+  k_grid_plain<<<(unsigned)((rows + 255) / 256), 256, 0, as_stream(stream)>>>(a);
+  AV_LAUNCH_CHECK();
+  return AV_OK;
+}
+
+size_t av_grid_tiled_workspace_size(int64_t nt, int64_t nb, int64_t nchan, int64_t n_u,
+                                    int64_t n_v, int64_t n_img_chan, int support) {
+  PlanGeom g;
+  plan_geometry(g, nt, nb, nchan, n_img_chan, n_u, n_v, support, 100);
+  return plan_workspace_bytes(g);
+}
+
+static int grid_geom_checked(PlanGeom &g, int64_t n_u, int64_t n_v, int support,
+                             int oversampling, int64_t nt, int64_t nb, int64_t nchan,
+                             int64_t n_img_chan, void *workspace, size_t workspace_bytes,
+                             Plan &p, const char *who) {
+  AV_CHECK_ARG(support >= 3 && support <= 9, "%s: support must be in [3, 9]", who);
+  AV_CHECK_ARG(oversampling >= 1 && oversampling <= 254, "%s: oversampling must be in [1, 254]",
+               who);
+  AV_CHECK_ARG(n_u >= support && n_v >= support && n_u < 131072 && n_v < 131072,
+               "%s: grid size out of range", who);
+  AV_CHECK_ARG(nt >= 0 && nb >= 0 && nchan >= 0 && n_img_chan >= 1, "%s: bad shape", who);
+  AV_CHECK_ARG(workspace && (((uintptr_t)workspace) & 255) == 0,
+               "%s: workspace must be 256-byte aligned", who);
+  plan_geometry(g, nt, nb, nchan, n_img_chan, n_u, n_v, support, oversampling);
+  g.convention = 0;
+  g.chk_x = g.chk_y = 0;
+  g.scale0 = g.scale1 = g.offset0 = g.offset1 = 0.0;
+  size_t need = plan_workspace_bytes(g);
+  if (workspace_bytes < need) {
+    set_error("%s: workspace %zu bytes < %zu needed", who, workspace_bytes, need);
+    return AV_ERR_WORKSPACE;
+  }
+  Workspace ws(workspace, workspace_bytes);
+  if (!plan_carve(g, ws, p)) {
+    set_error("%s: workspace carve failed", who);
+    return AV_ERR_WORKSPACE;
+  }
+  return AV_OK;
+}
+
+int av_grid_tiled_plan(const double *uvw, const double *freq, const int32_t *chan_map,
+                       int64_t n_u, int64_t n_v, double delta_l, double delta_m, int support,
+                       int oversampling, int64_t nt, int64_t nb, int64_t nchan,
+                       int64_t n_img_chan, void *workspace, size_t workspace_bytes,
+                       void *stream) {
+  clear_error();
+  AV_CHECK_ARG(uvw && freq && chan_map, "av_grid_tiled_plan: null pointer");
+  PlanGeom g;
+  Plan p;
+  int rc = grid_geom_checked(g, n_u, n_v, support, oversampling, nt, nb, nchan, n_img_chan,
+                             workspace, workspace_bytes, p, "av_grid_tiled_plan");
+  if (rc) return rc;
+  return plan_build(g, p, uvw, freq, chan_map, delta_l, delta_m, as_stream(stream));
+}
+
+int av_grid_tiled_execute(void *grid, int grid_dtype, double *sum_weight, int do_psf,
+                          const void *vis, int vis_dtype, const void *weight, int weight_dtype,
+                          const int32_t *pol_map, const double *cgk, int64_t n_u, int64_t n_v,
+                          int support, int oversampling, int64_t nt, int64_t nb, int64_t nchan,
+                          int64_t npol, int64_t n_img_chan, int64_t n_img_pol, void *workspace,
+                          size_t workspace_bytes, void *stream) {
+  clear_error();
+  AV_CHECK_ARG(grid && sum_weight && weight && pol_map && cgk,
+               "av_grid_tiled_execute: null pointer");
+  AV_CHECK_ARG(do_psf || vis, "av_grid_tiled_execute: vis is required unless do_psf");
+  AV_CHECK_ARG(grid_dtype == AV_C64 || grid_dtype == AV_C128,
+               "av_grid_tiled_execute: grid must be complex64 or complex128");
+  AV_CHECK_ARG(do_psf || vis_dtype == AV_C64, "av_grid_tiled_execute: vis must be complex64");
+  AV_CHECK_ARG(weight_dtype == AV_F32, "av_grid_tiled_execute: weight must be float32");
+  AV_CHECK_ARG(npol >= 0 && npol <= 4 && n_img_pol >= 1 && n_img_pol <= 4,
+               "av_grid_tiled_execute: npol and n_img_pol must be in [1, 4]");
+  PlanGeom g;
+  Plan p;
+  int rc = grid_geom_checked(g, n_u, n_v, support, oversampling, nt, nb, nchan, n_img_chan,
+                             workspace, workspace_bytes, p, "av_grid_tiled_execute");
+  if (rc) return rc;
+  int64_t rows = nt * nb * nchan;
+  if (rows == 0 || npol == 0) return AV_OK;
+  int npol_t = npol <= 1 ? 1 : (npol <= 2 ? 2 : 4);
+  TiledGridArgs a;
+  a.recs = p.recs;
+  a.tile_start = p.tile_start;
+  a.n_rec = p.offs + g.n_keys();
+  a.n_tiles = g.n_tiles();
+  a.ntu = g.ntu;
+  a.ntv = g.ntv;
+  int sms = sm_count();
+  int64_t chunk = (rows + (int64_t)sms * 4 - 1) / ((int64_t)sms * 4);
+  if (chunk < 2048) chunk = 2048;
+  a.chunk = chunk;
+  a.vis = (const float2 *)vis;
+  a.wt = (const float *)weight;
+  a.do_psf = do_psf;
+  a.cgk = cgk;
+  a.cgk_len = oversampling * (support / 2 + 1);
+  a.os = oversampling;
+  a.pol_map = pol_map;
+  a.npol = (int)npol;
+  a.npg = (int)n_img_pol;
+  a.grid = grid;
+  a.grid_c128 = grid_dtype == AV_C128;
+  a.sumw = sum_weight;
+  a.n_u = n_u;
+  a.n_v = n_v;
+  int64_t nblocks = (rows + chunk - 1) / chunk;
+  return dispatch_support(a, support, npol_t, nblocks, as_stream(stream));
+}
+
+int av_grid_tiled(void *grid, int grid_dtype, double *sum_weight, int do_psf,
+                  const void *vis, int vis_dtype, const void *weight, int weight_dtype,
+                  const double *uvw, const double *freq, const int32_t *chan_map,
+                  const int32_t *pol_map, const double *cgk, int64_t n_u, int64_t n_v,
+                  double delta_l, double delta_m, int support, int oversampling, int64_t nt,
+                  int64_t nb, int64_t nchan, int64_t npol, int64_t n_img_chan,
+                  int64_t n_img_pol, void *workspace, size_t workspace_bytes, void *stream) {
+  int rc = av_grid_tiled_plan(uvw, freq, chan_map, n_u, n_v, delta_l, delta_m, support,
+                              oversampling, nt, nb, nchan, n_img_chan, workspace,
+                              workspace_bytes, stream);
+  if (rc) return rc;
+  return av_grid_tiled_execute(grid, grid_dtype, sum_weight, do_psf, vis, vis_dtype, weight,
+                               weight_dtype, pol_map, cgk, n_u, n_v, support, oversampling, nt,
+                               nb, nchan, npol, n_img_chan, n_img_pol, workspace,
+                               workspace_bytes, stream);
+}
+
+}  // extern "C"

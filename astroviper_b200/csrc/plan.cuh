@@ -1,0 +1,152 @@
+// Binning plan shared by the tiled gridder and degridder.
+//
+// Every (time, baseline, channel) sample whose kernel footprint lies inside
+// the grid becomes one 8-byte record, sorted by key
+//   key = ((plane * ntu + tu) * ntv + tv) * KPT + cell-in-tile / R^2
+// where (tu, tv) is the T x T tile holding the footprint's first cell
+// (fu, fv), plane the image channel, and R the in-tile resolution of the key
+// (1 = one key per cell; coarser only when planes x cells would exceed the
+// key budget).  Sorting by cell makes samples that share a cell contiguous,
+// which is what lets the gridder keep runs in registers and the degridder
+// read its sub-grid by broadcast.
+//
+// The sort is a counting sort: count keys (warp-aggregated atomics), scan,
+// scatter (warp-aggregated atomic cursors).  Order inside a key is the
+// arrival order of the atomics.
+#pragma once
+#include "common.cuh"
+
+namespace av {
+
+constexpr int TILE = 32;                       // tile edge in cells
+constexpr int64_t KEY_BUDGET = int64_t(1) << 24;  // scan capacity: 4096 blocks x 4096
+
+struct __align__(8) Rec {
+  uint32_t row;     // (t * nb + b) * nchan + c
+  uint8_t du, dv;   // footprint start inside the tile (cells)
+  uint8_t ou, ov;   // kernel offsets + 128
+};
+
+struct PlanGeom {
+  int64_t n_rows;            // nt * nb * nchan
+  int64_t nb_nchan;          // nb * nchan (rows per time step)
+  int64_t nchan;
+  int64_t n_planes;          // image channels
+  int64_t n_u, n_v;          // grid extent of axes 2 and 3
+  int64_t ntu, ntv;          // tiles per axis
+  int64_t kpt;               // keys per tile
+  int res_shift;             // log2(R)
+  int support, os;
+  int convention;            // 0 = gridder (standard_grid.py), 1 = degridder
+  // degridder only: the reference's own bounds extents and the scale/offset
+  int64_t chk_x, chk_y;      // nx = shape[3], ny = shape[2] (standard_degrid.py:407)
+  double scale0, scale1, offset0, offset1;
+  int64_t n_tiles() const { return n_planes * ntu * ntv; }
+  int64_t n_keys() const { return n_tiles() * kpt; }
+};
+
+// Fill the tile / key geometry for a grid of (n_planes, n_u, n_v).
+inline void plan_geometry(PlanGeom &g, int64_t nt, int64_t nb, int64_t nchan,
+                          int64_t n_planes, int64_t n_u, int64_t n_v, int support, int os) {
+  g.n_rows = nt * nb * nchan;
+  g.nb_nchan = nb * nchan;
+  g.nchan = nchan;
+  g.n_planes = n_planes;
+  g.n_u = n_u;
+  g.n_v = n_v;
+  int64_t span_u = n_u - support + 1, span_v = n_v - support + 1;
+  if (span_u < 1) span_u = 1;
+  if (span_v < 1) span_v = 1;
+  g.ntu = (span_u + TILE - 1) / TILE;
+  g.ntv = (span_v + TILE - 1) / TILE;
+  g.support = support;
+  g.os = os;
+  g.res_shift = 0;
+  while (g.res_shift < 5 &&
+         g.n_planes * g.ntu * g.ntv * ((int64_t)(TILE >> g.res_shift) * (TILE >> g.res_shift)) >
+             KEY_BUDGET)
+    g.res_shift++;
+  int64_t side = TILE >> g.res_shift;
+  g.kpt = side * side;
+}
+
+inline size_t plan_workspace_bytes(const PlanGeom &g) {
+  size_t b = 0;
+  b += Workspace::need(sizeof(uint32_t) * (g.n_keys() + 1));  // offsets
+  b += Workspace::need(sizeof(uint32_t) * (g.n_keys() + 1));  // cursors
+  b += Workspace::need(sizeof(uint32_t) * (g.n_tiles() + 1)); // tile starts
+  b += Workspace::need(sizeof(Rec) * (g.n_rows > 0 ? g.n_rows : 1));
+  b += Workspace::need(sizeof(double) * 2 * (g.nchan > 0 ? g.nchan : 1));
+  b += Workspace::need(sizeof(uint32_t) * 4096);               // scan partials
+  b += Workspace::need(sizeof(uint32_t) * 16);                 // counters
+  return b;
+}
+
+struct Plan {
+  uint32_t *offs;      // n_keys + 1: start of each key (exclusive scan)
+  uint32_t *cursor;    // n_keys + 1
+  uint32_t *tile_start;// n_tiles + 1
+  Rec *recs;           // n_rows (only the first n_rec are used)
+  double *scale;       // 2 * nchan: per-channel uv scale (gridder convention)
+  uint32_t *scan_tmp;
+  uint32_t *counters;
+};
+
+// Position of one sample in the gridder's convention (standard_grid.py:
+// 297-352): returns false when it is skipped.  fu/fv = first footprint cell.
+__device__ __forceinline__ bool sample_pos_grid(double um, double vm, double us0, double us1,
+                                                int64_t n_u, int64_t n_v, int support, int os,
+                                                int &fu, int &fv, int &offu, int &offv) {
+  double u = __dmul_rn(um, us0), v = __dmul_rn(vm, us1);
+  if (isnan(u) || isnan(v)) return false;
+  double u_pos = __dadd_rn(u, (double)(n_u / 2));
+  double v_pos = __dadd_rn(v, (double)(n_v / 2));
+  long long ui = trunc_ll(__dadd_rn(u_pos, 0.5)), vi = trunc_ll(__dadd_rn(v_pos, 0.5));
+  long long sc = support / 2;
+  if (!((ui + sc < n_u) && (vi + sc < n_v) && (ui - sc >= 0) && (vi - sc >= 0))) return false;
+  double uo = __dsub_rn((double)ui, u_pos), vo = __dsub_rn((double)vi, v_pos);
+  offu = (int)floor(__dadd_rn(__dmul_rn(uo, (double)os), 0.5));
+  offv = (int)floor(__dadd_rn(__dmul_rn(vo, (double)os), 0.5));
+  fu = (int)(ui - sc);
+  fv = (int)(vi - sc);
+  return true;
+}
+
+// Position in the degridder's convention (standard_degrid.py:435-462):
+// np.round (half to even), loc/off stored as int32, bounds against the
+// reference's nx = shape[3], ny = shape[2] and the true extents.
+__device__ __forceinline__ bool sample_pos_degrid(double um, double vm, double freq,
+                                                  const PlanGeom &g, int &fu, int &fv,
+                                                  int &offu, int &offv) {
+  const double c = C_LIGHT;
+  double p0 = __dadd_rn(__ddiv_rn(__dmul_rn(__dmul_rn(g.scale0, um), freq), c), g.offset0);
+  double p1 = __dadd_rn(__ddiv_rn(__dmul_rn(__dmul_rn(g.scale1, vm), freq), c), g.offset1);
+  int x0 = (int)(unsigned)(unsigned long long)trunc_ll(rint(p0));
+  int y0 = (int)(unsigned)(unsigned long long)trunc_ll(rint(p1));
+  int o0 = (int)(unsigned)(unsigned long long)trunc_ll(
+      rint(__dmul_rn(__dsub_rn((double)x0, p0), (double)g.os)));
+  int o1 = (int)(unsigned)(unsigned long long)trunc_ll(
+      rint(__dmul_rn(__dsub_rn((double)y0, p1), (double)g.os)));
+  long long beg = -(g.support / 2), end = beg + g.support;
+  long long X0 = x0, Y0 = y0;
+  if (!((X0 + beg >= 0) && (X0 + end - 1 < g.chk_x) && (Y0 + beg >= 0) &&
+        (Y0 + end - 1 < g.chk_y)))
+    return false;
+  if (!(X0 + end - 1 < g.n_u && Y0 + end - 1 < g.n_v)) return false;
+  fu = (int)(X0 + beg);
+  fv = (int)(Y0 + beg);
+  offu = o0;
+  offv = o1;
+  return true;
+}
+
+// Host: enqueue the plan build for uvw / freq / chan_map (plane per channel;
+// entries outside [0, n_planes) drop the channel).  Nothing is synchronised:
+// the record count stays on the device in offs[n_keys].
+int plan_build(const PlanGeom &g, Plan &p, const double *uvw, const double *freq,
+               const int32_t *chan_map, double delta_l, double delta_m, cudaStream_t st);
+
+// Carve a Plan out of the workspace.
+bool plan_carve(const PlanGeom &g, Workspace &ws, Plan &p);
+
+}  // namespace av

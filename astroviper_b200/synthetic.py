@@ -185,7 +185,10 @@ def clean_workload(nx=2048, psf_factor=2, n_src=50, seed=20260103, n_time=50):
     ys = rng.integers(lo, lo + inner, size=n_src)
     dirty = np.zeros((nx, nx), dtype=np.float64)
     for k in range(n_src):
+        # dirty[y, x] += S psf[pn/2 + y - ys, pn/2 + x - xs] where inside the PSF
         y0 = pn // 2 - ys[k]
         x0 = pn // 2 - xs[k]
-        dirty += flux[k] * psf[y0:y0 + nx, x0:x0 + nx].astype(np.float64)
+        ya, yb = max(0, -y0), min(nx, pn - y0)
+        xa, xb = max(0, -x0), min(nx, pn - x0)
+        dirty[ya:yb, xa:xb] += flux[k] * psf[y0 + ya:y0 + yb, x0 + xa:x0 + xb].astype(np.float64)
     return dict(dirty=dirty.astype(np.float32), psf=psf, flux=flux, xs=xs, ys=ys)

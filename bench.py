@@ -1,0 +1,501 @@
+#!/usr/bin/env python
+"""Benchmark of the standard-gridder imaging path on B200.
+
+Workload (the reference's 33M-visibility imaging case, synthetic data of its
+shape): 64 antennas in a 2 km disk, 2016 baselines x 256 time steps of 10 s x
+64 channels (1.0-1.5 GHz) x 4 polarisations = 33.03 M visibilities
+(132 M correlations), complex64, Briggs robust 0.5 imaging weights, one
+continuum 2048^2 grid of 1 arcsec cells, PSWF support 7, oversampling 100.
+
+One step = grid (binning plan + FP64-accumulating tiled gridder) + degrid
+(binning plan + tiled degridder) of all samples, inputs resident in HBM
+(1.06 GB of visibilities per step, larger than L2).  Metric: Mvis/s of the
+grid+degrid pair.  Also reported: the plain FP64 GPU gridder on the same GPU,
+relative errors against the FP64 path (grid, dirty image, degridded
+visibilities), Hogbom CLEAN iterations/s, the CPU oracle timed on this host
+and an end-to-end number through the numpy drop-in API with host buffers.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
+"""
+import argparse
+import json
+import math
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "Mvis/s grid+degrid on 1 B200 at <=1e-5 rel err vs FP64; CLEAN iter/s"
+WORKLOAD = ("64 ant (2016 bl) x 256 t x 64 ch x 4 pol = 33.03M vis, complex64, Briggs 0.5, "
+            "2048^2 continuum, 1 arcsec, support 7, oversampling 100")
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--n-time", type=int, default=256)
+    ap.add_argument("--quick", action="store_true", help="skip CPU baseline / CLEAN / e2e")
+    ap.add_argument("--no-clean", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--clean-iters", type=int, default=20000)
+    return ap.parse_args()
+
+
+def load_peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks / throttle reasons sampled during the timed region."""
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index):
+        self.idx = gpu_index
+        try:
+            import torch
+            self.idx = "GPU-" + str(torch.cuda.get_device_properties(gpu_index).uuid)
+        except Exception:
+            pass
+        self.proc = None
+        self.rows = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.idx}", f"--query-gpu={self.Q}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except Exception:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.rows.append([x.strip() for x in line.split(",")])
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        self.t.join(timeout=2)
+        sm = [float(r[1]) for r in self.rows if len(r) >= 9 and r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in self.rows if len(r) >= 9 and r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = set()
+        for r in self.rows:
+            if len(r) >= 9:
+                for k, nm in enumerate(names):
+                    if r[5 + k].lower() == "active":
+                        reasons.add(nm)
+        return {"sm_mhz": float(np.median(sm)) if sm else None,
+                "sm_max_mhz": max(mx) if mx else None, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def rel(a, b):
+    import torch
+    if isinstance(a, torch.Tensor):
+        a = a.double() if not a.is_complex() else a.to(torch.complex128)
+        b = b.double() if not b.is_complex() else b.to(torch.complex128)
+        return float(torch.linalg.vector_norm(a - b) / torch.linalg.vector_norm(b))
+    return float(np.linalg.norm((a - b).ravel()) / np.linalg.norm(b.ravel()))
+
+
+# ---------------------------------------------------------------------------
+# CPU side (oracle port on the host cores)
+# ---------------------------------------------------------------------------
+def cpu_grid_degrid(W, t_sample, nthreads):
+    """Oracle (C port of the reference's Numba kernels) gridding + degridding
+    of the first t_sample time steps; returns (seconds, n_vis, threads)."""
+    import oracle as O
+    uvw = W["uvw_np"][:t_sample]
+    vis = W["vis_np"][:t_sample]
+    wt = W["wt_np"][:t_sample]
+    cgk = O.create_prolate_spheroidal_kernel_1D(100, 7)
+    n = int(W["image_size"][0])
+    mem_ok = max(1, int((_avail_mem() * 0.5) // (n * n * 4 * 16)))
+    nth = max(1, min(nthreads, mem_ok, 64))
+    t0 = time.perf_counter()
+    g, sw = O.standard_grid(vis, uvw, wt, W["freq"], cgk, W["image_size"], W["pixelincr"],
+                            nthreads=nth)
+    flag = np.zeros(vis.shape, np.uint8)
+    O.degrid(g, uvw, W["freq"], W["pixelincr"], flag=flag, nthreads=nth)
+    dt = time.perf_counter() - t0
+    return dt, uvw.shape[0] * uvw.shape[1] * len(W["freq"]), nth
+
+
+def _avail_mem():
+    try:
+        import psutil
+        return psutil.virtual_memory().available
+    except Exception:
+        return 64 << 30
+
+
+def make_host_workload(n_time):
+    """Host copy of the workload for the CPU legs (no GPU needed)."""
+    from astroviper_b200 import synthetic as S
+    W = S.workload_large(n_time=n_time, device=None)
+    W["uvw_np"] = W["uvw"]
+    W["vis_np"] = W["vis"]
+    W["wt_np"] = np.ones(W["vis"].shape, np.float32)
+    return W
+
+
+def reference_arm(args, rank, world):
+    """Times the reference's CPU implementation of the path (the oracle port of
+    its Numba gridder/degridder; the reference itself is Python+Numba and its
+    sources do not travel) with all host threads, on a bounded sample of the
+    workload per step."""
+    if rank != 0:
+        return
+    import oracle as O
+    nthreads = os.cpu_count() or 1
+    t_sample = 4
+    W = make_host_workload(t_sample)
+    times = []
+    for i in range(args.warmup + args.steps):
+        dt, nvis, nth = cpu_grid_degrid(W, t_sample, nthreads)
+        if i >= args.warmup:
+            times.append(dt)
+    ms = 1e3 * float(np.mean(times))
+    value = nvis / (ms / 1e3) / 1e6
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": "Mvis/s",
+        "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic", "config": {"workload": WORKLOAD,
+                                        "sample": f"first {t_sample} time steps per step"},
+        "cpu_baseline": {"value": value, "unit": "Mvis/s", "cores": nth, "kind": "port",
+                         "sample": f"{nvis} vis ({t_sample} of 256 time steps) grid+degrid"},
+        "e2e": {"value": value, "unit": "Mvis/s", "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+# ---------------------------------------------------------------------------
+# GPU arm
+# ---------------------------------------------------------------------------
+def main():
+    args = parse()
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        reference_arm(args, rank, world)
+        return
+    import torch
+    import torch.distributed as dist
+    torch.cuda.set_device(local)
+    if world > 1:
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=120),
+                                device_id=torch.device("cuda", local))
+    from astroviper_b200 import _kernels as K
+    from astroviper_b200 import _lib
+    from astroviper_b200 import synthetic as S
+    from astroviper_b200.gridder import Gridder
+    dev = torch.device("cuda", local)
+    n_time = args.n_time
+
+    # ---------------------------------------------------------------- inputs
+    W = S.workload_large(n_time=n_time, device=dev)
+    vis = W["vis"]
+    nt, nb, nchan, npol = (int(s) for s in vis.shape)
+    n_vis = nt * nb * nchan
+    n_corr = n_vis * npol
+    img = W["image_size"]
+    cell = W["pixelincr"]
+    # Briggs robust 0.5 imaging weights (unit data weights, no flags), once
+    ones = torch.ones((nt, nb, nchan, npol), dtype=torch.float32, device=dev)
+    dens, swd = K.weight_density(W["uvw"], W["freq"], ones, None, img, cell)
+    bf = K.briggs_factors(dens, swd, W["robust"])
+    iw, err = K.briggs_apply(dens, bf, W["uvw"], W["freq"], ones, None, img, cell,
+                             out_dtype=torch.float32)
+    assert int(err.item()) == 0
+    del dens, ones
+    G = Gridder(W["uvw"], W["freq"], img, cell, npol, support=7, oversampling=100)
+    grid = G.new_grid()
+    sumw = torch.zeros((1, npol), dtype=torch.float64, device=dev)
+    values = torch.zeros((nt, nb, nchan, npol), dtype=torch.complex64, device=dev)
+
+    def step(ev=None):
+        G._gplan = None  # the binning plans are rebuilt every step (counted in the time)
+        grid.zero_()
+        sumw.zero_()
+        values.zero_()
+        G._dplan = None
+        if ev is not None:
+            ev[0].record()
+        G.grid(vis, iw, grid=grid, sum_weight=sumw)
+        if ev is not None:
+            ev[1].record()
+        G.degrid(grid, values=values)
+        if ev is not None:
+            ev[2].record()
+
+    # ------------------------------------------------------- warm-up / timing
+    for _ in range(max(3, args.warmup)):
+        step()
+    torch.cuda.synchronize()
+    # kernel-only timing of the two main kernels (plans built outside)
+    G._gplan = None
+    G._dplan = None
+    G.grid(vis, iw, grid=grid.zero_(), sum_weight=sumw.zero_())
+    G.degrid(grid, values=values.zero_())
+    torch.cuda.synchronize()
+    kev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True),
+            torch.cuda.Event(enable_timing=True)) for _ in range(3)]
+    for a, b, c in kev:
+        grid.zero_()
+        values.zero_()
+        a.record()
+        G.grid(vis, iw, grid=grid, sum_weight=sumw)   # plan reused: the grid kernel alone
+        b.record()
+        G.degrid(grid, values=values)                 # plan reused: the degrid kernel alone
+        c.record()
+    torch.cuda.synchronize()
+    t_grid_k = float(np.mean([a.elapsed_time(b) for a, b, c in kev]))
+    t_degrid_k = float(np.mean([b.elapsed_time(c) for a, b, c in kev]))
+
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    clocks = ClockSampler(local)
+    clocks.start()
+    launches0 = _lib.lib().av_launch_count()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(args.steps):
+        step()
+    e1.record()
+    torch.cuda.synchronize()
+    launches = int(_lib.lib().av_launch_count() - launches0)
+    if world > 1:
+        dist.barrier()
+    clk = clocks.stop()
+    ms = e0.elapsed_time(e1) / args.steps
+    t = torch.tensor([ms], dtype=torch.float64, device=dev)
+    if world > 1:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    ms = float(t.item())
+    value = n_vis * world / (ms / 1e3) / 1e6
+
+    # ---------------------------------------------------------------- accuracy
+    # FP64 references on a sample of the time steps: the plain FP64 gridder /
+    # degridder (the reference's per-sample arithmetic in FP64)
+    ts = max(1, nt // 8)
+    uvw_s = W["uvw"][:ts]
+    vis_s = vis[:ts].to(torch.complex128)
+    iw_s = iw[:ts].to(torch.float64)
+    Gs = Gridder(uvw_s, W["freq"], img, cell, npol, support=7, oversampling=100)
+    g32, s32 = Gs.grid(vis[:ts], iw[:ts])
+    torch.cuda.synchronize()
+    pa = torch.cuda.Event(enable_timing=True)
+    pb = torch.cuda.Event(enable_timing=True)
+    pa.record()
+    g64, s64 = K.grid(vis_s, iw_s, uvw_s, W["freq"], np.zeros(nchan, int), np.arange(npol),
+                      G.cgk, img, cell, 7, 100, 1, npol, precision="fp64")
+    pb.record()
+    torch.cuda.synchronize()
+    t_plain = pa.elapsed_time(pb)
+    plain_mvis = ts * nb * nchan / (t_plain / 1e3) / 1e6
+    err_grid = rel(g32, g64)
+    im32 = Gs.image(g32, s32)
+    im64 = Gs.image(g64, s64)
+    err_img = rel(im32, im64)
+    v32 = Gs.degrid(g64)
+    nx, ny = int(img[0]), int(img[1])
+    v64 = K.degrid(g64, uvw_s, W["freq"], (-cell[0] * nx, -cell[1] * ny), (nx / 2, ny / 2),
+                   (np.arange(nchan) / nchan * 1).astype(int), np.arange(npol) % npol, G.cgk, 7,
+                   100, nvchan=nchan, nvpol=npol, precision="fp64")
+    err_vis = rel(v32, v64)
+    del g64, v64, v32, vis_s
+    torch.cuda.empty_cache()
+
+    # ------------------------------------------------------------------- CLEAN
+    clean = None
+    if not (args.quick or args.no_clean) and rank == 0:
+        clean = bench_clean(args, dev)
+
+    # ------------------------------------------------------------ CPU baseline
+    cpu = None
+    if not (args.quick or args.no_cpu) and rank == 0:
+        tsc = 8
+        Wh = {"uvw_np": W["uvw"][:tsc], "vis_np": vis[:tsc].cpu().numpy(),
+              "wt_np": iw[:tsc].cpu().numpy(), "freq": W["freq"], "image_size": img,
+              "pixelincr": cell}
+        nth = os.cpu_count() or 1
+        dt, nv, used = cpu_grid_degrid(Wh, tsc, nth)
+        cpu = {"value": nv / dt / 1e6, "unit": "Mvis/s", "cores": used, "kind": "port",
+               "sample": f"{nv} vis ({tsc} of {nt} time steps, 4 pol) grid+degrid, "
+                         f"C port of the reference kernels, {used} threads"}
+
+    # --------------------------------------------------------------------- e2e
+    e2e = None
+    if not (args.quick or args.no_e2e):
+        e2e = bench_e2e(W, vis, iw, G)
+
+    peak, peak_kind = load_peaks()
+    bytes_grid = n_corr * 12 + nt * nb * 24 + nx * ny * npol * 8
+    bytes_degrid = n_corr * 9 + nt * nb * 24 + nx * ny * npol * 8
+    dom = ("k_grid_tiled", bytes_grid, t_grid_k) if t_grid_k >= t_degrid_k else \
+        ("k_degrid_tiled", bytes_degrid, t_degrid_k)
+    achieved = dom[1] / (dom[2] / 1e3) / 1e9
+    line = {
+        "metric": METRIC, "value": value, "unit": "Mvis/s", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic",
+        "config": {"workload": WORKLOAD, "n_vis": n_vis, "n_corr": n_corr,
+                   "l2": "inputs larger than L2 (1.06 GB visibilities per step)",
+                   "step": "plan+grid+plan+degrid, grid and model visibilities zeroed each step",
+                   "parallelism": f"replicas x{world}"},
+        "roofline": {"bound": "hbm", "kernel": dom[0], "achieved": achieved, "peak": peak,
+                     "unit": "GB/s", "frac": achieved / peak, "traffic": None,
+                     "peak_kind": peak_kind, "algorithmic_bytes": dom[1],
+                     "kernel_ms": dom[2]},
+        "kernels_ms": {"grid_tiled": t_grid_k, "degrid_tiled": t_degrid_k,
+                       "plan_and_rest": ms - t_grid_k - t_degrid_k},
+        "fp64_plain_gridder": {"value": plain_mvis, "unit": "Mvis/s",
+                               "sample": f"{ts} of {nt} time steps"},
+        "speedup_vs_fp64_plain": (n_vis / (t_grid_k / 1e3) / 1e6) / plain_mvis,
+        "rel_err_vs_fp64": {"grid": err_grid, "dirty_image": err_img, "degrid_vis": err_vis,
+                            "sample": f"{ts} of {nt} time steps"},
+        "clocks": clk,
+        "gpu_launches": launches,
+        "cpu_baseline": cpu,
+        "e2e": e2e,
+        "clean": clean,
+    }
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+def bench_clean(args, dev):
+    """Hogbom CLEAN: 2048^2 FP32 dirty image of 50 sources, 4096^2 PSF of the
+    small array's sampling, gain 0.1, up to clean_iters iterations or 1 mJy."""
+    import torch
+    from astroviper_b200 import _kernels as K
+    from astroviper_b200 import synthetic as S
+    cw = S.clean_workload(nx=2048, psf_factor=2, n_src=50)
+    out = {}
+    for name, psf in (("psf_4096", cw["psf"]), ("psf_2048", cw["psf"][1024:3072, 1024:3072])):
+        run = K.HogbomRun(torch.as_tensor(cw["dirty"]), torch.as_tensor(np.ascontiguousarray(psf)),
+                          niter=args.clean_iters, gain=0.1, threshold=1e-3)
+        torch.cuda.synchronize()
+        a = torch.cuda.Event(enable_timing=True)
+        b = torch.cuda.Event(enable_timing=True)
+        a.record()
+        run.run(0, args.clean_iters)
+        b.record()
+        torch.cuda.synchronize()
+        st = run.read_state()
+        ms = a.elapsed_time(b)
+        out[name] = {"iterations": st["iter"], "ms": ms, "iter_per_s": st["iter"] / (ms / 1e3),
+                     "stopped_by_threshold": bool(st["stopped"])}
+    # CPU: the reference's own Hogbom module (built from its C++ sources), a
+    # bounded number of iterations on the same-size PSF
+    try:
+        import glob
+        import importlib.util
+        so = glob.glob(os.path.join(ROOT, "oracle", "_ref", "_hogbom_ext*.so"))
+        spec = importlib.util.spec_from_file_location("_hogbom_ext", so[0])
+        H = importlib.util.module_from_spec(spec)
+        spec.loader.exec_module(H)
+        n_cpu = 200
+        psf = np.ascontiguousarray(cw["psf"][1024:3072, 1024:3072])
+        t0 = time.perf_counter()
+        H.clean(cw["dirty"], psf, max_iter=n_cpu, gain=0.1, threshold=1e-3)
+        dt = time.perf_counter() - t0
+        out["cpu_reference"] = {"iter_per_s": n_cpu / dt, "cores": 1, "kind": "reference",
+                                "sample": f"{n_cpu} iterations, 2048^2, same-size PSF"}
+        out["speedup_psf_2048"] = out["psf_2048"]["iter_per_s"] / (n_cpu / dt)
+    except Exception as e:  # the compiled reference module is optional
+        out["cpu_reference"] = {"unavailable": str(e)}
+    return out
+
+
+def bench_e2e(W, vis_dev, iw_dev, G):
+    """Same step through the numpy drop-in API with host buffers in pinned
+    memory: standard_grid_numpy_wrap_input_checked + dgrid_numba, host->device
+    copies of the inputs and device->host copies of the grid and model
+    visibilities inside the timed region."""
+    import torch
+    from astroviper_b200.core.imaging.imaging_utils import standard_degrid as SD
+    from astroviper_b200.core.imaging.imaging_utils import standard_grid as SG
+
+    def pinned_like(t):
+        h = torch.empty(t.shape, dtype=t.dtype, pin_memory=True)
+        h.copy_(t)
+        return h.numpy()
+
+    vis_h = pinned_like(vis_dev)
+    iw_h = pinned_like(iw_dev)
+    uvw = W["uvw"]
+    freq = W["freq"]
+    nt, nb, nchan, npol = vis_h.shape
+    nx, ny = int(W["image_size"][0]), int(W["image_size"][1])
+    cgk = G.cgk.cpu().numpy()
+    values_h = pinned_like(torch.zeros(vis_dev.shape, dtype=torch.complex64))
+    flag_h = pinned_like(torch.zeros(vis_dev.shape, dtype=torch.bool))
+    scale = np.array([-W["pixelincr"][0] * nx, -W["pixelincr"][1] * ny, 0.0])
+    offset = np.array([nx / 2, ny / 2, 0.0])
+    chanmap = (np.arange(nchan) / nchan * 1).astype(int)
+    polmap = np.round(np.arange(npol) % npol).astype(int)
+
+    def one():
+        grid, sw = SG.standard_grid_numpy_wrap_input_checked(
+            vis_h, np.array([]), np.array([]), uvw, iw_h, freq, cgk, W["image_size"],
+            W["pixelincr"], 100, 7, True, False, "continuum")
+        values_h[...] = 0
+        SD.dgrid_numba(uvw, np.zeros((nt, nb)), values_h, flag_h, scale, offset, grid, freq,
+                       299792458.0, 7, 100, cgk, chanmap, polmap)
+        return grid
+
+    one()
+    torch.cuda.synchronize()
+    n = 2
+    t0 = time.perf_counter()
+    for _ in range(n):
+        one()
+    torch.cuda.synchronize()
+    dt = (time.perf_counter() - t0) / n
+    gbytes = 1 * npol * nx * ny * 16
+    h2d = vis_h.nbytes + iw_h.nbytes + uvw.nbytes + gbytes + values_h.nbytes + flag_h.nbytes
+    d2h = gbytes + npol * 8 + values_h.nbytes
+    return {"value": nt * nb * nchan / dt / 1e6, "unit": "Mvis/s",
+            "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h),
+            "ms_per_step": dt * 1e3,
+            "api": "standard_grid_numpy_wrap_input_checked + dgrid_numba (numpy, pinned)"}
+
+
+if __name__ == "__main__":
+    main()

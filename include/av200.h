@@ -1,0 +1,280 @@
+/*
+ * av200.h - C ABI of libav200.so, the B200 (sm_100a) kernels of the
+ * astroviper standard-gridder imaging path.
+ *
+ * Conventions
+ *   - Every entry point returns an int status (AV_OK = 0) and never aborts;
+ *     av_last_error() gives the message of the calling thread's last failure.
+ *   - All array arguments are DEVICE pointers to C-contiguous arrays owned by
+ *     the caller; shapes are passed explicitly.  Nothing is copied to or from
+ *     the host.  `stream` is a cudaStream_t (NULL = legacy default stream).
+ *   - Scratch memory is supplied by the caller as (workspace, workspace_bytes);
+ *     the matching *_workspace_size() call says how many bytes are needed.
+ *     Workspace pointers must be 256-byte aligned.
+ *   - Array layouts follow the reference: visibilities / weights / flags are
+ *     (n_time, n_baseline, n_chan, n_pol); uvw is (n_time, n_baseline, 3)
+ *     float64 metres; grids are (n_chan, n_pol, n_u, n_v) with u on axis 2.
+ *   - dtype codes: AV_F32, AV_F64 (real), AV_C64, AV_C128 (complex,
+ *     interleaved re/im).
+ *
+ * Reference interfaces each entry point replaces are cited as
+ * file:line inside the astroviper project (src/astroviper/...).
+ */
+#ifndef AV200_H
+#define AV200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+enum av_status {
+  AV_OK = 0,
+  AV_ERR_ARG = 1,          /* invalid shape, size, dtype or pointer */
+  AV_ERR_CUDA = 2,         /* a CUDA or cuFFT call failed */
+  AV_ERR_TIMEOUT = 3,      /* a bounded device-side wait gave up */
+  AV_ERR_NAN = 4,          /* NaN where the reference raises (Briggs factors) */
+  AV_ERR_UNSUPPORTED = 5,  /* valid request this kernel does not cover */
+  AV_ERR_WORKSPACE = 6     /* workspace missing, misaligned or too small */
+};
+
+enum av_dtype { AV_F32 = 0, AV_F64 = 1, AV_C64 = 2, AV_C128 = 3 };
+
+/* Library version (major*10000 + minor*100 + patch). */
+int av_version(void);
+/* Message of this thread's last failed call ("" if none). */
+const char *av_last_error(void);
+/* Number of SMs of the current device (for launch sizing by the host). */
+int av_device_sm_count(void);
+/* Kernels launched by this library since it was loaded (all threads). */
+unsigned long long av_launch_count(void);
+
+/* ---------------------------------------------------------------- PSWF -- */
+/* prolate_spheroidal_function, gcf_prolate_spheroidal.py:102-158:
+ * grdsf[i], kern[i] = (grdsf(u), (1-u^2) grdsf(u)) for u = u_in[i] (FP64).
+ * Either output may be NULL. */
+int av_pswf(const double *u_in, int64_t n, double *grdsf, double *kern, void *stream);
+
+/* create_prolate_spheroidal_kernel_1D, gcf_prolate_spheroidal.py:87-99:
+ * out has oversampling*(support/2+1) doubles. */
+int av_pswf_table(double *out, int oversampling, int support, void *stream);
+
+/* Grid-correction image of create_prolate_spheroidal_kernel,
+ * gcf_prolate_spheroidal.py:73-79: out (nx, ny) doubles. */
+int av_corr_term(double *out, int64_t nx, int64_t ny, void *stream);
+
+/* The 4-D oversampled kernel of create_prolate_spheroidal_kernel,
+ * gcf_prolate_spheroidal.py:28-67: out (n_os, n_os, support, support) doubles
+ * with n_os = oversampling + 1 for even oversampling, else oversampling. */
+int av_pswf_kernel4d(double *out, int oversampling, int support, void *stream);
+
+/* ------------------------------------------------------------- gridding -- */
+/* Common gridding arguments (standard_grid_jit, standard_grid.py:246-432):
+ *   vis        (nt, nb, nchan, npol) of vis_dtype (AV_C64 or AV_C128); may be
+ *              NULL when do_psf != 0
+ *   weight     (nt, nb, nchan, npol) of weight_dtype (AV_F32 or AV_F64)
+ *   uvw        (nt, nb, 3) float64; freq (nchan) float64
+ *   chan_map   (nchan) int32 -> image channel; pol_map (npol) int32 -> image pol
+ *   cgk        the 1-D half kernel (oversampling*(support/2+1) doubles)
+ *   grid       (n_img_chan, n_img_pol, n_u, n_v) of grid_dtype, accumulated
+ *              (+=); AV_C64 / AV_C128, or AV_F32 / AV_F64 with do_psf
+ *   sum_weight (n_img_chan, n_img_pol) float64, accumulated (+=)
+ *   delta_lm   cell size (2) in radians, as passed to the reference.
+ */
+
+/* Plain FP64 gridder: one thread per (time, baseline, channel) sample, the
+ * reference's arithmetic and order per sample, FP64 atomic accumulation.
+ * Covers every option of standard_grid_jit including do_imaging_weight.
+ * Replaces standard_grid_jit (standard_grid.py:246). */
+int av_grid_plain(void *grid, int grid_dtype, double *sum_weight, int do_psf,
+                  int do_imaging_weight, const void *vis, int vis_dtype, const void *weight,
+                  int weight_dtype, const double *uvw, const double *freq,
+                  const int32_t *chan_map, const int32_t *pol_map, const double *cgk,
+                  int64_t n_u, int64_t n_v, double delta_l, double delta_m, int support,
+                  int oversampling, int64_t nt, int64_t nb, int64_t nchan, int64_t npol,
+                  int64_t n_img_chan, int64_t n_img_pol, void *stream);
+
+/* Scratch bytes for av_grid_tiled with these sizes. */
+size_t av_grid_tiled_workspace_size(int64_t nt, int64_t nb, int64_t nchan, int64_t n_u,
+                                    int64_t n_v, int64_t n_img_chan, int support);
+
+/* Tiled gridder (same semantics as av_grid_plain without
+ * do_imaging_weight): samples are binned by uv cell in a plan held in the
+ * workspace, each CTA accumulates a tile's sub-grid in shared memory with
+ * register-resident runs, and flushes it once.  Reads complex64 visibilities
+ * and float32 weights; index math, tap weights and all accumulation in FP64
+ * (FP32 accumulation leaves 1e-4-level errors in grid-corrected images).
+ * The grid may be complex128 (full accuracy) or complex64.  Requires
+ * npol <= 4, n_img_pol <= 4, 3 <= support <= 9, oversampling <= 254.
+ * Replaces standard_grid_jit (standard_grid.py:246) for do_imaging_weight=0. */
+/* The two halves of av_grid_tiled: _plan bins the samples (depends only on
+ * uvw, freq, chan_map and the geometry) into the workspace; _execute grids
+ * vis / weights with that plan.  A plan is reusable for any number of
+ * executes with the same geometry (e.g. every major cycle), as long as the
+ * workspace is left untouched in between. */
+int av_grid_tiled_plan(const double *uvw, const double *freq, const int32_t *chan_map,
+                       int64_t n_u, int64_t n_v, double delta_l, double delta_m, int support,
+                       int oversampling, int64_t nt, int64_t nb, int64_t nchan,
+                       int64_t n_img_chan, void *workspace, size_t workspace_bytes,
+                       void *stream);
+int av_grid_tiled_execute(void *grid, int grid_dtype, double *sum_weight, int do_psf,
+                          const void *vis, int vis_dtype, const void *weight, int weight_dtype,
+                          const int32_t *pol_map, const double *cgk, int64_t n_u, int64_t n_v,
+                          int support, int oversampling, int64_t nt, int64_t nb, int64_t nchan,
+                          int64_t npol, int64_t n_img_chan, int64_t n_img_pol, void *workspace,
+                          size_t workspace_bytes, void *stream);
+int av_grid_tiled(void *grid, int grid_dtype, double *sum_weight, int do_psf,
+                  const void *vis, int vis_dtype, const void *weight, int weight_dtype,
+                  const double *uvw, const double *freq, const int32_t *chan_map,
+                  const int32_t *pol_map, const double *cgk, int64_t n_u, int64_t n_v,
+                  double delta_l, double delta_m, int support, int oversampling, int64_t nt,
+                  int64_t nb, int64_t nchan, int64_t npol, int64_t n_img_chan,
+                  int64_t n_img_pol, void *workspace, size_t workspace_bytes, void *stream);
+
+/* ----------------------------------------------------------- degridding -- */
+/* dgrid_numba, standard_degrid.py:388-485: values (nt, nb, nvchan, nvpol) of
+ * values_dtype (AV_C64 / AV_C128) += sum_k w_k grid_k conj(phasor) / sum_k w_k
+ * for unflagged samples whose support lies inside the grid.
+ *   flag (nt, nb, nvchan, nvpol) uint8 (0 = use); may be NULL (no flags)
+ *   dphase (nt, nb) float64; may be NULL (zero phase)
+ *   scale_x/y, offset_x/y: the first two entries of the reference's scale and
+ *              offset arrays (standard_degrid.py:572-573), by value
+ *   grid (g_nchan, g_npol, g_n2, g_n3) of grid_dtype (AV_C64 / AV_C128)
+ *   convFunc the 1-D half kernel (doubles); chanmap (nvchan), polmap (nvpol)
+ *   int32 */
+/* Plain FP64 degridder: one thread per sample and polarisation, the
+ * reference's summation order (bit-identical to it in FP64). */
+int av_degrid_plain(const double *uvw, const double *dphase, void *values, int values_dtype,
+                    const uint8_t *flag, double scale_x, double scale_y, double offset_x, double offset_y,
+                    const void *grid, int grid_dtype, int64_t g_nchan, int64_t g_npol,
+                    int64_t g_n2, int64_t g_n3, const double *freq, double c, int support,
+                    int sampling, const double *convFunc, const int32_t *chanmap,
+                    const int32_t *polmap, int64_t nt, int64_t nb, int64_t nvchan,
+                    int64_t nvpol, void *stream);
+
+size_t av_degrid_tiled_workspace_size(int64_t nt, int64_t nb, int64_t nvchan, int64_t g_n2,
+                                      int64_t g_n3, int64_t g_nchan, int support);
+
+/* FP32 tiled degridder: samples binned by uv cell, each CTA stages a tile's
+ * sub-grid in shared memory, one thread per sample, FP32 products and sums.
+ * Requires nvpol <= 4, g_npol <= 4, support <= 9, sampling <= 254. */
+/* The two halves of av_degrid_tiled (plan from uvw / freq / chanmap and the
+ * degridder's scale and offset; execute per model grid), reusable like the
+ * gridder's. */
+int av_degrid_tiled_plan(const double *uvw, const double *freq, const int32_t *chanmap,
+                         double scale_x, double scale_y, double offset_x, double offset_y,
+                         int64_t g_nchan, int64_t g_n2, int64_t g_n3, int support, int sampling,
+                         int64_t nt, int64_t nb, int64_t nvchan, void *workspace,
+                         size_t workspace_bytes, void *stream);
+int av_degrid_tiled_execute(const double *dphase, void *values, int values_dtype,
+                            const uint8_t *flag, const void *grid, int grid_dtype,
+                            int64_t g_nchan, int64_t g_npol, int64_t g_n2, int64_t g_n3,
+                            const double *freq, int support, int sampling,
+                            const double *convFunc, const int32_t *polmap, int64_t nt,
+                            int64_t nb, int64_t nvchan, int64_t nvpol, void *workspace,
+                            size_t workspace_bytes, void *stream);
+int av_degrid_tiled(const double *uvw, const double *dphase, void *values, int values_dtype,
+                    const uint8_t *flag, double scale_x, double scale_y, double offset_x, double offset_y,
+                    const void *grid, int grid_dtype, int64_t g_nchan, int64_t g_npol,
+                    int64_t g_n2, int64_t g_n3, const double *freq, double c, int support,
+                    int sampling, const double *convFunc, const int32_t *chanmap,
+                    const int32_t *polmap, int64_t nt, int64_t nb, int64_t nvchan,
+                    int64_t nvpol, void *workspace, size_t workspace_bytes, void *stream);
+
+/* ------------------------------------------------- image formation / FFT -- */
+size_t av_fft_workspace_size(int64_t nplanes, int64_t nx, int64_t ny, int precision);
+
+/* grid2image_spheroid_ms4's image step, standard_grid.py:693-708:
+ * image[p] = Re(fftshift(ifft2(ifftshift(grid[p])))) / corrTerm * nx*ny /
+ * sum_weight[p] for nplanes planes of (nx, ny).  grid AV_C64 or AV_C128;
+ * the transform is always an FP64 cuFFT Z2Z; image AV_F32 or AV_F64.
+ * sum_weight may be NULL (no division). apply_corr = 0 skips corrTerm. */
+size_t av_grid_to_image_workspace_size(int64_t nplanes, int64_t nx, int64_t ny);
+int av_grid_to_image(const void *grid, int grid_dtype, const double *sum_weight,
+                     void *image, int image_dtype, int64_t nplanes, int64_t nx, int64_t ny,
+                     int apply_corr, void *workspace, size_t workspace_bytes, void *stream);
+
+/* fft_lm_to_uv (fft.py:5) with inverse = 0 and ifft_uv_to_lm (ifft.py:5)
+ * with inverse = 1, over the last two axes of nplanes (nx, ny) planes:
+ * out = fftshift(fft2 / ifft2(ifftshift(in))).  in/out AV_C64 or AV_C128
+ * (same dtype); inverse output is complex (take .real on the host side). */
+int av_fft_shifted(const void *in, void *out, int dtype, int64_t nplanes, int64_t nx,
+                   int64_t ny, int inverse, void *workspace, size_t workspace_bytes,
+                   void *stream);
+
+/* -------------------------------------------------------- imaging weights -- */
+/* grid_imaging_weights_jit, grid_imaging_weights.py:93-206, fused with the
+ * flag->NaN and polarisation averaging of calculate_imaging_weights.py:183-198:
+ * wt (nt, nb, nchan, npol) of wt_dtype; flag same shape uint8 or NULL.
+ * density (nchan, 1, n_u, n_v) float64 and sum_weight (nchan, 1) float64 are
+ * accumulated.  npol in {1, 2, 4}: 2 averages pols (0,1), 4 averages (0,3). */
+int av_weight_density(double *density, double *sum_weight, const double *uvw,
+                      const double *freq, const void *wt, int wt_dtype, const uint8_t *flag,
+                      int64_t n_u, int64_t n_v, double delta_l, double delta_m, int64_t nt,
+                      int64_t nb, int64_t nchan, int64_t npol, void *stream);
+
+/* calculate_briggs_params, briggs_weighting.py:1-31 ("briggs"):
+ * factors (2, nplanes): [0] = (5*10^-robust)^2 / (sum(G^2)/sum_weight), [1] = 1.
+ * sum(G^2) is an FP64 reduction in a fixed order (deterministic). */
+size_t av_briggs_factors_workspace_size(int64_t nplanes);
+int av_briggs_factors(const double *density, const double *sum_weight, double *factors,
+                      int64_t nplanes, int64_t n_u, int64_t n_v, double robust,
+                      void *workspace, size_t workspace_bytes, void *stream);
+
+/* degrid_imaging_weights_jit, grid_imaging_weights.py:285-443, with the
+ * input preparation and the tiling to n_pol of calculate_imaging_weights.py
+ * (:228-261): out (nt, nb, nchan, npol) of out_dtype gets the imaging weight
+ * of each sample (0 off-grid, NaN where flagged).  *err_flag (device int32,
+ * zeroed by the caller) is set to 1 where the reference raises ValueError
+ * ("NaN in briggs_factors", a NaN factor on a used cell). */
+int av_briggs_apply(void *out, int out_dtype, const double *density, const double *factors,
+                    const double *uvw, const double *freq, const void *wt, int wt_dtype,
+                    const uint8_t *flag, int64_t n_u, int64_t n_v, double delta_l,
+                    double delta_m, int64_t nt, int64_t nb, int64_t nchan, int64_t npol,
+                    int32_t *err_flag, void *stream);
+
+/* ------------------------------------------------------------ Hogbom CLEAN -- */
+/* hclean::maximg, hclean.cpp:51-81: out[0] = min, out[1] = max over pixels
+ * with mask > 0.5 (mask may be NULL).  dtype AV_F32 / AV_F64; out of dtype. */
+int av_maximg(const void *image, const void *mask, int dtype, int64_t nx, int64_t ny,
+              void *out, void *stream);
+
+/* Persistent state of one Hogbom run (device memory, 256 bytes). */
+size_t av_hogbom_state_size(void);
+size_t av_hogbom_workspace_size(int64_t nx, int64_t ny, int dtype);
+
+/* hclean::clean, hclean.cpp:106-210 (bindings.cpp:63-208 for the box):
+ * runs iterations [iter_begin, iter_end) of Hogbom CLEAN on residual (ny, nx)
+ * in place, adding components to model (ny, nx); psf (pny, pnx) with its
+ * centre at (pny/2, pnx/2) - pnx = nx, pny = ny is the reference exactly.
+ * One cooperative persistent launch; each iteration fuses the PSF
+ * subtraction with the next peak search, with one bounded grid barrier.
+ * state carries the current peak between calls: pass init_state = 1 on the
+ * first call.  On return the host reads (via av_hogbom_state_read) the next
+ * iteration number, the peak (px, py, value, |value|) and whether the
+ * threshold stopped the loop.  Arithmetic is bit-identical to the reference
+ * (no fused multiply-add, first-maximum tie break). */
+int av_hogbom_run(void *model, void *residual, const void *psf, const void *mask, int dtype,
+                  int64_t nx, int64_t ny, int64_t pnx, int64_t pny, int xbeg, int xend,
+                  int ybeg, int yend, int niter, int siter, int iter_begin, int iter_end,
+                  double gain, double threshold, double speedup, void *state, int init_state,
+                  void *workspace, size_t workspace_bytes, void *stream);
+
+/* Copies the state to the host: out_i[0] = next iteration, [1] = px,
+ * [2] = py, [3] = stopped by threshold, [4] = device error code;
+ * out_d[0] = peak value, out_d[1] = |peak|.  Synchronises the stream. */
+int av_hogbom_state_read(const void *state, int32_t *out_i, double *out_d, void *stream);
+
+/* Sum of |model| over pixels in row-major order with sequential FP32/FP64
+ * addition (the total_flux_cleaned of bindings.cpp:181-186).  out one value
+ * of dtype. */
+size_t av_abs_sum_workspace_size(int64_t n, int dtype);
+int av_abs_sum_ordered(const void *model, int dtype, int64_t n, void *out, void *workspace,
+                       size_t workspace_bytes, void *stream);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* AV200_H */
