@@ -154,9 +154,10 @@ def grid(vis, weight, uvw, freq, chan_map, pol_map, cgk, n_uv, delta_lm, support
 
 def degrid(grid_t, uvw, freq, scale, offset, chanmap, polmap, cgk, support, sampling,
            values=None, flag=None, dphase=None, c=C_LIGHT, nvchan=None, nvpol=None,
-           precision="fp32"):
-    """values (nt, nb, nvchan, nvpol) += degridded model (allocated as zeros of
-    complex64 / complex128 when None)."""
+           precision="fp32", accumulate=True):
+    """values (nt, nb, nvchan, nvpol) += degridded model (accumulate) or =
+    model with zeros for skipped samples (not accumulate, tiled kernel only);
+    values are allocated (complex64 / complex128) when None."""
     dev = device()
     g = on_device(grid_t)
     if g.dtype not in (torch.complex64, torch.complex128):
@@ -176,11 +177,17 @@ def degrid(grid_t, uvw, freq, scale, offset, chanmap, polmap, cgk, support, samp
                 and float(c) == C_LIGHT)
     if values is None:
         vdt = torch.complex64 if tiled_ok else torch.complex128
-        values = torch.zeros((nt, nb, nvchan, nvpol), dtype=vdt, device=dev)
+        if tiled_ok and not accumulate:
+            values = torch.empty((nt, nb, nvchan, nvpol), dtype=vdt, device=dev)
+        else:
+            values = torch.zeros((nt, nb, nvchan, nvpol), dtype=vdt, device=dev)
+            accumulate = True
     assert values.is_contiguous()
-    args_common = (p(uvw), p(dph), p(values), dcode(values), p(fl), float(scale[0]),
-                   float(scale[1]), float(offset[0]), float(offset[1]))
     if not tiled_ok:
+        if not accumulate:
+            values.zero_()
+        args_common = (p(uvw), p(dph), p(values), dcode(values), p(fl), float(scale[0]),
+                       float(scale[1]), float(offset[0]), float(offset[1]))
         rc = lib().av_degrid_plain(*args_common, p(g), dcode(g), g_nchan, g_npol, g_n2, g_n3,
                                    p(freq), float(c), int(support), int(sampling), p(cgk), p(cm),
                                    p(pm), nt, nb, nvchan, nvpol, stream_ptr())
@@ -191,7 +198,9 @@ def degrid(grid_t, uvw, freq, scale, offset, chanmap, polmap, cgk, support, samp
     ws_bytes = lib().av_degrid_tiled_workspace_size(nt, nb, nvchan, g_n2, g_n3, g_nchan,
                                                     int(support))
     _buf, wptr, wbytes = workspace(ws_bytes)
-    rc = lib().av_degrid_tiled(*args_common, p(g), dcode(g), g_nchan, g_npol, g_n2, g_n3,
+    rc = lib().av_degrid_tiled(p(uvw), p(dph), p(values), dcode(values), int(bool(accumulate)),
+                               p(fl), float(scale[0]), float(scale[1]), float(offset[0]),
+                               float(offset[1]), p(g), dcode(g), g_nchan, g_npol, g_n2, g_n3,
                                p(freq), float(c), int(support), int(sampling), p(cgk), p(cm),
                                p(pm), nt, nb, nvchan, nvpol, wptr, wbytes, stream_ptr())
     check(rc, "av_degrid_tiled")

@@ -43,17 +43,23 @@ SIGNATURES = {
     "av_degrid_plain": (_i, [_vp, _vp, _vp, _i, _vp, _d, _d, _d, _d, _vp, _i, _i64, _i64, _i64,
                              _i64, _vp, _d, _i, _i, _vp, _vp, _vp, _i64, _i64, _i64, _i64,
                              _vp]),
+    "av_degrid_plain_adjoint": (_i, [_vp, _vp, _vp, _i, _vp, _d, _d, _d, _d, _vp, _i, _i64, _i64,
+                                     _i64, _i64, _vp, _d, _i, _i, _vp, _vp, _vp, _i64, _i64,
+                                     _i64, _i64, _vp]),
+    "av_degrid_tiled_adjoint": (_i, [_vp, _i, _vp, _i, _vp, _i64, _i64, _i64, _i64, _i, _i, _vp,
+                                     _vp, _i64, _i64, _i64, _i64, _vp, _sz, _vp]),
     "av_degrid_tiled_workspace_size": (_sz, [_i64, _i64, _i64, _i64, _i64, _i64, _i]),
     "av_degrid_tiled_plan": (_i, [_vp, _vp, _vp, _d, _d, _d, _d, _i64, _i64, _i64, _i, _i, _i64,
                                   _i64, _i64, _vp, _sz, _vp]),
-    "av_degrid_tiled_execute": (_i, [_vp, _vp, _i, _vp, _vp, _i, _i64, _i64, _i64, _i64, _vp, _i,
-                                     _i, _vp, _vp, _i64, _i64, _i64, _i64, _vp, _sz, _vp]),
-    "av_degrid_tiled": (_i, [_vp, _vp, _vp, _i, _vp, _d, _d, _d, _d, _vp, _i, _i64, _i64, _i64,
-                             _i64, _vp, _d, _i, _i, _vp, _vp, _vp, _i64, _i64, _i64, _i64, _vp,
-                             _sz, _vp]),
+    "av_degrid_tiled_execute": (_i, [_vp, _vp, _i, _i, _vp, _vp, _i, _i64, _i64, _i64, _i64, _vp,
+                                     _i, _i, _vp, _vp, _i64, _i64, _i64, _i64, _vp, _sz, _vp]),
+    "av_degrid_tiled": (_i, [_vp, _vp, _vp, _i, _i, _vp, _d, _d, _d, _d, _vp, _i, _i64, _i64,
+                             _i64, _i64, _vp, _d, _i, _i, _vp, _vp, _vp, _i64, _i64, _i64, _i64,
+                             _vp, _sz, _vp]),
     "av_fft_workspace_size": (_sz, [_i64, _i64, _i64, _i]),
     "av_grid_to_image_workspace_size": (_sz, [_i64, _i64, _i64]),
     "av_grid_to_image": (_i, [_vp, _i, _vp, _vp, _i, _i64, _i64, _i64, _i, _vp, _sz, _vp]),
+    "av_image_to_grid": (_i, [_vp, _i, _vp, _i, _i64, _i64, _i64, _i, _vp, _sz, _vp]),
     "av_fft_shifted": (_i, [_vp, _vp, _i, _i64, _i64, _i64, _i, _vp, _sz, _vp]),
     "av_weight_density": (_i, [_vp, _vp, _vp, _vp, _vp, _i, _vp, _i64, _i64, _d, _d, _i64, _i64,
                                _i64, _i64, _vp]),

@@ -118,6 +118,7 @@ def clean(dirty_image, psf, mask=None, clean_box=(-1, -1, -1, -1), max_iter=100,
         cycle = max(1, int((niter - siter) / 10)) if niter - siter >= 0 else 1
         run.run(siter, siter)  # peak of the first iteration only
         st = run.read_state()
+        last = None
         while True:
             it = st["iter"]
             if st["stopped"] or it >= niter:
@@ -135,10 +136,21 @@ def clean(dirty_image, psf, mask=None, clean_box=(-1, -1, -1, -1), max_iter=100,
             nxt = it + 1
             while nxt < niter and (nxt % cycle) != 1:
                 nxt += 1
-            run.run(it, min(nxt, niter))
+            end = min(nxt, niter)
+            if end == niter and it < niter - 1:
+                # stop one short so the peak of the last iteration is kept
+                run.run(it, niter - 1)
+                st = run.read_state()
+                continue
+            if it == niter - 1:
+                last = st
+            run.run(it, end)
             st = run.read_state()
         if st["iter"] > siter and progress_callback is not None:
-            progress_callback(st["iter"], st["px"], st["py"], float(tdt(st["peak"])))
+            # a loop that ran out of iterations reports the peak its last
+            # iteration subtracted (hclean.cpp:124,202-203)
+            rep = last if (st["iter"] >= niter and last is not None) else st
+            progress_callback(st["iter"], rep["px"], rep["py"], float(tdt(rep["peak"])))
     final_iter = min(st["iter"], niter) if st["iter"] > niter else st["iter"]
     mm = K.maximg(run.resid, run.mask).cpu().numpy()
     final_peak = max(abs(mm[0]), abs(mm[1]))

@@ -60,10 +60,7 @@ def _degrid_inplace(uvw, dphase, values, flag, scale, offset, grid, freq, c, sup
         d = np.asarray(dphase) if not H.is_torch(dphase) else dphase
         if H.is_torch(d) or np.any(d != 0):
             dph = H.dev(d, torch.float64)
-    if precision == "fp32" and vals.dtype == torch.complex128:
-        acc = vals  # FP32 products, added into the complex128 values
-    else:
-        acc = vals
+    acc = vals
     K.degrid(grid, uvw, freq, scale, offset, chanmap, polmap, convFunc, int(support),
              int(sampling), values=acc, flag=None if flag is None else H.dev(flag),
              dphase=dph, c=float(c), precision=precision)
@@ -121,11 +118,8 @@ def degrid_spheroid_ms4(vis, grid, pixelincr, support: int = 7, sampling: int = 
     uvw = vis.UVW.data
     dims = vis.dims
     dphase = None  # the reference grids at the phase centre: zero phase
-    if not incremental or "VISIBILITY_MODEL" not in vis:
-        modvis = np.zeros((dims["time"], dims["baseline_id"], dims["frequency"],
-                           dims["polarization"]), dtype=np.complex128)
-    else:
-        modvis = vis.VISIBILITY_MODEL.data
+    fresh = not incremental or "VISIBILITY_MODEL" not in vis
+    modvis = None if fresh else vis.VISIBILITY_MODEL.data
     flag = vis.FLAG.data
     uvwmask = np.isnan(np.asarray(uvw))
     nan_it, nan_ib = np.where(uvwmask.any(axis=-1))
@@ -141,8 +135,20 @@ def degrid_spheroid_ms4(vis, grid, pixelincr, support: int = 7, sampling: int = 
     npol = grid.shape[1]
     chanmap = (np.arange(dims["frequency"]) / dims["frequency"] * nchan).astype(int)
     polmap = np.round(np.arange(dims["polarization"]) % npol).astype(int)
-    _degrid_inplace(uvw, dphase, modvis, flag, scale, offset, grid, freq, C_LIGHT, support,
-                    sampling, convFunc, chanmap, polmap, precision)
+    if fresh:
+        # a fresh model (np.zeros then += in the reference): the tiled kernel
+        # stores every sample (zeros where skipped) straight into a complex128
+        # device array, which is copied back once
+        p = resolve_precision(precision)
+        shape = (dims["time"], dims["baseline_id"], dims["frequency"], dims["polarization"])
+        vals = torch.empty(shape, dtype=torch.complex128, device=K.device())
+        K.degrid(grid, uvw, freq, scale, offset, chanmap, polmap, convFunc, int(support),
+                 int(sampling), values=vals, flag=H.dev(flag), precision=p,
+                 accumulate=False)
+        modvis = H.host(vals)
+    else:
+        _degrid_inplace(uvw, dphase, modvis, flag, scale, offset, grid, freq, C_LIGHT, support,
+                        sampling, convFunc, chanmap, polmap, precision)
     datdims = vis.VISIBILITY.dims
     datcoords = vis.VISIBILITY.coords
     try:

@@ -32,10 +32,7 @@ def _grid_into(grid, sum_weight, do_psf, do_imaging_weight, vis_data, uvw, freq_
     sw_dev = H.dev(sum_weight, torch.float64)
     if precision == "fp32" and real_grid:
         precision = "fp64"  # the tiled kernel writes complex grids only
-    if precision == "fp32" and g_dev.dtype == torch.complex128:
-        target = g_dev  # FP32 products, accumulated into the complex128 grid
-    else:
-        target = g_dev
+    target = g_dev
     K.grid(None if do_psf else vis_data, H.dev(weight), uvw, freq_chan, chan_map, pol_map,
            cgk_1D, n_uv, delta_lm, support, oversampling, n_img_chan, n_img_pol,
            grid_out=target, sum_weight=sw_dev, do_psf=do_psf,
@@ -196,9 +193,8 @@ def grid2image_spheroid_ms4(
         freq_chan = elvis.coords["frequency"].values
         n_imag_chan, chan_map, n_imag_pol, pol_map = _maps(weight, chan_mode)
         if gridvis is None:
-            p = resolve_precision(precision)
-            gdt = torch.complex64 if p == "fp32" else torch.complex128
-            gridvis = torch.zeros((n_imag_chan, n_imag_pol, nx, ny), dtype=gdt,
+            # complex128 in both precisions: the fp32 kernel accumulates in FP64
+            gridvis = torch.zeros((n_imag_chan, n_imag_pol, nx, ny), dtype=torch.complex128,
                                   device=K.device())
             sumwt = torch.zeros((n_imag_chan, n_imag_pol), dtype=torch.float64,
                                 device=K.device())

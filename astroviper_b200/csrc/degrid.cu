@@ -106,16 +106,93 @@ __global__ void __launch_bounds__(256) k_degrid_plain(DegridArgs a) {
   }
 }
 
+// Adjoint of k_degrid_plain: grid[c, p, x, y] += w / norm * phasor * values
+// for each unflagged sample (FP64, atomics), with the degridder's exact
+// positions - the gradient of the degridder for finite-difference checks.
+__global__ void __launch_bounds__(256) k_degrid_adjoint_plain(DegridArgs a) {
+  int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  int64_t total = a.nt * a.nb * a.nvchan * a.nvpol;
+  if (k >= total) return;
+  int64_t row = k / a.nvpol;
+  int ipol = (int)(k - row * a.nvpol);
+  int64_t tb = row / a.nvchan;
+  int ichan = (int)(row - tb * a.nvchan);
+  int apol = a.polmap[ipol];
+  if (!(0 <= apol && apol < a.g_npol)) return;
+  int achan = a.chanmap[ichan];
+  if (!(0 <= achan && achan < a.g_nchan)) return;
+  if (a.flag && a.flag[k]) return;
+  const double f = a.freq[ichan];
+  double p0 = __dadd_rn(__ddiv_rn(__dmul_rn(__dmul_rn(a.scale0, a.uvw[3 * tb]), f), a.c), a.offset0);
+  double p1 = __dadd_rn(__ddiv_rn(__dmul_rn(__dmul_rn(a.scale1, a.uvw[3 * tb + 1]), f), a.c), a.offset1);
+  int x0 = (int)(unsigned)(unsigned long long)trunc_ll(rint(p0));
+  int y0 = (int)(unsigned)(unsigned long long)trunc_ll(rint(p1));
+  int o0 = (int)(unsigned)(unsigned long long)trunc_ll(rint(__dmul_rn(__dsub_rn((double)x0, p0), (double)a.sampling)));
+  int o1 = (int)(unsigned)(unsigned long long)trunc_ll(rint(__dmul_rn(__dsub_rn((double)y0, p1), (double)a.sampling)));
+  const long long beg = -(a.support / 2), end = beg + a.support;
+  if (!(((long long)x0 + beg >= 0) && ((long long)x0 + end - 1 < a.g_n3) &&
+        ((long long)y0 + beg >= 0) && ((long long)y0 + end - 1 < a.g_n2)))
+    return;
+  if (!((long long)x0 + end - 1 < a.g_n2 && (long long)y0 + end - 1 < a.g_n3)) return;
+  double norm = 0.0;
+  for (long long ix = beg; ix < end; ++ix) {
+    long long i1 = (long long)a.sampling * ix + o0;
+    double wtx = a.cf[i1 < 0 ? -i1 : i1];
+    for (long long iy = beg; iy < end; ++iy) {
+      long long i2 = (long long)a.sampling * iy + o1;
+      norm = __dadd_rn(norm, __dmul_rn(wtx, a.cf[i2 < 0 ? -i2 : i2]));
+    }
+  }
+  if (norm == 0.0) return;
+  double vr, vi;
+  if (a.values_c128) {
+    double2 v = ((const double2 *)a.values)[k];
+    vr = v.x; vi = v.y;
+  } else {
+    float2 v = ((const float2 *)a.values)[k];
+    vr = v.x; vi = v.y;
+  }
+  if (a.dphase) {
+    double phase = __ddiv_rn(__dmul_rn(__dmul_rn(-2.0 * 3.141592653589793, a.dphase[tb]), f), a.c);
+    double s, c;
+    sincos(phase, &s, &c);
+    double r = vr * c - vi * s, i = vr * s + vi * c;  // values * phasor
+    vr = r;
+    vi = i;
+  }
+  vr /= norm;
+  vi /= norm;
+  const int64_t plane = ((int64_t)achan * a.g_npol + apol) * a.g_n2 * a.g_n3;
+  for (long long ix = beg; ix < end; ++ix) {
+    long long i1 = (long long)a.sampling * ix + o0;
+    double wtx = a.cf[i1 < 0 ? -i1 : i1];
+    for (long long iy = beg; iy < end; ++iy) {
+      long long i2 = (long long)a.sampling * iy + o1;
+      double wt = wtx * a.cf[i2 < 0 ? -i2 : i2];
+      int64_t gi = plane + ((int64_t)x0 + ix) * a.g_n3 + ((int64_t)y0 + iy);
+      if (a.grid_c128) {
+        atomicAdd(&((double2 *)a.grid)[gi].x, wt * vr);
+        atomicAdd(&((double2 *)a.grid)[gi].y, wt * vi);
+      } else {
+        atomicAdd(&((float2 *)a.grid)[gi].x, (float)(wt * vr));
+        atomicAdd(&((float2 *)a.grid)[gi].y, (float)(wt * vi));
+      }
+    }
+  }
+}
+
 // ---------------------------------------------------------------- tiled ----
 constexpr int DT_THREADS = 256;
 
 struct TiledDegridArgs {
   const Rec *recs;
   const uint32_t *tile_start;
-  const uint32_t *n_rec;
+  const uint32_t *n_rec;    // device: usable records (offs[n_keys])
+  int64_t n_rows;           // all samples (the plan also lists skipped ones)
   int64_t n_tiles, ntu, ntv, chunk;
   DegridArgs d;
   int cgk_len;
+  int accumulate;           // 1: values +=, 0: values = (skipped samples get 0)
 };
 
 template <int S, int NPG>
@@ -124,7 +201,7 @@ struct DSmem {
   static constexpr int RW = (S + 3) & ~3;  // tap-table row (floats)
   static constexpr size_t tab_bytes = 256 * RW * sizeof(float);
   static constexpr size_t rs_bytes = 256 * sizeof(double);
-  static constexpr size_t sub_bytes = (size_t)NPG * W * W * sizeof(float2);
+  static constexpr size_t sub_bytes = (size_t)W * W * NPG * sizeof(float2);  // [cell][pol]
   static constexpr size_t total = tab_bytes + rs_bytes + sub_bytes;
 };
 
@@ -158,6 +235,28 @@ __device__ __forceinline__ int find_tile_d(const uint32_t *ts, int64_t n_tiles, 
   return (int)lo;
 }
 
+__device__ __forceinline__ void put_value(const DegridArgs &d, int accumulate, int64_t k,
+                                          double vr, double vi) {
+  if (d.values_c128) {
+    double2 *o = (double2 *)d.values + k;
+    if (accumulate) {
+      double2 cur = *o;
+      vr += cur.x;
+      vi += cur.y;
+    }
+    *o = make_double2(vr, vi);
+  } else {
+    float2 *o = (float2 *)d.values + k;
+    float2 v = make_float2((float)vr, (float)vi);
+    if (accumulate) {
+      float2 cur = *o;
+      v.x += cur.x;
+      v.y += cur.y;
+    }
+    *o = v;
+  }
+}
+
 template <int S, int NPG>
 __global__ void __launch_bounds__(DT_THREADS) k_degrid_tiled(TiledDegridArgs a) {
   using M = DSmem<S, NPG>;
@@ -169,17 +268,33 @@ __global__ void __launch_bounds__(DT_THREADS) k_degrid_tiled(TiledDegridArgs a) 
   const DegridArgs &d = a.d;
 
   const uint32_t n_rec = *a.n_rec;
+  const uint32_t n_all = a.accumulate ? n_rec : (uint32_t)a.n_rows;
   const uint32_t r0 = (uint32_t)(blockIdx.x * a.chunk);
-  if (r0 >= n_rec) return;
-  const uint32_t r1 = (uint32_t)min((int64_t)n_rec, (int64_t)r0 + a.chunk);
+  if (r0 >= n_all) return;
+  const uint32_t r1 = (uint32_t)min((int64_t)n_all, (int64_t)r0 + a.chunk);
+  // store mode: skipped samples (after the usable records) get zeros
+  if (!a.accumulate && r1 > n_rec) {
+    for (uint32_t r = max(r0, n_rec) + threadIdx.x; r < r1; r += DT_THREADS) {
+      const int64_t row = a.recs[r].row;
+      for (int p = 0; p < d.nvpol; ++p) put_value(d, 0, row * d.nvpol + p, 0.0, 0.0);
+    }
+  }
+  const uint32_t v1 = min(r1, n_rec);
+  if (r0 >= v1) return;
   build_tap_tables_d<S, RW>(tab, rs, d.cf, a.cgk_len, d.sampling);
+  int pmv[8];
+#pragma unroll
+  for (int p = 0; p < 8; ++p) {
+    int v = p < d.nvpol ? d.polmap[p] : -1;
+    pmv[p] = (v >= 0 && v < NPG && v < d.g_npol) ? v : -1;
+  }
 
   int t = find_tile_d(a.tile_start, a.n_tiles, r0);
   uint32_t seg_lo = r0;
   const int64_t gplane = d.g_n2 * d.g_n3;
-  while (seg_lo < r1) {
+  while (seg_lo < v1) {
     uint32_t t_end = a.tile_start[t + 1];
-    uint32_t seg_hi = min(r1, t_end);
+    uint32_t seg_hi = min(v1, t_end);
     if (seg_hi <= seg_lo) {
       ++t;
       continue;
@@ -188,10 +303,9 @@ __global__ void __launch_bounds__(DT_THREADS) k_degrid_tiled(TiledDegridArgs a) 
     const int64_t trem = t - plane * a.ntu * a.ntv;
     const int tu = (int)(trem / a.ntv), tv = (int)(trem - (int64_t)tu * a.ntv);
     __syncthreads();  // previous segment's readers are done with sub
-    // stage the sub-grid (zero outside the grid)
-    for (int i = threadIdx.x; i < NPG * W * W; i += DT_THREADS) {
-      int gp = i / (W * W);
-      int cell = i - gp * W * W;
+    // stage the sub-grid, polarisations interleaved per cell (zero outside)
+    for (int i = threadIdx.x; i < W * W * NPG; i += DT_THREADS) {
+      int cell = i / NPG, gp = i - cell * NPG;
       int iu = cell / W, iv = cell - iu * W;
       int64_t gu = (int64_t)tu * TILE + iu, gv = (int64_t)tv * TILE + iv;
       float2 v = make_float2(0.f, 0.f);
@@ -207,8 +321,12 @@ __global__ void __launch_bounds__(DT_THREADS) k_degrid_tiled(TiledDegridArgs a) 
       sub[i] = v;
     }
     __syncthreads();
-    for (uint32_t r = seg_lo + threadIdx.x; r < seg_hi; r += DT_THREADS) {
-      Rec rc = a.recs[r];
+    uint32_t r = seg_lo + threadIdx.x;
+    Rec nxt;
+    if (r < seg_hi) nxt = a.recs[r];
+    for (; r < seg_hi; r += DT_THREADS) {
+      const Rec rc = nxt;
+      if (r + DT_THREADS < seg_hi) nxt = a.recs[r + DT_THREADS];  // in flight meanwhile
       float cu[RW], cv[RW];
 #pragma unroll
       for (int k = 0; k < RW; k += 4) {
@@ -225,52 +343,62 @@ __global__ void __launch_bounds__(DT_THREADS) k_degrid_tiled(TiledDegridArgs a) 
         float2 rowacc[NPG];
 #pragma unroll
         for (int gp = 0; gp < NPG; ++gp) rowacc[gp] = make_float2(0.f, 0.f);
-        const int base = (rc.du + i) * W + rc.dv;
+        const float2 *row = sub + ((rc.du + i) * W + rc.dv) * NPG;
 #pragma unroll
-        for (int j = 0; j < S; ++j)
+        for (int j = 0; j < S; ++j) {
+          float2 gv[NPG];
+          if (NPG >= 2) {
+#pragma unroll
+            for (int gp = 0; gp < NPG; gp += 2) {
+              const float4 q = *(const float4 *)(row + j * NPG + gp);
+              gv[gp] = make_float2(q.x, q.y);
+              gv[(gp + 1) % NPG] = make_float2(q.z, q.w);
+            }
+          } else {
+            gv[0] = row[j];
+          }
 #pragma unroll
           for (int gp = 0; gp < NPG; ++gp)
-            rowacc[gp] = __ffma2_rn(make_float2(cv[j], cv[j]), sub[gp * W * W + base + j], rowacc[gp]);
+            rowacc[gp] = __ffma2_rn(make_float2(cv[j], cv[j]), gv[gp], rowacc[gp]);
+        }
 #pragma unroll
         for (int gp = 0; gp < NPG; ++gp)
           acc[gp] = __ffma2_rn(make_float2(cu[i], cu[i]), rowacc[gp], acc[gp]);
       }
       const double norm = rs[rc.ou] * rs[rc.ov];
-      if (norm == 0.0) continue;
-      const int64_t row = rc.row;
-      const int64_t tb = row / d.nvchan;
-      const int ichan = (int)(row - tb * d.nvchan);
+      const int64_t row_i = rc.row;
+      if (norm == 0.0) {  // the reference leaves such samples untouched
+        if (!a.accumulate)
+          for (int p = 0; p < d.nvpol; ++p) put_value(d, 0, row_i * d.nvpol + p, 0.0, 0.0);
+        continue;
+      }
       double ph_re = 1.0, ph_im = 0.0;
       if (d.dphase) {
+        const int64_t tb = row_i / d.nvchan;
+        const int ichan = (int)(row_i - tb * d.nvchan);
         double phase = (-2.0 * 3.141592653589793 * d.dphase[tb]) * d.freq[ichan] / d.c;
         sincos(phase, &ph_im, &ph_re);
       }
-      const float inv = (float)(1.0 / norm);
+      const double inv = 1.0 / norm;
       for (int p = 0; p < d.nvpol; ++p) {
-        int apol = d.polmap[p];
-        if (apol < 0 || apol >= NPG || apol >= d.g_npol) continue;
-        int64_t k = row * d.nvpol + p;
-        if (d.flag && d.flag[k]) continue;
+        const int64_t k = row_i * d.nvpol + p;
+        const int apol = p < 8 ? pmv[p] : -1;
+        if (apol < 0 || (d.flag && d.flag[k])) {
+          if (!a.accumulate) put_value(d, 0, k, 0.0, 0.0);
+          continue;
+        }
         float2 v = acc[0];
 #pragma unroll
         for (int gp = 1; gp < NPG; ++gp)
           if (apol == gp) v = acc[gp];
         double vr = v.x, vi = v.y;
         if (d.dphase) {
-          double cr = ph_re, ci = -ph_im;
-          double pr = vr * cr - vi * ci, pi = vr * ci + vi * cr;
+          const double cr = ph_re, ci = -ph_im;
+          const double pr = vr * cr - vi * ci, pi = vr * ci + vi * cr;
           vr = pr;
           vi = pi;
         }
-        if (d.values_c128) {
-          double2 *o = (double2 *)d.values + k;
-          double2 cur = *o;
-          *o = make_double2(cur.x + vr / norm, cur.y + vi / norm);
-        } else {
-          float2 *o = (float2 *)d.values + k;
-          float2 cur = *o;
-          *o = make_float2(cur.x + (float)vr * inv, cur.y + (float)vi * inv);
-        }
+        put_value(d, a.accumulate, k, vr * inv, vi * inv);
       }
     }
     seg_lo = seg_hi;
@@ -370,6 +498,28 @@ int av_degrid_plain(const double *uvw, const double *dphase, void *values, int v
   return AV_OK;
 }
 
+int av_degrid_plain_adjoint(const double *uvw, const double *dphase, const void *values,
+                            int values_dtype, const uint8_t *flag, double scale_x, double scale_y,
+                            double offset_x, double offset_y, void *grid, int grid_dtype,
+                            int64_t g_nchan, int64_t g_npol, int64_t g_n2, int64_t g_n3,
+                            const double *freq, double c, int support, int sampling,
+                            const double *convFunc, const int32_t *chanmap,
+                            const int32_t *polmap, int64_t nt, int64_t nb, int64_t nvchan,
+                            int64_t nvpol, void *stream) {
+  clear_error();
+  DegridArgs a;
+  int rc = fill_degrid_args(a, uvw, dphase, (void *)values, values_dtype, flag, scale_x, scale_y,
+                            offset_x, offset_y, grid, grid_dtype, g_nchan, g_npol, g_n2, g_n3,
+                            freq, c, support, sampling, convFunc, chanmap, polmap, nt, nb, nvchan,
+                            nvpol, "av_degrid_plain_adjoint");
+  if (rc) return rc;
+  int64_t total = nt * nb * nvchan * nvpol;
+  if (total == 0) return AV_OK;
+  k_degrid_adjoint_plain<<<(unsigned)((total + 255) / 256), 256, 0, as_stream(stream)>>>(a);
+  AV_LAUNCH_CHECK();
+  return AV_OK;
+}
+
 size_t av_degrid_tiled_workspace_size(int64_t nt, int64_t nb, int64_t nvchan, int64_t g_n2,
                                       int64_t g_n3, int64_t g_nchan, int support) {
   PlanGeom g;
@@ -427,7 +577,7 @@ int av_degrid_tiled_plan(const double *uvw, const double *freq, const int32_t *c
 }
 
 int av_degrid_tiled_execute(const double *dphase, void *values, int values_dtype,
-                            const uint8_t *flag, const void *grid, int grid_dtype,
+                            int accumulate, const uint8_t *flag, const void *grid, int grid_dtype,
                             int64_t g_nchan, int64_t g_npol, int64_t g_n2, int64_t g_n3,
                             const double *freq, int support, int sampling,
                             const double *convFunc, const int32_t *polmap, int64_t nt,
@@ -448,8 +598,9 @@ int av_degrid_tiled_execute(const double *dphase, void *values, int values_dtype
                                nt, nb, nvchan, workspace, workspace_bytes,
                                "av_degrid_tiled_execute");
   if (rc) return rc;
+  AV_CHECK_ARG(nvpol <= 8, "av_degrid_tiled_execute: at most 8 visibility polarisations");
   int64_t rows = nt * nb * nvchan;
-  if (rows == 0 || nvpol == 0 || g_nchan == 0) return AV_OK;
+  if (rows == 0 || nvpol == 0) return AV_OK;
   DegridArgs d;
   d.uvw = nullptr;
   d.dphase = dphase;
@@ -476,12 +627,14 @@ int av_degrid_tiled_execute(const double *dphase, void *values, int values_dtype
   a.chunk = chunk;
   a.d = d;
   a.cgk_len = sampling * (support / 2 + 1);
+  a.accumulate = accumulate ? 1 : 0;
+  a.n_rows = rows;
   int npg = g_npol <= 1 ? 1 : (g_npol <= 2 ? 2 : 4);
   return degrid_dispatch(a, support, npg, (rows + chunk - 1) / chunk, as_stream(stream));
 }
 
 int av_degrid_tiled(const double *uvw, const double *dphase, void *values, int values_dtype,
-                    const uint8_t *flag, double scale_x, double scale_y, double offset_x, double offset_y,
+                    int accumulate, const uint8_t *flag, double scale_x, double scale_y, double offset_x, double offset_y,
                     const void *grid, int grid_dtype, int64_t g_nchan, int64_t g_npol,
                     int64_t g_n2, int64_t g_n3, const double *freq, double c, int support,
                     int sampling, const double *convFunc, const int32_t *chanmap,
@@ -493,7 +646,8 @@ int av_degrid_tiled(const double *uvw, const double *dphase, void *values, int v
                                 g_n2, g_n3, support, sampling, nt, nb, nvchan, workspace,
                                 workspace_bytes, stream);
   if (rc) return rc;
-  return av_degrid_tiled_execute(dphase, values, values_dtype, flag, grid, grid_dtype, g_nchan,
+  return av_degrid_tiled_execute(dphase, values, values_dtype, accumulate, flag, grid, grid_dtype,
+                                 g_nchan,
                                  g_npol, g_n2, g_n3, freq, support, sampling, convFunc, polmap, nt,
                                  nb, nvchan, nvpol, workspace, workspace_bytes, stream);
 }

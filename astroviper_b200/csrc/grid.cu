@@ -155,7 +155,6 @@ __global__ void __launch_bounds__(256) k_grid_plain(GridArgs a) {
 // into FP64 registers and an FP64 shared-memory sub-grid.
 constexpr int GT_THREADS = 256;
 constexpr int GT_WARPS = GT_THREADS / 32;
-constexpr int GT_RPG = 32;  // records per group per batch
 
 struct TiledGridArgs {
   const Rec *recs;
@@ -172,40 +171,48 @@ struct TiledGridArgs {
   int npol, npg;
   void *grid;
   int grid_c128;
-  double *sumw;
+  double *sumw;             // may be NULL (no sum of weights)
   int64_t n_u, n_v;
+  // adjoint of the degridder: weight 1 / sum_k w_k per sample, flags honoured
+  int inv_norm;
+  const uint8_t *flag;      // may be NULL
 };
 
-// S taps, NPOL visibility polarisations, PPT polarisations per thread.
-template <int S, int NPOL, int PPT>
+// Thread mapping: a group of S lanes handles one sample at a time; lane g of
+// the group owns footprint row g for every polarisation and keeps S x NPOL
+// FP64 complex accumulators.  Each group streams its own contiguous slice of
+// the tile's cell-sorted samples, so its accumulators stay in one cell for a
+// whole run (median ~70 samples on the 33M workload) and the FP64 shared
+// sub-grid sees ~1 flush per run.  Every warp stages its groups' samples
+// itself (one sample per loader lane per round, loads for the next round in
+// flight while the current one is computed): no block barrier inside a tile.
+template <int S, int NPOL>
 struct GCfg {
-  static constexpr int W = TILE + S - 1;         // sub-grid edge
-  static constexpr int RW = (S + 1) & ~1;        // tap-table row (doubles)
-  static constexpr int LPG = S * (NPOL / PPT);   // lanes per group
-  static constexpr int GPW = 32 / LPG;           // groups per warp
-  static constexpr int NG = GT_WARPS * GPW;      // groups per CTA
-  static constexpr int B = NG * GT_RPG;          // records per batch
-  // padded per-group strides keep the groups of a warp on different banks
-  static constexpr int WD_STRIDE = GT_RPG * NPOL + 2;  // float2
-  static constexpr int MT_STRIDE = GT_RPG + 1;         // int2
-  static constexpr size_t tab_bytes = 256 * RW * sizeof(double);
+  static constexpr int W = TILE + S - 1;          // sub-grid edge
+  static constexpr int RW = (S + 1) & ~1;         // taps read per row (doubles)
+  static constexpr int RWP = (RW % 4 == 0) ? RW + 2 : RW;  // row stride: spreads banks
+  static constexpr int GPW = 32 / S;              // groups per warp
+  static constexpr int R = 32 / GPW;              // samples per group per round
+  static constexpr int NG = GT_WARPS * GPW;       // groups per CTA
+  static constexpr int WD_GSTRIDE = R * NPOL + 1; // double2 per group (+1: bank offset)
+  static constexpr size_t tab_bytes = 256 * RWP * sizeof(double);
   static constexpr size_t rs_bytes = 256 * sizeof(double);
-  static constexpr size_t wd_bytes = (size_t)NG * WD_STRIDE * sizeof(float2);
-  static constexpr size_t mt_bytes = (size_t)NG * MT_STRIDE * sizeof(int2);
+  static constexpr size_t wd_bytes = (size_t)GT_WARPS * GPW * WD_GSTRIDE * sizeof(double2);
+  static constexpr size_t mt_bytes = (size_t)GT_WARPS * GPW * (R + 1) * sizeof(int2);
   static size_t sub_bytes(int npg) { return (size_t)npg * W * W * sizeof(double2); }
   static size_t total(int npg) { return tab_bytes + rs_bytes + wd_bytes + mt_bytes + sub_bytes(npg); }
 };
 
-// Per-offset tap tables: tab[(o + 128) * RW + i] = cgk[|os * (i - S/2) + o|]
+// Per-offset tap tables: tab[(o + 128) * RWP + i] = cgk[|os * (i - S/2) + o|]
 // and rs[o + 128] = sum_i of the same (so sum_k w_k = rs[ou] * rs[ov]).
-template <int S, int RW>
+template <int S, int RW, int RWP>
 __device__ void build_tap_tables64(double *tab, double *rs, const double *cgk, int cgk_len,
                                    int os) {
   for (int o = threadIdx.x; o < 256; o += blockDim.x) {
     int off = o - 128;
     double s = 0.0;
 #pragma unroll
-    for (int i = 0; i < RW; ++i) {
+    for (int i = 0; i < RWP; ++i) {
       double v = 0.0;
       if (i < S) {
         int k = os * (i - S / 2) + off;
@@ -213,7 +220,7 @@ __device__ void build_tap_tables64(double *tab, double *rs, const double *cgk, i
         v = (k < cgk_len) ? cgk[k] : 0.0;
         s += v;
       }
-      tab[o * RW + i] = v;
+      tab[o * RWP + i] = v;
     }
     rs[o] = s;
   }
@@ -229,14 +236,58 @@ __device__ __forceinline__ int find_tile(const uint32_t *ts, int64_t n_tiles, ui
   return (int)lo;
 }
 
-template <int S, int NPOL, int PPT>
+// One staged sample in registers (loads in flight until used).
+template <int NPOL>
+struct Pref {
+  Rec rc;
+  float w[NPOL];
+  float2 v[NPOL];
+  bool ok;
+};
+
+template <int NPOL>
+__device__ __forceinline__ void prefetch(Pref<NPOL> &f, const TiledGridArgs &a, uint32_t r,
+                                         bool valid) {
+  f.ok = valid;
+  if (!valid) return;
+  f.rc = a.recs[r];
+  const int64_t vb = (int64_t)f.rc.row * a.npol;
+  if (a.wt == nullptr) {  // unit weights (degridder adjoint)
+#pragma unroll
+    for (int p = 0; p < NPOL; ++p) {
+      f.w[p] = p < a.npol ? ((a.flag && a.flag[vb + p]) ? 0.f : 1.f) : 0.f;
+      f.v[p] = p < a.npol ? __ldg(a.vis + vb + p) : make_float2(0.f, 0.f);
+    }
+    return;
+  }
+  if (NPOL == 4 && a.npol == 4) {
+    const float4 w4 = __ldg((const float4 *)(a.wt + vb));
+    f.w[0] = w4.x; f.w[1 % NPOL] = w4.y; f.w[2 % NPOL] = w4.z; f.w[3 % NPOL] = w4.w;
+    if (!a.do_psf) {
+      const float4 v01 = __ldg((const float4 *)(a.vis + vb));
+      const float4 v23 = __ldg((const float4 *)(a.vis + vb + 2));
+      f.v[0] = make_float2(v01.x, v01.y);
+      f.v[1 % NPOL] = make_float2(v01.z, v01.w);
+      f.v[2 % NPOL] = make_float2(v23.x, v23.y);
+      f.v[3 % NPOL] = make_float2(v23.z, v23.w);
+    }
+  } else {
+#pragma unroll
+    for (int p = 0; p < NPOL; ++p) {
+      f.w[p] = p < a.npol ? __ldg(a.wt + vb + p) : 0.f;
+      if (!a.do_psf) f.v[p] = p < a.npol ? __ldg(a.vis + vb + p) : make_float2(0.f, 0.f);
+    }
+  }
+}
+
+template <int S, int NPOL>
 __global__ void __launch_bounds__(GT_THREADS, 1) k_grid_tiled(TiledGridArgs a) {
-  using C = GCfg<S, NPOL, PPT>;
-  constexpr int W = C::W, RW = C::RW;
+  using C = GCfg<S, NPOL>;
+  constexpr int W = C::W, RW = C::RW, RWP = C::RWP, R = C::R, GPW = C::GPW;
   extern __shared__ __align__(16) unsigned char smem[];
   double *tab = (double *)smem;
   double *rs = (double *)(smem + C::tab_bytes);
-  float2 *st_wd = (float2 *)(smem + C::tab_bytes + C::rs_bytes);
+  double2 *st_wd = (double2 *)(smem + C::tab_bytes + C::rs_bytes);
   int2 *st_mt = (int2 *)(smem + C::tab_bytes + C::rs_bytes + C::wd_bytes);
   double2 *sub = (double2 *)(smem + C::tab_bytes + C::rs_bytes + C::wd_bytes + C::mt_bytes);
 
@@ -247,30 +298,25 @@ __global__ void __launch_bounds__(GT_THREADS, 1) k_grid_tiled(TiledGridArgs a) {
   const int npg = a.npg;
   const int sub_n = npg * W * W;
 
-  build_tap_tables64<S, RW>(tab, rs, a.cgk, a.cgk_len, a.os);
+  build_tap_tables64<S, RW, RWP>(tab, rs, a.cgk, a.cgk_len, a.os);
   for (int i = threadIdx.x; i < sub_n; i += GT_THREADS) sub[i] = make_double2(0.0, 0.0);
 
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  const int gq = lane / C::LPG, r = lane - gq * C::LPG;
-  const int g = r % S;        // footprint row owned by this lane
-  const int pg = r / S;       // polarisation group
-  const bool computes = gq < C::GPW;
-  const int q = warp * C::GPW + gq;  // group index in the CTA
-  // image polarisation of each of this lane's visibility polarisations (-1 drops)
-  int pm[PPT];
+  const int gq = lane / S, g = lane - gq * S;   // compute role: group in warp, row
+  const bool computes = gq < GPW;
+  const int lq = lane / R, lk = lane - lq * R;  // loader role: group in warp, slot
+  const bool loads = lq < GPW;
+  // image polarisation of each visibility polarisation (-1 drops it)
+  int pm[NPOL];
 #pragma unroll
-  for (int j = 0; j < PPT; ++j) {
-    int pp = pg * PPT + j;
-    int v = pp < a.npol ? a.pol_map[pp] : -1;
-    pm[j] = (v >= 0 && v < npg) ? v : -1;
+  for (int p = 0; p < NPOL; ++p) {
+    int v = p < a.npol ? a.pol_map[p] : -1;
+    pm[p] = (v >= 0 && v < npg) ? v : -1;
   }
-  // all polarisations, for sum_weight
-  int pmall[NPOL];
-#pragma unroll
-  for (int pp = 0; pp < NPOL; ++pp) {
-    int v = pp < a.npol ? a.pol_map[pp] : -1;
-    pmall[pp] = (v >= 0 && v < npg) ? v : -1;
-  }
+  double2 *wd_mine = st_wd + (warp * GPW + (computes ? gq : 0)) * C::WD_GSTRIDE;
+  int2 *mt_mine = st_mt + (warp * GPW + (computes ? gq : 0)) * (R + 1);
+  double2 *wd_load = st_wd + (warp * GPW + (loads ? lq : 0)) * C::WD_GSTRIDE;
+  int2 *mt_load = st_mt + (warp * GPW + (loads ? lq : 0)) * (R + 1);
 
   int t = find_tile(a.tile_start, a.n_tiles, r0);
   uint32_t seg_lo = r0;
@@ -285,130 +331,123 @@ __global__ void __launch_bounds__(GT_THREADS, 1) k_grid_tiled(TiledGridArgs a) {
     const int64_t plane = t / (a.ntu * a.ntv);
     const int64_t trem = t - plane * a.ntu * a.ntv;
     const int tu = (int)(trem / a.ntv), tv = (int)(trem - (int64_t)tu * a.ntv);
+    const uint32_t seg_n = seg_hi - seg_lo;
+    // contiguous slice of the segment per group
+    auto slice = [&](int q, uint32_t &lo, uint32_t &hi) {
+      lo = seg_lo + (uint32_t)(((uint64_t)seg_n * q) / C::NG);
+      hi = seg_lo + (uint32_t)(((uint64_t)seg_n * (q + 1)) / C::NG);
+    };
+    uint32_t my_lo, my_hi, ld_lo, ld_hi;
+    slice(warp * GPW + (computes ? gq : 0), my_lo, my_hi);
+    slice(warp * GPW + (loads ? lq : 0), ld_lo, ld_hi);
+    // rounds: the warp's longest slice
+    uint32_t len0, len1, wlo, whi;
+    slice(warp * GPW, wlo, len0);
+    slice(warp * GPW + GPW - 1, len1, whi);
+    const uint32_t max_len = ((uint64_t)seg_n + C::NG - 1) / C::NG;
+    const int n_rounds = (int)((max_len + R - 1) / R);
+    (void)len0; (void)len1; (void)wlo; (void)whi;
 
-    double2 acc[PPT][S];
+    double2 acc[NPOL][S];
 #pragma unroll
-    for (int j = 0; j < PPT; ++j)
+    for (int p = 0; p < NPOL; ++p)
 #pragma unroll
-      for (int k = 0; k < S; ++k) acc[j][k] = make_double2(0.0, 0.0);
+      for (int k = 0; k < S; ++k) acc[p][k] = make_double2(0.0, 0.0);
     int cur = -1;
     double sw[NPOL];
 #pragma unroll
-    for (int pp = 0; pp < NPOL; ++pp) sw[pp] = 0.0;
+    for (int p = 0; p < NPOL; ++p) sw[p] = 0.0;
 
     auto flush_acc = [&](int key) {
       const int du = key & 255, dv = (key >> 8) & 255;
       const int base = (du + g) * W + dv;
 #pragma unroll
-      for (int j = 0; j < PPT; ++j)
+      for (int p = 0; p < NPOL; ++p)
 #pragma unroll
         for (int k = 0; k < S; ++k) {
-          double2 v = acc[j][k];
-          if (pm[j] >= 0 && (v.x != 0.0 || v.y != 0.0)) {
-            double2 *d = &sub[pm[j] * W * W + base + k];
+          double2 v = acc[p][k];
+          if (pm[p] >= 0 && (v.x != 0.0 || v.y != 0.0)) {
+            double2 *d = &sub[pm[p] * W * W + base + k];
             atomicAdd(&d->x, v.x);
             atomicAdd(&d->y, v.y);
           }
-          acc[j][k] = make_double2(0.0, 0.0);
+          acc[p][k] = make_double2(0.0, 0.0);
         }
     };
 
-    for (uint32_t b0 = seg_lo; b0 < seg_hi; b0 += C::B) {
-      const int nbat = (int)min((uint32_t)C::B, seg_hi - b0);
-      // ---- stage: one thread per record
-      for (int j = threadIdx.x; j < nbat; j += GT_THREADS) {
-        Rec rc = a.recs[b0 + j];
-        const int qq = j / GT_RPG, jj = j - qq * GT_RPG;
-        const int64_t vb = (int64_t)rc.row * a.npol;
-        const double nrm = rs[rc.ou] * rs[rc.ov];
-        float2 wdv[NPOL];
-        float wv[NPOL];
-        if (NPOL == 4 && a.npol == 4) {
-          float4 w4 = *(const float4 *)(a.wt + vb);
-          wv[0] = w4.x; wv[1 % NPOL] = w4.y; wv[2 % NPOL] = w4.z; wv[3 % NPOL] = w4.w;
-          if (!a.do_psf) {
-            float4 v01 = *(const float4 *)(a.vis + vb);
-            float4 v23 = *(const float4 *)(a.vis + vb + 2);
-            wdv[0] = make_float2(v01.x * wv[0], v01.y * wv[0]);
-            wdv[1 % NPOL] = make_float2(v01.z * wv[1 % NPOL], v01.w * wv[1 % NPOL]);
-            wdv[2 % NPOL] = make_float2(v23.x * wv[2 % NPOL], v23.y * wv[2 % NPOL]);
-            wdv[3 % NPOL] = make_float2(v23.z * wv[3 % NPOL], v23.w * wv[3 % NPOL]);
-          } else {
+    Pref<NPOL> pf;
+    prefetch<NPOL>(pf, a, ld_lo + lk, loads && ld_lo + lk < ld_hi);
+    for (int rd = 0; rd < n_rounds; ++rd) {
+      // ---- stage this round's sample (one per loader lane) for its group
+      if (loads) {
+        int2 mt = make_int2(-1, 0);
+        if (pf.ok) {
+          const Rec rc = pf.rc;
+          const double nrm = rs[rc.ou] * rs[rc.ov];
+          const double scl = a.inv_norm ? (nrm != 0.0 ? 1.0 / nrm : 0.0) : 1.0;
 #pragma unroll
-            for (int pp = 0; pp < NPOL; ++pp) wdv[pp] = make_float2(wv[pp], 0.f);
+          for (int p = 0; p < NPOL; ++p) {
+            double2 d;
+            if (a.do_psf) d = make_double2((double)pf.w[p], 0.0);
+            else d = make_double2((double)pf.v[p].x * (double)pf.w[p] * scl,
+                                  (double)pf.v[p].y * (double)pf.w[p] * scl);
+            // the reference skips NaN and exact-zero weighted data (standard_grid.py:378)
+            const bool ok = p < a.npol && !isnan(d.x) && !isnan(d.y) && (d.x != 0.0 || d.y != 0.0);
+            wd_load[lk * NPOL + p] = ok ? d : make_double2(0.0, 0.0);
+            if (ok) sw[p] += (double)pf.w[p] * nrm;
           }
-        } else {
-#pragma unroll
-          for (int pp = 0; pp < NPOL; ++pp) {
-            wv[pp] = 0.f;
-            wdv[pp] = make_float2(0.f, 0.f);
-            if (pp < a.npol) {
-              wv[pp] = a.wt[vb + pp];
-              if (a.do_psf) {
-                wdv[pp] = make_float2(wv[pp], 0.f);
-              } else {
-                float2 v = a.vis[vb + pp];
-                wdv[pp] = make_float2(v.x * wv[pp], v.y * wv[pp]);
-              }
-            }
-          }
+          mt = make_int2((int)rc.du | ((int)rc.dv << 8), (int)rc.ou | ((int)rc.ov << 8));
         }
-        float2 *dst = st_wd + qq * C::WD_STRIDE + jj * NPOL;
-#pragma unroll
-        for (int pp = 0; pp < NPOL; ++pp) {
-          float2 d = wdv[pp];
-          // the reference skips NaN and exact-zero weighted data (standard_grid.py:378)
-          bool ok = pp < a.npol && !isnan(d.x) && !isnan(d.y) && (d.x != 0.f || d.y != 0.f);
-          dst[pp] = ok ? d : make_float2(0.f, 0.f);
-          if (ok) sw[pp] += (double)wv[pp] * nrm;
-        }
-        st_mt[qq * C::MT_STRIDE + jj] =
-            make_int2((int)rc.du | ((int)rc.dv << 8), (int)rc.ou | ((int)rc.ov << 8));
+        mt_load[lk] = mt;
       }
-      __syncthreads();
-      // ---- compute: group q takes its slice of the batch in order
+      __syncwarp();
+      // ---- next round's loads go out before this round is computed
+      if (rd + 1 < n_rounds) {
+        const uint32_t r = ld_lo + (uint32_t)(rd + 1) * R + lk;
+        prefetch<NPOL>(pf, a, r, loads && r < ld_hi);
+      }
+      // ---- compute: the group's samples of this round, in order
       if (computes) {
-        const int jn = min(GT_RPG, nbat - q * GT_RPG);
-        const float2 *wq = st_wd + q * C::WD_STRIDE;
-        const int2 *mq = st_mt + q * C::MT_STRIDE;
-        for (int jj = 0; jj < jn; ++jj) {
-          const int2 mt = mq[jj];
+        const uint32_t base_r = my_lo + (uint32_t)rd * R;
+        const int jn = base_r < my_hi ? (int)min((uint32_t)R, my_hi - base_r) : 0;
+        for (int j = 0; j < jn; ++j) {
+          const int2 mt = mt_mine[j];
           if (mt.x != cur) {
             if (cur >= 0) flush_acc(cur);
             cur = mt.x;
           }
-          const double cu = tab[(mt.y & 255) * RW + g];
-          const double *cvp = &tab[((mt.y >> 8) & 255) * RW];
+          const double cu = tab[(mt.y & 255) * RWP + g];
+          const double *cvp = &tab[((mt.y >> 8) & 255) * RWP];
           double cv[RW];
 #pragma unroll
           for (int k = 0; k < RW; k += 2) {
-            double2 c2 = *(const double2 *)(cvp + k);
+            const double2 c2 = *(const double2 *)(cvp + k);
             cv[k] = c2.x;
             cv[k + 1] = c2.y;
           }
 #pragma unroll
-          for (int j = 0; j < PPT; ++j) {
-            const float2 d = wq[jj * NPOL + pg * PPT + j];
-            const double tr = cu * (double)d.x, ti = cu * (double)d.y;
+          for (int p = 0; p < NPOL; ++p) {
+            const double2 d = wd_mine[j * NPOL + p];
+            const double tr = cu * d.x, ti = cu * d.y;
 #pragma unroll
             for (int k = 0; k < S; ++k) {
-              acc[j][k].x = fma(cv[k], tr, acc[j][k].x);
-              acc[j][k].y = fma(cv[k], ti, acc[j][k].y);
+              acc[p][k].x = fma(cv[k], tr, acc[p][k].x);
+              acc[p][k].y = fma(cv[k], ti, acc[p][k].y);
             }
           }
         }
       }
-      __syncthreads();
+      __syncwarp();
     }
     if (computes && cur >= 0) flush_acc(cur);
     // ---- sum_weight: warp reduction, one atomic per warp and polarisation
 #pragma unroll
-    for (int pp = 0; pp < NPOL; ++pp) {
-      double v = sw[pp];
+    for (int p = 0; p < NPOL; ++p) {
+      double v = sw[p];
 #pragma unroll
       for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
-      if (lane == 0 && pmall[pp] >= 0 && v != 0.0)
-        atomicAdd(&a.sumw[plane * npg + pmall[pp]], v);
+      if (lane == 0 && a.sumw && pm[p] >= 0 && v != 0.0)
+        atomicAdd(&a.sumw[plane * npg + pm[p]], v);
     }
     __syncthreads();
     // ---- flush the tile to the global grid and clear it
@@ -436,30 +475,28 @@ __global__ void __launch_bounds__(GT_THREADS, 1) k_grid_tiled(TiledGridArgs a) {
   }
 }
 
-template <int S, int NPOL, int PPT>
+template <int S, int NPOL>
 static int launch_grid_tiled(const TiledGridArgs &a, int64_t nblocks, cudaStream_t st) {
-  using C = GCfg<S, NPOL, PPT>;
+  using C = GCfg<S, NPOL>;
   size_t smem = C::total(a.npg);
   static bool configured[64] = {false};
   int dev = 0;
   AV_CUDA(cudaGetDevice(&dev));
   if (dev >= 0 && dev < 64 && !configured[dev]) {
-    AV_CUDA(cudaFuncSetAttribute(k_grid_tiled<S, NPOL, PPT>,
+    AV_CUDA(cudaFuncSetAttribute(k_grid_tiled<S, NPOL>,
                                  cudaFuncAttributeMaxDynamicSharedMemorySize, (int)C::total(4)));
     configured[dev] = true;
   }
-  k_grid_tiled<S, NPOL, PPT><<<(unsigned)nblocks, GT_THREADS, smem, st>>>(a);
+  k_grid_tiled<S, NPOL><<<(unsigned)nblocks, GT_THREADS, smem, st>>>(a);
   AV_LAUNCH_CHECK();
   return AV_OK;
 }
 
 template <int S>
 static int dispatch_npol(const TiledGridArgs &a, int npol, int64_t nb, cudaStream_t st) {
-  if (npol == 1) return launch_grid_tiled<S, 1, 1>(a, nb, st);
-  if (npol == 2) return launch_grid_tiled<S, 2, 1>(a, nb, st);
-  // four polarisations: one per lane while 4*S lanes fit a warp, else two
-  constexpr int PPT = (4 * S <= 32) ? 1 : 2;
-  return launch_grid_tiled<S, 4, PPT>(a, nb, st);
+  if (npol == 1) return launch_grid_tiled<S, 1>(a, nb, st);
+  if (npol == 2) return launch_grid_tiled<S, 2>(a, nb, st);
+  return launch_grid_tiled<S, 4>(a, nb, st);
 }
 
 static int dispatch_support(const TiledGridArgs &a, int support, int npol, int64_t nb,
@@ -618,8 +655,75 @@ int av_grid_tiled_execute(void *grid, int grid_dtype, double *sum_weight, int do
   a.sumw = sum_weight;
   a.n_u = n_u;
   a.n_v = n_v;
+  a.inv_norm = 0;
+  a.flag = nullptr;
   int64_t nblocks = (rows + chunk - 1) / chunk;
   return dispatch_support(a, support, npol_t, nblocks, as_stream(stream));
+}
+
+// Adjoint of the tiled degridder on a degrid plan (av_degrid_tiled_plan):
+// grid[c, p] += sum over unflagged samples of w_k / (sum_k w_k) * values,
+// with the degridder's cells, offsets, channel and polarisation maps.
+int av_degrid_tiled_adjoint(void *grid, int grid_dtype, const void *values, int values_dtype,
+                            const uint8_t *flag, int64_t g_nchan, int64_t g_npol, int64_t g_n2,
+                            int64_t g_n3, int support, int sampling, const double *convFunc,
+                            const int32_t *polmap, int64_t nt, int64_t nb, int64_t nvchan,
+                            int64_t nvpol, void *workspace, size_t workspace_bytes,
+                            void *stream) {
+  clear_error();
+  AV_CHECK_ARG(grid && values && convFunc && polmap, "av_degrid_tiled_adjoint: null pointer");
+  AV_CHECK_ARG(grid_dtype == AV_C64 || grid_dtype == AV_C128,
+               "av_degrid_tiled_adjoint: grid dtype");
+  AV_CHECK_ARG(values_dtype == AV_C64, "av_degrid_tiled_adjoint: values must be complex64");
+  AV_CHECK_ARG(nvpol >= 1 && nvpol <= 4 && g_npol >= 1 && g_npol <= 4,
+               "av_degrid_tiled_adjoint: polarisations must be in [1, 4]");
+  AV_CHECK_ARG(support >= 3 && support <= 9 && sampling >= 1 && sampling <= 254,
+               "av_degrid_tiled_adjoint: support / sampling out of range");
+  AV_CHECK_ARG(workspace && (((uintptr_t)workspace) & 255) == 0,
+               "av_degrid_tiled_adjoint: workspace must be 256-byte aligned");
+  PlanGeom g;
+  plan_geometry(g, nt, nb, nvchan, g_nchan > 0 ? g_nchan : 1, g_n2, g_n3, support, sampling);
+  if (workspace_bytes < plan_workspace_bytes(g)) {
+    set_error("av_degrid_tiled_adjoint: workspace too small");
+    return AV_ERR_WORKSPACE;
+  }
+  Workspace ws(workspace, workspace_bytes);
+  Plan p;
+  if (!plan_carve(g, ws, p)) {
+    set_error("av_degrid_tiled_adjoint: workspace carve failed");
+    return AV_ERR_WORKSPACE;
+  }
+  int64_t rows = nt * nb * nvchan;
+  if (rows == 0 || g_nchan == 0) return AV_OK;
+  TiledGridArgs a;
+  a.recs = p.recs;
+  a.tile_start = p.tile_start;
+  a.n_rec = p.offs + g.n_keys();
+  a.n_tiles = g.n_tiles();
+  a.ntu = g.ntu;
+  a.ntv = g.ntv;
+  int sms = sm_count();
+  int64_t chunk = (rows + (int64_t)sms * 4 - 1) / ((int64_t)sms * 4);
+  if (chunk < 2048) chunk = 2048;
+  a.chunk = chunk;
+  a.vis = (const float2 *)values;
+  a.wt = nullptr;
+  a.do_psf = 0;
+  a.cgk = convFunc;
+  a.cgk_len = sampling * (support / 2 + 1);
+  a.os = sampling;
+  a.pol_map = polmap;
+  a.npol = (int)nvpol;
+  a.npg = (int)g_npol;
+  a.grid = grid;
+  a.grid_c128 = grid_dtype == AV_C128;
+  a.sumw = nullptr;
+  a.n_u = g_n2;
+  a.n_v = g_n3;
+  a.inv_norm = 1;
+  a.flag = flag;
+  int npol_t = nvpol <= 1 ? 1 : (nvpol <= 2 ? 2 : 4);
+  return dispatch_support(a, support, npol_t, (rows + chunk - 1) / chunk, as_stream(stream));
 }
 
 int av_grid_tiled(void *grid, int grid_dtype, double *sum_weight, int do_psf,

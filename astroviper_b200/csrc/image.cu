@@ -116,6 +116,29 @@ __global__ void k_image_epilogue(const CT *buf, OT *img, const double *sumw, int
   img[k] = (OT)v;
 }
 
+// Real image -> ifftshift gather into the complex FP64 transform buffer,
+// divided by the grid correction grdsf(x) grdsf(y) when asked.
+template <typename IT>
+__global__ void k_image_prologue(const IT *img, double2 *buf, int64_t nplanes, int64_t nx,
+                                 int64_t ny, int apply_corr) {
+  int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  int64_t n = nplanes * nx * ny;
+  if (k >= n) return;
+  int64_t p = k / (nx * ny), r = k - p * nx * ny;
+  int64_t i = r / ny, j = r - i * ny;
+  int64_t si = i + nx / 2;
+  if (si >= nx) si -= nx;
+  int64_t sj = j + ny / 2;
+  if (sj >= ny) sj -= ny;
+  double v = (double)img[p * nx * ny + si * ny + sj];
+  if (apply_corr) {
+    double cx = (double)(si - nx / 2) / (double)nx;
+    double cy = (double)(sj - ny / 2) / (double)ny;
+    v = v / (pswf_grdsf(fabs(2.0 * cx)) * pswf_grdsf(fabs(2.0 * cy)));
+  }
+  buf[k] = make_double2(v, 0.0);
+}
+
 // fftshift gather of a complex result: out[i] = buf[(i + nx - nx/2) % nx].
 template <typename CT, typename OT>
 __global__ void k_shift_out(const CT *buf, OT *out, int64_t nplanes, int64_t nx, int64_t ny,
@@ -209,6 +232,51 @@ int av_grid_to_image(const void *grid, int grid_dtype, const double *sum_weight,
   else
     k_image_epilogue<double2, float><<<blocks, 256, 0, st>>>(buf, (float *)image, sum_weight,
                                                             nplanes, nx, ny, apply_corr);
+  AV_LAUNCH_CHECK();
+  return AV_OK;
+}
+
+// fft_lm_to_uv(image / corrTerm) (fft.py:5 with the grid correction of
+// gcf_prolate_spheroidal.py:73-79): the forward model's image -> grid step,
+// the adjoint of av_grid_to_image without sum_weight.  FP64 transform.
+int av_image_to_grid(const void *image, int image_dtype, void *grid, int grid_dtype,
+                     int64_t nplanes, int64_t nx, int64_t ny, int apply_corr, void *workspace,
+                     size_t workspace_bytes, void *stream) {
+  clear_error();
+  AV_CHECK_ARG(image && grid, "av_image_to_grid: null pointer");
+  AV_CHECK_ARG(image_dtype == AV_F32 || image_dtype == AV_F64, "av_image_to_grid: image dtype");
+  AV_CHECK_ARG(grid_dtype == AV_C64 || grid_dtype == AV_C128, "av_image_to_grid: grid dtype");
+  AV_CHECK_ARG(nplanes >= 0 && nx > 0 && ny > 0, "av_image_to_grid: bad shape");
+  if (nplanes == 0) return AV_OK;
+  FftPlan *p = nullptr;
+  int rc = get_plan(nplanes, nx, ny, 1, &p);
+  if (rc) return rc;
+  size_t bufb = (size_t)nplanes * nx * ny * 16;
+  if (!workspace || workspace_bytes < Workspace::need(bufb) + Workspace::need(p->work)) {
+    set_error("av_image_to_grid: workspace too small");
+    return AV_ERR_WORKSPACE;
+  }
+  Workspace ws(workspace, workspace_bytes);
+  double2 *buf = ws.take<double2>((size_t)nplanes * nx * ny);
+  void *work = ws.take<char>(p->work > 0 ? p->work : 1);
+  cudaStream_t st = as_stream(stream);
+  int64_t n = nplanes * nx * ny;
+  unsigned blocks = (unsigned)((n + 255) / 256);
+  if (image_dtype == AV_F64)
+    k_image_prologue<double><<<blocks, 256, 0, st>>>((const double *)image, buf, nplanes, nx, ny,
+                                                     apply_corr);
+  else
+    k_image_prologue<float><<<blocks, 256, 0, st>>>((const float *)image, buf, nplanes, nx, ny,
+                                                    apply_corr);
+  AV_LAUNCH_CHECK();
+  rc = run_fft(buf, 1, nplanes, nx, ny, CUFFT_FORWARD, work, st);
+  if (rc) return rc;
+  if (grid_dtype == AV_C128)
+    k_shift_out<double2, double2><<<blocks, 256, 0, st>>>(buf, (double2 *)grid, nplanes, nx, ny,
+                                                         1.0);
+  else
+    k_shift_out<double2, float2><<<blocks, 256, 0, st>>>(buf, (float2 *)grid, nplanes, nx, ny,
+                                                        1.0);
   AV_LAUNCH_CHECK();
   return AV_OK;
 }

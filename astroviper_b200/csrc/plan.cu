@@ -13,12 +13,23 @@ __global__ void k_chan_scale(const double *freq, int64_t nchan, double dl0, doub
   scale[2 * c + 1] = __ddiv_rn(-__dmul_rn(__dmul_rn(f, dl1), (double)n_v), C_LIGHT);
 }
 
+// Samples are enumerated time-fastest, k = (b * nchan + c) * nt + t, so the
+// 32 lanes of a warp hold consecutive time steps of one baseline and channel:
+// they fall in one or a few cells and the per-key atomics aggregate.
 __device__ __forceinline__ bool sample_key(const PlanGeom &g, const double *uvw,
                                            const double *freq, const double *scale,
-                                           const int32_t *chan_map, int64_t row,
+                                           const int32_t *chan_map, int64_t k,
                                            uint32_t &key, Rec &rec) {
-  int64_t tb = row / g.nchan;
-  int c = (int)(row - tb * g.nchan);
+  const int64_t nt = g.nt, nb = g.nb;
+  const int64_t t = k % nt;
+  const int64_t bc = k / nt;
+  const int c = (int)(bc % g.nchan);
+  const int64_t b = bc / g.nchan;
+  const int64_t tb = t * nb + b;
+  const int64_t row = tb * g.nchan + c;
+  rec.row = (uint32_t)row;
+  rec.du = rec.dv = rec.ou = rec.ov = 0;
+  key = (uint32_t)g.n_keys();  // skipped samples
   int plane = chan_map[c];
   if (plane < 0 || plane >= g.n_planes) return false;
   double um = uvw[3 * tb + 0], vm = uvw[3 * tb + 1];
@@ -36,7 +47,6 @@ __device__ __forceinline__ bool sample_key(const PlanGeom &g, const double *uvw,
   int side_shift = 5 - g.res_shift;  // log2(TILE >> res_shift)
   int64_t cell = ((int64_t)(du >> g.res_shift) << side_shift) + (dv >> g.res_shift);
   key = (uint32_t)(tile * g.kpt + cell);
-  rec.row = (uint32_t)row;
   rec.du = (uint8_t)du;
   rec.dv = (uint8_t)dv;
   rec.ou = (uint8_t)(ou + 128);
@@ -53,9 +63,10 @@ __global__ void __launch_bounds__(256) k_plan_count(PlanGeom g, const double *uv
     int64_t row = base + threadIdx.x;
     uint32_t key = 0xffffffffu;
     Rec rec;
-    bool ok = row < g.n_rows && sample_key(g, uvw, freq, scale, chan_map, row, key, rec);
-    unsigned active = __ballot_sync(0xffffffffu, ok);
-    if (ok) {
+    const bool in = row < g.n_rows;
+    if (in) sample_key(g, uvw, freq, scale, chan_map, row, key, rec);
+    unsigned active = __ballot_sync(0xffffffffu, in);
+    if (in) {
       unsigned peers = __match_any_sync(active, key);
       int leader = __ffs(peers) - 1;
       if ((int)(threadIdx.x & 31) == leader) atomicAdd(&hist[key], (uint32_t)__popc(peers));
@@ -74,9 +85,10 @@ __global__ void __launch_bounds__(256) k_plan_scatter(PlanGeom g, const double *
     int64_t row = base + threadIdx.x;
     uint32_t key = 0xffffffffu;
     Rec rec;
-    bool ok = row < g.n_rows && sample_key(g, uvw, freq, scale, chan_map, row, key, rec);
-    unsigned active = __ballot_sync(0xffffffffu, ok);
-    if (ok) {
+    const bool in = row < g.n_rows;
+    if (in) sample_key(g, uvw, freq, scale, chan_map, row, key, rec);
+    unsigned active = __ballot_sync(0xffffffffu, in);
+    if (in) {
       unsigned peers = __match_any_sync(active, key);
       int leader = __ffs(peers) - 1;
       uint32_t pos = 0;
@@ -186,7 +198,7 @@ static int scan_counts(uint32_t *counts_then_cursor, uint32_t *offs, int64_t n,
                        uint32_t *tmp, cudaStream_t st) {
   int64_t nb = (n + SCAN_TILE - 1) / SCAN_TILE;
   if (nb < 1) nb = 1;
-  if (nb > 4096) {
+  if (nb > SCAN_MAX_BLOCKS) {
     set_error("plan: key count %lld exceeds the scan capacity", (long long)n);
     return AV_ERR_UNSUPPORTED;
   }
@@ -208,12 +220,12 @@ __global__ void k_tile_starts(const uint32_t *offs, int64_t n_tiles, int64_t kpt
 }
 
 bool plan_carve(const PlanGeom &g, Workspace &ws, Plan &p) {
-  p.offs = ws.take<uint32_t>(g.n_keys() + 1);
-  p.cursor = ws.take<uint32_t>(g.n_keys() + 1);
+  p.offs = ws.take<uint32_t>(g.n_keys() + 2);
+  p.cursor = ws.take<uint32_t>(g.n_keys() + 2);
   p.tile_start = ws.take<uint32_t>(g.n_tiles() + 1);
   p.recs = ws.take<Rec>(g.n_rows > 0 ? g.n_rows : 1);
   p.scale = ws.take<double>(2 * (g.nchan > 0 ? g.nchan : 1));
-  p.scan_tmp = ws.take<uint32_t>(4096);
+  p.scan_tmp = ws.take<uint32_t>(SCAN_MAX_BLOCKS);
   p.counters = ws.take<uint32_t>(16);
   return p.offs && p.cursor && p.tile_start && p.recs && p.scale && p.scan_tmp && p.counters;
 }
@@ -226,7 +238,7 @@ int plan_build(const PlanGeom &g, Plan &p, const double *uvw, const double *freq
               (long long)g.n_rows);
     return AV_ERR_UNSUPPORTED;
   }
-  AV_CUDA(cudaMemsetAsync(p.cursor, 0, sizeof(uint32_t) * (nk + 1), st));
+  AV_CUDA(cudaMemsetAsync(p.cursor, 0, sizeof(uint32_t) * (nk + 2), st));
   if (g.nchan > 0) {
     k_chan_scale<<<(unsigned)((g.nchan + 127) / 128), 128, 0, st>>>(
         freq, g.nchan, delta_l, delta_m, g.n_u, g.n_v, p.scale);
@@ -240,7 +252,7 @@ int plan_build(const PlanGeom &g, Plan &p, const double *uvw, const double *freq
     k_plan_count<<<(unsigned)blocks, 256, 0, st>>>(g, uvw, freq, p.scale, chan_map, p.cursor);
     AV_LAUNCH_CHECK();
   }
-  int rc = scan_counts(p.cursor, p.offs, nk, p.scan_tmp, st);
+  int rc = scan_counts(p.cursor, p.offs, nk + 1, p.scan_tmp, st);
   if (rc) return rc;
   if (g.n_rows > 0) {
     k_plan_scatter<<<(unsigned)blocks, 256, 0, st>>>(g, uvw, freq, p.scale, chan_map, p.cursor,

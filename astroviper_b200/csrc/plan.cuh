@@ -12,14 +12,18 @@
 //
 // The sort is a counting sort: count keys (warp-aggregated atomics), scan,
 // scatter (warp-aggregated atomic cursors).  Order inside a key is the
-// arrival order of the atomics.
+// arrival order of the atomics.  Samples that are skipped (off the grid, NaN
+// uvw, channel outside the image) go to one extra key, n_keys, after all
+// tiles: offs[n_keys] counts the usable records and the rest of recs[] lists
+// the skipped rows (a store-mode degrid writes zeros there).
 #pragma once
 #include "common.cuh"
 
 namespace av {
 
 constexpr int TILE = 32;                       // tile edge in cells
-constexpr int64_t KEY_BUDGET = int64_t(1) << 24;  // scan capacity: 4096 blocks x 4096
+constexpr int SCAN_MAX_BLOCKS = 65536;                    // scan partials
+constexpr int64_t KEY_BUDGET = (int64_t(1) << 28) - 65536;  // scan capacity: 65536 x 4096 keys
 
 struct __align__(8) Rec {
   uint32_t row;     // (t * nb + b) * nchan + c
@@ -30,6 +34,7 @@ struct __align__(8) Rec {
 struct PlanGeom {
   int64_t n_rows;            // nt * nb * nchan
   int64_t nb_nchan;          // nb * nchan (rows per time step)
+  int64_t nt, nb;
   int64_t nchan;
   int64_t n_planes;          // image channels
   int64_t n_u, n_v;          // grid extent of axes 2 and 3
@@ -41,8 +46,8 @@ struct PlanGeom {
   // degridder only: the reference's own bounds extents and the scale/offset
   int64_t chk_x, chk_y;      // nx = shape[3], ny = shape[2] (standard_degrid.py:407)
   double scale0, scale1, offset0, offset1;
-  int64_t n_tiles() const { return n_planes * ntu * ntv; }
-  int64_t n_keys() const { return n_tiles() * kpt; }
+  __host__ __device__ int64_t n_tiles() const { return n_planes * ntu * ntv; }
+  __host__ __device__ int64_t n_keys() const { return n_tiles() * kpt; }
 };
 
 // Fill the tile / key geometry for a grid of (n_planes, n_u, n_v).
@@ -50,6 +55,8 @@ inline void plan_geometry(PlanGeom &g, int64_t nt, int64_t nb, int64_t nchan,
                           int64_t n_planes, int64_t n_u, int64_t n_v, int support, int os) {
   g.n_rows = nt * nb * nchan;
   g.nb_nchan = nb * nchan;
+  g.nt = nt;
+  g.nb = nb;
   g.nchan = nchan;
   g.n_planes = n_planes;
   g.n_u = n_u;
@@ -72,19 +79,20 @@ inline void plan_geometry(PlanGeom &g, int64_t nt, int64_t nb, int64_t nchan,
 
 inline size_t plan_workspace_bytes(const PlanGeom &g) {
   size_t b = 0;
-  b += Workspace::need(sizeof(uint32_t) * (g.n_keys() + 1));  // offsets
-  b += Workspace::need(sizeof(uint32_t) * (g.n_keys() + 1));  // cursors
+  b += Workspace::need(sizeof(uint32_t) * (g.n_keys() + 2));  // offsets
+  b += Workspace::need(sizeof(uint32_t) * (g.n_keys() + 2));  // cursors
   b += Workspace::need(sizeof(uint32_t) * (g.n_tiles() + 1)); // tile starts
   b += Workspace::need(sizeof(Rec) * (g.n_rows > 0 ? g.n_rows : 1));
   b += Workspace::need(sizeof(double) * 2 * (g.nchan > 0 ? g.nchan : 1));
-  b += Workspace::need(sizeof(uint32_t) * 4096);               // scan partials
+  b += Workspace::need(sizeof(uint32_t) * SCAN_MAX_BLOCKS);    // scan partials
   b += Workspace::need(sizeof(uint32_t) * 16);                 // counters
   return b;
 }
 
 struct Plan {
-  uint32_t *offs;      // n_keys + 1: start of each key (exclusive scan)
-  uint32_t *cursor;    // n_keys + 1
+  uint32_t *offs;      // n_keys + 2: start of each key (exclusive scan); the
+                       // last key (n_keys) holds the skipped samples
+  uint32_t *cursor;    // n_keys + 2
   uint32_t *tile_start;// n_tiles + 1
   Rec *recs;           // n_rows (only the first n_rec are used)
   double *scale;       // 2 * nchan: per-channel uv scale (gridder convention)

@@ -104,20 +104,24 @@ class Gridder:
             self._dplan = (key, ws)
         return self._dplan[1]
 
-    def degrid(self, grid, values=None, flag=None, dphase=None):
-        """values (nt, nb, nchan, npol) += model visibilities of grid, with the
-        conventions of degrid_spheroid_ms4 (chanmap int(i/nchan*g_nchan),
-        polmap i % g_npol)."""
+    def degrid(self, grid, values=None, flag=None, dphase=None, accumulate=False):
+        """Model visibilities of grid with the conventions of
+        degrid_spheroid_ms4 (chanmap int(i/nchan*g_nchan), polmap i % g_npol):
+        values = model (zeros for skipped samples), or values += model with
+        accumulate.  values (nt, nb, nchan, npol) complex64 / complex128 is
+        allocated when None."""
         g = grid if grid.is_contiguous() else grid.contiguous()
         g_nchan, g_npol = int(g.shape[0]), int(g.shape[1])
         ws = self._degrid_plan(g_nchan)
         if values is None:
-            values = torch.zeros((self.nt, self.nb, self.nchan, self.npol),
+            values = torch.empty((self.nt, self.nb, self.nchan, self.npol),
                                  dtype=torch.complex64, device=self.dev)
+            accumulate = False
         pm = K.on_device(np.round(np.arange(self.npol) % g_npol).astype(int), torch.int32)
         fl = None if flag is None else K.on_device(flag).to(torch.uint8).contiguous()
         dph = None if dphase is None else K.on_device(dphase, torch.float64)
-        check(lib().av_degrid_tiled_execute(K.p(dph), K.p(values), K.dcode(values), K.p(fl),
+        check(lib().av_degrid_tiled_execute(K.p(dph), K.p(values), K.dcode(values),
+                                            int(bool(accumulate)), K.p(fl),
                                             K.p(g), K.dcode(g), g_nchan, g_npol, self.nx,
                                             self.ny, K.p(self.freq), self.support, self.os,
                                             K.p(self.cgk), K.p(pm), self.nt, self.nb,

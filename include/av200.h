@@ -154,6 +154,20 @@ int av_degrid_plain(const double *uvw, const double *dphase, void *values, int v
                     const int32_t *polmap, int64_t nt, int64_t nb, int64_t nvchan,
                     int64_t nvpol, void *stream);
 
+/* Adjoint of av_degrid_plain (FP64, the degridder's exact positions and
+ * maps): grid (c128 / c64, +=) gets w_k / (sum_k w_k) * phasor * values for
+ * every unflagged sample - the gradient of the degridder with respect to the
+ * grid.  No counterpart function in the reference: it is the transpose of
+ * dgrid_numba (standard_degrid.py:388-485). */
+int av_degrid_plain_adjoint(const double *uvw, const double *dphase, const void *values,
+                            int values_dtype, const uint8_t *flag, double scale_x, double scale_y,
+                            double offset_x, double offset_y, void *grid, int grid_dtype,
+                            int64_t g_nchan, int64_t g_npol, int64_t g_n2, int64_t g_n3,
+                            const double *freq, double c, int support, int sampling,
+                            const double *convFunc, const int32_t *chanmap,
+                            const int32_t *polmap, int64_t nt, int64_t nb, int64_t nvchan,
+                            int64_t nvpol, void *stream);
+
 size_t av_degrid_tiled_workspace_size(int64_t nt, int64_t nb, int64_t nvchan, int64_t g_n2,
                                       int64_t g_n3, int64_t g_nchan, int support);
 
@@ -169,19 +183,32 @@ int av_degrid_tiled_plan(const double *uvw, const double *freq, const int32_t *c
                          int64_t nt, int64_t nb, int64_t nvchan, void *workspace,
                          size_t workspace_bytes, void *stream);
 int av_degrid_tiled_execute(const double *dphase, void *values, int values_dtype,
-                            const uint8_t *flag, const void *grid, int grid_dtype,
+                            int accumulate, const uint8_t *flag, const void *grid, int grid_dtype,
                             int64_t g_nchan, int64_t g_npol, int64_t g_n2, int64_t g_n3,
                             const double *freq, int support, int sampling,
                             const double *convFunc, const int32_t *polmap, int64_t nt,
                             int64_t nb, int64_t nvchan, int64_t nvpol, void *workspace,
                             size_t workspace_bytes, void *stream);
 int av_degrid_tiled(const double *uvw, const double *dphase, void *values, int values_dtype,
-                    const uint8_t *flag, double scale_x, double scale_y, double offset_x, double offset_y,
-                    const void *grid, int grid_dtype, int64_t g_nchan, int64_t g_npol,
-                    int64_t g_n2, int64_t g_n3, const double *freq, double c, int support,
-                    int sampling, const double *convFunc, const int32_t *chanmap,
-                    const int32_t *polmap, int64_t nt, int64_t nb, int64_t nvchan,
-                    int64_t nvpol, void *workspace, size_t workspace_bytes, void *stream);
+                    int accumulate, const uint8_t *flag, double scale_x, double scale_y,
+                    double offset_x, double offset_y, const void *grid, int grid_dtype,
+                    int64_t g_nchan, int64_t g_npol, int64_t g_n2, int64_t g_n3,
+                    const double *freq, double c, int support, int sampling,
+                    const double *convFunc, const int32_t *chanmap, const int32_t *polmap,
+                    int64_t nt, int64_t nb, int64_t nvchan, int64_t nvpol, void *workspace,
+                    size_t workspace_bytes, void *stream);
+
+/* Adjoint of the tiled degridder (zero phase), run on a plan built by
+ * av_degrid_tiled_plan in the same workspace: grid (+=) gets
+ * w_k / (sum_k w_k) * values for every unflagged sample (complex64 values,
+ * FP64 accumulation).  The transpose of dgrid_numba
+ * (standard_degrid.py:388-485); no counterpart function in the reference. */
+int av_degrid_tiled_adjoint(void *grid, int grid_dtype, const void *values, int values_dtype,
+                            const uint8_t *flag, int64_t g_nchan, int64_t g_npol, int64_t g_n2,
+                            int64_t g_n3, int support, int sampling, const double *convFunc,
+                            const int32_t *polmap, int64_t nt, int64_t nb, int64_t nvchan,
+                            int64_t nvpol, void *workspace, size_t workspace_bytes,
+                            void *stream);
 
 /* ------------------------------------------------- image formation / FFT -- */
 size_t av_fft_workspace_size(int64_t nplanes, int64_t nx, int64_t ny, int precision);
@@ -195,6 +222,15 @@ size_t av_grid_to_image_workspace_size(int64_t nplanes, int64_t nx, int64_t ny);
 int av_grid_to_image(const void *grid, int grid_dtype, const double *sum_weight,
                      void *image, int image_dtype, int64_t nplanes, int64_t nx, int64_t ny,
                      int apply_corr, void *workspace, size_t workspace_bytes, void *stream);
+
+/* fft_lm_to_uv(image / corrTerm) (fft.py:5, gcf_prolate_spheroidal.py:73-79)
+ * for nplanes real (nx, ny) planes (AV_F32 / AV_F64) into a complex grid
+ * (AV_C64 / AV_C128), FP64 transform; apply_corr = 0 skips the division.  The
+ * image -> grid step of the degridding forward model and the adjoint of
+ * av_grid_to_image without sum_weight. */
+int av_image_to_grid(const void *image, int image_dtype, void *grid, int grid_dtype,
+                     int64_t nplanes, int64_t nx, int64_t ny, int apply_corr, void *workspace,
+                     size_t workspace_bytes, void *stream);
 
 /* fft_lm_to_uv (fft.py:5) with inverse = 0 and ifft_uv_to_lm (ifft.py:5)
  * with inverse = 1, over the last two axes of nplanes (nx, ny) planes:

@@ -371,6 +371,70 @@ void orc_dgrid(const double *uvw, const double *dphase, cplx *values, const uint
 #endif
 }
 
+/* Transpose of dgrid_numba (standard_degrid.py:388-485): for every sample the
+ * degridder reads, grid[c, p, x0+ix, y0+iy] += wt * phasor * values / norm
+ * (same positions, taps, maps and flags, FP64).  Used to check the adjoint
+ * kernels of the degridding forward model. */
+void orc_dgrid_adjoint(const double *uvw, const double *dphase, const cplx *values,
+                       const uint8_t *flag, const double *scale, const double *offset,
+                       cplx *grid, int64_t g_nchan, int64_t g_npol, int64_t g_n2, int64_t g_n3,
+                       const double *freq, double c, int support, int sampling,
+                       const double *convFunc, const int64_t *chanmap, const int64_t *polmap,
+                       int64_t nt, int64_t nb, int64_t nvchan, int64_t nvpol) {
+  const int64_t nx = g_n3, ny = g_n2;
+  const int64_t supp_beg = -(support / 2), supp_end = supp_beg + support;
+  for (int64_t t = 0; t < nt; ++t)
+    for (int64_t b = 0; b < nb; ++b) {
+      const double *p_uvw = uvw + (t * nb + b) * 3;
+      for (int64_t ipol = 0; ipol < nvpol; ++ipol) {
+        int64_t apol = polmap[ipol];
+        if (!(0 <= apol && apol < g_npol)) continue;
+        for (int64_t ichan = 0; ichan < nvchan; ++ichan) {
+          int64_t achan = chanmap[ichan];
+          int64_t vidx = ((t * nb + b) * nvchan + ichan) * nvpol + ipol;
+          if (!(0 <= achan && achan < g_nchan) || (flag && flag[vidx])) continue;
+          double pos0 = scale[0] * p_uvw[0] * freq[ichan] / c + offset[0];
+          double pos1 = scale[1] * p_uvw[1] * freq[ichan] / c + offset[1];
+          int64_t x0 = (int32_t)(uint32_t)(uint64_t)trunc_i64(nearbyint(pos0));
+          int64_t y0 = (int32_t)(uint32_t)(uint64_t)trunc_i64(nearbyint(pos1));
+          int64_t off0 = (int32_t)(uint32_t)(uint64_t)trunc_i64(
+              nearbyint(((double)x0 - pos0) * (double)sampling));
+          int64_t off1 = (int32_t)(uint32_t)(uint64_t)trunc_i64(
+              nearbyint(((double)y0 - pos1) * (double)sampling));
+          if (!((x0 + supp_beg >= 0) && ((x0 + supp_end - 1) < nx) && (y0 + supp_beg >= 0) &&
+                ((y0 + supp_end - 1) < ny)))
+            continue;
+          if (x0 + supp_end - 1 >= g_n2 || y0 + supp_end - 1 >= g_n3) continue;
+          double norm = 0.0;
+          for (int64_t ix = supp_beg; ix < supp_end; ++ix) {
+            int64_t i1 = sampling * ix + off0;
+            for (int64_t iy = supp_beg; iy < supp_end; ++iy) {
+              int64_t i2 = sampling * iy + off1;
+              norm += convFunc[i1 < 0 ? -i1 : i1] * convFunc[i2 < 0 ? -i2 : i2];
+            }
+          }
+          if (norm == 0.0) continue;
+          double phase = dphase ? -2.0 * M_PI * dphase[t * nb + b] * freq[ichan] / c : 0.0;
+          double pr = cos(phase), pi = sin(phase);
+          double vr = values[vidx].re * pr - values[vidx].im * pi;
+          double vi = values[vidx].re * pi + values[vidx].im * pr;
+          cplx *plane = grid + (achan * g_npol + apol) * g_n2 * g_n3;
+          for (int64_t ix = supp_beg; ix < supp_end; ++ix) {
+            int64_t i1 = sampling * ix + off0;
+            double wtx = convFunc[i1 < 0 ? -i1 : i1];
+            for (int64_t iy = supp_beg; iy < supp_end; ++iy) {
+              int64_t i2 = sampling * iy + off1;
+              double wt = wtx * convFunc[i2 < 0 ? -i2 : i2];
+              cplx *g = &plane[(x0 + ix) * g_n3 + (y0 + iy)];
+              g->re += wt * vr / norm;
+              g->im += wt * vi / norm;
+            }
+          }
+        }
+      }
+    }
+}
+
 /* ---------------------------------------------------------------------------
  * grid_imaging_weights_jit, grid_imaging_weights.py:93-206.
  * grid (n_chan, n_gpol, n_u, n_v) real; data_weights (nt, nb, nchan, npol).

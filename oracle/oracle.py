@@ -48,6 +48,8 @@ def lib():
     L.orc_standard_grid_mt.restype = _i
     L.orc_dgrid.argtypes = [_dp, _dp, _vp, _u8p, _dp, _dp, _vp, _i64, _i64, _i64, _i64, _dp,
                             _d, _i, _i, _dp, _i64p, _i64p, _i64, _i64, _i64, _i64, _i]
+    L.orc_dgrid_adjoint.argtypes = [_dp, _dp, _vp, _u8p, _dp, _dp, _vp, _i64, _i64, _i64, _i64,
+                                    _dp, _d, _i, _i, _dp, _i64p, _i64p, _i64, _i64, _i64, _i64]
     L.orc_grid_imaging_weights.argtypes = [_dp, _i64, _dp, _dp, _dp, _i64p, _dp, _i64, _i64,
                                            _d, _d, _i64, _i64, _i64, _i64]
     L.orc_degrid_imaging_weights.argtypes = [_dp, _dp, _i64, _i64, _dp, _dp, _dp, _i64p,
@@ -234,6 +236,25 @@ def degrid(grid, uvw, freq, pixelincr, flag=None, support=7, sampling=100, nthre
     dgrid_numba(uvw, np.zeros((nt, nb)), values, flag, scale, offset, grid, freq, C_LIGHT,
                 support, sampling, cf, chanmap, polmap, nthreads=nthreads)
     return values
+
+
+def dgrid_adjoint(uvw, values, flag, scale, offset, grid_shape, freq, support, sampling,
+                  convFunc, chanmap, polmap, dphase=None, c=C_LIGHT):
+    """Transpose of dgrid_numba: a fresh complex128 grid of grid_shape."""
+    g = np.zeros(grid_shape, dtype=np.complex128)
+    nt, nb, nvchan, nvpol = values.shape
+    v = _c(values, np.complex128)
+    uvw = _c(uvw, np.float64)
+    fl = None if flag is None else _c(flag, np.uint8)
+    dph = None if dphase is None else _c(dphase, np.float64)
+    lib().orc_dgrid_adjoint(_p(uvw, _dp), None if dph is None else _p(dph, _dp), v.ctypes.data,
+                            None if fl is None else _p(fl, _u8p), _p(_c(scale, np.float64), _dp),
+                            _p(_c(offset, np.float64), _dp), g.ctypes.data, g.shape[0], g.shape[1],
+                            g.shape[2], g.shape[3], _p(_c(freq, np.float64), _dp), float(c),
+                            int(support), int(sampling), _p(_c(convFunc, np.float64), _dp),
+                            _p(_c(chanmap, np.int64), _i64p), _p(_c(polmap, np.int64), _i64p), nt,
+                            nb, nvchan, nvpol)
+    return g
 
 
 # ----------------------------------------------------------------------------
