@@ -3,6 +3,8 @@
 // calculate_imaging_weights.py:183-198, 228-261).
 #include <math_constants.h>
 
+#include <mutex>
+
 #include "common.cuh"
 
 namespace av {
@@ -226,6 +228,83 @@ int av_briggs_apply(void *out, int out_dtype, const double *density, const doubl
       delta_m, rows, nchan, npol, err_flag);
   AV_LAUNCH_CHECK();
   return AV_OK;
+}
+
+}  // extern "C"
+
+// ------------------------------------------------- allocation-free variant --
+// Some callers may not allocate device memory: a host program whose device
+// buffers all come from a pool it sized at start-up and that allows no
+// cudaMalloc/cudaFree while it processes (an allocation there synchronises
+// the device and can fail mid-run), or a plugin called by another framework
+// that owns all device memory and hands it only inputs and outputs.  For them
+// av_briggs_factors_noalloc keeps the reduction's partial sums in the static
+// array below instead of a caller workspace.
+
+namespace av {
+
+constexpr int kBriggsSlices = 64;  // partial sums per plane, as av_briggs_factors
+constexpr int kMaxDevices = 64;
+
+// The partial sums of up to AV_BRIGGS_NOALLOC_MAX_PLANES planes (512 KiB).
+// The module holds one copy on every device that loads it, until the process
+// exits.  In host code this name is a host-side stand-in: the device address
+// comes from cudaGetSymbolAddress, per device.
+static __device__ __align__(256) double
+    g_briggs_scratch[(size_t)AV_BRIGGS_NOALLOC_MAX_PLANES * kBriggsSlices];
+
+static std::mutex g_briggs_scratch_mu;
+static void *g_briggs_scratch_ptr[kMaxDevices];
+
+// Device address of the current device's copy of g_briggs_scratch, looked up
+// on the first call made with that device current and cached afterwards.
+static int briggs_scratch(void **out) {
+  int dev = 0;
+  AV_CUDA(cudaGetDevice(&dev));
+  if (dev < 0 || dev >= kMaxDevices) {
+    set_error("av_briggs_factors_noalloc: device %d beyond the %d this library tracks", dev,
+              kMaxDevices);
+    return AV_ERR_UNSUPPORTED;
+  }
+  std::lock_guard<std::mutex> lock(g_briggs_scratch_mu);
+  if (!g_briggs_scratch_ptr[dev]) {
+    void *ptr = nullptr;
+    cudaError_t e = cudaGetSymbolAddress((void **)&ptr, g_briggs_scratch);
+    if (e != cudaSuccess || !ptr) {
+      set_error("av_briggs_factors_noalloc: cudaGetSymbolAddress on device %d: %s", dev,
+                cudaGetErrorString(e));
+      return AV_ERR_CUDA;
+    }
+    g_briggs_scratch_ptr[dev] = ptr;
+  }
+  *out = g_briggs_scratch_ptr[dev];
+  return AV_OK;
+}
+
+}  // namespace av
+
+extern "C" {
+
+int av_briggs_factors_noalloc(const double *density, const double *sum_weight, double *factors,
+                              int64_t nplanes, int64_t n_u, int64_t n_v, double robust,
+                              void *stream) {
+  clear_error();
+  AV_CHECK_ARG(density && sum_weight && factors, "av_briggs_factors_noalloc: null pointer");
+  AV_CHECK_ARG(nplanes >= 0 && n_u > 0 && n_v > 0, "av_briggs_factors_noalloc: bad shape");
+  AV_CHECK_ARG(nplanes <= AV_BRIGGS_NOALLOC_MAX_PLANES,
+               "av_briggs_factors_noalloc: %lld planes exceed the static scratch's maximum of "
+               "%d planes; use av_briggs_factors with a workspace",
+               (long long)nplanes, AV_BRIGGS_NOALLOC_MAX_PLANES);
+  static_assert(sizeof(g_briggs_scratch) ==
+                    (size_t)AV_BRIGGS_NOALLOC_MAX_PLANES * kBriggsSlices * sizeof(double),
+                "scratch size");
+  void *scratch = nullptr;
+  int rc = briggs_scratch(&scratch);
+  if (rc != AV_OK) return rc;
+  // every partial k_briggs_finish reads, k_sum_sq of the same call writes
+  // first: nothing needs clearing between calls
+  return av_briggs_factors(density, sum_weight, factors, nplanes, n_u, n_v, robust, scratch,
+                           sizeof(g_briggs_scratch), stream);
 }
 
 }  // extern "C"

@@ -259,6 +259,26 @@ int av_briggs_factors(const double *density, const double *sum_weight, double *f
                       int64_t nplanes, int64_t n_u, int64_t n_v, double robust,
                       void *workspace, size_t workspace_bytes, void *stream);
 
+/* No counterpart in the reference.  av_briggs_factors for callers that may
+ * not allocate device memory: a host program that hands this library buffers
+ * from a pool it sized at start-up and allows no cudaMalloc/cudaFree on its
+ * processing path (an allocation there synchronises the device and can fail
+ * mid-run), or a plugin running inside another framework that owns all device
+ * memory and passes it only inputs and outputs.  Same arguments and result as
+ * av_briggs_factors, without the workspace: the partial sums live in a
+ * static device array of this library (AV_BRIGGS_NOALLOC_MAX_PLANES planes,
+ * 512 KiB, held on every GPU that loads the library until the process exits).
+ * nplanes above the maximum returns AV_ERR_ARG; the call makes no
+ * allocation.  The first call on a device looks up that device's copy of the
+ * array: make it before any stream capture.  All calls share the one array,
+ * so calls that overlap on the GPU (other streams, other host threads) race;
+ * serialise them.  Every partial a call reads it first writes, so the
+ * previous call's contents never leak into a result. */
+#define AV_BRIGGS_NOALLOC_MAX_PLANES 1024
+int av_briggs_factors_noalloc(const double *density, const double *sum_weight, double *factors,
+                              int64_t nplanes, int64_t n_u, int64_t n_v, double robust,
+                              void *stream);
+
 /* degrid_imaging_weights_jit, grid_imaging_weights.py:285-443, with the
  * input preparation and the tiling to n_pol of calculate_imaging_weights.py
  * (:228-261): out (nt, nb, nchan, npol) of out_dtype gets the imaging weight
