@@ -2,14 +2,15 @@
 //
 // av_grid_plain: one thread per (time, baseline, channel) sample, FP64, the
 //   reference's per-sample arithmetic and tap order, FP64 atomics.
-// av_grid_tiled: FP32 tiled gridder over a cell-sorted plan (plan.cuh).
-//   Each CTA walks a chunk of records; per tile it keeps a (T+S-1)^2 x npg
-//   complex sub-grid in shared memory.  Records are staged in batches; lanes
-//   form groups of S threads, lane g of a group owns footprint row g and
-//   keeps S x NPOL complex accumulators in registers for as long as the
-//   group's records stay in one cell (cell-sorted input makes that long),
-//   flushing to the sub-grid only on a cell change.  The tile is flushed to
-//   the global grid once.  Products use packed FP32 (fma.rn.f32x2).
+// av_grid_tiled: tiled gridder over a cell-sorted plan (plan.cuh) for FP32
+//   visibilities and weights, accumulating in FP64.  Persistent CTAs (one
+//   per SM) take chunks of records; per tile segment a CTA keeps a
+//   (T+S-1)^2 x npg FP64 complex sub-grid in shared memory.  Each warp
+//   streams a slice of the segment one sample at a time; each lane owns a
+//   footprint row x polarisation x column range and keeps its accumulators
+//   in registers while the samples stay in one cell, flushing to the
+//   sub-grid only on a cell change.  The sub-grid goes to the global grid
+//   once per segment.
 #include "plan.cuh"
 
 namespace av {
@@ -153,13 +154,13 @@ __global__ void __launch_bounds__(256) k_grid_plain(GridArgs a) {
 // FP64 leave ~4e-6.  The kernel therefore reads FP32 visibilities and
 // weights, forms tap weights from an FP64 table, and accumulates with DFMA
 // into FP64 registers and an FP64 shared-memory sub-grid.
-constexpr int GT_THREADS = 256;
-constexpr int GT_WARPS = GT_THREADS / 32;
+constexpr int GT_STAGE = 32;  // samples a warp stages per round (one per lane)
 
 struct TiledGridArgs {
   const Rec *recs;
   const uint32_t *tile_start;
   const uint32_t *n_rec;  // device: total records (offs[n_keys])
+  uint32_t *sched;        // device: [0] next chunk, [1] CTAs done (both 0 between launches)
   int64_t n_tiles, ntu, ntv;
   int64_t chunk;
   const float2 *vis;
@@ -178,34 +179,73 @@ struct TiledGridArgs {
   const uint8_t *flag;      // may be NULL
 };
 
-// Thread mapping: a group of S lanes handles one sample at a time; lane g of
-// the group owns footprint row g for every polarisation and keeps S x NPOL
-// FP64 complex accumulators.  Each group streams its own contiguous slice of
-// the tile's cell-sorted samples, so its accumulators stay in one cell for a
-// whole run (median ~70 samples on the 33M workload) and the FP64 shared
-// sub-grid sees ~1 flush per run.  Every warp stages its groups' samples
-// itself (one sample per loader lane per round, loads for the next round in
-// flight while the current one is computed): no block barrier inside a tile.
+// Thread mapping.  Each warp streams its own contiguous slice of a tile
+// segment's cell-sorted samples, one sample at a time for the whole warp, so
+// a change of cell (and the flush of the accumulators it triggers) is the
+// same for every lane of the warp.  A lane owns footprint row g,
+// polarisations [pg*PPL, pg*PPL+PPL) and footprint columns [cc*KC, cc*KC+KC)
+// and keeps PPL x KC FP64 complex accumulators in registers for a whole run
+// of samples in one cell (median ~70 on the 33M workload).  Per sample and
+// lane: 2 PPL DMUL (row tap x value) and 2 PPL KC DFMA.
+//
+// For supports up to 8 each quarter-warp is one (polarisation group, column
+// chunk) block and its lanes are the rows (lane = block * 8 + g): every
+// quarter then reads one address for the staged value and for the column
+// taps, which shared memory serves at its broadcast rate (2 wavefronts per
+// 16-byte load, against 4 when a quarter reads several addresses).  Support
+// 7 with 4 polarisations: 4 quarters x 7 rows, 7 accumulators per lane.
+//
+// The warp's lanes first stage 32 samples (one each: FP64 weighted values,
+// cell key, tap-table row offsets) into the warp's shared staging area; the
+// next round's values and the record of the round after are in flight while
+// a round is computed.
 template <int S, int NPOL>
 struct GCfg {
-  static constexpr int W = TILE + S - 1;          // sub-grid edge
-  static constexpr int RW = (S + 1) & ~1;         // taps read per row (doubles)
-  static constexpr int RWP = (RW % 4 == 0) ? RW + 2 : RW;  // row stride: spreads banks
-  static constexpr int GPW = 32 / S;              // groups per warp
-  static constexpr int R = 32 / GPW;              // samples per group per round
-  static constexpr int NG = GT_WARPS * GPW;       // groups per CTA
-  static constexpr int WD_GSTRIDE = R * NPOL + 1; // double2 per group (+1: bank offset)
+  // one CTA per SM; as many warps as the registers allow without spilling
+  static constexpr int THREADS = (S >= 9 && NPOL == 4) ? 384 : 512;
+  static constexpr int WARPS = THREADS / 32;
+  static constexpr int W = TILE + S - 1;                          // sub-grid edge
+  static constexpr bool QUARTERS = S <= 8;                         // lane = block * 8 + g
+  static constexpr int PPL = QUARTERS ? (NPOL <= 4 ? 1 : 2)
+                                      : (S * NPOL <= 32 ? 1 : (S * NPOL <= 64 ? 2 : 4));
+  static constexpr int NPGL = NPOL / PPL;                          // polarisation groups
+  static constexpr int NCC_FIT = QUARTERS ? 4 / NPGL : 32 / (S * NPGL);
+  static constexpr int NCC_CAP = NCC_FIT < 1 ? 1 : (NCC_FIT > S ? S : NCC_FIT);
+  static constexpr int KC = (S + NCC_CAP - 1) / NCC_CAP;          // columns per lane
+  static constexpr int NCC = (S + KC - 1) / KC;                    // column chunks
+  static constexpr int BLOCKS = NPGL * NCC;                        // (pol group, chunk)
+  static constexpr int LANES = QUARTERS ? 32 : S * BLOCKS;         // lanes with a role
+  static constexpr bool PAIRS = (KC % 2 == 0) || NCC == 1;         // 16-byte tap loads
+  static constexpr int KCE = PAIRS ? ((KC + 1) & ~1) : KC;         // taps addressed
+  static constexpr int RT0 = (NCC - 1) * KC + KCE;
+  static constexpr int RT = ((RT0 > S ? RT0 : S) + 1) & ~1;        // taps per table row
+  static constexpr int RWP = (RT % 4 == 0) ? RT + 2 : RT;          // row stride (banks)
   static constexpr size_t tab_bytes = 256 * RWP * sizeof(double);
   static constexpr size_t rs_bytes = 256 * sizeof(double);
-  static constexpr size_t wd_bytes = (size_t)GT_WARPS * GPW * WD_GSTRIDE * sizeof(double2);
-  static constexpr size_t mt_bytes = (size_t)GT_WARPS * GPW * (R + 1) * sizeof(int2);
-  static size_t sub_bytes(int npg) { return (size_t)npg * W * W * sizeof(double2); }
-  static size_t total(int npg) { return tab_bytes + rs_bytes + wd_bytes + mt_bytes + sub_bytes(npg); }
+  // staged values: [pol][sample] with a 33-entry stride, so the 32 lanes'
+  // stores are contiguous and the quarters' loads fall on different banks
+  static constexpr int SDS = GT_STAGE + 1;
+  static constexpr size_t std_bytes = (size_t)WARPS * NPOL * SDS * sizeof(double2);
+  // sub-grid: separate real and imaginary planes of npg x W rows of RS
+  // doubles; RS odd and PS = 1 mod 16 spread a flush's 8-byte atomics over
+  // the banks (rows and polarisations land on different bank pairs)
+  static constexpr int RS = W | 1;
+  static constexpr int PS = ((W * RS + 15) / 16) * 16 + 1;
+  static constexpr size_t stm_bytes = (size_t)WARPS * GT_STAGE * sizeof(int);
+  static constexpr size_t off_rs = tab_bytes;
+  static constexpr size_t off_std = off_rs + rs_bytes;
+  static constexpr size_t off_stm = off_std + std_bytes;
+  static constexpr size_t off_sub = off_stm + stm_bytes;
+  static size_t sub_bytes(int npg) { return (size_t)2 * npg * PS * sizeof(double); }
+  static size_t total(int npg) { return off_sub + sub_bytes(npg); }
+  static_assert(QUARTERS ? BLOCKS <= 4 : S * BLOCKS <= 32, "lane mapping");
+  static_assert(NPGL * PPL == NPOL, "polarisation split");
 };
 
 // Per-offset tap tables: tab[(o + 128) * RWP + i] = cgk[|os * (i - S/2) + o|]
-// and rs[o + 128] = sum_i of the same (so sum_k w_k = rs[ou] * rs[ov]).
-template <int S, int RW, int RWP>
+// for i < S (zero beyond) and rs[o + 128] = sum_i of the same, so the sum of
+// a sample's footprint weights is rs[ou] * rs[ov].
+template <int S, int RWP>
 __device__ void build_tap_tables64(double *tab, double *rs, const double *cgk, int cgk_len,
                                    int os) {
   for (int o = threadIdx.x; o < 256; o += blockDim.x) {
@@ -245,13 +285,16 @@ struct Pref {
   bool ok;
 };
 
+// Loads of one sample's weights and visibilities, issued from a record that
+// is already in a register (records are loaded one round earlier still, so
+// these addresses never wait on a load).
 template <int NPOL>
-__device__ __forceinline__ void prefetch(Pref<NPOL> &f, const TiledGridArgs &a, uint32_t r,
+__device__ __forceinline__ void prefetch(Pref<NPOL> &f, const TiledGridArgs &a, const Rec &rc,
                                          bool valid) {
   f.ok = valid;
   if (!valid) return;
-  f.rc = a.recs[r];
-  const int64_t vb = (int64_t)f.rc.row * a.npol;
+  f.rc = rc;
+  const int64_t vb = (int64_t)rc.row * a.npol;
   if (a.wt == nullptr) {  // unit weights (degridder adjoint)
 #pragma unroll
     for (int p = 0; p < NPOL; ++p) {
@@ -280,32 +323,73 @@ __device__ __forceinline__ void prefetch(Pref<NPOL> &f, const TiledGridArgs &a, 
   }
 }
 
+// Adds a lane's accumulators of one run (cell key: du | dv << 8) to the
+// shared sub-grid (real plane sre, imaginary plane sim) and clears them.
+// Columns past the support are padding.
+template <int S, int RS, int PS, int PPL, int KC>
+__device__ __forceinline__ void grid_flush(double2 (&acc)[PPL][KC], double *sre, double *sim,
+                                           int key, int g, int c0, const int (&ipm)[PPL],
+                                           bool owner) {
+  const int du = key & 255, dv = (key >> 8) & 255;
+  const int base = (du + g) * RS + dv + c0;
+#pragma unroll
+  for (int pp = 0; pp < PPL; ++pp) {
+#pragma unroll
+    for (int k = 0; k < KC; ++k) {
+      const double2 v = acc[pp][k];
+      if (owner && ipm[pp] >= 0 && c0 + k < S && (v.x != 0.0 || v.y != 0.0)) {
+        const int e = ipm[pp] * PS + base + k;
+        atomicAdd(sre + e, v.x);
+        atomicAdd(sim + e, v.y);
+      }
+      acc[pp][k] = make_double2(0.0, 0.0);
+    }
+  }
+}
+
+// Persistent: one CTA per SM takes chunks of records from a.sched[0] until
+// none are left; the last CTA to finish sets both counters back to zero for
+// the next launch on the same plan.
 template <int S, int NPOL>
-__global__ void __launch_bounds__(GT_THREADS, 1) k_grid_tiled(TiledGridArgs a) {
+__global__ void __launch_bounds__(GCfg<S, NPOL>::THREADS, 1) k_grid_tiled(TiledGridArgs a) {
   using C = GCfg<S, NPOL>;
-  constexpr int W = C::W, RW = C::RW, RWP = C::RWP, R = C::R, GPW = C::GPW;
+  constexpr int W = C::W, KC = C::KC, KCE = C::KCE, RWP = C::RWP, PPL = C::PPL;
   extern __shared__ __align__(16) unsigned char smem[];
   double *tab = (double *)smem;
-  double *rs = (double *)(smem + C::tab_bytes);
-  double2 *st_wd = (double2 *)(smem + C::tab_bytes + C::rs_bytes);
-  int2 *st_mt = (int2 *)(smem + C::tab_bytes + C::rs_bytes + C::wd_bytes);
-  double2 *sub = (double2 *)(smem + C::tab_bytes + C::rs_bytes + C::wd_bytes + C::mt_bytes);
+  double *rs = (double *)(smem + C::off_rs);
+  double2 *st_d = (double2 *)(smem + C::off_std);
+  int *st_m = (int *)(smem + C::off_stm);
+  double *sre = (double *)(smem + C::off_sub);
+  double *sim = sre + (size_t)a.npg * C::PS;
+  __shared__ int s_chunk;
 
   const uint32_t n_rec = *a.n_rec;
-  const uint32_t r0 = (uint32_t)(blockIdx.x * a.chunk);
-  if (r0 >= n_rec) return;
-  const uint32_t r1 = (uint32_t)min((int64_t)n_rec, (int64_t)r0 + a.chunk);
+  const int64_t n_chunks = ((int64_t)n_rec + a.chunk - 1) / a.chunk;
   const int npg = a.npg;
-  const int sub_n = npg * W * W;
+  const int sub_n = npg * W * W;  // cells of the tile's footprint area
 
-  build_tap_tables64<S, RW, RWP>(tab, rs, a.cgk, a.cgk_len, a.os);
-  for (int i = threadIdx.x; i < sub_n; i += GT_THREADS) sub[i] = make_double2(0.0, 0.0);
+  build_tap_tables64<S, RWP>(tab, rs, a.cgk, a.cgk_len, a.os);
+  for (int i = threadIdx.x; i < 2 * npg * C::PS; i += C::THREADS) sre[i] = 0.0;
 
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  const int gq = lane / S, g = lane - gq * S;   // compute role: group in warp, row
-  const bool computes = gq < GPW;
-  const int lq = lane / R, lk = lane - lq * R;  // loader role: group in warp, slot
-  const bool loads = lq < GPW;
+  // lane roles; lanes without one repeat a valid role (no divergent
+  // compute) but never flush
+  int g, blk;
+  bool owner;
+  if (C::QUARTERS) {
+    g = lane & 7;
+    blk = lane >> 3;
+    owner = g < S && blk < C::BLOCKS;
+    g = g < S ? g : S - 1;
+    blk = blk < C::BLOCKS ? blk : 0;
+  } else {
+    owner = lane < C::LANES;
+    const int li = lane % C::LANES;
+    g = li % S;
+    blk = li / S;
+  }
+  const int pg = blk / C::NCC;
+  const int c0 = (blk % C::NCC) * KC;
   // image polarisation of each visibility polarisation (-1 drops it)
   int pm[NPOL];
 #pragma unroll
@@ -313,165 +397,188 @@ __global__ void __launch_bounds__(GT_THREADS, 1) k_grid_tiled(TiledGridArgs a) {
     int v = p < a.npol ? a.pol_map[p] : -1;
     pm[p] = (v >= 0 && v < npg) ? v : -1;
   }
-  double2 *wd_mine = st_wd + (warp * GPW + (computes ? gq : 0)) * C::WD_GSTRIDE;
-  int2 *mt_mine = st_mt + (warp * GPW + (computes ? gq : 0)) * (R + 1);
-  double2 *wd_load = st_wd + (warp * GPW + (loads ? lq : 0)) * C::WD_GSTRIDE;
-  int2 *mt_load = st_mt + (warp * GPW + (loads ? lq : 0)) * (R + 1);
-
-  int t = find_tile(a.tile_start, a.n_tiles, r0);
-  uint32_t seg_lo = r0;
-  __syncthreads();
-  while (seg_lo < r1) {
-    uint32_t t_end = a.tile_start[t + 1];
-    uint32_t seg_hi = min(r1, t_end);
-    if (seg_hi <= seg_lo) {  // empty tile (uniform across the CTA)
-      ++t;
-      continue;
-    }
-    const int64_t plane = t / (a.ntu * a.ntv);
-    const int64_t trem = t - plane * a.ntu * a.ntv;
-    const int tu = (int)(trem / a.ntv), tv = (int)(trem - (int64_t)tu * a.ntv);
-    const uint32_t seg_n = seg_hi - seg_lo;
-    // contiguous slice of the segment per group
-    auto slice = [&](int q, uint32_t &lo, uint32_t &hi) {
-      lo = seg_lo + (uint32_t)(((uint64_t)seg_n * q) / C::NG);
-      hi = seg_lo + (uint32_t)(((uint64_t)seg_n * (q + 1)) / C::NG);
-    };
-    uint32_t my_lo, my_hi, ld_lo, ld_hi;
-    slice(warp * GPW + (computes ? gq : 0), my_lo, my_hi);
-    slice(warp * GPW + (loads ? lq : 0), ld_lo, ld_hi);
-    // rounds: the warp's longest slice
-    uint32_t len0, len1, wlo, whi;
-    slice(warp * GPW, wlo, len0);
-    slice(warp * GPW + GPW - 1, len1, whi);
-    const uint32_t max_len = ((uint64_t)seg_n + C::NG - 1) / C::NG;
-    const int n_rounds = (int)((max_len + R - 1) / R);
-    (void)len0; (void)len1; (void)wlo; (void)whi;
-
-    double2 acc[NPOL][S];
+  int ipm[PPL];  // this lane's polarisations
+#pragma unroll
+  for (int pp = 0; pp < PPL; ++pp) {
+    ipm[pp] = -1;
 #pragma unroll
     for (int p = 0; p < NPOL; ++p)
-#pragma unroll
-      for (int k = 0; k < S; ++k) acc[p][k] = make_double2(0.0, 0.0);
-    int cur = -1;
-    double sw[NPOL];
-#pragma unroll
-    for (int p = 0; p < NPOL; ++p) sw[p] = 0.0;
+      if (p == pg * PPL + pp) ipm[pp] = pm[p];
+  }
+  double2 *wd = st_d + warp * NPOL * C::SDS;
+  int *wm = st_m + warp * GT_STAGE;
 
-    auto flush_acc = [&](int key) {
-      const int du = key & 255, dv = (key >> 8) & 255;
-      const int base = (du + g) * W + dv;
-#pragma unroll
-      for (int p = 0; p < NPOL; ++p)
-#pragma unroll
-        for (int k = 0; k < S; ++k) {
-          double2 v = acc[p][k];
-          if (pm[p] >= 0 && (v.x != 0.0 || v.y != 0.0)) {
-            double2 *d = &sub[pm[p] * W * W + base + k];
-            atomicAdd(&d->x, v.x);
-            atomicAdd(&d->y, v.y);
-          }
-          acc[p][k] = make_double2(0.0, 0.0);
-        }
-    };
+  for (;;) {
+    __syncthreads();  // tables and sub-grid ready; previous s_chunk consumed
+    if (threadIdx.x == 0) s_chunk = (int)atomicAdd(&a.sched[0], 1u);
+    __syncthreads();
+    const int64_t ch = s_chunk;
+    if (ch >= n_chunks) break;
+    const uint32_t r0 = (uint32_t)(ch * a.chunk);
+    const uint32_t r1 = (uint32_t)min((int64_t)n_rec, (int64_t)r0 + a.chunk);
+    int t = find_tile(a.tile_start, a.n_tiles, r0);
+    uint32_t seg_lo = r0;
+    while (seg_lo < r1) {
+      const uint32_t t_end = a.tile_start[t + 1];
+      const uint32_t seg_hi = min(r1, t_end);
+      if (seg_hi <= seg_lo) {  // empty tile (uniform across the CTA)
+        ++t;
+        continue;
+      }
+      const int64_t plane = t / (a.ntu * a.ntv);
+      const int64_t trem = t - plane * a.ntu * a.ntv;
+      const int tu = (int)(trem / a.ntv), tv = (int)(trem - (int64_t)tu * a.ntv);
+      const uint32_t seg_n = seg_hi - seg_lo;
+      const uint32_t w_lo = seg_lo + (uint32_t)(((uint64_t)seg_n * warp) / C::WARPS);
+      const uint32_t w_hi = seg_lo + (uint32_t)(((uint64_t)seg_n * (warp + 1)) / C::WARPS);
+      const int n_rounds = (int)((w_hi - w_lo + GT_STAGE - 1) / GT_STAGE);
 
-    Pref<NPOL> pf;
-    prefetch<NPOL>(pf, a, ld_lo + lk, loads && ld_lo + lk < ld_hi);
-    for (int rd = 0; rd < n_rounds; ++rd) {
-      // ---- stage this round's sample (one per loader lane) for its group
-      if (loads) {
-        int2 mt = make_int2(-1, 0);
+      double2 acc[PPL][KC];
+#pragma unroll
+      for (int pp = 0; pp < PPL; ++pp)
+#pragma unroll
+        for (int k = 0; k < KC; ++k) acc[pp][k] = make_double2(0.0, 0.0);
+      int cur = -1;  // the warp's current cell
+      double sw[NPOL];
+#pragma unroll
+      for (int p = 0; p < NPOL; ++p) sw[p] = 0.0;
+
+      // software pipeline: values of round rd + 1 and the record of round
+      // rd + 2 are in flight while round rd is computed
+      Pref<NPOL> pf;
+      Rec rnext;
+      {
+        const uint32_t r = w_lo + lane;
+        Rec r0;
+        if (r < w_hi) r0 = a.recs[r];
+        prefetch<NPOL>(pf, a, r0, r < w_hi);
+      }
+      bool rnext_ok = w_lo + GT_STAGE + lane < w_hi;
+      if (rnext_ok) rnext = a.recs[w_lo + GT_STAGE + lane];
+      for (int rd = 0; rd < n_rounds; ++rd) {
+        // ---- stage this round's samples, one per lane: FP64 weighted
+        // values, the cell key and the offsets of the two tap-table rows
+        int my_key = -1;
         if (pf.ok) {
           const Rec rc = pf.rc;
           const double nrm = rs[rc.ou] * rs[rc.ov];
-          const double scl = a.inv_norm ? (nrm != 0.0 ? 1.0 / nrm : 0.0) : 1.0;
+          double scl = 1.0;
+          if (a.inv_norm) scl = nrm != 0.0 ? 1.0 / nrm : 0.0;
 #pragma unroll
           for (int p = 0; p < NPOL; ++p) {
             double2 d;
             if (a.do_psf) d = make_double2((double)pf.w[p], 0.0);
             else d = make_double2((double)pf.v[p].x * (double)pf.w[p] * scl,
                                   (double)pf.v[p].y * (double)pf.w[p] * scl);
-            // the reference skips NaN and exact-zero weighted data (standard_grid.py:378)
-            const bool ok = p < a.npol && !isnan(d.x) && !isnan(d.y) && (d.x != 0.0 || d.y != 0.0);
-            wd_load[lk * NPOL + p] = ok ? d : make_double2(0.0, 0.0);
+            // the reference skips NaN and exact-zero weighted data
+            // (standard_grid.py:378)
+            const bool ok = p < a.npol && !isnan(d.x) && !isnan(d.y) &&
+                            (d.x != 0.0 || d.y != 0.0);
+            wd[p * C::SDS + lane] = ok ? d : make_double2(0.0, 0.0);
             if (ok) sw[p] += (double)pf.w[p] * nrm;
           }
-          mt = make_int2((int)rc.du | ((int)rc.dv << 8), (int)rc.ou | ((int)rc.ov << 8));
+          my_key = (int)rc.du | ((int)rc.dv << 8);
+          wm[lane] = (int)rc.ou * RWP | (((int)rc.ov * RWP) << 16);
         }
-        mt_load[lk] = mt;
-      }
-      __syncwarp();
-      // ---- next round's loads go out before this round is computed
-      if (rd + 1 < n_rounds) {
-        const uint32_t r = ld_lo + (uint32_t)(rd + 1) * R + lk;
-        prefetch<NPOL>(pf, a, r, loads && r < ld_hi);
-      }
-      // ---- compute: the group's samples of this round, in order
-      if (computes) {
-        const uint32_t base_r = my_lo + (uint32_t)rd * R;
-        const int jn = base_r < my_hi ? (int)min((uint32_t)R, my_hi - base_r) : 0;
-        for (int j = 0; j < jn; ++j) {
-          const int2 mt = mt_mine[j];
-          if (mt.x != cur) {
-            if (cur >= 0) flush_acc(cur);
-            cur = mt.x;
+        // samples that open a new cell (the first compares with the last
+        // cell of the previous round)
+        int prev = __shfl_up_sync(0xffffffffu, my_key, 1);
+        if (lane == 0) prev = cur;
+        const unsigned starts = __ballot_sync(0xffffffffu, my_key >= 0 && my_key != prev);
+        __syncwarp();
+        // ---- next round's values go out before this round is computed
+        if (rd + 1 < n_rounds) {
+          prefetch<NPOL>(pf, a, rnext, rnext_ok);
+          const uint32_t r = w_lo + (uint32_t)(rd + 2) * GT_STAGE + lane;
+          rnext_ok = r < w_hi;
+          if (rnext_ok) rnext = a.recs[r];
+        }
+        // ---- compute the round's samples in runs of one cell
+        const int jn = (int)min((uint32_t)GT_STAGE, w_hi - (w_lo + (uint32_t)rd * GT_STAGE));
+        int j = 0;
+        while (j < jn) {
+          if ((starts >> j) & 1u) {
+            if (cur >= 0) grid_flush<S, C::RS, C::PS, PPL, KC>(acc, sre, sim, cur, g, c0, ipm, owner);
+            cur = __shfl_sync(0xffffffffu, my_key, j);
           }
-          const double cu = tab[(mt.y & 255) * RWP + g];
-          const double *cvp = &tab[((mt.y >> 8) & 255) * RWP];
-          double cv[RW];
+          const unsigned later = j < 31 ? (starts & (0xfffffffeu << j)) : 0u;
+          const int j1 = later ? min(jn, __ffs(later) - 1) : jn;
+          for (; j < j1; ++j) {
+            const int ro = wm[j];
+            const double cu = tab[(ro & 0xffff) + g];
+            const double *cvp = tab + (ro >> 16) + c0;
+            double cv[KCE];
+            if (C::PAIRS) {
 #pragma unroll
-          for (int k = 0; k < RW; k += 2) {
-            const double2 c2 = *(const double2 *)(cvp + k);
-            cv[k] = c2.x;
-            cv[k + 1] = c2.y;
-          }
+              for (int k = 0; k + 1 < KC; k += 2) {
+                const double2 c2 = *(const double2 *)(cvp + k);
+                cv[k] = c2.x;
+                cv[k + 1] = c2.y;
+              }
+              if (KC % 2) cv[KC - 1] = cvp[KC - 1];
+            } else {
 #pragma unroll
-          for (int p = 0; p < NPOL; ++p) {
-            const double2 d = wd_mine[j * NPOL + p];
-            const double tr = cu * d.x, ti = cu * d.y;
+              for (int k = 0; k < KC; ++k) cv[k] = cvp[k];
+            }
 #pragma unroll
-            for (int k = 0; k < S; ++k) {
-              acc[p][k].x = fma(cv[k], tr, acc[p][k].x);
-              acc[p][k].y = fma(cv[k], ti, acc[p][k].y);
+            for (int pp = 0; pp < PPL; ++pp) {
+              const double2 d = wd[(pg * PPL + pp) * C::SDS + j];
+              const double tr = cu * d.x, ti = cu * d.y;
+#pragma unroll
+              for (int k = 0; k < KC; ++k) {
+                acc[pp][k].x = fma(cv[k], tr, acc[pp][k].x);
+                acc[pp][k].y = fma(cv[k], ti, acc[pp][k].y);
+              }
             }
           }
         }
+        __syncwarp();
       }
-      __syncwarp();
-    }
-    if (computes && cur >= 0) flush_acc(cur);
-    // ---- sum_weight: warp reduction, one atomic per warp and polarisation
+      if (cur >= 0) grid_flush<S, C::RS, C::PS, PPL, KC>(acc, sre, sim, cur, g, c0, ipm, owner);
+      // ---- sum_weight: warp reduction, one atomic per warp and polarisation
 #pragma unroll
-    for (int p = 0; p < NPOL; ++p) {
-      double v = sw[p];
+      for (int p = 0; p < NPOL; ++p) {
+        double v = sw[p];
 #pragma unroll
-      for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
-      if (lane == 0 && a.sumw && pm[p] >= 0 && v != 0.0)
-        atomicAdd(&a.sumw[plane * npg + pm[p]], v);
-    }
-    __syncthreads();
-    // ---- flush the tile to the global grid and clear it
-    for (int i = threadIdx.x; i < sub_n; i += GT_THREADS) {
-      double2 v = sub[i];
-      if (v.x != 0.0 || v.y != 0.0) {
-        int gp = i / (W * W);
-        int cell = i - gp * W * W;
-        int iu = cell / W, iv = cell - iu * W;
-        int64_t gu = (int64_t)tu * TILE + iu, gv = (int64_t)tv * TILE + iv;
-        int64_t gi = ((plane * npg + gp) * a.n_u + gu) * a.n_v + gv;
-        if (a.grid_c128) {
-          double2 *gd = (double2 *)a.grid + gi;
-          atomicAdd(&gd->x, v.x);
-          atomicAdd(&gd->y, v.y);
-        } else {
-          atomicAdd((float2 *)a.grid + gi, make_float2((float)v.x, (float)v.y));
+        for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+        if (lane == 0 && a.sumw && pm[p] >= 0 && v != 0.0)
+          atomicAdd(&a.sumw[plane * npg + pm[p]], v);
+      }
+      __syncthreads();
+      // ---- flush the tile to the global grid and clear it
+      for (int i = threadIdx.x; i < sub_n; i += C::THREADS) {
+        const int gp = i / (W * W);
+        const int cell = i - gp * W * W;
+        const int iu = cell / W, iv = cell - iu * W;
+        const int e = gp * C::PS + iu * C::RS + iv;
+        const double2 v = make_double2(sre[e], sim[e]);
+        if (v.x != 0.0 || v.y != 0.0) {
+          int64_t gu = (int64_t)tu * TILE + iu, gv = (int64_t)tv * TILE + iv;
+          int64_t gi = ((plane * npg + gp) * a.n_u + gu) * a.n_v + gv;
+          if (a.grid_c128) {
+            double2 *gd = (double2 *)a.grid + gi;
+            atomicAdd(&gd->x, v.x);
+            atomicAdd(&gd->y, v.y);
+          } else {
+            atomicAdd((float2 *)a.grid + gi, make_float2((float)v.x, (float)v.y));
+          }
+          sre[e] = 0.0;
+          sim[e] = 0.0;
         }
-        sub[i] = make_double2(0.0, 0.0);
       }
+      __syncthreads();
+      seg_lo = seg_hi;
+      if (seg_hi == t_end) ++t;
     }
-    __syncthreads();
-    seg_lo = seg_hi;
-    if (seg_hi == t_end) ++t;
+  }
+  // every CTA has taken its last chunk: the last one to get here re-arms
+  if (threadIdx.x == 0) {
+    __threadfence();
+    if (atomicAdd(&a.sched[1], 1u) == gridDim.x - 1) {
+      a.sched[0] = 0u;
+      a.sched[1] = 0u;
+      __threadfence();
+    }
   }
 }
 
@@ -487,7 +594,7 @@ static int launch_grid_tiled(const TiledGridArgs &a, int64_t nblocks, cudaStream
                                  cudaFuncAttributeMaxDynamicSharedMemorySize, (int)C::total(4)));
     configured[dev] = true;
   }
-  k_grid_tiled<S, NPOL><<<(unsigned)nblocks, GT_THREADS, smem, st>>>(a);
+  k_grid_tiled<S, NPOL><<<(unsigned)nblocks, C::THREADS, smem, st>>>(a);
   AV_LAUNCH_CHECK();
   return AV_OK;
 }
@@ -497,6 +604,19 @@ static int dispatch_npol(const TiledGridArgs &a, int npol, int64_t nb, cudaStrea
   if (npol == 1) return launch_grid_tiled<S, 1>(a, nb, st);
   if (npol == 2) return launch_grid_tiled<S, 2>(a, nb, st);
   return launch_grid_tiled<S, 4>(a, nb, st);
+}
+
+// Chunks of records the persistent CTAs take one at a time: about 16 per SM,
+// so the last chunks even out the CTAs' finishing times, and at least 2048
+// records, so a chunk's tile flushes stay small against its samples.
+static int64_t grid_chunking(int64_t rows, int64_t &nblocks) {
+  const int sms = sm_count();
+  int64_t chunk = (rows + (int64_t)sms * 16 - 1) / ((int64_t)sms * 16);
+  if (chunk < 2048) chunk = 2048;
+  const int64_t n_chunks = (rows + chunk - 1) / chunk;
+  nblocks = n_chunks < sms ? n_chunks : sms;
+  if (nblocks < 1) nblocks = 1;
+  return chunk;
 }
 
 static int dispatch_support(const TiledGridArgs &a, int support, int npol, int64_t nb,
@@ -637,10 +757,9 @@ int av_grid_tiled_execute(void *grid, int grid_dtype, double *sum_weight, int do
   a.n_tiles = g.n_tiles();
   a.ntu = g.ntu;
   a.ntv = g.ntv;
-  int sms = sm_count();
-  int64_t chunk = (rows + (int64_t)sms * 4 - 1) / ((int64_t)sms * 4);
-  if (chunk < 2048) chunk = 2048;
-  a.chunk = chunk;
+  int64_t nblocks = 0;
+  a.chunk = grid_chunking(rows, nblocks);
+  a.sched = p.counters;
   a.vis = (const float2 *)vis;
   a.wt = (const float *)weight;
   a.do_psf = do_psf;
@@ -657,7 +776,6 @@ int av_grid_tiled_execute(void *grid, int grid_dtype, double *sum_weight, int do
   a.n_v = n_v;
   a.inv_norm = 0;
   a.flag = nullptr;
-  int64_t nblocks = (rows + chunk - 1) / chunk;
   return dispatch_support(a, support, npol_t, nblocks, as_stream(stream));
 }
 
@@ -702,10 +820,9 @@ int av_degrid_tiled_adjoint(void *grid, int grid_dtype, const void *values, int 
   a.n_tiles = g.n_tiles();
   a.ntu = g.ntu;
   a.ntv = g.ntv;
-  int sms = sm_count();
-  int64_t chunk = (rows + (int64_t)sms * 4 - 1) / ((int64_t)sms * 4);
-  if (chunk < 2048) chunk = 2048;
-  a.chunk = chunk;
+  int64_t nblocks = 0;
+  a.chunk = grid_chunking(rows, nblocks);
+  a.sched = p.counters;
   a.vis = (const float2 *)values;
   a.wt = nullptr;
   a.do_psf = 0;
@@ -723,7 +840,7 @@ int av_degrid_tiled_adjoint(void *grid, int grid_dtype, const void *values, int 
   a.inv_norm = 1;
   a.flag = flag;
   int npol_t = nvpol <= 1 ? 1 : (nvpol <= 2 ? 2 : 4);
-  return dispatch_support(a, support, npol_t, (rows + chunk - 1) / chunk, as_stream(stream));
+  return dispatch_support(a, support, npol_t, nblocks, as_stream(stream));
 }
 
 int av_grid_tiled(void *grid, int grid_dtype, double *sum_weight, int do_psf,

@@ -212,9 +212,12 @@ static int scan_counts(uint32_t *counts_then_cursor, uint32_t *offs, int64_t n,
   return AV_OK;
 }
 
+// Tile starts, and the plan's scheduling counters set to zero (the tiled
+// kernels take chunks from them and leave them at zero when they finish).
 __global__ void k_tile_starts(const uint32_t *offs, int64_t n_tiles, int64_t kpt,
-                              uint32_t *tile_start) {
+                              uint32_t *tile_start, uint32_t *counters) {
   int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (t < 16) counters[t] = 0u;
   if (t > n_tiles) return;
   tile_start[t] = offs[t * kpt];
 }
@@ -261,7 +264,7 @@ int plan_build(const PlanGeom &g, Plan &p, const double *uvw, const double *freq
   }
   int64_t nt = g.n_tiles() + 1;
   k_tile_starts<<<(unsigned)((nt + 255) / 256), 256, 0, st>>>(p.offs, g.n_tiles(), g.kpt,
-                                                              p.tile_start);
+                                                              p.tile_start, p.counters);
   AV_LAUNCH_CHECK();
   return AV_OK;
 }
