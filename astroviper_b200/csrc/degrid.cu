@@ -274,7 +274,10 @@ __global__ void __launch_bounds__(DT_THREADS) k_degrid_tiled(TiledDegridArgs a) 
   const uint32_t r1 = (uint32_t)min((int64_t)n_all, (int64_t)r0 + a.chunk);
   // store mode: skipped samples (after the usable records) get zeros
   if (!a.accumulate && r1 > n_rec) {
-    for (uint32_t r = max(r0, n_rec) + threadIdx.x; r < r1; r += DT_THREADS) {
+    const uint32_t z0 = max(r0, n_rec);
+    for (uint32_t rb = z0; rb < r1; rb += DT_THREADS) {
+      const uint32_t r = rb + threadIdx.x;
+      if (r >= r1) continue;
       const int64_t row = a.recs[r].row;
       for (int p = 0; p < d.nvpol; ++p) put_value(d, 0, row * d.nvpol + p, 0.0, 0.0);
     }
@@ -304,7 +307,9 @@ __global__ void __launch_bounds__(DT_THREADS) k_degrid_tiled(TiledDegridArgs a) 
     const int tu = (int)(trem / a.ntv), tv = (int)(trem - (int64_t)tu * a.ntv);
     __syncthreads();  // previous segment's readers are done with sub
     // stage the sub-grid, polarisations interleaved per cell (zero outside)
-    for (int i = threadIdx.x; i < W * W * NPG; i += DT_THREADS) {
+    for (int i0 = 0; i0 < W * W * NPG; i0 += DT_THREADS) {
+      const int i = i0 + threadIdx.x;
+      if (i >= W * W * NPG) continue;
       int cell = i / NPG, gp = i - cell * NPG;
       int iu = cell / W, iv = cell - iu * W;
       int64_t gu = (int64_t)tu * TILE + iu, gv = (int64_t)tv * TILE + iv;
@@ -321,12 +326,14 @@ __global__ void __launch_bounds__(DT_THREADS) k_degrid_tiled(TiledDegridArgs a) 
       sub[i] = v;
     }
     __syncthreads();
-    uint32_t r = seg_lo + threadIdx.x;
     Rec nxt;
-    if (r < seg_hi) nxt = a.recs[r];
-    for (; r < seg_hi; r += DT_THREADS) {
+    if (seg_lo + threadIdx.x < seg_hi) nxt = a.recs[seg_lo + threadIdx.x];
+    // one trip count per block, so every warp reaches the next barrier converged
+    for (uint32_t rb = seg_lo; rb < seg_hi; rb += DT_THREADS) {
+      const uint32_t r = rb + threadIdx.x;
       const Rec rc = nxt;
       if (r + DT_THREADS < seg_hi) nxt = a.recs[r + DT_THREADS];  // in flight meanwhile
+      if (r >= seg_hi) continue;
       float cu[RW], cv[RW];
 #pragma unroll
       for (int k = 0; k < RW; k += 4) {

@@ -369,7 +369,13 @@ __global__ void __launch_bounds__(GCfg<S, NPOL>::THREADS, 1) k_grid_tiled(TiledG
   const int sub_n = npg * W * W;  // cells of the tile's footprint area
 
   build_tap_tables64<S, RWP>(tab, rs, a.cgk, a.cgk_len, a.os);
-  for (int i = threadIdx.x; i < 2 * npg * C::PS; i += C::THREADS) sre[i] = 0.0;
+  // strided loops that precede a block barrier keep one trip count for the
+  // whole block (bounds test inside), so every warp reaches the barrier
+  // converged
+  for (int i0 = 0; i0 < 2 * npg * C::PS; i0 += C::THREADS) {
+    const int i = i0 + threadIdx.x;
+    if (i < 2 * npg * C::PS) sre[i] = 0.0;
+  }
 
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   // lane roles; lanes without one repeat a valid role (no divergent
@@ -546,7 +552,9 @@ __global__ void __launch_bounds__(GCfg<S, NPOL>::THREADS, 1) k_grid_tiled(TiledG
       }
       __syncthreads();
       // ---- flush the tile to the global grid and clear it
-      for (int i = threadIdx.x; i < sub_n; i += C::THREADS) {
+      for (int i0 = 0; i0 < sub_n; i0 += C::THREADS) {
+        const int i = i0 + threadIdx.x;
+        if (i >= sub_n) continue;
         const int gp = i / (W * W);
         const int cell = i - gp * W * W;
         const int iu = cell / W, iv = cell - iu * W;

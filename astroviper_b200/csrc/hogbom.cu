@@ -124,8 +124,11 @@ __global__ void __launch_bounds__(HOG_THREADS, 1) k_hogbom(HogArgs<T> a) {
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
 
   if (a.resident) {
-    for (int i = threadIdx.x; i < (y_hi - y_lo) * nx; i += HOG_THREADS)
-      band[i] = a.resid[(size_t)y_lo * nx + i];
+    // one trip count per block: every warp reaches the next barrier converged
+    for (int i0 = 0; i0 < (y_hi - y_lo) * nx; i0 += HOG_THREADS) {
+      const int i = i0 + threadIdx.x;
+      if (i < (y_hi - y_lo) * nx) band[i] = a.resid[(size_t)y_lo * nx + i];
+    }
   }
   // current peak
   int px, py, it = a.iter_begin;
@@ -311,8 +314,10 @@ __global__ void __launch_bounds__(HOG_THREADS, 1) k_hogbom(HogArgs<T> a) {
   // write the band back and publish the state
   __syncthreads();
   if (a.resident) {
-    for (int i = threadIdx.x; i < (y_hi - y_lo) * nx; i += HOG_THREADS)
-      a.resid[(size_t)y_lo * nx + i] = band[i];
+    for (int i0 = 0; i0 < (y_hi - y_lo) * nx; i0 += HOG_THREADS) {
+      const int i = i0 + threadIdx.x;
+      if (i < (y_hi - y_lo) * nx) a.resid[(size_t)y_lo * nx + i] = band[i];
+    }
   }
   if (b == 0 && threadIdx.x == 0) {
     a.state->iter = it;

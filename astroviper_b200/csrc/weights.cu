@@ -92,9 +92,12 @@ __global__ void __launch_bounds__(256) k_sum_sq(const double *G, int64_t plane_n
   int64_t lo = plane_n * s / slices, hi = plane_n * (s + 1) / slices;
   const double *g = G + p * plane_n;
   double acc = 0.0;
-  for (int64_t i = lo + threadIdx.x; i < hi; i += blockDim.x) {
-    double v = g[i];
-    acc += v * v;
+  for (int64_t i0 = lo; i0 < hi; i0 += blockDim.x) {  // one trip count per block
+    const int64_t i = i0 + threadIdx.x;
+    if (i < hi) {
+      double v = g[i];
+      acc += v * v;
+    }
   }
   __shared__ double sh[8];
   for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
