@@ -13,6 +13,7 @@ LIB_PATH = os.path.join(HERE, "libav200.so")
 AV_OK, AV_ERR_ARG, AV_ERR_CUDA, AV_ERR_TIMEOUT, AV_ERR_NAN, AV_ERR_UNSUPPORTED, AV_ERR_WORKSPACE = \
     range(7)
 AV_F32, AV_F64, AV_C64, AV_C128 = range(4)
+AV_TUNE_GRID_CHUNKS_PER_SM, AV_TUNE_DEGRID_CHUNKS_PER_SM = range(2)
 
 _vp = ctypes.c_void_p
 _i = ctypes.c_int
@@ -26,6 +27,8 @@ SIGNATURES = {
     "av_last_error": (ctypes.c_char_p, []),
     "av_device_sm_count": (_i, []),
     "av_launch_count": (ctypes.c_ulonglong, []),
+    "av_tune_set": (_i, [_i, _i64]),
+    "av_tune_get": (_i64, [_i]),
     "av_pswf": (_i, [_vp, _i64, _vp, _vp, _vp]),
     "av_pswf_table": (_i, [_vp, _i, _i, _vp]),
     "av_corr_term": (_i, [_vp, _i64, _i64, _vp]),

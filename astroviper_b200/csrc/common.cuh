@@ -130,4 +130,7 @@ inline size_t dtype_size(int dt) {
 // Number of SMs of the current device (cached per device).
 int sm_count();
 
+// Launch tuning knobs (av_tune_set); read at launch time.
+int64_t tune_value(int knob);
+
 }  // namespace av

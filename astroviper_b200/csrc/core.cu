@@ -101,6 +101,14 @@ __global__ void k_pswf_kernel4d(double *out, int os, int support, int n_os) {
   out[k] = __dmul_rn(kx, ky);
 }
 
+// ------------------------------------------------------------ tuning ---
+constexpr int kTuneKnobs = 2;
+static std::atomic<int64_t> g_tune[kTuneKnobs] = {{16}, {8}};
+
+int64_t tune_value(int knob) {
+  return (knob >= 0 && knob < kTuneKnobs) ? g_tune[knob].load() : 0;
+}
+
 }  // namespace av
 
 using namespace av;
@@ -114,6 +122,20 @@ const char *av_last_error(void) { return g_err; }
 int av_device_sm_count(void) { return sm_count(); }
 
 unsigned long long av_launch_count(void) { return g_launches.load(); }
+
+int av_tune_set(int knob, int64_t value) {
+  clear_error();
+  AV_CHECK_ARG(knob >= 0 && knob < kTuneKnobs, "av_tune_set: unknown knob %d", knob);
+  AV_CHECK_ARG(value >= 1 && value <= 1024, "av_tune_set: value %lld outside [1, 1024]",
+               (long long)value);
+  g_tune[knob].store(value);
+  return AV_OK;
+}
+
+int64_t av_tune_get(int knob) {
+  if (knob < 0 || knob >= kTuneKnobs) return -1;
+  return g_tune[knob].load();
+}
 
 int av_pswf(const double *u_in, int64_t n, double *grdsf, double *kern, void *stream) {
   clear_error();

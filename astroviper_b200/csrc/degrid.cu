@@ -629,7 +629,8 @@ int av_degrid_tiled_execute(const double *dphase, void *values, int values_dtype
   a.ntu = g.ntu;
   a.ntv = g.ntv;
   int sms = sm_count();
-  int64_t chunk = (rows + (int64_t)sms * 8 - 1) / ((int64_t)sms * 8);
+  const int64_t per_sm = tune_value(AV_TUNE_DEGRID_CHUNKS_PER_SM);
+  int64_t chunk = (rows + (int64_t)sms * per_sm - 1) / ((int64_t)sms * per_sm);
   if (chunk < 1024) chunk = 1024;
   a.chunk = chunk;
   a.d = d;

@@ -614,12 +614,14 @@ static int dispatch_npol(const TiledGridArgs &a, int npol, int64_t nb, cudaStrea
   return launch_grid_tiled<S, 4>(a, nb, st);
 }
 
-// Chunks of records the persistent CTAs take one at a time: about 16 per SM,
-// so the last chunks even out the CTAs' finishing times, and at least 2048
-// records, so a chunk's tile flushes stay small against its samples.
+// Chunks of records the persistent CTAs take one at a time: about
+// AV_TUNE_GRID_CHUNKS_PER_SM (16) per SM, so the last chunks even out the
+// CTAs' finishing times, and at least 2048 records, so a chunk's tile
+// flushes stay small against its samples.
 static int64_t grid_chunking(int64_t rows, int64_t &nblocks) {
   const int sms = sm_count();
-  int64_t chunk = (rows + (int64_t)sms * 16 - 1) / ((int64_t)sms * 16);
+  const int64_t per_sm = tune_value(AV_TUNE_GRID_CHUNKS_PER_SM);
+  int64_t chunk = (rows + (int64_t)sms * per_sm - 1) / ((int64_t)sms * per_sm);
   if (chunk < 2048) chunk = 2048;
   const int64_t n_chunks = (rows + chunk - 1) / chunk;
   nblocks = n_chunks < sms ? n_chunks : sms;

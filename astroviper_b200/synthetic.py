@@ -151,6 +151,39 @@ def workload_large(seed=20260102, n_time=256, n_chan=64, n_pol=4, device=None):
                 sources=(flux, dx, dy))
 
 
+def workload_batched(seed=20260105, n_time=496, n_chan=128, n_pol=2, image=1024,
+                     flag_lo=0.0, flag_hi=0.6, device=None):
+    """Batched uneven gridding: the same array at ``n_time`` steps x
+    ``n_chan`` channels (1.0-1.5 GHz) x ``n_pol`` polarisations, complex64,
+    cube mode (every channel its own image plane, every polarisation its own
+    grid: n_chan x n_pol independent ``image``^2 grids of 2 arcsec cells).
+    Each (channel, polarisation) grid has its own flag fraction, uniform in
+    [flag_lo, flag_hi); flags are i.i.d. per sample and enter as zero
+    weights, so per-grid sample counts are uneven.  With ``device`` the
+    visibilities and weights are made on that torch device."""
+    uvw, rng = array_uvw(64, n_time, seed=seed)
+    freq = np.linspace(1.0e9, 1.5e9, n_chan)
+    cell = 2.0 * ARCSEC
+    pixelincr = np.array([-cell, cell])
+    flux, dx, dy = random_sources(rng, 5, 0.1, 1.0, 100.0)
+    l, m = source_lm(dx, dy, pixelincr)
+    vis = point_source_vis(uvw, freq, n_pol, flux, l, m, 0.01, rng, dtype=np.complex64,
+                           device=device)
+    frac = rng.uniform(flag_lo, flag_hi, size=(n_chan, n_pol))
+    shape = (len(uvw), uvw.shape[1], n_chan, n_pol)
+    if device is None:
+        weight = (rng.uniform(size=shape) >= frac[None, None]).astype(np.float32)
+    else:
+        import torch
+        g = torch.Generator(device=device)
+        g.manual_seed(int(rng.integers(0, 2**62)))
+        u = torch.rand(shape, generator=g, dtype=torch.float32, device=device)
+        weight = (u >= torch.as_tensor(frac, dtype=torch.float32, device=device)).to(torch.float32)
+    return dict(uvw=uvw, freq=freq, vis=vis, weight=weight, flag_fraction=frac,
+                pixelincr=pixelincr, image_size=np.array([image, image]), support=7,
+                oversampling=100)
+
+
 def sampling_psf(uvw, freq, image_size, pixelincr):
     """A PSF from the uv sampling of ``uvw`` x ``freq``: nearest-cell counts of
     the samples and their conjugates, inverse FFT, peak-normalised to 1

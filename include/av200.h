@@ -51,6 +51,19 @@ int av_device_sm_count(void);
 /* Kernels launched by this library since it was loaded (all threads). */
 unsigned long long av_launch_count(void);
 
+/* Launch tuning (no counterpart in the reference, which has no GPU path):
+ * process-wide knobs read when a kernel is launched, set by the autotuner
+ * (astroviper_b200.autotune) or by hand.
+ *   AV_TUNE_GRID_CHUNKS_PER_SM   record chunks per SM handed out by the
+ *                                persistent tiled gridder (default 16)
+ *   AV_TUNE_DEGRID_CHUNKS_PER_SM record chunks per SM of the tiled
+ *                                degridder (default 8)
+ * av_tune_set returns AV_ERR_ARG for an unknown knob or a value outside
+ * [1, 1024]; av_tune_get returns -1 for an unknown knob. */
+enum av_tune { AV_TUNE_GRID_CHUNKS_PER_SM = 0, AV_TUNE_DEGRID_CHUNKS_PER_SM = 1 };
+int av_tune_set(int knob, int64_t value);
+int64_t av_tune_get(int knob);
+
 /* ---------------------------------------------------------------- PSWF -- */
 /* prolate_spheroidal_function, gcf_prolate_spheroidal.py:102-158:
  * grdsf[i], kern[i] = (grdsf(u), (1-u^2) grdsf(u)) for u = u_in[i] (FP64).
@@ -113,7 +126,11 @@ size_t av_grid_tiled_workspace_size(int64_t nt, int64_t nb, int64_t nchan, int64
  * uvw, freq, chan_map and the geometry) into the workspace; _execute grids
  * vis / weights with that plan.  A plan is reusable for any number of
  * executes with the same geometry (e.g. every major cycle), as long as the
- * workspace is left untouched in between. */
+ * workspace is left untouched in between.  The execute's persistent kernel
+ * takes its work chunks from counters in the workspace, so executes on one
+ * plan must not run concurrently (stream order is enough); neither call
+ * synchronises, allocates or touches the host, so both can be captured in a
+ * CUDA graph once the first execute on the device has run outside capture. */
 int av_grid_tiled_plan(const double *uvw, const double *freq, const int32_t *chan_map,
                        int64_t n_u, int64_t n_v, double delta_l, double delta_m, int support,
                        int oversampling, int64_t nt, int64_t nb, int64_t nchan,

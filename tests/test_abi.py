@@ -15,7 +15,7 @@ def declared():
     src = open(HEADER).read()
     src = re.sub(r"/\*.*?\*/", "", src, flags=re.S)
     out = {}
-    for m in re.finditer(r"\b(?:int|size_t|const char \*|unsigned long long)\s*\*?\s*(av_\w+)"
+    for m in re.finditer(r"\b(?:int|int64_t|size_t|const char \*|unsigned long long)\s*\*?\s*(av_\w+)"
                          r"\s*\(([^)]*)\)\s*;", src):
         args = [a for a in m.group(2).split(",") if a.strip() and a.strip() != "void"]
         out[m.group(1)] = len(args)
