@@ -184,6 +184,34 @@ def workload_batched(seed=20260105, n_time=496, n_chan=128, n_pol=2, image=1024,
                 oversampling=100)
 
 
+def workload_forward(seed=20260104, n_ant=128, n_time=128, n_chan=4, image=1024, n_blob=200,
+                     device=None):
+    """Differentiable imaging forward model: ``n_ant`` antennas in the 2 km
+    disk, ``n_time`` steps x ``n_chan`` channels (1.0-1.5 GHz) x 1
+    polarisation (4.16M visibilities at the defaults), an ``image``^2 truth of
+    ``n_blob`` Gaussian blobs (sigma 1-5 px, peak log-uniform 0.01-1,
+    centres in the inner 80 % of the field), 1 arcsec cells.  Returns the
+    truth as a float32 array (1, 1, image, image)."""
+    uvw, rng = array_uvw(n_ant, n_time, seed=seed)
+    freq = np.linspace(1.0e9, 1.5e9, n_chan)
+    cell = 1.0 * ARCSEC
+    truth = np.zeros((image, image), dtype=np.float64)
+    yy, xx = np.mgrid[0:image, 0:image]
+    lo, hi = 0.1 * image, 0.9 * image
+    for _ in range(n_blob):
+        cx, cy = rng.uniform(lo, hi, 2)
+        sig = rng.uniform(1.0, 5.0)
+        amp = 10.0 ** rng.uniform(-2.0, 0.0)
+        r = int(np.ceil(5 * sig))
+        x0, x1 = max(0, int(cx) - r), min(image, int(cx) + r + 1)
+        y0, y1 = max(0, int(cy) - r), min(image, int(cy) + r + 1)
+        truth[y0:y1, x0:x1] += amp * np.exp(-((xx[y0:y1, x0:x1] - cx) ** 2 +
+                                              (yy[y0:y1, x0:x1] - cy) ** 2) / (2 * sig * sig))
+    return dict(uvw=uvw, freq=freq, cell=np.array([-cell, cell]),
+                truth=truth.astype(np.float32)[None, None], noise_sigma=0.01,
+                image_size=np.array([image, image]), seed_rng=rng)
+
+
 def sampling_psf(uvw, freq, image_size, pixelincr):
     """A PSF from the uv sampling of ``uvw`` x ``freq``: nearest-cell counts of
     the samples and their conjugates, inverse FFT, peak-normalised to 1

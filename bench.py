@@ -48,6 +48,7 @@ def parse():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-batched", action="store_true")
+    ap.add_argument("--no-forward", action="store_true")
     ap.add_argument("--clean-iters", type=int, default=20000)
     return ap.parse_args()
 
@@ -122,6 +123,17 @@ class ClockSampler:
 # visibilities.
 NCU_VIS = 64 * 2016 * 64
 DRAM_BYTES_PER_VIS = {"k_grid_tiled": 481.64e6 / NCU_VIS, "k_degrid_tiled": 358.62e6 / NCU_VIS}
+
+
+def max_over_ranks(ms, world, device=None):
+    """The slowest rank's time (every rank calls this; one rank: unchanged)."""
+    if world <= 1:
+        return float(ms)
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([float(ms)], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
 
 
 def rel(a, b):
@@ -306,11 +318,7 @@ def main():
     if world > 1:
         dist.barrier()
     clk = clocks.stop()
-    ms = e0.elapsed_time(e1) / args.steps
-    t = torch.tensor([ms], dtype=torch.float64, device=dev)
-    if world > 1:
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    ms = float(t.item())
+    ms = max_over_ranks(e0.elapsed_time(e1) / args.steps, world, dev)
     value = n_vis * world / (ms / 1e3) / 1e6
 
     # ---------------------------------------------------------------- accuracy
@@ -349,6 +357,11 @@ def main():
     clean = None
     if not (args.quick or args.no_clean) and rank == 0:
         clean = bench_clean(args, dev)
+
+    # ------------------------------------------------------- forward model
+    forward = None
+    if not (args.quick or args.no_forward) and rank == 0:
+        forward = bench_forward(args, dev)
 
     # ------------------------------------------------------------- batched
     batched = None
@@ -410,6 +423,7 @@ def main():
         "e2e": e2e,
         "clean": clean,
         "batched_uneven": batched,
+        "forward_model": forward,
     }
     if rank == 0:
         print(json.dumps(line), flush=True)
@@ -495,6 +509,54 @@ def bench_batched(args, dev):
     return out
 
 
+def bench_forward(args, dev):
+    """Differentiable forward model: 1024^2 FP32 image -> grid correction ->
+    FFT -> degrid to 4.16M visibilities (128 antennas, 128 steps, 4 channels,
+    1 pol; truth 200 Gaussian blobs plus N(0, 0.01) noise), chi-squared
+    steepest descent for 200 steps with the hand-written adjoint as the
+    backward."""
+    import torch
+    from astroviper_b200 import synthetic as S
+    from astroviper_b200.forward_model import ForwardModel, chi2_solve
+    F = S.workload_forward()
+    n = int(F["image_size"][0])
+    m = ForwardModel(F["uvw"], F["freq"], (n, n), F["cell"], npol=1, precision="fp32")
+    truth = torch.as_tensor(F["truth"], device=dev)
+    v_obs = m.forward_op(truth)
+    g = torch.Generator(device=dev)
+    g.manual_seed(4)
+    noise = torch.complex(torch.randn(v_obs.shape, generator=g, device=dev),
+                          torch.randn(v_obs.shape, generator=g, device=dev))
+    v_obs = (v_obs + F["noise_sigma"] * noise).contiguous()
+    n_vis = int(v_obs.numel())
+
+    def timed(fn, reps=5):
+        torch.cuda.synchronize()
+        a = torch.cuda.Event(enable_timing=True)
+        b = torch.cuda.Event(enable_timing=True)
+        a.record()
+        for _ in range(reps):
+            fn()
+        b.record()
+        torch.cuda.synchronize()
+        return a.elapsed_time(b) / reps
+
+    fwd_ms = timed(lambda: m.forward_op(truth))
+    adj_ms = timed(lambda: m.adjoint_op(v_obs))
+    steps = 200
+    chi2_solve(m, v_obs, steps=2)  # warm-up
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    x, hist = chi2_solve(m, v_obs, steps=steps)
+    torch.cuda.synchronize()
+    dt = time.perf_counter() - t0
+    return {"n_vis": n_vis, "image": n, "forward_ms": fwd_ms, "adjoint_ms": adj_ms,
+            "steps": steps, "ms_per_step": dt / steps * 1e3,
+            "chi2_first": hist[0], "chi2_last": hist[-1],
+            "chi2_reduction": hist[-1] / hist[0],
+            "step": "forward (autograd) + adjoint backward + forward for the line search"}
+
+
 def bench_clean(args, dev):
     """Hogbom CLEAN: 2048^2 FP32 dirty image of 50 sources, 4096^2 PSF of the
     small array's sampling, gain 0.1, up to clean_iters iterations or 1 mJy."""
@@ -529,11 +591,26 @@ def bench_clean(args, dev):
         n_cpu = 200
         psf = np.ascontiguousarray(cw["psf"][1024:3072, 1024:3072])
         t0 = time.perf_counter()
-        H.clean(cw["dirty"], psf, max_iter=n_cpu, gain=0.1, threshold=1e-3)
+        ref = H.clean(cw["dirty"], psf, max_iter=n_cpu, gain=0.1, threshold=1e-3)
         dt = time.perf_counter() - t0
         out["cpu_reference"] = {"iter_per_s": n_cpu / dt, "cores": 1, "kind": "reference",
                                 "sample": f"{n_cpu} iterations, 2048^2, same-size PSF"}
         out["speedup_psf_2048"] = out["psf_2048"]["iter_per_s"] / (n_cpu / dt)
+        # the same first iterations on the GPU: components (model image) and
+        # residual against the reference module
+        run = K.HogbomRun(torch.as_tensor(cw["dirty"]), torch.as_tensor(psf), niter=n_cpu,
+                          gain=0.1, threshold=1e-3)
+        run.run(0, n_cpu)
+        model = run.model.cpu().numpy()
+        resid = run.resid.cpu().numpy()
+        out["components_vs_reference"] = {
+            "iterations": n_cpu,
+            "model_bit_exact": bool(np.array_equal(model, ref["model_image"])),
+            "residual_bit_exact": bool(np.array_equal(resid, ref["residual_image"])),
+            "n_components": int(np.count_nonzero(ref["model_image"])),
+            "max_flux_rel_diff": float(np.max(np.abs(model - ref["model_image"])) /
+                                       max(1e-30, float(np.max(np.abs(ref["model_image"]))))),
+        }
     except Exception as e:  # the compiled reference module is optional
         out["cpu_reference"] = {"unavailable": str(e)}
     return out
