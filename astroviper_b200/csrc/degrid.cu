@@ -257,6 +257,50 @@ __device__ __forceinline__ void put_value(const DegridArgs &d, int accumulate, i
   }
 }
 
+// Writes one sample's degridded values (all visibility polarisations):
+// normalised by sum_k w_k, phase-rotated when dphase is given, zeros in store
+// mode for flagged, unmapped and zero-norm samples.
+template <int NPG>
+__device__ __forceinline__ void degrid_write(const TiledDegridArgs &a, const DegridArgs &d,
+                                             const double *rs, const int (&pmv)[8],
+                                             const Rec &rc, const float2 (&acc)[NPG]) {
+  const double norm = rs[rc.ou] * rs[rc.ov];
+  const int64_t row_i = rc.row;
+  if (norm == 0.0) {  // the reference leaves such samples untouched
+    if (!a.accumulate)
+      for (int p = 0; p < d.nvpol; ++p) put_value(d, 0, row_i * d.nvpol + p, 0.0, 0.0);
+    return;
+  }
+  double ph_re = 1.0, ph_im = 0.0;
+  if (d.dphase) {
+    const int64_t tb = row_i / d.nvchan;
+    const int ichan = (int)(row_i - tb * d.nvchan);
+    double phase = (-2.0 * 3.141592653589793 * d.dphase[tb]) * d.freq[ichan] / d.c;
+    sincos(phase, &ph_im, &ph_re);
+  }
+  const double inv = 1.0 / norm;
+  for (int p = 0; p < d.nvpol; ++p) {
+    const int64_t k = row_i * d.nvpol + p;
+    const int apol = p < 8 ? pmv[p] : -1;
+    if (apol < 0 || (d.flag && d.flag[k])) {
+      if (!a.accumulate) put_value(d, 0, k, 0.0, 0.0);
+      continue;
+    }
+    float2 v = acc[0];
+#pragma unroll
+    for (int gp = 1; gp < NPG; ++gp)
+      if (apol == gp) v = acc[gp];
+    double vr = v.x, vi = v.y;
+    if (d.dphase) {
+      const double cr = ph_re, ci = -ph_im;
+      const double pr = vr * cr - vi * ci, pi = vr * ci + vi * cr;
+      vr = pr;
+      vi = pi;
+    }
+    put_value(d, a.accumulate, k, vr * inv, vi * inv);
+  }
+}
+
 template <int S, int NPG>
 __global__ void __launch_bounds__(DT_THREADS) k_degrid_tiled(TiledDegridArgs a) {
   using M = DSmem<S, NPG>;
@@ -326,87 +370,90 @@ __global__ void __launch_bounds__(DT_THREADS) k_degrid_tiled(TiledDegridArgs a) 
       sub[i] = v;
     }
     __syncthreads();
-    Rec nxt;
-    if (seg_lo + threadIdx.x < seg_hi) nxt = a.recs[seg_lo + threadIdx.x];
+    // each thread takes a pair of consecutive records: cell-sorted records
+    // usually share the cell, and then one read of the footprint serves
+    // both samples; a pair that straddles two cells reads the second
+    // footprint with loads predicated on the lanes that need it
+    Rec nxa, nxb;
+    {
+      const uint32_t r = seg_lo + 2 * threadIdx.x;
+      if (r < seg_hi) nxa = a.recs[r];
+      if (r + 1 < seg_hi) nxb = a.recs[r + 1];
+    }
     // one trip count per block, so every warp reaches the next barrier converged
-    for (uint32_t rb = seg_lo; rb < seg_hi; rb += DT_THREADS) {
-      const uint32_t r = rb + threadIdx.x;
-      const Rec rc = nxt;
-      if (r + DT_THREADS < seg_hi) nxt = a.recs[r + DT_THREADS];  // in flight meanwhile
+    for (uint32_t rb = seg_lo; rb < seg_hi; rb += 2 * DT_THREADS) {
+      const uint32_t r = rb + 2 * threadIdx.x;
+      const Rec ra = nxa, rbx = nxb;
+      {
+        const uint32_t rn = r + 2 * DT_THREADS;
+        if (rn < seg_hi) nxa = a.recs[rn];
+        if (rn + 1 < seg_hi) nxb = a.recs[rn + 1];
+      }
       if (r >= seg_hi) continue;
-      float cu[RW], cv[RW];
+      const bool has_b = r + 1 < seg_hi;
+      const Rec rcb = has_b ? rbx : ra;
+      float cua[RW], cva[RW], cub[RW], cvb[RW];
 #pragma unroll
       for (int k = 0; k < RW; k += 4) {
-        const float4 a4 = *(const float4 *)&tab[rc.ou * RW + k];
-        const float4 b4 = *(const float4 *)&tab[rc.ov * RW + k];
-        cu[k] = a4.x; cu[k + 1] = a4.y; cu[k + 2] = a4.z; cu[k + 3] = a4.w;
-        cv[k] = b4.x; cv[k + 1] = b4.y; cv[k + 2] = b4.z; cv[k + 3] = b4.w;
+        const float4 a4 = *(const float4 *)&tab[ra.ou * RW + k];
+        const float4 b4 = *(const float4 *)&tab[ra.ov * RW + k];
+        const float4 c4 = *(const float4 *)&tab[rcb.ou * RW + k];
+        const float4 d4 = *(const float4 *)&tab[rcb.ov * RW + k];
+        cua[k] = a4.x; cua[k + 1] = a4.y; cua[k + 2] = a4.z; cua[k + 3] = a4.w;
+        cva[k] = b4.x; cva[k + 1] = b4.y; cva[k + 2] = b4.z; cva[k + 3] = b4.w;
+        cub[k] = c4.x; cub[k + 1] = c4.y; cub[k + 2] = c4.z; cub[k + 3] = c4.w;
+        cvb[k] = d4.x; cvb[k + 1] = d4.y; cvb[k + 2] = d4.z; cvb[k + 3] = d4.w;
       }
-      float2 acc[NPG];
+      const bool same = rcb.du == ra.du && rcb.dv == ra.dv;
+      float2 acca[NPG], accb[NPG];
 #pragma unroll
-      for (int gp = 0; gp < NPG; ++gp) acc[gp] = make_float2(0.f, 0.f);
+      for (int gp = 0; gp < NPG; ++gp) {
+        acca[gp] = make_float2(0.f, 0.f);
+        accb[gp] = make_float2(0.f, 0.f);
+      }
 #pragma unroll
       for (int i = 0; i < S; ++i) {
-        float2 rowacc[NPG];
+        float2 rowa[NPG], rowb[NPG];
 #pragma unroll
-        for (int gp = 0; gp < NPG; ++gp) rowacc[gp] = make_float2(0.f, 0.f);
-        const float2 *row = sub + ((rc.du + i) * W + rc.dv) * NPG;
+        for (int gp = 0; gp < NPG; ++gp) {
+          rowa[gp] = make_float2(0.f, 0.f);
+          rowb[gp] = make_float2(0.f, 0.f);
+        }
+        const float2 *pa = sub + ((ra.du + i) * W + ra.dv) * NPG;
+        const float2 *pb = sub + ((rcb.du + i) * W + rcb.dv) * NPG;
 #pragma unroll
         for (int j = 0; j < S; ++j) {
-          float2 gv[NPG];
+          float2 ga[NPG], gb[NPG];
           if (NPG >= 2) {
 #pragma unroll
             for (int gp = 0; gp < NPG; gp += 2) {
-              const float4 q = *(const float4 *)(row + j * NPG + gp);
-              gv[gp] = make_float2(q.x, q.y);
-              gv[(gp + 1) % NPG] = make_float2(q.z, q.w);
+              const float4 qa = *(const float4 *)(pa + j * NPG + gp);
+              float4 qb = qa;
+              if (!same) qb = *(const float4 *)(pb + j * NPG + gp);
+              ga[gp] = make_float2(qa.x, qa.y);
+              ga[(gp + 1) % NPG] = make_float2(qa.z, qa.w);
+              gb[gp] = make_float2(qb.x, qb.y);
+              gb[(gp + 1) % NPG] = make_float2(qb.z, qb.w);
             }
           } else {
-            gv[0] = row[j];
+            ga[0] = pa[j];
+            gb[0] = ga[0];
+            if (!same) gb[0] = pb[j];
           }
 #pragma unroll
-          for (int gp = 0; gp < NPG; ++gp)
-            rowacc[gp] = __ffma2_rn(make_float2(cv[j], cv[j]), gv[gp], rowacc[gp]);
+          for (int gp = 0; gp < NPG; ++gp) {
+            rowa[gp] = __ffma2_rn(make_float2(cva[j], cva[j]), ga[gp], rowa[gp]);
+            rowb[gp] = __ffma2_rn(make_float2(cvb[j], cvb[j]), gb[gp], rowb[gp]);
+          }
         }
 #pragma unroll
-        for (int gp = 0; gp < NPG; ++gp)
-          acc[gp] = __ffma2_rn(make_float2(cu[i], cu[i]), rowacc[gp], acc[gp]);
-      }
-      const double norm = rs[rc.ou] * rs[rc.ov];
-      const int64_t row_i = rc.row;
-      if (norm == 0.0) {  // the reference leaves such samples untouched
-        if (!a.accumulate)
-          for (int p = 0; p < d.nvpol; ++p) put_value(d, 0, row_i * d.nvpol + p, 0.0, 0.0);
-        continue;
-      }
-      double ph_re = 1.0, ph_im = 0.0;
-      if (d.dphase) {
-        const int64_t tb = row_i / d.nvchan;
-        const int ichan = (int)(row_i - tb * d.nvchan);
-        double phase = (-2.0 * 3.141592653589793 * d.dphase[tb]) * d.freq[ichan] / d.c;
-        sincos(phase, &ph_im, &ph_re);
-      }
-      const double inv = 1.0 / norm;
-      for (int p = 0; p < d.nvpol; ++p) {
-        const int64_t k = row_i * d.nvpol + p;
-        const int apol = p < 8 ? pmv[p] : -1;
-        if (apol < 0 || (d.flag && d.flag[k])) {
-          if (!a.accumulate) put_value(d, 0, k, 0.0, 0.0);
-          continue;
+        for (int gp = 0; gp < NPG; ++gp) {
+          acca[gp] = __ffma2_rn(make_float2(cua[i], cua[i]), rowa[gp], acca[gp]);
+          accb[gp] = __ffma2_rn(make_float2(cub[i], cub[i]), rowb[gp], accb[gp]);
         }
-        float2 v = acc[0];
-#pragma unroll
-        for (int gp = 1; gp < NPG; ++gp)
-          if (apol == gp) v = acc[gp];
-        double vr = v.x, vi = v.y;
-        if (d.dphase) {
-          const double cr = ph_re, ci = -ph_im;
-          const double pr = vr * cr - vi * ci, pi = vr * ci + vi * cr;
-          vr = pr;
-          vi = pi;
-        }
-        put_value(d, a.accumulate, k, vr * inv, vi * inv);
       }
+      degrid_write<NPG>(a, d, rs, pmv, ra, acca);
+      if (has_b) degrid_write<NPG>(a, d, rs, pmv, rcb, accb);
     }
     seg_lo = seg_hi;
     if (seg_hi == t_end) ++t;
