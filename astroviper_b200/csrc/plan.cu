@@ -13,18 +13,14 @@ __global__ void k_chan_scale(const double *freq, int64_t nchan, double dl0, doub
   scale[2 * c + 1] = __ddiv_rn(-__dmul_rn(__dmul_rn(f, dl1), (double)n_v), C_LIGHT);
 }
 
-// Samples are enumerated time-fastest, k = (b * nchan + c) * nt + t, so the
-// 32 lanes of a warp hold consecutive time steps of one baseline and channel:
-// they fall in one or a few cells and the per-key atomics aggregate.
+// Key and record of sample (t, b, c).  The passes walk (baseline, channel)
+// series with a warp each, 32 consecutive time steps at a time: those fall in
+// one or a few cells, so the per-key atomics aggregate.
 __device__ __forceinline__ bool sample_key(const PlanGeom &g, const double *uvw,
                                            const double *freq, const double *scale,
-                                           const int32_t *chan_map, int64_t k,
-                                           uint32_t &key, Rec &rec) {
-  const int64_t nt = g.nt, nb = g.nb;
-  const int64_t t = k % nt;
-  const int64_t bc = k / nt;
-  const int c = (int)(bc % g.nchan);
-  const int64_t b = bc / g.nchan;
+                                           const int32_t *chan_map, int64_t t, int64_t b,
+                                           int c, uint32_t &key, Rec &rec) {
+  const int64_t nb = g.nb;
   const int64_t tb = t * nb + b;
   const int64_t row = tb * g.nchan + c;
   rec.row = (uint32_t)row;
@@ -54,48 +50,63 @@ __device__ __forceinline__ bool sample_key(const PlanGeom &g, const double *uvw,
   return true;
 }
 
-// Pass 1: count samples per key (warp-aggregated by key).
+// Pass 1: count samples per key (warp-aggregated by key).  Warp w takes
+// series w, w + n_warps, ... (series = b * nchan + c); the loops' trip counts
+// are the same on every lane of a warp.
 __global__ void __launch_bounds__(256) k_plan_count(PlanGeom g, const double *uvw,
                                                     const double *freq, const double *scale,
                                                     const int32_t *chan_map, uint32_t *hist) {
-  int64_t stride = (int64_t)gridDim.x * blockDim.x;
-  for (int64_t base = blockIdx.x * (int64_t)blockDim.x; base < g.n_rows; base += stride) {
-    int64_t row = base + threadIdx.x;
-    uint32_t key = 0xffffffffu;
-    Rec rec;
-    const bool in = row < g.n_rows;
-    if (in) sample_key(g, uvw, freq, scale, chan_map, row, key, rec);
-    unsigned active = __ballot_sync(0xffffffffu, in);
-    if (in) {
-      unsigned peers = __match_any_sync(active, key);
-      int leader = __ffs(peers) - 1;
-      if ((int)(threadIdx.x & 31) == leader) atomicAdd(&hist[key], (uint32_t)__popc(peers));
+  const int lane = threadIdx.x & 31;
+  const int64_t n_warps = ((int64_t)gridDim.x * blockDim.x) >> 5;
+  const int64_t n_series = g.nb * g.nchan;
+  for (int64_t sr = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5; sr < n_series;
+       sr += n_warps) {
+    const int64_t b = sr / g.nchan;
+    const int c = (int)(sr - b * g.nchan);
+    for (int64_t t0 = 0; t0 < g.nt; t0 += 32) {
+      const int64_t t = t0 + lane;
+      uint32_t key = 0xffffffffu;
+      Rec rec;
+      const bool in = t < g.nt;
+      if (in) sample_key(g, uvw, freq, scale, chan_map, t, b, c, key, rec);
+      const unsigned active = __ballot_sync(0xffffffffu, in);
+      if (in) {
+        const unsigned peers = __match_any_sync(active, key);
+        const int leader = __ffs(peers) - 1;
+        if (lane == leader) atomicAdd(&hist[key], (uint32_t)__popc(peers));
+      }
     }
   }
 }
 
-// Pass 2: scatter records to their key ranges.
+// Pass 2: scatter records to their key ranges (same walk as pass 1).
 __global__ void __launch_bounds__(256) k_plan_scatter(PlanGeom g, const double *uvw,
                                                       const double *freq, const double *scale,
                                                       const int32_t *chan_map,
                                                       uint32_t *cursor, Rec *recs) {
-  int64_t stride = (int64_t)gridDim.x * blockDim.x;
-  int lane = threadIdx.x & 31;
-  for (int64_t base = blockIdx.x * (int64_t)blockDim.x; base < g.n_rows; base += stride) {
-    int64_t row = base + threadIdx.x;
-    uint32_t key = 0xffffffffu;
-    Rec rec;
-    const bool in = row < g.n_rows;
-    if (in) sample_key(g, uvw, freq, scale, chan_map, row, key, rec);
-    unsigned active = __ballot_sync(0xffffffffu, in);
-    if (in) {
-      unsigned peers = __match_any_sync(active, key);
-      int leader = __ffs(peers) - 1;
-      uint32_t pos = 0;
-      if (lane == leader) pos = atomicAdd(&cursor[key], (uint32_t)__popc(peers));
-      pos = __shfl_sync(peers, pos, leader);
-      pos += __popc(peers & ((1u << lane) - 1u));
-      recs[pos] = rec;
+  const int lane = threadIdx.x & 31;
+  const int64_t n_warps = ((int64_t)gridDim.x * blockDim.x) >> 5;
+  const int64_t n_series = g.nb * g.nchan;
+  for (int64_t sr = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5; sr < n_series;
+       sr += n_warps) {
+    const int64_t b = sr / g.nchan;
+    const int c = (int)(sr - b * g.nchan);
+    for (int64_t t0 = 0; t0 < g.nt; t0 += 32) {
+      const int64_t t = t0 + lane;
+      uint32_t key = 0xffffffffu;
+      Rec rec;
+      const bool in = t < g.nt;
+      if (in) sample_key(g, uvw, freq, scale, chan_map, t, b, c, key, rec);
+      const unsigned active = __ballot_sync(0xffffffffu, in);
+      if (in) {
+        const unsigned peers = __match_any_sync(active, key);
+        const int leader = __ffs(peers) - 1;
+        uint32_t pos = 0;
+        if (lane == leader) pos = atomicAdd(&cursor[key], (uint32_t)__popc(peers));
+        pos = __shfl_sync(peers, pos, leader);
+        pos += __popc(peers & ((1u << lane) - 1u));
+        recs[pos] = rec;
+      }
     }
   }
 }
@@ -248,7 +259,8 @@ int plan_build(const PlanGeom &g, Plan &p, const double *uvw, const double *freq
     AV_LAUNCH_CHECK();
   }
   int sms = sm_count();
-  int64_t blocks = (g.n_rows + 255) / 256;
+  // one warp per (baseline, channel) series, 8 warps per block
+  int64_t blocks = (g.nb * g.nchan + 7) / 8;
   if (blocks > (int64_t)sms * 16) blocks = (int64_t)sms * 16;
   if (blocks < 1) blocks = 1;
   if (g.n_rows > 0) {
