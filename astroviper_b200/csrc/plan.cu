@@ -50,12 +50,14 @@ __device__ __forceinline__ bool sample_key(const PlanGeom &g, const double *uvw,
   return true;
 }
 
-// Pass 1: count samples per key (warp-aggregated by key).  Warp w takes
-// series w, w + n_warps, ... (series = b * nchan + c); the loops' trip counts
-// are the same on every lane of a warp.
+// Pass 1: key and record of every sample, stored in walk order (sample
+// index series * nt + t), and the count per key (warp-aggregated).  Warp w
+// takes series w, w + n_warps, ... (series = b * nchan + c); the loops' trip
+// counts are the same on every lane of a warp.
 __global__ void __launch_bounds__(256) k_plan_count(PlanGeom g, const double *uvw,
                                                     const double *freq, const double *scale,
-                                                    const int32_t *chan_map, uint32_t *hist) {
+                                                    const int32_t *chan_map, uint32_t *hist,
+                                                    uint32_t *walk_key, Rec *walk_rec) {
   const int lane = threadIdx.x & 31;
   const int64_t n_warps = ((int64_t)gridDim.x * blockDim.x) >> 5;
   const int64_t n_series = g.nb * g.nchan;
@@ -68,7 +70,11 @@ __global__ void __launch_bounds__(256) k_plan_count(PlanGeom g, const double *uv
       uint32_t key = 0xffffffffu;
       Rec rec;
       const bool in = t < g.nt;
-      if (in) sample_key(g, uvw, freq, scale, chan_map, t, b, c, key, rec);
+      if (in) {
+        sample_key(g, uvw, freq, scale, chan_map, t, b, c, key, rec);
+        walk_key[sr * g.nt + t] = key;
+        walk_rec[sr * g.nt + t] = rec;
+      }
       const unsigned active = __ballot_sync(0xffffffffu, in);
       if (in) {
         const unsigned peers = __match_any_sync(active, key);
@@ -79,24 +85,25 @@ __global__ void __launch_bounds__(256) k_plan_count(PlanGeom g, const double *uv
   }
 }
 
-// Pass 2: scatter records to their key ranges (same walk as pass 1).
-__global__ void __launch_bounds__(256) k_plan_scatter(PlanGeom g, const double *uvw,
-                                                      const double *freq, const double *scale,
-                                                      const int32_t *chan_map,
-                                                      uint32_t *cursor, Rec *recs) {
+// Pass 2: scatter the stored records to their key ranges (the same walk, so
+// the same warp aggregation; no position arithmetic).
+__global__ void __launch_bounds__(256) k_plan_scatter(PlanGeom g, const uint32_t *walk_key,
+                                                      const Rec *walk_rec, uint32_t *cursor,
+                                                      Rec *recs) {
   const int lane = threadIdx.x & 31;
   const int64_t n_warps = ((int64_t)gridDim.x * blockDim.x) >> 5;
   const int64_t n_series = g.nb * g.nchan;
   for (int64_t sr = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5; sr < n_series;
        sr += n_warps) {
-    const int64_t b = sr / g.nchan;
-    const int c = (int)(sr - b * g.nchan);
     for (int64_t t0 = 0; t0 < g.nt; t0 += 32) {
       const int64_t t = t0 + lane;
+      const bool in = t < g.nt;
       uint32_t key = 0xffffffffu;
       Rec rec;
-      const bool in = t < g.nt;
-      if (in) sample_key(g, uvw, freq, scale, chan_map, t, b, c, key, rec);
+      if (in) {
+        key = walk_key[sr * g.nt + t];
+        rec = walk_rec[sr * g.nt + t];
+      }
       const unsigned active = __ballot_sync(0xffffffffu, in);
       if (in) {
         const unsigned peers = __match_any_sync(active, key);
@@ -241,7 +248,10 @@ bool plan_carve(const PlanGeom &g, Workspace &ws, Plan &p) {
   p.scale = ws.take<double>(2 * (g.nchan > 0 ? g.nchan : 1));
   p.scan_tmp = ws.take<uint32_t>(SCAN_MAX_BLOCKS);
   p.counters = ws.take<uint32_t>(16);
-  return p.offs && p.cursor && p.tile_start && p.recs && p.scale && p.scan_tmp && p.counters;
+  p.walk_key = ws.take<uint32_t>(g.n_rows > 0 ? g.n_rows : 1);
+  p.walk_rec = ws.take<Rec>(g.n_rows > 0 ? g.n_rows : 1);
+  return p.offs && p.cursor && p.tile_start && p.recs && p.scale && p.scan_tmp &&
+         p.counters && p.walk_key && p.walk_rec;
 }
 
 int plan_build(const PlanGeom &g, Plan &p, const double *uvw, const double *freq,
@@ -264,13 +274,14 @@ int plan_build(const PlanGeom &g, Plan &p, const double *uvw, const double *freq
   if (blocks > (int64_t)sms * 16) blocks = (int64_t)sms * 16;
   if (blocks < 1) blocks = 1;
   if (g.n_rows > 0) {
-    k_plan_count<<<(unsigned)blocks, 256, 0, st>>>(g, uvw, freq, p.scale, chan_map, p.cursor);
+    k_plan_count<<<(unsigned)blocks, 256, 0, st>>>(g, uvw, freq, p.scale, chan_map, p.cursor,
+                                                  p.walk_key, p.walk_rec);
     AV_LAUNCH_CHECK();
   }
   int rc = scan_counts(p.cursor, p.offs, nk + 1, p.scan_tmp, st);
   if (rc) return rc;
   if (g.n_rows > 0) {
-    k_plan_scatter<<<(unsigned)blocks, 256, 0, st>>>(g, uvw, freq, p.scale, chan_map, p.cursor,
+    k_plan_scatter<<<(unsigned)blocks, 256, 0, st>>>(g, p.walk_key, p.walk_rec, p.cursor,
                                                     p.recs);
     AV_LAUNCH_CHECK();
   }

@@ -86,6 +86,9 @@ inline size_t plan_workspace_bytes(const PlanGeom &g) {
   b += Workspace::need(sizeof(double) * 2 * (g.nchan > 0 ? g.nchan : 1));
   b += Workspace::need(sizeof(uint32_t) * SCAN_MAX_BLOCKS);    // scan partials
   b += Workspace::need(sizeof(uint32_t) * 16);                 // counters
+  const size_t nr = g.n_rows > 0 ? (size_t)g.n_rows : 1;
+  b += Workspace::need(sizeof(uint32_t) * nr);                 // keys in walk order
+  b += Workspace::need(sizeof(Rec) * nr);                      // records in walk order
   return b;
 }
 
@@ -98,6 +101,8 @@ struct Plan {
   double *scale;       // 2 * nchan: per-channel uv scale (gridder convention)
   uint32_t *scan_tmp;
   uint32_t *counters;
+  uint32_t *walk_key;  // n_rows: key of each sample in walk order (pass 1)
+  Rec *walk_rec;       // n_rows: record of each sample in walk order (pass 1)
 };
 
 // Position of one sample in the gridder's convention (standard_grid.py:
