@@ -86,6 +86,22 @@ class Gridder:
                                           ws[2], K.stream_ptr()), "av_grid_tiled_execute")
         return grid, sum_weight
 
+    def plan(self, g_nchan=None):
+        """Build the gridding and the degridding plan (for a grid of g_nchan
+        channels, default n_img_chan) concurrently on two streams: both
+        depend only on uvw, the frequencies and the geometry, and neither
+        fills the GPU alone.  Later calls on the current stream see both."""
+        cur = torch.cuda.current_stream(self.dev)
+        if getattr(self, "_side", None) is None:
+            self._side = torch.cuda.Stream(self.dev)
+        self._side.wait_stream(cur)
+        with torch.cuda.stream(self._side):
+            ws = self._degrid_plan(self.n_img_chan if g_nchan is None else g_nchan)
+            self._dchanmap.record_stream(cur)
+        ws[0].record_stream(cur)
+        self._grid_plan()
+        cur.wait_stream(self._side)
+
     # ----------------------------------------------------------- degridding
     def _degrid_plan(self, g_nchan):
         key = int(g_nchan)

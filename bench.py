@@ -267,6 +267,7 @@ def main():
     def step(ev=None):
         G._gplan = None  # the binning plans are rebuilt every step (counted in the time)
         G._dplan = None
+        G.plan()         # both plans, concurrently on two streams
         grid.zero_()
         sumw.zero_()
         if ev is not None:
