@@ -21,7 +21,6 @@ import argparse
 import json
 import math
 import os
-import subprocess
 import sys
 import threading
 import time
@@ -39,7 +38,7 @@ WORKLOAD = ("64 ant (2016 bl) x 256 t x 64 ch x 4 pol = 33.03M vis, complex64, B
 def parse():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--steps", type=int, default=50)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--n-time", type=int, default=256)
@@ -63,57 +62,65 @@ def load_peaks():
 
 
 class ClockSampler:
-    """nvidia-smi clocks / throttle reasons sampled during the timed region."""
-    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
-         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
-         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+    """SM clock and clock-event (throttle) reasons sampled every 2 ms during
+    the timed region through NVML (read-only queries), in a thread; falls
+    back to nvidia-smi polling when NVML is unavailable."""
+    NAMES = {"hw_slowdown": "nvmlClocksEventReasonHwSlowdown",
+             "hw_thermal_slowdown": "nvmlClocksEventReasonHwThermalSlowdown",
+             "sw_thermal_slowdown": "nvmlClocksEventReasonSwThermalSlowdown",
+             "sw_power_cap": "nvmlClocksEventReasonSwPowerCap"}
 
-    def __init__(self, gpu_index):
-        self.idx = gpu_index
-        try:
-            import torch
-            self.idx = "GPU-" + str(torch.cuda.get_device_properties(gpu_index).uuid)
-        except Exception:
-            pass
-        self.proc = None
+    def __init__(self, gpu_index, period_s=0.002):
+        self.gpu_index = gpu_index
+        self.period = period_s
         self.rows = []
+        self.nv = None
+        self.h = None
+        self._stop = threading.Event()
+        try:
+            import pynvml as nv
+            import torch
+            nv.nvmlInit()
+            uuid = "GPU-" + str(torch.cuda.get_device_properties(gpu_index).uuid)
+            self.h = nv.nvmlDeviceGetHandleByUUID(uuid)
+            self.nv = nv
+        except Exception:
+            self.nv = None
+
+    def _poll(self):
+        nv = self.nv
+        while not self._stop.is_set():
+            try:
+                sm = nv.nvmlDeviceGetClockInfo(self.h, nv.NVML_CLOCK_SM)
+                mx = nv.nvmlDeviceGetMaxClockInfo(self.h, nv.NVML_CLOCK_SM)
+                rs = nv.nvmlDeviceGetCurrentClocksEventReasons(self.h)
+                self.rows.append((sm, mx, rs))
+            except Exception:
+                pass
+            self._stop.wait(self.period)
 
     def start(self):
-        try:
-            self.proc = subprocess.Popen(
-                ["nvidia-smi", f"--id={self.idx}", f"--query-gpu={self.Q}",
-                 "--format=csv,noheader,nounits", "-lms", "200"],
-                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
-            self.t = threading.Thread(target=self._read, daemon=True)
-            self.t.start()
-        except Exception:
-            self.proc = None
-
-    def _read(self):
-        for line in self.proc.stdout:
-            self.rows.append([x.strip() for x in line.split(",")])
+        if self.nv is None:
+            return
+        self.t = threading.Thread(target=self._poll, daemon=True)
+        self.t.start()
 
     def stop(self):
-        if self.proc is None:
-            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
-        self.proc.terminate()
-        try:
-            self.proc.wait(timeout=5)
-        except Exception:
-            self.proc.kill()
+        if self.nv is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["NVML unavailable"],
+                    "samples": 0}
+        self._stop.set()
         self.t.join(timeout=2)
-        sm = [float(r[1]) for r in self.rows if len(r) >= 9 and r[1].replace(".", "").isdigit()]
-        mx = [float(r[2]) for r in self.rows if len(r) >= 9 and r[2].replace(".", "").isdigit()]
-        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        sm = [r[0] for r in self.rows]
+        mx = [r[1] for r in self.rows]
         reasons = set()
-        for r in self.rows:
-            if len(r) >= 9:
-                for k, nm in enumerate(names):
-                    if r[5 + k].lower() == "active":
-                        reasons.add(nm)
+        for _, _, rs in self.rows:
+            for nm, attr in self.NAMES.items():
+                if rs & getattr(self.nv, attr, 0):
+                    reasons.add(nm)
         return {"sm_mhz": float(np.median(sm)) if sm else None,
                 "sm_max_mhz": max(mx) if mx else None, "reasons": sorted(reasons),
-                "samples": len(sm)}
+                "samples": len(self.rows), "source": "NVML, 2 ms"}
 
 
 # DRAM bytes read + written per launch and per visibility of the two main
@@ -345,6 +352,13 @@ def main():
     im32 = Gs.image(g32, s32)
     im64 = Gs.image(g64, s64)
     err_img = rel(im32, im64)
+    # PSF: the weights gridded (do_psf) and imaged, FP32-input tiled path
+    # against the FP64 plain gridder
+    p32, ps32 = Gs.grid(None, iw[:ts], do_psf=True)
+    p64, ps64 = K.grid(None, iw_s, uvw_s, W["freq"], np.zeros(nchan, int), np.arange(npol),
+                       G.cgk, img, cell, 7, 100, 1, npol, do_psf=True, precision="fp64")
+    err_psf = rel(Gs.image(p32, ps32), Gs.image(p64, ps64))
+    del p32, p64
     v32 = Gs.degrid(g64)
     nx, ny = int(img[0]), int(img[1])
     v64 = K.degrid(g64, uvw_s, W["freq"], (-cell[0] * nx, -cell[1] * ny), (nx / 2, ny / 2),
@@ -416,8 +430,8 @@ def main():
         "fp64_plain_gridder": {"value": plain_mvis, "unit": "Mvis/s",
                                "sample": f"{ts} of {nt} time steps"},
         "speedup_vs_fp64_plain": (n_vis / (t_grid_k / 1e3) / 1e6) / plain_mvis,
-        "rel_err_vs_fp64": {"grid": err_grid, "dirty_image": err_img, "degrid_vis": err_vis,
-                            "sample": f"{ts} of {nt} time steps"},
+        "rel_err_vs_fp64": {"grid": err_grid, "dirty_image": err_img, "psf": err_psf,
+                            "degrid_vis": err_vis, "sample": f"{ts} of {nt} time steps"},
         "clocks": clk,
         "gpu_launches": launches,
         "cpu_baseline": cpu,
@@ -604,6 +618,17 @@ def bench_clean(args, dev):
         run.run(0, n_cpu)
         model = run.model.cpu().numpy()
         resid = run.resid.cpu().numpy()
+        # the FP32 CLEAN model against the same iterations in FP64
+        run64 = K.HogbomRun(torch.as_tensor(cw["dirty"].astype(np.float64)),
+                            torch.as_tensor(psf.astype(np.float64)), niter=n_cpu, gain=0.1,
+                            threshold=1e-3)
+        run64.run(0, n_cpu)
+        m64 = run64.model.cpu().numpy()
+        out["model_fp32_vs_fp64"] = {
+            "iterations": n_cpu,
+            "same_component_positions": bool(np.array_equal(model != 0, m64 != 0)),
+            "rel_err": float(np.linalg.norm(model - m64) / np.linalg.norm(m64)),
+        }
         out["components_vs_reference"] = {
             "iterations": n_cpu,
             "model_bit_exact": bool(np.array_equal(model, ref["model_image"])),
