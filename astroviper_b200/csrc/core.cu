@@ -103,7 +103,7 @@ __global__ void k_pswf_kernel4d(double *out, int os, int support, int n_os) {
 
 // ------------------------------------------------------------ tuning ---
 constexpr int kTuneKnobs = 2;
-static std::atomic<int64_t> g_tune[kTuneKnobs] = {{16}, {8}};
+static std::atomic<int64_t> g_tune[kTuneKnobs] = {{16}, {16}};
 
 int64_t tune_value(int knob) {
   return (knob >= 0 && knob < kTuneKnobs) ? g_tune[knob].load() : 0;

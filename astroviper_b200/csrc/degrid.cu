@@ -192,6 +192,7 @@ struct TiledDegridArgs {
   int64_t n_tiles, ntu, ntv, chunk;
   DegridArgs d;
   int cgk_len;
+  uint32_t *sched;          // device: [0] next chunk, [1] CTAs done (0 between launches)
   int accumulate;           // 1: values +=, 0: values = (skipped samples get 0)
   // complex64 store mode, 4 visibility polarisations, no flags, no phase,
   // values 32-byte aligned: a sample's 4 values go out as two 16-byte stores
@@ -334,10 +335,27 @@ __global__ void __launch_bounds__(DT_THREADS) k_degrid_tiled(TiledDegridArgs a) 
   float2 *sub = (float2 *)(smem + M::tab_bytes + M::rs_bytes);
   const DegridArgs &d = a.d;
 
+  __shared__ int s_chunk;
   const uint32_t n_rec = *a.n_rec;
   const uint32_t n_all = a.accumulate ? n_rec : (uint32_t)a.n_rows;
-  const uint32_t r0 = (uint32_t)(blockIdx.x * a.chunk);
-  if (r0 >= n_all) return;
+  const int64_t n_chunks = ((int64_t)n_all + a.chunk - 1) / a.chunk;
+  build_tap_tables_d<S, RW>(tab, rs, d.cf, a.cgk_len, d.sampling);
+  int pmv[8];
+#pragma unroll
+  for (int p = 0; p < 8; ++p) {
+    int v = p < d.nvpol ? d.polmap[p] : -1;
+    pmv[p] = (v >= 0 && v < NPG && v < d.g_npol) ? v : -1;
+  }
+  const int64_t gplane = d.g_n2 * d.g_n3;
+
+  // persistent: chunks of records from a.sched[0] until none are left
+  for (;;) {
+  __syncthreads();  // tables built; the previous chunk is done with sub and s_chunk
+  if (threadIdx.x == 0) s_chunk = (int)atomicAdd(&a.sched[0], 1u);
+  __syncthreads();
+  const int64_t ch = s_chunk;
+  if (ch >= n_chunks) break;
+  const uint32_t r0 = (uint32_t)(ch * a.chunk);
   const uint32_t r1 = (uint32_t)min((int64_t)n_all, (int64_t)r0 + a.chunk);
   // store mode: skipped samples (after the usable records) get zeros
   if (!a.accumulate && r1 > n_rec) {
@@ -350,18 +368,10 @@ __global__ void __launch_bounds__(DT_THREADS) k_degrid_tiled(TiledDegridArgs a) 
     }
   }
   const uint32_t v1 = min(r1, n_rec);
-  if (r0 >= v1) return;
-  build_tap_tables_d<S, RW>(tab, rs, d.cf, a.cgk_len, d.sampling);
-  int pmv[8];
-#pragma unroll
-  for (int p = 0; p < 8; ++p) {
-    int v = p < d.nvpol ? d.polmap[p] : -1;
-    pmv[p] = (v >= 0 && v < NPG && v < d.g_npol) ? v : -1;
-  }
+  if (r0 >= v1) continue;
 
   int t = find_tile_d(a.tile_start, a.n_tiles, r0);
   uint32_t seg_lo = r0;
-  const int64_t gplane = d.g_n2 * d.g_n3;
   while (seg_lo < v1) {
     uint32_t t_end = a.tile_start[t + 1];
     uint32_t seg_hi = min(v1, t_end);
@@ -481,21 +491,39 @@ __global__ void __launch_bounds__(DT_THREADS) k_degrid_tiled(TiledDegridArgs a) 
     seg_lo = seg_hi;
     if (seg_hi == t_end) ++t;
   }
+  }
+  // every CTA has taken its last chunk: the last one to get here re-arms
+  if (threadIdx.x == 0) {
+    __threadfence();
+    if (atomicAdd(&a.sched[1], 1u) == gridDim.x - 1) {
+      a.sched[0] = 0u;
+      a.sched[1] = 0u;
+      __threadfence();
+    }
+  }
 }
 
 template <int S, int NPG>
 static int launch_degrid_tiled(const TiledDegridArgs &a, int64_t nblocks, cudaStream_t st) {
+  // persistent CTAs: at most as many as are resident at once
   size_t smem = DSmem<S, NPG>::total;
-  if (smem > 48 * 1024) {
-    static bool configured[64] = {false};
-    int dev = 0;
-    cudaGetDevice(&dev);
-    if (dev >= 0 && dev < 64 && !configured[dev]) {
+  static int resident[64] = {0};
+  int dev = 0;
+  AV_CUDA(cudaGetDevice(&dev));
+  if (dev < 0 || dev >= 64) {
+    set_error("av_degrid_tiled: device %d beyond the 64 this library tracks", dev);
+    return AV_ERR_UNSUPPORTED;
+  }
+  if (resident[dev] == 0) {
+    if (smem > 48 * 1024)
       AV_CUDA(cudaFuncSetAttribute(k_degrid_tiled<S, NPG>,
                                    cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-      configured[dev] = true;
-    }
+    int per_sm = 0;
+    AV_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_degrid_tiled<S, NPG>,
+                                                          DT_THREADS, smem));
+    resident[dev] = (per_sm > 0 ? per_sm : 1) * sm_count();
   }
+  if (nblocks > resident[dev]) nblocks = resident[dev];
   k_degrid_tiled<S, NPG><<<(unsigned)nblocks, DT_THREADS, smem, st>>>(a);
   AV_LAUNCH_CHECK();
   return AV_OK;
@@ -705,6 +733,7 @@ int av_degrid_tiled_execute(const double *dphase, void *values, int values_dtype
   a.chunk = chunk;
   a.d = d;
   a.cgk_len = sampling * (support / 2 + 1);
+  a.sched = p.counters + 2;
   a.accumulate = accumulate ? 1 : 0;
   a.n_rows = rows;
   a.fast_out = (!accumulate && values_dtype == AV_C64 && nvpol == 4 && flag == nullptr &&

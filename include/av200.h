@@ -56,8 +56,8 @@ unsigned long long av_launch_count(void);
  * (astroviper_b200.autotune) or by hand.
  *   AV_TUNE_GRID_CHUNKS_PER_SM   record chunks per SM handed out by the
  *                                persistent tiled gridder (default 16)
- *   AV_TUNE_DEGRID_CHUNKS_PER_SM record chunks per SM of the tiled
- *                                degridder (default 8)
+ *   AV_TUNE_DEGRID_CHUNKS_PER_SM record chunks per SM handed out by the
+ *                                persistent tiled degridder (default 16)
  * av_tune_set returns AV_ERR_ARG for an unknown knob or a value outside
  * [1, 1024]; av_tune_get returns -1 for an unknown knob. */
 enum av_tune { AV_TUNE_GRID_CHUNKS_PER_SM = 0, AV_TUNE_DEGRID_CHUNKS_PER_SM = 1 };
