@@ -50,6 +50,23 @@ __device__ __forceinline__ bool sample_key(const PlanGeom &g, const double *uvw,
   return true;
 }
 
+// Warp aggregation of per-key atomics over runs of equal keys in lane order
+// (a warp holds consecutive time steps of one series, so equal keys are
+// adjacent).  Returns whether this lane leads a run and, for a leader, the
+// run's length.  Lanes without a sample (in = false) form no run and end
+// the previous one; they are always at the top of the warp.
+__device__ __forceinline__ bool run_leader(uint32_t key, bool in, int lane, uint32_t &len) {
+  const uint32_t prev = __shfl_up_sync(0xffffffffu, key, 1);
+  const bool lead = in && (lane == 0 || prev != key);
+  const unsigned leaders = __ballot_sync(0xffffffffu, lead);
+  const unsigned valid = __ballot_sync(0xffffffffu, in);
+  // next leader above this lane, else the end of the valid lanes
+  const unsigned above = leaders & ~(0xffffffffu >> (31 - lane));
+  const int end = above ? __ffs(above) - 1 : 32 - __clz(valid);
+  len = (uint32_t)(end - lane);
+  return lead;
+}
+
 // Pass 1: key and record of every sample, stored in walk order (sample
 // index series * nt + t), and the count per key (warp-aggregated).  Warp w
 // takes series w, w + n_warps, ... (series = b * nchan + c); the loops' trip
@@ -75,12 +92,9 @@ __global__ void __launch_bounds__(256) k_plan_count(PlanGeom g, const double *uv
         walk_key[sr * g.nt + t] = key;
         walk_rec[sr * g.nt + t] = rec;
       }
-      const unsigned active = __ballot_sync(0xffffffffu, in);
-      if (in) {
-        const unsigned peers = __match_any_sync(active, key);
-        const int leader = __ffs(peers) - 1;
-        if (lane == leader) atomicAdd(&hist[key], (uint32_t)__popc(peers));
-      }
+      uint32_t len;
+      const bool lead = run_leader(key, in, lane, len);
+      if (lead) atomicAdd(&hist[key], len);
     }
   }
 }
@@ -104,16 +118,15 @@ __global__ void __launch_bounds__(256) k_plan_scatter(PlanGeom g, const uint32_t
         key = walk_key[sr * g.nt + t];
         rec = walk_rec[sr * g.nt + t];
       }
-      const unsigned active = __ballot_sync(0xffffffffu, in);
-      if (in) {
-        const unsigned peers = __match_any_sync(active, key);
-        const int leader = __ffs(peers) - 1;
-        uint32_t pos = 0;
-        if (lane == leader) pos = atomicAdd(&cursor[key], (uint32_t)__popc(peers));
-        pos = __shfl_sync(peers, pos, leader);
-        pos += __popc(peers & ((1u << lane) - 1u));
-        recs[pos] = rec;
-      }
+      uint32_t len;
+      const bool lead = run_leader(key, in, lane, len);
+      uint32_t pos = 0;
+      if (lead) pos = atomicAdd(&cursor[key], len);
+      // each lane's run leader: the highest leader at or below it
+      const unsigned leaders = __ballot_sync(0xffffffffu, lead);
+      const int ll = 31 - __clz(leaders & (0xffffffffu >> (31 - lane)));
+      pos = __shfl_sync(0xffffffffu, pos, ll) + (uint32_t)(lane - ll);
+      if (in) recs[pos] = rec;
     }
   }
 }
