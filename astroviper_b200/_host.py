@@ -44,6 +44,20 @@ def host(t, like=None, dtype=None):
 _TORCH = {np.dtype(v): k for k, v in _NP.items()}
 
 
+def streamable(*arrays, min_bytes=None):
+    """True when every given array (None skipped) is a numpy array and
+    together they hold at least two stream chunks: such inputs are copied to
+    the device in time chunks that overlap the kernels (_kernels.grid_streamed,
+    _kernels.degrid_streamed)."""
+    given = [a for a in arrays if a is not None]
+    if not given or not all(isinstance(a, np.ndarray) and a.ndim >= 2 for a in given):
+        return False
+    if len({a.shape[0] for a in given}) != 1:
+        return False
+    need = 2 * K.STREAM_CHUNK_BYTES if min_bytes is None else min_bytes
+    return sum(a.nbytes for a in given) >= need
+
+
 def write_back(dst, src_t):
     """Copy a device result into a caller's array in place."""
     if is_torch(dst):

@@ -7,6 +7,7 @@ and is handed to the library as (pointer, bytes).
 """
 import math
 
+import numpy as np
 import torch
 
 from . import _lib
@@ -97,6 +98,18 @@ def pswf_kernel4d(oversampling, support):
 
 
 # ----------------------------------------------------------------- gridding --
+def grid_tiled_ok(precision, do_imaging_weight, support, oversampling, npol, n_img_pol):
+    """Whether grid() runs the tiled kernel for these options."""
+    return not (precision == "fp64" or do_imaging_weight or support > 9 or support < 3
+                or oversampling > 254 or npol > 4 or n_img_pol > 4)
+
+
+def degrid_tiled_ok(precision, support, sampling, g_npol, c):
+    """Whether degrid() runs the tiled kernel for these options."""
+    return (precision != "fp64" and 3 <= support <= 9 and sampling <= 254 and g_npol <= 4
+            and float(c) == C_LIGHT)
+
+
 def grid(vis, weight, uvw, freq, chan_map, pol_map, cgk, n_uv, delta_lm, support,
          oversampling, n_img_chan, n_img_pol, grid_out=None, sum_weight=None, do_psf=False,
          do_imaging_weight=False, precision="fp32"):
@@ -115,8 +128,8 @@ def grid(vis, weight, uvw, freq, chan_map, pol_map, cgk, n_uv, delta_lm, support
     cm = on_device(chan_map, torch.int32)
     pm = on_device(pol_map, torch.int32)
     cgk = on_device(cgk, torch.float64)
-    fp64 = precision == "fp64" or do_imaging_weight or support > 9 or support < 3 \
-        or oversampling > 254 or npol > 4 or n_img_pol > 4
+    fp64 = not grid_tiled_ok(precision, do_imaging_weight, support, oversampling, npol,
+                             n_img_pol)
     if grid_out is None:
         grid_out = torch.zeros((n_img_chan, n_img_pol, nu, nv), dtype=torch.complex128,
                                device=dev)
@@ -173,8 +186,7 @@ def degrid(grid_t, uvw, freq, scale, offset, chanmap, polmap, cgk, support, samp
     fl = None if flag is None else on_device(flag).to(torch.uint8).contiguous()
     dph = None if dphase is None else on_device(dphase, torch.float64)
     g_nchan, g_npol, g_n2, g_n3 = (int(s) for s in g.shape)
-    tiled_ok = (precision != "fp64" and 3 <= support <= 9 and sampling <= 254 and g_npol <= 4
-                and float(c) == C_LIGHT)
+    tiled_ok = degrid_tiled_ok(precision, support, sampling, g_npol, c)
     if values is None:
         vdt = torch.complex64 if tiled_ok else torch.complex128
         if tiled_ok and not accumulate:
@@ -193,8 +205,6 @@ def degrid(grid_t, uvw, freq, scale, offset, chanmap, polmap, cgk, support, samp
                                    p(pm), nt, nb, nvchan, nvpol, stream_ptr())
         check(rc, "av_degrid_plain")
         return values
-    if g.dtype == torch.complex128:
-        g = g.to(torch.complex64)
     ws_bytes = lib().av_degrid_tiled_workspace_size(nt, nb, nvchan, g_n2, g_n3, g_nchan,
                                                     int(support))
     _buf, wptr, wbytes = workspace(ws_bytes)
@@ -204,6 +214,145 @@ def degrid(grid_t, uvw, freq, scale, offset, chanmap, polmap, cgk, support, samp
                                p(freq), float(c), int(support), int(sampling), p(cgk), p(cm),
                                p(pm), nt, nb, nvchan, nvpol, wptr, wbytes, stream_ptr())
     check(rc, "av_degrid_tiled")
+    return values
+
+
+# ------------------------------------------------- streamed host inputs ----
+# Large host (numpy) inputs go to the device in time chunks on a copy stream
+# while the previous chunk is planned and gridded / degridded on the current
+# stream (and, for the degridder, the chunk before that is copied back on a
+# third stream): the kernels and the copies in both directions overlap.  The
+# overlap needs page-locked host arrays; pageable ones are copied
+# synchronously, with the same results.
+STREAM_CHUNK_BYTES = 128 << 20
+_streams = {}
+
+
+def _side_stream(name):
+    key = (name, torch.cuda.current_device())
+    if key not in _streams:
+        _streams[key] = torch.cuda.Stream()
+    return _streams[key]
+
+
+def time_chunks(nt, bytes_per_t, chunk_bytes=None):
+    """[(t0, t1), ...] covering range(nt) in about chunk_bytes pieces
+    (STREAM_CHUNK_BYTES when None)."""
+    chunk_bytes = STREAM_CHUNK_BYTES if chunk_bytes is None else chunk_bytes
+    n = int(max(1, min(nt, -(-int(nt * bytes_per_t) // int(chunk_bytes)))))
+    edges = [nt * i // n for i in range(n + 1)]
+    return list(zip(edges[:-1], edges[1:]))
+
+
+def _h2d(dst, host_slice):
+    dst.copy_(torch.from_numpy(np.ascontiguousarray(host_slice)), non_blocking=True)
+
+
+def grid_streamed(vis, weight, uvw, freq, chan_map, pol_map, cgk, n_uv, delta_lm, support,
+                  oversampling, n_img_chan, n_img_pol, grid_out, sum_weight, do_psf=False,
+                  chunk_bytes=None):
+    """grid() of host arrays vis / weight / uvw (tiled kernel), copied to the
+    device in time chunks that overlap the gridding of the previous chunk.
+    Accumulates into the device arrays grid_out / sum_weight."""
+    nt = int(uvw.shape[0])
+    per_t = weight[0].nbytes + (0 if do_psf else vis[0].nbytes) + uvw[0].nbytes
+    chunks = time_chunks(nt, per_t, chunk_bytes)
+    tmax = max(t1 - t0 for t0, t1 in chunks)
+    dev = device()
+    freq = on_device(freq, torch.float64)
+    chan_map = on_device(chan_map, torch.int32)
+    pol_map = on_device(pol_map, torch.int32)
+    cgk = on_device(cgk, torch.float64)
+    cur = torch.cuda.current_stream()
+    cp = _side_stream("h2d")
+    mk = lambda a: torch.empty((tmax,) + tuple(a.shape[1:]),
+                               dtype=torch.from_numpy(a[:1]).dtype, device=dev)
+    slots = [dict(w=mk(weight), u=mk(uvw), v=None if do_psf else mk(vis)) for _ in range(2)]
+    free = [None, None]
+    cp.wait_stream(cur)
+    for i, (t0, t1) in enumerate(chunks):
+        sl = slots[i % 2]
+        n = t1 - t0
+        with torch.cuda.stream(cp):
+            if free[i % 2] is not None:
+                cp.wait_event(free[i % 2])
+            _h2d(sl["w"][:n], weight[t0:t1])
+            _h2d(sl["u"][:n], uvw[t0:t1])
+            if not do_psf:
+                _h2d(sl["v"][:n], vis[t0:t1])
+            ready = torch.cuda.Event()
+            ready.record(cp)
+        cur.wait_event(ready)
+        grid(None if do_psf else sl["v"][:n], sl["w"][:n], sl["u"][:n], freq, chan_map, pol_map,
+             cgk, n_uv, delta_lm, support, oversampling, n_img_chan, n_img_pol,
+             grid_out=grid_out, sum_weight=sum_weight, do_psf=do_psf, precision="fp32")
+        ev = torch.cuda.Event()
+        ev.record(cur)
+        free[i % 2] = ev
+    return grid_out, sum_weight
+
+
+def degrid_streamed(grid_t, uvw, freq, scale, offset, chanmap, polmap, cgk, support, sampling,
+                    values, flag=None, dphase=None, chunk_bytes=None):
+    """values (host array, updated in place) += degridded model of the device
+    grid grid_t (tiled kernel), in time chunks: chunk i+1 is copied in while
+    chunk i is degridded and chunk i-1 copied back.  Returns when values
+    holds the result."""
+    nt = int(uvw.shape[0])
+    per_t = values[0].nbytes * 2 + uvw[0].nbytes + (0 if flag is None else flag[0].nbytes)
+    chunks = time_chunks(nt, per_t, chunk_bytes)
+    tmax = max(t1 - t0 for t0, t1 in chunks)
+    dev = device()
+    grid_t = on_device(grid_t)
+    freq = on_device(freq, torch.float64)
+    chanmap = on_device(chanmap, torch.int32)
+    polmap = on_device(polmap, torch.int32)
+    cgk = on_device(cgk, torch.float64)
+    cur = torch.cuda.current_stream()
+    cin = _side_stream("h2d")
+    cout = _side_stream("d2h")
+    vt = torch.from_numpy(values[:1]).dtype
+    slots = []
+    for _ in range(2):
+        slots.append(dict(
+            v=torch.empty((tmax,) + tuple(values.shape[1:]), dtype=vt, device=dev),
+            u=torch.empty((tmax,) + tuple(uvw.shape[1:]), dtype=torch.float64, device=dev),
+            f=None if flag is None else torch.empty((tmax,) + tuple(flag.shape[1:]),
+                                                    dtype=torch.uint8, device=dev),
+            d=None if dphase is None else torch.empty((tmax,) + tuple(np.shape(dphase)[1:]),
+                                                      dtype=torch.float64, device=dev)))
+    vals_t = torch.from_numpy(values)
+    free = [None, None]
+    cin.wait_stream(cur)
+    for i, (t0, t1) in enumerate(chunks):
+        sl = slots[i % 2]
+        n = t1 - t0
+        with torch.cuda.stream(cin):
+            if free[i % 2] is not None:
+                cin.wait_event(free[i % 2])
+            _h2d(sl["v"][:n], values[t0:t1])
+            _h2d(sl["u"][:n], np.asarray(uvw[t0:t1], dtype=np.float64))
+            if flag is not None:
+                f = np.asarray(flag[t0:t1])
+                _h2d(sl["f"][:n], f.view(np.uint8) if f.dtype == np.bool_ else f.astype(np.uint8))
+            if dphase is not None:
+                _h2d(sl["d"][:n], np.asarray(dphase[t0:t1], dtype=np.float64))
+            ready = torch.cuda.Event()
+            ready.record(cin)
+        cur.wait_event(ready)
+        degrid(grid_t, sl["u"][:n], freq, scale, offset, chanmap, polmap, cgk, support,
+               sampling, values=sl["v"][:n], flag=None if flag is None else sl["f"][:n],
+               dphase=None if dphase is None else sl["d"][:n], accumulate=True)
+        done = torch.cuda.Event()
+        done.record(cur)
+        with torch.cuda.stream(cout):
+            cout.wait_event(done)
+            vals_t[t0:t1].copy_(sl["v"][:n], non_blocking=True)
+            back = torch.cuda.Event()
+            back.record(cout)
+        free[i % 2] = back
+    cur.wait_stream(cout)
+    cout.synchronize()
     return values
 
 

@@ -52,6 +52,20 @@ def sgrid_numba(uvw, dphase, freq, c, scale, offset, sampling):
 def _degrid_inplace(uvw, dphase, values, flag, scale, offset, grid, freq, c, support, sampling,
                     convFunc, chanmap, polmap, precision=None):
     precision = resolve_precision(precision)
+    if (isinstance(values, np.ndarray) and values.flags.c_contiguous and values.flags.writeable
+            and np.iscomplexobj(values) and np.ndim(grid) == 4
+            and H.streamable(values, uvw, None if flag is None else np.asarray(flag))
+            and K.degrid_tiled_ok(precision, int(support), int(sampling),
+                                  int(np.shape(grid)[1]), c)):
+        # large host arrays: values / flags / uvw in time chunks, copied in
+        # and back while neighbouring chunks are degridded
+        dph = None
+        if dphase is not None and np.any(np.asarray(dphase) != 0):
+            dph = np.asarray(dphase, dtype=np.float64)
+        K.degrid_streamed(grid, uvw, freq, scale, offset, chanmap, polmap, convFunc,
+                          int(support), int(sampling), values,
+                          flag=None if flag is None else np.asarray(flag), dphase=dph)
+        return
     vals = H.dev(values)
     if not vals.is_complex():
         raise TypeError("values must be complex")

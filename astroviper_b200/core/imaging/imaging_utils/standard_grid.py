@@ -33,10 +33,19 @@ def _grid_into(grid, sum_weight, do_psf, do_imaging_weight, vis_data, uvw, freq_
     if precision == "fp32" and real_grid:
         precision = "fp64"  # the tiled kernel writes complex grids only
     target = g_dev
-    K.grid(None if do_psf else vis_data, H.dev(weight), uvw, freq_chan, chan_map, pol_map,
-           cgk_1D, n_uv, delta_lm, support, oversampling, n_img_chan, n_img_pol,
-           grid_out=target, sum_weight=sw_dev, do_psf=do_psf,
-           do_imaging_weight=do_imaging_weight, precision=precision)
+    vis_in = None if do_psf else vis_data
+    if (not real_grid and H.streamable(vis_in, weight, uvw)
+            and K.grid_tiled_ok(precision, do_imaging_weight, support, oversampling,
+                                int(weight.shape[3]), n_img_pol)):
+        # large host inputs: copied in time chunks that overlap the gridding
+        K.grid_streamed(vis_in, weight, uvw, freq_chan, chan_map, pol_map, cgk_1D, n_uv,
+                        delta_lm, support, oversampling, n_img_chan, n_img_pol,
+                        grid_out=target, sum_weight=sw_dev, do_psf=do_psf)
+    else:
+        K.grid(vis_in, H.dev(weight), uvw, freq_chan, chan_map, pol_map,
+               cgk_1D, n_uv, delta_lm, support, oversampling, n_img_chan, n_img_pol,
+               grid_out=target, sum_weight=sw_dev, do_psf=do_psf,
+               do_imaging_weight=do_imaging_weight, precision=precision)
     if H.is_torch(grid):
         if grid.data_ptr() != target.data_ptr():
             grid.copy_(target)

@@ -152,3 +152,26 @@ def test_product_path_refuses_to_run_without_gpu():
         create_prolate_spheroidal_kernel_1D
     with pytest.raises(RuntimeError, match="needs a CUDA device"):
         create_prolate_spheroidal_kernel_1D(100, 7)
+
+
+def test_stream_time_chunks_cover_every_step_once():
+    """The time chunks of the streamed host-input paths tile range(nt)."""
+    from astroviper_b200 import _kernels as K
+    for nt, per_t, cb in ((1, 10, 4096), (7, 4096, 4096), (100, 1000, 4096), (5, 1, None),
+                          (1000, 3 << 20, None)):
+        ch = K.time_chunks(nt, per_t, cb)
+        assert ch[0][0] == 0 and ch[-1][1] == nt
+        assert all(a[1] == b[0] for a, b in zip(ch, ch[1:]))
+        assert all(t1 > t0 for t0, t1 in ch)
+        if cb is not None:
+            assert len(ch) == min(nt, -(-nt * per_t // cb))
+
+
+def test_streamable_needs_numpy_arrays_of_two_chunks():
+    from astroviper_b200 import _host as H
+    a = np.zeros((8, 100))
+    assert H.streamable(a, None, min_bytes=a.nbytes)
+    assert not H.streamable(a, min_bytes=a.nbytes + 1)
+    assert not H.streamable(a, np.zeros((7, 100)), min_bytes=1)
+    assert not H.streamable(None, min_bytes=1)
+    assert not H.streamable(a, [[1.0]], min_bytes=1)
