@@ -13,41 +13,51 @@ __global__ void k_chan_scale(const double *freq, int64_t nchan, double dl0, doub
   scale[2 * c + 1] = __ddiv_rn(-__dmul_rn(__dmul_rn(f, dl1), (double)n_v), C_LIGHT);
 }
 
-// Key and record of sample (t, b, c).  The passes walk (baseline, channel)
-// series with a warp each, 32 consecutive time steps at a time: those fall in
-// one or a few cells, so the per-key atomics aggregate.
-__device__ __forceinline__ bool sample_key(const PlanGeom &g, const double *uvw,
-                                           const double *freq, const double *scale,
-                                           const int32_t *chan_map, int64_t t, int64_t b,
-                                           int c, uint32_t &key, Rec &rec) {
-  const int64_t nb = g.nb;
-  const int64_t tb = t * nb + b;
-  const int64_t row = tb * g.nchan + c;
-  rec.row = (uint32_t)row;
-  rec.du = rec.dv = rec.ou = rec.ov = 0;
-  key = (uint32_t)g.n_keys();  // skipped samples
-  int plane = chan_map[c];
-  if (plane < 0 || plane >= g.n_planes) return false;
-  double um = uvw[3 * tb + 0], vm = uvw[3 * tb + 1];
+// Work units of the two passes: unit u = (baseline b, block of 32 time
+// steps), lane = time step inside the block.  A warp takes units u, u +
+// n_warps, ... and walks the unit's channels one after the other, so the
+// uvw row is read once per unit and the 32 lanes of one channel hold
+// consecutive time steps of one (baseline, channel) series: those fall in
+// one or a few cells, so the per-key atomics aggregate.  Walk order (the
+// index of the stored keys and records) is (b * nchan + c) * nt + t.  All
+// indices fit 32 bits (plan_build checks n_keys and n_rows).
+struct Unit {
+  uint32_t b, t;  // baseline, this lane's time step
+  bool in;        // t < nt
+};
+
+__device__ __forceinline__ Unit unit_of(uint32_t u, uint32_t ntb, uint32_t nt, int lane) {
+  Unit w;
+  w.b = u / ntb;
+  w.t = (u - w.b * ntb) * 32u + (uint32_t)lane;
+  w.in = w.t < nt;
+  return w;
+}
+
+// Key and record (row | du | dv << 8 | (ou + 128) << 16 | (ov + 128) << 24
+// in the second word, the byte layout of Rec) of one sample with uvw row
+// (um, vm), channel c on image plane `plane`; skipped samples get key n_keys
+// and a zero second word.
+__device__ __forceinline__ uint32_t sample_key(const PlanGeom &g, double um, double vm,
+                                               double us0, double us1, double f, int plane,
+                                               uint32_t row, uint2 &rec) {
+  rec = make_uint2(row, 0u);
+  const uint32_t skip = (uint32_t)g.n_keys();
+  if (plane < 0 || plane >= g.n_planes) return skip;
   int fu, fv, ou, ov;
-  bool ok;
-  if (g.convention == 0)
-    ok = sample_pos_grid(um, vm, scale[2 * c], scale[2 * c + 1], g.n_u, g.n_v, g.support, g.os,
-                         fu, fv, ou, ov);
-  else
-    ok = sample_pos_degrid(um, vm, freq[c], g, fu, fv, ou, ov);
-  if (!ok) return false;
-  int tu = fu / TILE, tv = fv / TILE;
-  int du = fu - tu * TILE, dv = fv - tv * TILE;
-  int64_t tile = ((int64_t)plane * g.ntu + tu) * g.ntv + tv;
-  int side_shift = 5 - g.res_shift;  // log2(TILE >> res_shift)
-  int64_t cell = ((int64_t)(du >> g.res_shift) << side_shift) + (dv >> g.res_shift);
-  key = (uint32_t)(tile * g.kpt + cell);
-  rec.du = (uint8_t)du;
-  rec.dv = (uint8_t)dv;
-  rec.ou = (uint8_t)(ou + 128);
-  rec.ov = (uint8_t)(ov + 128);
-  return true;
+  const bool ok = g.convention == 0
+                      ? sample_pos_grid(um, vm, us0, us1, g.n_u, g.n_v, g.support, g.os, fu, fv,
+                                        ou, ov)
+                      : sample_pos_degrid(um, vm, f, g, fu, fv, ou, ov);
+  if (!ok) return skip;
+  // fu, fv >= 0 here
+  const uint32_t tu = (uint32_t)fu / TILE, tv = (uint32_t)fv / TILE;
+  const uint32_t du = (uint32_t)fu - tu * TILE, dv = (uint32_t)fv - tv * TILE;
+  const uint32_t tile = ((uint32_t)plane * (uint32_t)g.ntu + tu) * (uint32_t)g.ntv + tv;
+  const int side_shift = 5 - g.res_shift;  // log2(TILE >> res_shift)
+  const uint32_t cell = ((du >> g.res_shift) << side_shift) + (dv >> g.res_shift);
+  rec.y = du | (dv << 8) | ((uint32_t)(ou + 128) << 16) | ((uint32_t)(ov + 128) << 24);
+  return tile * (uint32_t)g.kpt + cell;
 }
 
 // Warp aggregation of per-key atomics over runs of equal keys in lane order
@@ -67,66 +77,93 @@ __device__ __forceinline__ bool run_leader(uint32_t key, bool in, int lane, uint
   return lead;
 }
 
-// Pass 1: key and record of every sample, stored in walk order (sample
-// index series * nt + t), and the count per key (warp-aggregated).  Warp w
-// takes series w, w + n_warps, ... (series = b * nchan + c); the loops' trip
-// counts are the same on every lane of a warp.
-__global__ void __launch_bounds__(256) k_plan_count(PlanGeom g, const double *uvw,
-                                                    const double *freq, const double *scale,
-                                                    const int32_t *chan_map, uint32_t *hist,
-                                                    uint32_t *walk_key, Rec *walk_rec) {
+// Pass 1: key and record of every sample, stored in walk order, and the
+// count per key (warp-aggregated).  Loop trip counts are uniform per warp.
+__global__ void __launch_bounds__(256) k_plan_count(PlanGeom g, const double *__restrict__ uvw,
+                                                    const double *__restrict__ freq,
+                                                    const double *__restrict__ scale,
+                                                    const int32_t *__restrict__ chan_map,
+                                                    uint32_t *hist, uint32_t *walk_key,
+                                                    uint2 *walk_rec) {
   const int lane = threadIdx.x & 31;
-  const int64_t n_warps = ((int64_t)gridDim.x * blockDim.x) >> 5;
-  const int64_t n_series = g.nb * g.nchan;
-  for (int64_t sr = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5; sr < n_series;
-       sr += n_warps) {
-    const int64_t b = sr / g.nchan;
-    const int c = (int)(sr - b * g.nchan);
-    for (int64_t t0 = 0; t0 < g.nt; t0 += 32) {
-      const int64_t t = t0 + lane;
+  const uint32_t n_warps = (gridDim.x * blockDim.x) >> 5;
+  const uint32_t nt = (uint32_t)g.nt, nb = (uint32_t)g.nb, nchan = (uint32_t)g.nchan;
+  const uint32_t ntb = (nt + 31u) >> 5;
+  const uint32_t n_units = nb * ntb;
+  for (uint32_t u = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; u < n_units; u += n_warps) {
+    const Unit w = unit_of(u, ntb, nt, lane);
+    const uint32_t tb = w.t * nb + w.b;  // uvw row (meaningful when in)
+    double um = 0.0, vm = 0.0;
+    if (w.in) {
+      um = uvw[3 * (size_t)tb + 0];
+      vm = uvw[3 * (size_t)tb + 1];
+    }
+    uint32_t widx = w.b * nchan * nt + w.t;
+    for (uint32_t c = 0; c < nchan; ++c, widx += nt) {
+      const int plane = __ldg(chan_map + c);
+      const double us0 = __ldg(scale + 2 * c), us1 = __ldg(scale + 2 * c + 1);
+      const double f = __ldg(freq + c);
       uint32_t key = 0xffffffffu;
-      Rec rec;
-      const bool in = t < g.nt;
-      if (in) {
-        sample_key(g, uvw, freq, scale, chan_map, t, b, c, key, rec);
-        walk_key[sr * g.nt + t] = key;
-        walk_rec[sr * g.nt + t] = rec;
+      if (w.in) {
+        uint2 rec;
+        key = sample_key(g, um, vm, us0, us1, f, plane, tb * nchan + c, rec);
+        walk_key[widx] = key;
+        walk_rec[widx] = rec;
       }
       uint32_t len;
-      const bool lead = run_leader(key, in, lane, len);
+      const bool lead = run_leader(key, w.in, lane, len);
       if (lead) atomicAdd(&hist[key], len);
     }
   }
 }
 
-// Pass 2: scatter the stored records to their key ranges (the same walk, so
-// the same warp aggregation; no position arithmetic).
-__global__ void __launch_bounds__(256) k_plan_scatter(PlanGeom g, const uint32_t *walk_key,
-                                                      const Rec *walk_rec, uint32_t *cursor,
-                                                      Rec *recs) {
+// Pass 2: scatter the stored records to their key ranges (the same walk and
+// warp aggregation; no position arithmetic).  SC channels at a time, so that
+// many cursor atomics are in flight per warp before their records are stored.
+constexpr int SC = 4;
+
+__global__ void __launch_bounds__(256) k_plan_scatter(PlanGeom g,
+                                                      const uint32_t *__restrict__ walk_key,
+                                                      const uint2 *__restrict__ walk_rec,
+                                                      uint32_t *cursor, uint2 *recs) {
   const int lane = threadIdx.x & 31;
-  const int64_t n_warps = ((int64_t)gridDim.x * blockDim.x) >> 5;
-  const int64_t n_series = g.nb * g.nchan;
-  for (int64_t sr = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5; sr < n_series;
-       sr += n_warps) {
-    for (int64_t t0 = 0; t0 < g.nt; t0 += 32) {
-      const int64_t t = t0 + lane;
-      const bool in = t < g.nt;
-      uint32_t key = 0xffffffffu;
-      Rec rec;
-      if (in) {
-        key = walk_key[sr * g.nt + t];
-        rec = walk_rec[sr * g.nt + t];
+  const uint32_t n_warps = (gridDim.x * blockDim.x) >> 5;
+  const uint32_t nt = (uint32_t)g.nt, nb = (uint32_t)g.nb, nchan = (uint32_t)g.nchan;
+  const uint32_t ntb = (nt + 31u) >> 5;
+  const uint32_t n_units = nb * ntb;
+  const unsigned below = 0xffffffffu >> (31 - lane);  // lanes 0..lane
+  for (uint32_t u = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; u < n_units; u += n_warps) {
+    const Unit w = unit_of(u, ntb, nt, lane);
+    const uint32_t wbase = w.b * nchan * nt + w.t;
+    for (uint32_t c0 = 0; c0 < nchan; c0 += SC) {
+      uint32_t key[SC], pos[SC];
+      uint2 rec[SC];
+      bool in[SC], lead[SC];
+#pragma unroll
+      for (int k = 0; k < SC; ++k) {
+        in[k] = w.in && c0 + k < nchan;
+        key[k] = 0xffffffffu;
+        if (in[k]) {
+          const uint32_t widx = wbase + (c0 + k) * nt;
+          key[k] = walk_key[widx];
+          rec[k] = walk_rec[widx];
+        }
       }
-      uint32_t len;
-      const bool lead = run_leader(key, in, lane, len);
-      uint32_t pos = 0;
-      if (lead) pos = atomicAdd(&cursor[key], len);
-      // each lane's run leader: the highest leader at or below it
-      const unsigned leaders = __ballot_sync(0xffffffffu, lead);
-      const int ll = 31 - __clz(leaders & (0xffffffffu >> (31 - lane)));
-      pos = __shfl_sync(0xffffffffu, pos, ll) + (uint32_t)(lane - ll);
-      if (in) recs[pos] = rec;
+#pragma unroll
+      for (int k = 0; k < SC; ++k) {
+        uint32_t len;
+        lead[k] = run_leader(key[k], in[k], lane, len);
+        pos[k] = 0;
+        if (lead[k]) pos[k] = atomicAdd(&cursor[key[k]], len);
+      }
+#pragma unroll
+      for (int k = 0; k < SC; ++k) {
+        // each lane's run leader: the highest leader at or below it
+        const unsigned leaders = __ballot_sync(0xffffffffu, lead[k]);
+        const int ll = 31 - __clz(leaders & below);
+        const uint32_t p = __shfl_sync(0xffffffffu, pos[k], ll & 31) + (uint32_t)(lane - ll);
+        if (in[k]) recs[p] = rec[k];
+      }
     }
   }
 }
@@ -282,20 +319,20 @@ int plan_build(const PlanGeom &g, Plan &p, const double *uvw, const double *freq
     AV_LAUNCH_CHECK();
   }
   int sms = sm_count();
-  // one warp per (baseline, channel) series, 8 warps per block
-  int64_t blocks = (g.nb * g.nchan + 7) / 8;
+  // one warp per (baseline, 32 time steps) unit, 8 warps per block
+  int64_t blocks = (g.nb * ((g.nt + 31) / 32) + 7) / 8;
   if (blocks > (int64_t)sms * 16) blocks = (int64_t)sms * 16;
   if (blocks < 1) blocks = 1;
   if (g.n_rows > 0) {
     k_plan_count<<<(unsigned)blocks, 256, 0, st>>>(g, uvw, freq, p.scale, chan_map, p.cursor,
-                                                  p.walk_key, p.walk_rec);
+                                                  p.walk_key, (uint2 *)p.walk_rec);
     AV_LAUNCH_CHECK();
   }
   int rc = scan_counts(p.cursor, p.offs, nk + 1, p.scan_tmp, st);
   if (rc) return rc;
   if (g.n_rows > 0) {
-    k_plan_scatter<<<(unsigned)blocks, 256, 0, st>>>(g, p.walk_key, p.walk_rec, p.cursor,
-                                                    p.recs);
+    k_plan_scatter<<<(unsigned)blocks, 256, 0, st>>>(g, p.walk_key, (const uint2 *)p.walk_rec,
+                                                    p.cursor, (uint2 *)p.recs);
     AV_LAUNCH_CHECK();
   }
   int64_t nt = g.n_tiles() + 1;
