@@ -513,3 +513,88 @@ class HogbomRun:
               "av_hogbom_state_read")
         return dict(iter=oi[0], px=oi[1], py=oi[2], stopped=oi[3], err=oi[4], peak=od[0],
                     absval=od[1])
+
+
+# ------------------------------------------------------------------ imager --
+def pol_transform(x, matrix, pol_axis, out_dtype):
+    """out[..., o, ...] = sum_i matrix[o, i] x[..., i, ...] along pol_axis
+    (av_pol_transform); matrix (n_out, n_in) complex, out_dtype a torch
+    dtype (real output keeps the real part)."""
+    t = on_device(x)
+    if t.dtype not in (torch.float32, torch.float64, torch.complex64, torch.complex128):
+        t = t.to(torch.float64)
+    m = np.asarray(matrix, dtype=np.complex128)
+    n_out, n_in = m.shape
+    ax = pol_axis % t.ndim
+    if int(t.shape[ax]) != n_in:
+        raise ValueError(f"polarisation axis has {int(t.shape[ax])} entries, matrix takes {n_in}")
+    n_outer = int(np.prod(t.shape[:ax], dtype=np.int64))
+    n_pix = int(np.prod(t.shape[ax + 1:], dtype=np.int64))
+    shape = list(t.shape)
+    shape[ax] = n_out
+    out = torch.empty(shape, dtype=out_dtype, device=t.device)
+    flat = np.ascontiguousarray(np.stack([m.real, m.imag], axis=-1).reshape(-1))
+    check(lib().av_pol_transform(p(t), dcode(t), p(out), dcode(out),
+                                 flat.ctypes.data, n_in, n_out, n_outer,
+                                 n_pix, stream_ptr()), "av_pol_transform")
+    return out
+
+
+def argmax(x, mode):
+    """(index, value) of np.argmax(np.abs(x)) (mode 0) / np.argmax(x) (mode 1)
+    over the flattened x; value is x at that index.  Synchronises."""
+    t = on_device(x)
+    if t.dtype not in (torch.float32, torch.float64):
+        t = t.to(torch.float64)
+    n = t.numel()
+    res = torch.empty(2, dtype=torch.float64, device=t.device)
+    idx = torch.empty(1, dtype=torch.int64, device=t.device)
+    _buf, wptr, wbytes = workspace(lib().av_argmax_workspace_size(n))
+    check(lib().av_argmax(p(t), dcode(t), n, int(mode), p(idx), p(res), wptr, wbytes,
+                          stream_ptr()), "av_argmax")
+    return int(idx.item()), float(res[0].item())
+
+
+def psf_sidelobe(psf, window=(41, 41), threshold=0.35):
+    """max_sidelobe of extract_main_lobe(window, threshold, psf plane)."""
+    t = on_device(psf)
+    if t.dtype not in (torch.float32, torch.float64):
+        t = t.to(torch.float64)
+    ny, nx = int(t.shape[-2]), int(t.shape[-1])
+    if t.numel() != ny * nx:
+        raise ValueError("psf_sidelobe takes one (ny, nx) plane")
+    out = torch.empty(2, dtype=torch.float64, device=t.device)
+    w0, w1 = int(window[0]), int(window[1])
+    _buf, wptr, wbytes = workspace(lib().av_psf_sidelobe_workspace_size(ny, nx, w0, w1))
+    check(lib().av_psf_sidelobe(p(t), dcode(t), ny, nx, w0, w1, float(threshold), p(out), wptr,
+                                wbytes, stream_ptr()), "av_psf_sidelobe")
+    r = out.cpu().numpy()
+    if r[1] != 0:
+        raise ValueError("PSF peak x threshold is negative: the main lobe is undefined")
+    return float(r[0])
+
+
+def plane_sum(x):
+    """FP64 sums of each (..., ny, nx) plane of x, as a device tensor of the
+    leading shape."""
+    t = on_device(x)
+    if t.dtype not in (torch.float32, torch.float64):
+        t = t.to(torch.float64)
+    ny, nx = int(t.shape[-2]), int(t.shape[-1])
+    npl = int(t.numel() // max(1, ny * nx))
+    out = torch.empty(tuple(t.shape[:-2]), dtype=torch.float64, device=t.device)
+    _buf, wptr, wbytes = workspace(lib().av_plane_sum_workspace_size(npl, ny * nx))
+    check(lib().av_plane_sum(p(t), dcode(t), npl, ny * nx, p(out), wptr, wbytes, stream_ptr()),
+          "av_plane_sum")
+    return out
+
+
+def vis_residual(vis, model, out=None):
+    """vis - model (complex64 / complex128 device tensors of one shape)."""
+    v = on_device(vis)
+    m = on_device(model, v.dtype)
+    if out is None:
+        out = torch.empty_like(v)
+    check(lib().av_vis_residual(p(v), p(m), p(out), dcode(v), v.numel(), stream_ptr()),
+          "av_vis_residual")
+    return out

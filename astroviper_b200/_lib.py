@@ -79,6 +79,14 @@ SIGNATURES = {
     "av_hogbom_state_read": (_i, [_vp, _vp, _vp, _vp]),
     "av_abs_sum_workspace_size": (_sz, [_i64, _i]),
     "av_abs_sum_ordered": (_i, [_vp, _i, _i64, _vp, _vp, _sz, _vp]),
+    "av_pol_transform": (_i, [_vp, _i, _vp, _i, _vp, _i, _i, _i64, _i64, _vp]),
+    "av_argmax_workspace_size": (_sz, [_i64]),
+    "av_argmax": (_i, [_vp, _i, _i64, _i, _vp, _vp, _vp, _sz, _vp]),
+    "av_psf_sidelobe_workspace_size": (_sz, [_i64, _i64, _i, _i]),
+    "av_psf_sidelobe": (_i, [_vp, _i, _i64, _i64, _i, _i, _d, _vp, _vp, _sz, _vp]),
+    "av_plane_sum_workspace_size": (_sz, [_i64, _i64]),
+    "av_plane_sum": (_i, [_vp, _i, _i64, _i64, _vp, _vp, _sz, _vp]),
+    "av_vis_residual": (_i, [_vp, _vp, _vp, _i, _i64, _vp]),
 }
 
 _LIB = None

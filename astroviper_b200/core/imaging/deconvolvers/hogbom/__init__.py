@@ -19,8 +19,26 @@ from ..... import _kernels as K
 __all__ = ["maximg", "clean", "clean_nc", "get_dtype_name", "is_float32", "is_float64"]
 
 
+_TORCH_OF = {np.float32: torch.float32, np.float64: torch.float64}
+
+
 def _is_dtype(a, dt):
+    if isinstance(a, torch.Tensor):
+        return a.dtype == _TORCH_OF[dt]
     return isinstance(a, np.ndarray) and a.dtype == dt
+
+
+def _size(a):
+    return a.numel() if isinstance(a, torch.Tensor) else np.asarray(a).size
+
+
+def _t(a):
+    """Device tensor of a converted array (numpy arrays are staged)."""
+    return a if isinstance(a, torch.Tensor) else torch.from_numpy(a)
+
+
+def _out(t, on_device):
+    return t if on_device else t.cpu().numpy()
 
 
 def _pick_dtype(*arrays):
@@ -33,6 +51,8 @@ def _pick_dtype(*arrays):
 
 
 def _as(a, dt):
+    if isinstance(a, torch.Tensor):
+        return a.to(device=K.device(), dtype=_TORCH_OF[dt]).contiguous()
     return np.ascontiguousarray(np.asarray(a), dtype=dt)
 
 
@@ -44,13 +64,13 @@ def maximg(image, mask=None):
     if img.ndim != 2:
         raise RuntimeError("Image must be 2D array")
     m = None
-    if mask is not None and np.asarray(mask).size > 0:
+    if mask is not None and _size(mask) > 0:
         m = _as(mask, dt)
         if m.ndim != 2:
             raise RuntimeError("Mask must be 2D array")
-        if m.shape != img.shape:
+        if tuple(m.shape) != tuple(img.shape):
             raise RuntimeError("Mask dimensions must match image spatial dimensions")
-    out = K.maximg(torch.from_numpy(img), None if m is None else torch.from_numpy(m))
+    out = K.maximg(_t(img), None if m is None else _t(m))
     o = out.cpu().numpy()
     return (float(o[0]), float(o[1]))
 
@@ -82,8 +102,11 @@ def clean(dirty_image, psf, mask=None, clean_box=(-1, -1, -1, -1), max_iter=100,
     Returns {model_image, residual_image, iterations_performed, final_peak,
     total_flux_cleaned, converged}.  With large_psf=True a PSF larger than
     the image is accepted (centre at its (ny/2, nx/2)); the reference requires
-    equal shapes."""
-    m_given = mask if (mask is not None and np.asarray(mask).size > 0) else None
+    equal shapes.  torch tensors are accepted too (same dtype rule, torch
+    float32 / float64 in place of numpy's); the model and residual then stay
+    on the device."""
+    on_device = isinstance(dirty_image, torch.Tensor)
+    m_given = mask if (mask is not None and _size(mask) > 0) else None
     dt = _pick_dtype(dirty_image, psf, mask)
     d = _as(dirty_image, dt)
     p = _as(psf, dt)
@@ -95,19 +118,18 @@ def clean(dirty_image, psf, mask=None, clean_box=(-1, -1, -1, -1), max_iter=100,
     if large_psf:
         if p.shape[0] < ny or p.shape[1] < nx:
             raise RuntimeError("PSF must be at least as large as the image")
-    elif p.shape != d.shape:
+    elif tuple(p.shape) != tuple(d.shape):
         raise RuntimeError("PSF dimensions must match image spatial dimensions")
     m = None
     if m_given is not None:
         m = _as(m_given, dt)
-        if m.ndim != 2 or m.shape != d.shape:
+        if m.ndim != 2 or tuple(m.shape) != tuple(d.shape):
             raise RuntimeError("Mask must be 2D with same spatial dimensions as image")
     box = _box(tuple(clean_box), nx, ny)
     tdt = np.dtype(dt).type
     niter, siter = int(max_iter), int(start_iter)
     gain_t, thres_t, speed_t = tdt(gain), tdt(threshold), tdt(speedup)
-    run = K.HogbomRun(torch.from_numpy(d), torch.from_numpy(p),
-                      mask=None if m is None else torch.from_numpy(m), box=box, niter=niter,
+    run = K.HogbomRun(_t(d), _t(p), mask=None if m is None else _t(m), box=box, niter=niter,
                       siter=siter, gain=float(gain_t), threshold=float(thres_t),
                       speedup=float(speed_t))
     callbacks = progress_callback is not None or stop_callback is not None
@@ -156,8 +178,8 @@ def clean(dirty_image, psf, mask=None, clean_box=(-1, -1, -1, -1), max_iter=100,
     final_peak = max(abs(mm[0]), abs(mm[1]))
     total = K.abs_sum_ordered(run.model).cpu().numpy()[0]
     return {
-        "model_image": run.model.cpu().numpy(),
-        "residual_image": run.resid.cpu().numpy(),
+        "model_image": _out(run.model, on_device),
+        "residual_image": _out(run.resid, on_device),
         "iterations_performed": int(final_iter),
         "final_peak": float(final_peak),
         "total_flux_cleaned": float(total),

@@ -347,6 +347,53 @@ size_t av_abs_sum_workspace_size(int64_t n, int dtype);
 int av_abs_sum_ordered(const void *model, int dtype, int64_t n, void *out, void *workspace,
                        size_t workspace_bytes, void *stream);
 
+/* ------------------------------------------------- major/minor-cycle imager -- */
+/* corr_to_stokes / stokes_to_corr (corr_to_stokes.py:71-138) as used by
+ * image_corr_to_stokes and image_stokes_to_corr (:141-305, :307-487):
+ * out[k, o, p] = sum_i M[o][i] in[k, i, p] for in (n_outer, n_in, n_pix) and
+ * out (n_outer, n_out, n_pix); matrix is the complex n_out x n_in matrix M,
+ * row-major, as (re, im) pairs in host memory.  Element types AV_F32 / AV_F64
+ * / AV_C64 / AV_C128; a real output keeps the real part (the .real of
+ * image_corr_to_stokes for real images).  Terms with a zero coefficient are
+ * left out and nothing is fused, so the reference's tables give numpy's
+ * results exactly. */
+int av_pol_transform(const void *in, int in_dtype, void *out, int out_dtype,
+                     const double *matrix, int n_in, int n_out, int64_t n_outer, int64_t n_pix,
+                     void *stream);
+
+/* np.argmax(np.abs(x)) (mode 0) or np.argmax(x) (mode 1) over n values
+ * (AV_F32 / AV_F64): first index of the maximum, NaN above every number.
+ * Device outputs: *out_index, and *out_value = x at that index (signed), the
+ * value image_peak_residual returns (image_statistics.py:83-86). */
+size_t av_argmax_workspace_size(int64_t n);
+int av_argmax(const void *x, int dtype, int64_t n, int mode, int64_t *out_index,
+              double *out_value, void *workspace, size_t workspace_bytes, void *stream);
+
+/* max_sidelobe of extract_main_lobe(npix_window = (win0, win1), threshold,
+ * psf) (psf_gaussian_fit.py:46-126) for one (ny, nx) PSF plane: the main lobe
+ * is the 4-connected set of pixels above threshold x peak, inside the window
+ * around the PSF peak, that holds the window maximum; the result is the
+ * maximum over the plane with the main lobe counted as 0.  out (device, 2
+ * doubles): out[0] = max_sidelobe, out[1] = 0, or out[0] = NaN and out[1] = 1
+ * for a negative threshold x peak (the reference would label the whole image
+ * outside the window).  Windows up to 16384 pixels. */
+size_t av_psf_sidelobe_workspace_size(int64_t ny, int64_t nx, int win0, int win1);
+int av_psf_sidelobe(const void *psf, int dtype, int64_t ny, int64_t nx, int win0, int win1,
+                    double threshold, double *out, void *workspace, size_t workspace_bytes,
+                    void *stream);
+
+/* Per-plane sums in FP64 of x (n_planes, n_pix), AV_F32 / AV_F64: the model
+ * flux of deconvolve (deconvolution.py:262, np.sum of a plane); out (device)
+ * n_planes doubles.  Up to 65535 planes. */
+size_t av_plane_sum_workspace_size(int64_t n_planes, int64_t n_pix);
+int av_plane_sum(const void *x, int dtype, int64_t n_planes, int64_t n_pix, double *out,
+                 void *workspace, size_t workspace_bytes, void *stream);
+
+/* compute_residual_visibilities (imager.py:82-85): out = vis - model over n
+ * complex values (AV_C64 / AV_C128); out may alias vis or model. */
+int av_vis_residual(const void *vis, const void *model, void *out, int dtype, int64_t n,
+                    void *stream);
+
 #ifdef __cplusplus
 }
 #endif
