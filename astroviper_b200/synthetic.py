@@ -253,3 +253,58 @@ def clean_workload(nx=2048, psf_factor=2, n_src=50, seed=20260103, n_time=50):
         xa, xb = max(0, -x0), min(nx, pn - x0)
         dirty[ya:yb, xa:xb] += flux[k] * psf[y0 + ya:y0 + yb, x0 + xa:x0 + xb].astype(np.float64)
     return dict(dirty=dirty.astype(np.float32), psf=psf, flux=flux, xs=xs, ys=ys)
+
+
+class _Column:
+    def __init__(self, values, dims):
+        self.values = values
+        self.data = values
+        self.dims = tuple(dims)
+        self.coords = {}
+
+    def __len__(self):
+        return len(self.values)
+
+
+class Ms4Node:
+    """A measurement-set node shaped like an xradio MSv4 DataTree node as
+    far as the imaging path reads one: VISIBILITY / UVW / WEIGHT / FLAG
+    columns with .data / .values / .dims, the frequency / polarization / time
+    coordinates, dims and the phase_center attribute; columns can be added
+    (VISIBILITY_MODEL, RESIDUAL)."""
+
+    def __init__(self, vis, uvw, weight, flag, freq, pols, phase_center=(0.0, 0.0), dt_s=10.0):
+        self._d = {}
+        vdims = ("time", "baseline_id", "frequency", "polarization")
+        self["VISIBILITY"] = _Column(vis, vdims)
+        self["UVW"] = _Column(uvw, ("time", "baseline_id", "uvw_label"))
+        self["WEIGHT"] = _Column(weight, vdims)
+        self["FLAG"] = _Column(flag, vdims)
+        self.frequency = _Column(np.asarray(freq), ("frequency",))
+        self.coords = {"frequency": _Column(np.asarray(freq), ("frequency",)),
+                       "polarization": _Column(np.asarray(pols), ("polarization",)),
+                       "time": _Column(np.arange(vis.shape[0]) * dt_s, ("time",))}
+        nt, nb, nc, npol = vis.shape
+        self.dims = {"time": nt, "baseline_id": nb, "frequency": nc, "polarization": npol}
+        self.attrs = {"phase_center": tuple(phase_center)}
+
+    def __getitem__(self, k):
+        return self._d[k]
+
+    def __setitem__(self, k, v):
+        self._d[k] = v
+        setattr(self, k, v)
+
+    def __contains__(self, k):
+        return k in self._d
+
+
+def ms4_small(seed=20260101, n_time=50):
+    """workload_small as an Ms4Node (XX, YY) and its imaging parameters
+    (512^2, 2 arcsec cells, support 7, oversampling 100)."""
+    W = workload_small(seed=seed, n_time=n_time)
+    node = Ms4Node(W["vis"].copy(), W["uvw"].copy(), W["weight"].copy(), W["flag"].copy(),
+                   W["freq"], ["XX", "YY"])
+    cell = np.abs(W["pixelincr"])
+    return node, {"image_size": (512, 512), "cell_size": (float(cell[0]), float(cell[1])),
+                  "support": 7, "oversampling": 100}
