@@ -598,3 +598,67 @@ def vis_residual(vis, model, out=None):
     check(lib().av_vis_residual(p(v), p(m), p(out), dcode(v), v.numel(), stream_ptr()),
           "av_vis_residual")
     return out
+
+
+# ------------------------------------------------------------------ mosaic --
+def cf_phase_product(conv_kernel, phase_gradient):
+    """conv_kernel (..., cu, cv) x phase_gradient (cu, cv): complex128."""
+    k = on_device(conv_kernel)
+    if k.dtype not in (torch.float64, torch.complex128):
+        k = k.to(torch.complex128 if k.is_complex() else torch.float64)
+    pg = on_device(phase_gradient, torch.complex128)
+    cu, cv = int(k.shape[-2]), int(k.shape[-1])
+    if tuple(pg.shape) != (cu, cv):
+        raise ValueError(f"phase gradient {tuple(pg.shape)} does not match the kernel's "
+                         f"({cu}, {cv})")
+    out = torch.empty(k.shape, dtype=torch.complex128, device=k.device)
+    n_cf = int(k.numel() // (cu * cv))
+    check(lib().av_cf_phase_product(p(k), dcode(k), p(pg), p(out), n_cf, cu, cv, stream_ptr()),
+          "av_cf_phase_product")
+    return out
+
+
+def mosaic_grid(grid, sum_weight, do_psf, vis, weight, uvw, freq, chan_map, pol_map, cfb_map,
+                cfc_map, cfp_map, cf, support, n_uv, delta_lm, oversampling, aperture=False):
+    """av_mosaic_grid / av_aperture_grid into the device arrays grid
+    (complex128) and sum_weight (float64)."""
+    w = on_device(weight, torch.float64)
+    nt, nb, nchan, npol = (int(s) for s in w.shape)
+    v = None if (do_psf or aperture) else on_device(vis, torch.complex128)
+    uvw_d = on_device(uvw, torch.float64)
+    freq_d = on_device(freq, torch.float64)
+    maps = [on_device(np.asarray(m), torch.int32) for m in
+            (chan_map, pol_map, cfb_map, cfc_map, cfp_map)]
+    sup = on_device(np.asarray(support), torch.int32)
+    n_cfb, n_cfc, n_cfp, cu, cv = (int(s) for s in cf.shape)
+    os_u, os_v = (int(oversampling[0]), int(oversampling[1])) if np.ndim(oversampling) else \
+        (int(oversampling), int(oversampling))
+    max_sup = int(np.max(np.asarray(support)))
+    args = [p(grid), p(sum_weight), int(bool(do_psf)), p(v), p(w), p(uvw_d), p(freq_d)] + \
+        [p(m) for m in maps] + [p(cf), n_cfb, n_cfc, n_cfp, cu, cv, p(sup), max_sup,
+                                int(n_uv[0]), int(n_uv[1]), float(delta_lm[0]),
+                                float(delta_lm[1]), os_u, os_v, nt, nb, nchan, npol,
+                                int(grid.shape[0]), int(grid.shape[1])]
+    if aperture:
+        _buf, wptr, wbytes = workspace(lib().av_aperture_grid_workspace_size(n_cfb, nchan, npol))
+        check(lib().av_aperture_grid(*args, wptr, wbytes, stream_ptr()), "av_aperture_grid")
+    else:
+        check(lib().av_mosaic_grid(*args, stream_ptr()), "av_mosaic_grid")
+    return grid, sum_weight
+
+
+def airy_pattern(freq, n_pol, dish, blockage, image_size, image_center, cell, ipower, casa,
+                 rorder):
+    """Primary-beam patterns of make_pb_symmetric (device float64)."""
+    f = on_device(np.atleast_1d(np.asarray(freq, dtype=np.float64)), torch.float64)
+    dish = np.ascontiguousarray(np.asarray(dish, dtype=np.float64).ravel())
+    blk = np.ascontiguousarray(np.asarray(blockage, dtype=np.float64).ravel())
+    nd, nf = len(dish), int(f.numel())
+    nx, ny = int(image_size[0]), int(image_size[1])
+    shape = (nd, nf, int(n_pol), nx, ny) if rorder else (nx, ny, nf, int(n_pol), nd)
+    out = torch.empty(shape, dtype=torch.float64, device=f.device)
+    check(lib().av_airy_pattern(p(out), dish.ctypes.data, blk.ctypes.data, nd, p(f), nf,
+                                int(n_pol), nx, ny, int(image_center[0]), int(image_center[1]),
+                                float(cell[0]), float(cell[1]), int(ipower), int(bool(casa)),
+                                int(bool(rorder)), stream_ptr()), "av_airy_pattern")
+    return out

@@ -21,6 +21,10 @@ _i64 = ctypes.c_int64
 _d = ctypes.c_double
 _sz = ctypes.c_size_t
 
+# the common arguments of av_mosaic_grid and av_aperture_grid
+_MOSAIC = [_vp, _vp, _i, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _i64, _i64, _i64,
+           _i64, _i64, _vp, _i, _i64, _i64, _d, _d, _i, _i, _i64, _i64, _i64, _i64, _i64, _i64]
+
 # name: (restype, [argtypes])
 SIGNATURES = {
     "av_version": (_i, []),
@@ -87,6 +91,12 @@ SIGNATURES = {
     "av_plane_sum_workspace_size": (_sz, [_i64, _i64]),
     "av_plane_sum": (_i, [_vp, _i, _i64, _i64, _vp, _vp, _sz, _vp]),
     "av_vis_residual": (_i, [_vp, _vp, _vp, _i, _i64, _vp]),
+    "av_cf_phase_product": (_i, [_vp, _i, _vp, _vp, _i64, _i64, _i64, _vp]),
+    "av_airy_pattern": (_i, [_vp, _vp, _vp, _i64, _vp, _i64, _i64, _i64, _i64, _i64, _i64, _d,
+                             _d, _i, _i, _i, _vp]),
+    "av_mosaic_grid": (_i, _MOSAIC + [_vp]),
+    "av_aperture_grid_workspace_size": (_sz, [_i64, _i64, _i64]),
+    "av_aperture_grid": (_i, _MOSAIC + [_vp, _sz, _vp]),
 }
 
 _LIB = None

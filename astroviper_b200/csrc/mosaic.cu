@@ -1,0 +1,461 @@
+// Mosaic / A-projection gridding with general convolution functions
+// (mosaic_grid.py): each sample's footprint is a window of a 2-D complex
+// convolution function chosen by (baseline, channel, polarisation) maps,
+// premultiplied by the field's phase gradient.
+//
+// av_mosaic_grid      mosaic_grid_jit (mosaic_grid.py:307-486): one warp per
+//                     (time, baseline, channel) sample, lanes over the
+//                     support window, FP64 atomics into the grid; the
+//                     window's norm is reduced in the warp for sum_weight.
+// av_aperture_grid    aperture_grid_jit (mosaic_grid.py:13-153): every
+//                     sample adds its function at the grid centre, so the
+//                     weights are first summed per (function baseline,
+//                     channel, polarisation) class and each class then adds
+//                     its function once.
+// av_cf_phase_product conv_kernel x phase_gradient[0] (mosaic_grid.py:384,
+//                     :56-58), elementwise without fused multiply-add.
+#include "common.cuh"
+
+namespace av {
+
+struct MosaicArgs {
+  double2 *grid;
+  double *sumw;
+  int do_psf;
+  const double2 *vis;      // (nt, nb, nchan, npol), NULL for do_psf
+  const double *wt;        // (nt, nb, nchan, npol)
+  const double *uvw, *freq;
+  const int32_t *chan_map, *pol_map, *cfb_map, *cfc_map, *cfp_map;
+  const double2 *cf;       // (n_cfb, n_cfc, n_cfp, cu, cv), phase gradient applied
+  int64_t n_cfb, n_cfc, n_cfp, cu, cv;
+  const int32_t *support;  // (n_cfb, n_cfc, n_cfp, 2)
+  int max_support;         // np.max(weight_support)
+  int64_t n_u, n_v;
+  double dl0, dl1;
+  int os_u, os_v;
+  int64_t nt, nb, nchan, npol, n_img_chan, n_img_pol;
+};
+
+__device__ __forceinline__ double2 cmul(double2 a, double2 b) {
+  return make_double2(__dsub_rn(__dmul_rn(a.x, b.x), __dmul_rn(a.y, b.y)),
+                      __dadd_rn(__dmul_rn(a.x, b.y), __dmul_rn(a.y, b.x)));
+}
+
+// Position of a sample (mosaic_grid.py:384-405): centre cell and the offset
+// index into the function; false when off the grid or NaN.
+__device__ __forceinline__ bool mosaic_pos(const MosaicArgs &a, int64_t tb, int64_t c,
+                                           long long &uc, long long &vc, long long &uo,
+                                           long long &vo) {
+  const double f = a.freq[c];
+  const double s0 = __ddiv_rn(-__dmul_rn(__dmul_rn(f, a.dl0), (double)a.n_u), C_LIGHT);
+  const double s1 = __ddiv_rn(-__dmul_rn(__dmul_rn(f, a.dl1), (double)a.n_v), C_LIGHT);
+  const double u = __dmul_rn(a.uvw[3 * tb], s0), v = __dmul_rn(a.uvw[3 * tb + 1], s1);
+  if (isnan(u) || isnan(v)) return false;
+  const double up = __dadd_rn(u, (double)(a.n_u / 2)), vp = __dadd_rn(v, (double)(a.n_v / 2));
+  uc = trunc_ll(__dadd_rn(up, 0.5));
+  vc = trunc_ll(__dadd_rn(vp, 0.5));
+  const long long ms = a.max_support;
+  if (!(uc + ms < a.n_u && vc + ms < a.n_v && uc - ms >= 0 && vc - ms >= 0)) return false;
+  uo = (long long)floor(__dadd_rn(__dmul_rn(__dsub_rn((double)uc, up), (double)a.os_u), 0.5)) +
+       a.cu / 2;
+  vo = (long long)floor(__dadd_rn(__dmul_rn(__dsub_rn((double)vc, vp), (double)a.os_v), 0.5)) +
+       a.cv / 2;
+  return true;
+}
+
+constexpr int MG_THREADS = 256;
+
+__global__ void __launch_bounds__(MG_THREADS) k_mosaic_grid(MosaicArgs a) {
+  const int lane = threadIdx.x & 31;
+  const int64_t n_warps = ((int64_t)gridDim.x * blockDim.x) >> 5;
+  const int64_t n_rows = a.nt * a.nb * a.nchan;
+  for (int64_t row = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5; row < n_rows;
+       row += n_warps) {
+    const int64_t tb = row / a.nchan;
+    const int64_t c = row - tb * a.nchan;
+    const int64_t b = tb % a.nb;
+    long long uc, vc, uo, vo;
+    if (!mosaic_pos(a, tb, c, uc, vc, uo, vo)) continue;
+    const int cfb = a.cfb_map[b], cfc = a.cfc_map[c], ach = a.chan_map[c];
+    if (ach < 0 || ach >= a.n_img_chan || cfb < 0 || cfb >= a.n_cfb || cfc < 0 ||
+        cfc >= a.n_cfc)
+      continue;
+    for (int64_t p = 0; p < a.npol; ++p) {
+      const int64_t k = row * a.npol + p;
+      const double w = a.wt[k];
+      double2 wd;
+      if (a.do_psf) wd = make_double2(w, 0.0);
+      else {
+        const double2 vv = a.vis[k];
+        wd = make_double2(__dmul_rn(vv.x, w), __dmul_rn(vv.y, w));
+      }
+      if (isnan(wd.x) || isnan(wd.y) || (wd.x == 0.0 && wd.y == 0.0)) continue;
+      const int cfp = a.cfp_map[p], apol = a.pol_map[p];
+      if (cfp < 0 || cfp >= a.n_cfp || apol < 0 || apol >= a.n_img_pol) continue;
+      const int64_t fidx = ((int64_t)cfb * a.n_cfc + cfc) * a.n_cfp + cfp;
+      const int su = a.support[2 * fidx], sv = a.support[2 * fidx + 1];
+      const int su0 = -(su / 2), sv0 = -(sv / 2);
+      const double2 *f = a.cf + fidx * a.cu * a.cv;
+      double2 *g = a.grid + ((int64_t)ach * a.n_img_pol + apol) * a.n_u * a.n_v;
+      double2 norm = make_double2(0.0, 0.0);
+      const int n_tap = su * sv;
+      for (int t0 = 0; t0 < n_tap; t0 += 32) {
+        const int t = t0 + lane;
+        if (t >= n_tap) continue;
+        const int iv = sv0 + t / su, iu = su0 + t % su;  // v outer, u inner
+        const long long fu = (long long)a.os_u * iu + uo, fv = (long long)a.os_v * iv + vo;
+        // a window reaching past the function (the reference reads beyond it)
+        if (fu < 0 || fu >= a.cu || fv < 0 || fv >= a.cv) continue;
+        const double2 conv = f[fu * a.cv + fv];
+        const double2 x = cmul(conv, wd);
+        double2 *cell = g + (uc + iu) * a.n_v + (vc + iv);
+        atomicAdd(&cell->x, x.x);
+        atomicAdd(&cell->y, x.y);
+        norm.x += conv.x;
+        norm.y += conv.y;
+      }
+      for (int off = 16; off > 0; off >>= 1) {
+        norm.x += __shfl_down_sync(0xffffffffu, norm.x, off);
+        norm.y += __shfl_down_sync(0xffffffffu, norm.y, off);
+      }
+      if (lane == 0 && a.sumw) {
+        // do_psf: w Re(norm); else w Re(norm^2) (the function enters twice)
+        const double re = a.do_psf ? norm.x
+                                   : __dsub_rn(__dmul_rn(norm.x, norm.x), __dmul_rn(norm.y, norm.y));
+        atomicAdd(&a.sumw[(int64_t)ach * a.n_img_pol + apol], __dmul_rn(w, re));
+      }
+    }
+  }
+}
+
+// aperture_grid_jit, pass 1: weight sums per (function baseline, channel,
+// polarisation) class over the samples that pass the grid bounds.
+__global__ void __launch_bounds__(MG_THREADS) k_aperture_classes(MosaicArgs a, double *cls) {
+  const int64_t n_rows = a.nt * a.nb * a.nchan;
+  for (int64_t row = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; row < n_rows;
+       row += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t tb = row / a.nchan;
+    const int64_t c = row - tb * a.nchan;
+    const int64_t b = tb % a.nb;
+    long long uc, vc, uo, vo;
+    if (!mosaic_pos(a, tb, c, uc, vc, uo, vo)) continue;
+    const int cfb = a.cfb_map[b];
+    if (cfb < 0 || cfb >= a.n_cfb) continue;
+    for (int64_t p = 0; p < a.npol; ++p) {
+      const double w = a.wt[row * a.npol + p];
+      if (isnan(w) || w == 0.0) continue;
+      atomicAdd(&cls[((int64_t)cfb * a.nchan + c) * a.npol + p], w);
+    }
+  }
+}
+
+// pass 2: one block per class adds w_class x function window at the grid
+// centre and w_class x Re(norm) to sum_weight.
+__global__ void __launch_bounds__(MG_THREADS) k_aperture_add(MosaicArgs a, const double *cls) {
+  const int64_t cl = blockIdx.x;
+  const double w = cls[cl];
+  if (w == 0.0) return;
+  const int64_t p = cl % a.npol;
+  const int64_t c = (cl / a.npol) % a.nchan;
+  const int64_t cfb = cl / (a.npol * a.nchan);
+  const int cfc = a.cfc_map[c], cfp = a.cfp_map[p], ach = a.chan_map[c], apol = a.pol_map[p];
+  if (cfc < 0 || cfc >= a.n_cfc || cfp < 0 || cfp >= a.n_cfp || ach < 0 ||
+      ach >= a.n_img_chan || apol < 0 || apol >= a.n_img_pol)
+    return;
+  const int64_t fidx = (cfb * a.n_cfc + cfc) * a.n_cfp + cfp;
+  const int su = a.support[2 * fidx], sv = a.support[2 * fidx + 1];
+  const int su0 = -(su / 2), sv0 = -(sv / 2);
+  const double2 *f = a.cf + fidx * a.cu * a.cv;
+  double2 *g = a.grid + ((int64_t)ach * a.n_img_pol + apol) * a.n_u * a.n_v;
+  double2 norm = make_double2(0.0, 0.0);
+  const int n_tap = su * sv;
+  for (int t0 = 0; t0 < n_tap; t0 += blockDim.x) {
+    const int t = t0 + threadIdx.x;
+    if (t >= n_tap) continue;
+    const int iv = sv0 + t / su, iu = su0 + t % su;
+    const long long fu = (long long)a.os_u * iu + a.cu / 2, fv = (long long)a.os_v * iv + a.cv / 2;
+    const long long gu = a.n_u / 2 + iu, gv = a.n_v / 2 + iv;
+    if (fu < 0 || fu >= a.cu || fv < 0 || fv >= a.cv || gu < 0 || gu >= a.n_u || gv < 0 ||
+        gv >= a.n_v)
+      continue;
+    const double2 conv = f[fu * a.cv + fv];
+    double2 *cell = g + gu * a.n_v + gv;
+    atomicAdd(&cell->x, __dmul_rn(conv.x, w));
+    atomicAdd(&cell->y, __dmul_rn(conv.y, w));
+    norm.x += conv.x;
+  }
+  __shared__ double sh[MG_THREADS / 32];
+  double s = norm.x;
+  for (int off = 16; off > 0; off >>= 1) s += __shfl_down_sync(0xffffffffu, s, off);
+  if ((threadIdx.x & 31) == 0) sh[threadIdx.x >> 5] = s;
+  __syncthreads();
+  if (threadIdx.x == 0 && a.sumw) {
+    double r = 0.0;
+    for (int i = 0; i < (int)(blockDim.x >> 5); ++i) r += sh[i];
+    atomicAdd(&a.sumw[(int64_t)ach * a.n_img_pol + apol], __dmul_rn(w, r));
+  }
+}
+
+__global__ void k_cf_phase_product(const void *kern, int kern_complex, const double2 *pg,
+                                   double2 *out, int64_t n_cf, int64_t n_pix) {
+  const int64_t n = n_cf * n_pix;
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
+       i += (int64_t)gridDim.x * blockDim.x) {
+    const double2 g = pg[i % n_pix];
+    if (kern_complex) {
+      out[i] = cmul(((const double2 *)kern)[i], g);
+    } else {
+      const double r = ((const double *)kern)[i];
+      out[i] = make_double2(__dmul_rn(r, g.x), __dmul_rn(r, g.y));
+    }
+  }
+}
+
+// Airy-disk primary beams (make_pb_symmetric.py:1-280), one value per
+// thread in the reference's operation order; J1 is CUDA's j1.
+struct AiryArgs {
+  double *out;
+  int64_t n_dish, n_freq, nx, ny, cx, cy, n_pol;
+  double cell_x, cell_y;
+  int ipower, casa, rorder;
+  double dish[16], block[16];
+  const double *freq;
+};
+
+__global__ void k_airy_pattern(AiryArgs a) {
+  const int64_t n = a.n_dish * a.n_freq * a.nx * a.ny;
+  for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < n;
+       t += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t iy = t % a.ny;
+    const int64_t ix = (t / a.ny) % a.nx;
+    const int64_t f = (t / (a.ny * a.nx)) % a.n_freq;
+    const int64_t d = t / (a.ny * a.nx * a.n_freq);
+    double v = 1.0;
+    if (!(ix == a.cx && iy == a.cy)) {
+      const double x = __dmul_rn((double)(ix - a.cx), a.cell_x);
+      const double y = __dmul_rn((double)(iy - a.cy), a.cell_y);
+      const double k = __ddiv_rn(__dmul_rn(2.0 * 3.141592653589793, a.freq[f]), C_LIGHT);
+      const double r = __dmul_rn(__dmul_rn(__dsqrt_rn(__dadd_rn(__dmul_rn(x, x),
+                                                                 __dmul_rn(y, y))), k),
+                                 __ddiv_rn(a.dish[d], 2.0));
+      const double dd = a.dish[d], bd = a.block[d];
+      if (bd == 0.0) {
+        v = __ddiv_rn(__dmul_rn(2.0, j1(r)), r);
+      } else if (!a.casa) {
+        const double e = __ddiv_rn(bd, dd);
+        const double t1 = __ddiv_rn(__dmul_rn(2.0, j1(r)), r);
+        const double t2 = __ddiv_rn(__dmul_rn(__dmul_rn(2.0, e), j1(__dmul_rn(r, e))), r);
+        v = __ddiv_rn(__dsub_rn(t1, t2), __dsub_rn(1.0, __dmul_rn(e, e)));
+      } else {
+        const double lr = __ddiv_rn(dd, bd);
+        const double ar = __dmul_rn(lr, lr);
+        const double t1 = __ddiv_rn(__dmul_rn(__dmul_rn(ar, 2.0), j1(r)), r);
+        const double rl = __dmul_rn(r, lr);
+        const double t2 = __ddiv_rn(__dmul_rn(2.0, j1(rl)), rl);
+        v = __ddiv_rn(__dsub_rn(t1, t2), __dsub_rn(ar, 1.0));
+      }
+      double p = v;
+      for (int i = 1; i < a.ipower; ++i) p = __dmul_rn(p, v);
+      v = a.ipower == 0 ? 1.0 : p;
+    }
+    for (int64_t q = 0; q < a.n_pol; ++q) {
+      int64_t o;
+      if (a.rorder)  // (dish, freq, pol, x, y)
+        o = (((d * a.n_freq + f) * a.n_pol + q) * a.nx + ix) * a.ny + iy;
+      else  // (x, y, freq, pol, dish)
+        o = (((ix * a.ny + iy) * a.n_freq + f) * a.n_pol + q) * a.n_dish + d;
+      a.out[o] = v;
+    }
+  }
+}
+
+static unsigned mg_blocks(int64_t n_items, int per_block) {
+  int64_t b = (n_items + per_block - 1) / per_block;
+  const int64_t cap = (int64_t)sm_count() * 32;
+  if (b > cap) b = cap;
+  if (b < 1) b = 1;
+  return (unsigned)b;
+}
+
+static int fill_mosaic(MosaicArgs &a, void *grid, double *sum_weight, int do_psf,
+                       const void *vis, const double *weight, const double *uvw,
+                       const double *freq, const int32_t *chan_map, const int32_t *pol_map,
+                       const int32_t *cfb_map, const int32_t *cfc_map, const int32_t *cfp_map,
+                       const void *cf, int64_t n_cfb, int64_t n_cfc, int64_t n_cfp,
+                       int64_t conv_u, int64_t conv_v, const int32_t *support,
+                       int max_support, int64_t n_u, int64_t n_v, double delta_l,
+                       double delta_m, int os_u, int os_v, int64_t nt, int64_t nb,
+                       int64_t nchan, int64_t npol, int64_t n_img_chan, int64_t n_img_pol) {
+  a.grid = (double2 *)grid;
+  a.sumw = sum_weight;
+  a.do_psf = do_psf;
+  a.vis = (const double2 *)vis;
+  a.wt = weight;
+  a.uvw = uvw;
+  a.freq = freq;
+  a.chan_map = chan_map;
+  a.pol_map = pol_map;
+  a.cfb_map = cfb_map;
+  a.cfc_map = cfc_map;
+  a.cfp_map = cfp_map;
+  a.cf = (const double2 *)cf;
+  a.n_cfb = n_cfb;
+  a.n_cfc = n_cfc;
+  a.n_cfp = n_cfp;
+  a.cu = conv_u;
+  a.cv = conv_v;
+  a.support = support;
+  a.max_support = max_support;
+  a.n_u = n_u;
+  a.n_v = n_v;
+  a.dl0 = delta_l;
+  a.dl1 = delta_m;
+  a.os_u = os_u;
+  a.os_v = os_v;
+  a.nt = nt;
+  a.nb = nb;
+  a.nchan = nchan;
+  a.npol = npol;
+  a.n_img_chan = n_img_chan;
+  a.n_img_pol = n_img_pol;
+  return AV_OK;
+}
+
+}  // namespace av
+
+using namespace av;
+
+extern "C" {
+
+int av_cf_phase_product(const void *conv_kernel, int kernel_dtype, const void *phase_gradient,
+                        void *out, int64_t n_cf, int64_t conv_u, int64_t conv_v, void *stream) {
+  clear_error();
+  AV_CHECK_ARG(conv_kernel && phase_gradient && out, "av_cf_phase_product: null pointer");
+  AV_CHECK_ARG(kernel_dtype == AV_F64 || kernel_dtype == AV_C128,
+               "av_cf_phase_product: kernel must be float64 or complex128");
+  AV_CHECK_ARG(n_cf >= 0 && conv_u >= 1 && conv_v >= 1, "av_cf_phase_product: bad shape");
+  if (n_cf == 0) return AV_OK;
+  const int64_t n = n_cf * conv_u * conv_v;
+  k_cf_phase_product<<<mg_blocks(n, 256), 256, 0, as_stream(stream)>>>(
+      conv_kernel, kernel_dtype == AV_C128, (const double2 *)phase_gradient, (double2 *)out,
+      n_cf, conv_u * conv_v);
+  AV_LAUNCH_CHECK();
+  return AV_OK;
+}
+
+int av_airy_pattern(double *out, const double *dish_diameters, const double *blockage_diameters,
+                    int64_t n_dish, const double *freq, int64_t n_freq, int64_t n_pol,
+                    int64_t nx, int64_t ny, int64_t cx, int64_t cy, double cell_x,
+                    double cell_y, int ipower, int casa, int rorder, void *stream) {
+  clear_error();
+  AV_CHECK_ARG(out && dish_diameters && blockage_diameters && freq,
+               "av_airy_pattern: null pointer");
+  AV_CHECK_ARG(n_dish >= 1 && n_dish <= 16, "av_airy_pattern: 1 to 16 dish types");
+  AV_CHECK_ARG(n_freq >= 1 && n_pol >= 1 && nx >= 1 && ny >= 1 && ipower >= 0 && ipower <= 8,
+               "av_airy_pattern: bad shape or power");
+  AiryArgs a;
+  a.out = out;
+  a.n_dish = n_dish;
+  a.n_freq = n_freq;
+  a.nx = nx;
+  a.ny = ny;
+  a.cx = cx;
+  a.cy = cy;
+  a.n_pol = n_pol;
+  a.cell_x = cell_x;
+  a.cell_y = cell_y;
+  a.ipower = ipower;
+  a.casa = casa;
+  a.rorder = rorder;
+  a.freq = freq;
+  for (int i = 0; i < 16; ++i) {
+    a.dish[i] = i < n_dish ? dish_diameters[i] : 0.0;
+    a.block[i] = i < n_dish ? blockage_diameters[i] : 0.0;
+  }
+  const int64_t n = n_dish * n_freq * nx * ny;
+  k_airy_pattern<<<mg_blocks(n, 256), 256, 0, as_stream(stream)>>>(a);
+  AV_LAUNCH_CHECK();
+  return AV_OK;
+}
+
+#define AV_MOSAIC_PARAMS                                                                   \
+  void *grid, double *sum_weight, int do_psf, const void *vis, const double *weight,       \
+      const double *uvw, const double *freq, const int32_t *chan_map,                      \
+      const int32_t *pol_map, const int32_t *cf_baseline_map, const int32_t *cf_chan_map,  \
+      const int32_t *cf_pol_map, const void *cf, int64_t n_cf_baseline, int64_t n_cf_chan, \
+      int64_t n_cf_pol, int64_t conv_u, int64_t conv_v, const int32_t *support,            \
+      int max_support, int64_t n_u, int64_t n_v, double delta_l, double delta_m, int os_u, \
+      int os_v, int64_t nt, int64_t nb, int64_t nchan, int64_t npol, int64_t n_img_chan,    \
+      int64_t n_img_pol
+
+static int check_mosaic(const char *who, AV_MOSAIC_PARAMS) {
+  AV_CHECK_ARG(grid && weight && uvw && freq && chan_map && pol_map && cf_baseline_map &&
+                   cf_chan_map && cf_pol_map && cf && support,
+               "%s: null pointer", who);
+  AV_CHECK_ARG(do_psf || vis, "%s: vis is required unless do_psf", who);
+  AV_CHECK_ARG(n_cf_baseline >= 1 && n_cf_chan >= 1 && n_cf_pol >= 1 && conv_u >= 1 &&
+                   conv_v >= 1,
+               "%s: bad convolution-function shape", who);
+  AV_CHECK_ARG(n_u >= 1 && n_v >= 1 && os_u >= 1 && os_v >= 1 && max_support >= 0,
+               "%s: bad grid or oversampling", who);
+  AV_CHECK_ARG(nt >= 0 && nb >= 0 && nchan >= 0 && npol >= 0 && n_img_chan >= 1 &&
+                   n_img_pol >= 1,
+               "%s: bad shape", who);
+  return AV_OK;
+}
+
+int av_mosaic_grid(AV_MOSAIC_PARAMS, void *stream) {
+  clear_error();
+  int rc = check_mosaic("av_mosaic_grid", grid, sum_weight, do_psf, vis, weight, uvw, freq,
+                        chan_map, pol_map, cf_baseline_map, cf_chan_map, cf_pol_map, cf,
+                        n_cf_baseline, n_cf_chan, n_cf_pol, conv_u, conv_v, support,
+                        max_support, n_u, n_v, delta_l, delta_m, os_u, os_v, nt, nb, nchan,
+                        npol, n_img_chan, n_img_pol);
+  if (rc) return rc;
+  const int64_t rows = nt * nb * nchan;
+  if (rows == 0 || npol == 0) return AV_OK;
+  MosaicArgs a;
+  fill_mosaic(a, grid, sum_weight, do_psf, vis, weight, uvw, freq, chan_map, pol_map,
+              cf_baseline_map, cf_chan_map, cf_pol_map, cf, n_cf_baseline, n_cf_chan, n_cf_pol,
+              conv_u, conv_v, support, max_support, n_u, n_v, delta_l, delta_m, os_u, os_v, nt,
+              nb, nchan, npol, n_img_chan, n_img_pol);
+  k_mosaic_grid<<<mg_blocks(rows, MG_THREADS / 32), MG_THREADS, 0, as_stream(stream)>>>(a);
+  AV_LAUNCH_CHECK();
+  return AV_OK;
+}
+
+size_t av_aperture_grid_workspace_size(int64_t n_cf_baseline, int64_t nchan, int64_t npol) {
+  return Workspace::need(sizeof(double) * (size_t)(n_cf_baseline < 1 ? 1 : n_cf_baseline) *
+                         (nchan < 1 ? 1 : nchan) * (npol < 1 ? 1 : npol));
+}
+
+int av_aperture_grid(AV_MOSAIC_PARAMS, void *workspace, size_t workspace_bytes, void *stream) {
+  clear_error();
+  int rc = check_mosaic("av_aperture_grid", grid, sum_weight, 1, vis, weight, uvw, freq,
+                        chan_map, pol_map, cf_baseline_map, cf_chan_map, cf_pol_map, cf,
+                        n_cf_baseline, n_cf_chan, n_cf_pol, conv_u, conv_v, support,
+                        max_support, n_u, n_v, delta_l, delta_m, os_u, os_v, nt, nb, nchan,
+                        npol, n_img_chan, n_img_pol);
+  if (rc) return rc;
+  const int64_t rows = nt * nb * nchan;
+  if (rows == 0 || npol == 0) return AV_OK;
+  const int64_t n_cls = n_cf_baseline * nchan * npol;
+  AV_CHECK_ARG(n_cls <= 0x7fffffff, "av_aperture_grid: too many weight classes");
+  Workspace ws(workspace, workspace_bytes);
+  double *cls = ws.take<double>((size_t)n_cls);
+  AV_CHECK_ARG(cls, "av_aperture_grid: workspace too small");
+  MosaicArgs a;
+  fill_mosaic(a, grid, sum_weight, 1, nullptr, weight, uvw, freq, chan_map, pol_map,
+              cf_baseline_map, cf_chan_map, cf_pol_map, cf, n_cf_baseline, n_cf_chan, n_cf_pol,
+              conv_u, conv_v, support, max_support, n_u, n_v, delta_l, delta_m, os_u, os_v, nt,
+              nb, nchan, npol, n_img_chan, n_img_pol);
+  cudaStream_t st = as_stream(stream);
+  AV_CUDA(cudaMemsetAsync(cls, 0, sizeof(double) * (size_t)n_cls, st));
+  k_aperture_classes<<<mg_blocks(rows, MG_THREADS), MG_THREADS, 0, st>>>(a, cls);
+  AV_LAUNCH_CHECK();
+  k_aperture_add<<<(unsigned)n_cls, MG_THREADS, 0, st>>>(a, cls);
+  AV_LAUNCH_CHECK();
+  return AV_OK;
+}
+
+}  // extern "C"

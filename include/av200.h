@@ -394,6 +394,68 @@ int av_plane_sum(const void *x, int dtype, int64_t n_planes, int64_t n_pix, doub
 int av_vis_residual(const void *vis, const void *model, void *out, int dtype, int64_t n,
                     void *stream);
 
+/* ------------------------------------------------- mosaic / A-projection -- */
+/* conv_kernel x phase_gradient[0] (mosaic_grid.py:56-58, :384): out
+ * (n_cf, conv_u, conv_v) complex128 from a float64 or complex128 kernel of
+ * that shape and one (conv_u, conv_v) complex128 phase gradient; products
+ * without fused multiply-add. */
+int av_cf_phase_product(const void *conv_kernel, int kernel_dtype, const void *phase_gradient,
+                        void *out, int64_t n_cf, int64_t conv_u, int64_t conv_v, void *stream);
+
+/* Airy-disk primary beams of make_pb_symmetric.py: airy_disk (:1-58) and
+ * casa_airy_disk (:61-125) with rorder = 0, out (nx, ny, n_freq, n_pol,
+ * n_dish); airy_disk_rorder (:128-190) and casa_airy_disk_rorder (:193-280)
+ * with rorder = 1, out (n_dish, n_freq, n_pol, nx, ny); casa selects the
+ * CASA blockage formula.  Pixel offsets from (cx, cy) times (cell_x, cell_y)
+ * radians, freq (n_freq) device float64 in Hz, dish and blockage diameters
+ * (n_dish <= 16) in host memory, metres; the pattern raised to ipower (0-8),
+ * 1 at the centre; J1 is CUDA's j1 (a few ulp from scipy's). */
+int av_airy_pattern(double *out, const double *dish_diameters, const double *blockage_diameters,
+                    int64_t n_dish, const double *freq, int64_t n_freq, int64_t n_pol,
+                    int64_t nx, int64_t ny, int64_t cx, int64_t cy, double cell_x,
+                    double cell_y, int ipower, int casa, int rorder, void *stream);
+
+/* mosaic_grid_jit (mosaic_grid.py:307-486): grid (n_img_chan, n_img_pol,
+ * n_u, n_v) complex128 and sum_weight (n_img_chan, n_img_pol) += the
+ * samples' windows of the convolution function cf (n_cf_baseline,
+ * n_cf_chan, n_cf_pol, conv_u, conv_v) complex128 (phase gradient applied,
+ * see av_cf_phase_product), chosen per sample by cf_baseline_map (nb),
+ * cf_chan_map (nchan) and cf_pol_map (npol); window sizes support
+ * (n_cf_baseline, n_cf_chan, n_cf_pol, 2); max_support = np.max(support)
+ * sets the grid-edge test.  vis (nt, nb, nchan, npol) complex128 (NULL with
+ * do_psf), weight float64 of the same shape, uvw (nt, nb, 3), freq (nchan).
+ * sum_weight gets w Re(norm) with do_psf, else w Re(norm^2), norm the sum of
+ * the window.  Window taps that fall outside cf (the reference reads past the
+ * array there) are left out. */
+int av_mosaic_grid(void *grid, double *sum_weight, int do_psf, const void *vis,
+                   const double *weight, const double *uvw, const double *freq,
+                   const int32_t *chan_map, const int32_t *pol_map,
+                   const int32_t *cf_baseline_map, const int32_t *cf_chan_map,
+                   const int32_t *cf_pol_map, const void *cf, int64_t n_cf_baseline,
+                   int64_t n_cf_chan, int64_t n_cf_pol, int64_t conv_u, int64_t conv_v,
+                   const int32_t *support, int max_support, int64_t n_u, int64_t n_v,
+                   double delta_l, double delta_m, int os_u, int os_v, int64_t nt, int64_t nb,
+                   int64_t nchan, int64_t npol, int64_t n_img_chan, int64_t n_img_pol,
+                   void *stream);
+
+/* aperture_grid_jit (mosaic_grid.py:13-153): every sample that passes the
+ * grid-edge test adds weight x its function window at the grid centre
+ * (and weight x Re(norm) to sum_weight); the weights are summed per
+ * (cf baseline, channel, polarisation) first.  Same arguments as
+ * av_mosaic_grid (do_psf and vis unused) plus a workspace of
+ * av_aperture_grid_workspace_size bytes. */
+size_t av_aperture_grid_workspace_size(int64_t n_cf_baseline, int64_t nchan, int64_t npol);
+int av_aperture_grid(void *grid, double *sum_weight, int do_psf, const void *vis,
+                     const double *weight, const double *uvw, const double *freq,
+                     const int32_t *chan_map, const int32_t *pol_map,
+                     const int32_t *cf_baseline_map, const int32_t *cf_chan_map,
+                     const int32_t *cf_pol_map, const void *cf, int64_t n_cf_baseline,
+                     int64_t n_cf_chan, int64_t n_cf_pol, int64_t conv_u, int64_t conv_v,
+                     const int32_t *support, int max_support, int64_t n_u, int64_t n_v,
+                     double delta_l, double delta_m, int os_u, int os_v, int64_t nt,
+                     int64_t nb, int64_t nchan, int64_t npol, int64_t n_img_chan,
+                     int64_t n_img_pol, void *workspace, size_t workspace_bytes, void *stream);
+
 #ifdef __cplusplus
 }
 #endif
