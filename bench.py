@@ -49,6 +49,7 @@ def parse():
     ap.add_argument("--no-batched", action="store_true")
     ap.add_argument("--no-forward", action="store_true")
     ap.add_argument("--no-imager", action="store_true")
+    ap.add_argument("--no-mosaic", action="store_true")
     ap.add_argument("--clean-iters", type=int, default=20000)
     return ap.parse_args()
 
@@ -384,6 +385,10 @@ def main():
     if not (args.quick or args.no_imager) and rank == 0:
         imaging = bench_imager(args, dev)
 
+    mosaic = None
+    if not (args.quick or args.no_mosaic) and rank == 0:
+        mosaic = bench_mosaic(args, dev)
+
     # ------------------------------------------------------------- batched
     batched = None
     if not (args.quick or args.no_batched) and rank == 0:
@@ -446,6 +451,7 @@ def main():
         "batched_uneven": batched,
         "forward_model": forward,
         "imaging_loop": imaging,
+        "mosaic_grid": mosaic,
     }
     if rank == 0:
         print(json.dumps(line), flush=True)
@@ -702,6 +708,99 @@ def bench_imager(args, dev):
             "speedup_vs_cpu": t_cpu / t_gpu,
             "workload": "64 ant, 50 t x 2016 bl x 1 ch x 2 pol (100800 vis), 512^2, 2 arcsec, "
                         "support 7, os 100, Hogbom niter 1000, nmajor 5, cyclefactor 1.5"}
+
+
+def bench_mosaic(args, dev):
+    """mosaic_grid_jit (FP64, av_mosaic_grid) on 64 antennas x 64 time steps x
+    8 channels (1.0-1.5 GHz) x 2 pol = 1.03M samples into a 1024^2 grid of
+    2 arcsec cells, with Airy-disk convolution functions of 12 m and 25 m
+    dishes built by the helpers (oversampling 4, cut 0.025, a field 30 cells
+    off the phase centre), against the oracle's C restatement on 4 of the 64
+    time steps."""
+    import torch
+
+    import oracle as O
+    from astroviper_b200 import _kernels as K
+    from astroviper_b200 import synthetic as S
+    from astroviper_b200.core.imaging import make_gridding_convolution_function as G
+    from astroviper_b200.core.imaging.imaging_utils import make_pb_symmetric as PB
+    nt, nchan, npol, n = 64, 8, 2, 1024
+    uvw, rng = S.array_uvw(64, nt, seed=20260122)
+    nb = uvw.shape[1]
+    freq = np.linspace(1.0e9, 1.5e9, nchan)
+    cell = np.array([-2.0, 2.0]) * np.pi / 180 / 3600
+    shape = (nt, nb, nchan, npol)
+    vis = rng.normal(size=shape) + 1j * rng.normal(size=shape)
+    wt = rng.uniform(0.5, 2.0, size=shape)
+    ant_type = np.arange(64) % 2
+    bant = np.array([[i, j] for i in range(64) for j in range(i + 1, 64)])
+    cfb, pairs = G.create_cf_baseline_map(ant_type, bant, 2)
+    cfc, pb_freq = G.create_cf_chan_map(freq, 0.05)
+    os_, ms = np.array([4, 4]), np.array([11, 11])
+    gcf = {"list_dish_diameters": np.array([12.0, 25.0]),
+           "list_blockage_diameters": np.array([0.75, 0.0]), "oversampling": os_,
+           "max_support": ms, "support_cut_level": 0.025, "resize_conv_size": (ms + 1) * os_,
+           "phase_direction": np.array([0.0, -0.5])}
+    grid_p = {"image_size": np.array([n, n]), "image_size_padded": np.array([n, n]),
+              "cell_size": cell}
+    gcf["ipower"] = 1
+    bp = G.make_baseline_patterns(pb_freq, np.array([0]), pairs, PB.airy_disk_rorder, gcf,
+                                  grid_p)
+    gcf["ipower"] = 2
+    bp2 = G.make_baseline_patterns(pb_freq, np.array([0]), pairs, PB.airy_disk_rorder, gcf,
+                                   grid_p)
+    rk, _rkc, sup = G.resize_and_calc_support(G.conv_kernels(bp), G.conv_kernels(bp2), gcf,
+                                              grid_p)
+    pg = G.make_phase_gradient(np.array([[30 * abs(cell[0]), -0.5]]), gcf, grid_p)
+    cf = K.cf_phase_product(torch.as_tensor(rk, device=dev), torch.as_tensor(pg[0], device=dev))
+    vis_d = torch.as_tensor(vis, device=dev)
+    wt_d = torch.as_tensor(wt, device=dev)
+    uvw_d = torch.as_tensor(uvw, device=dev)
+    cm, pm, cfp = np.arange(nchan), np.arange(npol), np.zeros(npol, dtype=int)
+    grid = torch.zeros((nchan, npol, n, n), dtype=torch.complex128, device=dev)
+    sw = torch.zeros((nchan, npol), dtype=torch.float64, device=dev)
+
+    def run():
+        K.mosaic_grid(grid, sw, False, vis_d, wt_d, uvw_d, freq, cm, pm, cfb, cfc, cfp, cf, sup,
+                      (n, n), cell, os_)
+
+    for _ in range(3):
+        run()
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(2)]
+    reps = 10
+    torch.cuda.synchronize()
+    ev[0].record()
+    for _ in range(reps):
+        run()
+    ev[1].record()
+    torch.cuda.synchronize()
+    ms_gpu = ev[0].elapsed_time(ev[1]) / reps
+    n_vis = nt * nb * nchan
+    # accuracy and the CPU baseline on a sample of the time steps
+    ts = 4
+    g1 = torch.zeros_like(grid)
+    s1 = torch.zeros_like(sw)
+    K.mosaic_grid(g1, s1, False, vis_d[:ts], wt_d[:ts], uvw_d[:ts], freq, cm, pm, cfb, cfc, cfp,
+                  cf, sup, (n, n), cell, os_)
+    go = np.zeros((nchan, npol, n, n), dtype=np.complex128)
+    so = np.zeros((nchan, npol))
+    t0 = time.perf_counter()
+    O.mosaic_grid(go, so, False, vis[:ts], uvw[:ts], freq, cm, pm, cfb, cfc, cfp, wt[:ts],
+                  cf.cpu().numpy(), sup, (n, n), cell, os_)
+    t_cpu = time.perf_counter() - t0
+    cpu_mvis = ts * nb * nchan / t_cpu / 1e6
+    gpu_mvis = n_vis / (ms_gpu / 1e3) / 1e6
+    return {"value": gpu_mvis, "unit": "Mvis/s", "ms_per_call": ms_gpu,
+            "supports": sorted(set(int(x) for x in np.asarray(sup).ravel())),
+            "n_functions": int(np.prod(np.asarray(sup).shape[:3])),
+            "rel_err_vs_oracle": {"grid": rel(g1.cpu().numpy(), go),
+                                  "sum_weight": rel(s1.cpu().numpy(), so),
+                                  "sample": f"{ts} of {nt} time steps"},
+            "cpu_baseline": {"value": cpu_mvis, "unit": "Mvis/s", "cores": 1, "kind": "port",
+                             "sample": f"{ts} of {nt} time steps, the oracle's C restatement"},
+            "speedup_vs_cpu": gpu_mvis / cpu_mvis,
+            "workload": "64 ant, 64 t x 2016 bl x 8 ch x 2 pol (1.03M vis), 1024^2 cube, "
+                        "2 arcsec, Airy functions 12 m / 25 m, oversampling 4"}
 
 
 def bench_e2e(W, vis_dev, iw_dev, G):

@@ -16,6 +16,7 @@
  *   src/astroviper/core/imaging/imaging_utils/standard_degrid.py
  *   src/astroviper/core/imaging/imaging_weighting/grid_imaging_weights.py
  *   src/astroviper/core/imaging/deconvolvers/hogbom/src/hclean.cpp
+ *   src/astroviper/core/imaging/imaging_utils/mosaic_grid.py
  */
 #include <math.h>
 #include <stdint.h>
@@ -604,6 +605,84 @@ void orc_maximg_f64(const double *img, int domask, const double *mask, int nx, i
     }
   *fmin = mn;
   *fmax = mx;
+}
+
+/* ---------------------------------------------------------------------------
+ * Mosaic gridder, mosaic_grid_jit (mosaic_grid.py:307-486): each sample's
+ * window of the convolution function cf (n_cfb, n_cfc, n_cfp, cu, cv),
+ * phase gradient already applied, v outer and u inner, in sample order.
+ * grid (n_img_chan, n_img_pol, n_u, n_v) and sum_weight (n_img_chan,
+ * n_img_pol) are accumulated.  Window taps outside cf (the reference reads
+ * past the array there) are left out.
+ * ------------------------------------------------------------------------- */
+static inline cplx cmul(cplx a, cplx b) {
+  cplx r = {a.re * b.re - a.im * b.im, a.re * b.im + a.im * b.re};
+  return r;
+}
+
+void orc_mosaic_grid(cplx *grid, double *sum_weight, int do_psf, const cplx *vis,
+                     const double *uvw, const double *freq, const int64_t *chan_map,
+                     const int64_t *pol_map, const int64_t *cfb_map, const int64_t *cfc_map,
+                     const int64_t *cfp_map, const double *weight, const cplx *cf, int64_t n_cfc,
+                     int64_t n_cfp, int64_t cu, int64_t cv, const int64_t *support,
+                     int64_t max_support, int64_t n_u, int64_t n_v, double dl0, double dl1,
+                     int64_t os_u, int64_t os_v, int64_t nt, int64_t nb, int64_t nchan,
+                     int64_t npol, int64_t n_img_pol) {
+  const double c = 299792458.0;
+  for (int64_t t = 0; t < nt; ++t)
+    for (int64_t b = 0; b < nb; ++b) {
+      const int64_t cfb = cfb_map[b];
+      for (int64_t ch = 0; ch < nchan; ++ch) {
+        const double s0 = -(freq[ch] * dl0 * (double)n_u) / c;
+        const double s1 = -(freq[ch] * dl1 * (double)n_v) / c;
+        const int64_t tb = t * nb + b;
+        const double u = uvw[3 * tb] * s0, v = uvw[3 * tb + 1] * s1;
+        if (isnan(u) || isnan(v)) continue;
+        const double up = u + (double)(n_u / 2), vp = v + (double)(n_v / 2);
+        const int64_t uc = trunc_i64(up + 0.5), vc = trunc_i64(vp + 0.5);
+        if (!(uc + max_support < n_u && vc + max_support < n_v && uc - max_support >= 0 &&
+              vc - max_support >= 0))
+          continue;
+        const int64_t uo = (int64_t)floor(((double)uc - up) * (double)os_u + 0.5) + cu / 2;
+        const int64_t vo = (int64_t)floor(((double)vc - vp) * (double)os_v + 0.5) + cv / 2;
+        const int64_t cfc = cfc_map[ch], ach = chan_map[ch];
+        for (int64_t p = 0; p < npol; ++p) {
+          const int64_t k = (tb * nchan + ch) * npol + p;
+          const double w = weight[k];
+          cplx wd;
+          if (do_psf) {
+            wd.re = w;
+            wd.im = 0.0;
+          } else {
+            wd.re = vis[k].re * w;
+            wd.im = vis[k].im * w;
+          }
+          if (isnan(wd.re) || isnan(wd.im) || (wd.re == 0.0 && wd.im == 0.0)) continue;
+          const int64_t cfp = cfp_map[p], apol = pol_map[p];
+          const int64_t fidx = (cfb * n_cfc + cfc) * n_cfp + cfp;
+          const int64_t su = support[2 * fidx], sv = support[2 * fidx + 1];
+          const cplx *f = cf + fidx * cu * cv;
+          cplx *g = grid + (ach * n_img_pol + apol) * n_u * n_v;
+          cplx norm = {0.0, 0.0};
+          for (int64_t iv = -(sv / 2); iv < sv - sv / 2; ++iv) {
+            const int64_t fv = os_v * iv + vo;
+            for (int64_t iu = -(su / 2); iu < su - su / 2; ++iu) {
+              const int64_t fu = os_u * iu + uo;
+              if (fu < 0 || fu >= cu || fv < 0 || fv >= cv) continue;
+              const cplx cw = f[fu * cv + fv];
+              const cplx x = cmul(cw, wd);
+              cplx *cell = g + (uc + iu) * n_v + (vc + iv);
+              cell->re += x.re;
+              cell->im += x.im;
+              norm.re += cw.re;
+              norm.im += cw.im;
+            }
+          }
+          const double re = do_psf ? norm.re : norm.re * norm.re - norm.im * norm.im;
+          sum_weight[ach * n_img_pol + apol] += w * re;
+        }
+      }
+    }
 }
 
 int orc_num_threads(void) {

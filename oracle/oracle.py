@@ -65,6 +65,9 @@ def lib():
     L.orc_maximg_f32.argtypes = [_fp, _i, _fp, _i, _i, _fp, _fp]
     L.orc_maximg_f64.argtypes = [_dp, _i, _dp, _i, _i, _dp, _dp]
     L.orc_num_threads.restype = _i
+    L.orc_mosaic_grid.argtypes = [_vp, _dp, _i, _vp, _dp, _dp, _i64p, _i64p, _i64p, _i64p,
+                                  _i64p, _dp, _vp, _i64, _i64, _i64, _i64, _i64p, _i64, _i64,
+                                  _i64, _d, _d, _i64, _i64, _i64, _i64, _i64, _i64, _i64]
     _LIB = L
     return L
 
@@ -407,6 +410,28 @@ def maximg(image, mask=None):
     lib().orc_maximg_f64(_p(im, _dp), domask, _p(m, _dp), nx, ny, ctypes.byref(a),
                          ctypes.byref(b))
     return a.value, b.value
+
+
+def mosaic_grid(grid, sum_weight, do_psf, vis, uvw, freq, chan_map, pol_map, cfb_map, cfc_map,
+                cfp_map, weight, cf, support, n_uv, delta_lm, oversampling):
+    """Restates mosaic_grid_jit (mosaic_grid.py:307-486) with cf the
+    convolution function already multiplied by phase_gradient[0]; grid
+    (complex128) and sum_weight are updated in place."""
+    assert grid.flags.c_contiguous and grid.dtype == np.complex128
+    nt, nb, nchan, npol = weight.shape
+    v = _c(vis if not do_psf else np.zeros(weight.shape, np.complex128), np.complex128)
+    cfa = _c(cf, np.complex128)
+    sup = _c(support, np.int64)
+    n_cfb, n_cfc, n_cfp, cu, cv = cfa.shape
+    os_ = np.broadcast_to(np.asarray(oversampling, dtype=np.int64), (2,))
+    maps = [_c(m, np.int64) for m in (chan_map, pol_map, cfb_map, cfc_map, cfp_map)]
+    lib().orc_mosaic_grid(grid.ctypes.data, _p(sum_weight, _dp), int(bool(do_psf)),
+                          v.ctypes.data, _p(_c(uvw, np.float64), _dp),
+                          _p(_c(freq, np.float64), _dp), *[_p(m, _i64p) for m in maps],
+                          _p(_c(weight, np.float64), _dp), cfa.ctypes.data, n_cfc, n_cfp, cu, cv,
+                          _p(sup, _i64p), int(np.max(sup)), int(n_uv[0]), int(n_uv[1]),
+                          float(delta_lm[0]), float(delta_lm[1]), int(os_[0]), int(os_[1]), nt,
+                          nb, nchan, npol, grid.shape[1])
 
 
 def num_threads():

@@ -66,3 +66,22 @@ def test_mosaic_wrapper_helpers_and_errors():
         M.mosaic_grid_numpy_wrap(None, None, w, None, None, None, None, None, None, None, None,
                                  {"chan_mode": "cube", "image_size_padded": [8, 8],
                                   "complex_grid": False})
+
+
+def test_oracle_mosaic_grid_matches_reference():
+    """The oracle's C restatement of mosaic_grid_jit against the Numba
+    kernel's own grids (the CPU baseline of the benchmark)."""
+    import oracle as O
+    g = golden("mosaic.npz")
+    cf = g["rk"] * g["mg_pg"][0]
+    n_uv = g["grid_image_size_padded"]
+    for tag, cm, nic in (("cube", np.arange(2), 2), ("cont", np.zeros(2, dtype=int), 1)):
+        for do_psf in (False, True):
+            grid = np.zeros((nic, 2, n_uv[0], n_uv[1]), dtype=np.complex128)
+            sw = np.zeros((nic, 2))
+            O.mosaic_grid(grid, sw, do_psf, g["mg_vis"], g["mg_uvw"], g["mg_freq"], cm,
+                          np.arange(2), g["mg_cfb"], g["mg_cfc"], g["mg_cfp"], g["mg_wt"], cf,
+                          g["support"], n_uv, g["grid_cell"], g["gcf_oversampling"])
+            want = g[f"mg_{tag}_{int(do_psf)}_grid"]
+            assert np.array_equal(grid, want), (tag, do_psf)
+            assert np.array_equal(sw, g[f"mg_{tag}_{int(do_psf)}_sw"]), (tag, do_psf)
