@@ -127,7 +127,8 @@ def deconvolve_planes(dirty, psf, gain, niter, threshold, start_model=None):
     return recs, model, resid
 
 
-def run_imaging_loop(vis, uvw, weight, flag, freq, params, controller, merge, ReturnDict):
+def run_imaging_loop(vis, uvw, weight, flag, freq, params, controller, merge, ReturnDict,
+                     initial_model=None):
     """imager.py:108-351 on arrays (vis (nt, nb, nchan, npol) complex128).
     weight / flag / uvw are modified in place as the reference modifies the
     measurement set.  Returns dict(model, residual, cycles, vis_model,
@@ -155,7 +156,8 @@ def run_imaging_loop(vis, uvw, weight, flag, freq, params, controller, merge, Re
     psf_corr = grid_image(None, np.array([-cell[0], cell[1]]), True, (image_size[1],
                                                                        image_size[0]))
     psf_i = image_corr_to_stokes(psf_corr[None], corr_type, 2, ["I"])
-    model = np.zeros((len(freq), len(stokes), ny, nx))
+    model = np.zeros((len(freq), len(stokes), ny, nx)) if initial_model is None else \
+        np.array(initial_model, dtype=float)
     combined = ReturnDict()
     column = vis
     out = {"cycles": []}

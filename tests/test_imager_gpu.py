@@ -181,7 +181,7 @@ class ImagingMS4:
         return k in self._d
 
 
-def _loop_inputs(n_time=16, n_chan=2):
+def _loop_inputs(n_time=16, n_chan=2, pol_scale=(1.0, 0.8)):
     from astroviper_b200 import synthetic as S
     W = S.workload_small(n_time=n_time)
     uvw = W["uvw"].copy()
@@ -189,8 +189,9 @@ def _loop_inputs(n_time=16, n_chan=2):
     rng = np.random.default_rng(11)
     flux, dx, dy = W["sources"]
     l, m = S.source_lm(dx / 2, dy / 2, W["pixelincr"])
-    vis = S.point_source_vis(uvw, freq, 2, flux, l, m, 0.01, rng)
-    vis[:, :, :, 1] *= 0.8  # YY fainter than XX: Stokes Q is not zero
+    vis = S.point_source_vis(uvw, freq, len(pol_scale), flux, l, m, 0.01, rng)
+    # distinct correlations (e.g. YY fainter than XX), so Q (V) is not zero
+    vis = vis * np.asarray(pol_scale)
     weight = np.ones(vis.shape)
     flag = np.zeros(vis.shape, dtype=bool)
     flag[3, 10:20] = True
@@ -204,14 +205,14 @@ def _params(cell):
             "chan_mode": "cube"}
 
 
-def _run_oracle(vis, uvw, weight, flag, freq, params):
+def _run_oracle(vis, uvw, weight, flag, freq, params, initial_model=None):
     from astroviper_b200.core.imaging.imaging_utils import iteration_control as IC
     from astroviper_b200.core.imaging.imaging_utils.return_dict import ReturnDict
     ctl = IC.IterationController(niter=params["niter"], nmajor=params["nmajor"],
                                  threshold=params["threshold"], gain=params["gain"],
                                  cyclefactor=params["cyclefactor"])
     return OI.run_imaging_loop(vis, uvw, weight, flag, freq, params, ctl, IC.merge_return_dicts,
-                               ReturnDict)
+                               ReturnDict, initial_model)
 
 
 @pytest.mark.parametrize("precision", ["fp64", "fp32"])
@@ -246,9 +247,48 @@ def test_imaging_loop_matches_oracle(precision):
     assert np.array_equal(ms["RESIDUAL"].data, vis - vm)
 
 
-def _nan_rows(uvw, uv_only=False):
+def _nan_rows(uvw, uv_only=False, nchan=2, npol=2):
     bad = np.isnan(uvw[:, :, :2] if uv_only else uvw).any(axis=-1)
-    return np.broadcast_to(bad[:, :, None, None], bad.shape + (2, 2))
+    return np.broadcast_to(bad[:, :, None, None], bad.shape + (nchan, npol))
+
+
+@pytest.mark.parametrize("case", ["linear4", "circular2", "initial_model_threshold"])
+def test_imaging_loop_variants_match_oracle(case):
+    """Four correlations (IQUV, complex model correlations in the predict),
+    circular feeds (I, V), and a loop started from an initial model with a
+    global threshold (the stop code, like everything else the controller
+    decides, must be the oracle's); FP64 mode against the oracle's loop."""
+    from astroviper_b200.core.imaging.imager import run_imaging_loop
+    scale = {"linear4": (1.0, 0.1, 0.05, 0.8), "circular2": (1.0, 0.7),
+             "initial_model_threshold": (1.0, 0.8)}[case]
+    pols = {"linear4": ["XX", "XY", "YX", "YY"], "circular2": ["RR", "LL"],
+            "initial_model_threshold": ["XX", "YY"]}[case]
+    vis, uvw, weight, flag, freq, cell = _loop_inputs(n_time=12, pol_scale=scale)
+    params = _params(cell)
+    params.update(niter=120, nmajor=3)
+    init = None
+    if case == "circular2":
+        params["corr_type"] = "circular"
+    if case == "initial_model_threshold":
+        params.update(threshold=0.05, nmajor=6, niter=2000)
+        init = np.zeros((2, 2, 128, 128))
+        init[0, 0, 60, 64] = 0.3
+    ref = _run_oracle(vis.copy(), uvw.copy(), weight.copy(), flag.copy(), freq, params,
+                      init)
+    ms = ImagingMS4(vis.copy(), uvw.copy(), weight.copy(), flag.copy(), freq, pols)
+    model, resid, combined, ctl = run_imaging_loop(ms, params, initial_model=init,
+                                                   precision="fp64")
+    rctl = ref["controller"]
+    assert ctl.get_state() == rctl.get_state()
+    assert model.shape == ref["model"].shape
+    assert rel(model, ref["model"]) <= 1e-9 and rel(resid, ref["residual"]) <= 1e-9
+    for k in combined.data:
+        a, b = combined.data[k], ref["combined"].data[k]
+        assert a["iter_done"] == b["iter_done"], k
+        assert a["start_model_flux"] == pytest.approx(b["start_model_flux"], rel=1e-12,
+                                                      abs=1e-12)
+    if ref["vis_model"] is not None:
+        assert rel(ms["VISIBILITY_MODEL"].data, ref["vis_model"]) <= 1e-9
 
 
 def test_imaging_loop_drop_in_steps():
