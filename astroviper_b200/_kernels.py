@@ -618,10 +618,22 @@ def cf_phase_product(conv_kernel, phase_gradient):
     return out
 
 
+def mosaic_tiled_ok(support, oversampling, n_img_pol):
+    """Whether the binned mosaic gridder covers these functions."""
+    ms = int(np.max(np.asarray(support)))
+    os_ = np.broadcast_to(np.asarray(oversampling), (2,))
+    return (1 <= ms <= 32 and int(os_[0]) == int(os_[1]) and 1 <= int(os_[0]) <= 254
+            and int(n_img_pol) <= 4 and (31 + ms) ** 2 * int(n_img_pol) * 16 <= 220 * 1024
+            and int(np.min(np.asarray(support))) >= 1)
+
+
 def mosaic_grid(grid, sum_weight, do_psf, vis, weight, uvw, freq, chan_map, pol_map, cfb_map,
-                cfc_map, cfp_map, cf, support, n_uv, delta_lm, oversampling, aperture=False):
+                cfc_map, cfp_map, cf, support, n_uv, delta_lm, oversampling, aperture=False,
+                tiled=None):
     """av_mosaic_grid / av_aperture_grid into the device arrays grid
-    (complex128) and sum_weight (float64)."""
+    (complex128) and sum_weight (float64).  tiled (default: when
+    mosaic_tiled_ok) bins the samples first and grids tile by tile
+    (av_mosaic_tiled_plan + _execute)."""
     w = on_device(weight, torch.float64)
     nt, nb, nchan, npol = (int(s) for s in w.shape)
     v = None if (do_psf or aperture) else on_device(vis, torch.complex128)
@@ -642,8 +654,22 @@ def mosaic_grid(grid, sum_weight, do_psf, vis, weight, uvw, freq, chan_map, pol_
     if aperture:
         _buf, wptr, wbytes = workspace(lib().av_aperture_grid_workspace_size(n_cfb, nchan, npol))
         check(lib().av_aperture_grid(*args, wptr, wbytes, stream_ptr()), "av_aperture_grid")
-    else:
+        return grid, sum_weight
+    if tiled is None:
+        tiled = mosaic_tiled_ok(support, oversampling, grid.shape[1])
+    if not tiled:
         check(lib().av_mosaic_grid(*args, stream_ptr()), "av_mosaic_grid")
+        return grid, sum_weight
+    n_img_chan = int(grid.shape[0])
+    need = lib().av_mosaic_tiled_workspace_size(nt, nb, nchan, int(n_uv[0]), int(n_uv[1]),
+                                                n_img_chan, max_sup)
+    _buf, wptr, wbytes = workspace(need)
+    check(lib().av_mosaic_tiled_plan(p(uvw_d), p(freq_d), p(maps[0]), int(n_uv[0]), int(n_uv[1]),
+                                     float(delta_lm[0]), float(delta_lm[1]), max_sup, os_u, nt,
+                                     nb, nchan, n_img_chan, wptr, wbytes, stream_ptr()),
+          "av_mosaic_tiled_plan")
+    check(lib().av_mosaic_tiled_execute(*args, wptr, wbytes, stream_ptr()),
+          "av_mosaic_tiled_execute")
     return grid, sum_weight
 
 

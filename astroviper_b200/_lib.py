@@ -96,6 +96,10 @@ SIGNATURES = {
                              _d, _i, _i, _i, _vp]),
     "av_mosaic_grid": (_i, _MOSAIC + [_vp]),
     "av_aperture_grid_workspace_size": (_sz, [_i64, _i64, _i64]),
+    "av_mosaic_tiled_workspace_size": (_sz, [_i64, _i64, _i64, _i64, _i64, _i64, _i]),
+    "av_mosaic_tiled_plan": (_i, [_vp, _vp, _vp, _i64, _i64, _d, _d, _i, _i, _i64, _i64, _i64,
+                                  _i64, _vp, _sz, _vp]),
+    "av_mosaic_tiled_execute": (_i, _MOSAIC + [_vp, _sz, _vp]),
     "av_aperture_grid": (_i, _MOSAIC + [_vp, _sz, _vp]),
 }
 

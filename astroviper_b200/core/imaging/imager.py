@@ -189,27 +189,29 @@ class _ResidentMs4:
         self.resid_vis = None
         self.predicted = False
 
-    def _grid(self, vis, uvw, shape_uv, cell, do_psf):
-        if self.precision == "fp32" and not do_psf and shape_uv == (self.ny, self.nx) and \
-                cell is self.cell:
-            return self.g_dirty.grid(vis, self.weight)
-        return K.grid(None if do_psf else vis, self.weight, uvw, self.freq, self.chan_map,
-                      self.pol_map, self.cgk, shape_uv, cell, self.support, self.os,
-                      len(np.unique(self.chan_map)), self.n_pol, do_psf=do_psf,
-                      precision=self.precision)
-
     def psf(self):
-        """make_psf: (n_freq, n_pol, image_size[1], image_size[0]) float64."""
-        shape_uv = (self.nx, self.ny)
+        """make_psf: (n_freq, n_pol, image_size[1], image_size[0]) float64,
+        gridded once with pixel increment (-cell[0], cell[1])."""
         cell = np.array([-self.cell[0], self.cell[1]])
-        g, sw = self._grid(None, self.uvw_grid, shape_uv, cell, do_psf=True)
+        g, sw = K.grid(None, self.weight, self.uvw_grid, self.freq, self.chan_map,
+                       self.pol_map, self.cgk, (self.nx, self.ny), cell, self.support, self.os,
+                       len(np.unique(self.chan_map)), self.n_pol, do_psf=True,
+                       precision=self.precision)
         return K.grid_to_image(g, sw, apply_corr=True, out_dtype=torch.float64)
 
     def dirty(self, column):
+        """Dirty image of VISIBILITY or RESIDUAL; FP32 mode grids with the
+        plan built once for the loop."""
         vis = self.vis if column == "VISIBILITY" else self.resid_vis
         if vis is None:
             raise KeyError(column)
-        g, sw = self._grid(vis, self.uvw_grid, (self.ny, self.nx), self.cell, do_psf=False)
+        if self.precision == "fp32":
+            g, sw = self.g_dirty.grid(vis, self.weight)
+        else:
+            g, sw = K.grid(vis, self.weight, self.uvw_grid, self.freq, self.chan_map,
+                           self.pol_map, self.cgk, (self.ny, self.nx), self.cell, self.support,
+                           self.os, len(np.unique(self.chan_map)), self.n_pol,
+                           precision="fp64")
         return K.grid_to_image(g, sw, apply_corr=True, out_dtype=torch.float64)
 
     def predict(self, model_corr):

@@ -14,7 +14,7 @@
 //                     its function once.
 // av_cf_phase_product conv_kernel x phase_gradient[0] (mosaic_grid.py:384,
 //                     :56-58), elementwise without fused multiply-add.
-#include "common.cuh"
+#include "plan.cuh"
 
 namespace av {
 
@@ -269,6 +269,213 @@ __global__ void k_airy_pattern(AiryArgs a) {
   }
 }
 
+// ----------------------------------------------------------------- tiled --
+// Binned version of k_mosaic_grid: the gridder's plan (plan.cuh) with a
+// footprint window of S = max_support cells and the mosaic's edge margin
+// (np.max(weight_support)) holds every kept sample's cell and kernel offset;
+// a persistent CTA per SM takes record chunks, keeps an FP64 complex
+// sub-grid of (32 + S - 1)^2 x n_img_pol in shared memory per tile segment
+// and flushes it once.  A warp takes one record at a time; its lanes cover
+// the support window packed as (32 / su) rows of su columns.
+constexpr int MT_THREADS = 512;
+constexpr int MT_WARPS = MT_THREADS / 32;
+
+struct MosaicTiledArgs {
+  MosaicArgs m;
+  const Rec *recs;
+  const uint32_t *tile_start;
+  const uint32_t *n_rec;
+  uint32_t *sched;
+  int64_t n_tiles, ntu, ntv, chunk;
+  int S;   // footprint window (max_support)
+  int W;   // sub-grid edge, TILE + S - 1
+};
+
+__global__ void __launch_bounds__(MT_THREADS, 1) k_mosaic_tiled(MosaicTiledArgs t) {
+  const MosaicArgs &a = t.m;
+  extern __shared__ __align__(16) unsigned char smem[];
+  // real and imaginary planes [apol][W * W]: a warp's 8-byte atomics along a
+  // window row fall on consecutive banks
+  const int W = t.W, npg = (int)a.n_img_pol;
+  const int sub_n = npg * W * W;
+  double *sre = (double *)smem;
+  double *sim = sre + sub_n;
+  __shared__ int s_chunk;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const uint32_t n_rec = *t.n_rec;
+  const int64_t n_chunks = ((int64_t)n_rec + t.chunk - 1) / t.chunk;
+  const uint32_t nchan = (uint32_t)a.nchan, nb = (uint32_t)a.nb;
+  for (int i0 = 0; i0 < sub_n; i0 += MT_THREADS) {
+    const int i = i0 + threadIdx.x;
+    if (i < sub_n) {
+      sre[i] = 0.0;
+      sim[i] = 0.0;
+    }
+  }
+  for (;;) {
+    __syncthreads();  // sub-grid clear; previous s_chunk consumed
+    if (threadIdx.x == 0) s_chunk = (int)atomicAdd(&t.sched[0], 1u);
+    __syncthreads();
+    const int64_t ch = s_chunk;
+    if (ch >= n_chunks) break;
+    const uint32_t r0 = (uint32_t)(ch * t.chunk);
+    const uint32_t r1 = (uint32_t)min((int64_t)n_rec, (int64_t)r0 + t.chunk);
+    int64_t lo = 0, hi = t.n_tiles;  // tile holding r0
+    while (hi - lo > 1) {
+      const int64_t mid = (lo + hi) >> 1;
+      if (t.tile_start[mid] <= r0) lo = mid; else hi = mid;
+    }
+    int64_t tile = lo;
+    uint32_t seg_lo = r0;
+    while (seg_lo < r1) {
+      const uint32_t t_end = t.tile_start[tile + 1];
+      const uint32_t seg_hi = min(r1, t_end);
+      if (seg_hi <= seg_lo) {
+        ++tile;
+        continue;
+      }
+      const int64_t plane = tile / (t.ntu * t.ntv);
+      const int64_t trem = tile - plane * t.ntu * t.ntv;
+      const int tu = (int)(trem / t.ntv), tv = (int)(trem - (int64_t)tu * t.ntv);
+      double swacc[4] = {0.0, 0.0, 0.0, 0.0};
+      // one trip count per block: every warp reaches the barrier converged
+      for (uint32_t rb = seg_lo; rb < seg_hi; rb += MT_WARPS) {
+        const uint32_t r = rb + warp;
+        if (r >= seg_hi) continue;
+        const Rec rc = t.recs[r];
+        const int64_t row = rc.row;
+        const uint32_t tb = rc.row / nchan;  // rows fit 32 bits (the plan checks)
+        const uint32_t c = rc.row - tb * nchan;
+        const uint32_t b = tb % nb;
+        const int cfb = a.cfb_map[b], cfc = a.cfc_map[c];
+        if (cfb < 0 || cfb >= a.n_cfb || cfc < 0 || cfc >= a.n_cfc) continue;
+        const long long uo = (long long)rc.ou - 128 + a.cu / 2;
+        const long long vo = (long long)rc.ov - 128 + a.cv / 2;
+        const int cu0 = rc.du + t.S / 2, cv0 = rc.dv + t.S / 2;  // centre in the sub-grid
+        for (int64_t p = 0; p < a.npol; ++p) {
+          const int64_t k = row * a.npol + p;
+          const double w = a.wt[k];
+          double2 wd;
+          if (a.do_psf) wd = make_double2(w, 0.0);
+          else {
+            const double2 vv = a.vis[k];
+            wd = make_double2(__dmul_rn(vv.x, w), __dmul_rn(vv.y, w));
+          }
+          if (isnan(wd.x) || isnan(wd.y) || (wd.x == 0.0 && wd.y == 0.0)) continue;
+          const int cfp = a.cfp_map[p], apol = a.pol_map[p];
+          if (cfp < 0 || cfp >= a.n_cfp || apol < 0 || apol >= npg) continue;
+          const int64_t fidx = ((int64_t)cfb * a.n_cfc + cfc) * a.n_cfp + cfp;
+          const int su = a.support[2 * fidx], sv = a.support[2 * fidx + 1];
+          // a window larger than the footprint the plan reserved would leave
+          // the sub-grid: such functions are skipped (the host passes
+          // max_support = np.max(support))
+          if (su < 1 || sv < 1 || su > t.S || sv > t.S) continue;
+          const double2 *f = a.cf + fidx * a.cu * a.cv;
+          double *pre = sre + (size_t)apol * W * W, *pim = sim + (size_t)apol * W * W;
+          // lanes along the window's v (contiguous) axis: lane = ir * sv + jv,
+          // 32 / sv u-rows per pass
+          const unsigned usv = (unsigned)sv;
+          const int rp = (int)(32u / usv);
+          const int ir = (int)((unsigned)lane / usv);
+          const int iv = -(sv / 2) + (lane - ir * sv);
+          const long long fv = (long long)a.os_v * iv + vo;
+          const bool v_ok = ir < rp && fv >= 0 && fv < a.cv;
+          double2 norm = make_double2(0.0, 0.0);
+          for (int iu0 = 0; iu0 < su; iu0 += rp) {
+            const int iui = iu0 + ir;
+            if (!v_ok || iui >= su) continue;
+            const int iu = -(su / 2) + iui;
+            const long long fu = (long long)a.os_u * iu + uo;
+            if (fu < 0 || fu >= a.cu) continue;
+            const double2 conv = __ldg(f + fu * a.cv + fv);
+            const double2 x = cmul(conv, wd);
+            const int cell = (cu0 + iu) * W + (cv0 + iv);
+            atomicAdd(pre + cell, x.x);
+            atomicAdd(pim + cell, x.y);
+            norm.x += conv.x;
+            norm.y += conv.y;
+          }
+          for (int off = 16; off > 0; off >>= 1) {
+            norm.x += __shfl_down_sync(0xffffffffu, norm.x, off);
+            norm.y += __shfl_down_sync(0xffffffffu, norm.y, off);
+          }
+          const double re = a.do_psf ? norm.x
+                                     : __dsub_rn(__dmul_rn(norm.x, norm.x),
+                                                 __dmul_rn(norm.y, norm.y));
+#pragma unroll
+          for (int q = 0; q < 4; ++q)
+            if (q == apol) swacc[q] += __dmul_rn(w, re);
+        }
+      }
+      if (lane == 0 && a.sumw)
+        for (int q = 0; q < npg && q < 4; ++q)
+          if (swacc[q] != 0.0) atomicAdd(&a.sumw[plane * npg + q], swacc[q]);
+      __syncthreads();
+      // flush the segment's sub-grid to the global grid and clear it
+      for (int i0 = 0; i0 < sub_n; i0 += MT_THREADS) {
+        const int i = i0 + threadIdx.x;
+        if (i >= sub_n) continue;
+        const double vr = sre[i], vi = sim[i];
+        if (vr == 0.0 && vi == 0.0) continue;
+        const int gp = i / (W * W);
+        const int cell = i - gp * W * W;
+        const int iu = cell / W, iv = cell - iu * W;
+        const int64_t gu = (int64_t)tu * TILE + iu, gv = (int64_t)tv * TILE + iv;
+        double2 *gd = a.grid + ((plane * npg + gp) * a.n_u + gu) * a.n_v + gv;
+        atomicAdd(&gd->x, vr);
+        atomicAdd(&gd->y, vi);
+        sre[i] = 0.0;
+        sim[i] = 0.0;
+      }
+      seg_lo = seg_hi;
+      if (seg_hi == t_end) ++tile;
+    }
+  }
+  if (threadIdx.x == 0) {
+    __threadfence();
+    if (atomicAdd(&t.sched[1], 1u) == gridDim.x - 1) {
+      t.sched[0] = 0u;
+      t.sched[1] = 0u;
+      __threadfence();
+    }
+  }
+}
+
+static size_t mosaic_tiled_smem(int S, int64_t n_img_pol) {
+  const int W = TILE + S - 1;
+  return (size_t)W * W * (size_t)n_img_pol * sizeof(double2);
+}
+
+static int mosaic_geom(PlanGeom &g, Plan &p, int64_t n_u, int64_t n_v, int max_support,
+                       int os, int64_t nt, int64_t nb, int64_t nchan, int64_t n_img_chan,
+                       void *workspace, size_t workspace_bytes, const char *who) {
+  AV_CHECK_ARG(max_support >= 1 && max_support <= 32, "%s: max_support must be in [1, 32]",
+               who);
+  AV_CHECK_ARG(os >= 1 && os <= 254, "%s: oversampling must be in [1, 254]", who);
+  AV_CHECK_ARG(n_u > 2 * max_support && n_v > 2 * max_support && n_u < 131072 &&
+                   n_v < 131072,
+               "%s: grid size out of range", who);
+  AV_CHECK_ARG(nt >= 0 && nb >= 0 && nchan >= 0 && n_img_chan >= 1, "%s: bad shape", who);
+  AV_CHECK_ARG(workspace && (((uintptr_t)workspace) & 255) == 0,
+               "%s: workspace must be 256-byte aligned", who);
+  plan_geometry(g, nt, nb, nchan, n_img_chan, n_u, n_v, max_support, os);
+  g.margin = max_support;
+  g.convention = 0;
+  g.chk_x = g.chk_y = 0;
+  g.scale0 = g.scale1 = g.offset0 = g.offset1 = 0.0;
+  const size_t need = plan_workspace_bytes(g);
+  if (workspace_bytes < need) {
+    set_error("%s: workspace %zu bytes < %zu needed", who, workspace_bytes, need);
+    return AV_ERR_WORKSPACE;
+  }
+  Workspace ws(workspace, workspace_bytes);
+  if (!plan_carve(g, ws, p)) {
+    set_error("%s: workspace carve failed", who);
+    return AV_ERR_WORKSPACE;
+  }
+  return AV_OK;
+}
+
 static unsigned mg_blocks(int64_t n_items, int per_block) {
   int64_t b = (n_items + per_block - 1) / per_block;
   const int64_t cap = (int64_t)sm_count() * 32;
@@ -420,6 +627,79 @@ int av_mosaic_grid(AV_MOSAIC_PARAMS, void *stream) {
               conv_u, conv_v, support, max_support, n_u, n_v, delta_l, delta_m, os_u, os_v, nt,
               nb, nchan, npol, n_img_chan, n_img_pol);
   k_mosaic_grid<<<mg_blocks(rows, MG_THREADS / 32), MG_THREADS, 0, as_stream(stream)>>>(a);
+  AV_LAUNCH_CHECK();
+  return AV_OK;
+}
+
+size_t av_mosaic_tiled_workspace_size(int64_t nt, int64_t nb, int64_t nchan, int64_t n_u,
+                                      int64_t n_v, int64_t n_img_chan, int max_support) {
+  PlanGeom g;
+  plan_geometry(g, nt, nb, nchan, n_img_chan, n_u, n_v, max_support < 1 ? 1 : max_support,
+                100);
+  return plan_workspace_bytes(g);
+}
+
+int av_mosaic_tiled_plan(const double *uvw, const double *freq, const int32_t *chan_map,
+                         int64_t n_u, int64_t n_v, double delta_l, double delta_m,
+                         int max_support, int oversampling, int64_t nt, int64_t nb,
+                         int64_t nchan, int64_t n_img_chan, void *workspace,
+                         size_t workspace_bytes, void *stream) {
+  clear_error();
+  AV_CHECK_ARG(uvw && freq && chan_map, "av_mosaic_tiled_plan: null pointer");
+  PlanGeom g;
+  Plan p;
+  int rc = mosaic_geom(g, p, n_u, n_v, max_support, oversampling, nt, nb, nchan, n_img_chan,
+                       workspace, workspace_bytes, "av_mosaic_tiled_plan");
+  if (rc) return rc;
+  return plan_build(g, p, uvw, freq, chan_map, delta_l, delta_m, as_stream(stream));
+}
+
+int av_mosaic_tiled_execute(AV_MOSAIC_PARAMS, void *workspace, size_t workspace_bytes,
+                            void *stream) {
+  clear_error();
+  int rc = check_mosaic("av_mosaic_tiled_execute", grid, sum_weight, do_psf, vis, weight, uvw,
+                        freq, chan_map, pol_map, cf_baseline_map, cf_chan_map, cf_pol_map, cf,
+                        n_cf_baseline, n_cf_chan, n_cf_pol, conv_u, conv_v, support,
+                        max_support, n_u, n_v, delta_l, delta_m, os_u, os_v, nt, nb, nchan,
+                        npol, n_img_chan, n_img_pol);
+  if (rc) return rc;
+  AV_CHECK_ARG(os_u == os_v, "av_mosaic_tiled_execute: oversampling must be the same on u, v");
+  AV_CHECK_ARG(n_img_pol <= 4, "av_mosaic_tiled_execute: at most 4 image polarisations");
+  const size_t smem = mosaic_tiled_smem(max_support, n_img_pol);
+  AV_CHECK_ARG(smem <= 220 * 1024,
+               "av_mosaic_tiled_execute: sub-grid of %zu bytes exceeds shared memory", smem);
+  PlanGeom g;
+  Plan p;
+  rc = mosaic_geom(g, p, n_u, n_v, max_support, os_u, nt, nb, nchan, n_img_chan, workspace,
+                   workspace_bytes, "av_mosaic_tiled_execute");
+  if (rc) return rc;
+  const int64_t rows = nt * nb * nchan;
+  if (rows == 0 || npol == 0) return AV_OK;
+  MosaicTiledArgs t;
+  fill_mosaic(t.m, grid, sum_weight, do_psf, vis, weight, uvw, freq, chan_map, pol_map,
+              cf_baseline_map, cf_chan_map, cf_pol_map, cf, n_cf_baseline, n_cf_chan, n_cf_pol,
+              conv_u, conv_v, support, max_support, n_u, n_v, delta_l, delta_m, os_u, os_v, nt,
+              nb, nchan, npol, n_img_chan, n_img_pol);
+  t.recs = p.recs;
+  t.tile_start = p.tile_start;
+  t.n_rec = p.offs + g.n_keys();
+  t.sched = p.counters;
+  t.n_tiles = g.n_tiles();
+  t.ntu = g.ntu;
+  t.ntv = g.ntv;
+  t.S = max_support;
+  t.W = TILE + max_support - 1;
+  const int sms = sm_count();
+  int64_t chunk = (rows + (int64_t)sms * 16 - 1) / ((int64_t)sms * 16);
+  if (chunk < 1024) chunk = 1024;
+  t.chunk = chunk;
+  int64_t nblocks = (rows + chunk - 1) / chunk;
+  if (nblocks > sms) nblocks = sms;
+  if (nblocks < 1) nblocks = 1;
+  if (smem > 48 * 1024)
+    AV_CUDA(cudaFuncSetAttribute(k_mosaic_tiled, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)smem));
+  k_mosaic_tiled<<<(unsigned)nblocks, MT_THREADS, smem, as_stream(stream)>>>(t);
   AV_LAUNCH_CHECK();
   return AV_OK;
 }

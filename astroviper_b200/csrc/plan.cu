@@ -46,8 +46,8 @@ __device__ __forceinline__ uint32_t sample_key(const PlanGeom &g, double um, dou
   if (plane < 0 || plane >= g.n_planes) return skip;
   int fu, fv, ou, ov;
   const bool ok = g.convention == 0
-                      ? sample_pos_grid(um, vm, us0, us1, g.n_u, g.n_v, g.support, g.os, fu, fv,
-                                        ou, ov)
+                      ? sample_pos_grid(um, vm, us0, us1, g.n_u, g.n_v, g.support, g.os,
+                                        g.margin, fu, fv, ou, ov)
                       : sample_pos_degrid(um, vm, f, g, fu, fv, ou, ov);
   if (!ok) return skip;
   // fu, fv >= 0 here

@@ -42,6 +42,10 @@ struct PlanGeom {
   int64_t kpt;               // keys per tile
   int res_shift;             // log2(R)
   int support, os;
+  // gridder convention: a sample is kept when its centre cell is at least
+  // `margin` cells from both grid edges (support / 2 for standard_grid_jit;
+  // np.max(weight_support) for mosaic_grid_jit, mosaic_grid.py:398-403)
+  int margin;
   int convention;            // 0 = gridder (standard_grid.py), 1 = degridder
   // degridder only: the reference's own bounds extents and the scale/offset
   int64_t chk_x, chk_y;      // nx = shape[3], ny = shape[2] (standard_degrid.py:407)
@@ -68,6 +72,7 @@ inline void plan_geometry(PlanGeom &g, int64_t nt, int64_t nb, int64_t nchan,
   g.ntv = (span_v + TILE - 1) / TILE;
   g.support = support;
   g.os = os;
+  g.margin = support / 2;
   g.res_shift = 0;
   while (g.res_shift < 5 &&
          g.n_planes * g.ntu * g.ntv * ((int64_t)(TILE >> g.res_shift) * (TILE >> g.res_shift)) >
@@ -109,14 +114,15 @@ struct Plan {
 // 297-352): returns false when it is skipped.  fu/fv = first footprint cell.
 __device__ __forceinline__ bool sample_pos_grid(double um, double vm, double us0, double us1,
                                                 int64_t n_u, int64_t n_v, int support, int os,
-                                                int &fu, int &fv, int &offu, int &offv) {
+                                                int margin, int &fu, int &fv, int &offu,
+                                                int &offv) {
   double u = __dmul_rn(um, us0), v = __dmul_rn(vm, us1);
   if (isnan(u) || isnan(v)) return false;
   double u_pos = __dadd_rn(u, (double)(n_u / 2));
   double v_pos = __dadd_rn(v, (double)(n_v / 2));
   long long ui = trunc_ll(__dadd_rn(u_pos, 0.5)), vi = trunc_ll(__dadd_rn(v_pos, 0.5));
-  long long sc = support / 2;
-  if (!((ui + sc < n_u) && (vi + sc < n_v) && (ui - sc >= 0) && (vi - sc >= 0))) return false;
+  const long long sc = support / 2, mg = margin;
+  if (!((ui + mg < n_u) && (vi + mg < n_v) && (ui - mg >= 0) && (vi - mg >= 0))) return false;
   double uo = __dsub_rn((double)ui, u_pos), vo = __dsub_rn((double)vi, v_pos);
   offu = (int)floor(__dadd_rn(__dmul_rn(uo, (double)os), 0.5));
   offv = (int)floor(__dadd_rn(__dmul_rn(vo, (double)os), 0.5));

@@ -438,6 +438,33 @@ int av_mosaic_grid(void *grid, double *sum_weight, int do_psf, const void *vis,
                    int64_t nchan, int64_t npol, int64_t n_img_chan, int64_t n_img_pol,
                    void *stream);
 
+/* Binned mosaic gridding, the same sums as av_mosaic_grid: _plan bins the
+ * samples (cells and kernel offsets, the mosaic's edge margin of
+ * max_support cells) into the workspace, _execute grids with that plan; a
+ * persistent CTA per SM keeps an FP64 sub-grid per tile in shared memory.
+ * Needs max_support <= 32 (the largest window; support entries above it are
+ * skipped), os_u == os_v <= 254, n_img_pol <= 4 and
+ * (31 + max_support)^2 x n_img_pol x 16 bytes of shared memory <= 220 KiB.
+ * Executes on one plan must not overlap (stream order is enough). */
+size_t av_mosaic_tiled_workspace_size(int64_t nt, int64_t nb, int64_t nchan, int64_t n_u,
+                                      int64_t n_v, int64_t n_img_chan, int max_support);
+int av_mosaic_tiled_plan(const double *uvw, const double *freq, const int32_t *chan_map,
+                         int64_t n_u, int64_t n_v, double delta_l, double delta_m,
+                         int max_support, int oversampling, int64_t nt, int64_t nb,
+                         int64_t nchan, int64_t n_img_chan, void *workspace,
+                         size_t workspace_bytes, void *stream);
+int av_mosaic_tiled_execute(void *grid, double *sum_weight, int do_psf, const void *vis,
+                            const double *weight, const double *uvw, const double *freq,
+                            const int32_t *chan_map, const int32_t *pol_map,
+                            const int32_t *cf_baseline_map, const int32_t *cf_chan_map,
+                            const int32_t *cf_pol_map, const void *cf, int64_t n_cf_baseline,
+                            int64_t n_cf_chan, int64_t n_cf_pol, int64_t conv_u, int64_t conv_v,
+                            const int32_t *support, int max_support, int64_t n_u, int64_t n_v,
+                            double delta_l, double delta_m, int os_u, int os_v, int64_t nt,
+                            int64_t nb, int64_t nchan, int64_t npol, int64_t n_img_chan,
+                            int64_t n_img_pol, void *workspace, size_t workspace_bytes,
+                            void *stream);
+
 /* aperture_grid_jit (mosaic_grid.py:13-153): every sample that passes the
  * grid-edge test adds weight x its function window at the grid centre
  * (and weight x Re(norm) to sum_weight); the weights are summed per
