@@ -102,8 +102,8 @@ __global__ void k_pswf_kernel4d(double *out, int os, int support, int n_os) {
 }
 
 // ------------------------------------------------------------ tuning ---
-constexpr int kTuneKnobs = 2;
-static std::atomic<int64_t> g_tune[kTuneKnobs] = {{16}, {16}};
+constexpr int kTuneKnobs = 3;
+static std::atomic<int64_t> g_tune[kTuneKnobs] = {{16}, {16}, {AV_GRID_LANES_MMA}};
 
 int64_t tune_value(int knob) {
   return (knob >= 0 && knob < kTuneKnobs) ? g_tune[knob].load() : 0;
@@ -127,6 +127,9 @@ int av_tune_set(int knob, int64_t value) {
   clear_error();
   AV_CHECK_ARG(knob >= 0 && knob < kTuneKnobs, "av_tune_set: unknown knob %d", knob);
   AV_CHECK_ARG(value >= 1 && value <= 1024, "av_tune_set: value %lld outside [1, 1024]",
+               (long long)value);
+  AV_CHECK_ARG(knob != AV_TUNE_GRID_LANES || value <= 2,
+               "av_tune_set: AV_TUNE_GRID_LANES takes 1 (mma) or 2 (rows), not %lld",
                (long long)value);
   g_tune[knob].store(value);
   return AV_OK;

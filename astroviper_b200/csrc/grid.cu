@@ -6,11 +6,14 @@
 //   visibilities and weights, accumulating in FP64.  Persistent CTAs (one
 //   per SM) take chunks of records; per tile segment a CTA keeps a
 //   (T+S-1)^2 x npg FP64 complex sub-grid in shared memory.  Each warp
-//   streams a slice of the segment one sample at a time; each lane owns a
-//   footprint row x polarisation x column range and keeps its accumulators
-//   in registers while the samples stay in one cell, flushing to the
-//   sub-grid only on a cell change.  The sub-grid goes to the global grid
-//   once per segment.
+//   streams a slice of the segment and keeps its accumulators in registers
+//   while the samples stay in one cell, flushing to the sub-grid only on a
+//   cell change: for supports up to 8 as FP64 tensor-core tiles
+//   (mma.sync.m16n8k4.f64, four samples per step), otherwise with each
+//   lane owning a footprint row x polarisation x column range (DFMA).  The
+//   sub-grid goes to the global grid once per segment.
+#include <type_traits>
+
 #include "plan.cuh"
 
 namespace av {
@@ -179,32 +182,51 @@ struct TiledGridArgs {
   const uint8_t *flag;      // may be NULL
 };
 
-// Thread mapping.  Each warp streams its own contiguous slice of a tile
-// segment's cell-sorted samples, one sample at a time for the whole warp, so
-// a change of cell (and the flush of the accumulators it triggers) is the
-// same for every lane of the warp.  A lane owns footprint row g,
-// polarisations [pg*PPL, pg*PPL+PPL) and footprint columns [cc*KC, cc*KC+KC)
-// and keeps PPL x KC FP64 complex accumulators in registers for a whole run
-// of samples in one cell (median ~70 on the 33M workload).  Per sample and
-// lane: 2 PPL DMUL (row tap x value) and 2 PPL KC DFMA.
+// Lane mappings.  Each warp streams its own contiguous slice of a tile
+// segment's cell-sorted samples, a whole run of samples in one cell (median
+// ~70 on the 33M workload) at a time, so a change of cell (and the flush of
+// the accumulators it triggers) is the same for every lane of the warp.  The
+// accumulators stay in registers for the run and go to the shared sub-grid
+// only on a cell change.  Two mappings of the run's footprint sums onto the
+// lanes:
 //
-// For supports up to 8 each quarter-warp is one (polarisation group, column
-// chunk) block and its lanes are the rows (lane = block * 8 + g): every
-// quarter then reads one address for the staged value and for the column
-// taps, which shared memory serves at its broadcast rate (2 wavefronts per
-// 16-byte load, against 4 when a quarter reads several addresses).  Support
-// 7 with 4 polarisations: 4 quarters x 7 rows, 7 accumulators per lane.
+// RowLanes (supports 3-9).  A lane owns footprint row g, polarisations
+// [pg*PPL, pg*PPL+PPL) and footprint columns [cc*KC, cc*KC+KC) and keeps
+// PPL x KC FP64 complex accumulators.  Per sample and lane: 2 PPL DMUL (row
+// tap x value) and 2 PPL KC DFMA.  For supports up to 8 each quarter-warp is
+// one (polarisation group, column chunk) block and its lanes are the rows
+// (lane = block * 8 + g): every quarter then reads one address for the
+// staged value and for the column taps, which shared memory serves at its
+// broadcast rate.  Support 7 with 4 polarisations: 4 quarters x 7 rows, 7
+// accumulators per lane.
+//
+// MmaLanes (supports 3-8).  A run's footprint sums are a matrix product,
+//   acc[p](ri, r, c) += sum over samples k of (ri(v_k[p]) cu_k[r]) cv_k[c],
+// with ri the real or imaginary part, cu / cv the row / column taps.  Per
+// group of four samples of a run and per polarisation, one FP64
+// mma.sync.m16n8k4: A (16 x 4) holds the real parts' row taps in rows 0-7
+// and the imaginary parts' in rows 8-15, B (4 x 8) the column taps, D
+// (16 x 8) the 8 x 8 footprint of both planes (taps past the support are
+// zero in the table).  With lane = 4 g + t the fragments are a0 = A[g][t],
+// a1 = A[g + 8][t], b0 = B[t][g], d = D[g][2t, 2t + 1], D[g + 8][2t, 2t + 1]:
+// lane (g, t) reads sample t of the group, row tap g and column tap g, and
+// owns cells (g, 2t) and (g, 2t + 1).  Each product is an FP64 multiply-add,
+// as a DFMA is; a group's four are summed in the tensor core's order.  Per
+// group and lane: 2 tap loads, NPOL staged values, 2 NPOL DMUL and NPOL mma
+// (about a quarter of RowLanes' instructions and shared-memory wavefronts
+// per sample, for 512 instead of 392 multiply-adds at the FP64 rate).
 //
 // The warp's lanes first stage 32 samples (one each: FP64 weighted values,
 // cell key, tap-table row offsets) into the warp's shared staging area; the
 // next round's values and the record of the round after are in flight while
 // a round is computed.
-template <int S, int NPOL>
+template <int S, int NPOL, bool MMA = false>
 struct GCfg {
   // one CTA per SM; as many warps as the registers allow without spilling
-  static constexpr int THREADS = (S >= 9 && NPOL == 4) ? 384 : 512;
+  static constexpr int THREADS = (!MMA && S >= 9 && NPOL == 4) ? 384 : 512;
   static constexpr int WARPS = THREADS / 32;
   static constexpr int W = TILE + S - 1;                          // sub-grid edge
+  // RowLanes' split of (polarisation, row, column) over the lanes
   static constexpr bool QUARTERS = S <= 8;                         // lane = block * 8 + g
   static constexpr int PPL = QUARTERS ? (NPOL <= 4 ? 1 : 2)
                                       : (S * NPOL <= 32 ? 1 : (S * NPOL <= 64 ? 2 : 4));
@@ -219,7 +241,8 @@ struct GCfg {
   static constexpr int KCE = PAIRS ? ((KC + 1) & ~1) : KC;         // taps addressed
   static constexpr int RT0 = (NCC - 1) * KC + KCE;
   static constexpr int RT = ((RT0 > S ? RT0 : S) + 1) & ~1;        // taps per table row
-  static constexpr int RWP = (RT % 4 == 0) ? RT + 2 : RT;          // row stride (banks)
+  // table row stride (banks); MmaLanes reads taps 0-7 of a row
+  static constexpr int RWP = MMA ? 10 : ((RT % 4 == 0) ? RT + 2 : RT);
   static constexpr size_t tab_bytes = 256 * RWP * sizeof(double);
   static constexpr size_t rs_bytes = 256 * sizeof(double);
   // staged values: [pol][sample] with a 33-entry stride, so the 32 lanes'
@@ -240,6 +263,7 @@ struct GCfg {
   static size_t total(int npg) { return off_sub + sub_bytes(npg); }
   static_assert(QUARTERS ? BLOCKS <= 4 : S * BLOCKS <= 32, "lane mapping");
   static_assert(NPGL * PPL == NPOL, "polarisation split");
+  static_assert(!MMA || (S <= 8 && RWP >= 8), "one 8 x 8 footprint per polarisation");
 };
 
 // Per-offset tap tables: tab[(o + 128) * RWP + i] = cgk[|os * (i - S/2) + o|]
@@ -323,37 +347,182 @@ __device__ __forceinline__ void prefetch(Pref<NPOL> &f, const TiledGridArgs &a, 
   }
 }
 
-// Adds a lane's accumulators of one run (cell key: du | dv << 8) to the
-// shared sub-grid (real plane sre, imaginary plane sim) and clears them.
-// Columns past the support are padding.
-template <int S, int RS, int PS, int PPL, int KC>
-__device__ __forceinline__ void grid_flush(double2 (&acc)[PPL][KC], double *sre, double *sim,
-                                           int key, int g, int c0, const int (&ipm)[PPL],
-                                           bool owner) {
-  const int du = key & 255, dv = (key >> 8) & 255;
-  const int base = (du + g) * RS + dv + c0;
+template <int S, int NPOL>
+struct RowLanes {
+  using C = GCfg<S, NPOL, false>;
+  static constexpr int PPL = C::PPL, KC = C::KC, KCE = C::KCE;
+  double2 acc[PPL][KC];
+  int g, pg, c0;
+  bool owner;
+  int ipm[PPL];  // this lane's image polarisations (-1: none)
+
+  // lanes without a role repeat a valid one (no divergent compute) but
+  // never flush
+  __device__ __forceinline__ void setup(int lane, const int (&pm)[NPOL]) {
+    int blk;
+    if (C::QUARTERS) {
+      g = lane & 7;
+      blk = lane >> 3;
+      owner = g < S && blk < C::BLOCKS;
+      g = g < S ? g : S - 1;
+      blk = blk < C::BLOCKS ? blk : 0;
+    } else {
+      owner = lane < C::LANES;
+      const int li = lane % C::LANES;
+      g = li % S;
+      blk = li / S;
+    }
+    pg = blk / C::NCC;
+    c0 = (blk % C::NCC) * KC;
 #pragma unroll
-  for (int pp = 0; pp < PPL; ++pp) {
+    for (int pp = 0; pp < PPL; ++pp) {
+      ipm[pp] = -1;
 #pragma unroll
-    for (int k = 0; k < KC; ++k) {
-      const double2 v = acc[pp][k];
-      if (owner && ipm[pp] >= 0 && c0 + k < S && (v.x != 0.0 || v.y != 0.0)) {
-        const int e = ipm[pp] * PS + base + k;
-        atomicAdd(sre + e, v.x);
-        atomicAdd(sim + e, v.y);
+      for (int p = 0; p < NPOL; ++p)
+        if (p == pg * PPL + pp) ipm[pp] = pm[p];
+    }
+    clear();
+  }
+
+  __device__ __forceinline__ void clear() {
+#pragma unroll
+    for (int pp = 0; pp < PPL; ++pp)
+#pragma unroll
+      for (int k = 0; k < KC; ++k) acc[pp][k] = make_double2(0.0, 0.0);
+  }
+
+  // Adds the run's accumulators (cell key: du | dv << 8) to the shared
+  // sub-grid (real plane sre, imaginary plane sim) and clears them.
+  // Columns past the support are padding.
+  __device__ __forceinline__ void flush(double *sre, double *sim, int key) {
+    const int du = key & 255, dv = (key >> 8) & 255;
+    const int base = (du + g) * C::RS + dv + c0;
+#pragma unroll
+    for (int pp = 0; pp < PPL; ++pp) {
+#pragma unroll
+      for (int k = 0; k < KC; ++k) {
+        const double2 v = acc[pp][k];
+        if (owner && ipm[pp] >= 0 && c0 + k < S && (v.x != 0.0 || v.y != 0.0)) {
+          const int e = ipm[pp] * C::PS + base + k;
+          atomicAdd(sre + e, v.x);
+          atomicAdd(sim + e, v.y);
+        }
+        acc[pp][k] = make_double2(0.0, 0.0);
       }
-      acc[pp][k] = make_double2(0.0, 0.0);
     }
   }
+
+  // Staged samples [j, j1) of the current round, all in the current cell.
+  __device__ __forceinline__ void run(int j, int j1, const double2 *wd, const int *wm,
+                                      const double *tab) {
+    for (; j < j1; ++j) {
+      const int ro = wm[j];
+      const double cu = tab[(ro & 0xffff) + g];
+      const double *cvp = tab + (ro >> 16) + c0;
+      double cv[KCE];
+      if (C::PAIRS) {
+#pragma unroll
+        for (int k = 0; k + 1 < KC; k += 2) {
+          const double2 c2 = *(const double2 *)(cvp + k);
+          cv[k] = c2.x;
+          cv[k + 1] = c2.y;
+        }
+        if (KC % 2) cv[KC - 1] = cvp[KC - 1];
+      } else {
+#pragma unroll
+        for (int k = 0; k < KC; ++k) cv[k] = cvp[k];
+      }
+#pragma unroll
+      for (int pp = 0; pp < PPL; ++pp) {
+        const double2 d = wd[(pg * PPL + pp) * C::SDS + j];
+        const double tr = cu * d.x, ti = cu * d.y;
+#pragma unroll
+        for (int k = 0; k < KC; ++k) {
+          acc[pp][k].x = fma(cv[k], tr, acc[pp][k].x);
+          acc[pp][k].y = fma(cv[k], ti, acc[pp][k].y);
+        }
+      }
+    }
+  }
+};
+
+// D += A B for one m16n8k4 FP64 tile (fragment layout above).
+__device__ __forceinline__ void mma_f64_m16n8k4(double (&d)[4], double a0, double a1,
+                                                double b0) {
+  asm("mma.sync.aligned.m16n8k4.row.col.f64.f64.f64.f64 {%0,%1,%2,%3}, {%4,%5}, {%6}, "
+      "{%0,%1,%2,%3};\n"
+      : "+d"(d[0]), "+d"(d[1]), "+d"(d[2]), "+d"(d[3])
+      : "d"(a0), "d"(a1), "d"(b0));
 }
+
+template <int S, int NPOL>
+struct MmaLanes {
+  using C = GCfg<S, NPOL, true>;
+  double acc[NPOL][4];  // per polarisation: re (g, 2t), re (g, 2t+1), im (g, 2t), im (g, 2t+1)
+  int g, t;
+  int ipm[NPOL];
+
+  __device__ __forceinline__ void setup(int lane, const int (&pm)[NPOL]) {
+    g = lane >> 2;
+    t = lane & 3;
+#pragma unroll
+    for (int p = 0; p < NPOL; ++p) ipm[p] = pm[p];
+    clear();
+  }
+
+  __device__ __forceinline__ void clear() {
+#pragma unroll
+    for (int p = 0; p < NPOL; ++p) acc[p][0] = acc[p][1] = acc[p][2] = acc[p][3] = 0.0;
+  }
+
+  // Rows and columns past the support hold zeros (zero taps) and are skipped.
+  __device__ __forceinline__ void flush(double *sre, double *sim, int key) {
+    const int du = key & 255, dv = (key >> 8) & 255;
+    const int base = (du + g) * C::RS + dv + 2 * t;
+#pragma unroll
+    for (int p = 0; p < NPOL; ++p) {
+#pragma unroll
+      for (int q = 0; q < 2; ++q) {
+        const double re = acc[p][q], im = acc[p][2 + q];
+        if (ipm[p] >= 0 && g < S && 2 * t + q < S && (re != 0.0 || im != 0.0)) {
+          const int e = ipm[p] * C::PS + base + q;
+          atomicAdd(sre + e, re);
+          atomicAdd(sim + e, im);
+        }
+      }
+    }
+    clear();
+  }
+
+  // Staged samples [j, j1) of the current round, all in the current cell, in
+  // groups of four; a short last group has zero A columns for its empty
+  // slots (which then read a valid sample's taps).
+  __device__ __forceinline__ void run(int j, int j1, const double2 *wd, const int *wm,
+                                      const double *tab) {
+    for (; j < j1; j += 4) {
+      const bool kv = j + t < j1;
+      const int s = kv ? j + t : j;
+      const int ro = wm[s];
+      const double cu = tab[(ro & 0xffff) + g];
+      const double cv = tab[(ro >> 16) + g];
+#pragma unroll
+      for (int p = 0; p < NPOL; ++p) {
+        const double2 d = wd[p * C::SDS + s];
+        mma_f64_m16n8k4(acc[p], kv ? cu * d.x : 0.0, kv ? cu * d.y : 0.0, cv);
+      }
+    }
+  }
+};
 
 // Persistent: one CTA per SM takes chunks of records from a.sched[0] until
 // none are left; the last CTA to finish sets both counters back to zero for
 // the next launch on the same plan.
-template <int S, int NPOL>
-__global__ void __launch_bounds__(GCfg<S, NPOL>::THREADS, 1) k_grid_tiled(TiledGridArgs a) {
-  using C = GCfg<S, NPOL>;
-  constexpr int W = C::W, KC = C::KC, KCE = C::KCE, RWP = C::RWP, PPL = C::PPL;
+template <int S, int NPOL, bool MMA>
+__global__ void __launch_bounds__(GCfg<S, NPOL, MMA>::THREADS, 1)
+    k_grid_tiled(TiledGridArgs a) {
+  using C = GCfg<S, NPOL, MMA>;
+  using Lanes = typename std::conditional<MMA, MmaLanes<S, NPOL>, RowLanes<S, NPOL>>::type;
+  constexpr int W = C::W, RWP = C::RWP;
   extern __shared__ __align__(16) unsigned char smem[];
   double *tab = (double *)smem;
   double *rs = (double *)(smem + C::off_rs);
@@ -378,24 +547,6 @@ __global__ void __launch_bounds__(GCfg<S, NPOL>::THREADS, 1) k_grid_tiled(TiledG
   }
 
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  // lane roles; lanes without one repeat a valid role (no divergent
-  // compute) but never flush
-  int g, blk;
-  bool owner;
-  if (C::QUARTERS) {
-    g = lane & 7;
-    blk = lane >> 3;
-    owner = g < S && blk < C::BLOCKS;
-    g = g < S ? g : S - 1;
-    blk = blk < C::BLOCKS ? blk : 0;
-  } else {
-    owner = lane < C::LANES;
-    const int li = lane % C::LANES;
-    g = li % S;
-    blk = li / S;
-  }
-  const int pg = blk / C::NCC;
-  const int c0 = (blk % C::NCC) * KC;
   // image polarisation of each visibility polarisation (-1 drops it)
   int pm[NPOL];
 #pragma unroll
@@ -403,14 +554,8 @@ __global__ void __launch_bounds__(GCfg<S, NPOL>::THREADS, 1) k_grid_tiled(TiledG
     int v = p < a.npol ? a.pol_map[p] : -1;
     pm[p] = (v >= 0 && v < npg) ? v : -1;
   }
-  int ipm[PPL];  // this lane's polarisations
-#pragma unroll
-  for (int pp = 0; pp < PPL; ++pp) {
-    ipm[pp] = -1;
-#pragma unroll
-    for (int p = 0; p < NPOL; ++p)
-      if (p == pg * PPL + pp) ipm[pp] = pm[p];
-  }
+  Lanes lanes;
+  lanes.setup(lane, pm);
   double2 *wd = st_d + warp * NPOL * C::SDS;
   int *wm = st_m + warp * GT_STAGE;
 
@@ -439,11 +584,6 @@ __global__ void __launch_bounds__(GCfg<S, NPOL>::THREADS, 1) k_grid_tiled(TiledG
       const uint32_t w_hi = seg_lo + (uint32_t)(((uint64_t)seg_n * (warp + 1)) / C::WARPS);
       const int n_rounds = (int)((w_hi - w_lo + GT_STAGE - 1) / GT_STAGE);
 
-      double2 acc[PPL][KC];
-#pragma unroll
-      for (int pp = 0; pp < PPL; ++pp)
-#pragma unroll
-        for (int k = 0; k < KC; ++k) acc[pp][k] = make_double2(0.0, 0.0);
       int cur = -1;  // the warp's current cell
       double sw[NPOL];
 #pragma unroll
@@ -504,43 +644,17 @@ __global__ void __launch_bounds__(GCfg<S, NPOL>::THREADS, 1) k_grid_tiled(TiledG
         int j = 0;
         while (j < jn) {
           if ((starts >> j) & 1u) {
-            if (cur >= 0) grid_flush<S, C::RS, C::PS, PPL, KC>(acc, sre, sim, cur, g, c0, ipm, owner);
+            if (cur >= 0) lanes.flush(sre, sim, cur);
             cur = __shfl_sync(0xffffffffu, my_key, j);
           }
           const unsigned later = j < 31 ? (starts & (0xfffffffeu << j)) : 0u;
           const int j1 = later ? min(jn, __ffs(later) - 1) : jn;
-          for (; j < j1; ++j) {
-            const int ro = wm[j];
-            const double cu = tab[(ro & 0xffff) + g];
-            const double *cvp = tab + (ro >> 16) + c0;
-            double cv[KCE];
-            if (C::PAIRS) {
-#pragma unroll
-              for (int k = 0; k + 1 < KC; k += 2) {
-                const double2 c2 = *(const double2 *)(cvp + k);
-                cv[k] = c2.x;
-                cv[k + 1] = c2.y;
-              }
-              if (KC % 2) cv[KC - 1] = cvp[KC - 1];
-            } else {
-#pragma unroll
-              for (int k = 0; k < KC; ++k) cv[k] = cvp[k];
-            }
-#pragma unroll
-            for (int pp = 0; pp < PPL; ++pp) {
-              const double2 d = wd[(pg * PPL + pp) * C::SDS + j];
-              const double tr = cu * d.x, ti = cu * d.y;
-#pragma unroll
-              for (int k = 0; k < KC; ++k) {
-                acc[pp][k].x = fma(cv[k], tr, acc[pp][k].x);
-                acc[pp][k].y = fma(cv[k], ti, acc[pp][k].y);
-              }
-            }
-          }
+          lanes.run(j, j1, wd, wm, tab);
+          j = j1;
         }
         __syncwarp();
       }
-      if (cur >= 0) grid_flush<S, C::RS, C::PS, PPL, KC>(acc, sre, sim, cur, g, c0, ipm, owner);
+      if (cur >= 0) lanes.flush(sre, sim, cur);
       // ---- sum_weight: warp reduction, one atomic per warp and polarisation
 #pragma unroll
       for (int p = 0; p < NPOL; ++p) {
@@ -590,21 +704,32 @@ __global__ void __launch_bounds__(GCfg<S, NPOL>::THREADS, 1) k_grid_tiled(TiledG
   }
 }
 
-template <int S, int NPOL>
-static int launch_grid_tiled(const TiledGridArgs &a, int64_t nblocks, cudaStream_t st) {
-  using C = GCfg<S, NPOL>;
+template <int S, int NPOL, bool MMA>
+static int launch_grid_tiled_as(const TiledGridArgs &a, int64_t nblocks, cudaStream_t st) {
+  using C = GCfg<S, NPOL, MMA>;
   size_t smem = C::total(a.npg);
   static bool configured[64] = {false};
   int dev = 0;
   AV_CUDA(cudaGetDevice(&dev));
   if (dev >= 0 && dev < 64 && !configured[dev]) {
-    AV_CUDA(cudaFuncSetAttribute(k_grid_tiled<S, NPOL>,
+    AV_CUDA(cudaFuncSetAttribute(k_grid_tiled<S, NPOL, MMA>,
                                  cudaFuncAttributeMaxDynamicSharedMemorySize, (int)C::total(4)));
     configured[dev] = true;
   }
-  k_grid_tiled<S, NPOL><<<(unsigned)nblocks, C::THREADS, smem, st>>>(a);
+  k_grid_tiled<S, NPOL, MMA><<<(unsigned)nblocks, C::THREADS, smem, st>>>(a);
   AV_LAUNCH_CHECK();
   return AV_OK;
+}
+
+// The FP64 tensor-core lanes for supports up to 8 unless the
+// AV_TUNE_GRID_LANES knob asks for the row lanes.
+template <int S, int NPOL>
+static int launch_grid_tiled(const TiledGridArgs &a, int64_t nblocks, cudaStream_t st) {
+  if constexpr (S <= 8) {
+    if (tune_value(AV_TUNE_GRID_LANES) == AV_GRID_LANES_MMA)
+      return launch_grid_tiled_as<S, NPOL, true>(a, nblocks, st);
+  }
+  return launch_grid_tiled_as<S, NPOL, false>(a, nblocks, st);
 }
 
 template <int S>

@@ -58,9 +58,20 @@ unsigned long long av_launch_count(void);
  *                                persistent tiled gridder (default 16)
  *   AV_TUNE_DEGRID_CHUNKS_PER_SM record chunks per SM handed out by the
  *                                persistent tiled degridder (default 16)
+ *   AV_TUNE_GRID_LANES           how the tiled gridder sums a run of samples
+ *                                for supports up to 8: AV_GRID_LANES_MMA
+ *                                (FP64 tensor-core tiles, default) or
+ *                                AV_GRID_LANES_ROWS (a footprint row per
+ *                                lane, DFMA); support 9 always uses rows
  * av_tune_set returns AV_ERR_ARG for an unknown knob or a value outside
- * [1, 1024]; av_tune_get returns -1 for an unknown knob. */
-enum av_tune { AV_TUNE_GRID_CHUNKS_PER_SM = 0, AV_TUNE_DEGRID_CHUNKS_PER_SM = 1 };
+ * [1, 1024] ([1, 2] for AV_TUNE_GRID_LANES); av_tune_get returns -1 for an
+ * unknown knob. */
+enum av_tune {
+  AV_TUNE_GRID_CHUNKS_PER_SM = 0,
+  AV_TUNE_DEGRID_CHUNKS_PER_SM = 1,
+  AV_TUNE_GRID_LANES = 2
+};
+enum av_grid_lanes { AV_GRID_LANES_MMA = 1, AV_GRID_LANES_ROWS = 2 };
 int av_tune_set(int knob, int64_t value);
 int64_t av_tune_get(int knob);
 

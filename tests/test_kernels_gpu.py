@@ -237,22 +237,36 @@ def test_tiled_degrid_every_support(support, os_):
     assert rel(v.cpu().numpy(), ref) <= 1e-6
 
 
+@pytest.fixture(params=["mma", "rows"])
+def grid_lanes(request):
+    """Runs a test under each of the tiled gridder's lane mappings: FP64
+    tensor-core tiles (supports up to 8) and a footprint row per lane."""
+    from astroviper_b200 import _lib
+    L = _lib.lib()
+    old = L.av_tune_get(_lib.AV_TUNE_GRID_LANES)
+    want = _lib.AV_GRID_LANES_MMA if request.param == "mma" else _lib.AV_GRID_LANES_ROWS
+    assert L.av_tune_set(_lib.AV_TUNE_GRID_LANES, want) == _lib.AV_OK
+    yield request.param
+    L.av_tune_set(_lib.AV_TUNE_GRID_LANES, old)
+
+
+@pytest.mark.parametrize("npol", [1, 2, 4])
 @pytest.mark.parametrize("support", [3, 4, 5, 6, 7, 8, 9])
-def test_tiled_grid_every_support(support):
-    """The tiled gridder against the oracle for every support (2 channels
-    into 2 image channels, 2 polarisations)."""
+def test_tiled_grid_every_support(support, npol, grid_lanes):
+    """The tiled gridder against the oracle for every support and
+    polarisation count (3 channels into 3 image channels)."""
     g = golden("degrid.npz")
-    rng = np.random.default_rng(support)
+    rng = np.random.default_rng(support * 10 + npol)
     nt, nb = g["uvw"].shape[:2]
-    vis = (rng.normal(size=(nt, nb, 3, 2)) + 1j * rng.normal(size=(nt, nb, 3, 2)))
-    wt = rng.uniform(0.5, 2.0, size=(nt, nb, 3, 2))
+    vis = (rng.normal(size=(nt, nb, 3, npol)) + 1j * rng.normal(size=(nt, nb, 3, npol)))
+    wt = rng.uniform(0.5, 2.0, size=(nt, nb, 3, npol))
     cf = O.create_prolate_spheroidal_kernel_1D(100, support)
     cell = np.array([-1.0, 1.0]) * 20.0 * np.pi / (180 * 3600)
     rg, rs = O.standard_grid(vis, g["uvw"], wt, g["freq"], cf, np.array([64, 64]), cell,
                              support=support, chan_mode="cube")
     gr, sw = K().grid(vis.astype(np.complex64), torch.as_tensor(wt.astype(np.float32)), g["uvw"],
-                      g["freq"], np.arange(3), np.arange(2), cf, np.array([64, 64]), cell,
-                      support, 100, 3, 2, precision="fp32")
+                      g["freq"], np.arange(3), np.arange(npol), cf, np.array([64, 64]), cell,
+                      support, 100, 3, npol, precision="fp32")
     vis32 = vis.astype(np.complex64).astype(complex)
     wt32 = wt.astype(np.float32).astype(float)
     rg32, rs32 = O.standard_grid(vis32, g["uvw"], wt32, g["freq"], cf, np.array([64, 64]), cell,
@@ -260,6 +274,24 @@ def test_tiled_grid_every_support(support):
     assert rel(gr.cpu().numpy(), rg32) <= 1e-12
     assert np.allclose(sw.cpu().numpy(), rs32, rtol=1e-12)
     assert rel(gr.cpu().numpy(), rg) <= 1e-6
+
+
+def test_tiled_grid_long_runs_match_fp64(grid_lanes):
+    """Runs of one cell that span many staged rounds (8 time steps of the
+    33M-sample workload, continuum 2048^2, 4 polarisations): the tiled
+    gridder against the plain FP64 gridder on the same complex64 inputs."""
+    from astroviper_b200 import synthetic as S
+    W = S.workload_large(n_time=8, n_chan=16, device=torch.device("cuda"))
+    nt, nb, nchan, npol = W["vis"].shape
+    cf = O.create_prolate_spheroidal_kernel_1D(100, 7)
+    wt = torch.rand(W["vis"].shape, dtype=torch.float32, device="cuda",
+                    generator=torch.Generator("cuda").manual_seed(5)) + 0.5
+    args = (W["uvw"], W["freq"], np.zeros(nchan, int), np.arange(npol), cf, W["image_size"],
+            W["pixelincr"], 7, 100, 1, npol)
+    g32, s32 = K().grid(W["vis"], wt, *args, precision="fp32")
+    g64, s64 = K().grid(W["vis"].to(torch.complex128), wt.double(), *args, precision="fp64")
+    assert rel(g32.cpu().numpy(), g64.cpu().numpy()) <= 1e-12
+    assert np.allclose(s32.cpu().numpy(), s64.cpu().numpy(), rtol=1e-12)
 
 
 def test_degrid_store_mode_four_pol_fast_output():
