@@ -164,6 +164,7 @@ struct TiledGridArgs {
   const uint32_t *tile_start;
   const uint32_t *n_rec;  // device: total records (offs[n_keys])
   uint32_t *sched;        // device: [0] next chunk, [1] CTAs done (both 0 between launches)
+  int a16;                 // vis and weight rows are 16-byte aligned (16-byte loads / copies)
   int64_t n_tiles, ntu, ntv;
   int64_t chunk;
   const float2 *vis;
@@ -217,16 +218,17 @@ struct TiledGridArgs {
 // per sample, for 512 instead of 392 multiply-adds at the FP64 rate).
 //
 // The warp's lanes first stage 32 samples (one each: FP64 weighted values,
-// cell key, tap-table row offsets) into the warp's shared staging area; the
-// next round's values and the record of the round after are in flight while
-// a round is computed.
-template <int S, int NPOL, bool MMA = false>
+// cell key, tap-table row offsets) into the warp's shared staging area.
+// k_grid_tiled (RowLanes) keeps the next round's values and the record of
+// the round after in registers while a round is computed; k_grid_mma
+// (MmaLanes) copies raw values two rounds ahead into a per-warp ring in
+// shared memory with cp.async, which holds more loads in flight per SM.
+template <int S, int NPOL>
 struct GCfg {
   // one CTA per SM; as many warps as the registers allow without spilling
-  static constexpr int THREADS = (!MMA && S >= 9 && NPOL == 4) ? 384 : 512;
+  static constexpr int THREADS = (S >= 9 && NPOL == 4) ? 384 : 512;
   static constexpr int WARPS = THREADS / 32;
   static constexpr int W = TILE + S - 1;                          // sub-grid edge
-  // RowLanes' split of (polarisation, row, column) over the lanes
   static constexpr bool QUARTERS = S <= 8;                         // lane = block * 8 + g
   static constexpr int PPL = QUARTERS ? (NPOL <= 4 ? 1 : 2)
                                       : (S * NPOL <= 32 ? 1 : (S * NPOL <= 64 ? 2 : 4));
@@ -241,8 +243,7 @@ struct GCfg {
   static constexpr int KCE = PAIRS ? ((KC + 1) & ~1) : KC;         // taps addressed
   static constexpr int RT0 = (NCC - 1) * KC + KCE;
   static constexpr int RT = ((RT0 > S ? RT0 : S) + 1) & ~1;        // taps per table row
-  // table row stride (banks); MmaLanes reads taps 0-7 of a row
-  static constexpr int RWP = MMA ? 10 : ((RT % 4 == 0) ? RT + 2 : RT);
+  static constexpr int RWP = (RT % 4 == 0) ? RT + 2 : RT;          // row stride (banks)
   static constexpr size_t tab_bytes = 256 * RWP * sizeof(double);
   static constexpr size_t rs_bytes = 256 * sizeof(double);
   // staged values: [pol][sample] with a 33-entry stride, so the 32 lanes'
@@ -263,7 +264,40 @@ struct GCfg {
   static size_t total(int npg) { return off_sub + sub_bytes(npg); }
   static_assert(QUARTERS ? BLOCKS <= 4 : S * BLOCKS <= 32, "lane mapping");
   static_assert(NPGL * PPL == NPOL, "polarisation split");
-  static_assert(!MMA || (S <= 8 && RWP >= 8), "one 8 x 8 footprint per polarisation");
+};
+
+// k_grid_mma's shared memory: tap table (rows of 8 taps, zero past the
+// support, stride 10), rs, the warps' rings, the warps' tap-row offsets and
+// the sub-grid.  A ring slot holds one round: NPOL planes of SDS double2
+// entries ([pol][sample]); the raw FP32 values of sample s arrive in its own
+// entries (vis pols 0-1 in plane 0, 2-3 in plane 1, weights in plane 2 for
+// NPOL 4; vis in plane 0, weights in plane 1 for NPOL 2; vis then weight in
+// entry 0 for NPOL 1) and are replaced by the FP64 weighted values.  Entry
+// GT_STAGE of each plane (and of the offsets) is a zero sample that empty
+// group slots read.
+template <int S, int NPOL>
+struct MCfg {
+  static constexpr int THREADS = 512;
+  static constexpr int WARPS = THREADS / 32;
+  static constexpr int SLOTS = 3;                                  // rounds per ring
+  static constexpr int W = TILE + S - 1;
+  static constexpr int RWP = 10;
+  static constexpr int SDS = GT_STAGE + 1;
+  static constexpr int SLOT = NPOL * SDS;                          // double2 per slot
+  static constexpr int RS = W | 1;
+  static constexpr int PS = ((W * RS + 15) / 16) * 16 + 1;
+  static constexpr size_t tab_bytes = 256 * RWP * sizeof(double);
+  static constexpr size_t rs_bytes = 256 * sizeof(double);
+  static constexpr size_t ring_bytes = (size_t)WARPS * SLOTS * SLOT * sizeof(double2);
+  static constexpr size_t stm_bytes = (size_t)WARPS * SDS * sizeof(int);
+  static constexpr size_t off_rs = tab_bytes;
+  static constexpr size_t off_ring = off_rs + rs_bytes;
+  static constexpr size_t off_stm = off_ring + ring_bytes;
+  static constexpr size_t off_sub = off_stm + stm_bytes;
+  static size_t sub_bytes(int npg) { return (size_t)2 * npg * PS * sizeof(double); }
+  static size_t total(int npg) { return off_sub + sub_bytes(npg); }
+  static_assert(S <= 8, "one 8 x 8 footprint per polarisation");
+  static_assert(off_ring % 16 == 0, "ring alignment");
 };
 
 // Per-offset tap tables: tab[(o + 128) * RWP + i] = cgk[|os * (i - S/2) + o|]
@@ -327,7 +361,7 @@ __device__ __forceinline__ void prefetch(Pref<NPOL> &f, const TiledGridArgs &a, 
     }
     return;
   }
-  if (NPOL == 4 && a.npol == 4) {
+  if (NPOL == 4 && a.npol == 4 && a.a16) {  // 16-byte loads need 16-byte aligned rows
     const float4 w4 = __ldg((const float4 *)(a.wt + vb));
     f.w[0] = w4.x; f.w[1 % NPOL] = w4.y; f.w[2 % NPOL] = w4.z; f.w[3 % NPOL] = w4.w;
     if (!a.do_psf) {
@@ -349,7 +383,7 @@ __device__ __forceinline__ void prefetch(Pref<NPOL> &f, const TiledGridArgs &a, 
 
 template <int S, int NPOL>
 struct RowLanes {
-  using C = GCfg<S, NPOL, false>;
+  using C = GCfg<S, NPOL>;
   static constexpr int PPL = C::PPL, KC = C::KC, KCE = C::KCE;
   double2 acc[PPL][KC];
   int g, pg, c0;
@@ -457,7 +491,7 @@ __device__ __forceinline__ void mma_f64_m16n8k4(double (&d)[4], double a0, doubl
 
 template <int S, int NPOL>
 struct MmaLanes {
-  using C = GCfg<S, NPOL, true>;
+  using C = MCfg<S, NPOL>;
   double acc[NPOL][4];  // per polarisation: re (g, 2t), re (g, 2t+1), im (g, 2t), im (g, 2t+1)
   int g, t;
   int ipm[NPOL];
@@ -494,34 +528,89 @@ struct MmaLanes {
     clear();
   }
 
-  // Staged samples [j, j1) of the current round, all in the current cell, in
-  // groups of four; a short last group has zero A columns for its empty
-  // slots (which then read a valid sample's taps).
+  // Staged samples [j, j1) of the current round (values wd[p * SDS + s]),
+  // all in the current cell, in groups of four; a short group's empty slots
+  // read the zero sample (entry GT_STAGE: zero values, offset row 0), so
+  // their A columns are zero.
   __device__ __forceinline__ void run(int j, int j1, const double2 *wd, const int *wm,
                                       const double *tab) {
     for (; j < j1; j += 4) {
-      const bool kv = j + t < j1;
-      const int s = kv ? j + t : j;
+      const int s = j + t < j1 ? j + t : GT_STAGE;
       const int ro = wm[s];
       const double cu = tab[(ro & 0xffff) + g];
       const double cv = tab[(ro >> 16) + g];
 #pragma unroll
       for (int p = 0; p < NPOL; ++p) {
         const double2 d = wd[p * C::SDS + s];
-        mma_f64_m16n8k4(acc[p], kv ? cu * d.x : 0.0, kv ? cu * d.y : 0.0, cv);
+        mma_f64_m16n8k4(acc[p], cu * d.x, cu * d.y, cv);
       }
     }
   }
 };
 
+// Sum of weights of a warp's slice: one atomic per warp and polarisation.
+template <int NPOL>
+__device__ __forceinline__ void add_sum_weight(const TiledGridArgs &a, double (&sw)[NPOL],
+                                               const int (&pm)[NPOL], int64_t plane, int lane) {
+#pragma unroll
+  for (int p = 0; p < NPOL; ++p) {
+    double v = sw[p];
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    if (lane == 0 && a.sumw && pm[p] >= 0 && v != 0.0)
+      atomicAdd(&a.sumw[plane * a.npg + pm[p]], v);
+  }
+}
+
+// Adds a tile's shared sub-grid to the global grid and clears it (the whole
+// block; one trip count for every thread).
+template <int W, int RS, int PS, int THREADS>
+__device__ __forceinline__ void flush_subgrid(const TiledGridArgs &a, double *sre, double *sim,
+                                              int64_t plane, int tu, int tv) {
+  const int sub_n = a.npg * W * W;
+  for (int i0 = 0; i0 < sub_n; i0 += THREADS) {
+    const int i = i0 + threadIdx.x;
+    if (i >= sub_n) continue;
+    const int gp = i / (W * W);
+    const int cell = i - gp * W * W;
+    const int iu = cell / W, iv = cell - iu * W;
+    const int e = gp * PS + iu * RS + iv;
+    const double2 v = make_double2(sre[e], sim[e]);
+    if (v.x != 0.0 || v.y != 0.0) {
+      int64_t gu = (int64_t)tu * TILE + iu, gv = (int64_t)tv * TILE + iv;
+      int64_t gi = ((plane * a.npg + gp) * a.n_u + gu) * a.n_v + gv;
+      if (a.grid_c128) {
+        double2 *gd = (double2 *)a.grid + gi;
+        atomicAdd(&gd->x, v.x);
+        atomicAdd(&gd->y, v.y);
+      } else {
+        atomicAdd((float2 *)a.grid + gi, make_float2((float)v.x, (float)v.y));
+      }
+      sre[e] = 0.0;
+      sim[e] = 0.0;
+    }
+  }
+}
+
+// Every CTA has taken its last chunk: the last one to get here re-arms the
+// plan's counters for the next launch.
+__device__ __forceinline__ void rearm_schedule(const TiledGridArgs &a) {
+  if (threadIdx.x == 0) {
+    __threadfence();
+    if (atomicAdd(&a.sched[1], 1u) == gridDim.x - 1) {
+      a.sched[0] = 0u;
+      a.sched[1] = 0u;
+      __threadfence();
+    }
+  }
+}
+
 // Persistent: one CTA per SM takes chunks of records from a.sched[0] until
 // none are left; the last CTA to finish sets both counters back to zero for
 // the next launch on the same plan.
-template <int S, int NPOL, bool MMA>
-__global__ void __launch_bounds__(GCfg<S, NPOL, MMA>::THREADS, 1)
-    k_grid_tiled(TiledGridArgs a) {
-  using C = GCfg<S, NPOL, MMA>;
-  using Lanes = typename std::conditional<MMA, MmaLanes<S, NPOL>, RowLanes<S, NPOL>>::type;
+template <int S, int NPOL>
+__global__ void __launch_bounds__(GCfg<S, NPOL>::THREADS, 1) k_grid_tiled(TiledGridArgs a) {
+  using C = GCfg<S, NPOL>;
   constexpr int W = C::W, RWP = C::RWP;
   extern __shared__ __align__(16) unsigned char smem[];
   double *tab = (double *)smem;
@@ -535,7 +624,6 @@ __global__ void __launch_bounds__(GCfg<S, NPOL, MMA>::THREADS, 1)
   const uint32_t n_rec = *a.n_rec;
   const int64_t n_chunks = ((int64_t)n_rec + a.chunk - 1) / a.chunk;
   const int npg = a.npg;
-  const int sub_n = npg * W * W;  // cells of the tile's footprint area
 
   build_tap_tables64<S, RWP>(tab, rs, a.cgk, a.cgk_len, a.os);
   // strided loops that precede a block barrier keep one trip count for the
@@ -554,7 +642,7 @@ __global__ void __launch_bounds__(GCfg<S, NPOL, MMA>::THREADS, 1)
     int v = p < a.npol ? a.pol_map[p] : -1;
     pm[p] = (v >= 0 && v < npg) ? v : -1;
   }
-  Lanes lanes;
+  RowLanes<S, NPOL> lanes;
   lanes.setup(lane, pm);
   double2 *wd = st_d + warp * NPOL * C::SDS;
   int *wm = st_m + warp * GT_STAGE;
@@ -655,81 +743,320 @@ __global__ void __launch_bounds__(GCfg<S, NPOL, MMA>::THREADS, 1)
         __syncwarp();
       }
       if (cur >= 0) lanes.flush(sre, sim, cur);
-      // ---- sum_weight: warp reduction, one atomic per warp and polarisation
-#pragma unroll
-      for (int p = 0; p < NPOL; ++p) {
-        double v = sw[p];
-#pragma unroll
-        for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
-        if (lane == 0 && a.sumw && pm[p] >= 0 && v != 0.0)
-          atomicAdd(&a.sumw[plane * npg + pm[p]], v);
-      }
+      add_sum_weight<NPOL>(a, sw, pm, plane, lane);
       __syncthreads();
-      // ---- flush the tile to the global grid and clear it
-      for (int i0 = 0; i0 < sub_n; i0 += C::THREADS) {
-        const int i = i0 + threadIdx.x;
-        if (i >= sub_n) continue;
-        const int gp = i / (W * W);
-        const int cell = i - gp * W * W;
-        const int iu = cell / W, iv = cell - iu * W;
-        const int e = gp * C::PS + iu * C::RS + iv;
-        const double2 v = make_double2(sre[e], sim[e]);
-        if (v.x != 0.0 || v.y != 0.0) {
-          int64_t gu = (int64_t)tu * TILE + iu, gv = (int64_t)tv * TILE + iv;
-          int64_t gi = ((plane * npg + gp) * a.n_u + gu) * a.n_v + gv;
-          if (a.grid_c128) {
-            double2 *gd = (double2 *)a.grid + gi;
-            atomicAdd(&gd->x, v.x);
-            atomicAdd(&gd->y, v.y);
-          } else {
-            atomicAdd((float2 *)a.grid + gi, make_float2((float)v.x, (float)v.y));
-          }
-          sre[e] = 0.0;
-          sim[e] = 0.0;
-        }
-      }
+      flush_subgrid<W, C::RS, C::PS, C::THREADS>(a, sre, sim, plane, tu, tv);
       __syncthreads();
       seg_lo = seg_hi;
       if (seg_hi == t_end) ++t;
     }
   }
-  // every CTA has taken its last chunk: the last one to get here re-arms
-  if (threadIdx.x == 0) {
-    __threadfence();
-    if (atomicAdd(&a.sched[1], 1u) == gridDim.x - 1) {
-      a.sched[0] = 0u;
-      a.sched[1] = 0u;
-      __threadfence();
+  rearm_schedule(a);
+}
+
+__device__ __forceinline__ void cp_async16(void *dst, const void *src) {
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(
+                   (unsigned)__cvta_generic_to_shared(dst)),
+               "l"(src));
+}
+__device__ __forceinline__ void cp_async8(void *dst, const void *src) {
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(
+                   (unsigned)__cvta_generic_to_shared(dst)),
+               "l"(src));
+}
+__device__ __forceinline__ void cp_async4(void *dst, const void *src) {
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(
+                   (unsigned)__cvta_generic_to_shared(dst)),
+               "l"(src));
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() {
+  asm volatile("cp.async.wait_group %0;\n" ::"n"(N));
+}
+
+// Raw values of one sample (this lane's record) into its entries of a ring
+// slot (layout at MCfg): 16-byte copies when a.a16 says the rows allow them,
+// else one copy per polarisation.
+template <int NPOL>
+__device__ __forceinline__ void issue_raw(const TiledGridArgs &a, double2 *slot, int s,
+                                          uint32_t row) {
+  constexpr int SDS = GT_STAGE + 1;
+  const int64_t vb = (int64_t)row * a.npol;
+  unsigned char *e0 = (unsigned char *)(slot + s);
+  unsigned char *e1 = (unsigned char *)(slot + (NPOL > 1 ? SDS : 0) + s);
+  unsigned char *e2 = (unsigned char *)(slot + (NPOL > 2 ? 2 * SDS : 0) + s);
+  if (NPOL == 4) {  // vis 0-1 -> plane 0, vis 2-3 -> plane 1, weights -> plane 2
+    if (a.a16) {
+      if (!a.do_psf) {
+        cp_async16(e0, a.vis + vb);
+        cp_async16(e1, a.vis + vb + 2);
+      }
+      cp_async16(e2, a.wt + vb);
+    } else {
+      for (int p = 0; p < a.npol; ++p) {
+        if (!a.do_psf) cp_async8((p < 2 ? e0 : e1) + 8 * (p & 1), a.vis + vb + p);
+        cp_async4(e2 + 4 * p, a.wt + vb + p);
+      }
+    }
+  } else if (NPOL == 2) {  // vis -> plane 0, weights -> plane 1
+    if (a.a16 && a.npol == 2) {
+      if (!a.do_psf) cp_async16(e0, a.vis + vb);
+      cp_async8(e1, a.wt + vb);
+    } else {
+      for (int p = 0; p < a.npol; ++p) {
+        if (!a.do_psf) cp_async8(e0 + 8 * p, a.vis + vb + p);
+        cp_async4(e1 + 4 * p, a.wt + vb + p);
+      }
+    }
+  } else {  // vis then weight in entry 0
+    if (!a.do_psf) cp_async8(e0, a.vis + vb);
+    cp_async4(e0 + 8, a.wt + vb);
+  }
+}
+
+// Reads sample s's raw values back from its ring entries (after the copies
+// are complete).
+template <int NPOL>
+__device__ __forceinline__ void read_raw(const TiledGridArgs &a, const double2 *slot, int s,
+                                         float2 (&v)[NPOL], float (&w)[NPOL]) {
+  constexpr int SDS = GT_STAGE + 1;
+  if (NPOL == 4) {
+    const float4 v01 = *(const float4 *)(slot + s);
+    const float4 v23 = *(const float4 *)(slot + SDS + s);
+    const float4 w4 = *(const float4 *)(slot + 2 * SDS + s);
+    v[0] = make_float2(v01.x, v01.y);
+    v[1 % NPOL] = make_float2(v01.z, v01.w);
+    v[2 % NPOL] = make_float2(v23.x, v23.y);
+    v[3 % NPOL] = make_float2(v23.z, v23.w);
+    w[0] = w4.x; w[1 % NPOL] = w4.y; w[2 % NPOL] = w4.z; w[3 % NPOL] = w4.w;
+  } else if (NPOL == 2) {
+    const float4 v01 = *(const float4 *)(slot + s);
+    const float2 w2 = *(const float2 *)(slot + (NPOL > 1 ? SDS : 0) + s);
+    v[0] = make_float2(v01.x, v01.y);
+    v[1 % NPOL] = make_float2(v01.z, v01.w);
+    w[0] = w2.x;
+    w[1 % NPOL] = w2.y;
+  } else {
+    const float4 e = *(const float4 *)(slot + s);
+    v[0] = make_float2(e.x, e.y);
+    w[0] = e.z;
+  }
+#pragma unroll
+  for (int p = 0; p < NPOL; ++p) {
+    if (p >= a.npol) {  // polarisations past npol were not copied
+      v[p] = make_float2(0.f, 0.f);
+      w[p] = 0.f;
+    } else if (a.do_psf) {
+      v[p] = make_float2(0.f, 0.f);
     }
   }
 }
 
-template <int S, int NPOL, bool MMA>
-static int launch_grid_tiled_as(const TiledGridArgs &a, int64_t nblocks, cudaStream_t st) {
-  using C = GCfg<S, NPOL, MMA>;
+// k_grid_tiled's schedule and segments with MmaLanes and a cp.async ring:
+// the raw values of round rd + 2 are copied while round rd is computed, and
+// records are loaded one round before their copies are issued.  Only for
+// weighted gridding (a.wt != NULL, no 1 / norm scaling).
+template <int S, int NPOL>
+__global__ void __launch_bounds__(MCfg<S, NPOL>::THREADS, 1) k_grid_mma(TiledGridArgs a) {
+  using C = MCfg<S, NPOL>;
+  constexpr int W = C::W, RWP = C::RWP;
+  extern __shared__ __align__(16) unsigned char smem[];
+  double *tab = (double *)smem;
+  double *rs = (double *)(smem + C::off_rs);
+  double2 *ring = (double2 *)(smem + C::off_ring);
+  int *st_m = (int *)(smem + C::off_stm);
+  double *sre = (double *)(smem + C::off_sub);
+  double *sim = sre + (size_t)a.npg * C::PS;
+  __shared__ int s_chunk;
+
+  const uint32_t n_rec = *a.n_rec;
+  const int64_t n_chunks = ((int64_t)n_rec + a.chunk - 1) / a.chunk;
+  const int npg = a.npg;
+
+  build_tap_tables64<S, RWP>(tab, rs, a.cgk, a.cgk_len, a.os);
+  for (int i0 = 0; i0 < 2 * npg * C::PS; i0 += C::THREADS) {
+    const int i = i0 + threadIdx.x;
+    if (i < 2 * npg * C::PS) sre[i] = 0.0;
+  }
+
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  int pm[NPOL];
+#pragma unroll
+  for (int p = 0; p < NPOL; ++p) {
+    int v = p < a.npol ? a.pol_map[p] : -1;
+    pm[p] = (v >= 0 && v < npg) ? v : -1;
+  }
+  MmaLanes<S, NPOL> lanes;
+  lanes.setup(lane, pm);
+  double2 *wring = ring + (size_t)warp * C::SLOTS * C::SLOT;
+  int *wm = st_m + warp * C::SDS;
+  if (lane == 0) {  // the zero samples (nothing else writes entry GT_STAGE)
+    for (int k = 0; k < C::SLOTS; ++k)
+#pragma unroll
+      for (int p = 0; p < NPOL; ++p)
+        wring[k * C::SLOT + p * C::SDS + GT_STAGE] = make_double2(0.0, 0.0);
+    wm[GT_STAGE] = 0;
+  }
+
+  for (;;) {
+    __syncthreads();  // tables and sub-grid ready; previous s_chunk consumed
+    if (threadIdx.x == 0) s_chunk = (int)atomicAdd(&a.sched[0], 1u);
+    __syncthreads();
+    const int64_t ch = s_chunk;
+    if (ch >= n_chunks) break;
+    const uint32_t r0 = (uint32_t)(ch * a.chunk);
+    const uint32_t r1 = (uint32_t)min((int64_t)n_rec, (int64_t)r0 + a.chunk);
+    int t = find_tile(a.tile_start, a.n_tiles, r0);
+    uint32_t seg_lo = r0;
+    while (seg_lo < r1) {
+      const uint32_t t_end = a.tile_start[t + 1];
+      const uint32_t seg_hi = min(r1, t_end);
+      if (seg_hi <= seg_lo) {
+        ++t;
+        continue;
+      }
+      const int64_t plane = t / (a.ntu * a.ntv);
+      const int64_t trem = t - plane * a.ntu * a.ntv;
+      const int tu = (int)(trem / a.ntv), tv = (int)(trem - (int64_t)tu * a.ntv);
+      const uint32_t seg_n = seg_hi - seg_lo;
+      const uint32_t w_lo = seg_lo + (uint32_t)(((uint64_t)seg_n * warp) / C::WARPS);
+      const uint32_t w_hi = seg_lo + (uint32_t)(((uint64_t)seg_n * (warp + 1)) / C::WARPS);
+      const int n_rounds = (int)((w_hi - w_lo + GT_STAGE - 1) / GT_STAGE);
+
+      int cur = -1;
+      double sw[NPOL];
+#pragma unroll
+      for (int p = 0; p < NPOL; ++p) sw[p] = 0.0;
+
+      // records of rounds rd .. rd + 2 (row 0xffffffff: none)
+      Rec rc0, rc1, rc2;
+      auto load_rec = [&](int rd) {
+        const uint32_t r = w_lo + (uint32_t)rd * GT_STAGE + lane;
+        Rec x;
+        if (rd < n_rounds && r < w_hi) x = a.recs[r];
+        else x.row = 0xffffffffu;
+        return x;
+      };
+      rc0 = load_rec(0);
+      rc1 = load_rec(1);
+      rc2 = load_rec(2);
+      if (rc0.row != 0xffffffffu) issue_raw<NPOL>(a, wring, lane, rc0.row);
+      cp_async_commit();
+      if (rc1.row != 0xffffffffu) issue_raw<NPOL>(a, wring + C::SLOT, lane, rc1.row);
+      cp_async_commit();
+      for (int rd = 0; rd < n_rounds; ++rd) {
+        double2 *slot = wring + (rd % C::SLOTS) * C::SLOT;
+        cp_async_wait<1>();  // this lane's copies of round rd are complete
+        // ---- stage: FP64 weighted values in place of the raw ones, the
+        // cell key and the offsets of the two tap-table rows
+        int my_key = -1;
+        if (rc0.row != 0xffffffffu) {
+          float2 v[NPOL];
+          float w[NPOL];
+          read_raw<NPOL>(a, slot, lane, v, w);
+          const double nrm = rs[rc0.ou] * rs[rc0.ov];
+#pragma unroll
+          for (int p = 0; p < NPOL; ++p) {
+            double2 d;
+            if (a.do_psf) d = make_double2((double)w[p], 0.0);
+            else d = make_double2((double)v[p].x * (double)w[p], (double)v[p].y * (double)w[p]);
+            // the reference skips NaN and exact-zero weighted data
+            // (standard_grid.py:378)
+            const bool ok = p < a.npol && !isnan(d.x) && !isnan(d.y) &&
+                            (d.x != 0.0 || d.y != 0.0);
+            slot[p * C::SDS + lane] = ok ? d : make_double2(0.0, 0.0);
+            if (ok) sw[p] += (double)w[p] * nrm;
+          }
+          my_key = (int)rc0.du | ((int)rc0.dv << 8);
+          wm[lane] = (int)rc0.ou * RWP | (((int)rc0.ov * RWP) << 16);
+        }
+        int prev = __shfl_up_sync(0xffffffffu, my_key, 1);
+        if (lane == 0) prev = cur;
+        const unsigned starts = __ballot_sync(0xffffffffu, my_key >= 0 && my_key != prev);
+        // ---- copies of round rd + 2 (into the slot round rd - 1 used) and
+        // the record of round rd + 3
+        if (rc2.row != 0xffffffffu)
+          issue_raw<NPOL>(a, wring + ((rd + 2) % C::SLOTS) * C::SLOT, lane, rc2.row);
+        cp_async_commit();
+        const Rec rc3 = load_rec(rd + 3);
+        __syncwarp();
+        // ---- compute the round's samples in runs of one cell
+        const int jn = (int)min((uint32_t)GT_STAGE, w_hi - (w_lo + (uint32_t)rd * GT_STAGE));
+        int j = 0;
+        while (j < jn) {
+          if ((starts >> j) & 1u) {
+            if (cur >= 0) lanes.flush(sre, sim, cur);
+            cur = __shfl_sync(0xffffffffu, my_key, j);
+          }
+          const unsigned later = j < 31 ? (starts & (0xfffffffeu << j)) : 0u;
+          const int j1 = later ? min(jn, __ffs(later) - 1) : jn;
+          lanes.run(j, j1, slot, wm, tab);
+          j = j1;
+        }
+        __syncwarp();
+        rc0 = rc1;
+        rc1 = rc2;
+        rc2 = rc3;
+      }
+      cp_async_wait<0>();
+      if (cur >= 0) lanes.flush(sre, sim, cur);
+      add_sum_weight<NPOL>(a, sw, pm, plane, lane);
+      __syncthreads();
+      flush_subgrid<W, C::RS, C::PS, C::THREADS>(a, sre, sim, plane, tu, tv);
+      __syncthreads();
+      seg_lo = seg_hi;
+      if (seg_hi == t_end) ++t;
+    }
+  }
+  rearm_schedule(a);
+}
+
+template <int S, int NPOL>
+static int launch_grid_rows(const TiledGridArgs &a, int64_t nblocks, cudaStream_t st) {
+  using C = GCfg<S, NPOL>;
   size_t smem = C::total(a.npg);
   static bool configured[64] = {false};
   int dev = 0;
   AV_CUDA(cudaGetDevice(&dev));
   if (dev >= 0 && dev < 64 && !configured[dev]) {
-    AV_CUDA(cudaFuncSetAttribute(k_grid_tiled<S, NPOL, MMA>,
+    AV_CUDA(cudaFuncSetAttribute(k_grid_tiled<S, NPOL>,
                                  cudaFuncAttributeMaxDynamicSharedMemorySize, (int)C::total(4)));
     configured[dev] = true;
   }
-  k_grid_tiled<S, NPOL, MMA><<<(unsigned)nblocks, C::THREADS, smem, st>>>(a);
+  k_grid_tiled<S, NPOL><<<(unsigned)nblocks, C::THREADS, smem, st>>>(a);
   AV_LAUNCH_CHECK();
   return AV_OK;
 }
 
-// The FP64 tensor-core lanes for supports up to 8 unless the
-// AV_TUNE_GRID_LANES knob asks for the row lanes.
+template <int S, int NPOL>
+static int launch_grid_mma(const TiledGridArgs &a, int64_t nblocks, cudaStream_t st) {
+  using C = MCfg<S, NPOL>;
+  size_t smem = C::total(a.npg);
+  static bool configured[64] = {false};
+  int dev = 0;
+  AV_CUDA(cudaGetDevice(&dev));
+  if (dev >= 0 && dev < 64 && !configured[dev]) {
+    AV_CUDA(cudaFuncSetAttribute(k_grid_mma<S, NPOL>,
+                                 cudaFuncAttributeMaxDynamicSharedMemorySize, (int)C::total(4)));
+    configured[dev] = true;
+  }
+  k_grid_mma<S, NPOL><<<(unsigned)nblocks, C::THREADS, smem, st>>>(a);
+  AV_LAUNCH_CHECK();
+  return AV_OK;
+}
+
+// k_grid_mma for weighted gridding with supports up to 8 unless the
+// AV_TUNE_GRID_LANES knob asks for the row lanes; k_grid_tiled otherwise
+// (support 9, the degridder's adjoint).
 template <int S, int NPOL>
 static int launch_grid_tiled(const TiledGridArgs &a, int64_t nblocks, cudaStream_t st) {
   if constexpr (S <= 8) {
-    if (tune_value(AV_TUNE_GRID_LANES) == AV_GRID_LANES_MMA)
-      return launch_grid_tiled_as<S, NPOL, true>(a, nblocks, st);
+    if (a.wt != nullptr && !a.inv_norm &&
+        tune_value(AV_TUNE_GRID_LANES) == AV_GRID_LANES_MMA)
+      return launch_grid_mma<S, NPOL>(a, nblocks, st);
   }
-  return launch_grid_tiled_as<S, NPOL, false>(a, nblocks, st);
+  return launch_grid_rows<S, NPOL>(a, nblocks, st);
 }
 
 template <int S>
@@ -911,6 +1238,11 @@ int av_grid_tiled_execute(void *grid, int grid_dtype, double *sum_weight, int do
   a.n_v = n_v;
   a.inv_norm = 0;
   a.flag = nullptr;
+  {
+    const uintptr_t vp = (uintptr_t)vis, wp = (uintptr_t)weight;
+    const bool v16 = do_psf || vp % 16 == 0;
+    a.a16 = v16 && ((npol == 4 && wp % 16 == 0) || (npol == 2 && wp % 8 == 0));
+  }
   return dispatch_support(a, support, npol_t, nblocks, as_stream(stream));
 }
 
@@ -974,6 +1306,7 @@ int av_degrid_tiled_adjoint(void *grid, int grid_dtype, const void *values, int 
   a.n_v = g_n3;
   a.inv_norm = 1;
   a.flag = flag;
+  a.a16 = 0;
   int npol_t = nvpol <= 1 ? 1 : (nvpol <= 2 ? 2 : 4);
   return dispatch_support(a, support, npol_t, nblocks, as_stream(stream));
 }
