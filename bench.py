@@ -125,13 +125,14 @@ class ClockSampler:
                 "samples": len(self.rows), "source": "NVML, 2 ms"}
 
 
-# DRAM bytes read + written per launch and per visibility of the two main
-# kernels, from one ncu capture (dram__bytes_read.sum + dram__bytes_write.sum)
-# of the 8.26M-visibility case (64 time steps): k_grid_tiled 484.11 MB,
-# k_degrid_tiled 286.84 MB.  The traffic is per record, so it scales with the
-# visibilities.
+# DRAM bytes read + written per launch and per visibility of the main
+# kernels, from ncu captures (dram__bytes_read.sum + dram__bytes_write.sum)
+# of the 8.26M-visibility case (64 time steps): k_grid_mma 481.40 MB,
+# k_grid_tiled (row lanes) 484.11 MB, k_degrid_tiled 286.84 MB.  The traffic
+# is per record, so it scales with the visibilities.
 NCU_VIS = 64 * 2016 * 64
-DRAM_BYTES_PER_VIS = {"k_grid_tiled": 484.11e6 / NCU_VIS, "k_degrid_tiled": 286.84e6 / NCU_VIS}
+DRAM_BYTES_PER_VIS = {"k_grid_mma": 481.40e6 / NCU_VIS, "k_grid_tiled": 484.11e6 / NCU_VIS,
+                      "k_degrid_tiled": 286.84e6 / NCU_VIS}
 
 
 def max_over_ranks(ms, world, device=None):
@@ -418,7 +419,10 @@ def main():
     peak, peak_kind = load_peaks()
     bytes_grid = n_corr * 12 + nt * nb * 24 + nx * ny * npol * 8
     bytes_degrid = n_corr * 9 + nt * nb * 24 + nx * ny * npol * 8
-    dom = ("k_grid_tiled", bytes_grid, t_grid_k) if t_grid_k >= t_degrid_k else \
+    from astroviper_b200 import _lib
+    grid_kernel = ("k_grid_mma" if _lib.lib().av_tune_get(_lib.AV_TUNE_GRID_LANES) ==
+                   _lib.AV_GRID_LANES_MMA else "k_grid_tiled")
+    dom = (grid_kernel, bytes_grid, t_grid_k) if t_grid_k >= t_degrid_k else \
         ("k_degrid_tiled", bytes_degrid, t_degrid_k)
     achieved = dom[1] / (dom[2] / 1e3) / 1e9
     line = {
