@@ -102,8 +102,9 @@ __global__ void k_pswf_kernel4d(double *out, int os, int support, int n_os) {
 }
 
 // ------------------------------------------------------------ tuning ---
-constexpr int kTuneKnobs = 3;
-static std::atomic<int64_t> g_tune[kTuneKnobs] = {{16}, {16}, {AV_GRID_LANES_MMA}};
+constexpr int kTuneKnobs = 4;
+static std::atomic<int64_t> g_tune[kTuneKnobs] = {
+    {16}, {16}, {AV_GRID_LANES_MMA}, {AV_DEGRID_LANES_TF32}};
 
 int64_t tune_value(int knob) {
   return (knob >= 0 && knob < kTuneKnobs) ? g_tune[knob].load() : 0;
@@ -130,6 +131,9 @@ int av_tune_set(int knob, int64_t value) {
                (long long)value);
   AV_CHECK_ARG(knob != AV_TUNE_GRID_LANES || value <= 2,
                "av_tune_set: AV_TUNE_GRID_LANES takes 1 (mma) or 2 (rows), not %lld",
+               (long long)value);
+  AV_CHECK_ARG(knob != AV_TUNE_DEGRID_LANES || value <= 2,
+               "av_tune_set: AV_TUNE_DEGRID_LANES takes 1 (tf32) or 2 (fp32), not %lld",
                (long long)value);
   g_tune[knob].store(value);
   return AV_OK;

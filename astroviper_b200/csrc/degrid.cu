@@ -503,6 +503,308 @@ __global__ void __launch_bounds__(DT_THREADS) k_degrid_tiled(TiledDegridArgs a) 
   }
 }
 
+// ------------------------------------------------------- tensor cores ----
+// k_degrid_tc: the tiled degridder's fast store path (complex64 values, 4
+// visibility and 4 grid polarisations, no flags, no phase) on the TF32 tensor
+// path.  For one cell the degridded values of 16 samples are a matrix product
+//   D[s][q] = sum over k of W[s][k] P[k][q],   k = (r, c) in 8 x 8,
+// with W[s][(r, c)] = cu_s[r] cv_s[c] (the sample's tap products) and
+// P[(r, c)][q] the cell's footprint value at row r, column c for output q =
+// (grid polarisation, real | imaginary): eight k-steps of
+// mma.sync.m16n8k8.tf32 per 16 samples.  TF32 keeps 11 significant bits, so
+// both operands are split into a TF32 high part and the TF32-rounded
+// remainder, and the products hi.hi, hi.lo and lo.hi are accumulated in FP32
+// in three independent chains; what is left out is below 2^-22 of each
+// product.  Fragment layout (lane = 4 g + t): a = W[g][t], W[g + 8][t],
+// W[g][t + 4], W[g + 8][t + 4]; b = P[t][g], P[t + 4][g]; d = D[g][2t, 2t + 1],
+// D[g + 8][2t, 2t + 1].  Lane (g, t) thus computes the tap products of samples
+// g and g + 8 for columns t and t + 4, holds the patch values of output g, and
+// receives polarisation t of samples g and g + 8.
+constexpr int TC_THREADS = 256;
+constexpr int TC_ROUND = 64;  // records a warp stages per round (two per lane)
+
+template <int S>
+struct TCSmem {
+  static constexpr int W = TILE + S - 1;
+  static constexpr int RW = 8;  // taps 0-7 of a row, zero past the support
+  static constexpr size_t tab_bytes = 256 * RW * sizeof(float);
+  static constexpr size_t rs_bytes = 256 * sizeof(double);
+  static constexpr size_t rec_bytes = (size_t)(TC_THREADS / 32) * TC_ROUND * sizeof(Rec);
+  static constexpr size_t inv_bytes = (size_t)(TC_THREADS / 32) * TC_ROUND * sizeof(float);
+  static constexpr size_t off_rec = tab_bytes + rs_bytes;
+  static constexpr size_t off_inv = off_rec + rec_bytes;
+  static constexpr size_t off_sub = off_inv + inv_bytes;
+  static constexpr size_t sub_bytes = (size_t)W * W * 4 * sizeof(float2);  // [cell][pol]
+  static constexpr size_t total = off_sub + sub_bytes;
+  static_assert(off_sub % 16 == 0, "alignment");
+  static_assert(S <= 8, "an 8 x 8 footprint");
+};
+
+__device__ __forceinline__ uint32_t tf32_rna(float x) {
+  uint32_t r;
+  asm("cvt.rna.tf32.f32 %0, %1;\n" : "=r"(r) : "f"(x));
+  return r;
+}
+
+// x = hi + lo, both TF32 (lo: the remainder rounded to TF32)
+__device__ __forceinline__ void tf32_split(float x, uint32_t &hi, uint32_t &lo) {
+  hi = tf32_rna(x);
+  lo = tf32_rna(x - __uint_as_float(hi));
+}
+
+// x = hi + lo with hi in TF32 and lo the exact FP32 remainder, which the
+// tensor core reads as TF32 by dropping its 13 low bits (a relative error of
+// at most 2^-10 of lo, 2^-21 of x)
+__device__ __forceinline__ void tf32_split_fast(float x, uint32_t &hi, uint32_t &lo) {
+  hi = tf32_rna(x);
+  lo = __float_as_uint(x - __uint_as_float(hi));
+}
+
+__device__ __forceinline__ void mma_tf32(float (&d)[4], uint32_t a0, uint32_t a1, uint32_t a2,
+                                         uint32_t a3, uint32_t b0, uint32_t b1) {
+  asm("mma.sync.aligned.m16n8k8.row.col.f32.tf32.tf32.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, "
+      "{%8,%9}, {%0,%1,%2,%3};\n"
+      : "+f"(d[0]), "+f"(d[1]), "+f"(d[2]), "+f"(d[3])
+      : "r"(a0), "r"(a1), "r"(a2), "r"(a3), "r"(b0), "r"(b1));
+}
+
+template <int S>
+__global__ void __launch_bounds__(TC_THREADS, 3) k_degrid_tc(TiledDegridArgs a) {
+  using M = TCSmem<S>;
+  constexpr int W = M::W, RW = M::RW, WARPS = TC_THREADS / 32;
+  constexpr unsigned FULL = 0xffffffffu;
+  extern __shared__ __align__(16) unsigned char smem[];
+  float *tab = (float *)smem;
+  double *rs = (double *)(smem + M::tab_bytes);
+  Rec *st_rec = (Rec *)(smem + M::off_rec);
+  float *st_inv = (float *)(smem + M::off_inv);
+  float2 *sub = (float2 *)(smem + M::off_sub);
+  const DegridArgs &d = a.d;
+
+  __shared__ int s_chunk;
+  const uint32_t n_rec = *a.n_rec;
+  const uint32_t n_all = (uint32_t)a.n_rows;  // store mode: every sample is written
+  const int64_t n_chunks = ((int64_t)n_all + a.chunk - 1) / a.chunk;
+  build_tap_tables_d<S, RW>(tab, rs, d.cf, a.cgk_len, d.sampling);
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int g = lane >> 2, t = lane & 3;
+  // output polarisation t takes grid polarisation polmap[t], held by lane 4 g + polmap[t]
+  int src = -1;
+  {
+    const int v = d.polmap[t];
+    if (v >= 0 && v < 4 && v < d.g_npol) src = 4 * g + v;
+  }
+  const int64_t gplane = d.g_n2 * d.g_n3;
+
+  for (;;) {
+    __syncthreads();  // tables built; the previous chunk is done with sub and s_chunk
+    if (threadIdx.x == 0) s_chunk = (int)atomicAdd(&a.sched[0], 1u);
+    __syncthreads();
+    const int64_t ch = s_chunk;
+    if (ch >= n_chunks) break;
+    const uint32_t r0 = (uint32_t)(ch * a.chunk);
+    const uint32_t r1 = (uint32_t)min((int64_t)n_all, (int64_t)r0 + a.chunk);
+    if (r1 > n_rec) {  // skipped samples (after the usable records) get zeros
+      const uint32_t z0 = max(r0, n_rec);
+      for (uint32_t rb = z0; rb < r1; rb += TC_THREADS) {
+        const uint32_t r = rb + threadIdx.x;
+        if (r >= r1) continue;
+        const int64_t row = a.recs[r].row;
+        for (int p = 0; p < 4; ++p) put_value(d, 0, row * 4 + p, 0.0, 0.0);
+      }
+    }
+    const uint32_t v1 = min(r1, n_rec);
+    if (r0 >= v1) continue;
+
+    int tt = find_tile_d(a.tile_start, a.n_tiles, r0);
+    uint32_t seg_lo = r0;
+    while (seg_lo < v1) {
+      const uint32_t t_end = a.tile_start[tt + 1];
+      const uint32_t seg_hi = min(v1, t_end);
+      if (seg_hi <= seg_lo) {
+        ++tt;
+        continue;
+      }
+      const int64_t plane = tt / (a.ntu * a.ntv);
+      const int64_t trem = tt - plane * a.ntu * a.ntv;
+      const int tu = (int)(trem / a.ntv), tv = (int)(trem - (int64_t)tu * a.ntv);
+      __syncthreads();  // previous segment's readers are done with sub
+      for (int i0 = 0; i0 < W * W * 4; i0 += TC_THREADS) {
+        const int i = i0 + threadIdx.x;
+        if (i >= W * W * 4) continue;
+        const int cell = i >> 2, gp = i & 3;
+        const int iu = cell / W, iv = cell - iu * W;
+        const int64_t gu = (int64_t)tu * TILE + iu, gv = (int64_t)tv * TILE + iv;
+        float2 v = make_float2(0.f, 0.f);
+        if (gp < d.g_npol && gu < d.g_n2 && gv < d.g_n3) {
+          const int64_t gi = (plane * d.g_npol + gp) * gplane + gu * d.g_n3 + gv;
+          if (d.grid_c128) {
+            const double2 x = ((const double2 *)d.grid)[gi];
+            v = make_float2((float)x.x, (float)x.y);
+          } else {
+            v = ((const float2 *)d.grid)[gi];
+          }
+        }
+        sub[i] = v;
+      }
+      __syncthreads();
+
+      // this warp's slice of the segment, in rounds of 64 records (two per
+      // lane): records and 1 / norm go to the warp's staging area, from which
+      // the lanes of a group read the samples they need
+      const uint32_t seg_n = seg_hi - seg_lo;
+      const uint32_t w_lo = seg_lo + (uint32_t)(((uint64_t)seg_n * warp) / WARPS);
+      const uint32_t w_hi = seg_lo + (uint32_t)(((uint64_t)seg_n * (warp + 1)) / WARPS);
+      const int n_rounds = (int)((w_hi - w_lo + TC_ROUND - 1) / TC_ROUND);
+      Rec *wrec = st_rec + warp * TC_ROUND;
+      float *winv = st_inv + warp * TC_ROUND;
+      int cur = -1;
+      uint32_t bh[8][2], bl[8][2];  // patch fragments of the current cell
+#pragma unroll
+      for (int jj = 0; jj < 8; ++jj) bh[jj][0] = bh[jj][1] = bl[jj][0] = bl[jj][1] = 0u;
+      Rec na, nb;
+      if (w_lo + lane < w_hi) na = a.recs[w_lo + lane];
+      if (w_lo + 32 + lane < w_hi) nb = a.recs[w_lo + 32 + lane];
+      for (int rd = 0; rd < n_rounds; ++rd) {
+        const uint32_t r = w_lo + (uint32_t)rd * TC_ROUND + lane;
+        const bool va = r < w_hi, vb = r + 32 < w_hi;
+        const Rec ra = na, rb = nb;
+        if (r + TC_ROUND < w_hi) na = a.recs[r + TC_ROUND];
+        if (r + TC_ROUND + 32 < w_hi) nb = a.recs[r + TC_ROUND + 32];
+        const int ka = va ? ((int)ra.du | ((int)ra.dv << 8)) : -1;
+        const int kb = vb ? ((int)rb.du | ((int)rb.dv << 8)) : -1;
+        __syncwarp();  // the previous round's groups are done with the staging area
+        if (va) {
+          const double norm = rs[ra.ou] * rs[ra.ov];
+          // 1 / norm in FP64, the scaling in FP32; zero-norm samples get 0
+          wrec[lane] = ra;
+          winv[lane] = norm != 0.0 ? (float)(1.0 / norm) : 0.f;
+        }
+        if (vb) {
+          const double norm = rs[rb.ou] * rs[rb.ov];
+          wrec[lane + 32] = rb;
+          winv[lane + 32] = norm != 0.0 ? (float)(1.0 / norm) : 0.f;
+        }
+        int pa = __shfl_up_sync(FULL, ka, 1);
+        if (lane == 0) pa = cur;
+        int pb = __shfl_up_sync(FULL, kb, 1);
+        const int ka_last = __shfl_sync(FULL, ka, 31);
+        if (lane == 0) pb = ka_last;
+        const unsigned long long starts =
+            (unsigned long long)__ballot_sync(FULL, ka >= 0 && ka != pa) |
+            ((unsigned long long)__ballot_sync(FULL, kb >= 0 && kb != pb) << 32);
+        __syncwarp();
+        const int jn = (int)min((uint32_t)TC_ROUND, w_hi - (w_lo + (uint32_t)rd * TC_ROUND));
+        int j = 0;
+        while (j < jn) {
+          if ((starts >> j) & 1ull) {
+            const Rec rj = wrec[j];
+            cur = (int)rj.du | ((int)rj.dv << 8);
+            const int du = rj.du, dv = rj.dv;
+#pragma unroll
+            for (int jj = 0; jj < 8; ++jj) {
+              float x0 = 0.f, x1 = 0.f;
+              if (jj < S && t < S) {
+                const float2 v = sub[((du + jj) * W + dv + t) * 4 + (g >> 1)];
+                x0 = (g & 1) ? v.y : v.x;
+              }
+              if (jj < S && t + 4 < S) {
+                const float2 v = sub[((du + jj) * W + dv + t + 4) * 4 + (g >> 1)];
+                x1 = (g & 1) ? v.y : v.x;
+              }
+              tf32_split(x0, bh[jj][0], bl[jj][0]);
+              tf32_split(x1, bh[jj][1], bl[jj][1]);
+            }
+          }
+          const unsigned long long later = j < 63 ? (starts & (~1ull << j)) : 0ull;
+          const int j1 = later ? min(jn, __ffsll((long long)later) - 1) : jn;
+          for (int j0 = j; j0 < j1; j0 += 16) {
+            // samples j0 + g and j0 + g + 8 of the round (an empty slot reads
+            // sample j0 and contributes a zero row of W)
+            const int sg = j0 + g, sh = j0 + g + 8;
+            const bool vg = sg < j1, vh = sh < j1;
+            const Rec recg = wrec[vg ? sg : j0], rech = wrec[vh ? sh : j0];
+            const float invg = winv[vg ? sg : j0], invh = winv[vh ? sh : j0];
+            const int oug = recg.ou, ovg = recg.ov, ouh = rech.ou, ovh = rech.ov;
+            const float *cug = tab + oug * RW, *cuh = tab + ouh * RW;  // row taps
+            // an empty slot of the group contributes a zero row of W
+            const float cvg0 = vg ? tab[ovg * RW + t] : 0.f;
+            const float cvg1 = vg ? tab[ovg * RW + t + 4] : 0.f;
+            const float cvh0 = vh ? tab[ovh * RW + t] : 0.f;
+            const float cvh1 = vh ? tab[ovh * RW + t + 4] : 0.f;
+            float d0[4] = {0.f, 0.f, 0.f, 0.f}, d1[4] = {0.f, 0.f, 0.f, 0.f},
+                  d2[4] = {0.f, 0.f, 0.f, 0.f};
+#pragma unroll
+            for (int jj = 0; jj < S; ++jj) {  // rows past the support are zero
+              uint32_t a0h, a0l, a1h, a1l, a2h, a2l, a3h, a3l;
+              tf32_split_fast(cug[jj] * cvg0, a0h, a0l);
+              tf32_split_fast(cuh[jj] * cvh0, a1h, a1l);
+              tf32_split_fast(cug[jj] * cvg1, a2h, a2l);
+              tf32_split_fast(cuh[jj] * cvh1, a3h, a3l);
+              mma_tf32(d0, a0h, a1h, a2h, a3h, bh[jj][0], bh[jj][1]);
+              mma_tf32(d1, a0h, a1h, a2h, a3h, bl[jj][0], bl[jj][1]);
+              mma_tf32(d2, a0l, a1l, a2l, a3l, bh[jj][0], bh[jj][1]);
+            }
+            const float gre = (d2[0] + d1[0]) + d0[0], gim = (d2[1] + d1[1]) + d0[1];
+            const float hre = (d2[2] + d1[2]) + d0[2], him = (d2[3] + d1[3]) + d0[3];
+            // polarisation t of samples g and g + 8
+            const float xgre = __shfl_sync(FULL, gre, src & 31);
+            const float xgim = __shfl_sync(FULL, gim, src & 31);
+            const float xhre = __shfl_sync(FULL, hre, src & 31);
+            const float xhim = __shfl_sync(FULL, him, src & 31);
+            float2 *out = (float2 *)d.values;
+            if (vg)
+              out[(int64_t)recg.row * 4 + t] = src >= 0 ? make_float2(__fmul_rn(xgre, invg),
+                                                                      __fmul_rn(xgim, invg))
+                                                        : make_float2(0.f, 0.f);
+            if (vh)
+              out[(int64_t)rech.row * 4 + t] = src >= 0 ? make_float2(__fmul_rn(xhre, invh),
+                                                                      __fmul_rn(xhim, invh))
+                                                        : make_float2(0.f, 0.f);
+          }
+          j = j1;
+        }
+      }
+      seg_lo = seg_hi;
+      if (seg_hi == t_end) ++tt;
+    }
+  }
+  // every CTA has taken its last chunk: the last one to get here re-arms
+  if (threadIdx.x == 0) {
+    __threadfence();
+    if (atomicAdd(&a.sched[1], 1u) == gridDim.x - 1) {
+      a.sched[0] = 0u;
+      a.sched[1] = 0u;
+      __threadfence();
+    }
+  }
+}
+
+template <int S>
+static int launch_degrid_tc(const TiledDegridArgs &a, int64_t nblocks, cudaStream_t st) {
+  size_t smem = TCSmem<S>::total;
+  static int resident[64] = {0};
+  int dev = 0;
+  AV_CUDA(cudaGetDevice(&dev));
+  if (dev < 0 || dev >= 64) {
+    set_error("av_degrid_tiled: device %d beyond the 64 this library tracks", dev);
+    return AV_ERR_UNSUPPORTED;
+  }
+  if (resident[dev] == 0) {
+    if (smem > 48 * 1024)
+      AV_CUDA(cudaFuncSetAttribute(k_degrid_tc<S>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                   (int)smem));
+    int per_sm = 0;
+    AV_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_degrid_tc<S>, TC_THREADS,
+                                                          smem));
+    resident[dev] = (per_sm > 0 ? per_sm : 1) * sm_count();
+  }
+  if (nblocks > resident[dev]) nblocks = resident[dev];
+  k_degrid_tc<S><<<(unsigned)nblocks, TC_THREADS, smem, st>>>(a);
+  AV_LAUNCH_CHECK();
+  return AV_OK;
+}
+
 template <int S, int NPG>
 static int launch_degrid_tiled(const TiledDegridArgs &a, int64_t nblocks, cudaStream_t st) {
   // persistent CTAs: at most as many as are resident at once
@@ -529,10 +831,18 @@ static int launch_degrid_tiled(const TiledDegridArgs &a, int64_t nblocks, cudaSt
   return AV_OK;
 }
 
+// The TF32 tensor-core kernel for the fast store path with 4 grid
+// polarisations and supports up to 8, unless AV_TUNE_DEGRID_LANES asks for
+// the FP32 kernel.
 template <int S>
 static int degrid_dispatch_npg(const TiledDegridArgs &a, int npg, int64_t nb, cudaStream_t st) {
   if (npg == 1) return launch_degrid_tiled<S, 1>(a, nb, st);
   if (npg == 2) return launch_degrid_tiled<S, 2>(a, nb, st);
+  if constexpr (S <= 8) {
+    if (a.fast_out && a.d.g_npol == 4 &&
+        tune_value(AV_TUNE_DEGRID_LANES) == AV_DEGRID_LANES_TF32)
+      return launch_degrid_tc<S>(a, nb, st);
+  }
   return launch_degrid_tiled<S, 4>(a, nb, st);
 }
 

@@ -237,6 +237,45 @@ def test_tiled_degrid_every_support(support, os_):
     assert rel(v.cpu().numpy(), ref) <= 1e-6
 
 
+@pytest.fixture(params=["tf32", "fp32"])
+def degrid_lanes(request):
+    """Runs a test under each setting of the tiled degridder's fast store
+    path: TF32 tensor-core tiles with split operands, and FP32 FMA."""
+    from astroviper_b200 import _lib
+    L = _lib.lib()
+    old = L.av_tune_get(_lib.AV_TUNE_DEGRID_LANES)
+    want = (_lib.AV_DEGRID_LANES_TF32 if request.param == "tf32"
+            else _lib.AV_DEGRID_LANES_FP32)
+    assert L.av_tune_set(_lib.AV_TUNE_DEGRID_LANES, want) == _lib.AV_OK
+    yield request.param
+    L.av_tune_set(_lib.AV_TUNE_DEGRID_LANES, old)
+
+
+@pytest.mark.parametrize("polmap", [(0, 1, 2, 3), (2, 0, 3, 1)])
+@pytest.mark.parametrize("support", [3, 4, 5, 6, 7, 8])
+def test_degrid_fast_store_every_support(support, polmap, degrid_lanes):
+    """The fast store path (complex64 values, 4 visibility and 4 grid
+    polarisations, no flags or phase) against the oracle's dgrid_numba on a
+    random 4-polarisation grid, for every support it covers and a permuted
+    polarisation map; samples the degridder skips get zeros."""
+    g = golden("degrid.npz")
+    rng = np.random.default_rng(100 + support)
+    nt, nb = g["uvw"].shape[:2]
+    n2, n3 = g["grid"].shape[2:]
+    grid = rng.normal(size=(2, 4, n2, n3)) + 1j * rng.normal(size=(2, 4, n2, n3))
+    cf = O.create_prolate_spheroidal_kernel_1D(100, support)
+    pm = np.array(polmap, dtype=np.int32)
+    ref = np.zeros((nt, nb, 3, 4), complex)
+    O.dgrid_numba(g["uvw"], np.zeros((nt, nb)), ref, np.zeros((nt, nb, 3, 4), bool),
+                  g["scale"], g["offset"], grid, g["freq"], 299792458.0, support, 100, cf,
+                  g["chanmap"], pm)
+    v = K().degrid(torch.as_tensor(grid), g["uvw"], g["freq"], g["scale"][:2], g["offset"][:2],
+                   g["chanmap"], pm, cf, support, 100, nvchan=3, nvpol=4, precision="fp32",
+                   accumulate=False)
+    assert v.dtype == torch.complex64
+    assert rel(v.cpu().numpy(), ref) <= 1e-6
+
+
 @pytest.fixture(params=["mma", "rows"])
 def grid_lanes(request):
     """Runs a test under each of the tiled gridder's lane mappings: FP64
@@ -324,7 +363,7 @@ def test_tiled_grid_long_runs_match_fp64(grid_lanes):
     assert np.allclose(s32.cpu().numpy(), s64.cpu().numpy(), rtol=1e-12)
 
 
-def test_degrid_store_mode_four_pol_fast_output():
+def test_degrid_store_mode_four_pol_fast_output(degrid_lanes):
     """Store mode, complex64, 4 polarisations, no flags / phase: the kernel
     writes each sample's 4 values as two 16-byte stores with FP32 scaling;
     against the FP64 plain degridder on a slice of the 33M workload."""
