@@ -33,6 +33,7 @@ SIGNATURES = {
     "av_version": (_i, []),
     "av_last_error": (ctypes.c_char_p, []),
     "av_device_sm_count": (_i, []),
+    "av_probe_fp64_mma": (_i, [_vp, _vp]),
     "av_launch_count": (ctypes.c_ulonglong, []),
     "av_tune_set": (_i, [_i, _i64]),
     "av_tune_get": (_i64, [_i]),

@@ -110,11 +110,76 @@ int64_t tune_value(int knob) {
   return (knob >= 0 && knob < kTuneKnobs) ? g_tune[knob].load() : 0;
 }
 
+// ------------------------------------------------------------ probes ---
+// FP64 tensor rate: every warp runs four independent chains of
+// mma.sync.m16n8k4.f64 (one dependent chain already keeps an SMSP's pipe
+// full); thread 0 of each block writes one double to a static sink.
+constexpr int kProbeIters = 4096;
+constexpr int kProbeThreads = 256;
+static __device__ double g_probe_sink[4096];
+
+__global__ void __launch_bounds__(kProbeThreads) k_probe_dmma(double s) {
+  double d[4][4];
+#pragma unroll
+  for (int j = 0; j < 4; ++j) d[j][0] = d[j][1] = d[j][2] = d[j][3] = 0.0;
+  const double a0 = s + threadIdx.x * 1e-6, a1 = s * 0.5, b = s - threadIdx.x * 1e-6;
+  for (int it = 0; it < kProbeIters; ++it) {
+#pragma unroll
+    for (int j = 0; j < 4; ++j)
+      asm volatile(
+          "mma.sync.aligned.m16n8k4.row.col.f64.f64.f64.f64 {%0,%1,%2,%3}, {%4,%5}, {%6}, "
+          "{%0,%1,%2,%3};\n"
+          : "+d"(d[j][0]), "+d"(d[j][1]), "+d"(d[j][2]), "+d"(d[j][3])
+          : "d"(a0), "d"(a1), "d"(b));
+  }
+  double t = 0.0;
+#pragma unroll
+  for (int j = 0; j < 4; ++j) t += d[j][0] + d[j][1] + d[j][2] + d[j][3];
+  if (threadIdx.x == 0) g_probe_sink[blockIdx.x & 4095] = t;
+}
+
 }  // namespace av
 
 using namespace av;
 
 extern "C" {
+
+int av_probe_fp64_mma(double *tflops, void *stream) {
+  clear_error();
+  AV_CHECK_ARG(tflops, "av_probe_fp64_mma: null pointer");
+  cudaStream_t st = as_stream(stream);
+  const int blocks = sm_count() * 8;
+  cudaEvent_t e0 = nullptr, e1 = nullptr;
+  AV_CUDA(cudaEventCreate(&e0));
+  if (cudaEventCreate(&e1) != cudaSuccess) {
+    cudaEventDestroy(e0);
+    set_error("av_probe_fp64_mma: event creation failed");
+    return AV_ERR_CUDA;
+  }
+  int rc = AV_OK;
+  float ms = 0.f;
+  k_probe_dmma<<<blocks, kProbeThreads, 0, st>>>(0.999);  // warm-up
+  count_launch();
+  cudaEventRecord(e0, st);
+  for (int r = 0; r < 3; ++r) {
+    k_probe_dmma<<<blocks, kProbeThreads, 0, st>>>(0.999);
+    count_launch();
+  }
+  cudaEventRecord(e1, st);
+  cudaError_t err = cudaEventSynchronize(e1);
+  if (err == cudaSuccess) err = cudaGetLastError();
+  if (err == cudaSuccess) err = cudaEventElapsedTime(&ms, e0, e1);
+  if (err != cudaSuccess || ms <= 0.f) {
+    set_error("av_probe_fp64_mma: %s", cudaGetErrorString(err));
+    rc = AV_ERR_CUDA;
+  } else {
+    const double flop = 3.0 * blocks * (kProbeThreads / 32) * (double)kProbeIters * 4 * 512 * 2;
+    *tflops = flop / (ms * 1e-3) / 1e12;
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  return rc;
+}
 
 int av_version(void) { return 100; }
 

@@ -128,11 +128,11 @@ class ClockSampler:
 # DRAM bytes read + written per launch and per visibility of the main
 # kernels, from ncu captures (dram__bytes_read.sum + dram__bytes_write.sum)
 # of the 8.26M-visibility case (64 time steps): k_grid_mma 481.40 MB,
-# k_grid_tiled (row lanes) 484.11 MB, k_degrid_tiled 286.84 MB.  The traffic
-# is per record, so it scales with the visibilities.
+# k_grid_tiled (row lanes) 484.11 MB, k_degrid_tc 312.69 MB, k_degrid_tiled
+# 286.84 MB.  The traffic is per record, so it scales with the visibilities.
 NCU_VIS = 64 * 2016 * 64
 DRAM_BYTES_PER_VIS = {"k_grid_mma": 481.40e6 / NCU_VIS, "k_grid_tiled": 484.11e6 / NCU_VIS,
-                      "k_degrid_tiled": 286.84e6 / NCU_VIS}
+                      "k_degrid_tc": 312.69e6 / NCU_VIS, "k_degrid_tiled": 286.84e6 / NCU_VIS}
 
 
 def max_over_ranks(ms, world, device=None):
@@ -422,9 +422,23 @@ def main():
     from astroviper_b200 import _lib
     grid_kernel = ("k_grid_mma" if _lib.lib().av_tune_get(_lib.AV_TUNE_GRID_LANES) ==
                    _lib.AV_GRID_LANES_MMA else "k_grid_tiled")
+    degrid_kernel = ("k_degrid_tc" if _lib.lib().av_tune_get(_lib.AV_TUNE_DEGRID_LANES) ==
+                     _lib.AV_DEGRID_LANES_TF32 else "k_degrid_tiled")
     dom = (grid_kernel, bytes_grid, t_grid_k) if t_grid_k >= t_degrid_k else \
-        ("k_degrid_tiled", bytes_degrid, t_degrid_k)
+        (degrid_kernel, bytes_degrid, t_degrid_k)
     achieved = dom[1] / (dom[2] / 1e3) / 1e9
+    # the gridder's FP64 footprint sums against the device's FP64 tensor rate:
+    # 49 taps x 2 FMA per correlation plus the 49 tap products per sample
+    import ctypes
+    fp64_peak = ctypes.c_double(0.0)
+    fp64_tensor = None
+    if _lib.lib().av_probe_fp64_mma(ctypes.byref(fp64_peak), None) == 0 and fp64_peak.value > 0:
+        grid_flops = n_corr * 196 + n_vis * 49
+        ach = grid_flops / (t_grid_k / 1e3) / 1e12
+        fp64_tensor = {"kernel": grid_kernel, "achieved": ach, "peak": fp64_peak.value,
+                       "unit": "TFLOP/s", "frac": ach / fp64_peak.value,
+                       "flops": grid_flops,
+                       "peak_source": "av_probe_fp64_mma (mma.sync.m16n8k4.f64) on this GPU"}
     line = {
         "metric": METRIC, "value": value, "unit": "Mvis/s", "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
@@ -440,6 +454,7 @@ def main():
                      "traffic_source": "ncu dram bytes of the 8.26M-vis case, scaled by vis",
                      "peak_kind": peak_kind, "algorithmic_bytes": dom[1],
                      "kernel_ms": dom[2]},
+        "fp64_tensor": fp64_tensor,
         "kernels_ms": {"grid_tiled": t_grid_k, "degrid_tiled": t_degrid_k,
                        "plan_and_rest": ms - t_grid_k - t_degrid_k},
         "fp64_plain_gridder": {"value": plain_mvis, "unit": "Mvis/s",

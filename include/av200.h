@@ -48,6 +48,13 @@ int av_version(void);
 const char *av_last_error(void);
 /* Number of SMs of the current device (for launch sizing by the host). */
 int av_device_sm_count(void);
+/* No counterpart in the reference: the FP64 tensor-core rate of the current
+ * device in TFLOP/s (mma.sync.m16n8k4.f64, 8 CTAs of 8 warps per SM, four
+ * independent chains per warp; three timed launches after one warm-up).  It
+ * is the ceiling of the gridder's FP64 footprint sums, reported beside its
+ * HBM roofline.  Synchronises the stream; writes into a 32 KiB static device
+ * array, allocates nothing. */
+int av_probe_fp64_mma(double *tflops, void *stream);
 /* Kernels launched by this library since it was loaded (all threads). */
 unsigned long long av_launch_count(void);
 

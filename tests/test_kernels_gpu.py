@@ -380,3 +380,13 @@ def test_degrid_store_mode_four_pol_fast_output(degrid_lanes):
                      (nx / 2, ny / 2), np.zeros(nchan, int), np.arange(npol), G.cgk, 7, 100,
                      nvchan=nchan, nvpol=npol, precision="fp64")
     assert rel(v.cpu().numpy(), ref.cpu().numpy()) <= 1e-6
+
+
+def test_fp64_mma_probe_reports_a_rate():
+    """The FP64 tensor-rate probe runs and returns a plausible B200 figure."""
+    import ctypes
+    from astroviper_b200 import _lib
+    v = ctypes.c_double(0.0)
+    assert _lib.lib().av_probe_fp64_mma(ctypes.byref(v), None) == _lib.AV_OK
+    assert 5.0 < v.value < 200.0
+    assert _lib.lib().av_probe_fp64_mma(None, None) == _lib.AV_ERR_ARG
