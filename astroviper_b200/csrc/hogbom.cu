@@ -13,6 +13,7 @@
 // differences are rounded separately (no FMA), the model is accumulated in
 // iteration order by one thread.
 #include <algorithm>
+#include <type_traits>
 
 #include "common.cuh"
 
@@ -28,7 +29,13 @@ struct __align__(16) HogState {
   int pad;
   double peak;   // r[py, px] for iteration `iter`
   double absval; // |peak| found (0 when no pixel exceeded 0)
-  double pad2[26];
+  // FP32: the iteration's winner as one 64-bit maximum over the CTAs, bits of
+  // |r| above the complement of 2 * index + sign (0: no pixel above 0), two
+  // of them used in turn; kpar: the one the next launch starts with
+  unsigned long long key[2];
+  int kpar;
+  int pad3;
+  double pad2[23];
 };
 static_assert(sizeof(HogState) == 256, "state size");
 
@@ -74,7 +81,8 @@ __device__ __forceinline__ bool beats(T aa, int ai, T ba, int bi) {
 
 // Grid barrier with a bounded wait (~2 s of wall time); returns false on
 // timeout and records it in the state.
-__device__ bool grid_barrier(HogState *st, int *s_flag) {
+// The last CTA to arrive clears *reset (if given) before releasing the others.
+__device__ bool grid_barrier(HogState *st, int *s_flag, unsigned long long *reset = nullptr) {
   __syncthreads();
   if (threadIdx.x == 0) {
     volatile unsigned *vgen = &st->gen;
@@ -83,6 +91,7 @@ __device__ bool grid_barrier(HogState *st, int *s_flag) {
     unsigned arrived = atomicAdd(&st->count, 1u);
     int ok = 1;
     if (arrived == gridDim.x - 1) {
+      if (reset) atomicExch(reset, 0ull);
       atomicExch(&st->count, 0u);
       __threadfence();
       atomicAdd(&st->gen, 1u);
@@ -108,6 +117,13 @@ __device__ bool grid_barrier(HogState *st, int *s_flag) {
 }
 
 constexpr int HOG_THREADS = 1024;
+// band pass for images up to HOG_NPR * HOG_THREADS columns: a thread's
+// columns are fixed, so whether the PSF window and the clean box cover them
+// is decided once per iteration and per row, not per pixel
+constexpr int HOG_NPR = 2;
+constexpr int HOG_RB = 7;  // rows whose PSF values are loaded together
+// candidates a lane loads at once in the reduction after the grid barrier
+constexpr int HOG_CPL = 4;
 
 template <typename T>
 __global__ void __launch_bounds__(HOG_THREADS, 1) k_hogbom(HogArgs<T> a) {
@@ -117,6 +133,8 @@ __global__ void __launch_bounds__(HOG_THREADS, 1) k_hogbom(HogArgs<T> a) {
   __shared__ int s_flag;
   __shared__ T s_prev;
   __shared__ int s_has_prev;
+  __shared__ int s_use_key;
+  constexpr bool KEYED = std::is_same<T, float>::value;
   const int G = gridDim.x, b = blockIdx.x;
   const int y_lo = (int)((long long)a.ny * b / G), y_hi = (int)((long long)a.ny * (b + 1) / G);
   const int nx = a.nx;
@@ -144,7 +162,7 @@ __global__ void __launch_bounds__(HOG_THREADS, 1) k_hogbom(HogArgs<T> a) {
   }
   __syncthreads();
 
-  int par = 0;
+  int par = a.init ? 0 : a.state->kpar;
   bool first = a.init != 0;
   bool stopped = false;
   for (;;) {
@@ -172,6 +190,118 @@ __global__ void __launch_bounds__(HOG_THREADS, 1) k_hogbom(HogArgs<T> a) {
     T best_abs = (T)0;
     int best_idx = -1;
     T best_val = (T)0;
+    const int npr = (nx + HOG_THREADS - 1) / HOG_THREADS;
+    const int tpr4 = nx >> 2;  // FP32, 4 pixels per thread: threads per row
+    if (std::is_same<T, float>::value && (nx & 3) == 0 && tpr4 > 0 && tpr4 <= HOG_THREADS &&
+        HOG_THREADS % tpr4 == 0) {
+      // thread t: columns c0 .. c0 + 3 of rows y_lo + t / tpr4, + rpp, ...
+      const int rpp = HOG_THREADS / tpr4;
+      const int c0 = (threadIdx.x % tpr4) * 4, rofs = threadIdx.x / tpr4;
+      // which of the 4 columns the PSF window (with an existing PSF column)
+      // and the clean box cover, once per iteration
+      const int wlo = max(x1, px - a.pnx / 2), whi = min(x2, px + a.pnx / 2 - 1);
+      unsigned wm = 0u, bm = 0u;
+#pragma unroll
+      for (int j = 0; j < 4; ++j) {
+        const int c = c0 + j;
+        if (do_sub && c >= wlo && c <= whi) wm |= 1u << j;
+        if (c >= a.xbeg && c < a.xend) bm |= 1u << j;
+      }
+      const int pxo0 = a.pnx / 2 + c0 - px;  // PSF column of c0
+      for (int iy = y_lo + rofs; iy < y_hi; iy += rpp) {
+        const int psf_y = a.pny / 2 + iy - py;
+        const bool rsub = wm != 0u && iy >= y1 && iy <= y2 && psf_y >= 0 && psf_y < a.pny;
+        float *rp = (float *)band + (size_t)(iy - y_lo) * nx + c0;
+        const float4 r4 = *(const float4 *)rp;
+        float rr[4] = {r4.x, r4.y, r4.z, r4.w};
+        if (rsub) {
+          const float *pp = (const float *)a.psf + (size_t)psf_y * a.pnx + pxo0;
+          float p4[4];
+          if (wm == 0xfu && (((uintptr_t)pp) & 15) == 0) {
+            const float4 q = __ldg((const float4 *)pp);
+            p4[0] = q.x; p4[1] = q.y; p4[2] = q.z; p4[3] = q.w;
+          } else {
+#pragma unroll
+            for (int j = 0; j < 4; ++j) p4[j] = ((wm >> j) & 1u) ? __ldg(pp + j) : 0.f;
+          }
+          const float fpv = (float)pv;
+#pragma unroll
+          for (int j = 0; j < 4; ++j)
+            if ((wm >> j) & 1u) rr[j] = __fsub_rn(rr[j], __fmul_rn(fpv, p4[j]));
+          *(float4 *)rp = make_float4(rr[0], rr[1], rr[2], rr[3]);
+        }
+        if (bm != 0u && iy >= a.ybeg && iy < a.yend) {
+#pragma unroll
+          for (int j = 0; j < 4; ++j) {
+            if (!((bm >> j) & 1u)) continue;
+            if (a.mask != nullptr && !(a.mask[(size_t)iy * nx + c0 + j] > (T)0.5)) continue;
+            const float v = rr[j] < 0.f ? -rr[j] : rr[j];
+            if ((T)v > best_abs) {
+              best_abs = (T)v;
+              best_idx = iy * nx + c0 + j;
+              best_val = (T)rr[j];
+            }
+          }
+        }
+      }
+    } else if (npr <= HOG_NPR) {
+      // this thread's columns ix = threadIdx.x + k * HOG_THREADS: whether the
+      // PSF window (with an existing PSF column) and the clean box cover them
+      const int wlo = max(x1, px - a.pnx / 2), whi = min(x2, px + a.pnx / 2 - 1);
+      bool colw[HOG_NPR], colb[HOG_NPR];
+      int pxo[HOG_NPR];
+#pragma unroll
+      for (int k = 0; k < HOG_NPR; ++k) {
+        const int ix = threadIdx.x + k * HOG_THREADS;
+        const bool valid = k < npr && ix < nx;
+        colw[k] = valid && do_sub && ix >= wlo && ix <= whi;
+        colb[k] = valid && ix >= a.xbeg && ix < a.xend;
+        pxo[k] = a.pnx / 2 + ix - px;
+      }
+      for (int iy0 = y_lo; iy0 < y_hi; iy0 += HOG_RB) {
+        // the PSF values of HOG_RB rows through the read-only path, all
+        // issued before the band is touched: one L2 round trip per batch
+        T pk[HOG_RB][HOG_NPR];
+#pragma unroll
+        for (int q = 0; q < HOG_RB; ++q) {
+          const int iy = iy0 + q;
+          const int psf_y = a.pny / 2 + iy - py;
+          const bool rsub = iy < y_hi && iy >= y1 && iy <= y2 && psf_y >= 0 && psf_y < a.pny;
+          const T *prow = a.psf + (size_t)(rsub ? psf_y : 0) * a.pnx;
+#pragma unroll
+          for (int k = 0; k < HOG_NPR; ++k)
+            pk[q][k] = (rsub && colw[k]) ? __ldg(prow + pxo[k]) : (T)0;
+        }
+#pragma unroll
+        for (int q = 0; q < HOG_RB; ++q) {
+          const int iy = iy0 + q;
+          if (iy >= y_hi) break;  // the same for every thread of the block
+          const int psf_y = a.pny / 2 + iy - py;
+          const bool rsub = iy >= y1 && iy <= y2 && psf_y >= 0 && psf_y < a.pny;
+          const bool rbox = iy >= a.ybeg && iy < a.yend;
+          T *rrow = band + (size_t)(iy - y_lo) * nx;
+#pragma unroll
+          for (int k = 0; k < HOG_NPR; ++k) {
+            const int ix = threadIdx.x + k * HOG_THREADS;
+            if (k >= npr || ix >= nx) continue;
+            T r = rrow[ix];
+            if (rsub && colw[k]) {
+              r = rn_sub(r, rn_mul(pv, pk[q][k]));
+              rrow[ix] = r;
+            }
+            if (rbox && colb[k] &&
+                (a.mask == nullptr || a.mask[(size_t)iy * nx + ix] > (T)0.5)) {
+              const T v = r < (T)0 ? -r : r;
+              if (v > best_abs) {
+                best_abs = v;
+                best_idx = iy * nx + ix;
+                best_val = r;
+              }
+            }
+          }
+        }
+      }
+    } else
     for (int iy = y_lo; iy < y_hi; ++iy) {
       const bool row_sub = do_sub && iy >= y1 && iy <= y2;
       const bool row_box = iy >= a.ybeg && iy < a.yend;
@@ -247,30 +377,64 @@ __global__ void __launch_bounds__(HOG_THREADS, 1) k_hogbom(HogArgs<T> a) {
         c.has_prev = s_has_prev;
         c.at_prev = s_has_prev ? s_prev : (T)0;
         a.cand[par * G + b] = c;
+        if (KEYED && best_idx >= 0) {
+          const uint32_t code = 2u * (uint32_t)best_idx + (best_val < (T)0 ? 1u : 0u);
+          const unsigned long long key =
+              ((unsigned long long)__float_as_uint((float)best_abs) << 32) |
+              (unsigned long long)(0xffffffffu - code);
+          atomicMax(&a.state->key[par], key);
+        }
       }
     }
-    if (!grid_barrier(a.state, &s_flag)) break;
-    // every CTA reduces all candidates the same way
-    if (warp == 0) {
+    if (!grid_barrier(a.state, &s_flag, KEYED ? &a.state->key[par ^ 1] : nullptr)) break;
+    // FP32: the winner from the 64-bit maximum (one load); otherwise, and
+    // when no pixel was above 0, every CTA reduces all candidates the same way
+    if (KEYED) {
+      if (threadIdx.x == 0) {
+        const unsigned long long kv = *(volatile unsigned long long *)&a.state->key[par];
+        s_use_key = kv != 0ull;
+        if (kv != 0ull) {
+          const uint32_t code = 0xffffffffu - (uint32_t)kv;
+          const float av = __uint_as_float((uint32_t)(kv >> 32));
+          s_abs[0] = (T)av;
+          s_idx[0] = (int)(code >> 1);
+          s_val[0] = (code & 1u) ? (T)-av : (T)av;
+        }
+      }
+      __syncthreads();
+    }
+    if (!(KEYED && s_use_key) && warp == 0) {
       T ga = (T)0, gv = (T)0, gprev = (T)0;
       int gi = -1, ghp = 0;
-      for (int k = lane; k < G; k += 32) {
-        // L2 loads: other CTAs wrote these before the barrier
-        const HogCand<T> *cp = a.cand + par * G + k;
-        HogCand<T> c;
-        c.absval = __ldcg(&cp->absval);
-        c.val = __ldcg(&cp->val);
-        c.at_prev = __ldcg(&cp->at_prev);
-        c.idx = __ldcg(&cp->idx);
-        c.has_prev = __ldcg(&cp->has_prev);
-        if (beats(c.absval, c.idx, ga, gi)) {
-          ga = c.absval;
-          gi = c.idx;
-          gv = c.val;
+      for (int k0 = 0; k0 < G; k0 += 32 * HOG_CPL) {
+        // L2 loads (other CTAs wrote these before the barrier), HOG_CPL
+        // candidates per lane issued together, then reduced in index order
+        HogCand<T> c[HOG_CPL];
+#pragma unroll
+        for (int q = 0; q < HOG_CPL; ++q) {
+          const int k = k0 + lane + 32 * q;
+          c[q].idx = -1;
+          c[q].has_prev = 0;
+          if (k < G) {
+            const HogCand<T> *cp = a.cand + par * G + k;
+            c[q].absval = __ldcg(&cp->absval);
+            c[q].val = __ldcg(&cp->val);
+            c[q].at_prev = __ldcg(&cp->at_prev);
+            c[q].idx = __ldcg(&cp->idx);
+            c[q].has_prev = __ldcg(&cp->has_prev);
+          }
         }
-        if (c.has_prev) {
-          gprev = c.at_prev;
-          ghp = 1;
+#pragma unroll
+        for (int q = 0; q < HOG_CPL; ++q) {
+          if (beats(c[q].absval, c[q].idx, ga, gi)) {
+            ga = c[q].absval;
+            gi = c[q].idx;
+            gv = c[q].val;
+          }
+          if (c[q].has_prev) {
+            gprev = c[q].at_prev;
+            ghp = 1;
+          }
         }
       }
       for (int o = 16; o > 0; o >>= 1) {
@@ -320,6 +484,7 @@ __global__ void __launch_bounds__(HOG_THREADS, 1) k_hogbom(HogArgs<T> a) {
     }
   }
   if (b == 0 && threadIdx.x == 0) {
+    a.state->kpar = par;
     a.state->iter = it;
     a.state->px = px;
     a.state->py = py;
