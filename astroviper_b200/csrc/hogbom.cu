@@ -13,6 +13,7 @@
 // differences are rounded separately (no FMA), the model is accumulated in
 // iteration order by one thread.
 #include <algorithm>
+#include <cstddef>
 #include <type_traits>
 
 #include "common.cuh"
@@ -32,12 +33,14 @@ struct __align__(16) HogState {
   // FP32: the iteration's winner as one 64-bit maximum over the CTAs, bits of
   // |r| above the complement of 2 * index + sign (0: no pixel above 0), two
   // of them used in turn; kpar: the one the next launch starts with
+  double pad1[10];  // the keys on the second cache line, away from gen / count
   unsigned long long key[2];
   int kpar;
   int pad3;
-  double pad2[23];
+  double pad2[13];
 };
 static_assert(sizeof(HogState) == 256, "state size");
+static_assert(offsetof(HogState, key) == 128, "keys on their own cache line");
 
 template <typename T>
 struct __align__(16) HogCand {
