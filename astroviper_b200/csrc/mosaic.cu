@@ -280,8 +280,34 @@ __global__ void k_airy_pattern(AiryArgs a) {
 constexpr int MT_THREADS = 512;
 constexpr int MT_WARPS = MT_THREADS / 32;
 
+// Unsigned 32-bit division by an invariant d (Granlund and Montgomery,
+// "Division by invariant integers using multiplication", 1994): with
+// l = ceil(log2 d), m = floor(2^32 (2^l - d) / d) + 1, t = mulhi(m, n),
+// n / d = (t + ((n - t) >> 1)) >> (l - 1); d = 1 uses m = 0 and no shifts.
+struct FastDiv {
+  uint32_t m;
+  int s1, s2;
+};
+
+static FastDiv fast_div(uint32_t d) {
+  FastDiv f{0u, 0, 0};
+  if (d <= 1) return f;
+  int l = 0;
+  while ((1ull << l) < d) ++l;
+  f.m = (uint32_t)((((uint64_t)1 << 32) * (((uint64_t)1 << l) - d)) / d + 1);
+  f.s1 = 1;
+  f.s2 = l - 1;
+  return f;
+}
+
+__device__ __forceinline__ uint32_t fdiv(uint32_t n, const FastDiv &f) {
+  const uint32_t t = __umulhi(f.m, n);
+  return (t + ((n - t) >> f.s1)) >> f.s2;
+}
+
 struct MosaicTiledArgs {
   MosaicArgs m;
+  FastDiv div_nchan, div_nb;  // row -> (time x baseline, channel), -> baseline
   const Rec *recs;
   const uint32_t *tile_start;
   const uint32_t *n_rec;
@@ -301,10 +327,18 @@ __global__ void __launch_bounds__(MT_THREADS, 1) k_mosaic_tiled(MosaicTiledArgs 
   double *sre = (double *)smem;
   double *sim = sre + sub_n;
   __shared__ int s_chunk;
+  // lane packing of a window with sv columns: 32 / sv rows per pass, lane
+  // ir = lane / sv (sv <= max_support <= 32)
+  __shared__ unsigned char s_ir[33][32], s_rp[33];
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const uint32_t n_rec = *t.n_rec;
   const int64_t n_chunks = ((int64_t)n_rec + t.chunk - 1) / t.chunk;
   const uint32_t nchan = (uint32_t)a.nchan, nb = (uint32_t)a.nb;
+  for (int i = threadIdx.x; i < 33 * 32; i += MT_THREADS) {
+    const int sv = i >> 5, l = i & 31;
+    s_ir[sv][l] = (unsigned char)(sv ? l / sv : 0);
+    if (l == 0) s_rp[sv] = (unsigned char)(sv ? 32 / sv : 0);
+  }
   for (int i0 = 0; i0 < sub_n; i0 += MT_THREADS) {
     const int i = i0 + threadIdx.x;
     if (i < sub_n) {
@@ -344,14 +378,18 @@ __global__ void __launch_bounds__(MT_THREADS, 1) k_mosaic_tiled(MosaicTiledArgs 
         if (r >= seg_hi) continue;
         const Rec rc = t.recs[r];
         const int64_t row = rc.row;
-        const uint32_t tb = rc.row / nchan;  // rows fit 32 bits (the plan checks)
+        const uint32_t tb = fdiv(rc.row, t.div_nchan);  // rows fit 32 bits (the plan checks)
         const uint32_t c = rc.row - tb * nchan;
-        const uint32_t b = tb % nb;
+        const uint32_t b = tb - fdiv(tb, t.div_nb) * nb;
         const int cfb = a.cfb_map[b], cfc = a.cfc_map[c];
         if (cfb < 0 || cfb >= a.n_cfb || cfc < 0 || cfc >= a.n_cfc) continue;
         const long long uo = (long long)rc.ou - 128 + a.cu / 2;
         const long long vo = (long long)rc.ov - 128 + a.cv / 2;
         const int cu0 = rc.du + t.S / 2, cv0 = rc.dv + t.S / 2;  // centre in the sub-grid
+        // the window's norm depends on the function only (same sample): kept
+        // for the next polarisation that uses the same function
+        int64_t norm_fidx = -1;
+        double2 norm_prev = make_double2(0.0, 0.0);
         for (int64_t p = 0; p < a.npol; ++p) {
           const int64_t k = row * a.npol + p;
           const double w = a.wt[k];
@@ -374,9 +412,8 @@ __global__ void __launch_bounds__(MT_THREADS, 1) k_mosaic_tiled(MosaicTiledArgs 
           double *pre = sre + (size_t)apol * W * W, *pim = sim + (size_t)apol * W * W;
           // lanes along the window's v (contiguous) axis: lane = ir * sv + jv,
           // 32 / sv u-rows per pass
-          const unsigned usv = (unsigned)sv;
-          const int rp = (int)(32u / usv);
-          const int ir = (int)((unsigned)lane / usv);
+          const int rp = s_rp[sv];
+          const int ir = s_ir[sv][lane];
           const int iv = -(sv / 2) + (lane - ir * sv);
           const long long fv = (long long)a.os_v * iv + vo;
           const bool v_ok = ir < rp && fv >= 0 && fv < a.cv;
@@ -395,9 +432,15 @@ __global__ void __launch_bounds__(MT_THREADS, 1) k_mosaic_tiled(MosaicTiledArgs 
             norm.x += conv.x;
             norm.y += conv.y;
           }
-          for (int off = 16; off > 0; off >>= 1) {
-            norm.x += __shfl_down_sync(0xffffffffu, norm.x, off);
-            norm.y += __shfl_down_sync(0xffffffffu, norm.y, off);
+          if (fidx == norm_fidx) {
+            norm = norm_prev;
+          } else {
+            for (int off = 16; off > 0; off >>= 1) {
+              norm.x += __shfl_down_sync(0xffffffffu, norm.x, off);
+              norm.y += __shfl_down_sync(0xffffffffu, norm.y, off);
+            }
+            norm_fidx = fidx;
+            norm_prev = norm;
           }
           const double re = a.do_psf ? norm.x
                                      : __dsub_rn(__dmul_rn(norm.x, norm.x),
@@ -689,6 +732,8 @@ int av_mosaic_tiled_execute(AV_MOSAIC_PARAMS, void *workspace, size_t workspace_
   t.ntv = g.ntv;
   t.S = max_support;
   t.W = TILE + max_support - 1;
+  t.div_nchan = fast_div((uint32_t)nchan);
+  t.div_nb = fast_div((uint32_t)nb);
   const int sms = sm_count();
   int64_t chunk = (rows + (int64_t)sms * 16 - 1) / ((int64_t)sms * 16);
   if (chunk < 1024) chunk = 1024;
