@@ -104,7 +104,7 @@ __global__ void k_pswf_kernel4d(double *out, int os, int support, int n_os) {
 // ------------------------------------------------------------ tuning ---
 constexpr int kTuneKnobs = 4;
 static std::atomic<int64_t> g_tune[kTuneKnobs] = {
-    {16}, {16}, {AV_GRID_LANES_MMA}, {AV_DEGRID_LANES_TF32}};
+    {16}, {16}, {AV_GRID_LANES_AUTO}, {AV_DEGRID_LANES_AUTO}};
 
 int64_t tune_value(int knob) {
   return (knob >= 0 && knob < kTuneKnobs) ? g_tune[knob].load() : 0;
@@ -194,11 +194,12 @@ int av_tune_set(int knob, int64_t value) {
   AV_CHECK_ARG(knob >= 0 && knob < kTuneKnobs, "av_tune_set: unknown knob %d", knob);
   AV_CHECK_ARG(value >= 1 && value <= 1024, "av_tune_set: value %lld outside [1, 1024]",
                (long long)value);
-  AV_CHECK_ARG(knob != AV_TUNE_GRID_LANES || value <= 2,
-               "av_tune_set: AV_TUNE_GRID_LANES takes 1 (mma) or 2 (rows), not %lld",
+  AV_CHECK_ARG(knob != AV_TUNE_GRID_LANES || value <= 3,
+               "av_tune_set: AV_TUNE_GRID_LANES takes 1 (mma), 2 (rows) or 3 (auto), not %lld",
                (long long)value);
-  AV_CHECK_ARG(knob != AV_TUNE_DEGRID_LANES || value <= 2,
-               "av_tune_set: AV_TUNE_DEGRID_LANES takes 1 (tf32) or 2 (fp32), not %lld",
+  AV_CHECK_ARG(knob != AV_TUNE_DEGRID_LANES || value <= 3,
+               "av_tune_set: AV_TUNE_DEGRID_LANES takes 1 (tf32), 2 (fp32) or 3 (auto), "
+               "not %lld",
                (long long)value);
   g_tune[knob].store(value);
   return AV_OK;

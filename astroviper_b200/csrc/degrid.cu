@@ -832,16 +832,17 @@ static int launch_degrid_tiled(const TiledDegridArgs &a, int64_t nblocks, cudaSt
 }
 
 // The TF32 tensor-core kernel for the fast store path with 4 grid
-// polarisations and supports up to 8, unless AV_TUNE_DEGRID_LANES asks for
-// the FP32 kernel.
+// polarisations as AV_TUNE_DEGRID_LANES says (automatically for supports 7
+// and 8, where it is the faster), the FP32 kernel otherwise.
 template <int S>
 static int degrid_dispatch_npg(const TiledDegridArgs &a, int npg, int64_t nb, cudaStream_t st) {
   if (npg == 1) return launch_degrid_tiled<S, 1>(a, nb, st);
   if (npg == 2) return launch_degrid_tiled<S, 2>(a, nb, st);
   if constexpr (S <= 8) {
-    if (a.fast_out && a.d.g_npol == 4 &&
-        tune_value(AV_TUNE_DEGRID_LANES) == AV_DEGRID_LANES_TF32)
-      return launch_degrid_tc<S>(a, nb, st);
+    const int64_t lanes = tune_value(AV_TUNE_DEGRID_LANES);
+    const bool tf32 =
+        lanes == AV_DEGRID_LANES_TF32 || (lanes == AV_DEGRID_LANES_AUTO && S >= 7);
+    if (a.fast_out && a.d.g_npol == 4 && tf32) return launch_degrid_tc<S>(a, nb, st);
   }
   return launch_degrid_tiled<S, 4>(a, nb, st);
 }

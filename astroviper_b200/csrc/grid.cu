@@ -1046,15 +1046,16 @@ static int launch_grid_mma(const TiledGridArgs &a, int64_t nblocks, cudaStream_t
   return AV_OK;
 }
 
-// k_grid_mma for weighted gridding with supports up to 8 unless the
-// AV_TUNE_GRID_LANES knob asks for the row lanes; k_grid_tiled otherwise
+// k_grid_mma for weighted gridding as the AV_TUNE_GRID_LANES knob says
+// (automatically for supports 5-8: with smaller footprints most of the 8 x 8
+// tile is padding and the row lanes are faster); k_grid_tiled otherwise
 // (support 9, the degridder's adjoint).
 template <int S, int NPOL>
 static int launch_grid_tiled(const TiledGridArgs &a, int64_t nblocks, cudaStream_t st) {
   if constexpr (S <= 8) {
-    if (a.wt != nullptr && !a.inv_norm &&
-        tune_value(AV_TUNE_GRID_LANES) == AV_GRID_LANES_MMA)
-      return launch_grid_mma<S, NPOL>(a, nblocks, st);
+    const int64_t lanes = tune_value(AV_TUNE_GRID_LANES);
+    const bool mma = lanes == AV_GRID_LANES_MMA || (lanes == AV_GRID_LANES_AUTO && S >= 5);
+    if (a.wt != nullptr && !a.inv_norm && mma) return launch_grid_mma<S, NPOL>(a, nblocks, st);
   }
   return launch_grid_rows<S, NPOL>(a, nblocks, st);
 }

@@ -420,10 +420,11 @@ def main():
     bytes_grid = n_corr * 12 + nt * nb * 24 + nx * ny * npol * 8
     bytes_degrid = n_corr * 9 + nt * nb * 24 + nx * ny * npol * 8
     from astroviper_b200 import _lib
-    grid_kernel = ("k_grid_mma" if _lib.lib().av_tune_get(_lib.AV_TUNE_GRID_LANES) ==
-                   _lib.AV_GRID_LANES_MMA else "k_grid_tiled")
-    degrid_kernel = ("k_degrid_tc" if _lib.lib().av_tune_get(_lib.AV_TUNE_DEGRID_LANES) ==
-                     _lib.AV_DEGRID_LANES_TF32 else "k_degrid_tiled")
+    # support 7: the tensor-core kernels unless the lane knobs force the others
+    grid_kernel = ("k_grid_tiled" if _lib.lib().av_tune_get(_lib.AV_TUNE_GRID_LANES) ==
+                   _lib.AV_GRID_LANES_ROWS else "k_grid_mma")
+    degrid_kernel = ("k_degrid_tiled" if _lib.lib().av_tune_get(_lib.AV_TUNE_DEGRID_LANES) ==
+                     _lib.AV_DEGRID_LANES_FP32 else "k_degrid_tc")
     dom = (grid_kernel, bytes_grid, t_grid_k) if t_grid_k >= t_degrid_k else \
         (degrid_kernel, bytes_degrid, t_degrid_k)
     achieved = dom[1] / (dom[2] / 1e3) / 1e9

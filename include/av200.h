@@ -65,19 +65,23 @@ unsigned long long av_launch_count(void);
  *                                persistent tiled gridder (default 16)
  *   AV_TUNE_DEGRID_CHUNKS_PER_SM record chunks per SM handed out by the
  *                                persistent tiled degridder (default 16)
- *   AV_TUNE_GRID_LANES           how the tiled gridder sums a run of samples
- *                                for supports up to 8: AV_GRID_LANES_MMA
- *                                (FP64 tensor-core tiles, default) or
- *                                AV_GRID_LANES_ROWS (a footprint row per
- *                                lane, DFMA); support 9 always uses rows
+ *   AV_TUNE_GRID_LANES           how the tiled gridder sums a run of samples:
+ *                                AV_GRID_LANES_MMA (FP64 tensor-core tiles,
+ *                                supports up to 8), AV_GRID_LANES_ROWS (a
+ *                                footprint row per lane, DFMA) or
+ *                                AV_GRID_LANES_AUTO (default: tensor-core
+ *                                tiles for supports 5-8, where they are the
+ *                                faster, rows otherwise); support 9 always
+ *                                uses rows
  *   AV_TUNE_DEGRID_LANES         how the tiled degridder's fast store path
  *                                (complex64 values, 4 polarisations, no flags
- *                                or phase) runs for supports up to 8:
- *                                AV_DEGRID_LANES_TF32 (TF32 tensor-core tiles
- *                                with split operands, default) or
- *                                AV_DEGRID_LANES_FP32 (FP32 FMA)
+ *                                or phase) runs: AV_DEGRID_LANES_TF32 (TF32
+ *                                tensor-core tiles with split operands,
+ *                                supports up to 8), AV_DEGRID_LANES_FP32 (FP32
+ *                                FMA) or AV_DEGRID_LANES_AUTO (default: TF32
+ *                                for supports 7 and 8, FP32 otherwise)
  * av_tune_set returns AV_ERR_ARG for an unknown knob or a value outside
- * [1, 1024] ([1, 2] for the two lane knobs); av_tune_get returns -1 for an
+ * [1, 1024] ([1, 3] for the two lane knobs); av_tune_get returns -1 for an
  * unknown knob. */
 enum av_tune {
   AV_TUNE_GRID_CHUNKS_PER_SM = 0,
@@ -85,8 +89,12 @@ enum av_tune {
   AV_TUNE_GRID_LANES = 2,
   AV_TUNE_DEGRID_LANES = 3
 };
-enum av_grid_lanes { AV_GRID_LANES_MMA = 1, AV_GRID_LANES_ROWS = 2 };
-enum av_degrid_lanes { AV_DEGRID_LANES_TF32 = 1, AV_DEGRID_LANES_FP32 = 2 };
+enum av_grid_lanes { AV_GRID_LANES_MMA = 1, AV_GRID_LANES_ROWS = 2, AV_GRID_LANES_AUTO = 3 };
+enum av_degrid_lanes {
+  AV_DEGRID_LANES_TF32 = 1,
+  AV_DEGRID_LANES_FP32 = 2,
+  AV_DEGRID_LANES_AUTO = 3
+};
 int av_tune_set(int knob, int64_t value);
 int64_t av_tune_get(int knob);
 
