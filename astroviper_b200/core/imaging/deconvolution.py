@@ -214,7 +214,8 @@ def deconvolve(dirty_image_xds, psf_xds, model_xds=None, algorithm: str = "hogbo
                 ps = psf[tt, nn, 0 if broadcast else pp]
                 mk = None if mask is None else mask[tt, nn, pp]
                 start_peakres = _peak_residual(d, mk)
-                start_peakres_nomask = _peak_residual(d)
+                # without a mask both statistics are the same value
+                start_peakres_nomask = start_peakres if mk is None else _peak_residual(d)
                 start_model_flux = float(start_flux[tt, nn, pp]) if start_flux is not None \
                     else 0.0
                 results, model_arr, resid_arr = hogbom_clean(
@@ -226,7 +227,7 @@ def deconvolve(dirty_image_xds, psf_xds, model_xds=None, algorithm: str = "hogbo
                 if model_arr.dtype == torch.float32:
                     flux = float(np.float32(flux))  # np.sum of a float32 plane
                 peakres = _peak_residual(resid_out[tt, nn, pp], mk)
-                peakres_nomask = _peak_residual(resid_out[tt, nn, pp])
+                peakres_nomask = peakres if mk is None else _peak_residual(resid_out[tt, nn, pp])
                 rd.add({
                     "niter": deconv_params.get("niter", None),
                     "threshold": deconv_params.get("threshold", None),

@@ -94,6 +94,15 @@ def _box(clean_box, nx, ny):
     return xbeg, xend, ybeg, yend
 
 
+def _final_stats(run):
+    """(min, max) of the residual (maximg) and the ordered sum of the model's
+    |x| as one host array (FP64 holds the FP32 results exactly)."""
+    mm = K.maximg(run.resid, run.mask)
+    total = K.abs_sum_ordered(run.model)
+    return torch.cat([mm.reshape(-1).to(torch.float64),
+                      total.reshape(-1)[:1].to(torch.float64)]).cpu().numpy()
+
+
 def clean(dirty_image, psf, mask=None, clean_box=(-1, -1, -1, -1), max_iter=100, start_iter=0,
           gain=0.1, threshold=0.0, speedup=0.0, progress_callback=None, stop_callback=None, *,
           large_psf=False):
@@ -135,6 +144,9 @@ def clean(dirty_image, psf, mask=None, clean_box=(-1, -1, -1, -1), max_iter=100,
     callbacks = progress_callback is not None or stop_callback is not None
     if not callbacks:
         run.run(siter, niter)
+        # the final statistics are queued before the state is read, so the
+        # host waits once
+        stats = _final_stats(run)
         st = run.read_state()
     else:
         cycle = max(1, int((niter - siter) / 10)) if niter - siter >= 0 else 1
@@ -173,10 +185,11 @@ def clean(dirty_image, psf, mask=None, clean_box=(-1, -1, -1, -1), max_iter=100,
             # iteration subtracted (hclean.cpp:124,202-203)
             rep = last if (st["iter"] >= niter and last is not None) else st
             progress_callback(st["iter"], rep["px"], rep["py"], float(tdt(rep["peak"])))
+        stats = _final_stats(run)
     final_iter = min(st["iter"], niter) if st["iter"] > niter else st["iter"]
-    mm = K.maximg(run.resid, run.mask).cpu().numpy()
+    mm = stats[:2]
     final_peak = max(abs(mm[0]), abs(mm[1]))
-    total = K.abs_sum_ordered(run.model).cpu().numpy()[0]
+    total = stats[2]
     return {
         "model_image": _out(run.model, on_device),
         "residual_image": _out(run.resid, on_device),
