@@ -63,7 +63,9 @@ def test_grid_plain_fp64(case, do_psf, mode):
 @pytest.mark.parametrize("case", ["a", "b", "c"])
 @pytest.mark.parametrize("do_psf", [False, True])
 @pytest.mark.parametrize("mode", ["continuum", "cube"])
-def test_grid_tiled_fp32(case, do_psf, mode):
+def test_grid_tiled_fp32(case, do_psf, mode, grid_lanes):
+    """The tiled gridder on the reference's golden cases (data and PSF
+    gridding), under both lane mappings."""
     gr, sw, rg, rs = _grid_case(case, "fp32", do_psf, mode)
     assert rel(gr, rg) <= 1e-5
     assert np.allclose(sw, rs, rtol=1e-6, atol=0)
