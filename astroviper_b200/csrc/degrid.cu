@@ -506,20 +506,22 @@ __global__ void __launch_bounds__(DT_THREADS) k_degrid_tiled(TiledDegridArgs a) 
 // ------------------------------------------------------- tensor cores ----
 // k_degrid_tc: the tiled degridder's fast store path (complex64 values, 4
 // visibility and 4 grid polarisations, no flags, no phase) on the TF32 tensor
-// path.  For one cell the degridded values of 16 samples are a matrix product
-//   D[s][q] = sum over k of W[s][k] P[k][q],   k = (r, c) in 8 x 8,
-// with W[s][(r, c)] = cu_s[r] cv_s[c] (the sample's tap products) and
-// P[(r, c)][q] the cell's footprint value at row r, column c for output q =
-// (grid polarisation, real | imaginary): eight k-steps of
-// mma.sync.m16n8k8.tf32 per 16 samples.  TF32 keeps 11 significant bits, so
-// both operands are split into a TF32 high part and the TF32-rounded
-// remainder, and the products hi.hi, hi.lo and lo.hi are accumulated in FP32
-// in three independent chains; what is left out is below 2^-22 of each
-// product.  Fragment layout (lane = 4 g + t): a = W[g][t], W[g + 8][t],
-// W[g][t + 4], W[g + 8][t + 4]; b = P[t][g], P[t + 4][g]; d = D[g][2t, 2t + 1],
-// D[g + 8][2t, 2t + 1].  Lane (g, t) thus computes the tap products of samples
-// g and g + 8 for columns t and t + 4, holds the patch values of output g, and
-// receives polarisation t of samples g and g + 8.
+// path.  For one cell and 16 samples the row sums are a matrix product,
+//   D[m][(q, r)] = sum over c of cv_m[c] P[q][r][c],
+// with cv_m the sample's column taps and P[q][r][c] the cell's footprint value
+// at row r, column c for output q = (grid polarisation, real | imaginary):
+// one mma.sync.m16n8k8.tf32 per output (8 rows, k = 8 columns), and then
+// V[m][q] = sum over r of cu_m[r] D[m][(q, r)] on the FP32 pipe.  TF32 keeps
+// 11 significant bits, so both operands are split into a TF32 high part and
+// the TF32-rounded remainder (the taps once, in a table; the patch once per
+// cell) and the products hi.hi, hi.lo and lo.hi are accumulated in FP32: what
+// is left out is below 2^-22 of each product.  Fragment layout (lane = 4 g +
+// t): a = cv[g][t], cv[g + 8][t], cv[g][t + 4], cv[g + 8][t + 4] (samples g
+// and g + 8); b = P[q][g][t], P[q][g][t + 4]; d = D[g][(q, 2t)],
+// D[g][(q, 2t + 1)], D[g + 8][(q, 2t)], D[g + 8][(q, 2t + 1)].  Lane (g, t)
+// thus weights rows 2t and 2t + 1 with its row taps; two shuffles within the
+// quad complete the sum over rows, and the lane writes polarisation t of
+// samples g and g + 8.
 constexpr int TC_THREADS = 256;
 constexpr int TC_ROUND = 64;  // records a warp stages per round (two per lane)
 
@@ -528,10 +530,14 @@ struct TCSmem {
   static constexpr int W = TILE + S - 1;
   static constexpr int RW = 8;  // taps 0-7 of a row, zero past the support
   static constexpr size_t tab_bytes = 256 * RW * sizeof(float);
+  // the same taps split into TF32 (high, remainder) pairs
+  static constexpr size_t tabs_bytes = 256 * RW * sizeof(uint2);
   static constexpr size_t rs_bytes = 256 * sizeof(double);
   static constexpr size_t rec_bytes = (size_t)(TC_THREADS / 32) * TC_ROUND * sizeof(Rec);
   static constexpr size_t inv_bytes = (size_t)(TC_THREADS / 32) * TC_ROUND * sizeof(float);
-  static constexpr size_t off_rec = tab_bytes + rs_bytes;
+  static constexpr size_t off_tabs = tab_bytes;
+  static constexpr size_t off_rs = off_tabs + tabs_bytes;
+  static constexpr size_t off_rec = off_rs + rs_bytes;
   static constexpr size_t off_inv = off_rec + rec_bytes;
   static constexpr size_t off_sub = off_inv + inv_bytes;
   static constexpr size_t sub_bytes = (size_t)W * W * 4 * sizeof(float2);  // [cell][pol]
@@ -552,14 +558,6 @@ __device__ __forceinline__ void tf32_split(float x, uint32_t &hi, uint32_t &lo) 
   lo = tf32_rna(x - __uint_as_float(hi));
 }
 
-// x = hi + lo with hi in TF32 and lo the exact FP32 remainder, which the
-// tensor core reads as TF32 by dropping its 13 low bits (a relative error of
-// at most 2^-10 of lo, 2^-21 of x)
-__device__ __forceinline__ void tf32_split_fast(float x, uint32_t &hi, uint32_t &lo) {
-  hi = tf32_rna(x);
-  lo = __float_as_uint(x - __uint_as_float(hi));
-}
-
 __device__ __forceinline__ void mma_tf32(float (&d)[4], uint32_t a0, uint32_t a1, uint32_t a2,
                                          uint32_t a3, uint32_t b0, uint32_t b1) {
   asm("mma.sync.aligned.m16n8k8.row.col.f32.tf32.tf32.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, "
@@ -569,13 +567,14 @@ __device__ __forceinline__ void mma_tf32(float (&d)[4], uint32_t a0, uint32_t a1
 }
 
 template <int S>
-__global__ void __launch_bounds__(TC_THREADS, 3) k_degrid_tc(TiledDegridArgs a) {
+__global__ void __launch_bounds__(TC_THREADS, 2) k_degrid_tc(TiledDegridArgs a) {
   using M = TCSmem<S>;
   constexpr int W = M::W, RW = M::RW, WARPS = TC_THREADS / 32;
   constexpr unsigned FULL = 0xffffffffu;
   extern __shared__ __align__(16) unsigned char smem[];
   float *tab = (float *)smem;
-  double *rs = (double *)(smem + M::tab_bytes);
+  uint2 *tabs = (uint2 *)(smem + M::off_tabs);
+  double *rs = (double *)(smem + M::off_rs);
   Rec *st_rec = (Rec *)(smem + M::off_rec);
   float *st_inv = (float *)(smem + M::off_inv);
   float2 *sub = (float2 *)(smem + M::off_sub);
@@ -586,13 +585,19 @@ __global__ void __launch_bounds__(TC_THREADS, 3) k_degrid_tc(TiledDegridArgs a) 
   const uint32_t n_all = (uint32_t)a.n_rows;  // store mode: every sample is written
   const int64_t n_chunks = ((int64_t)n_all + a.chunk - 1) / a.chunk;
   build_tap_tables_d<S, RW>(tab, rs, d.cf, a.cgk_len, d.sampling);
+  __syncthreads();
+  for (int i = threadIdx.x; i < 256 * RW; i += TC_THREADS) {
+    uint2 hl;
+    tf32_split(tab[i], hl.x, hl.y);
+    tabs[i] = hl;
+  }
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const int g = lane >> 2, t = lane & 3;
-  // output polarisation t takes grid polarisation polmap[t], held by lane 4 g + polmap[t]
+  // output polarisation t takes grid polarisation polmap[t]
   int src = -1;
   {
     const int v = d.polmap[t];
-    if (v >= 0 && v < 4 && v < d.g_npol) src = 4 * g + v;
+    if (v >= 0 && v < 4 && v < d.g_npol) src = v;
   }
   const int64_t gplane = d.g_n2 * d.g_n3;
 
@@ -659,9 +664,11 @@ __global__ void __launch_bounds__(TC_THREADS, 3) k_degrid_tc(TiledDegridArgs a) 
       Rec *wrec = st_rec + warp * TC_ROUND;
       float *winv = st_inv + warp * TC_ROUND;
       int cur = -1;
-      uint32_t bh[8][2], bl[8][2];  // patch fragments of the current cell
+      // patch fragments of the current cell, one n-tile per output q =
+      // (polarisation q / 2, real | imaginary): b = P[q][r = g][c = t, t + 4]
+      uint32_t bh[8][2], bl[8][2];
 #pragma unroll
-      for (int jj = 0; jj < 8; ++jj) bh[jj][0] = bh[jj][1] = bl[jj][0] = bl[jj][1] = 0u;
+      for (int q = 0; q < 8; ++q) bh[q][0] = bh[q][1] = bl[q][0] = bl[q][1] = 0u;
       Rec na, nb;
       if (w_lo + lane < w_hi) na = a.recs[w_lo + lane];
       if (w_lo + 32 + lane < w_hi) nb = a.recs[w_lo + 32 + lane];
@@ -701,19 +708,16 @@ __global__ void __launch_bounds__(TC_THREADS, 3) k_degrid_tc(TiledDegridArgs a) 
             const Rec rj = wrec[j];
             cur = (int)rj.du | ((int)rj.dv << 8);
             const int du = rj.du, dv = rj.dv;
+            const bool rok = g < S;
 #pragma unroll
-            for (int jj = 0; jj < 8; ++jj) {
-              float x0 = 0.f, x1 = 0.f;
-              if (jj < S && t < S) {
-                const float2 v = sub[((du + jj) * W + dv + t) * 4 + (g >> 1)];
-                x0 = (g & 1) ? v.y : v.x;
-              }
-              if (jj < S && t + 4 < S) {
-                const float2 v = sub[((du + jj) * W + dv + t + 4) * 4 + (g >> 1)];
-                x1 = (g & 1) ? v.y : v.x;
-              }
-              tf32_split(x0, bh[jj][0], bl[jj][0]);
-              tf32_split(x1, bh[jj][1], bl[jj][1]);
+            for (int pol = 0; pol < 4; ++pol) {
+              float2 v0 = make_float2(0.f, 0.f), v1 = make_float2(0.f, 0.f);
+              if (rok && t < S) v0 = sub[((du + g) * W + dv + t) * 4 + pol];
+              if (rok && t + 4 < S) v1 = sub[((du + g) * W + dv + t + 4) * 4 + pol];
+              tf32_split(v0.x, bh[2 * pol][0], bl[2 * pol][0]);
+              tf32_split(v1.x, bh[2 * pol][1], bl[2 * pol][1]);
+              tf32_split(v0.y, bh[2 * pol + 1][0], bl[2 * pol + 1][0]);
+              tf32_split(v1.y, bh[2 * pol + 1][1], bl[2 * pol + 1][1]);
             }
           }
           const unsigned long long later = j < 63 ? (starts & (~1ull << j)) : 0ull;
@@ -726,32 +730,50 @@ __global__ void __launch_bounds__(TC_THREADS, 3) k_degrid_tc(TiledDegridArgs a) 
             const Rec recg = wrec[vg ? sg : j0], rech = wrec[vh ? sh : j0];
             const float invg = winv[vg ? sg : j0], invh = winv[vh ? sh : j0];
             const int oug = recg.ou, ovg = recg.ov, ouh = rech.ou, ovh = rech.ov;
-            const float *cug = tab + oug * RW, *cuh = tab + ouh * RW;  // row taps
-            // an empty slot of the group contributes a zero row of W
-            const float cvg0 = vg ? tab[ovg * RW + t] : 0.f;
-            const float cvg1 = vg ? tab[ovg * RW + t + 4] : 0.f;
-            const float cvh0 = vh ? tab[ovh * RW + t] : 0.f;
-            const float cvh1 = vh ? tab[ovh * RW + t + 4] : 0.f;
-            float d0[4] = {0.f, 0.f, 0.f, 0.f}, d1[4] = {0.f, 0.f, 0.f, 0.f},
-                  d2[4] = {0.f, 0.f, 0.f, 0.f};
+            // A = the column taps of samples g and g + 8 (columns t, t + 4),
+            // split in the table; an empty slot is a zero row
+            const uint2 z = make_uint2(0u, 0u);
+            const uint2 ag0 = vg ? tabs[ovg * RW + t] : z, ag1 = vg ? tabs[ovg * RW + t + 4] : z;
+            const uint2 ah0 = vh ? tabs[ovh * RW + t] : z, ah1 = vh ? tabs[ovh * RW + t + 4] : z;
+            // row taps r = 2t, 2t + 1 for the final sum over rows
+            const float2 cg = *(const float2 *)&tab[oug * RW + 2 * t];
+            const float2 ch = *(const float2 *)&tab[ouh * RW + 2 * t];
+            // D[m][(q, r)] = sum_c cv_m[c] P[q][r][c]: the row sums, one
+            // n-tile (8 rows) per output q, three TF32 products each
+            float dq[8][4];
 #pragma unroll
-            for (int jj = 0; jj < S; ++jj) {  // rows past the support are zero
-              uint32_t a0h, a0l, a1h, a1l, a2h, a2l, a3h, a3l;
-              tf32_split_fast(cug[jj] * cvg0, a0h, a0l);
-              tf32_split_fast(cuh[jj] * cvh0, a1h, a1l);
-              tf32_split_fast(cug[jj] * cvg1, a2h, a2l);
-              tf32_split_fast(cuh[jj] * cvh1, a3h, a3l);
-              mma_tf32(d0, a0h, a1h, a2h, a3h, bh[jj][0], bh[jj][1]);
-              mma_tf32(d1, a0h, a1h, a2h, a3h, bl[jj][0], bl[jj][1]);
-              mma_tf32(d2, a0l, a1l, a2l, a3l, bh[jj][0], bh[jj][1]);
+            for (int q = 0; q < 8; ++q) {
+              dq[q][0] = dq[q][1] = dq[q][2] = dq[q][3] = 0.f;
+              mma_tf32(dq[q], ag0.y, ah0.y, ag1.y, ah1.y, bh[q][0], bh[q][1]);
+              mma_tf32(dq[q], ag0.x, ah0.x, ag1.x, ah1.x, bl[q][0], bl[q][1]);
+              mma_tf32(dq[q], ag0.x, ah0.x, ag1.x, ah1.x, bh[q][0], bh[q][1]);
             }
-            const float gre = (d2[0] + d1[0]) + d0[0], gim = (d2[1] + d1[1]) + d0[1];
-            const float hre = (d2[2] + d1[2]) + d0[2], him = (d2[3] + d1[3]) + d0[3];
-            // polarisation t of samples g and g + 8
-            const float xgre = __shfl_sync(FULL, gre, src & 31);
-            const float xgim = __shfl_sync(FULL, gim, src & 31);
-            const float xhre = __shfl_sync(FULL, hre, src & 31);
-            const float xhim = __shfl_sync(FULL, him, src & 31);
+            // V[m][q] = sum_r cu_m[r] D[m][(q, r)]: rows 2t, 2t + 1 here, the
+            // other rows in the quad's other lanes
+            float vgq[8], vhq[8];
+#pragma unroll
+            for (int q = 0; q < 8; ++q) {
+              float pg = __fmul_rn(cg.x, dq[q][0]);
+              pg = __fmaf_rn(cg.y, dq[q][1], pg);
+              float ph = __fmul_rn(ch.x, dq[q][2]);
+              ph = __fmaf_rn(ch.y, dq[q][3], ph);
+              pg = __fadd_rn(pg, __shfl_xor_sync(FULL, pg, 1));
+              ph = __fadd_rn(ph, __shfl_xor_sync(FULL, ph, 1));
+              pg = __fadd_rn(pg, __shfl_xor_sync(FULL, pg, 2));
+              ph = __fadd_rn(ph, __shfl_xor_sync(FULL, ph, 2));
+              vgq[q] = pg;
+              vhq[q] = ph;
+            }
+            // this lane writes polarisation t, from grid polarisation src
+            float xgre = 0.f, xgim = 0.f, xhre = 0.f, xhim = 0.f;
+#pragma unroll
+            for (int pol = 0; pol < 4; ++pol)
+              if (pol == src) {
+                xgre = vgq[2 * pol];
+                xgim = vgq[2 * pol + 1];
+                xhre = vhq[2 * pol];
+                xhim = vhq[2 * pol + 1];
+              }
             float2 *out = (float2 *)d.values;
             if (vg)
               out[(int64_t)recg.row * 4 + t] = src >= 0 ? make_float2(__fmul_rn(xgre, invg),
