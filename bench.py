@@ -128,11 +128,11 @@ class ClockSampler:
 # DRAM bytes read + written per launch and per visibility of the main
 # kernels, from ncu captures (dram__bytes_read.sum + dram__bytes_write.sum)
 # of the 8.26M-visibility case (64 time steps): k_grid_mma 481.40 MB,
-# k_grid_tiled (row lanes) 484.11 MB, k_degrid_tc 312.69 MB, k_degrid_tiled
+# k_grid_tiled (row lanes) 484.11 MB, k_degrid_tc 286.43 MB, k_degrid_tiled
 # 286.84 MB.  The traffic is per record, so it scales with the visibilities.
 NCU_VIS = 64 * 2016 * 64
 DRAM_BYTES_PER_VIS = {"k_grid_mma": 481.40e6 / NCU_VIS, "k_grid_tiled": 484.11e6 / NCU_VIS,
-                      "k_degrid_tc": 312.69e6 / NCU_VIS, "k_degrid_tiled": 286.84e6 / NCU_VIS}
+                      "k_degrid_tc": 286.43e6 / NCU_VIS, "k_degrid_tiled": 286.84e6 / NCU_VIS}
 
 
 def max_over_ranks(ms, world, device=None):
