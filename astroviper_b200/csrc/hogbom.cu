@@ -135,7 +135,6 @@ __global__ void __launch_bounds__(HOG_THREADS, 1) k_hogbom(HogArgs<T> a) {
   __shared__ int s_idx[32];
   __shared__ int s_flag;
   __shared__ T s_prev;
-  __shared__ int s_has_prev;
   __shared__ int s_use_key;
   constexpr bool KEYED = std::is_same<T, float>::value;
   const int G = gridDim.x, b = blockIdx.x;
@@ -332,14 +331,6 @@ __global__ void __launch_bounds__(HOG_THREADS, 1) k_hogbom(HogArgs<T> a) {
         }
       }
     }
-    // value at the current peak, published by its owner (used when no pixel
-    // beats 0, where the reference keeps the previous position)
-    if (threadIdx.x == 0) s_has_prev = 0;
-    __syncthreads();
-    if (py >= y_lo && py < y_hi && threadIdx.x == 0) {
-      s_prev = band[(size_t)(py - y_lo) * nx + px];
-      s_has_prev = 1;
-    }
     // block reduction (only strictly positive maxima count)
     if (best_idx >= 0 && !(best_abs > (T)0)) best_idx = -1;
     for (int o = 16; o > 0; o >>= 1) {
@@ -377,8 +368,12 @@ __global__ void __launch_bounds__(HOG_THREADS, 1) k_hogbom(HogArgs<T> a) {
         c.absval = best_abs;
         c.val = best_val;
         c.idx = best_idx;
-        c.has_prev = s_has_prev;
-        c.at_prev = s_has_prev ? s_prev : (T)0;
+        // value at the current peak, published by its owner (used when no
+        // pixel beats 0, where the reference keeps the previous position);
+        // the block barrier above has ordered the band pass's writes
+        const bool hp = py >= y_lo && py < y_hi;
+        c.has_prev = hp ? 1 : 0;
+        c.at_prev = hp ? band[(size_t)(py - y_lo) * nx + px] : (T)0;
         a.cand[par * G + b] = c;
         if (KEYED && best_idx >= 0) {
           const uint32_t code = 2u * (uint32_t)best_idx + (best_val < (T)0 ? 1u : 0u);
