@@ -688,3 +688,19 @@ def airy_pattern(freq, n_pol, dish, blockage, image_size, image_center, cell, ip
                                 float(cell[0]), float(cell[1]), int(ipower), int(bool(casa)),
                                 int(bool(rorder)), stream_ptr()), "av_airy_pattern")
     return out
+
+
+def plane_rescale(t, mode, s, corr=None, w=None):
+    """In place on the contiguous device tensor t (..., ny, nx):
+    av_plane_rescale mode 0 (t /= s), 1 (t *= s) or 2
+    (t *= s / (corr * w[plane]), corr (ny, nx) and w one value per plane)."""
+    assert t.is_contiguous() and t.is_cuda
+    ny, nx = int(t.shape[-2]), int(t.shape[-1])
+    npl = int(t.numel() // max(1, ny * nx))
+    c = None if corr is None else on_device(corr, torch.float64)
+    ww = None if w is None else on_device(w, torch.float64).reshape(-1)
+    if mode == 2:
+        assert c.numel() == ny * nx and ww.numel() == npl
+    check(lib().av_plane_rescale(p(t), dcode(t), npl, ny * nx, int(mode), float(s), p(c), p(ww),
+                                 stream_ptr()), "av_plane_rescale")
+    return t

@@ -1,0 +1,123 @@
+"""The image <-> uv-grid transforms and their normalisations on B200.
+
+Drop-in for fft_to_uv, ifft_to_lm, correct_fft_to_uv and correct_ifft_to_lm of
+src/astroviper/core/imaging/imaging_utils/standard_image_grid_preparation.py
+(:312-492): same arguments, defaults, variable-name rules, exceptions and
+in-place updates of the image dataset.  The transforms are this package's
+cuFFT fft_lm_to_uv / ifft_uv_to_lm; the normalisations run in libav200
+(av_plane_rescale), one launch per variable, in numpy's arithmetic for an
+array scaled by a scalar, so their results are bit-identical to the
+reference's for the same transform output.
+
+The image may be a SkyImage (its variables numpy arrays or device tensors) or
+an xarray Dataset.  numpy variables are updated in place in their own
+buffers, as the reference's `image[var].data /= ...` does; device tensors are
+updated on the device.
+"""
+from typing import List, Union
+
+import numpy as np
+
+from .... import _host as H
+from .... import _kernels as K
+from ..fft import fft_lm_to_uv
+from ..ifft import ifft_uv_to_lm
+
+_DIV, _MUL, _SPHEROID = 0, 1, 2
+
+
+def _try_vars(data_vars, default):
+    if not data_vars:
+        return list(default)
+    if isinstance(data_vars, str):
+        return [data_vars]
+    return data_vars
+
+
+def _rescale(x, mode, s, corr=None, w=None):
+    """x (..., a, b) scaled in place by av_plane_rescale; returns x."""
+    if H.is_torch(x) and x.is_cuda and x.is_contiguous():
+        return K.plane_rescale(x, mode, s, corr, w)
+    t = H.dev(x)
+    K.plane_rescale(t, mode, s, corr, w)
+    H.write_back(x, t)
+    return x
+
+
+def fft_to_uv(image, data_vars: Union[str, List[str]] = "") -> None:
+    """standard_image_grid_preparation.py:312-341: VISIBILITY_<var> =
+    fft_lm_to_uv(<var>) over axes 3, 4 for each of SKY, RESIDUAL, MODEL (or
+    data_vars) present; the VISIBILITY_<var> variable must exist."""
+    for sky_var in _try_vars(data_vars, ("SKY", "RESIDUAL", "MODEL")):
+        if sky_var in image.data_vars:
+            dat_name = "VISIBILITY_" + sky_var
+            if dat_name not in image.data_vars:
+                raise Exception(f"{dat_name} is not in {image}")
+            image[dat_name].data = fft_lm_to_uv(image[sky_var].data, axes=[3, 4])
+
+
+def ifft_to_lm(image, data_vars: Union[str, List[str]] = "") -> None:
+    """standard_image_grid_preparation.py:344-377: SKY = ifft_uv_to_lm(
+    VISIBILITY) and <name> = ifft_uv_to_lm(VISIBILITY_<name>) over axes 3, 4
+    for each of VISIBILITY, VISIBILITY_RESIDUAL, VISIBILITY_MODEL (or
+    data_vars) present; the target variable must exist."""
+    for vis_var in _try_vars(data_vars,
+                             ("VISIBILITY", "VISIBILITY_RESIDUAL", "VISIBILITY_MODEL")):
+        if vis_var in image.data_vars:
+            dat_name = ("SKY" if vis_var == "VISIBILITY"
+                        else vis_var.split("VISIBILITY_", 1)[1])
+            image[dat_name].data = ifft_uv_to_lm(image[vis_var].data, axes=[3, 4])
+
+
+def correct_fft_to_uv(image, data_vars: Union[str, List[str]] = "") -> None:
+    """standard_image_grid_preparation.py:380-409: each of VISIBILITY,
+    VISIBILITY_RESIDUAL, VISIBILITY_MODEL (or data_vars) present is divided
+    in place by the grid's u x v size."""
+    try_vars = _try_vars(data_vars, ("VISIBILITY", "VISIBILITY_RESIDUAL", "VISIBILITY_MODEL"))
+    u_size = image.sizes["u"]
+    v_size = image.sizes["v"]
+    for vis_var in try_vars:
+        if vis_var in image.data_vars:
+            _rescale(image[vis_var].data, _DIV, u_size * v_size)
+
+
+def correct_ifft_to_lm(image, data_vars: Union[str, List[str]] = "",
+                       doSpheroidCorr: bool = False, convsampling: int = 100,
+                       convsupport: int = 7) -> None:
+    """standard_image_grid_preparation.py:412-492: each of SKY, RESIDUAL (or
+    data_vars) present is multiplied in place by l x m; with doSpheroidCorr
+    each (time, frequency, polarization) plane is multiplied instead by
+    l x m / (corrTerm x norm), corrTerm the grid correction of the
+    prolate-spheroidal kernel for the (l, m) image and norm the plane's
+    value of VISIBILITY_NORMALIZATION (for SKY) or
+    VISIBILITY_<var>_NORMALIZATION, which must exist.  The correction is
+    applied over the variable's dims in the order (time, frequency,
+    polarization, l, m)."""
+    try_vars = _try_vars(data_vars, ("SKY", "RESIDUAL"))
+    nx = image.sizes["l"]
+    ny = image.sizes["m"]
+    corr = None
+    if doSpheroidCorr:
+        # create_prolate_spheroidal_kernel's kernel image depends only on the
+        # image size, so the kernel itself (unused here) is not built.
+        corr = K.corr_term(nx, ny)
+    for sky_var in try_vars:
+        if sky_var in image.data_vars:
+            if not doSpheroidCorr:
+                _rescale(image[sky_var].data, _MUL, nx * ny)
+                continue
+            sumwt = ("VISIBILITY_NORMALIZATION" if sky_var == "SKY"
+                     else "VISIBILITY_" + sky_var + "_NORMALIZATION")
+            if sumwt not in image.data_vars:
+                raise Exception(f"Do not have {sumwt} to do image correction")
+            var = image[sky_var]
+            dims = tuple(getattr(var, "dims", ()))
+            if dims and dims[-2:] != ("l", "m"):
+                raise ValueError(f"{sky_var}: dims {dims} do not end with (l, m)")
+            x = var.data
+            norm = image[sumwt].data
+            n_planes = int(np.prod(x.shape[:-2]))
+            if int(np.prod(norm.shape)) != n_planes:
+                raise ValueError(f"{sumwt} has {int(np.prod(norm.shape))} values for "
+                                 f"{n_planes} planes of {sky_var}")
+            _rescale(x, _SPHEROID, nx * ny, corr, norm)

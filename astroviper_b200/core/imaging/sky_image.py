@@ -25,6 +25,12 @@ class _Var:
     def data(self):
         return self.values
 
+    @data.setter
+    def data(self, values):
+        if tuple(values.shape) != tuple(self.values.shape):
+            raise ValueError("replacement data must keep the variable's shape")
+        self.values = values
+
     @property
     def shape(self):
         return tuple(self.values.shape)
@@ -58,8 +64,11 @@ class SkyImage:
 
     @property
     def sizes(self):
-        for v in self._vars.values():
-            return dict(zip(DIMS, (int(s) for s in v.values.shape)))
+        if self._vars:
+            out = {}
+            for v in self._vars.values():
+                out.update(zip(v.dims, (int(s) for s in v.values.shape)))
+            return out
         return {d: len(self._coords[d]) for d in DIMS if d in self._coords}
 
     @property
@@ -79,13 +88,26 @@ class SkyImage:
         return self._coords[name]
 
     def __setitem__(self, name, value):
+        """ds[name] = array (dims DIMS, or their first three for a per-plane
+        variable such as a normalisation) or (dims, array), as xarray takes
+        it; a uv image is ("time", "frequency", "polarization", "u", "v")."""
+        dims = None
+        if isinstance(value, tuple) and len(value) == 2:
+            dims, value = tuple(value[0]), value[1]
         vals = value.values if hasattr(value, "values") and not isinstance(
             value, (np.ndarray, torch.Tensor)) else value
         if not isinstance(vals, (np.ndarray, torch.Tensor)):
             vals = np.asarray(vals)
-        if len(vals.shape) != len(DIMS):
-            raise ValueError(f"{name}: data variables have dims {DIMS}")
-        self._vars[name] = _Var(vals, DIMS)
+        if dims is None:
+            if len(vals.shape) == len(DIMS):
+                dims = DIMS
+            elif len(vals.shape) == 3:
+                dims = DIMS[:3]
+            else:
+                raise ValueError(f"{name}: data variables have dims {DIMS} (or {DIMS[:3]})")
+        if len(dims) != len(vals.shape):
+            raise ValueError(f"{name}: {len(dims)} dims for a {len(vals.shape)}-d array")
+        self._vars[name] = _Var(vals, dims)
 
     def copy(self, deep=True):
         out = SkyImage(attrs=self.attrs)

@@ -435,11 +435,113 @@ static unsigned stride_blocks(int64_t n, int threads) {
   return (unsigned)b;
 }
 
+// ------------------------------------------------ plane normalisation ---
+// correct_fft_to_uv / correct_ifft_to_lm (standard_image_grid_preparation.py:
+// 380-492) on x (n_planes, n_pix), real or complex, in place and in numpy's
+// arithmetic for an array updated by a scalar:
+//   mode 0, x /= s: a real x divided by s; a complex x (a, b) scaled as numpy
+//     divides by the complex (s, 0): ((a + b*0) * r, (b - a*0) * r), r = 1/s,
+//     all in the data's precision;
+//   mode 1, x *= s: a real x times s; a complex x times (s, 0):
+//     (a*s - b*0, a*0 + b*s), in the data's precision (s, a pixel count, is
+//     exact in FP32 up to 2^24);
+//   mode 2, x *= f with f = s / (corr[i] * w[plane]) rounded in FP64 and the
+//     product formed in FP64 (as mode 1's formula for a complex x), then
+//     rounded to the data's precision.
+// The signs of zeros and the NaNs of infinite parts follow from these
+// formulas, so they are written with the rounding intrinsics, uncontracted.
+__device__ __forceinline__ float r_div(float a, float b) { return __fdiv_rn(a, b); }
+__device__ __forceinline__ double r_div(double a, double b) { return __ddiv_rn(a, b); }
+__device__ __forceinline__ float r_mul(float a, float b) { return __fmul_rn(a, b); }
+__device__ __forceinline__ double r_mul(double a, double b) { return __dmul_rn(a, b); }
+__device__ __forceinline__ float r_add(float a, float b) { return __fadd_rn(a, b); }
+__device__ __forceinline__ double r_add(double a, double b) { return __dadd_rn(a, b); }
+__device__ __forceinline__ float r_sub(float a, float b) { return __fsub_rn(a, b); }
+__device__ __forceinline__ double r_sub(double a, double b) { return __dsub_rn(a, b); }
+
+template <typename R>
+__device__ __forceinline__ void cplx_scale(R &a, R &b, R f) {
+  const R z = R(0);
+  const R re = r_sub(r_mul(a, f), r_mul(b, z));
+  const R im = r_add(r_mul(a, z), r_mul(b, f));
+  a = re;
+  b = im;
+}
+
+template <typename T, int COMPS>
+__global__ void __launch_bounds__(256) k_plane_rescale(T *x, int64_t n_planes, int64_t n_pix,
+                                                       int mode, double s, const double *corr,
+                                                       const double *w) {
+  const int64_t n = n_planes * n_pix;
+  const T st = (T)s;
+  const T rt = r_div(T(1), st);
+  for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < n;
+       e += (int64_t)gridDim.x * blockDim.x) {
+    if (COMPS == 1) {
+      if (mode == 0) {
+        x[e] = r_div(x[e], st);
+      } else if (mode == 1) {
+        x[e] = r_mul(x[e], st);
+      } else {
+        const int64_t pl = e / n_pix, i = e - pl * n_pix;
+        const double f = __ddiv_rn(s, __dmul_rn(corr[i], w[pl]));
+        x[e] = (T)__dmul_rn((double)x[e], f);
+      }
+    } else {
+      T a = x[2 * e], b = x[2 * e + 1];
+      if (mode == 0) {
+        const T z = T(0);
+        const T re = r_mul(r_add(a, r_mul(b, z)), rt);
+        const T im = r_mul(r_sub(b, r_mul(a, z)), rt);
+        a = re;
+        b = im;
+      } else if (mode == 1) {
+        cplx_scale<T>(a, b, st);
+      } else {
+        const int64_t pl = e / n_pix, i = e - pl * n_pix;
+        const double f = __ddiv_rn(s, __dmul_rn(corr[i], w[pl]));
+        double ad = (double)a, bd = (double)b;
+        cplx_scale<double>(ad, bd, f);
+        a = (T)ad;
+        b = (T)bd;
+      }
+      x[2 * e] = a;
+      x[2 * e + 1] = b;
+    }
+  }
+}
+
 }  // namespace av
 
 using namespace av;
 
 extern "C" {
+
+int av_plane_rescale(void *x, int dtype, int64_t n_planes, int64_t n_pix, int mode, double s,
+                     const double *corr, const double *w, void *stream) {
+  clear_error();
+  AV_CHECK_ARG(x, "av_plane_rescale: null pointer");
+  AV_CHECK_ARG(dtype >= AV_F32 && dtype <= AV_C128, "av_plane_rescale: dtype");
+  AV_CHECK_ARG(mode >= 0 && mode <= 2, "av_plane_rescale: mode must be 0, 1 or 2");
+  AV_CHECK_ARG(mode != 2 || (corr && w), "av_plane_rescale: mode 2 needs corr and w");
+  AV_CHECK_ARG(n_planes >= 0 && n_pix >= 0, "av_plane_rescale: bad shape");
+  const int64_t n = n_planes * n_pix;
+  if (n == 0) return AV_OK;
+  cudaStream_t st = as_stream(stream);
+  const unsigned blocks = stride_blocks(n, 256);
+  if (dtype == AV_F32)
+    k_plane_rescale<float, 1><<<blocks, 256, 0, st>>>((float *)x, n_planes, n_pix, mode, s, corr, w);
+  else if (dtype == AV_F64)
+    k_plane_rescale<double, 1><<<blocks, 256, 0, st>>>((double *)x, n_planes, n_pix, mode, s, corr,
+                                                       w);
+  else if (dtype == AV_C64)
+    k_plane_rescale<float, 2><<<blocks, 256, 0, st>>>((float *)x, n_planes, n_pix, mode, s, corr, w);
+  else
+    k_plane_rescale<double, 2><<<blocks, 256, 0, st>>>((double *)x, n_planes, n_pix, mode, s, corr,
+                                                       w);
+  AV_LAUNCH_CHECK();
+  return AV_OK;
+}
 
 int av_pol_transform(const void *in, int in_dtype, void *out, int out_dtype,
                      const double *matrix, int n_in, int n_out, int64_t n_outer, int64_t n_pix,

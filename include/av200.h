@@ -423,6 +423,20 @@ size_t av_plane_sum_workspace_size(int64_t n_planes, int64_t n_pix);
 int av_plane_sum(const void *x, int dtype, int64_t n_planes, int64_t n_pix, double *out,
                  void *workspace, size_t workspace_bytes, void *stream);
 
+/* correct_fft_to_uv / correct_ifft_to_lm (standard_image_grid_preparation.py:
+ * 380-492): x (n_planes, n_pix) of AV_F32 / AV_F64 / AV_C64 / AV_C128, in
+ * place.  mode 0: x /= s (correct_fft_to_uv, s = u x v); mode 1: x *= s
+ * (correct_ifft_to_lm without the spheroid correction, s = l x m); mode 2:
+ * x *= s / (corr[pix] * w[plane]) (with it: corr the grid-correction term of
+ * create_prolate_spheroidal_kernel, n_pix doubles, w the planes'
+ * normalisations, n_planes doubles).  Modes 0 and 1 compute in the data's
+ * precision, mode 2 forms its factor and the product in FP64, as numpy does;
+ * a complex x is scaled as numpy divides or multiplies it by the complex
+ * (s, 0) (division: both parts times the reciprocal of s), which also fixes
+ * the signs of zeros and the NaNs of infinite parts. */
+int av_plane_rescale(void *x, int dtype, int64_t n_planes, int64_t n_pix, int mode, double s,
+                     const double *corr, const double *w, void *stream);
+
 /* compute_residual_visibilities (imager.py:82-85): out = vis - model over n
  * complex values (AV_C64 / AV_C128); out may alias vis or model. */
 int av_vis_residual(const void *vis, const void *model, void *out, int dtype, int64_t n,

@@ -210,3 +210,28 @@ def run_imaging_loop(vis, uvw, weight, flag, freq, params, controller, merge, Re
                residual_vis=None if vis_model is None else vis - vis_model,
                controller=controller, combined=combined)
     return out
+
+
+# ----------------------------------------------------------------------------
+# Normalisation helpers (standard_image_grid_preparation.py:312-492)
+# ----------------------------------------------------------------------------
+def correct_fft_to_uv_planes(x, u_size, v_size):
+    """standard_image_grid_preparation.py:405-409: x /= u * v in place, in
+    numpy's own arithmetic for the array's dtype."""
+    x /= u_size * v_size
+    return x
+
+
+def correct_ifft_to_lm_planes(x, nx, ny, corr=None, norm=None):
+    """standard_image_grid_preparation.py:458-492 on x (time, frequency,
+    polarization, l, m), in place: x *= nx * ny, or with the spheroid
+    correction each plane x[t, f, p] *= (nx * ny) / (corr * norm[t, f, p])
+    (corr the (l, m) grid-correction term)."""
+    if corr is None:
+        x *= nx * ny
+        return x
+    for t in range(x.shape[0]):
+        for f in range(x.shape[1]):
+            for p in range(x.shape[2]):
+                x[t, f, p] *= (nx * ny) / (corr * norm[t, f, p])
+    return x

@@ -1,0 +1,223 @@
+"""Generates image_prep.npz in this folder from the reference itself.
+
+Run in a container that has the astroviper source tree (default
+``/root/reference``, override with ``AV_REFERENCE_ROOT``):
+
+    python tests/golden/make_golden_image_prep.py
+
+Runs the reference's fft_to_uv, ifft_to_lm, correct_fft_to_uv and
+correct_ifft_to_lm (standard_image_grid_preparation.py:312-492), imported
+unmodified, on a small dataset stand-in (the xarray surface those functions
+use: sizes, data_vars, item get / set, .data, in-place *=, coords and .sel
+returning views), with stand-in modules for xarray and xradio and for
+standard_grid (imported by name only).  The inputs and the outputs go into
+image_prep.npz, keyed <case>/<variable>/{in,out}.
+"""
+import os
+import sys
+import types
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+REF = os.environ.get("AV_REFERENCE_ROOT", "/root/reference")
+SRC = os.path.join(REF, "src", "astroviper")
+os.environ.setdefault("NUMBA_CACHE_DIR", "/tmp/numba_cache_golden")
+sys.path.insert(0, HERE)
+
+from make_golden import _DataArray, _DataTree, _mod, _pkg  # noqa: E402
+
+IMAGE_DIMS = ("time", "frequency", "polarization", "l", "m")
+UV_DIMS = ("time", "frequency", "polarization", "u", "v")
+
+
+class _Coord:
+    def __init__(self, v):
+        self.values = np.asarray(v)
+
+
+class _DA:
+    """A data variable: .data (a numpy buffer), .dims, .coords, in-place *=
+    on the buffer, and .sel by coordinate value returning a view."""
+
+    def __init__(self, data, dims, coords):
+        self._data = data
+        self.dims = tuple(dims)
+        self.coords = {d: _Coord(coords[d]) for d in self.dims if d in coords}
+
+    @property
+    def data(self):
+        return self._data
+
+    @data.setter
+    def data(self, v):
+        if v.shape != self._data.shape:
+            raise ValueError("shape change")
+        self._data = v
+
+    def __imul__(self, k):
+        self._data *= k
+        return self
+
+    def sel(self, **kw):
+        idx = []
+        for d in self.dims:
+            if d in kw:
+                idx.append(int(np.flatnonzero(self.coords[d].values == kw[d])[0]))
+            else:
+                idx.append(slice(None))
+        rest = [d for d in self.dims if d not in kw]
+        return _DA(self._data[tuple(idx) + (Ellipsis,)], rest, {})
+
+
+class _DS:
+    def __init__(self, variables, coords):
+        self.coords = coords
+        self.data_vars = {}
+        for name, (dims, data) in variables.items():
+            self.data_vars[name] = _DA(data, dims, coords)
+
+    @property
+    def sizes(self):
+        out = {}
+        for v in self.data_vars.values():
+            out.update(zip(v.dims, v.data.shape))
+        return out
+
+    def __getitem__(self, name):
+        return self.data_vars[name]
+
+    def __setitem__(self, name, value):
+        self.data_vars[name] = value
+
+    def __repr__(self):
+        return "<image>"
+
+
+def load_reference():
+    xr = types.ModuleType("xarray")
+    core = types.ModuleType("xarray.core")
+    dt = types.ModuleType("xarray.core.datatree")
+    dt.DataTree = _DataTree
+    core.datatree = dt
+    xr.core = core
+    xr.DataArray = _DataArray
+    xr.DataTree = _DataTree
+    xr.Dataset = _DS
+    sys.modules.update({"xarray": xr, "xarray.core": core, "xarray.core.datatree": dt})
+    xd = types.ModuleType("xradio")
+    xdi = types.ModuleType("xradio.image")
+    xdii = types.ModuleType("xradio.image.image")
+    xdii.make_empty_lmuv_image = xdii.make_empty_sky_image = None
+    sys.modules.update({"xradio": xd, "xradio.image": xdi, "xradio.image.image": xdii})
+    _pkg("astroviper", SRC)
+    _pkg("astroviper.core", SRC + "/core")
+    _pkg("astroviper.core.imaging", SRC + "/core/imaging")
+    _pkg("astroviper.core.imaging.imaging_utils", SRC + "/core/imaging/imaging_utils")
+    sg = types.ModuleType("astroviper.core.imaging.imaging_utils.standard_grid")
+    sg.standard_grid_numpy_wrap_input_checked = None
+    sys.modules[sg.__name__] = sg
+    iu = SRC + "/core/imaging/imaging_utils/"
+    _mod("astroviper.core.imaging.fft", SRC + "/core/imaging/fft.py")
+    _mod("astroviper.core.imaging.ifft", SRC + "/core/imaging/ifft.py")
+    _mod("astroviper.core.imaging.imaging_utils.gcf_prolate_spheroidal",
+         iu + "gcf_prolate_spheroidal.py")
+    return _mod("astroviper.core.imaging.imaging_utils.standard_image_grid_preparation",
+                iu + "standard_image_grid_preparation.py")
+
+
+def _coords(shape):
+    return {"time": np.arange(shape[0]) * 10.0 + 5.0,
+            "frequency": 1.0e9 + np.arange(shape[1]) * 1.0e6,
+            "polarization": np.array(["XX", "XY", "YX", "YY"][:shape[2]])}
+
+
+def _cplx(rng, shape, dtype):
+    x = (rng.normal(size=shape) + 1j * rng.normal(size=shape)).astype(dtype)
+    flat = x.reshape(-1)
+    ft = flat.real.dtype
+    specials = [(-0.0, 1.0), (1.0, -0.0), (-0.0, -0.0), (np.inf, 1.0), (1.0, -np.inf),
+                (np.nan, 2.0), (3.0e-39 if ft == np.float32 else 3.0e-310, -1.0)]
+    for k, (a, b) in enumerate(specials):
+        flat.real[k * 7] = a
+        flat.imag[k * 7] = b
+    return x
+
+
+def run(ref):
+    rng = np.random.default_rng(20261203)
+    out = {}
+
+    def record(case, ds, names_in, call):
+        for n in names_in:
+            out[f"{case}/{n}/in"] = ds[n].data.copy()
+        call(ds)
+        for n, v in ds.data_vars.items():
+            out[f"{case}/{n}/out"] = v.data.copy()
+
+    # correct_fft_to_uv on complex grids, u x v = 12 x 10 (not a power of 2)
+    for tag, dt in (("c128", np.complex128), ("c64", np.complex64)):
+        shp = (2, 2, 2, 12, 10)
+        ds = _DS({"VISIBILITY": (UV_DIMS, _cplx(rng, shp, dt)),
+                  "VISIBILITY_RESIDUAL": (UV_DIMS, _cplx(rng, shp, dt)),
+                  "OTHER": (UV_DIMS, _cplx(rng, shp, dt))}, _coords(shp))
+        record(f"cfu_{tag}", ds, list(ds.data_vars), lambda d: ref.correct_fft_to_uv(d))
+        ds = _DS({"VISIBILITY_MODEL": (UV_DIMS, _cplx(rng, shp, dt))}, _coords(shp))
+        record(f"cfu_named_{tag}", ds, list(ds.data_vars),
+               lambda d: ref.correct_fft_to_uv(d, "VISIBILITY_MODEL"))
+
+    # correct_ifft_to_lm without the spheroid correction: real and complex
+    for tag, dt in (("f64", np.float64), ("f32", np.float32)):
+        shp = (2, 3, 2, 14, 10)
+        sky = rng.normal(size=shp).astype(dt)
+        sky.reshape(-1)[:4] = [-0.0, np.inf, np.nan, 1e-39 if dt == np.float32 else 1e-310]
+        ds = _DS({"SKY": (IMAGE_DIMS, sky),
+                  "RESIDUAL": (IMAGE_DIMS, rng.normal(size=shp).astype(dt)),
+                  "MODEL": (IMAGE_DIMS, rng.normal(size=shp).astype(dt))}, _coords(shp))
+        record(f"cil_{tag}", ds, list(ds.data_vars), lambda d: ref.correct_ifft_to_lm(d))
+    shp = (1, 2, 2, 9, 11)
+    ds = _DS({"RESIDUAL": (IMAGE_DIMS, _cplx(rng, shp, np.complex64))}, _coords(shp))
+    record("cil_c64", ds, list(ds.data_vars), lambda d: ref.correct_ifft_to_lm(d, ["RESIDUAL"]))
+
+    # correct_ifft_to_lm with the spheroid correction (default 100 / 7 kernel)
+    shp = (2, 2, 2, 16, 12)
+    ds = _DS({"SKY": (IMAGE_DIMS, rng.normal(size=shp)),
+              "RESIDUAL": (IMAGE_DIMS, rng.normal(size=shp).astype(np.float32)),
+              "VISIBILITY_NORMALIZATION": (IMAGE_DIMS[:3], rng.uniform(10, 1e4, shp[:3])),
+              "VISIBILITY_RESIDUAL_NORMALIZATION":
+                  (IMAGE_DIMS[:3], rng.uniform(10, 1e4, shp[:3]).astype(np.float32))},
+             _coords(shp))
+    record("cil_sph", ds, list(ds.data_vars),
+           lambda d: ref.correct_ifft_to_lm(d, doSpheroidCorr=True))
+    shp = (1, 3, 1, 20, 20)
+    ds = _DS({"RESIDUAL": (IMAGE_DIMS, rng.normal(size=shp)),
+              "VISIBILITY_RESIDUAL_NORMALIZATION": (IMAGE_DIMS[:3], rng.uniform(1, 9, shp[:3]))},
+             _coords(shp))
+    record("cil_sph_named", ds, list(ds.data_vars),
+           lambda d: ref.correct_ifft_to_lm(d, "RESIDUAL", True, 64, 9))
+    out["cil_sph_named/corr"] = sys.modules[
+        "astroviper.core.imaging.imaging_utils.gcf_prolate_spheroidal"
+    ].create_prolate_spheroidal_kernel(64, 9, np.array([20, 20]))[1]
+
+    # the transforms
+    shp = (1, 2, 2, 16, 12)
+    ds = _DS({"SKY": (IMAGE_DIMS, rng.normal(size=shp)),
+              "MODEL": (IMAGE_DIMS, rng.normal(size=shp)),
+              "VISIBILITY_SKY": (UV_DIMS, np.zeros(shp, complex)),
+              "VISIBILITY_MODEL": (UV_DIMS, np.zeros(shp, complex))}, _coords(shp))
+    record("fft", ds, ["SKY", "MODEL"], lambda d: ref.fft_to_uv(d))
+    ds = _DS({"VISIBILITY": (UV_DIMS, _cplx(rng, shp, np.complex128)),
+              "VISIBILITY_RESIDUAL": (UV_DIMS, _cplx(rng, shp, np.complex128)),
+              "SKY": (IMAGE_DIMS, np.zeros(shp)),
+              "RESIDUAL": (IMAGE_DIMS, np.zeros(shp))}, _coords(shp))
+    for n in ("VISIBILITY", "VISIBILITY_RESIDUAL"):
+        ds[n].data[~np.isfinite(ds[n].data)] = 0.5
+    record("ifft", ds, ["VISIBILITY", "VISIBILITY_RESIDUAL"], lambda d: ref.ifft_to_lm(d))
+
+    np.savez_compressed(os.path.join(HERE, "image_prep.npz"), **out)
+    return out
+
+
+if __name__ == "__main__":
+    with np.errstate(all="ignore"):
+        run(load_reference())

@@ -1,0 +1,232 @@
+"""fft_to_uv / ifft_to_lm / correct_fft_to_uv / correct_ifft_to_lm
+(standard_image_grid_preparation.py:312-492).
+
+CPU: the oracle's restatement of the two normalisations against the
+reference's outputs in tests/golden/image_prep.npz (bit-exact, NaN positions
+compared as positions).  GPU: the drop-in functions on SkyImage datasets
+against the same outputs: the normalisations bit-exact where the reference's
+inputs are used as they are (with the spheroid correction, to 1e-13
+relative, since the device's grid-correction term is within 1e-14 of the
+reference's; the rescale itself bit-exact against the oracle given the same
+term); the transforms to 1e-12 of each plane's peak (cuFFT against numpy's
+pocketfft).
+"""
+import numpy as np
+import pytest
+
+import oracle as O
+import oracle.imager as OI
+from conftest import golden
+
+UV_DIMS = ("time", "frequency", "polarization", "u", "v")
+
+
+def same_bits(a, b):
+    """Equal values bit for bit (signs of zeros included); NaNs compared by
+    position, since NaN payloads are not specified by either side."""
+    a = np.asarray(a)
+    b = np.asarray(b)
+    if a.shape != b.shape or a.dtype != b.dtype:
+        return False
+    if np.iscomplexobj(a):
+        return same_bits(a.real.copy(), b.real.copy()) and same_bits(a.imag.copy(), b.imag.copy())
+    na, nb = np.isnan(a), np.isnan(b)
+    if not np.array_equal(na, nb):
+        return False
+    u = np.uint32 if a.dtype == np.float32 else np.uint64
+    return np.array_equal(a[~na].view(u), b[~nb].view(u))
+
+
+def _cases(g, prefix):
+    names = sorted({k.split("/")[0] for k in g.files if k.split("/")[0].startswith(prefix)})
+    return names
+
+
+def _vars(g, case, which):
+    return {k.split("/")[1]: g[k] for k in g.files
+            if k.startswith(case + "/") and k.endswith("/" + which)}
+
+
+# ----------------------------------------------------------------- CPU ---
+def test_oracle_correct_fft_to_uv_matches_reference():
+    g = golden("image_prep.npz")
+    cases = _cases(g, "cfu_")
+    assert len(cases) == 4
+    for case in cases:
+        ins, outs = _vars(g, case, "in"), _vars(g, case, "out")
+        named = "named" in case
+        for n, x in ins.items():
+            y = x.copy()
+            if named or n in ("VISIBILITY", "VISIBILITY_RESIDUAL", "VISIBILITY_MODEL"):
+                with np.errstate(all="ignore"):
+                    OI.correct_fft_to_uv_planes(y, x.shape[3], x.shape[4])
+            assert same_bits(y, outs[n]), (case, n)
+
+
+def test_oracle_correct_ifft_to_lm_matches_reference():
+    g = golden("image_prep.npz")
+    for case in ("cil_f64", "cil_f32", "cil_c64"):
+        ins, outs = _vars(g, case, "in"), _vars(g, case, "out")
+        for n, x in ins.items():
+            y = x.copy()
+            if n in ("SKY", "RESIDUAL"):
+                with np.errstate(all="ignore"):
+                    OI.correct_ifft_to_lm_planes(y, x.shape[3], x.shape[4])
+            assert same_bits(y, outs[n]), (case, n)
+    ins, outs = _vars(g, "cil_sph", "in"), _vars(g, "cil_sph", "out")
+    nx, ny = ins["SKY"].shape[3:]
+    corr = O.corr_term((nx, ny))
+    for n, norm in (("SKY", "VISIBILITY_NORMALIZATION"),
+                    ("RESIDUAL", "VISIBILITY_RESIDUAL_NORMALIZATION")):
+        y = ins[n].copy()
+        OI.correct_ifft_to_lm_planes(y, nx, ny, corr, ins[norm])
+        assert same_bits(y, outs[n]), n
+    ins, outs = _vars(g, "cil_sph_named", "in"), _vars(g, "cil_sph_named", "out")
+    y = ins["RESIDUAL"].copy()
+    OI.correct_ifft_to_lm_planes(y, 20, 20, g["cil_sph_named/corr"],
+                                 ins["VISIBILITY_RESIDUAL_NORMALIZATION"])
+    assert same_bits(y, outs["RESIDUAL"])
+
+
+def test_oracle_transforms_match_reference():
+    g = golden("image_prep.npz")
+    for n in ("SKY", "MODEL"):
+        ref = g[f"fft/VISIBILITY_{n}/out"]
+        assert np.array_equal(O.fft_lm_to_uv(g[f"fft/{n}/in"], axes=[3, 4]), ref)
+    for n, dst in (("VISIBILITY", "SKY"), ("VISIBILITY_RESIDUAL", "RESIDUAL")):
+        assert np.array_equal(O.ifft_uv_to_lm(g[f"ifft/{n}/in"], axes=[3, 4]),
+                              g[f"ifft/{dst}/out"])
+
+
+# ----------------------------------------------------------------- GPU ---
+def _prep():
+    from astroviper_b200.core.imaging.imaging_utils import standard_image_grid_preparation as P
+    return P
+
+
+def _image(ins, uv_names=(), to_device=False):
+    import torch
+    from astroviper_b200.core.imaging.sky_image import SkyImage
+    img = SkyImage()
+    for n, x in ins.items():
+        v = x.copy()
+        if to_device:
+            v = torch.from_numpy(v).cuda()
+        img[n] = (UV_DIMS, v) if n in uv_names or n.startswith("VISIBILITY") and v.ndim == 5 \
+            else v
+    return img
+
+
+def _np(x):
+    return x.cpu().numpy() if hasattr(x, "cpu") else np.asarray(x)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("on_device", [False, True])
+def test_correct_fft_to_uv_bit_exact(on_device):
+    P = _prep()
+    g = golden("image_prep.npz")
+    for case in _cases(g, "cfu_"):
+        ins, outs = _vars(g, case, "in"), _vars(g, case, "out")
+        img = _image(ins, uv_names=tuple(ins), to_device=on_device)
+        before = {n: img[n].data for n in ins}
+        if "named" in case:
+            P.correct_fft_to_uv(img, "VISIBILITY_MODEL")
+        else:
+            P.correct_fft_to_uv(img)
+        for n in ins:
+            assert img[n].data is before[n], "the variable must be updated in place"
+            assert same_bits(_np(img[n].data), outs[n]), (case, n, on_device)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("on_device", [False, True])
+def test_correct_ifft_to_lm_bit_exact(on_device):
+    P = _prep()
+    g = golden("image_prep.npz")
+    for case in ("cil_f64", "cil_f32", "cil_c64"):
+        ins, outs = _vars(g, case, "in"), _vars(g, case, "out")
+        img = _image(ins, to_device=on_device)
+        if case == "cil_c64":
+            P.correct_ifft_to_lm(img, ["RESIDUAL"])
+        else:
+            P.correct_ifft_to_lm(img)
+        for n in ins:
+            assert same_bits(_np(img[n].data), outs[n]), (case, n, on_device)
+
+
+@pytest.mark.gpu
+def test_correct_ifft_to_lm_spheroid():
+    P = _prep()
+    g = golden("image_prep.npz")
+    for case, args in (("cil_sph", dict(doSpheroidCorr=True)),
+                       ("cil_sph_named", dict(data_vars="RESIDUAL", doSpheroidCorr=True,
+                                              convsampling=64, convsupport=9))):
+        ins, outs = _vars(g, case, "in"), _vars(g, case, "out")
+        img = _image(ins)
+        P.correct_ifft_to_lm(img, **args)
+        for n in ins:
+            got, ref = _np(img[n].data), outs[n]
+            if n.endswith("NORMALIZATION"):
+                assert same_bits(got, ref)
+                continue
+            tol = 1e-13 if got.dtype == np.float64 else 2e-7
+            assert np.max(np.abs(got - ref) / np.abs(ref)) <= tol, (case, n)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("dtype", [np.float64, np.float32, np.complex64, np.complex128])
+def test_plane_rescale_spheroid_bit_exact_given_the_term(dtype):
+    from astroviper_b200 import _kernels as K
+    import torch
+    rng = np.random.default_rng(7)
+    shp = (2, 3, 2, 18, 14)
+    x = rng.normal(size=shp)
+    if np.dtype(dtype).kind == "c":
+        x = x + 1j * rng.normal(size=shp)
+    x = x.astype(dtype)
+    x.reshape(-1)[:3] = [-0.0, np.inf, np.nan]
+    norm = rng.uniform(1, 1e5, shp[:3])
+    corr = K.corr_term(18, 14)
+    t = torch.from_numpy(x.copy()).cuda()
+    K.plane_rescale(t, 2, 18 * 14, corr, norm)
+    want = x.copy()
+    with np.errstate(all="ignore"):
+        OI.correct_ifft_to_lm_planes(want, 18, 14, corr.cpu().numpy(), norm)
+    assert same_bits(t.cpu().numpy(), want)
+
+
+@pytest.mark.gpu
+def test_transforms_match_reference():
+    P = _prep()
+    g = golden("image_prep.npz")
+    ins, outs = _vars(g, "fft", "in"), _vars(g, "fft", "out")
+    img = _image({**ins, "VISIBILITY_SKY": outs["VISIBILITY_SKY"] * 0,
+                  "VISIBILITY_MODEL": outs["VISIBILITY_MODEL"] * 0})
+    P.fft_to_uv(img)
+    for n in ("VISIBILITY_SKY", "VISIBILITY_MODEL"):
+        got, ref = _np(img[n].data), outs[n]
+        peak = np.max(np.abs(ref), axis=(3, 4), keepdims=True)
+        assert np.max(np.abs(got - ref) / peak) <= 1e-12, n
+    ins, outs = _vars(g, "ifft", "in"), _vars(g, "ifft", "out")
+    img = _image({**ins, "SKY": outs["SKY"] * 0, "RESIDUAL": outs["RESIDUAL"] * 0})
+    P.ifft_to_lm(img)
+    for n in ("SKY", "RESIDUAL"):
+        got, ref = _np(img[n].data), outs[n]
+        peak = np.max(np.abs(ref), axis=(3, 4), keepdims=True)
+        assert np.max(np.abs(got - ref) / peak) <= 1e-12, n
+
+
+@pytest.mark.gpu
+def test_errors_follow_the_reference():
+    P = _prep()
+    rng = np.random.default_rng(3)
+    img = _image({"SKY": rng.normal(size=(1, 1, 1, 8, 8))})
+    with pytest.raises(Exception, match="Do not have VISIBILITY_NORMALIZATION"):
+        P.correct_ifft_to_lm(img, doSpheroidCorr=True)
+    with pytest.raises(Exception, match="VISIBILITY_SKY is not in"):
+        P.fft_to_uv(img)
+    with pytest.raises(KeyError):
+        P.correct_fft_to_uv(img)  # no u / v dims, as image.sizes["u"] fails there
+    with pytest.raises(KeyError):
+        P.ifft_to_lm(_image({"VISIBILITY": np.zeros((1, 1, 1, 4, 4), complex)}))
