@@ -704,3 +704,25 @@ def plane_rescale(t, mode, s, corr=None, w=None):
     check(lib().av_plane_rescale(p(t), dcode(t), npl, ny * nx, int(mode), float(s), p(c), p(ww),
                                  stream_ptr()), "av_plane_rescale")
     return t
+
+
+def apply_pb(t, pb, multiply):
+    """In place on the contiguous device tensor t (nt, nc, np, ny, nx), or of
+    any shape when pb has the same shape: av_apply_pb with the contiguous
+    real device tensor pb (pt, pc, pp, ny, nx)."""
+    assert t.is_contiguous() and t.is_cuda and pb.is_contiguous() and pb.is_cuda
+    if tuple(t.shape) == tuple(pb.shape):
+        n_pix = int(t.shape[-1]) * int(t.shape[-2]) if t.ndim >= 2 else int(t.numel())
+        npl = int(t.numel() // max(1, n_pix))
+        dims, pdims = (1, 1, npl), (1, 1, npl)
+    else:
+        if t.ndim != 5 or pb.ndim != 5 or tuple(t.shape[3:]) != tuple(pb.shape[3:]):
+            raise ValueError("a primary beam of another shape must be 5-D like the image, "
+                             "with the same (l, m) extent")
+        n_pix = int(t.shape[3]) * int(t.shape[4])
+        dims, pdims = tuple(int(d) for d in t.shape[:3]), tuple(int(d) for d in pb.shape[:3])
+    if pb.dtype not in (torch.float32, torch.float64):
+        raise TypeError("apply_pb: the primary beam must be float32 or float64")
+    check(lib().av_apply_pb(p(t), dcode(t), *dims, p(pb), dcode(pb), *pdims, n_pix,
+                            int(bool(multiply)), stream_ptr()), "av_apply_pb")
+    return t

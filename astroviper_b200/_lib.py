@@ -94,6 +94,7 @@ SIGNATURES = {
     "av_psf_sidelobe": (_i, [_vp, _i, _i64, _i64, _i, _i, _d, _vp, _vp, _sz, _vp]),
     "av_plane_sum_workspace_size": (_sz, [_i64, _i64]),
     "av_plane_rescale": (_i, [_vp, _i, _i64, _i64, _i, _d, _vp, _vp, _vp]),
+    "av_apply_pb": (_i, [_vp, _i, _i64, _i64, _i64, _vp, _i, _i64, _i64, _i64, _i64, _i, _vp]),
     "av_plane_sum": (_i, [_vp, _i, _i64, _i64, _vp, _vp, _sz, _vp]),
     "av_vis_residual": (_i, [_vp, _vp, _vp, _i, _i64, _vp]),
     "av_cf_phase_product": (_i, [_vp, _i, _vp, _vp, _i64, _i64, _i64, _vp]),

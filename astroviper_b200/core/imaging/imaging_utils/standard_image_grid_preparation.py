@@ -1,13 +1,17 @@
-"""The image <-> uv-grid transforms and their normalisations on B200.
+"""The image <-> uv-grid transforms, their normalisations and the primary
+beam on B200.
 
-Drop-in for fft_to_uv, ifft_to_lm, correct_fft_to_uv and correct_ifft_to_lm of
+Drop-in for remove_padding, apply_pb, fft_to_uv, ifft_to_lm,
+correct_fft_to_uv and correct_ifft_to_lm of
 src/astroviper/core/imaging/imaging_utils/standard_image_grid_preparation.py
-(:312-492): same arguments, defaults, variable-name rules, exceptions and
+(:99-492): same arguments, defaults, variable-name rules, exceptions and
 in-place updates of the image dataset.  The transforms are this package's
-cuFFT fft_lm_to_uv / ifft_uv_to_lm; the normalisations run in libav200
-(av_plane_rescale), one launch per variable, in numpy's arithmetic for an
-array scaled by a scalar, so their results are bit-identical to the
-reference's for the same transform output.
+cuFFT fft_lm_to_uv / ifft_uv_to_lm; the normalisations (av_plane_rescale)
+and the primary-beam product or quotient (av_apply_pb) run in libav200, one
+launch per variable, in numpy's arithmetic for the reference's in-place
+updates, so their results are bit-identical to the reference's for the same
+inputs.  The dataset constructors of the same file (make_image_xds,
+make_empty_padded_uv_image) build xradio images and are not provided.
 
 The image may be a SkyImage (its variables numpy arrays or device tensors) or
 an xarray Dataset.  numpy variables are updated in place in their own
@@ -42,6 +46,48 @@ def _rescale(x, mode, s, corr=None, w=None):
     K.plane_rescale(t, mode, s, corr, w)
     H.write_back(x, t)
     return x
+
+
+def remove_padding(image, image_size):
+    """standard_image_grid_preparation.py:99-120: the centre image_size
+    (l, m) pixels of every variable, as views (image.isel)."""
+    image_size = np.array(image_size)
+    image_size_padded = np.array([image.sizes["l"], image.sizes["m"]])
+    start_xy = image_size_padded // 2 - image_size // 2
+    end_xy = start_xy + image_size
+    return image.isel(l=slice(start_xy[0], end_xy[0]), m=slice(start_xy[1], end_xy[1]))
+
+
+def apply_pb(image, pb=None, multiply: bool = True,
+             data_vars: Union[str, List[str]] = "") -> None:
+    """standard_image_grid_preparation.py:236-275: each of SKY, RESIDUAL,
+    MODEL (or data_vars) present is multiplied (or divided, with NaN where
+    the beam is 0) in place by PRIMARY_BEAM of pb, or of the image when pb is
+    None.  The beam must be real."""
+    if (pb is None) and ("PRIMARY_BEAM" not in image):
+        raise Exception(f"No Primary beam information in {image}")
+    pb_da = pb["PRIMARY_BEAM"] if pb is not None else image["PRIMARY_BEAM"]
+    try_vars = _try_vars(data_vars, ("SKY", "RESIDUAL", "MODEL"))
+    if tuple(pb_da.shape[-2:]) != tuple(image[try_vars[0]].shape[-2:]):
+        raise Exception("shapes on sky are not the same")
+    for sky_var in try_vars:
+        if sky_var in image.data_vars:
+            _mult_div(image[sky_var], pb_da, multiply=multiply)
+
+
+def _mult_div(im_da, pb_da, multiply: bool = True) -> None:
+    """standard_image_grid_preparation.py:278-309: im_da *= or /= pb_da,
+    element by element for equal shapes, else (time, frequency,
+    polarization) plane by plane with pb's index 0 along each axis whose
+    extent differs."""
+    x = im_da.data
+    pbt = H.dev(pb_da.data)
+    if H.is_torch(x) and x.is_cuda and x.is_contiguous():
+        K.apply_pb(x, pbt, multiply)
+        return
+    t = H.dev(x)
+    K.apply_pb(t, pbt, multiply)
+    H.write_back(x, t)
 
 
 def fft_to_uv(image, data_vars: Union[str, List[str]] = "") -> None:

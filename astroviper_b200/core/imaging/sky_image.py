@@ -120,6 +120,22 @@ class SkyImage:
     def load(self):
         return self
 
+    def isel(self, **indexers):
+        """Views of the variables and coordinates with the named dims indexed
+        by the given slices (xarray's isel for slices)."""
+        for d, sl in indexers.items():
+            if not isinstance(sl, slice):
+                raise TypeError(f"isel: {d} must be indexed by a slice")
+
+        def cut(v):
+            idx = tuple(indexers.get(d, slice(None)) for d in v.dims)
+            return _Var(v.values[idx], v.dims)
+
+        out = SkyImage(attrs=self.attrs)
+        out._coords = {k: cut(c) for k, c in self._coords.items()}
+        out._vars = {k: cut(v) for k, v in self._vars.items()}
+        return out
+
     def rename_vars(self, mapping):
         out = self.copy(deep=False)
         out._vars = {mapping.get(k, k): v for k, v in self._vars.items()}

@@ -511,6 +511,65 @@ __global__ void __launch_bounds__(256) k_plane_rescale(T *x, int64_t n_planes, i
   }
 }
 
+// ------------------------------------------------------ primary beam ---
+// _mult_div of apply_pb (standard_image_grid_preparation.py:236-309): x
+// (nt, nc, np, n_pix) times or divided by pb (pt, pc, pp, n_pix), in place;
+// pb's plane is (t, c, p) with each index 0 where pb's extent differs from
+// x's.  numpy's arithmetic for x op= pb: computed in P, the promoted real
+// precision of the two, then rounded to x's type.  A complex x is multiplied
+// as by the complex (p, 0), (a*p - b*0, a*0 + b*p), and divided by it with
+// numpy's complex division, ((a + b*q) * g, (b - a*q) * g), q = 0/p,
+// g = 1/(p + 0*q).  Division by a pb of 0 (either sign) leaves NaN, and
+// (NaN, 0) for a complex x, as the reference's NaN fill does.
+template <typename TX, typename TP, typename P, int COMPS>
+__global__ void __launch_bounds__(256) k_apply_pb(TX *x, const TP *pb, int64_t nt, int64_t nc,
+                                                  int64_t npl, int64_t pt, int64_t pc,
+                                                  int64_t pp, int64_t n_pix, int multiply) {
+  const int64_t n = nt * nc * npl * n_pix;
+  for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < n;
+       e += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t pl = e / n_pix, i = e - pl * n_pix;
+    const int64_t p = pl % npl, tc = pl / npl;
+    const int64_t c = tc % nc, t = tc / nc;
+    const int64_t tu = (pt == nt) ? t : 0, cu = (pc == nc) ? c : 0, pu = (pp == npl) ? p : 0;
+    const P w = (P)pb[((tu * pc + cu) * pp + pu) * n_pix + i];
+    const P z = P(0);
+    const bool zero_fill = !multiply && w == z;
+    if (COMPS == 1) {
+      const P a = (P)x[e];
+      P r = multiply ? r_mul(a, w) : r_div(a, w);
+      if (zero_fill) r = (P)__int_as_float(0x7fc00000);  // a quiet NaN
+      x[e] = (TX)r;
+    } else {
+      const P a = (P)x[2 * e], b = (P)x[2 * e + 1];
+      P re, im;
+      if (multiply) {
+        re = r_sub(r_mul(a, w), r_mul(b, z));
+        im = r_add(r_mul(a, z), r_mul(b, w));
+      } else if (zero_fill) {
+        re = (P)__int_as_float(0x7fc00000);
+        im = z;
+      } else {
+        const P q = r_div(z, w);
+        const P g = r_div(P(1), r_add(w, r_mul(z, q)));
+        re = r_mul(r_add(a, r_mul(b, q)), g);
+        im = r_mul(r_sub(b, r_mul(a, q)), g);
+      }
+      x[2 * e] = (TX)re;
+      x[2 * e + 1] = (TX)im;
+    }
+  }
+}
+
+template <typename TX, typename TP, typename P, int COMPS>
+static void launch_apply_pb(void *x, const void *pb, int64_t nt, int64_t nc, int64_t npl,
+                            int64_t pt, int64_t pc, int64_t pp, int64_t n_pix, int multiply,
+                            cudaStream_t st) {
+  const unsigned blocks = stride_blocks(nt * nc * npl * n_pix, 256);
+  k_apply_pb<TX, TP, P, COMPS><<<blocks, 256, 0, st>>>((TX *)x, (const TP *)pb, nt, nc, npl, pt,
+                                                       pc, pp, n_pix, multiply);
+}
+
 }  // namespace av
 
 using namespace av;
@@ -539,6 +598,48 @@ int av_plane_rescale(void *x, int dtype, int64_t n_planes, int64_t n_pix, int mo
   else
     k_plane_rescale<double, 2><<<blocks, 256, 0, st>>>((double *)x, n_planes, n_pix, mode, s, corr,
                                                        w);
+  AV_LAUNCH_CHECK();
+  return AV_OK;
+}
+
+int av_apply_pb(void *x, int x_dtype, int64_t nt, int64_t nc, int64_t npl, const void *pb,
+                int pb_dtype, int64_t pt, int64_t pc, int64_t pp, int64_t n_pix, int multiply,
+                void *stream) {
+  clear_error();
+  AV_CHECK_ARG(x && pb, "av_apply_pb: null pointer");
+  AV_CHECK_ARG(x_dtype >= AV_F32 && x_dtype <= AV_C128, "av_apply_pb: image dtype");
+  AV_CHECK_ARG(pb_dtype == AV_F32 || pb_dtype == AV_F64,
+               "av_apply_pb: the primary beam must be AV_F32 or AV_F64");
+  AV_CHECK_ARG(nt >= 0 && nc >= 0 && npl >= 0 && n_pix >= 0, "av_apply_pb: bad image shape");
+  AV_CHECK_ARG(pt >= 1 && pc >= 1 && pp >= 1, "av_apply_pb: bad primary-beam shape");
+  if (nt * nc * npl * n_pix == 0) return AV_OK;
+  cudaStream_t st = as_stream(stream);
+  const bool pb64 = pb_dtype == AV_F64;
+  switch (x_dtype) {
+    case AV_F32:
+      if (pb64) launch_apply_pb<float, double, double, 1>(x, pb, nt, nc, npl, pt, pc, pp, n_pix,
+                                                          multiply, st);
+      else launch_apply_pb<float, float, float, 1>(x, pb, nt, nc, npl, pt, pc, pp, n_pix,
+                                                   multiply, st);
+      break;
+    case AV_F64:
+      if (pb64) launch_apply_pb<double, double, double, 1>(x, pb, nt, nc, npl, pt, pc, pp, n_pix,
+                                                           multiply, st);
+      else launch_apply_pb<double, float, double, 1>(x, pb, nt, nc, npl, pt, pc, pp, n_pix,
+                                                     multiply, st);
+      break;
+    case AV_C64:
+      if (pb64) launch_apply_pb<float, double, double, 2>(x, pb, nt, nc, npl, pt, pc, pp, n_pix,
+                                                          multiply, st);
+      else launch_apply_pb<float, float, float, 2>(x, pb, nt, nc, npl, pt, pc, pp, n_pix,
+                                                   multiply, st);
+      break;
+    default:
+      if (pb64) launch_apply_pb<double, double, double, 2>(x, pb, nt, nc, npl, pt, pc, pp, n_pix,
+                                                           multiply, st);
+      else launch_apply_pb<double, float, double, 2>(x, pb, nt, nc, npl, pt, pc, pp, n_pix,
+                                                     multiply, st);
+  }
   AV_LAUNCH_CHECK();
   return AV_OK;
 }

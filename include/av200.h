@@ -437,6 +437,18 @@ int av_plane_sum(const void *x, int dtype, int64_t n_planes, int64_t n_pix, doub
 int av_plane_rescale(void *x, int dtype, int64_t n_planes, int64_t n_pix, int mode, double s,
                      const double *corr, const double *w, void *stream);
 
+/* apply_pb (standard_image_grid_preparation.py:236-275) through _mult_div
+ * (:278-309): x (nt, nc, np, n_pix) of AV_F32 / AV_F64 / AV_C64 / AV_C128
+ * multiplied (multiply != 0) or divided in place by the primary beam pb
+ * (pt, pc, pp, n_pix) of AV_F32 / AV_F64; x's plane (t, c, p) uses pb's plane
+ * with each index 0 where pb's extent differs from x's (equal shapes map
+ * plane to plane).  numpy's arithmetic for x op= pb (the promoted precision,
+ * rounded to x's type; a complex x as numpy multiplies or divides by
+ * (pb, 0)); dividing by a zero beam leaves NaN, (NaN, 0) for a complex x. */
+int av_apply_pb(void *x, int x_dtype, int64_t nt, int64_t nc, int64_t npl, const void *pb,
+                int pb_dtype, int64_t pt, int64_t pc, int64_t pp, int64_t n_pix, int multiply,
+                void *stream);
+
 /* compute_residual_visibilities (imager.py:82-85): out = vis - model over n
  * complex values (AV_C64 / AV_C128); out may alias vis or model. */
 int av_vis_residual(const void *vis, const void *model, void *out, int dtype, int64_t n,

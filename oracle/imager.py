@@ -235,3 +235,28 @@ def correct_ifft_to_lm_planes(x, nx, ny, corr=None, norm=None):
             for p in range(x.shape[2]):
                 x[t, f, p] *= (nx * ny) / (corr * norm[t, f, p])
     return x
+
+
+def mult_div_planes(x, pb, multiply=True):
+    """_mult_div of apply_pb (standard_image_grid_preparation.py:278-309) on
+    numpy arrays, in place: x *= pb or x /= pb with NaN where pb == 0, for
+    equal shapes at once, else per (time, frequency, polarization) plane with
+    pb's index 0 along each axis whose extent differs from x's."""
+    if x.shape == pb.shape:
+        if multiply:
+            x *= pb
+        else:
+            x /= pb
+            x[pb == 0.0] = np.nan
+        return x
+    te, ce, pe = (x.shape[k] == pb.shape[k] for k in range(3))
+    for t in range(x.shape[0]):
+        for c in range(x.shape[1]):
+            for p in range(x.shape[2]):
+                w = pb[t if te else 0, c if ce else 0, p if pe else 0]
+                if multiply:
+                    x[t, c, p] *= w
+                else:
+                    x[t, c, p] /= w
+                    x[t, c, p][w == 0] = np.nan
+    return x

@@ -5,11 +5,12 @@ Run in a container that has the astroviper source tree (default
 
     python tests/golden/make_golden_image_prep.py
 
-Runs the reference's fft_to_uv, ifft_to_lm, correct_fft_to_uv and
-correct_ifft_to_lm (standard_image_grid_preparation.py:312-492), imported
+Runs the reference's remove_padding, apply_pb, fft_to_uv, ifft_to_lm,
+correct_fft_to_uv and correct_ifft_to_lm (standard_image_grid_preparation.py:
+99-492), imported
 unmodified, on a small dataset stand-in (the xarray surface those functions
-use: sizes, data_vars, item get / set, .data, in-place *=, coords and .sel
-returning views), with stand-in modules for xarray and xradio and for
+use: sizes, data_vars, item get / set, .data, in-place *= and /=, ==,
+coords, .sel and .isel returning views), with stand-in modules for xarray and xradio and for
 standard_grid (imported by name only).  The inputs and the outputs go into
 image_prep.npz, keyed <case>/<variable>/{in,out}.
 """
@@ -55,9 +56,33 @@ class _DA:
             raise ValueError("shape change")
         self._data = v
 
+    @property
+    def shape(self):
+        return self._data.shape
+
+    def __array__(self, dtype=None, copy=None):
+        return self._data
+
+    def _raw(self, k):
+        return k._data if isinstance(k, _DA) else k
+
     def __imul__(self, k):
-        self._data *= k
+        self._data *= self._raw(k)
         return self
+
+    def __itruediv__(self, k):
+        self._data /= self._raw(k)
+        return self
+
+    def __eq__(self, k):
+        return self._data == self._raw(k)
+
+    def __getitem__(self, idx):
+        return _DA(self._data[idx], self.dims[-self._data[idx].ndim:] if self._data[idx].ndim
+                   else (), {})
+
+    def __setitem__(self, idx, value):
+        self._data[idx] = self._raw(value)
 
     def sel(self, **kw):
         idx = []
@@ -86,6 +111,16 @@ class _DS:
 
     def __getitem__(self, name):
         return self.data_vars[name]
+
+    def __contains__(self, name):
+        return name in self.data_vars or name in self.coords
+
+    def isel(self, **kw):
+        out = _DS({}, {})
+        for n, v in self.data_vars.items():
+            idx = tuple(kw.get(d, slice(None)) for d in v.dims)
+            out.data_vars[n] = _DA(v.data[idx], v.dims, {})
+        return out
 
     def __setitem__(self, name, value):
         self.data_vars[name] = value
@@ -213,6 +248,49 @@ def run(ref):
     for n in ("VISIBILITY", "VISIBILITY_RESIDUAL"):
         ds[n].data[~np.isfinite(ds[n].data)] = 0.5
     record("ifft", ds, ["VISIBILITY", "VISIBILITY_RESIDUAL"], lambda d: ref.ifft_to_lm(d))
+
+    # apply_pb: equal shapes and planes broadcast from index 0, multiply and
+    # divide (NaN where the beam is 0), real and complex images
+    shp = (2, 3, 2, 10, 8)
+
+    def beam(shape, dtype):
+        b = rng.uniform(0.0, 1.0, shape).astype(dtype)
+        b.reshape(-1)[::9] = 0.0
+        b.reshape(-1)[4::23] = -0.0
+        return b
+
+    for tag, pshape, dt, pdt in (("eq_f64", shp, np.float64, np.float64),
+                                 ("eq_f32_pb64", shp, np.float32, np.float64),
+                                 ("bc_f64", (1, 3, 1, 10, 8), np.float64, np.float64),
+                                 ("bc_f32", (1, 1, 1, 10, 8), np.float32, np.float32),
+                                 ("bc_mixed", (2, 2, 2, 10, 8), np.float64, np.float32),
+                                 ("eq_c64", shp, np.complex64, np.float32),
+                                 ("bc_c128_pb32", (1, 3, 2, 10, 8), np.complex128, np.float32),
+                                 ("bc_c64_pb64", (2, 1, 1, 10, 8), np.complex64, np.float64)):
+        for mult in (True, False):
+            if np.dtype(dt).kind == "c":
+                sky = _cplx(rng, shp, dt)
+            else:
+                sky = rng.normal(size=shp).astype(dt)
+                sky.reshape(-1)[:3] = [-0.0, np.inf, np.nan]
+            ds = _DS({"SKY": (IMAGE_DIMS, sky),
+                      "MODEL": (IMAGE_DIMS, rng.normal(size=shp).astype(dt)),
+                      "PRIMARY_BEAM": (IMAGE_DIMS, beam(pshape, pdt))}, _coords(shp))
+            record(f"pb_{tag}_{'mul' if mult else 'div'}", ds, list(ds.data_vars),
+                   lambda d: ref.apply_pb(d, multiply=mult))
+    ds = _DS({"RESIDUAL": (IMAGE_DIMS, rng.normal(size=shp))}, _coords(shp))
+    pbds = _DS({"PRIMARY_BEAM": (IMAGE_DIMS, beam(shp, np.float64))}, _coords(shp))
+    out["pb_separate_div/PRIMARY_BEAM/in"] = pbds["PRIMARY_BEAM"].data.copy()
+    record("pb_separate_div", ds, ["RESIDUAL"],
+           lambda d: ref.apply_pb(d, pbds, False, "RESIDUAL"))
+
+    # remove_padding: the centre of odd and even padded sizes
+    for tag, (pl, pm), size in (("even", (16, 12), (10, 7)), ("odd", (15, 13), (8, 9))):
+        shp = (1, 2, 1, pl, pm)
+        ds = _DS({"SKY": (IMAGE_DIMS, rng.normal(size=shp))}, _coords(shp))
+        out[f"pad_{tag}/SKY/in"] = ds["SKY"].data.copy()
+        out[f"pad_{tag}/size"] = np.array(size)
+        out[f"pad_{tag}/SKY/out"] = ref.remove_padding(ds, np.array(size))["SKY"].data.copy()
 
     np.savez_compressed(os.path.join(HERE, "image_prep.npz"), **out)
     return out

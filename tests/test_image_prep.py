@@ -1,10 +1,11 @@
-"""fft_to_uv / ifft_to_lm / correct_fft_to_uv / correct_ifft_to_lm
-(standard_image_grid_preparation.py:312-492).
+"""remove_padding / apply_pb / fft_to_uv / ifft_to_lm / correct_fft_to_uv /
+correct_ifft_to_lm (standard_image_grid_preparation.py:99-492).
 
-CPU: the oracle's restatement of the two normalisations against the
-reference's outputs in tests/golden/image_prep.npz (bit-exact, NaN positions
-compared as positions).  GPU: the drop-in functions on SkyImage datasets
-against the same outputs: the normalisations bit-exact where the reference's
+CPU: the oracle's restatement of the two normalisations and of apply_pb's
+_mult_div against the reference's outputs in tests/golden/image_prep.npz
+(bit-exact, NaN positions compared as positions); remove_padding on a
+SkyImage against the reference's crops.  GPU: the drop-in functions on SkyImage datasets
+against the same outputs: the normalisations and apply_pb bit-exact where the reference's
 inputs are used as they are (with the spheroid correction, to 1e-13
 relative, since the device's grid-correction term is within 1e-14 of the
 reference's; the rescale itself bit-exact against the oracle given the same
@@ -96,6 +97,41 @@ def test_oracle_transforms_match_reference():
     for n, dst in (("VISIBILITY", "SKY"), ("VISIBILITY_RESIDUAL", "RESIDUAL")):
         assert np.array_equal(O.ifft_uv_to_lm(g[f"ifft/{n}/in"], axes=[3, 4]),
                               g[f"ifft/{dst}/out"])
+
+
+def _pb_cases(g):
+    return sorted({k.split("/")[0] for k in g.files
+                   if k.startswith("pb_") and k.endswith("/PRIMARY_BEAM/in")})
+
+
+def test_oracle_apply_pb_matches_reference():
+    g = golden("image_prep.npz")
+    cases = _pb_cases(g)
+    assert len(cases) == 17
+    for case in cases:
+        ins, outs = _vars(g, case, "in"), _vars(g, case, "out")
+        multiply = case.endswith("_mul")
+        for n, x in ins.items():
+            if n == "PRIMARY_BEAM":
+                continue
+            y = x.copy()
+            with np.errstate(all="ignore"):
+                OI.mult_div_planes(y, ins["PRIMARY_BEAM"], multiply)
+            assert same_bits(y, outs[n]), (case, n)
+
+
+def test_remove_padding_matches_reference():
+    from astroviper_b200.core.imaging.imaging_utils.standard_image_grid_preparation import (
+        remove_padding)
+    from astroviper_b200.core.imaging.sky_image import SkyImage
+    g = golden("image_prep.npz")
+    for tag in ("even", "odd"):
+        x = g[f"pad_{tag}/SKY/in"]
+        img = SkyImage({"SKY": x.copy()}, coords={"l": np.arange(x.shape[3]),
+                                                  "m": np.arange(x.shape[4])})
+        out = remove_padding(img, g[f"pad_{tag}/size"])
+        assert np.array_equal(out["SKY"].data, g[f"pad_{tag}/SKY/out"])
+        assert out.sizes["l"] == out.coords["l"].values.size
 
 
 # ----------------------------------------------------------------- GPU ---
@@ -230,3 +266,44 @@ def test_errors_follow_the_reference():
         P.correct_fft_to_uv(img)  # no u / v dims, as image.sizes["u"] fails there
     with pytest.raises(KeyError):
         P.ifft_to_lm(_image({"VISIBILITY": np.zeros((1, 1, 1, 4, 4), complex)}))
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("on_device", [False, True])
+def test_apply_pb_bit_exact(on_device):
+    import torch
+    from astroviper_b200.core.imaging.sky_image import SkyImage
+    P = _prep()
+    g = golden("image_prep.npz")
+    for case in _pb_cases(g):
+        ins, outs = _vars(g, case, "in"), _vars(g, case, "out")
+        multiply = case.endswith("_mul")
+        if case == "pb_separate_div":
+            img = _image({"RESIDUAL": ins["RESIDUAL"]}, to_device=on_device)
+            beam = SkyImage({"PRIMARY_BEAM": ins["PRIMARY_BEAM"].copy()})
+            before = img["RESIDUAL"].data
+            P.apply_pb(img, beam, False, "RESIDUAL")
+            assert img["RESIDUAL"].data is before
+            assert same_bits(_np(img["RESIDUAL"].data), outs["RESIDUAL"]), case
+            continue
+        img = _image(ins, to_device=on_device)
+        before = {n: img[n].data for n in ins}
+        P.apply_pb(img, multiply=multiply)
+        for n in ins:
+            assert img[n].data is before[n]
+            assert same_bits(_np(img[n].data), outs[n]), (case, n, on_device)
+
+
+@pytest.mark.gpu
+def test_apply_pb_errors_follow_the_reference():
+    P = _prep()
+    rng = np.random.default_rng(5)
+    img = _image({"SKY": rng.normal(size=(1, 1, 1, 8, 8))})
+    with pytest.raises(Exception, match="No Primary beam information"):
+        P.apply_pb(img)
+    img = _image({"SKY": rng.normal(size=(1, 1, 1, 8, 8)),
+                  "PRIMARY_BEAM": rng.normal(size=(1, 1, 1, 8, 6))})
+    with pytest.raises(Exception, match="shapes on sky are not the same"):
+        P.apply_pb(img)
+    with pytest.raises(KeyError):
+        P.apply_pb(img, data_vars="RESIDUAL")
