@@ -2,9 +2,9 @@
 beam on B200.
 
 Drop-in for remove_padding, apply_pb, fft_to_uv, ifft_to_lm,
-correct_fft_to_uv and correct_ifft_to_lm of
+correct_fft_to_uv, correct_ifft_to_lm and grid2xradio_spheroid_ms4 of
 src/astroviper/core/imaging/imaging_utils/standard_image_grid_preparation.py
-(:99-492): same arguments, defaults, variable-name rules, exceptions and
+(:99-580): same arguments, defaults, variable-name rules, exceptions and
 in-place updates of the image dataset.  The transforms are this package's
 cuFFT fft_lm_to_uv / ifft_uv_to_lm; the normalisations (av_plane_rescale)
 and the primary-beam product or quotient (av_apply_pb) run in libav200, one
@@ -26,6 +26,8 @@ from .... import _host as H
 from .... import _kernels as K
 from ..fft import fft_lm_to_uv
 from ..ifft import ifft_uv_to_lm
+from .gcf_prolate_spheroidal import create_prolate_spheroidal_kernel_1D
+from .standard_grid import _is_datatree, standard_grid_numpy_wrap_input_checked
 
 _DIV, _MUL, _SPHEROID = 0, 1, 2
 
@@ -167,3 +169,53 @@ def correct_ifft_to_lm(image, data_vars: Union[str, List[str]] = "",
                 raise ValueError(f"{sumwt} has {int(np.prod(norm.shape))} values for "
                                  f"{n_planes} planes of {sky_var}")
             _rescale(x, _SPHEROID, nx * ny, corr, norm)
+
+
+def grid2xradio_spheroid_ms4(vis, image, support: int = 7, sampling: int = 100,
+                             data_var: str = "VISIBILITY", chan_mode: str = "continuum", *,
+                             precision=None):
+    """standard_image_grid_preparation.py:495-580: grids every MSv4 node of
+    vis (one node or a list) into the image's data_var uv grid and its
+    <data_var>_NORMALIZATION sums, in place, for each time plane of the
+    image (as the reference, every node is gridded into every time plane).
+    UV_SAMPLING grids the weights (do_psf).  The cell size is the spacing of
+    the image's l and m coordinates.  As the reference, flagged samples get
+    weight 0 in each node's WEIGHT array.  The gridding is
+    standard_grid_numpy_wrap_input_checked on the device; precision is the
+    package's option ("fp32", the default of config.precision: the tiled
+    FP32 gridder; "fp64": the reference's FP64 arithmetic)."""
+    listvis = [vis] if _is_datatree(vis) else vis
+    nx = image.sizes["u"]
+    ny = image.sizes["v"]
+    dopsf = data_var == "UV_SAMPLING"
+    lc = np.asarray(image.coords["l"].values)
+    mc = np.asarray(image.coords["m"].values)
+    pixelincr = np.array([np.abs(lc[1] - lc[0]), np.abs(mc[1] - mc[0])])
+    if data_var not in image.data_vars:
+        raise Exception(f"{data_var} is not in {image}")
+    sumwt_var = data_var + "_NORMALIZATION"
+    dat_array = image[data_var]
+    sumwt_array = image[sumwt_var]
+    for da in (dat_array, sumwt_array):
+        dims = tuple(getattr(da, "dims", ("time",)))
+        if dims[0] != "time":
+            raise ValueError(f"grid2xradio_spheroid_ms4: time must be the first dim, not {dims}")
+    cgk_1D = create_prolate_spheroidal_kernel_1D(sampling, support)
+    n_time = len(np.atleast_1d(np.asarray(image.coords["time"].values)))
+    for it in range(n_time):
+        gridvis = dat_array.data[it]
+        sumwt = sumwt_array.data[it]
+        for elvis in listvis:
+            if not _is_datatree(elvis):
+                raise TypeError("One of the elements of vis is not an xarray datatree")
+            vis_data = elvis[data_var].data
+            uvw = elvis.UVW.data
+            weight = elvis.WEIGHT.data
+            flag = elvis.FLAG.data
+            weight[flag] = 0.0
+            freq_chan = elvis.coords["frequency"].values
+            gridvis, sumwt = standard_grid_numpy_wrap_input_checked(
+                vis_data, gridvis, sumwt, uvw, weight, freq_chan, cgk_1D,
+                image_size=np.array([nx, ny], dtype=int), cell_size=pixelincr,
+                oversampling=sampling, support=support, complex_grid=True, do_psf=dopsf,
+                chan_mode=chan_mode, precision=precision)

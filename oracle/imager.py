@@ -260,3 +260,23 @@ def mult_div_planes(x, pb, multiply=True):
                     x[t, c, p] /= w
                     x[t, c, p][w == 0] = np.nan
     return x
+
+
+def grid_ms4_into_image(nodes, grid, sumwt, cell, support=7, sampling=100, do_psf=False,
+                        chan_mode="continuum"):
+    """grid2xradio_spheroid_ms4 (standard_image_grid_preparation.py:495-580)
+    on arrays: every node (vis, uvw, weight, flag, freq) gridded with the
+    oracle's standard_grid_jit into each time plane of grid (time, frequency,
+    polarization, u, v) complex128 and sumwt (time, frequency, polarization),
+    in place; flagged weights set to 0 in the nodes' weight arrays."""
+    cgk = O.create_prolate_spheroidal_kernel_1D(sampling, support)
+    nu, nv = grid.shape[-2:]
+    for it in range(grid.shape[0]):
+        for vis, uvw, weight, flag, freq in nodes:
+            weight[flag] = 0.0
+            nchan, npol = weight.shape[2], weight.shape[3]
+            chan_map = (np.arange(nchan) if chan_mode == "cube" else np.zeros(nchan)).astype(int)
+            O.standard_grid_jit(grid[it], sumwt[it], do_psf, False, vis, uvw, freq, chan_map,
+                                np.arange(npol), weight, cgk, np.array([nu, nv]),
+                                np.asarray(cell), support, sampling)
+    return grid, sumwt

@@ -10,8 +10,8 @@ correct_fft_to_uv and correct_ifft_to_lm (standard_image_grid_preparation.py:
 99-492), imported
 unmodified, on a small dataset stand-in (the xarray surface those functions
 use: sizes, data_vars, item get / set, .data, in-place *= and /=, ==,
-coords, .sel and .isel returning views), with stand-in modules for xarray and xradio and for
-standard_grid (imported by name only).  The inputs and the outputs go into
+coords, .sel and .isel returning views), with stand-in modules for xarray and xradio; grid2xradio_spheroid_ms4
+grids duck-typed MSv4 nodes with the reference's own Numba gridder.  The inputs and the outputs go into
 image_prep.npz, keyed <case>/<variable>/{in,out}.
 """
 import os
@@ -26,7 +26,7 @@ SRC = os.path.join(REF, "src", "astroviper")
 os.environ.setdefault("NUMBA_CACHE_DIR", "/tmp/numba_cache_golden")
 sys.path.insert(0, HERE)
 
-from make_golden import _DataArray, _DataTree, _mod, _pkg  # noqa: E402
+from make_golden import MS4Double, _DataArray, _DataTree, _mod, _pkg  # noqa: E402
 
 IMAGE_DIMS = ("time", "frequency", "polarization", "l", "m")
 UV_DIMS = ("time", "frequency", "polarization", "u", "v")
@@ -125,6 +125,12 @@ class _DS:
     def __setitem__(self, name, value):
         self.data_vars[name] = value
 
+    def __getattr__(self, name):
+        coords = self.__dict__.get("coords", {})
+        if name in coords:
+            return _DA(np.asarray(coords[name]), (name,), {})
+        raise AttributeError(name)
+
     def __repr__(self):
         return "<image>"
 
@@ -149,10 +155,8 @@ def load_reference():
     _pkg("astroviper.core", SRC + "/core")
     _pkg("astroviper.core.imaging", SRC + "/core/imaging")
     _pkg("astroviper.core.imaging.imaging_utils", SRC + "/core/imaging/imaging_utils")
-    sg = types.ModuleType("astroviper.core.imaging.imaging_utils.standard_grid")
-    sg.standard_grid_numpy_wrap_input_checked = None
-    sys.modules[sg.__name__] = sg
     iu = SRC + "/core/imaging/imaging_utils/"
+    _mod("astroviper.core.imaging.imaging_utils.standard_grid", iu + "standard_grid.py")
     _mod("astroviper.core.imaging.fft", SRC + "/core/imaging/fft.py")
     _mod("astroviper.core.imaging.ifft", SRC + "/core/imaging/ifft.py")
     _mod("astroviper.core.imaging.imaging_utils.gcf_prolate_spheroidal",
@@ -291,6 +295,37 @@ def run(ref):
         out[f"pad_{tag}/SKY/in"] = ds["SKY"].data.copy()
         out[f"pad_{tag}/size"] = np.array(size)
         out[f"pad_{tag}/SKY/out"] = ref.remove_padding(ds, np.array(size))["SKY"].data.copy()
+
+    # grid2xradio_spheroid_ms4: two MSv4 nodes into two time planes, the
+    # visibilities in continuum mode and the weights (UV_SAMPLING) as a cube
+    for tag, data_var, chan_mode in (("vis", "VISIBILITY", "continuum"),
+                                     ("psf", "UV_SAMPLING", "cube")):
+        nodes = []
+        nchan, npol, nt, nb = 3, 2, 4, 15
+        freq = 1.0e9 + np.arange(nchan) * 2.0e7
+        for k in range(2):
+            uvw = rng.uniform(-900.0, 900.0, (nt, nb, 3))
+            vis = rng.normal(size=(nt, nb, nchan, npol)) + 1j * rng.normal(size=(nt, nb, nchan, npol))
+            weight = rng.uniform(0.5, 2.0, (nt, nb, nchan, npol))
+            flag = rng.uniform(size=(nt, nb, nchan, npol)) < 0.1
+            node = MS4Double(vis, uvw, weight, flag, freq)
+            node._d["UV_SAMPLING"] = node._d["VISIBILITY"]
+            nodes.append(node)
+            for n, a in (("vis", vis), ("uvw", uvw), ("weight", weight), ("flag", flag)):
+                out[f"ms4_{tag}/node{k}/{n}"] = a.copy()
+            out[f"ms4_{tag}/freq"] = freq
+        n_img_chan = nchan if chan_mode == "cube" else 1
+        shp = (2, n_img_chan, npol, 64, 48)
+        coords = _coords(shp)
+        coords["l"] = (np.arange(64) - 32) * -2.0e-5
+        coords["m"] = (np.arange(48) - 24) * 2.4e-5
+        ds = _DS({data_var: (UV_DIMS, np.zeros(shp, complex)),
+                  data_var + "_NORMALIZATION": (UV_DIMS[:3], np.zeros(shp[:3]))}, coords)
+        ref.grid2xradio_spheroid_ms4(nodes, ds, data_var=data_var, chan_mode=chan_mode)
+        out[f"ms4_{tag}/grid"] = ds[data_var].data.copy()
+        out[f"ms4_{tag}/sumwt"] = ds[data_var + "_NORMALIZATION"].data.copy()
+        for k, node in enumerate(nodes):
+            out[f"ms4_{tag}/node{k}/weight_after"] = node.WEIGHT.data.copy()
 
     np.savez_compressed(os.path.join(HERE, "image_prep.npz"), **out)
     return out
