@@ -1,17 +1,21 @@
 """The image <-> uv-grid transforms, their normalisations and the primary
 beam on B200.
 
-Drop-in for remove_padding, apply_pb, fft_to_uv, ifft_to_lm,
-correct_fft_to_uv, correct_ifft_to_lm and grid2xradio_spheroid_ms4 of
+Drop-in for make_image_xds, remove_padding, make_empty_padded_uv_image,
+apply_pb, fft_to_uv, ifft_to_lm, correct_fft_to_uv, correct_ifft_to_lm and
+grid2xradio_spheroid_ms4 of
 src/astroviper/core/imaging/imaging_utils/standard_image_grid_preparation.py
-(:99-580): same arguments, defaults, variable-name rules, exceptions and
+(:19-580): same arguments, defaults, variable-name rules, exceptions and
 in-place updates of the image dataset.  The transforms are this package's
 cuFFT fft_lm_to_uv / ifft_uv_to_lm; the normalisations (av_plane_rescale)
 and the primary-beam product or quotient (av_apply_pb) run in libav200, one
 launch per variable, in numpy's arithmetic for the reference's in-place
 updates, so their results are bit-identical to the reference's for the same
 inputs.  The dataset constructors of the same file (make_image_xds,
-make_empty_padded_uv_image) build xradio images and are not provided.
+make_empty_padded_uv_image) build SkyImage datasets here, since xradio is
+not a dependency: the same variables, dims, dtypes, sizes and data_groups,
+with (l, m) coordinates as make_sky_image and (u, v) ones as
+sky_image.make_uv_coords.
 
 The image may be a SkyImage (its variables numpy arrays or device tensors) or
 an xarray Dataset.  numpy variables are updated in place in their own
@@ -26,6 +30,7 @@ from .... import _host as H
 from .... import _kernels as K
 from ..fft import fft_lm_to_uv
 from ..ifft import ifft_uv_to_lm
+from ..sky_image import _Var, make_sky_image, make_uv_coords
 from .gcf_prolate_spheroidal import create_prolate_spheroidal_kernel_1D
 from .standard_grid import _is_datatree, standard_grid_numpy_wrap_input_checked
 
@@ -48,6 +53,83 @@ def _rescale(x, mode, s, corr=None, w=None):
     K.plane_rescale(t, mode, s, corr, w)
     H.write_back(x, t)
     return x
+
+
+def make_image_xds(imsize, cell, freq, freqinc, phasecent, which: str = "SKY", pol=None,
+                   time=None):
+    """standard_image_grid_preparation.py:19-96: an empty sky image with
+    one float32 zero variable `which` (time, frequency, polarization, l, m);
+    pol defaults to ["I"], time to [0.0]; freqinc, when given, is kept as the
+    frequency coordinate's channel_width attribute."""
+    if pol is None:
+        pol = np.array(["I"])
+    if time is None:
+        time = np.array([0.0])
+    freq_coords = np.atleast_1d(np.asarray(freq, dtype=float))
+    image = make_sky_image(phasecent, imsize, cell, freq_coords, pol, time)
+    if freqinc is not None:
+        image.coords["frequency"].attrs["channel_width"] = {"data": freqinc, "units": "Hz"}
+    shape = (len(np.atleast_1d(time)), len(freq_coords), len(pol), int(imsize[0]),
+             int(imsize[1]))
+    image[which] = np.zeros(shape, dtype=np.float32)
+    image.attrs.setdefault("data_groups", {"base": {}})["base"][which.lower()] = which
+    return image
+
+
+def _phase_center(image):
+    attrs = getattr(image, "attrs", {})
+    if "phase_center" in attrs:
+        return attrs["phase_center"]
+    return image.coordinate_system_info["reference_direction"]["data"]
+
+
+def make_empty_padded_uv_image(image, image_size, uv_data_array: str = "VISIBILITY_RESIDUAL",
+                               insert_res_or_mod=True):
+    """standard_image_grid_preparation.py:123-233: an empty uv image of
+    image_size (u, v) cells for the image's time / frequency / polarization
+    coordinates and cell size: uv_data_array complex64 zeros (time,
+    frequency, polarization, u, v) and <uv_data_array>_NORMALIZATION float64
+    zeros (time, frequency, polarization), both named in
+    attrs["data_groups"]["base"]; with insert_res_or_mod, RESIDUAL (for
+    VISIBILITY_RESIDUAL) or MODEL (for VISIBILITY_MODEL) of the image, when
+    present, is copied as float32 into the centre of a zero (l, m) plane of
+    image_size.  Raises when the image is larger than image_size."""
+    image_size = np.array(image_size)
+    image_size_current = np.array([image.sizes["l"], image.sizes["m"]])
+    if np.any(image_size_current > image_size):
+        raise Exception(
+            f"current image size {image_size_current} is larger than requested {image_size}")
+    lc = np.asarray(image.coords["l"].values)
+    mc = np.asarray(image.coords["m"].values)
+    cellsize = np.array([np.abs(lc[1] - lc[0]), np.abs(mc[1] - mc[0])])
+    freq = np.asarray(image.coords["frequency"].values)
+    pol = np.asarray(image.coords["polarization"].values)
+    tim = np.asarray(image.coords["time"].values)
+    out_im = make_sky_image(_phase_center(image), image_size, cellsize, freq, pol, tim)
+    for name, values in make_uv_coords(image_size, cellsize).items():
+        out_im.coords[name] = _Var(values, (name,))
+    groups = out_im.attrs.setdefault("data_groups", {"base": {}})["base"]
+    shape = (len(tim), len(freq), len(pol), int(image_size[0]), int(image_size[1]))
+    out_im[uv_data_array] = (("time", "frequency", "polarization", "u", "v"),
+                             np.zeros(shape, dtype=np.complex64))
+    out_im[uv_data_array + "_NORMALIZATION"] = (("time", "frequency", "polarization"),
+                                                np.zeros(shape[:3], dtype=np.float64))
+    groups[uv_data_array.lower()] = uv_data_array
+    groups[uv_data_array.lower() + "_normalization"] = uv_data_array + "_NORMALIZATION"
+    if insert_res_or_mod:
+        dat_name = {"VISIBILITY_MODEL": "MODEL",
+                    "VISIBILITY_RESIDUAL": "RESIDUAL"}.get(uv_data_array, "")
+        if dat_name and dat_name in image.data_vars:
+            dat = image[dat_name].values
+            if H.is_torch(dat):
+                dat = dat.detach().cpu().numpy()
+            blc = (image_size - np.array(dat.shape[-2:])) // 2
+            trc = blc + np.array(dat.shape[-2:])
+            plane = np.zeros(shape, dtype=np.float32)
+            plane[:, :, :, blc[0]:trc[0], blc[1]:trc[1]] = dat
+            out_im[dat_name] = plane
+            groups[dat_name.lower()] = dat_name
+    return out_im
 
 
 def remove_padding(image, image_size):

@@ -17,9 +17,10 @@ DIMS = ("time", "frequency", "polarization", "l", "m")
 class _Var:
     """A data variable or coordinate: .values / .data and .dims."""
 
-    def __init__(self, values, dims):
+    def __init__(self, values, dims, attrs=None):
         self.values = values
         self.dims = tuple(dims)
+        self.attrs = dict(attrs or {})
 
     @property
     def data(self):
@@ -68,6 +69,10 @@ class SkyImage:
             out = {}
             for v in self._vars.values():
                 out.update(zip(v.dims, (int(s) for s in v.values.shape)))
+            # dimension coordinates of dims no variable uses, as xarray lists them
+            for name, c in self._coords.items():
+                if c.dims == (name,) and name not in out:
+                    out[name] = len(c)
             return out
         return {d: len(self._coords[d]) for d in DIMS if d in self._coords}
 
@@ -111,7 +116,7 @@ class SkyImage:
 
     def copy(self, deep=True):
         out = SkyImage(attrs=self.attrs)
-        out._coords = {k: _Var(_copy(c.values) if deep else c.values, c.dims)
+        out._coords = {k: _Var(_copy(c.values) if deep else c.values, c.dims, c.attrs)
                        for k, c in self._coords.items()}
         out._vars = {k: _Var(_copy(v.values) if deep else v.values, v.dims)
                      for k, v in self._vars.items()}
@@ -129,7 +134,7 @@ class SkyImage:
 
         def cut(v):
             idx = tuple(indexers.get(d, slice(None)) for d in v.dims)
-            return _Var(v.values[idx], v.dims)
+            return _Var(v.values[idx], v.dims, v.attrs)
 
         out = SkyImage(attrs=self.attrs)
         out._coords = {k: cut(c) for k, c in self._coords.items()}
@@ -161,3 +166,14 @@ def make_sky_image(phase_center, image_size, cell_size, frequency_coords, pol_co
     }
     return SkyImage(coords=coords, attrs={"phase_center": tuple(phase_center),
                                           "cell_size": tuple(float(c) for c in cell)})
+
+
+def make_uv_coords(image_size, cell_size):
+    """u / v coordinates of the uv grid paired by the FFT with an (l, m)
+    image of image_size pixels of cell_size radians: spacing
+    1 / (n * cell) wavelengths, 0 at pixel n // 2."""
+    out = {}
+    for name, n, c in (("u", int(image_size[0]), float(cell_size[0])),
+                       ("v", int(image_size[1]), float(cell_size[1]))):
+        out[name] = (np.arange(n) - n // 2) / (n * abs(c))
+    return out

@@ -159,6 +159,74 @@ def test_oracle_grid2xradio_spheroid_ms4_matches_reference():
             assert np.array_equal(node[2], g[f"ms4_{tag}/node{k}/weight_after"])
 
 
+def _ref_test_image(npol=1, nchan=1, which="SKY", fill=1.0):
+    """The image of the reference's own tests of this module
+    (test_standard_image_grid_preparation.py:17-65): 200 x 200 pixels of
+    4.8e-6 rad, frequencies 1e9 + k 1e8, pols from RR LL LR RL, one epoch,
+    the variable `which` float32 ones."""
+    from astroviper_b200.core.imaging.imaging_utils.standard_image_grid_preparation import (
+        make_image_xds)
+    freq = np.arange(1, nchan + 1) * 1e8 + 1e9
+    pol = np.array(["RR", "LL", "LR", "RL"])[:npol]
+    a = make_image_xds([200, 200], [4.8e-6, 4.8e-6], freq, None, [1.0, 0.0], which=which,
+                       pol=pol, time=[5.7e4])
+    a[which].data[...] = fill
+    return a
+
+
+def test_make_image_xds_layout():
+    from astroviper_b200.core.imaging.imaging_utils.standard_image_grid_preparation import (
+        make_image_xds)
+    a = make_image_xds([30, 20], [1e-5, 2e-5], 1.4e9, 1e6, [0.5, -0.3], which="MODEL")
+    assert a.sizes == {"time": 1, "frequency": 1, "polarization": 1, "l": 30, "m": 20}
+    assert a["MODEL"].data.dtype == np.float32 and not a["MODEL"].data.any()
+    assert list(a.coords["polarization"].values) == ["I"]
+    assert list(a.coords["time"].values) == [0.0]
+    assert a.coords["frequency"].attrs["channel_width"] == {"data": 1e6, "units": "Hz"}
+    assert np.isclose(abs(a.coords["l"].values[1] - a.coords["l"].values[0]), 1e-5)
+    assert np.isclose(abs(a.coords["m"].values[1] - a.coords["m"].values[0]), 2e-5)
+    b = make_image_xds([8, 8], [1e-5, 1e-5], [1e9, 2e9], None, [0, 0],
+                       pol=["XX", "YY"], time=[1.0, 2.0, 3.0])
+    assert b["SKY"].shape == (3, 2, 2, 8, 8)
+    assert "channel_width" not in b.coords["frequency"].attrs
+
+
+def test_make_empty_padded_uv_image_as_reference_test():
+    """test_standard_image_grid_preparation.py:82-95, plus the copy of the
+    residual into the centre and the size check."""
+    from astroviper_b200.core.imaging.imaging_utils.standard_image_grid_preparation import (
+        make_empty_padded_uv_image)
+    a = _ref_test_image(which="RESIDUAL")
+    a["RESIDUAL"].data[0, 0, 0, 3, 5] = 7.0
+    b = make_empty_padded_uv_image(a, [250, 250], "VISIBILITY_RESIDUAL")
+    assert b.sizes["u"] == 250
+    assert "residual" in b.attrs["data_groups"]["base"]
+    assert b["VISIBILITY_RESIDUAL"].shape[3] == 250
+    assert b["VISIBILITY_RESIDUAL"].data.dtype == np.complex64
+    assert b["VISIBILITY_RESIDUAL_NORMALIZATION"].shape == (1, 1, 1)
+    r = b["RESIDUAL"].data
+    assert r.shape == (1, 1, 1, 250, 250) and r.dtype == np.float32
+    assert r[0, 0, 0, 25 + 3, 25 + 5] == 7.0 and r.sum() == 200 * 200 - 1 + 7.0
+    assert b.coords["u"].values[125] == 0.0 and b.coords["v"].values[125] == 0.0
+    c = make_empty_padded_uv_image(a, [250, 250], "VISIBILITY_MODEL")
+    assert "MODEL" not in c.data_vars and "RESIDUAL" not in c.data_vars
+    with pytest.raises(Exception, match="is larger than requested"):
+        make_empty_padded_uv_image(a, [150, 250])
+
+
+def test_remove_padding_as_reference_test():
+    """test_standard_image_grid_preparation.py:67-80 on the l / m
+    coordinates: pixel (99, 99) of 200 x 200 is pixel (89, 89) of the
+    180 x 180 centre."""
+    from astroviper_b200.core.imaging.imaging_utils.standard_image_grid_preparation import (
+        remove_padding)
+    a = _ref_test_image()
+    lo, mo = a.coords["l"].values[99], a.coords["m"].values[99]
+    b = remove_padding(a, [180, 180])
+    assert b.coords["l"].values[89] == lo and b.coords["m"].values[89] == mo
+    assert b["SKY"].shape == (1, 1, 1, 180, 180)
+
+
 # ----------------------------------------------------------------- GPU ---
 def _prep():
     from astroviper_b200.core.imaging.imaging_utils import standard_image_grid_preparation as P
@@ -384,3 +452,35 @@ def test_grid2xradio_spheroid_ms4_matches_reference(on_device, precision, tol):
     with pytest.raises(TypeError, match="not an xarray datatree"):
         P.grid2xradio_spheroid_ms4([nodes[0], object()], img, data_var="UV_SAMPLING",
                                    chan_mode="cube")
+
+
+@pytest.mark.gpu
+def test_reference_unit_tests_known_answers():
+    """The known answers of test_standard_image_grid_preparation.py:97-148
+    (_mult_div, apply_pb, fft_to_uv + correct_fft_to_uv, ifft_to_lm).  The
+    FFT values are compared to 1e-6 relative (the reference asserts numpy's
+    exact values; cuFFT rounds differently)."""
+    P = _prep()
+    for via_apply in (False, True):
+        a = _ref_test_image(npol=1, nchan=2)
+        a["PRIMARY_BEAM"] = np.ones(a["SKY"].shape, dtype=np.float32)
+        a["PRIMARY_BEAM"].data[0, 1, 0, :, :] = 0
+        if via_apply:
+            P.apply_pb(a, data_vars="SKY", multiply=True)
+        else:
+            P._mult_div(a["SKY"], a["PRIMARY_BEAM"], multiply=True)
+        assert np.max(a["SKY"].data[0, 0, 0, :, :]) == 1.0
+        assert np.max(a["SKY"].data[0, 1, 0, :, :]) == 0.0
+    a = _ref_test_image(which="RESIDUAL")
+    b = P.make_empty_padded_uv_image(a, image_size=[200, 200])
+    P.fft_to_uv(b)
+    vis = b["VISIBILITY_RESIDUAL"].data
+    assert abs(vis[0, 0, 0, 100, 100] - 200 * 200) <= 1e-6 * 200 * 200
+    P.correct_fft_to_uv(b)
+    vis = b["VISIBILITY_RESIDUAL"].data
+    assert abs(vis[0, 0, 0, 100, 100] - 1.0) <= 1e-6
+    assert abs(vis[0, 0, 0, 99, 99]) <= 1e-6
+    b = P.make_empty_padded_uv_image(a, image_size=[200, 200])
+    b["VISIBILITY_RESIDUAL"].data[0, 0, 0, 100, 100] = 10
+    P.ifft_to_lm(b)
+    assert abs(float(np.max(b["RESIDUAL"].data)) - 10.0 / 200.0 / 200.0) <= 1e-6 * 2.5e-4
