@@ -120,6 +120,12 @@ def test_module_layout_mirrors_reference():
         "astroviper_b200.core.imaging.deconvolution": ["hogbom_clean", "progress_callback"],
         "astroviper_b200.core.imaging.fft": ["fft_lm_to_uv"],
         "astroviper_b200.core.imaging.ifft": ["ifft_uv_to_lm"],
+        "astroviper_b200.core.imaging.imaging_utils.standard_image_grid_preparation": [
+            "make_image_xds", "remove_padding", "make_empty_padded_uv_image", "apply_pb",
+            "_mult_div", "fft_to_uv", "ifft_to_lm", "correct_fft_to_uv", "correct_ifft_to_lm",
+            "grid2xradio_spheroid_ms4"],
+        "astroviper_b200.core.imaging.imaging_utils.make_primary_beam": [
+            "cube_single_field_primary_beam"],
     }.items():
         m = importlib.import_module(mod)
         for n in names:
@@ -152,6 +158,11 @@ def test_product_path_refuses_to_run_without_gpu():
         create_prolate_spheroidal_kernel_1D
     with pytest.raises(RuntimeError, match="needs a CUDA device"):
         create_prolate_spheroidal_kernel_1D(100, 7)
+    from astroviper_b200.core.imaging.imaging_utils.standard_image_grid_preparation import (
+        correct_ifft_to_lm, make_image_xds)
+    img = make_image_xds([8, 8], [1e-5, 1e-5], 1e9, None, [0.0, 0.0])
+    with pytest.raises(RuntimeError, match="needs a CUDA device"):
+        correct_ifft_to_lm(img)
 
 
 def test_stream_time_chunks_cover_every_step_once():
