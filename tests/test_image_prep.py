@@ -140,8 +140,8 @@ def _ms4_nodes(g, tag):
             + (g[f"ms4_{tag}/freq"],) for k in range(2)]
 
 
-def _ms4_cell(shape):
-    return np.array([2.0e-5, 2.4e-5])
+# the cell of the grid2xradio_spheroid_ms4 fixtures: the spacing of their l / m coordinates
+MS4_CELL = np.array([2.0e-5, 2.4e-5])
 
 
 def test_oracle_grid2xradio_spheroid_ms4_matches_reference():
@@ -151,7 +151,7 @@ def test_oracle_grid2xradio_spheroid_ms4_matches_reference():
         grid = np.zeros(ref.shape, complex)
         sumwt = np.zeros(ref.shape[:3])
         nodes = _ms4_nodes(g, tag)
-        OI.grid_ms4_into_image(nodes, grid, sumwt, _ms4_cell(ref.shape), do_psf=psf,
+        OI.grid_ms4_into_image(nodes, grid, sumwt, MS4_CELL, do_psf=psf,
                                chan_mode=mode)
         assert np.max(np.abs(grid - ref)) <= 1e-12 * np.max(np.abs(ref)), tag
         assert np.allclose(sumwt, g[f"ms4_{tag}/sumwt"], rtol=1e-13, atol=0), tag
@@ -364,7 +364,6 @@ def test_errors_follow_the_reference():
 @pytest.mark.gpu
 @pytest.mark.parametrize("on_device", [False, True])
 def test_apply_pb_bit_exact(on_device):
-    import torch
     from astroviper_b200.core.imaging.sky_image import SkyImage
     P = _prep()
     g = golden("image_prep.npz")
@@ -435,8 +434,8 @@ def test_grid2xradio_spheroid_ms4_matches_reference(on_device, precision, tol):
         sumwt = np.zeros(ref.shape[:3])
         if on_device:
             grid, sumwt = torch.from_numpy(grid).cuda(), torch.from_numpy(sumwt).cuda()
-        img = SkyImage(coords={"time": [5.0, 15.0], "l": (np.arange(64) - 32) * -2.0e-5,
-                               "m": (np.arange(48) - 24) * 2.4e-5})
+        img = SkyImage(coords={"time": [5.0, 15.0], "l": (np.arange(64) - 32) * -MS4_CELL[0],
+                               "m": (np.arange(48) - 24) * MS4_CELL[1]})
         img[data_var] = (UV_DIMS, grid)
         img[data_var + "_NORMALIZATION"] = sumwt
         P.grid2xradio_spheroid_ms4(nodes, img, data_var=data_var, chan_mode=mode,
