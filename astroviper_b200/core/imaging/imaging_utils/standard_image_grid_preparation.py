@@ -12,9 +12,9 @@ and the primary-beam product or quotient (av_apply_pb) run in libav200, one
 launch per variable, in numpy's arithmetic for the reference's in-place
 updates, so their results are bit-identical to the reference's for the same
 inputs; the spheroid correction agrees to the 1e-14 relative of the device's
-grid-correction term, and the transforms to cuFFT's rounding.  The dataset constructors of the same file (make_image_xds,
-make_empty_padded_uv_image) build SkyImage datasets here, since xradio is
-not a dependency: the same variables, dims, dtypes, sizes and data_groups,
+grid-correction term, and the transforms to cuFFT's rounding.  The dataset
+constructors of the same file (make_image_xds, make_empty_padded_uv_image)
+build SkyImage datasets here, since xradio is not a dependency: the same variables, dims, dtypes, sizes and data_groups,
 with (l, m) coordinates as make_sky_image and (u, v) ones as
 sky_image.make_uv_coords.
 

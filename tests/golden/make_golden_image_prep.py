@@ -6,13 +6,14 @@ Run in a container that has the astroviper source tree (default
     python tests/golden/make_golden_image_prep.py
 
 Runs the reference's remove_padding, apply_pb, fft_to_uv, ifft_to_lm,
-correct_fft_to_uv and correct_ifft_to_lm (standard_image_grid_preparation.py:
-99-492), imported
-unmodified, on a small dataset stand-in (the xarray surface those functions
-use: sizes, data_vars, item get / set, .data, in-place *= and /=, ==,
-coords, .sel and .isel returning views), with stand-in modules for xarray and xradio; grid2xradio_spheroid_ms4
-grids duck-typed MSv4 nodes with the reference's own Numba gridder.  The inputs and the outputs go into
-image_prep.npz, keyed <case>/<variable>/{in,out}.
+correct_fft_to_uv, correct_ifft_to_lm and grid2xradio_spheroid_ms4
+(standard_image_grid_preparation.py:99-580), imported unmodified, on a small
+dataset stand-in (the xarray surface those functions use: sizes, data_vars,
+item get / set, .data, in-place *= and /=, ==, coords, .sel and .isel
+returning views), with stand-in modules for xarray and xradio;
+grid2xradio_spheroid_ms4 grids duck-typed MSv4 nodes with the reference's
+own Numba gridder.  The inputs and the outputs go into image_prep.npz, keyed
+<case>/<variable>/{in,out}.
 """
 import os
 import sys
@@ -305,7 +306,8 @@ def run(ref):
         freq = 1.0e9 + np.arange(nchan) * 2.0e7
         for k in range(2):
             uvw = rng.uniform(-900.0, 900.0, (nt, nb, 3))
-            vis = rng.normal(size=(nt, nb, nchan, npol)) + 1j * rng.normal(size=(nt, nb, nchan, npol))
+            shape = (nt, nb, nchan, npol)
+            vis = rng.normal(size=shape) + 1j * rng.normal(size=shape)
             weight = rng.uniform(0.5, 2.0, (nt, nb, nchan, npol))
             flag = rng.uniform(size=(nt, nb, nchan, npol)) < 0.1
             node = MS4Double(vis, uvw, weight, flag, freq)
