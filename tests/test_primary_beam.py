@@ -45,6 +45,9 @@ def test_validation_follows_the_reference():
             M.cube_single_field_primary_beam(_params(**{key: (1.0,)}), "ALMA")
     with pytest.raises(ValueError, match="Unsupported telescope"):
         M.cube_single_field_primary_beam(_params(), telescope="VLA")
+    # the parameters are checked before the telescope, as in the reference
+    with pytest.raises(ValueError, match="'image_size' must be a 2D tuple"):
+        M.cube_single_field_primary_beam(_params(image_size=[64, 64]), telescope="VLA")
 
 
 @pytest.mark.gpu
