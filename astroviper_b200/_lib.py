@@ -14,7 +14,8 @@ AV_OK, AV_ERR_ARG, AV_ERR_CUDA, AV_ERR_TIMEOUT, AV_ERR_NAN, AV_ERR_UNSUPPORTED, 
     range(7)
 AV_F32, AV_F64, AV_C64, AV_C128 = range(4)
 AV_TUNE_GRID_CHUNKS_PER_SM, AV_TUNE_DEGRID_CHUNKS_PER_SM, AV_TUNE_GRID_LANES, \
-    AV_TUNE_DEGRID_LANES = range(4)
+    AV_TUNE_DEGRID_LANES, AV_TUNE_HOGBOM_BARRIER_TIMEOUT_US = range(5)
+AV_HOGBOM_BARRIER_TIMEOUT_US_DEFAULT = 2000000
 AV_GRID_LANES_MMA, AV_GRID_LANES_ROWS, AV_GRID_LANES_AUTO = 1, 2, 3
 AV_DEGRID_LANES_TF32, AV_DEGRID_LANES_FP32, AV_DEGRID_LANES_AUTO = 1, 2, 3
 

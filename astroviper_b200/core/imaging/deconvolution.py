@@ -40,35 +40,30 @@ def get_phase_center(dirty_image_xds):
     return f"{float(pc[0])},{float(pc[1])}"
 
 
+# Hogbom parameters: (name, default, test a given value passes, message when
+# it fails).  Names, defaults, tests and messages are the reference's
+# (deconvolution.py:86-118): callers and tests match on the messages.
+_HOGBOM_PARAMS = (
+    ("gain", 0.1, lambda v: 0 < v <= 1, "CLEAN gain must be between 0 and 1."),
+    ("niter", 1000, lambda v: isinstance(v, int) and v > 0,
+     "Maximum number of iterations must be a positive integer."),
+    ("threshold", 0.0, lambda v: v is None or not v < 0,
+     "Threshold must be non-negative or None."),
+    ("clean_box", (-1, -1, -1, -1), lambda v: v is None or (isinstance(v, tuple) and len(v) == 4),
+     "Clean box must be a 4-tuple (xmin, xmax, ymin, ymax) or None."),
+)
+
+
 def _validate_deconv_params(deconv_params):
-    """deconvolution.py:74-120: fills defaults and checks gain, niter,
-    threshold and clean_box (same ValueError messages)."""
-    default_params = {
-        "gain": 0.1,
-        "niter": 1000,
-        "threshold": 0.0,
-        "clean_box": (-1, -1, -1, -1),
-    }
-    for key, default_value in default_params.items():
-        if key not in deconv_params:
-            logger.info(
-                f"Deconvolution parameter '{key}' not specified. Using default: {default_value}")
-            deconv_params[key] = default_value
-        else:
-            if key == "gain":
-                if not (0 < deconv_params[key] <= 1):
-                    raise ValueError("CLEAN gain must be between 0 and 1.")
-            elif key == "niter":
-                if not (isinstance(deconv_params[key], int) and deconv_params[key] > 0):
-                    raise ValueError("Maximum number of iterations must be a positive integer.")
-            elif key == "threshold":
-                if deconv_params[key] is not None and deconv_params[key] < 0:
-                    raise ValueError("Threshold must be non-negative or None.")
-            elif key == "clean_box":
-                if deconv_params[key] is not None and not (
-                        isinstance(deconv_params[key], tuple) and len(deconv_params[key]) == 4):
-                    raise ValueError(
-                        "Clean box must be a 4-tuple (xmin, xmax, ymin, ymax) or None.")
+    """Checks the given Hogbom parameters in table order and fills in the
+    missing ones, in place (deconvolution.py:74-120): the first failing value
+    raises ValueError; a missing one is logged and set to its default."""
+    for name, default, passes, message in _HOGBOM_PARAMS:
+        if name not in deconv_params:
+            logger.info(f"Deconvolution parameter '{name}' not specified. Using default: {default}")
+            deconv_params[name] = default
+        elif not passes(deconv_params[name]):
+            raise ValueError(message)
     return deconv_params
 
 
@@ -78,41 +73,30 @@ def _is_plane(a):
 
 def hogbom_clean(dirty_image: np.ndarray, psf: np.ndarray, deconv_params: Optional[dict] = None,
                  output_dir: str = ".", *, progress=True):
-    """deconvolution.py:332-426: returns (stats dict, model, residual) for one
-    2-D plane (numpy arrays, or device tensors that the results stay beside).
-    progress=False leaves out the logging callback; the arithmetic, and so
-    every result, is the same with and without it."""
-    deconv_params = _validate_deconv_params(deconv_params)
-    if not _is_plane(dirty_image):
-        raise ValueError("dirty_image must be a 2D numpy array with shape (ny, nx)")
-    if not _is_plane(psf):
-        raise ValueError("psf must be a 2D numpy array with shape (ny, nx)")
+    """One plane of Hogbom CLEAN (deconvolution.py:332-426): returns the
+    result statistics (iterations_performed, final_peak, total_flux_cleaned,
+    converged), the model and the residual.
+
+    dirty_image and psf are 2-D arrays of one shape (numpy arrays, or device
+    tensors, which the results then stay beside); deconv_params is checked
+    and completed in place.  The CLEAN runs in FP32, as the reference's call
+    selects it with an empty float32 mask.  progress=False leaves out the
+    logging callback; the arithmetic, and so every result, is the same."""
+    params = _validate_deconv_params(deconv_params)
+    for name, plane in (("dirty_image", dirty_image), ("psf", psf)):
+        if not _is_plane(plane):
+            raise ValueError(f"{name} must be a 2D numpy array with shape (ny, nx)")
     if tuple(dirty_image.shape) != tuple(psf.shape):
         raise ValueError(
             f"dirty_image and psf must have same shape. Got {dirty_image.shape} and {psf.shape}")
-    logger.debug(f"Dirty image shape: {dirty_image.shape}")
-    logger.debug(f"PSF shape: {psf.shape}")
-    fmin, fmax = hogbom.maximg(dirty_image)
-    initial_peak = max(abs(fmin), abs(fmax))
-    logger.debug(f"Initial peak flux: {initial_peak:.6f}")
-    logger.info("\nRunning Hogbom CLEAN algorithm...")
-    results = hogbom.clean(
-        dirty_image=dirty_image,
-        psf=psf,
-        mask=np.array([], dtype=np.float32),
-        gain=deconv_params["gain"],
-        threshold=deconv_params["threshold"],
-        max_iter=deconv_params["niter"],
-        clean_box=(deconv_params["clean_box"] if deconv_params["clean_box"]
-                   else (-1, -1, -1, -1)),
-        progress_callback=progress_callback if progress else None,
-        stop_callback=None,
-    )
-    model_array = results["model_image"]
-    residual_array = results["residual_image"]
-    final_results = {k: v for k, v in results.items()
-                     if k not in ["model_image", "residual_image"]}
-    return final_results, model_array, residual_array
+    stats = hogbom.clean(dirty_image, psf, mask=np.array([], dtype=np.float32),
+                         clean_box=params["clean_box"] or (-1, -1, -1, -1),
+                         max_iter=params["niter"], gain=params["gain"],
+                         threshold=params["threshold"],
+                         progress_callback=progress_callback if progress else None)
+    model = stats.pop("model_image")
+    residual = stats.pop("residual_image")
+    return stats, model, residual
 
 
 # ---------------------------------------------------------------- deconvolve --

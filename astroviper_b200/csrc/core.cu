@@ -102,9 +102,9 @@ __global__ void k_pswf_kernel4d(double *out, int os, int support, int n_os) {
 }
 
 // ------------------------------------------------------------ tuning ---
-constexpr int kTuneKnobs = 4;
+constexpr int kTuneKnobs = 5;
 static std::atomic<int64_t> g_tune[kTuneKnobs] = {
-    {16}, {16}, {AV_GRID_LANES_AUTO}, {AV_DEGRID_LANES_AUTO}};
+    {16}, {16}, {AV_GRID_LANES_AUTO}, {AV_DEGRID_LANES_AUTO}, {2000000}};
 
 int64_t tune_value(int knob) {
   return (knob >= 0 && knob < kTuneKnobs) ? g_tune[knob].load() : 0;
@@ -192,6 +192,13 @@ unsigned long long av_launch_count(void) { return g_launches.load(); }
 int av_tune_set(int knob, int64_t value) {
   clear_error();
   AV_CHECK_ARG(knob >= 0 && knob < kTuneKnobs, "av_tune_set: unknown knob %d", knob);
+  if (knob == AV_TUNE_HOGBOM_BARRIER_TIMEOUT_US) {
+    AV_CHECK_ARG(value >= 0 && value <= 600000000,
+                 "av_tune_set: AV_TUNE_HOGBOM_BARRIER_TIMEOUT_US %lld outside [0, 600000000]",
+                 (long long)value);
+    g_tune[knob].store(value);
+    return AV_OK;
+  }
   AV_CHECK_ARG(value >= 1 && value <= 1024, "av_tune_set: value %lld outside [1, 1024]",
                (long long)value);
   AV_CHECK_ARG(knob != AV_TUNE_GRID_LANES || value <= 3,

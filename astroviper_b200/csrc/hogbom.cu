@@ -63,6 +63,7 @@ struct HogArgs {
   HogCand<T> *cand;  // 2 x gridDim.x
   int init;
   int resident;
+  unsigned long long timeout_ns;  // bounded wait at the grid barrier
 };
 
 __device__ __forceinline__ float rn_mul(float a, float b) { return __fmul_rn(a, b); }
@@ -82,10 +83,14 @@ __device__ __forceinline__ bool beats(T aa, int ai, T ba, int bi) {
   return aa > ba || (aa == ba && ai < bi);
 }
 
-// Grid barrier with a bounded wait (~2 s of wall time); returns false on
-// timeout and records it in the state.
+// Grid barrier with a bounded wait (timeout_ns of wall time, 2 s unless the
+// AV_TUNE_HOGBOM_BARRIER_TIMEOUT_US knob says otherwise); returns false on
+// timeout and records it in the state.  Every CTA adds itself to the count
+// exactly once per barrier, timed out or not, so the last one to arrive still
+// releases the barrier and no CTA waits beyond its own bound.
 // The last CTA to arrive clears *reset (if given) before releasing the others.
-__device__ bool grid_barrier(HogState *st, int *s_flag, unsigned long long *reset = nullptr) {
+__device__ bool grid_barrier(HogState *st, int *s_flag, unsigned long long timeout_ns,
+                             unsigned long long *reset = nullptr) {
   __syncthreads();
   if (threadIdx.x == 0) {
     volatile unsigned *vgen = &st->gen;
@@ -105,7 +110,7 @@ __device__ bool grid_barrier(HogState *st, int *s_flag, unsigned long long *rese
         __nanosleep(32);
         unsigned long long t1;
         asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t1));
-        if (t1 - t0 > 2000000000ull) {
+        if (t1 - t0 > timeout_ns) {
           ok = 0;
           atomicExch(&st->err, 1);
           break;
@@ -384,7 +389,8 @@ __global__ void __launch_bounds__(HOG_THREADS, 1) k_hogbom(HogArgs<T> a) {
         }
       }
     }
-    if (!grid_barrier(a.state, &s_flag, KEYED ? &a.state->key[par ^ 1] : nullptr)) break;
+    if (!grid_barrier(a.state, &s_flag, a.timeout_ns, KEYED ? &a.state->key[par ^ 1] : nullptr))
+      break;
     // FP32: the winner from the 64-bit maximum (one load); otherwise, and
     // when no pixel was above 0, every CTA reduces all candidates the same way
     if (KEYED) {
@@ -655,6 +661,8 @@ int av_hogbom_run(void *model, void *residual, const void *psf, const void *mask
   cudaStream_t st = as_stream(stream);
   int dev = 0;
   AV_CUDA(cudaGetDevice(&dev));
+  const unsigned long long timeout_ns =
+      (unsigned long long)tune_value(AV_TUNE_HOGBOM_BARRIER_TIMEOUT_US) * 1000ull;
   int sms = sm_count();
   int grid = (int)std::min<int64_t>(sms, ny);
   if (grid > 1024) grid = 1024;
@@ -684,7 +692,7 @@ int av_hogbom_run(void *model, void *residual, const void *psf, const void *mask
     a.niter = niter; a.siter = siter; a.iter_begin = iter_begin; a.iter_end = iter_end;
     a.gain = (float)gain; a.thres = (float)threshold; a.speedup = (float)speedup;
     a.state = (HogState *)state; a.cand = (HogCand<float> *)workspace;
-    a.init = init_state; a.resident = resident;
+    a.init = init_state; a.resident = resident; a.timeout_ns = timeout_ns;
     return hogbom_launch<float>(a, grid, smem, st);
   }
   AV_CUDA(cudaFuncSetAttribute(k_hogbom<double>, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -704,7 +712,7 @@ int av_hogbom_run(void *model, void *residual, const void *psf, const void *mask
   a.niter = niter; a.siter = siter; a.iter_begin = iter_begin; a.iter_end = iter_end;
   a.gain = gain; a.thres = threshold; a.speedup = speedup;
   a.state = (HogState *)state; a.cand = (HogCand<double> *)workspace;
-  a.init = init_state; a.resident = resident;
+  a.init = init_state; a.resident = resident; a.timeout_ns = timeout_ns;
   return hogbom_launch<double>(a, grid, smem, st);
 }
 

@@ -260,10 +260,23 @@ static std::mutex g_briggs_scratch_mu;
 static void *g_briggs_scratch_ptr[kMaxDevices];
 
 // Device address of the current device's copy of g_briggs_scratch, looked up
-// on the first call made with that device current and cached afterwards.
-static int briggs_scratch(void **out) {
+// on the first call made with that device current and cached afterwards (the
+// cache does not survive cudaDeviceReset, which may move the array).  The
+// stream must belong to the current device: the kernels would otherwise run
+// on another device with this device's address.
+static int briggs_scratch(cudaStream_t st, void **out) {
   int dev = 0;
   AV_CUDA(cudaGetDevice(&dev));
+  if (st != nullptr) {
+    int sdev = dev;
+    AV_CUDA(cudaStreamGetDevice(st, &sdev));
+    if (sdev != dev) {
+      set_error("av_briggs_factors_noalloc: the stream belongs to device %d, the current "
+                "device is %d",
+                sdev, dev);
+      return AV_ERR_ARG;
+    }
+  }
   if (dev < 0 || dev >= kMaxDevices) {
     set_error("av_briggs_factors_noalloc: device %d beyond the %d this library tracks", dev,
               kMaxDevices);
@@ -302,7 +315,7 @@ int av_briggs_factors_noalloc(const double *density, const double *sum_weight, d
                     (size_t)AV_BRIGGS_NOALLOC_MAX_PLANES * kBriggsSlices * sizeof(double),
                 "scratch size");
   void *scratch = nullptr;
-  int rc = briggs_scratch(&scratch);
+  int rc = briggs_scratch(as_stream(stream), &scratch);
   if (rc != AV_OK) return rc;
   // every partial k_briggs_finish reads, k_sum_sq of the same call writes
   // first: nothing needs clearing between calls

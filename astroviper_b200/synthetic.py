@@ -132,13 +132,17 @@ def workload_small(seed=20260101, n_time=50):
                 oversampling=100, sources=(flux, dx, dy))
 
 
-def workload_large(seed=20260102, n_time=256, n_chan=64, n_pol=4, device=None):
+def workload_large(seed=20260102, n_time=256, n_chan=64, n_pol=4, device=None,
+                   time_slice=None):
     """Same array at ``n_time`` steps x ``n_chan`` channels (1.0-1.5 GHz) x
     ``n_pol`` polarisations, complex64 data, unit weights, no flags; 2048^2
     image of 1 arcsec cells, Briggs robust 0.5 (weights computed by the
     caller), support 7, oversampling 100.  With ``device`` the visibilities are
-    made on that torch device."""
-    uvw, rng = array_uvw(64, n_time, seed=seed)
+    made on that torch device.  With ``time_slice`` (a slice of the time
+    steps) only those steps' visibilities are made; ``uvw`` still holds every
+    step (``uvw_all``) and ``uvw`` the sliced ones."""
+    uvw_all, rng = array_uvw(64, n_time, seed=seed)
+    uvw = uvw_all if time_slice is None else np.ascontiguousarray(uvw_all[time_slice])
     freq = np.linspace(1.0e9, 1.5e9, n_chan)
     cell = 1.0 * ARCSEC
     pixelincr = np.array([-cell, cell])
@@ -146,7 +150,7 @@ def workload_large(seed=20260102, n_time=256, n_chan=64, n_pol=4, device=None):
     l, m = source_lm(dx, dy, pixelincr)
     vis = point_source_vis(uvw, freq, n_pol, flux, l, m, 0.01, rng, dtype=np.complex64,
                            device=device)
-    return dict(uvw=uvw, freq=freq, vis=vis, pixelincr=pixelincr,
+    return dict(uvw=uvw, uvw_all=uvw_all, freq=freq, vis=vis, pixelincr=pixelincr,
                 image_size=np.array([2048, 2048]), support=7, oversampling=100, robust=0.5,
                 sources=(flux, dx, dy))
 

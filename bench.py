@@ -33,6 +33,9 @@ sys.path.insert(0, ROOT)
 METRIC = "Mvis/s grid+degrid on 1 B200 at <=1e-5 rel err vs FP64; CLEAN iter/s"
 WORKLOAD = ("64 ant (2016 bl) x 256 t x 64 ch x 4 pol = 33.03M vis, complex64, Briggs 0.5, "
             "2048^2 continuum, 1 arcsec, support 7, oversampling 100")
+N_TIME = 256          # time steps of the full workload
+CPU_SAMPLE_T = 64     # time steps of one CPU step: 8.26M vis, 33.0M corr
+CPU_SINGLE_T = 8      # time steps for the one-thread rate
 
 
 def parse():
@@ -41,7 +44,7 @@ def parse():
     ap.add_argument("--steps", type=int, default=50)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
-    ap.add_argument("--n-time", type=int, default=256)
+    ap.add_argument("--n-time", type=int, default=N_TIME)
     ap.add_argument("--quick", action="store_true", help="skip CPU baseline / CLEAN / e2e")
     ap.add_argument("--no-clean", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
@@ -158,70 +161,128 @@ def rel(a, b):
 # ---------------------------------------------------------------------------
 # CPU side (oracle port on the host cores)
 # ---------------------------------------------------------------------------
-def cpu_grid_degrid(W, t_sample, nthreads):
-    """Oracle (C port of the reference's Numba kernels) gridding + degridding
-    of the first t_sample time steps; returns (seconds, n_vis, threads)."""
-    import oracle as O
-    uvw = W["uvw_np"][:t_sample]
-    vis = W["vis_np"][:t_sample]
-    wt = W["wt_np"][:t_sample]
-    cgk = O.create_prolate_spheroidal_kernel_1D(100, 7)
-    n = int(W["image_size"][0])
-    mem_ok = max(1, int((_avail_mem() * 0.5) // (n * n * 4 * 16)))
-    nth = max(1, min(nthreads, mem_ok, 64))
-    t0 = time.perf_counter()
-    g, sw = O.standard_grid(vis, uvw, wt, W["freq"], cgk, W["image_size"], W["pixelincr"],
-                            nthreads=nth)
-    flag = np.zeros(vis.shape, np.uint8)
-    O.degrid(g, uvw, W["freq"], W["pixelincr"], flag=flag, nthreads=nth)
-    dt = time.perf_counter() - t0
-    return dt, uvw.shape[0] * uvw.shape[1] * len(W["freq"]), nth
+def bench_config(world, n_time=None):
+    """The workload description, the same in both arms."""
+    n_vis = (n_time or N_TIME) * 2016 * 64
+    return {"workload": WORKLOAD, "n_vis": n_vis, "n_corr": 4 * n_vis,
+            "l2": "inputs larger than L2 (1.06 GB visibilities per step)",
+            "step": "plan+grid+plan+degrid; grid zeroed, model visibilities written each step",
+            "parallelism": f"replicas x{world}"}
 
 
-def _avail_mem():
+def host_threads():
+    """Host threads this process may run on (its CPU affinity)."""
     try:
-        import psutil
-        return psutil.virtual_memory().available
+        return len(os.sched_getaffinity(0))
     except Exception:
-        return 64 << 30
+        return os.cpu_count() or 1
 
 
-def make_host_workload(n_time):
-    """Host copy of the workload for the CPU legs (no GPU needed)."""
-    from astroviper_b200 import synthetic as S
-    W = S.workload_large(n_time=n_time, device=None)
-    W["uvw_np"] = W["uvw"]
-    W["vis_np"] = W["vis"]
-    W["wt_np"] = np.ones(W["vis"].shape, np.float32)
-    return W
+def cpu_sample(uvw, vis, weight, freq, image_size, pixelincr):
+    """A host sample for the CPU legs, converted once to the oracle's dtypes
+    (complex128 visibilities, float64 weights) outside any timing."""
+    return {"uvw": np.ascontiguousarray(uvw, dtype=np.float64),
+            "vis": np.ascontiguousarray(vis, dtype=np.complex128),
+            "wt": np.ascontiguousarray(weight, dtype=np.float64),
+            "flag": np.zeros(vis.shape, np.uint8), "freq": np.asarray(freq, np.float64),
+            "image_size": image_size, "pixelincr": pixelincr}
+
+
+def cpu_grid_degrid(smp, nthreads, t_steps=None):
+    """The oracle's C restatement of the reference's Numba kernels on the
+    host: standard_grid_jit (rows of the grid owned by threads) then
+    dgrid_numba (time steps split over threads) of the sample's first
+    ``t_steps`` time steps.  Returns (seconds, vis processed)."""
+    import oracle as O
+    t = smp["uvw"].shape[0] if t_steps is None else t_steps
+    uvw, vis, wt, flag = smp["uvw"][:t], smp["vis"][:t], smp["wt"][:t], smp["flag"][:t]
+    cgk = O.create_prolate_spheroidal_kernel_1D(100, 7)
+    t0 = time.perf_counter()
+    g, _sw = O.standard_grid(vis, uvw, wt, smp["freq"], cgk, smp["image_size"],
+                             smp["pixelincr"], nthreads=nthreads, rows=True)
+    O.degrid(g, uvw, smp["freq"], smp["pixelincr"], flag=flag, nthreads=nthreads)
+    dt = time.perf_counter() - t0
+    return dt, uvw.shape[0] * uvw.shape[1] * len(smp["freq"])
+
+
+def cpu_baseline_leg(smp, nthreads, reps=1):
+    """cpu_baseline object: the N-thread rate on the whole sample (mean of
+    ``reps`` runs after one untimed run) and the one-thread rate on its first
+    CPU_SINGLE_T steps."""
+    times = []
+    for i in range(reps + 1):  # the first run warms the allocator and the caches
+        dt, nv = cpu_grid_degrid(smp, nthreads)
+        if i > 0:
+            times.append(dt)
+    dt1, nv1 = cpu_grid_degrid(smp, 1, CPU_SINGLE_T)
+    t = smp["uvw"].shape[0]
+    return {"value": nv / float(np.mean(times)) / 1e6, "unit": "Mvis/s", "cores": nthreads,
+            "kind": "port",
+            "sample": f"first {t} of {N_TIME} time steps ({nv} vis, {4 * nv} corr), Briggs 0.5 "
+                      "weights: the oracle's C restatement of standard_grid_jit (grid rows "
+                      "owned by threads) + dgrid_numba (time steps split over threads)",
+            "single_thread": {"value": nv1 / dt1 / 1e6, "unit": "Mvis/s",
+                              "sample": f"first {CPU_SINGLE_T} time steps ({nv1} vis)"},
+            "host_cpus": os.cpu_count(), "threads_allowed": host_threads()}
+
+
+def host_briggs_weights(uvw_all, freq, image_size, pixelincr, robust, t_sample, npol):
+    """Briggs imaging weights of the first ``t_sample`` time steps with the
+    density of every step (unit data weights), through the oracle: the same
+    weights the GPU arm computes on the device."""
+    import oracle as O
+    nt, nb = uvw_all.shape[:2]
+    nchan = len(freq)
+    nu, nv = int(image_size[0]), int(image_size[1])
+    G = np.zeros((nchan, 1, nu, nv), dtype=np.float64)
+    sw = np.zeros((nchan, 1), dtype=np.float64)
+    O.grid_imaging_weights_jit(G, sw, uvw_all, freq, np.arange(nchan),
+                               np.ones((nt, nb, nchan, 1)), np.array([nu, nv]), pixelincr)
+    bf = O.calculate_briggs_params(G, sw, {"weighting": "briggs", "robust": robust})
+    iw = np.zeros((t_sample, nb, nchan, 1), dtype=np.float64)
+    O.degrid_imaging_weights_jit(iw, G, bf, np.ascontiguousarray(uvw_all[:t_sample]), freq,
+                                 np.arange(nchan), np.arange(1), np.ones((t_sample, nb, nchan, 1)),
+                                 np.array([nu, nv]), pixelincr)
+    return np.repeat(iw, npol, axis=3)
 
 
 def reference_arm(args, rank, world):
-    """Times the reference's CPU implementation of the path (the oracle port of
-    its Numba gridder/degridder; the reference itself is Python+Numba and its
-    sources do not travel) with all host threads, on a bounded sample of the
-    workload per step."""
+    """Times the reference's CPU implementation of the path (the oracle's C
+    restatement of its Numba gridder and degridder; the reference itself is
+    Python+Numba, its sources do not travel) with every host thread this
+    process may use, each step one grid+degrid of the first CPU_SAMPLE_T of
+    the workload's 256 time steps with the workload's Briggs weights."""
     if rank != 0:
         return
-    import oracle as O
-    nthreads = os.cpu_count() or 1
-    t_sample = 4
-    W = make_host_workload(t_sample)
+    from astroviper_b200 import synthetic as S
+    W = S.workload_large(n_time=N_TIME, time_slice=slice(0, CPU_SAMPLE_T))
+    iw = host_briggs_weights(W["uvw_all"], W["freq"], W["image_size"], W["pixelincr"],
+                             W["robust"], CPU_SAMPLE_T, W["vis"].shape[3])
+    smp = cpu_sample(W["uvw"], W["vis"], iw, W["freq"], W["image_size"], W["pixelincr"])
+    del W, iw
+    nthreads = host_threads()
     times = []
     for i in range(args.warmup + args.steps):
-        dt, nvis, nth = cpu_grid_degrid(W, t_sample, nthreads)
+        dt, nvis = cpu_grid_degrid(smp, nthreads)
         if i >= args.warmup:
             times.append(dt)
     ms = 1e3 * float(np.mean(times))
     value = nvis / (ms / 1e3) / 1e6
+    dt1, nv1 = cpu_grid_degrid(smp, 1, CPU_SINGLE_T)
     line = {
         "impl": "reference", "metric": METRIC, "value": value, "unit": "Mvis/s",
         "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
-        "data": "synthetic", "config": {"workload": WORKLOAD,
-                                        "sample": f"first {t_sample} time steps per step"},
-        "cpu_baseline": {"value": value, "unit": "Mvis/s", "cores": nth, "kind": "port",
-                         "sample": f"{nvis} vis ({t_sample} of 256 time steps) grid+degrid"},
+        "data": "synthetic", "config": bench_config(world),
+        "cpu_baseline": {
+            "value": value, "unit": "Mvis/s", "cores": nthreads, "kind": "port",
+            "sample": f"each step: first {CPU_SAMPLE_T} of {N_TIME} time steps ({nvis} vis, "
+                      f"{4 * nvis} corr), Briggs 0.5 weights; the oracle's C restatement of "
+                      "standard_grid_jit (grid rows owned by threads) + dgrid_numba (time steps "
+                      "split over threads)",
+            "single_thread": {"value": nv1 / dt1 / 1e6, "unit": "Mvis/s",
+                              "sample": f"first {CPU_SINGLE_T} time steps ({nv1} vis)"},
+            "host_cpus": os.cpu_count(), "threads_allowed": nthreads},
         "e2e": {"value": value, "unit": "Mvis/s", "h2d_bytes_per_step": 0,
                 "d2h_bytes_per_step": 0},
     }
@@ -401,15 +462,11 @@ def main():
     # ------------------------------------------------------------ CPU baseline
     cpu = None
     if not (args.quick or args.no_cpu) and rank == 0:
-        tsc = 8
-        Wh = {"uvw_np": W["uvw"][:tsc], "vis_np": vis[:tsc].cpu().numpy(),
-              "wt_np": iw[:tsc].cpu().numpy(), "freq": W["freq"], "image_size": img,
-              "pixelincr": cell}
-        nth = os.cpu_count() or 1
-        dt, nv, used = cpu_grid_degrid(Wh, tsc, nth)
-        cpu = {"value": nv / dt / 1e6, "unit": "Mvis/s", "cores": used, "kind": "port",
-               "sample": f"{nv} vis ({tsc} of {nt} time steps, 4 pol) grid+degrid, "
-                         f"C port of the reference kernels, {used} threads"}
+        tsc = min(CPU_SAMPLE_T, nt)
+        smp = cpu_sample(W["uvw"][:tsc], vis[:tsc].cpu().numpy(), iw[:tsc].cpu().numpy(),
+                         W["freq"], img, cell)
+        cpu = cpu_baseline_leg(smp, host_threads(), reps=2)
+        del smp
 
     # --------------------------------------------------------------------- e2e
     e2e = None
@@ -445,10 +502,7 @@ def main():
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
         "data": "synthetic",
-        "config": {"workload": WORKLOAD, "n_vis": n_vis, "n_corr": n_corr,
-                   "l2": "inputs larger than L2 (1.06 GB visibilities per step)",
-                   "step": "plan+grid+plan+degrid; grid zeroed, model visibilities written each step",
-                   "parallelism": f"replicas x{world}"},
+        "config": bench_config(world, n_time),
         "roofline": {"bound": "hbm", "kernel": dom[0], "achieved": achieved, "peak": peak,
                      "unit": "GB/s", "frac": achieved / peak,
                      "traffic": DRAM_BYTES_PER_VIS[dom[0]] * n_vis,

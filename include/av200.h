@@ -80,14 +80,26 @@ unsigned long long av_launch_count(void);
  *                                supports up to 8), AV_DEGRID_LANES_FP32 (FP32
  *                                FMA) or AV_DEGRID_LANES_AUTO (default: TF32
  *                                for supports 7 and 8, FP32 otherwise)
+ *   AV_TUNE_HOGBOM_BARRIER_TIMEOUT_US  how long (microseconds of wall time,
+ *                                default 2000000) a CTA of av_hogbom_run
+ *                                waits at the per-iteration grid barrier
+ *                                before it gives up; on giving up the launch
+ *                                ends, av_hogbom_state_read returns
+ *                                AV_ERR_TIMEOUT ("grid barrier timed out")
+ *                                and the run must be started again
+ *                                (init_state = 1).  0 makes every CTA but
+ *                                the last to arrive give up at its first
+ *                                barrier, which is how the timeout path is
+ *                                tested.  Range [0, 600000000].
  * av_tune_set returns AV_ERR_ARG for an unknown knob or a value outside
- * [1, 1024] ([1, 3] for the two lane knobs); av_tune_get returns -1 for an
- * unknown knob. */
+ * [1, 1024] ([1, 3] for the two lane knobs, [0, 600000000] for the barrier
+ * timeout); av_tune_get returns -1 for an unknown knob. */
 enum av_tune {
   AV_TUNE_GRID_CHUNKS_PER_SM = 0,
   AV_TUNE_DEGRID_CHUNKS_PER_SM = 1,
   AV_TUNE_GRID_LANES = 2,
-  AV_TUNE_DEGRID_LANES = 3
+  AV_TUNE_DEGRID_LANES = 3,
+  AV_TUNE_HOGBOM_BARRIER_TIMEOUT_US = 4
 };
 enum av_grid_lanes { AV_GRID_LANES_MMA = 1, AV_GRID_LANES_ROWS = 2, AV_GRID_LANES_AUTO = 3 };
 enum av_degrid_lanes {
@@ -321,7 +333,11 @@ int av_briggs_factors(const double *density, const double *sum_weight, double *f
  * 512 KiB, held on every GPU that loads the library until the process exits).
  * nplanes above the maximum returns AV_ERR_ARG; the call makes no
  * allocation.  The first call on a device looks up that device's copy of the
- * array: make it before any stream capture.  All calls share the one array,
+ * array: make it before any stream capture.  The lookup is kept for the life
+ * of the process and does not survive cudaDeviceReset (after a reset the
+ * array may sit elsewhere): do not call this function after resetting a
+ * device it has been called on.  The stream must belong to the current
+ * device (AV_ERR_ARG otherwise).  All calls share the one array,
  * so calls that overlap on the GPU (other streams, other host threads) race;
  * serialise them.  Every partial a call reads it first writes, so the
  * previous call's contents never leak into a result. */

@@ -224,8 +224,25 @@ void orc_standard_grid(void *grid, int is_complex, double *sum_weight, int do_ps
              nb, nchan, npol, n_img_pol, 0, nt * nb);
 }
 
-/* Multi-threaded baseline: (t, b) rows split across threads, each into a
- * private complex grid, summed at the end.  Same per-sample arithmetic. */
+/* Multi-threaded gridding by owned grid rows (the CPU baseline and the
+ * large-size parity checks).  Every image plane's u rows are cut into one
+ * band per thread; a thread walks every sample in the reference's order and
+ * adds only the taps whose u row lies in its band.  Each cell therefore
+ * receives its addends in the serial order, and the grid is bit-identical to
+ * orc_standard_grid.  sum_weight is added, per sample, by the thread owning
+ * the footprint's first row, in sample order within a thread and then over
+ * the threads in band order, so it can differ from the serial sum in the last
+ * bits.  A first parallel pass computes every sample's cell and kernel
+ * offsets once (the reference's expressions, standard_grid.py:297-352) and a
+ * histogram of footprint rows; the cuts give every band about the same
+ * number of taps.  No per-thread grid is allocated: the extra memory is
+ * 16 bytes per (time, baseline, channel) sample.  do_imaging_weight is not
+ * supported here (the serial restatement covers it).
+ * Returns the number of threads used, -1 when memory runs out, -2 for a
+ * support outside [1, ORC_MAX_SUPPORT]. */
+typedef struct { int32_t ui, vi, uoi, voi; } orc_cell;
+#define ORC_MAX_SUPPORT 64
+
 int orc_standard_grid_mt(cplx *grid, double *sum_weight, int do_psf, const cplx *vis,
                          const double *uvw, const double *freq, const int64_t *chan_map,
                          const int64_t *pol_map, const double *weight, const double *cgk,
@@ -237,39 +254,144 @@ int orc_standard_grid_mt(cplx *grid, double *sum_weight, int do_psf, const cplx 
 #else
   nthreads = 1;
 #endif
-  const int64_t gsz = n_img_chan * n_img_pol * n_u * n_v;
+  if (support < 1 || support > ORC_MAX_SUPPORT) return -2;
+  const double c = 299792458.0;
+  const int64_t sc = support / 2, s0 = -sc, s1 = support - sc;
+  const int64_t uc0 = n_u / 2, uc1 = n_v / 2;
+  const int64_t ntb = nt * nb, nsamp = ntb * nchan;
   const int64_t ssz = n_img_chan * n_img_pol;
-  cplx **priv = (cplx **)calloc(nthreads, sizeof(cplx *));
-  double **psw = (double **)calloc(nthreads, sizeof(double *));
-  for (int t = 0; t < nthreads; ++t) {
-    priv[t] = (cplx *)calloc(gsz, sizeof(cplx));
-    psw[t] = (double *)calloc(ssz, sizeof(double));
-    if (!priv[t] || !psw[t]) return -1;
+  orc_cell *cells = (orc_cell *)malloc(sizeof(orc_cell) * (size_t)(nsamp > 0 ? nsamp : 1));
+  double *us = (double *)malloc(sizeof(double) * 2 * (size_t)(nchan > 0 ? nchan : 1));
+  int64_t *hist = (int64_t *)calloc((size_t)nthreads * (size_t)n_u, sizeof(int64_t));
+  int64_t *cut = (int64_t *)malloc(sizeof(int64_t) * (size_t)(nthreads + 1));
+  double *psw = (double *)calloc((size_t)nthreads * (size_t)(ssz > 0 ? ssz : 1), sizeof(double));
+  if (!cells || !us || !hist || !cut || !psw) {
+    free(cells); free(us); free(hist); free(cut); free(psw);
+    return -1;
   }
-  const int64_t ntb = nt * nb;
+  for (int64_t k = 0; k < nchan; ++k) {
+    us[2 * k] = -(freq[k] * dl0 * (double)n_u) / c;
+    us[2 * k + 1] = -(freq[k] * dl1 * (double)n_v) / c;
+  }
+  /* pass 1: cells and offsets, histogram of first footprint rows */
 #pragma omp parallel num_threads(nthreads)
   {
-    int t = 0, T = 1;
+    int t = 0;
 #ifdef _OPENMP
     t = omp_get_thread_num();
-    T = omp_get_num_threads();
 #endif
-    int64_t lo = ntb * t / T, hi = ntb * (t + 1) / T;
-    grid_range(priv[t], 1, psw[t], do_psf, 0, vis, uvw, freq, chan_map, pol_map, weight, cgk,
-               n_u, n_v, dl0, dl1, support, oversampling, nt, nb, nchan, npol, n_img_pol, lo,
-               hi);
+    int64_t *h = hist + (int64_t)t * n_u;
+#pragma omp for schedule(static)
+    for (int64_t tb = 0; tb < ntb; ++tb) {
+      const double *p_uvw = uvw + tb * 3;
+      for (int64_t ic = 0; ic < nchan; ++ic) {
+        orc_cell *cl = &cells[tb * nchan + ic];
+        cl->ui = INT32_MIN;
+        double u = p_uvw[0] * us[2 * ic];
+        double v = p_uvw[1] * us[2 * ic + 1];
+        if (isnan(u) || isnan(v)) continue;
+        double u_pos = u + (double)uc0, v_pos = v + (double)uc1;
+        int64_t ui = trunc_i64(u_pos + 0.5), vi = trunc_i64(v_pos + 0.5);
+        if (!((ui + sc < n_u) && (vi + sc < n_v) && (ui - sc >= 0) && (vi - sc >= 0))) continue;
+        cl->ui = (int32_t)ui;
+        cl->vi = (int32_t)vi;
+        cl->uoi = (int32_t)(int64_t)floor(((double)ui - u_pos) * (double)oversampling + 0.5);
+        cl->voi = (int32_t)(int64_t)floor(((double)vi - v_pos) * (double)oversampling + 0.5);
+        h[ui + s0] += 1;
+      }
+    }
   }
-#pragma omp parallel for num_threads(nthreads) schedule(static)
-  for (int64_t g = 0; g < gsz; ++g) {
-    double re = grid[g].re, im = grid[g].im;
-    for (int t = 0; t < nthreads; ++t) { re += priv[t][g].re; im += priv[t][g].im; }
-    grid[g].re = re;
-    grid[g].im = im;
+  /* row cuts: rows weighted by the footprints that cover them */
+  {
+    double total = 0.0;
+    double *cover = (double *)calloc((size_t)n_u, sizeof(double));
+    if (!cover) {
+      free(cells); free(us); free(hist); free(cut); free(psw);
+      return -1;
+    }
+    for (int64_t r = 0; r < n_u; ++r) {
+      int64_t n0 = 0;
+      for (int t = 0; t < nthreads; ++t) n0 += hist[(int64_t)t * n_u + r];
+      for (int64_t d = 0; d < support && r + d < n_u; ++d) cover[r + d] += (double)n0;
+      total += (double)n0 * (double)support;
+    }
+    cut[0] = 0;
+    int k = 1;
+    double acc = 0.0;
+    for (int64_t r = 0; r < n_u && k < nthreads; ++r) {
+      acc += cover[r];
+      while (k < nthreads && acc >= total * (double)k / (double)nthreads) cut[k++] = r + 1;
+    }
+    while (k <= nthreads) cut[k++] = n_u;
+    free(cover);
+  }
+  /* pass 2: every band walks all samples in order.  The tap products
+   * conv = cgk[|os iu + uoi|] * cgk[|os iv + voi|] and their sum (norm, in
+   * the reference's iv-outer, iu-inner order) do not depend on the
+   * polarisation: they are formed once per sample, with the same operands
+   * and order as the reference forms them per polarisation. */
+#pragma omp parallel for num_threads(nthreads) schedule(dynamic, 1)
+  for (int t = 0; t < nthreads; ++t) {
+    const int64_t lo = cut[t], hi = cut[t + 1];
+    double *sw_t = psw + (int64_t)t * ssz;
+    double conv[ORC_MAX_SUPPORT * ORC_MAX_SUPPORT];
+    if (lo >= hi) continue;
+    for (int64_t tb = 0; tb < ntb; ++tb) {
+      for (int64_t ic = 0; ic < nchan; ++ic) {
+        const orc_cell cl = cells[tb * nchan + ic];
+        if (cl.ui == INT32_MIN) continue;
+        const int64_t ui = cl.ui, vi = cl.vi;
+        if (ui + s1 <= lo || ui + s0 >= hi) continue;
+        const int64_t iu_lo = lo - ui > s0 ? lo - ui : s0;
+        const int64_t iu_hi = hi - ui < s1 ? hi - ui : s1;
+        const int owns_sw = (ui + s0 >= lo) && (ui + s0 < hi);
+        const int64_t a_chan = chan_map[ic];
+        double norm = 0.0;
+        for (int64_t iv = s0; iv < s1; ++iv) {
+          const int64_t vo = (int64_t)oversampling * iv + cl.voi;
+          const double conv_v = cgk[vo < 0 ? -vo : vo];
+          for (int64_t iu = s0; iu < s1; ++iu) {
+            const int64_t uo = (int64_t)oversampling * iu + cl.uoi;
+            const double cv = cgk[uo < 0 ? -uo : uo] * conv_v;
+            conv[(iv - s0) * support + (iu - s0)] = cv;
+            norm = norm + cv;
+          }
+        }
+        for (int64_t ip = 0; ip < npol; ++ip) {
+          const int64_t idx = (tb * nchan + ic) * npol + ip;
+          double sel_weight = weight[idx];
+          cplx wd;
+          if (do_psf) {
+            wd.re = weight[idx];
+            wd.im = 0.0;
+          } else {
+            wd.re = vis[idx].re * weight[idx];
+            wd.im = vis[idx].im * weight[idx];
+          }
+          if (isnan(wd.re) || isnan(wd.im)) continue;
+          if (!(wd.re != 0.0 || wd.im != 0.0)) continue;
+          const int64_t a_pol = pol_map[ip];
+          cplx *plane = grid + (a_chan * n_img_pol + a_pol) * n_u * n_v;
+          for (int64_t iv = s0; iv < s1; ++iv) {
+            const double *crow = conv + (iv - s0) * support - s0;
+            cplx *grow = plane + (vi + iv);
+            for (int64_t iu = iu_lo; iu < iu_hi; ++iu) {
+              cplx *g = grow + (ui + iu) * n_v;
+              g->re = g->re + crow[iu] * wd.re;
+              g->im = g->im + crow[iu] * wd.im;
+            }
+          }
+          if (owns_sw) sw_t[a_chan * n_img_pol + a_pol] += sel_weight * norm;
+        }
+      }
+    }
   }
   for (int64_t s = 0; s < ssz; ++s)
-    for (int t = 0; t < nthreads; ++t) sum_weight[s] += psw[t][s];
-  for (int t = 0; t < nthreads; ++t) { free(priv[t]); free(psw[t]); }
-  free(priv);
+    for (int t = 0; t < nthreads; ++t) sum_weight[s] += psw[(int64_t)t * ssz + s];
+  free(cells);
+  free(us);
+  free(hist);
+  free(cut);
   free(psw);
   return nthreads;
 }
@@ -291,62 +413,85 @@ static void dgrid_range(const double *uvw, const double *dphase, cplx *values,
   const int64_t nx = g_n3, ny = g_n2; /* as named in the reference */
   const int64_t supp_centre = support / 2;
   const int64_t supp_beg = -supp_centre, supp_end = supp_beg + support;
+  (void)nt;
+  /* The reference loops polarisation outside channel; every value is
+   * computed on its own, so the walk here takes the channel outside and
+   * forms the position, the phasor and the tap products wt = wtx * wty (and
+   * their sum, norm, in the reference's ix-outer, iy-inner order) once for
+   * all polarisations: same operands, same order, same results. */
+  double *wt = (double *)malloc(sizeof(double) * (size_t)support * (size_t)support);
+  if (!wt) return;
   for (int64_t t = t_lo; t < t_hi; ++t) {
     for (int64_t b = 0; b < nb; ++b) {
       const double *p_uvw = uvw + (t * nb + b) * 3;
-      for (int64_t ipol = 0; ipol < nvpol; ++ipol) {
-        int64_t apol = polmap[ipol];
-        if (!(0 <= apol && apol < g_npol)) continue;
-        for (int64_t ichan = 0; ichan < nvchan; ++ichan) {
-          int64_t achan = chanmap[ichan];
+      for (int64_t ichan = 0; ichan < nvchan; ++ichan) {
+        int64_t achan = chanmap[ichan];
+        if (!(0 <= achan && achan < g_nchan)) continue;
+        double pos0 = scale[0] * p_uvw[0] * freq[ichan] / c + offset[0];
+        double pos1 = scale[1] * p_uvw[1] * freq[ichan] / c + offset[1];
+        double r0 = nearbyint(pos0), r1 = nearbyint(pos1);
+        /* loc and off are stored in int32 arrays by the reference
+         * (standard_degrid.py:413-414): keep its wrap-around. */
+        int64_t loc0 = (int32_t)(uint32_t)(uint64_t)trunc_i64(r0);
+        int64_t loc1 = (int32_t)(uint32_t)(uint64_t)trunc_i64(r1);
+        int64_t off0 = (int32_t)(uint32_t)(uint64_t)trunc_i64(
+            nearbyint(((double)loc0 - pos0) * (double)sampling));
+        int64_t off1 = (int32_t)(uint32_t)(uint64_t)trunc_i64(
+            nearbyint(((double)loc1 - pos1) * (double)sampling));
+        int64_t x0 = loc0, y0 = loc1;
+        if (!((x0 + supp_beg >= 0) && ((x0 + supp_end - 1) < nx) && (y0 + supp_beg >= 0) &&
+              ((y0 + supp_end - 1) < ny)))
+          continue;
+        if (x0 + supp_end - 1 >= g_n2 || y0 + supp_end - 1 >= g_n3) continue;
+        int any = 0;
+        for (int64_t ipol = 0; ipol < nvpol && !any; ++ipol) {
+          int64_t apol = polmap[ipol];
           int64_t vidx = ((t * nb + b) * nvchan + ichan) * nvpol + ipol;
-          if (!(0 <= achan && achan < g_nchan) || flag[vidx]) continue;
-          double pos0 = scale[0] * p_uvw[0] * freq[ichan] / c + offset[0];
-          double pos1 = scale[1] * p_uvw[1] * freq[ichan] / c + offset[1];
-          double r0 = nearbyint(pos0), r1 = nearbyint(pos1);
-          /* loc and off are stored in int32 arrays by the reference
-           * (standard_degrid.py:413-414): keep its wrap-around. */
-          int64_t loc0 = (int32_t)(uint32_t)(uint64_t)trunc_i64(r0);
-          int64_t loc1 = (int32_t)(uint32_t)(uint64_t)trunc_i64(r1);
-          int64_t off0 = (int32_t)(uint32_t)(uint64_t)trunc_i64(
-              nearbyint(((double)loc0 - pos0) * (double)sampling));
-          int64_t off1 = (int32_t)(uint32_t)(uint64_t)trunc_i64(
-              nearbyint(((double)loc1 - pos1) * (double)sampling));
-          double phase = -2.0 * M_PI * dphase[t * nb + b] * freq[ichan] / c;
-          double ph_re = cos(phase), ph_im = sin(phase);
-          int64_t x0 = loc0, y0 = loc1;
-          if (!((x0 + supp_beg >= 0) && ((x0 + supp_end - 1) < nx) && (y0 + supp_beg >= 0) &&
-                ((y0 + supp_end - 1) < ny)))
-            continue;
-          if (x0 + supp_end - 1 >= g_n2 || y0 + supp_end - 1 >= g_n3) continue;
-          double nv_re = 0.0, nv_im = 0.0, norm = 0.0;
+          any = (0 <= apol && apol < g_npol) && !flag[vidx];
+        }
+        if (!any) continue;
+        double phase = -2.0 * M_PI * dphase[t * nb + b] * freq[ichan] / c;
+        double ph_re = cos(phase), ph_im = sin(phase);
+        double norm = 0.0;
+        for (int64_t ix = supp_beg; ix < supp_end; ++ix) {
+          int64_t i1 = sampling * ix + off0;
+          double wtx = convFunc[i1 < 0 ? -i1 : i1];
+          for (int64_t iy = supp_beg; iy < supp_end; ++iy) {
+            int64_t i2 = sampling * iy + off1;
+            double w = wtx * convFunc[i2 < 0 ? -i2 : i2];
+            wt[(ix - supp_beg) * support + (iy - supp_beg)] = w;
+            norm += w;
+          }
+        }
+        if (norm == 0.0) continue;
+        for (int64_t ipol = 0; ipol < nvpol; ++ipol) {
+          int64_t apol = polmap[ipol];
+          if (!(0 <= apol && apol < g_npol)) continue;
+          int64_t vidx = ((t * nb + b) * nvchan + ichan) * nvpol + ipol;
+          if (flag[vidx]) continue;
+          double nv_re = 0.0, nv_im = 0.0;
           const cplx *plane = grid + (achan * g_npol + apol) * g_n2 * g_n3;
           for (int64_t ix = supp_beg; ix < supp_end; ++ix) {
-            int64_t i1 = sampling * ix + off0;
-            double wtx = convFunc[i1 < 0 ? -i1 : i1];
+            const cplx *grow = plane + (x0 + ix) * g_n3 + y0;
+            const double *wrow = wt + (ix - supp_beg) * support - supp_beg;
             for (int64_t iy = supp_beg; iy < supp_end; ++iy) {
-              int64_t i2 = sampling * iy + off1;
-              double wty = convFunc[i2 < 0 ? -i2 : i2];
-              double wt = wtx * wty;
-              norm += wt;
-              cplx gv = plane[(x0 + ix) * g_n3 + (y0 + iy)];
-              nv_re = nv_re + wt * gv.re;
-              nv_im = nv_im + wt * gv.im;
+              cplx gv = grow[iy];
+              nv_re = nv_re + wrow[iy] * gv.re;
+              nv_im = nv_im + wrow[iy] * gv.im;
             }
           }
-          if (norm != 0.0) {
-            /* nvalue * conj(phasor), then / norm (component-wise for a real
-             * divisor, as the complex quotient reduces to it). */
-            double cr = ph_re, ci = -ph_im;
-            double pr = nv_re * cr - nv_im * ci;
-            double pi = nv_re * ci + nv_im * cr;
-            values[vidx].re = values[vidx].re + pr / norm;
-            values[vidx].im = values[vidx].im + pi / norm;
-          }
+          /* nvalue * conj(phasor), then / norm (component-wise for a real
+           * divisor, as the complex quotient reduces to it). */
+          double cr = ph_re, ci = -ph_im;
+          double pr = nv_re * cr - nv_im * ci;
+          double pi = nv_re * ci + nv_im * cr;
+          values[vidx].re = values[vidx].re + pr / norm;
+          values[vidx].im = values[vidx].im + pi / norm;
         }
       }
     }
   }
+  free(wt);
 }
 
 void orc_dgrid(const double *uvw, const double *dphase, cplx *values, const uint8_t *flag,

@@ -5,9 +5,10 @@
 # checker and as the CPU baseline for CLEAN.  Needs the reference tree, so it
 # runs in the build container; the built module travels with the repository.
 set -e
-REF=${AV_REFERENCE_ROOT:-/root/reference}
-HB=$REF/src/astroviper/core/imaging/deconvolvers/hogbom
 HERE="$(cd "$(dirname "$0")" && pwd)"
+# the reference checkout: $AV_REFERENCE_ROOT, else reference/ beside this repository
+REF=${AV_REFERENCE_ROOT:-$(cd "$HERE/../.." && pwd)/reference}
+HB=$REF/src/astroviper/core/imaging/deconvolvers/hogbom
 [ -f "$HB/src/hclean.cpp" ] || { echo "reference tree not found at $REF" >&2; exit 1; }
 mkdir -p "$HERE/_ref"
 EXT=$(python3 -c "import sysconfig; print(sysconfig.get_config_var('EXT_SUFFIX'))")

@@ -137,10 +137,13 @@ def standard_grid_jit(grid, sum_weight, do_psf, do_imaging_weight, vis_data, uvw
 
 def standard_grid(vis_data, uvw, weight, freq_chan, cgk_1D, image_size, cell_size,
                   oversampling=100, support=7, do_psf=False, chan_mode="continuum",
-                  nthreads=1):
+                  nthreads=1, rows=False):
     """standard_grid_numpy_wrap (standard_grid.py:88-165) on fresh arrays:
-    returns (grid complex128, sum_weight).  nthreads > 1 uses the private-grid
-    OpenMP variant (same per-sample arithmetic, different summation order)."""
+    returns (grid complex128, sum_weight).  nthreads > 1 (or 0: every OpenMP
+    thread) uses the row-owner OpenMP variant: the grid is bit-identical to
+    the serial one, sum_weight may differ in the last bits (it is summed per
+    thread first).  rows=True takes that variant at one thread too (the CPU
+    baseline's one-thread rate)."""
     nchan, npol = weight.shape[2], weight.shape[3]
     if chan_mode == "cube":
         n_img_chan, chan_map = nchan, np.arange(nchan, dtype=np.int64)
@@ -150,7 +153,7 @@ def standard_grid(vis_data, uvw, weight, freq_chan, cgk_1D, image_size, cell_siz
     nu, nv = int(image_size[0]), int(image_size[1])
     grid = np.zeros((n_img_chan, npol, nu, nv), dtype=np.complex128)
     sw = np.zeros((n_img_chan, npol), dtype=np.float64)
-    if nthreads == 1:
+    if nthreads == 1 and not rows:
         standard_grid_jit(grid, sw, do_psf, False, vis_data, uvw, freq_chan, chan_map, pol_map,
                           weight, cgk_1D, np.array([nu, nv]), cell_size, support, oversampling)
         return grid, sw
@@ -166,8 +169,10 @@ def standard_grid(vis_data, uvw, weight, freq_chan, cgk_1D, image_size, cell_siz
                                      _p(cgk, _dp), nu, nv, float(cell_size[0]),
                                      float(cell_size[1]), int(support), int(oversampling), nt,
                                      nb, nchan, npol, n_img_chan, npol, int(nthreads))
+    if got == -2:
+        raise ValueError(f"oracle: support {support} outside the row-owner gridder's range")
     if got < 0:
-        raise MemoryError("oracle: private grids could not be allocated")
+        raise MemoryError("oracle: the per-sample cell table could not be allocated")
     return grid, sw
 
 

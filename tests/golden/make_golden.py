@@ -1,7 +1,7 @@
 """Generates the golden fixtures in this folder from the reference itself.
 
 Run in a container that has the astroviper source tree (default
-``/root/reference``, override with ``AV_REFERENCE_ROOT``) and the reference's
+``reference/`` beside this repository, override with ``AV_REFERENCE_ROOT``) and the reference's
 Hogbom extension built by ``oracle/build_ref.sh``:
 
     python tests/golden/make_golden.py
@@ -22,7 +22,8 @@ import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 REPO = os.path.dirname(os.path.dirname(HERE))
-REF = os.environ.get("AV_REFERENCE_ROOT", "/root/reference")
+REF = os.environ.get("AV_REFERENCE_ROOT",
+                     os.path.join(os.path.dirname(REPO), "reference"))
 SRC = os.path.join(REF, "src", "astroviper")
 os.environ.setdefault("NUMBA_CACHE_DIR", "/tmp/numba_cache_golden")
 sys.path.insert(0, REPO)
@@ -228,6 +229,36 @@ def make_image(R):
     np.savez_compressed(os.path.join(HERE, "image.npz"), **out)
 
 
+def make_psf_planes(R):
+    """The PSF planes make_psf (make_point_spread_function.py:41-53) computes
+    before xradio wraps them: grid2image_spheroid_ms4 with dopsf=True and
+    pixel increment [-cell0, cell1] into a zero array of shape
+    (n_freq, n_pol, image_size[1], image_size[0]).  xradio is absent here, so
+    the function itself cannot run; its call is made exactly as it makes it.
+    Non-square sizes show the transposed array shape."""
+    rng = np.random.default_rng(2112)
+    from astroviper_b200 import synthetic as S
+    uvw, _ = S.array_uvw(12, 6, radius_m=500.0, seed=78)
+    freq = np.array([1.3e9, 1.4e9])
+    nt, nb = uvw.shape[:2]
+    vis = rng.normal(size=(nt, nb, 2, 2)) + 1j * rng.normal(size=(nt, nb, 2, 2))
+    weight = rng.uniform(0.5, 1.5, size=vis.shape)
+    flag = rng.uniform(size=vis.shape) < 0.1
+    uvw[3, 4, 1] = np.nan
+    cell = np.array([25.0, 30.0]) * np.pi / (180 * 3600)
+    out = dict(uvw=uvw, freq=freq, vis=vis, weight=weight, flag=flag, cell=cell)
+    for mode, nch, image_size in (("cube", 2, (64, 48)), ("continuum", 1, (48, 64))):
+        w = weight[:, :, :nch].copy()
+        ms = MS4Double(vis[:, :, :nch].copy(), uvw.copy(), w, flag[:, :, :nch].copy(), freq[:nch])
+        psf = np.zeros([nch, 2, image_size[1], image_size[0]], dtype=float)
+        R.sg.grid2image_spheroid_ms4(ms, psf, np.array([-cell[0], cell[1]]), 7, 100, True,
+                                     "VISIBILITY", mode)
+        out[f"psf_{mode}"] = psf
+        out[f"image_size_{mode}"] = np.array(image_size)
+        out[f"weight_after_{mode}"] = w
+    np.savez_compressed(os.path.join(HERE, "psf_dropin.npz"), **out)
+
+
 def make_degrid(R):
     rng = np.random.default_rng(3003)
     from astroviper_b200 import synthetic as S
@@ -351,17 +382,20 @@ def make_hogbom(R):
     np.savez_compressed(os.path.join(HERE, "hogbom.npz"), **out)
 
 
-def main():
+MAKERS = {"pswf": make_pswf, "grid": make_grid, "image": make_image,
+          "psf_dropin": make_psf_planes, "degrid": make_degrid, "weights": make_weights,
+          "hogbom": make_hogbom}
+
+
+def main(names=None):
+    """Writes every fixture, or only the named ones
+    (``python tests/golden/make_golden.py psf_dropin``)."""
     R = load_reference()
-    make_pswf(R)
-    make_grid(R)
-    make_image(R)
-    make_degrid(R)
-    make_weights(R)
-    make_hogbom(R)
+    for name in (names or list(MAKERS)):
+        MAKERS[name](R)
     for f in sorted(glob.glob(os.path.join(HERE, "*.npz"))):
         print(os.path.basename(f), os.path.getsize(f))
 
 
 if __name__ == "__main__":
-    main()
+    main(sys.argv[1:])

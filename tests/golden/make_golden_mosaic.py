@@ -1,7 +1,7 @@
 """Generates the mosaic-gridding fixtures in this folder from the reference.
 
 Run in a container that has the astroviper source tree (default
-``/root/reference``, override with ``AV_REFERENCE_ROOT``):
+``reference/`` beside this repository, override with ``AV_REFERENCE_ROOT``):
 
     python tests/golden/make_golden_mosaic.py
 
@@ -22,7 +22,8 @@ import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 REPO = os.path.dirname(os.path.dirname(HERE))
-REF = os.environ.get("AV_REFERENCE_ROOT", "/root/reference")
+REF = os.environ.get("AV_REFERENCE_ROOT",
+                     os.path.join(os.path.dirname(REPO), "reference"))
 SRC = os.path.join(REF, "src", "astroviper")
 os.environ.setdefault("NUMBA_CACHE_DIR", "/tmp/numba_cache_golden")
 sys.path.insert(0, REPO)

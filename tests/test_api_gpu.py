@@ -97,6 +97,37 @@ def test_grid2image_spheroid_ms4(precision, tol):
         SG.grid2image_spheroid_ms4(ms, np.zeros((3, 2, 64, 64)), g["cell"])
 
 
+@pytest.mark.parametrize("mode", ["cube", "continuum"])
+@pytest.mark.parametrize("precision,tol", [("fp64", 1e-12), (None, 1e-6)])
+def test_make_psf_dropin(mode, precision, tol):
+    """make_psf (make_point_spread_function.py:1-79): the planes the reference
+    computes (grid2image_spheroid_ms4 with dopsf and pixelincr [-cell0, cell1]
+    into an (n_freq, n_pol, image_size[1], image_size[0]) array; non-square
+    sizes show the transpose), as the POINT_SPREAD_FUNCTION of a sky image
+    over the visibilities' frequencies, polarisations and first time."""
+    from astroviper_b200 import synthetic as S
+    from astroviper_b200.core.imaging.imaging_utils.make_point_spread_function import make_psf
+    g = golden("psf_dropin.npz")
+    nch = 2 if mode == "cube" else 1
+    node = S.Ms4Node(g["vis"][:, :, :nch].copy(), g["uvw"].copy(),
+                     g["weight"][:, :, :nch].copy(), g["flag"][:, :, :nch].copy(),
+                     g["freq"][:nch], ["XX", "YY"])
+    size = tuple(int(n) for n in g[f"image_size_{mode}"])
+    img = make_psf(node, {"image_size": size, "cell_size": g["cell"], "phase_center": (0.3, -0.5),
+                          "chan_mode": mode}, {"sampling": 100, "support": 7},
+                   precision=precision)
+    psf = img["POINT_SPREAD_FUNCTION"]
+    ref = g[f"psf_{mode}"]
+    assert psf.dims == ("time", "frequency", "polarization", "l", "m")
+    assert psf.values.shape == (1, nch, 2, size[1], size[0]) == (1,) + ref.shape
+    assert rel(psf.values[0], ref) <= tol
+    assert np.array_equal(node["WEIGHT"].data, g[f"weight_after_{mode}"])
+    assert np.array_equal(img.coords["frequency"].values, g["freq"][:nch])
+    assert list(img.coords["polarization"].values) == ["XX", "YY"]
+    assert img.coords["time"].values[0] == node.coords["time"].values[0]
+    assert img.attrs["phase_center"] == (0.3, -0.5)
+
+
 def test_reference_lattice_known_answer_on_gpu():
     """test_standard_grid.py:14-111 of the reference through the drop-in API."""
     from astroviper_b200.core.imaging.fft import fft_lm_to_uv

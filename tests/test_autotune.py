@@ -34,6 +34,15 @@ def test_tune_knobs_set_get_and_reject():
     assert L.av_tune_set(_lib.AV_TUNE_DEGRID_LANES, _lib.AV_DEGRID_LANES_FP32) == _lib.AV_OK
     assert L.av_tune_set(_lib.AV_TUNE_DEGRID_LANES, _lib.AV_DEGRID_LANES_AUTO) == _lib.AV_OK
     assert L.av_tune_set(_lib.AV_TUNE_GRID_CHUNKS_PER_SM, g) == _lib.AV_OK
+    # the Hogbom barrier timeout (microseconds): 0 is allowed, the default is 2 s
+    knob = _lib.AV_TUNE_HOGBOM_BARRIER_TIMEOUT_US
+    assert L.av_tune_get(knob) == _lib.AV_HOGBOM_BARRIER_TIMEOUT_US_DEFAULT
+    assert L.av_tune_set(knob, -1) == _lib.AV_ERR_ARG
+    assert L.av_tune_set(knob, 600000001) == _lib.AV_ERR_ARG
+    assert "AV_TUNE_HOGBOM_BARRIER_TIMEOUT_US" in _lib.last_error()
+    assert L.av_tune_set(knob, 0) == _lib.AV_OK
+    assert L.av_tune_get(knob) == 0
+    assert L.av_tune_set(knob, _lib.AV_HOGBOM_BARRIER_TIMEOUT_US_DEFAULT) == _lib.AV_OK
 
 
 def test_autotuner_picks_fastest_and_caches(tmp_path):

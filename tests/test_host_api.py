@@ -36,6 +36,21 @@ def test_validate_threshold():
         D._validate_deconv_params({"threshold": -1e-9})
 
 
+def test_validate_edge_values_and_order_as_reference():
+    # deconvolution.py:100-118: a NaN gain fails "0 < g <= 1"; a NaN threshold
+    # passes "not < 0"; the parameters are checked in the order gain, niter,
+    # threshold, clean_box, defaults filled in on the way
+    with pytest.raises(ValueError, match="CLEAN gain"):
+        D._validate_deconv_params({"gain": float("nan")})
+    got = D._validate_deconv_params({"threshold": float("nan")})
+    assert np.isnan(got["threshold"]) and got["gain"] == 0.1
+    p = {"niter": 0, "clean_box": "x"}
+    with pytest.raises(ValueError, match="Maximum number of iterations"):
+        D._validate_deconv_params(p)
+    assert p["gain"] == 0.1 and "threshold" not in p
+    assert D._validate_deconv_params({"clean_box": None})["clean_box"] is None
+
+
 @pytest.mark.parametrize("box", [(1, 2), (1, 2, 3), (1, 2, 3, 4, 5), "box", []])
 def test_validate_clean_box_rejected(box):
     with pytest.raises(ValueError, match="Clean box must be a 4-tuple.*or None"):

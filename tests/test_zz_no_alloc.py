@@ -1,8 +1,9 @@
 """av_briggs_factors_noalloc, the allocation-free variant of av_briggs_factors
 whose partial sums live in a static device array of the library: its factors
-against those of av_briggs_factors with a caller workspace, on two calls in a
-row (the second smaller than the first, so stale partials of the first call
-would show), and its rejection of a plane count above the static maximum."""
+against those of av_briggs_factors with a caller workspace, bit for bit, on
+two calls in a row (the second smaller than the first, so stale partials of
+the first call would show); the device's free memory unchanged by a call; and
+its rejection of a plane count above the static maximum."""
 import ctypes
 import os
 import re
@@ -42,10 +43,11 @@ def _with_workspace(L, d, sw, robust):
     return out
 
 
-def _no_alloc(L, d, sw, robust):
+def _no_alloc(L, d, sw, robust, out=None):
     from astroviper_b200 import _kernels as K
     npl, nu, nv = d.shape
-    out = torch.full((2, npl), np.nan, dtype=torch.float64, device="cuda")
+    if out is None:
+        out = torch.full((2, npl), np.nan, dtype=torch.float64, device="cuda")
     _lib.check(L.av_briggs_factors_noalloc(d.data_ptr(), sw.data_ptr(), out.data_ptr(), npl, nu,
                                            nv, robust, K.stream_ptr()),
                "av_briggs_factors_noalloc")
@@ -54,6 +56,8 @@ def _no_alloc(L, d, sw, robust):
 
 @pytest.mark.gpu
 def test_no_alloc_factors_match_the_workspace_entry_point_twice():
+    """Both entry points launch the same kernels over the same slices, so the
+    factors must be bit-identical, on the first call and on the next."""
     L = _lib.lib()
     cases = [(1, (_max_planes(), 32, 48), 0.5), (2, (3, 300, 200), -1.0)]
     for seed, shape, robust in cases:
@@ -63,7 +67,24 @@ def test_no_alloc_factors_match_the_workspace_entry_point_twice():
         torch.cuda.synchronize()
         r, g = ref.cpu().numpy(), got.cpu().numpy()
         assert np.all(np.isfinite(g))
-        assert np.allclose(g, r, rtol=1e-12, atol=0)
+        assert np.array_equal(g, r)
+
+
+@pytest.mark.gpu
+def test_no_alloc_call_takes_no_device_memory():
+    """After a first call (which loads the kernels and looks up the array), a
+    call leaves the device's free memory exactly as it was."""
+    L = _lib.lib()
+    d, sw = _density(3, 16, 64, 64)
+    out = torch.full((2, 16), np.nan, dtype=torch.float64, device="cuda")
+    _no_alloc(L, d, sw, 0.5, out)
+    torch.cuda.synchronize()
+    free0, _total = torch.cuda.mem_get_info()
+    _no_alloc(L, d, sw, 0.5, out)
+    torch.cuda.synchronize()
+    free1, _total = torch.cuda.mem_get_info()
+    assert free1 == free0
+    assert np.all(np.isfinite(out.cpu().numpy()))
 
 
 def test_no_alloc_rejects_more_planes_than_the_static_maximum():
