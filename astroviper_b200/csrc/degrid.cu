@@ -269,7 +269,22 @@ __device__ __forceinline__ void degrid_write(const TiledDegridArgs &a, const Deg
                                              const double *rs, const int (&pmv)[8],
                                              const Rec &rc, const float2 (&acc)[NPG]) {
   const double norm = rs[rc.ou] * rs[rc.ov];
-  const int64_t row_i = rc.row;
+  const int64_t row_i = rc.row & ~REC_DEGRID_EXC;
+  if (rc.row & REC_DEGRID_EXC) {
+    // a shared plan's sample whose degridder convention differs: zeros in
+    // store mode (k_degrid_exceptions then writes the ones the degridder
+    // keeps), nothing when accumulating
+    if (!a.accumulate) {
+      if (a.fast_out) {
+        float4 *o = (float4 *)((float2 *)d.values + row_i * 4);
+        o[0] = make_float4(0.f, 0.f, 0.f, 0.f);
+        o[1] = make_float4(0.f, 0.f, 0.f, 0.f);
+      } else {
+        for (int p = 0; p < d.nvpol; ++p) put_value(d, 0, row_i * d.nvpol + p, 0.0, 0.0);
+      }
+    }
+    return;
+  }
   if (a.fast_out) {
     // 1 / norm in FP64, the scaling in FP32 (one more rounding, ~6e-8)
     const float inv = norm != 0.0 ? (float)(1.0 / norm) : 0.f;
@@ -774,15 +789,19 @@ __global__ void __launch_bounds__(TC_THREADS, 2) k_degrid_tc(TiledDegridArgs a) 
                 xhre = vhq[2 * pol];
                 xhim = vhq[2 * pol + 1];
               }
+            // a shared plan's marked sample gets 0 here (k_degrid_exceptions
+            // writes the ones the degridder keeps)
             float2 *out = (float2 *)d.values;
+            const bool mg = (recg.row & REC_DEGRID_EXC) == 0u;
+            const bool mh = (rech.row & REC_DEGRID_EXC) == 0u;
             if (vg)
-              out[(int64_t)recg.row * 4 + t] = src >= 0 ? make_float2(__fmul_rn(xgre, invg),
-                                                                      __fmul_rn(xgim, invg))
-                                                        : make_float2(0.f, 0.f);
+              out[(int64_t)(recg.row & ~REC_DEGRID_EXC) * 4 + t] =
+                  (src >= 0 && mg) ? make_float2(__fmul_rn(xgre, invg), __fmul_rn(xgim, invg))
+                                   : make_float2(0.f, 0.f);
             if (vh)
-              out[(int64_t)rech.row * 4 + t] = src >= 0 ? make_float2(__fmul_rn(xhre, invh),
-                                                                      __fmul_rn(xhim, invh))
-                                                        : make_float2(0.f, 0.f);
+              out[(int64_t)(rech.row & ~REC_DEGRID_EXC) * 4 + t] =
+                  (src >= 0 && mh) ? make_float2(__fmul_rn(xhre, invh), __fmul_rn(xhim, invh))
+                                   : make_float2(0.f, 0.f);
           }
           j = j1;
         }
@@ -798,6 +817,98 @@ __global__ void __launch_bounds__(TC_THREADS, 2) k_degrid_tc(TiledDegridArgs a) 
       a.sched[0] = 0u;
       a.sched[1] = 0u;
       __threadfence();
+    }
+  }
+}
+
+// ------------------------------------------------- shared-plan exceptions --
+// The samples a shared plan lists for the degridder (plan.cuh): each in the
+// degridder's own convention (sample_pos_degrid, standard_degrid.py:435-462)
+// and in FP64, the reference's tap and summation order, one thread per
+// sample, all visibility polarisations.  Runs after the tiled kernel, which
+// left zeros there in store mode.  Reads the plan's copies of u, v, the
+// frequencies, the channel map and the degridder's scale / offset.
+struct ExcArgs {
+  const uint32_t *count, *rows;
+  const double2 *uv;
+  const double *freq;
+  const int32_t *chan_map;
+  const double *dpar;
+  PlanGeom g;  // the degridder's geometry (scale / offset come from dpar)
+  DegridArgs d;
+  int accumulate;
+};
+
+__global__ void __launch_bounds__(128) k_degrid_exceptions(ExcArgs e) {
+  const uint32_t n = *e.count;
+  if (n == 0u) return;
+  const DegridArgs &d = e.d;
+  PlanGeom g = e.g;
+  g.scale0 = e.dpar[0];
+  g.scale1 = e.dpar[1];
+  g.offset0 = e.dpar[2];
+  g.offset1 = e.dpar[3];
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    const uint32_t row = e.rows[i];
+    const int64_t tb = row / d.nvchan;
+    const int ichan = (int)(row - tb * d.nvchan);
+    const int achan = e.chan_map[ichan];
+    const double f = e.freq[ichan];
+    const double2 uv = e.uv[tb];
+    int fu, fv, o0, o1;
+    if (achan < 0 || achan >= d.g_nchan || !sample_pos_degrid(uv.x, uv.y, f, g, fu, fv, o0, o1))
+      continue;  // not listed by the plan; kept for safety
+    const long long beg = -(d.support / 2), end = beg + d.support;
+    const long long x0 = (long long)fu - beg, y0 = (long long)fv - beg;
+    double norm = 0.0;
+    for (long long ix = beg; ix < end; ++ix) {
+      const long long i1 = (long long)d.sampling * ix + o0;
+      const double wtx = d.cf[i1 < 0 ? -i1 : i1];
+      for (long long iy = beg; iy < end; ++iy) {
+        const long long i2 = (long long)d.sampling * iy + o1;
+        norm = __dadd_rn(norm, __dmul_rn(wtx, d.cf[i2 < 0 ? -i2 : i2]));
+      }
+    }
+    double ph_re = 1.0, ph_im = 0.0;
+    if (d.dphase) {
+      const double phase =
+          __ddiv_rn(__dmul_rn(__dmul_rn(-2.0 * 3.141592653589793, d.dphase[tb]), f), d.c);
+      sincos(phase, &ph_im, &ph_re);
+    }
+    for (int p = 0; p < d.nvpol; ++p) {
+      const int64_t k = (int64_t)row * d.nvpol + p;
+      const int apol = d.polmap[p];
+      if (apol < 0 || apol >= d.g_npol || (d.flag && d.flag[k]) || norm == 0.0) {
+        if (!e.accumulate) put_value(d, 0, k, 0.0, 0.0);
+        continue;
+      }
+      const int64_t plane = ((int64_t)achan * d.g_npol + apol) * d.g_n2 * d.g_n3;
+      double nv_re = 0.0, nv_im = 0.0;
+      for (long long ix = beg; ix < end; ++ix) {
+        const long long i1 = (long long)d.sampling * ix + o0;
+        const double wtx = d.cf[i1 < 0 ? -i1 : i1];
+        for (long long iy = beg; iy < end; ++iy) {
+          const long long i2 = (long long)d.sampling * iy + o1;
+          const double wt = __dmul_rn(wtx, d.cf[i2 < 0 ? -i2 : i2]);
+          const int64_t gi = plane + (x0 + ix) * d.g_n3 + (y0 + iy);
+          double gr, gim;
+          if (d.grid_c128) {
+            const double2 gv = ((const double2 *)d.grid)[gi];
+            gr = gv.x;
+            gim = gv.y;
+          } else {
+            const float2 gv = ((const float2 *)d.grid)[gi];
+            gr = gv.x;
+            gim = gv.y;
+          }
+          nv_re = __dadd_rn(nv_re, __dmul_rn(wt, gr));
+          nv_im = __dadd_rn(nv_im, __dmul_rn(wt, gim));
+        }
+      }
+      const double cr = ph_re, ci = -ph_im;
+      const double pr = __dsub_rn(__dmul_rn(nv_re, cr), __dmul_rn(nv_im, ci));
+      const double pi = __dadd_rn(__dmul_rn(nv_re, ci), __dmul_rn(nv_im, cr));
+      put_value(d, e.accumulate, k, __ddiv_rn(pr, norm), __ddiv_rn(pi, norm));
     }
   }
 }
@@ -1072,7 +1183,25 @@ int av_degrid_tiled_execute(const double *dphase, void *values, int values_dtype
   a.fast_out = (!accumulate && values_dtype == AV_C64 && nvpol == 4 && flag == nullptr &&
                 dphase == nullptr && (((uintptr_t)values) & 31) == 0) ? 1 : 0;
   int npg = g_npol <= 1 ? 1 : (g_npol <= 2 ? 2 : 4);
-  return degrid_dispatch(a, support, npg, (rows + chunk - 1) / chunk, as_stream(stream));
+  rc = degrid_dispatch(a, support, npg, (rows + chunk - 1) / chunk, as_stream(stream));
+  if (rc) return rc;
+  // a shared plan's exceptions (none listed in a degridder plan: the kernel
+  // reads a zero count and returns)
+  ExcArgs e;
+  e.count = p.exc_count;
+  e.rows = p.exc_rows;
+  e.uv = p.uv;
+  e.freq = p.freq;
+  e.chan_map = p.chan_map;
+  e.dpar = p.dpar;
+  e.g = g;
+  e.g.scale0 = e.g.scale1 = e.g.offset0 = e.g.offset1 = 0.0;
+  e.d = d;
+  e.d.cf = convFunc;
+  e.accumulate = a.accumulate;
+  k_degrid_exceptions<<<(unsigned)sms, 128, 0, as_stream(stream)>>>(e);
+  AV_LAUNCH_CHECK();
+  return AV_OK;
 }
 
 int av_degrid_tiled(const double *uvw, const double *dphase, void *values, int values_dtype,

@@ -684,11 +684,11 @@ __global__ void __launch_bounds__(GCfg<S, NPOL>::THREADS, 1) k_grid_tiled(TiledG
       {
         const uint32_t r = w_lo + lane;
         Rec r0;
-        if (r < w_hi) r0 = a.recs[r];
+        if (r < w_hi) r0 = grid_rec(a.recs, r);
         prefetch<NPOL>(pf, a, r0, r < w_hi);
       }
       bool rnext_ok = w_lo + GT_STAGE + lane < w_hi;
-      if (rnext_ok) rnext = a.recs[w_lo + GT_STAGE + lane];
+      if (rnext_ok) rnext = grid_rec(a.recs, w_lo + GT_STAGE + lane);
       for (int rd = 0; rd < n_rounds; ++rd) {
         // ---- stage this round's samples, one per lane: FP64 weighted
         // values, the cell key and the offsets of the two tap-table rows
@@ -725,7 +725,7 @@ __global__ void __launch_bounds__(GCfg<S, NPOL>::THREADS, 1) k_grid_tiled(TiledG
           prefetch<NPOL>(pf, a, rnext, rnext_ok);
           const uint32_t r = w_lo + (uint32_t)(rd + 2) * GT_STAGE + lane;
           rnext_ok = r < w_hi;
-          if (rnext_ok) rnext = a.recs[r];
+          if (rnext_ok) rnext = grid_rec(a.recs, r);
         }
         // ---- compute the round's samples in runs of one cell
         const int jn = (int)min((uint32_t)GT_STAGE, w_hi - (w_lo + (uint32_t)rd * GT_STAGE));
@@ -934,7 +934,7 @@ __global__ void __launch_bounds__(MCfg<S, NPOL>::THREADS, 1) k_grid_mma(TiledGri
       auto load_rec = [&](int rd) {
         const uint32_t r = w_lo + (uint32_t)rd * GT_STAGE + lane;
         Rec x;
-        if (rd < n_rounds && r < w_hi) x = a.recs[r];
+        if (rd < n_rounds && r < w_hi) x = grid_rec(a.recs, r);
         else x.row = 0xffffffffu;
         return x;
       };
@@ -1187,6 +1187,50 @@ int av_grid_tiled_plan(const double *uvw, const double *freq, const int32_t *cha
                              workspace, workspace_bytes, p, "av_grid_tiled_plan");
   if (rc) return rc;
   return plan_build(g, p, uvw, freq, chan_map, delta_l, delta_m, as_stream(stream));
+}
+
+int av_tiled_plan_shared(const double *uvw, const double *freq, const int32_t *chan_map,
+                         int64_t n_u, int64_t n_v, double delta_l, double delta_m, int support,
+                         int oversampling, int64_t nt, int64_t nb, int64_t nchan,
+                         int64_t n_img_chan, void *workspace, size_t workspace_bytes,
+                         void *stream) {
+  clear_error();
+  AV_CHECK_ARG(uvw && freq && chan_map, "av_tiled_plan_shared: null pointer");
+  PlanGeom g;
+  Plan p;
+  int rc = grid_geom_checked(g, n_u, n_v, support, oversampling, nt, nb, nchan, n_img_chan,
+                             workspace, workspace_bytes, p, "av_tiled_plan_shared");
+  if (rc) return rc;
+  // the degridder's conventions for a grid of (n_img_chan, pols, n_u, n_v)
+  // and cell (delta_l, delta_m), as degrid_spheroid_ms4 passes them
+  // (standard_degrid.py:568-584): scale -cell * n, offset n / 2, bounds
+  // against shape[3] and shape[2]
+  g.convention = 2;
+  g.chk_x = n_v;
+  g.chk_y = n_u;
+  g.scale0 = -delta_l * (double)n_u;
+  g.scale1 = -delta_m * (double)n_v;
+  g.offset0 = (double)n_u / 2.0;
+  g.offset1 = (double)n_v / 2.0;
+  return plan_build(g, p, uvw, freq, chan_map, delta_l, delta_m, as_stream(stream));
+}
+
+int av_tiled_plan_counts(int64_t nt, int64_t nb, int64_t nchan, int64_t n_u, int64_t n_v,
+                         int64_t n_img_chan, int support, const void *workspace,
+                         size_t workspace_bytes, uint32_t *out, void *stream) {
+  clear_error();
+  AV_CHECK_ARG(out, "av_tiled_plan_counts: null pointer");
+  PlanGeom g;
+  Plan p;
+  int rc = grid_geom_checked(g, n_u, n_v, support, 100, nt, nb, nchan, n_img_chan,
+                             (void *)workspace, workspace_bytes, p, "av_tiled_plan_counts");
+  if (rc) return rc;
+  cudaStream_t st = as_stream(stream);
+  AV_CUDA(cudaMemcpyAsync(&out[0], p.offs + g.n_keys(), sizeof(uint32_t), cudaMemcpyDeviceToHost,
+                          st));
+  AV_CUDA(cudaMemcpyAsync(&out[1], p.exc_count, sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
+  AV_CUDA(cudaStreamSynchronize(st));
+  return AV_OK;
 }
 
 int av_grid_tiled_execute(void *grid, int grid_dtype, double *sum_weight, int do_psf,

@@ -60,6 +60,57 @@ __device__ __forceinline__ uint32_t sample_key(const PlanGeom &g, double um, dou
   return tile * (uint32_t)g.kpt + cell;
 }
 
+// Shared plan: the gridder's key and record of one sample, marked for the
+// degridder.  When the gridder keeps the sample and all its rounded
+// quantities lie clear of a rounding boundary (sample_pos_grid's `safe`),
+// the degridder's half-even rounding of its own FP64 position (which differs
+// from the gridder's by less than 1e-10 cells) gives the same cell and
+// offsets, so only its bounds tests (against the reference's swapped
+// extents, standard_degrid.py:457-462) are evaluated, in integers.
+// Otherwise the degridder's position is computed exactly.  A record the
+// degridder cannot use as it stands gets REC_DEGRID_EXC; `exc` says the
+// degridder keeps the sample, so it goes to the exception list.
+__device__ __forceinline__ uint32_t sample_key_shared(const PlanGeom &g, double um, double vm,
+                                                      double us0, double us1, double f,
+                                                      int plane, uint32_t row, uint2 &rec,
+                                                      bool &exc) {
+  rec = make_uint2(row, 0u);
+  exc = false;
+  const uint32_t skip = (uint32_t)g.n_keys();
+  if (plane < 0 || plane >= g.n_planes) return skip;  // neither convention maps the channel
+  int fu, fv, ou, ov;
+  bool safe = false;
+  const bool ok = sample_pos_grid(um, vm, us0, us1, g.n_u, g.n_v, g.support, g.os, g.margin, fu,
+                                  fv, ou, ov, &safe);
+  bool dok, same;
+  if (ok && safe) {
+    const long long sc = g.support / 2, beg = -sc, end = beg + g.support;
+    const long long X0 = (long long)fu + sc, Y0 = (long long)fv + sc;
+    dok = (X0 + beg >= 0) && (X0 + end - 1 < g.chk_x) && (Y0 + beg >= 0) &&
+          (Y0 + end - 1 < g.chk_y) && (X0 + end - 1 < g.n_u) && (Y0 + end - 1 < g.n_v);
+    same = true;
+  } else {
+    int dfu, dfv, dou, dov;
+    dok = sample_pos_degrid(um, vm, f, g, dfu, dfv, dou, dov);
+    same = ok && dok && dfu == fu && dfv == fv && dou == ou && dov == ov;
+  }
+  if (!ok) {
+    exc = dok;  // the gridder skips it, the degridder keeps it
+    return skip;
+  }
+  const uint32_t tu = (uint32_t)fu / TILE, tv = (uint32_t)fv / TILE;
+  const uint32_t du = (uint32_t)fu - tu * TILE, dv = (uint32_t)fv - tv * TILE;
+  const uint32_t tile = ((uint32_t)plane * (uint32_t)g.ntu + tu) * (uint32_t)g.ntv + tv;
+  const int side_shift = 5 - g.res_shift;
+  const uint32_t cell = ((du >> g.res_shift) << side_shift) + (dv >> g.res_shift);
+  rec.y = du | (dv << 8) | ((uint32_t)(ou + 128) << 16) | ((uint32_t)(ov + 128) << 24);
+  if (!(same && dok)) {
+    rec.x |= REC_DEGRID_EXC;
+    exc = dok;
+  }
+  return tile * (uint32_t)g.kpt + cell;
+}
+
 // Warp aggregation of per-key atomics over runs of equal keys in lane order
 // (a warp holds consecutive time steps of one series, so equal keys are
 // adjacent).  Returns whether this lane leads a run and, for a leader, the
@@ -84,7 +135,8 @@ __global__ void __launch_bounds__(256) k_plan_count(PlanGeom g, const double *__
                                                     const double *__restrict__ scale,
                                                     const int32_t *__restrict__ chan_map,
                                                     uint32_t *hist, uint32_t *walk_key,
-                                                    uint2 *walk_rec) {
+                                                    uint2 *walk_rec, uint32_t *exc_count,
+                                                    uint32_t *exc_rows) {
   const int lane = threadIdx.x & 31;
   const uint32_t n_warps = (gridDim.x * blockDim.x) >> 5;
   const uint32_t nt = (uint32_t)g.nt, nb = (uint32_t)g.nb, nchan = (uint32_t)g.nchan;
@@ -106,7 +158,13 @@ __global__ void __launch_bounds__(256) k_plan_count(PlanGeom g, const double *__
       uint32_t key = 0xffffffffu;
       if (w.in) {
         uint2 rec;
-        key = sample_key(g, um, vm, us0, us1, f, plane, tb * nchan + c, rec);
+        if (g.convention == 2) {
+          bool exc;
+          key = sample_key_shared(g, um, vm, us0, us1, f, plane, tb * nchan + c, rec, exc);
+          if (exc) exc_rows[atomicAdd(exc_count, 1u)] = tb * nchan + c;  // rare
+        } else {
+          key = sample_key(g, um, vm, us0, us1, f, plane, tb * nchan + c, rec);
+        }
         walk_key[widx] = key;
         walk_rec[widx] = rec;
       }
@@ -300,8 +358,36 @@ bool plan_carve(const PlanGeom &g, Workspace &ws, Plan &p) {
   p.counters = ws.take<uint32_t>(16);
   p.walk_key = ws.take<uint32_t>(g.n_rows > 0 ? g.n_rows : 1);
   p.walk_rec = ws.take<Rec>(g.n_rows > 0 ? g.n_rows : 1);
+  p.exc_count = ws.take<uint32_t>(4);
+  p.exc_rows = ws.take<uint32_t>(g.n_rows > 0 ? g.n_rows : 1);
+  p.uv = ws.take<double2>(g.nt * g.nb > 0 ? g.nt * g.nb : 1);
+  p.freq = ws.take<double>(g.nchan > 0 ? g.nchan : 1);
+  p.chan_map = ws.take<int32_t>(g.nchan > 0 ? g.nchan : 1);
+  p.dpar = ws.take<double>(4);
   return p.offs && p.cursor && p.tile_start && p.recs && p.scale && p.scan_tmp &&
-         p.counters && p.walk_key && p.walk_rec;
+         p.counters && p.walk_key && p.walk_rec && p.exc_count && p.exc_rows && p.uv &&
+         p.freq && p.chan_map && p.dpar;
+}
+
+// What the exception kernel of a shared plan reads: u, v of every (time,
+// baseline), the frequencies, the channel map and the degridder's scale /
+// offset (so the plan stands on its own after the caller's arrays change).
+__global__ void k_shared_copy(const double *uvw, int64_t ntb, const double *freq,
+                              const int32_t *chan_map, int64_t nchan, double s0, double s1,
+                              double o0, double o1, double2 *uv, double *fcopy, int32_t *ccopy,
+                              double *dpar) {
+  const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (i < ntb) uv[i] = make_double2(uvw[3 * i], uvw[3 * i + 1]);
+  if (i < nchan) {
+    fcopy[i] = freq[i];
+    ccopy[i] = chan_map[i];
+  }
+  if (i == 0) {
+    dpar[0] = s0;
+    dpar[1] = s1;
+    dpar[2] = o0;
+    dpar[3] = o1;
+  }
 }
 
 int plan_build(const PlanGeom &g, Plan &p, const double *uvw, const double *freq,
@@ -312,7 +398,21 @@ int plan_build(const PlanGeom &g, Plan &p, const double *uvw, const double *freq
               (long long)g.n_rows);
     return AV_ERR_UNSUPPORTED;
   }
+  if (g.convention == 2 && g.n_rows >= (int64_t)REC_DEGRID_EXC) {
+    set_error("plan: %lld samples exceed a shared plan's 31-bit rows", (long long)g.n_rows);
+    return AV_ERR_UNSUPPORTED;
+  }
   AV_CUDA(cudaMemsetAsync(p.cursor, 0, sizeof(uint32_t) * (nk + 2), st));
+  AV_CUDA(cudaMemsetAsync(p.exc_count, 0, sizeof(uint32_t) * 4, st));
+  if (g.convention == 2) {
+    const int64_t n = std::max<int64_t>(g.nt * g.nb, g.nchan);
+    if (n > 0) {
+      k_shared_copy<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(
+          uvw, g.nt * g.nb, freq, chan_map, g.nchan, g.scale0, g.scale1, g.offset0, g.offset1,
+          p.uv, p.freq, p.chan_map, p.dpar);
+      AV_LAUNCH_CHECK();
+    }
+  }
   if (g.nchan > 0) {
     k_chan_scale<<<(unsigned)((g.nchan + 127) / 128), 128, 0, st>>>(
         freq, g.nchan, delta_l, delta_m, g.n_u, g.n_v, p.scale);
@@ -325,7 +425,8 @@ int plan_build(const PlanGeom &g, Plan &p, const double *uvw, const double *freq
   if (blocks < 1) blocks = 1;
   if (g.n_rows > 0) {
     k_plan_count<<<(unsigned)blocks, 256, 0, st>>>(g, uvw, freq, p.scale, chan_map, p.cursor,
-                                                  p.walk_key, (uint2 *)p.walk_rec);
+                                                  p.walk_key, (uint2 *)p.walk_rec,
+                                                  p.exc_count, p.exc_rows);
     AV_LAUNCH_CHECK();
   }
   int rc = scan_counts(p.cursor, p.offs, nk + 1, p.scan_tmp, st);

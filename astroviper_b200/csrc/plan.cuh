@@ -16,6 +16,18 @@
 // uvw, channel outside the image) go to one extra key, n_keys, after all
 // tiles: offs[n_keys] counts the usable records and the rest of recs[] lists
 // the skipped rows (a store-mode degrid writes zeros there).
+//
+// A shared plan (convention 2) serves the gridder and the degridder at once:
+// records are sorted by the gridder's key (int(x + 0.5) rounding,
+// standard_grid.py:337-352), and the samples whose cell, kernel offsets or
+// bounds verdict differ under the degridder's half-even rounding
+// (standard_degrid.py:435-462) are marked for it: their records carry
+// REC_DEGRID_EXC in the row's top bit (the gridder masks it off; the
+// degridder writes zero there or skips them), and those the degridder keeps
+// are listed in exc_rows, which a small FP64 kernel degrids after the tiled
+// one.  The degridder's position is computed exactly only for samples near a
+// rounding boundary (see sample_key_shared in plan.cu); elsewhere the two
+// conventions provably agree.
 #pragma once
 #include "common.cuh"
 
@@ -25,11 +37,22 @@ constexpr int TILE = 32;                       // tile edge in cells
 constexpr int SCAN_MAX_BLOCKS = 65536;                    // scan partials
 constexpr int64_t KEY_BUDGET = (int64_t(1) << 28) - 65536;  // scan capacity: 65536 x 4096 keys
 
+// top bit of Rec::row in a shared plan: the degridder's convention differs
+// for this sample (never set in a plan of one convention)
+constexpr uint32_t REC_DEGRID_EXC = 0x80000000u;
+
 struct __align__(8) Rec {
   uint32_t row;     // (t * nb + b) * nchan + c
   uint8_t du, dv;   // footprint start inside the tile (cells)
   uint8_t ou, ov;   // kernel offsets + 128
 };
+
+// A record as the gridder reads it: the degridder's mark cleared.
+__device__ __forceinline__ Rec grid_rec(const Rec *recs, uint32_t r) {
+  Rec x = recs[r];
+  x.row &= ~REC_DEGRID_EXC;
+  return x;
+}
 
 struct PlanGeom {
   int64_t n_rows;            // nt * nb * nchan
@@ -46,7 +69,8 @@ struct PlanGeom {
   // `margin` cells from both grid edges (support / 2 for standard_grid_jit;
   // np.max(weight_support) for mosaic_grid_jit, mosaic_grid.py:398-403)
   int margin;
-  int convention;            // 0 = gridder (standard_grid.py), 1 = degridder
+  int convention;            // 0 = gridder (standard_grid.py), 1 = degridder,
+                             // 2 = shared (gridder order, degridder exceptions)
   // degridder only: the reference's own bounds extents and the scale/offset
   int64_t chk_x, chk_y;      // nx = shape[3], ny = shape[2] (standard_degrid.py:407)
   double scale0, scale1, offset0, offset1;
@@ -94,6 +118,17 @@ inline size_t plan_workspace_bytes(const PlanGeom &g) {
   const size_t nr = g.n_rows > 0 ? (size_t)g.n_rows : 1;
   b += Workspace::need(sizeof(uint32_t) * nr);                 // keys in walk order
   b += Workspace::need(sizeof(Rec) * nr);                      // records in walk order
+  // degridder exceptions of a shared plan (count, rows) and what their
+  // kernel needs: u, v per (time, baseline), frequencies, channel map and
+  // the degridder's scale / offset
+  const size_t ntb = g.nt * g.nb > 0 ? (size_t)(g.nt * g.nb) : 1;
+  const size_t nc = g.nchan > 0 ? (size_t)g.nchan : 1;
+  b += Workspace::need(sizeof(uint32_t) * 4);
+  b += Workspace::need(sizeof(uint32_t) * nr);
+  b += Workspace::need(sizeof(double2) * ntb);
+  b += Workspace::need(sizeof(double) * nc);
+  b += Workspace::need(sizeof(int32_t) * nc);
+  b += Workspace::need(sizeof(double) * 4);
   return b;
 }
 
@@ -108,26 +143,49 @@ struct Plan {
   uint32_t *counters;
   uint32_t *walk_key;  // n_rows: key of each sample in walk order (pass 1)
   Rec *walk_rec;       // n_rows: record of each sample in walk order (pass 1)
+  uint32_t *exc_count; // [0]: degridder exceptions listed (0 unless shared)
+  uint32_t *exc_rows;  // n_rows: their rows
+  double2 *uv;         // nt * nb: u, v of each (time, baseline) (shared only)
+  double *freq;        // nchan (shared only)
+  int32_t *chan_map;   // nchan (shared only)
+  double *dpar;        // scale0, scale1, offset0, offset1 (shared only)
 };
+
+// Distance of x from the nearest integer.
+__device__ __forceinline__ double int_dist(double x) { return fabs(__dsub_rn(x, rint(x))); }
+
+// Margins that make the gridder's and the degridder's roundings agree (see
+// sample_key_shared in plan.cu): the two FP64 positions of a sample differ
+// by less than 1e-10 cells, its kernel-offset arguments by less than 3e-8.
+constexpr double CELL_SLACK = 1e-7, OFFSET_SLACK = 1e-5;
 
 // Position of one sample in the gridder's convention (standard_grid.py:
 // 297-352): returns false when it is skipped.  fu/fv = first footprint cell.
+// With `safe`, also whether all four rounded quantities (the cells' and the
+// offsets' int(x + 0.5) arguments) lie more than CELL_SLACK / OFFSET_SLACK
+// from a rounding boundary.
 __device__ __forceinline__ bool sample_pos_grid(double um, double vm, double us0, double us1,
                                                 int64_t n_u, int64_t n_v, int support, int os,
                                                 int margin, int &fu, int &fv, int &offu,
-                                                int &offv) {
+                                                int &offv, bool *safe = nullptr) {
   double u = __dmul_rn(um, us0), v = __dmul_rn(vm, us1);
   if (isnan(u) || isnan(v)) return false;
   double u_pos = __dadd_rn(u, (double)(n_u / 2));
   double v_pos = __dadd_rn(v, (double)(n_v / 2));
-  long long ui = trunc_ll(__dadd_rn(u_pos, 0.5)), vi = trunc_ll(__dadd_rn(v_pos, 0.5));
+  const double au = __dadd_rn(u_pos, 0.5), av = __dadd_rn(v_pos, 0.5);
+  long long ui = trunc_ll(au), vi = trunc_ll(av);
   const long long sc = support / 2, mg = margin;
   if (!((ui + mg < n_u) && (vi + mg < n_v) && (ui - mg >= 0) && (vi - mg >= 0))) return false;
   double uo = __dsub_rn((double)ui, u_pos), vo = __dsub_rn((double)vi, v_pos);
-  offu = (int)floor(__dadd_rn(__dmul_rn(uo, (double)os), 0.5));
-  offv = (int)floor(__dadd_rn(__dmul_rn(vo, (double)os), 0.5));
+  const double bu = __dadd_rn(__dmul_rn(uo, (double)os), 0.5);
+  const double bv = __dadd_rn(__dmul_rn(vo, (double)os), 0.5);
+  offu = (int)floor(bu);
+  offv = (int)floor(bv);
   fu = (int)(ui - sc);
   fv = (int)(vi - sc);
+  if (safe)
+    *safe = int_dist(au) > CELL_SLACK && int_dist(av) > CELL_SLACK &&
+            int_dist(bu) > OFFSET_SLACK && int_dist(bv) > OFFSET_SLACK;
   return true;
 }
 
@@ -161,7 +219,10 @@ __device__ __forceinline__ bool sample_pos_degrid(double um, double vm, double f
 
 // Host: enqueue the plan build for uvw / freq / chan_map (plane per channel;
 // entries outside [0, n_planes) drop the channel).  Nothing is synchronised:
-// the record count stays on the device in offs[n_keys].
+// the record count stays on the device in offs[n_keys] (and a shared plan's
+// exception count in exc_count[0]).  A shared plan (g.convention == 2) needs
+// the degridder's scale / offset / bounds extents in g as well as the
+// gridder's cell size (delta_l, delta_m).
 int plan_build(const PlanGeom &g, Plan &p, const double *uvw, const double *freq,
                const int32_t *chan_map, double delta_l, double delta_m, cudaStream_t st);
 

@@ -40,12 +40,16 @@ class Gridder:
         else:
             self.n_img_chan = 1
             cm = np.zeros(self.nchan, dtype=int)
+        self._cm_host = np.asarray(cm)
         self.chan_map = K.on_device(cm, torch.int32)
         self.n_img_pol = int(n_img_pol if n_img_pol is not None else npol)
         self.pol_map = K.on_device(np.arange(self.npol) % self.n_img_pol, torch.int32)
         self.cgk = K.pswf_table(self.os, self.support)
         self._gplan = None
         self._dplan = None
+        # plan() builds one plan for both directions where it can; False
+        # builds the two separately
+        self.shared_plan = True
 
     # ------------------------------------------------------------- gridding
     def _grid_plan(self):
@@ -88,9 +92,29 @@ class Gridder:
 
     def plan(self, g_nchan=None):
         """Build the gridding and the degridding plan (for a grid of g_nchan
-        channels, default n_img_chan) concurrently on two streams: both
-        depend only on uvw, the frequencies and the geometry, and neither
-        fills the GPU alone.  Later calls on the current stream see both."""
+        channels, default n_img_chan).  When the degridder's channel map
+        int(i / nchan * g_nchan) equals the gridder's (continuum and cube
+        images), one shared plan serves both (av_tiled_plan_shared): the two
+        conventions differ only in their rounding, and the rare samples where
+        that matters are degridded apart in FP64.  Otherwise the two plans
+        are built concurrently on two streams: both depend only on uvw, the
+        frequencies and the geometry, and neither fills the GPU alone.  Later
+        calls on the current stream see the plans."""
+        key = int(self.n_img_chan if g_nchan is None else g_nchan)
+        dmap = (np.arange(self.nchan) / self.nchan * key).astype(int)
+        if (self.shared_plan and key == self.n_img_chan
+                and np.array_equal(dmap, self._cm_host)):
+            need = lib().av_grid_tiled_workspace_size(self.nt, self.nb, self.nchan, self.nx,
+                                                      self.ny, self.n_img_chan, self.support)
+            ws = K.workspace(need)
+            check(lib().av_tiled_plan_shared(K.p(self.uvw), K.p(self.freq), K.p(self.chan_map),
+                                             self.nx, self.ny, self.cell[0], self.cell[1],
+                                             self.support, self.os, self.nt, self.nb,
+                                             self.nchan, self.n_img_chan, ws[1], ws[2],
+                                             K.stream_ptr()), "av_tiled_plan_shared")
+            self._gplan = ws
+            self._dplan = (key, ws)
+            return
         cur = torch.cuda.current_stream(self.dev)
         if getattr(self, "_side", None) is None:
             self._side = torch.cuda.Stream(self.dev)

@@ -196,6 +196,34 @@ int av_grid_tiled(void *grid, int grid_dtype, double *sum_weight, int do_psf,
                   int64_t nb, int64_t nchan, int64_t npol, int64_t n_img_chan,
                   int64_t n_img_pol, void *workspace, size_t workspace_bytes, void *stream);
 
+/* No counterpart in the reference: one plan for both av_grid_tiled_execute
+ * and av_degrid_tiled_execute (the gridder's and the degridder's binning
+ * differ only in their rounding, standard_grid.py:337-352 against
+ * standard_degrid.py:442-450).  Same arguments as av_grid_tiled_plan and the
+ * same workspace size (av_grid_tiled_workspace_size, or
+ * av_degrid_tiled_workspace_size with the same sizes).  Records are sorted
+ * by the gridder's cells; samples whose cell, offsets or bounds verdict differ
+ * under the degridder's half-even rounding are marked, and those it keeps are
+ * degridded separately in FP64 by av_degrid_tiled_execute, so both
+ * executes give what a plan of their own would (the degridder's values of
+ * those samples in FP64 instead of FP32).  Valid for a degrid of a grid of
+ * n_img_chan channels and (n_u, n_v) cells whose channel map
+ * int(i / nchan * n_img_chan) equals chan_map (continuum: all 0; cube: the
+ * identity), with the degridder's scale (-delta_l * n_u, -delta_m * n_v) and
+ * offset (n_u / 2, n_v / 2), as degrid_spheroid_ms4 passes them.  Not for
+ * av_degrid_tiled_adjoint.  At most 2^31 - 1 samples. */
+int av_tiled_plan_shared(const double *uvw, const double *freq, const int32_t *chan_map,
+                         int64_t n_u, int64_t n_v, double delta_l, double delta_m, int support,
+                         int oversampling, int64_t nt, int64_t nb, int64_t nchan,
+                         int64_t n_img_chan, void *workspace, size_t workspace_bytes,
+                         void *stream);
+/* No counterpart in the reference (diagnostics): out[0] = usable records of
+ * a tiled plan (gridder, degridder or shared), out[1] = samples a shared plan
+ * lists for the degridder's FP64 pass (0 for the others).  Synchronises. */
+int av_tiled_plan_counts(int64_t nt, int64_t nb, int64_t nchan, int64_t n_u, int64_t n_v,
+                         int64_t n_img_chan, int support, const void *workspace,
+                         size_t workspace_bytes, uint32_t *out, void *stream);
+
 /* ----------------------------------------------------------- degridding -- */
 /* dgrid_numba, standard_degrid.py:388-485: values (nt, nb, nvchan, nvpol) of
  * values_dtype (AV_C64 / AV_C128) += sum_k w_k grid_k conj(phasor) / sum_k w_k
