@@ -188,6 +188,7 @@ struct TiledDegridArgs {
   const Rec *recs;
   const uint32_t *tile_start;
   const uint32_t *n_rec;    // device: usable records (offs[n_keys])
+  const uint32_t *exc_mark; // device: a shared plan's marks (zero otherwise)
   int64_t n_rows;           // all samples (the plan also lists skipped ones)
   int64_t n_tiles, ntu, ntv, chunk;
   DegridArgs d;
@@ -230,15 +231,6 @@ __device__ void build_tap_tables_d(float *tab, double *rs, const double *cgk, in
   }
 }
 
-__device__ __forceinline__ int find_tile_d(const uint32_t *ts, int64_t n_tiles, uint32_t r) {
-  int64_t lo = 0, hi = n_tiles;
-  while (hi - lo > 1) {
-    int64_t mid = (lo + hi) >> 1;
-    if (ts[mid] <= r) lo = mid; else hi = mid;
-  }
-  return (int)lo;
-}
-
 __device__ __forceinline__ void put_value(const DegridArgs &d, int accumulate, int64_t k,
                                           double vr, double vi) {
   if (d.values_c128) {
@@ -267,10 +259,11 @@ __device__ __forceinline__ void put_value(const DegridArgs &d, int accumulate, i
 template <int NPG>
 __device__ __forceinline__ void degrid_write(const TiledDegridArgs &a, const DegridArgs &d,
                                              const double *rs, const int (&pmv)[8],
-                                             const Rec &rc, const float2 (&acc)[NPG]) {
+                                             const Rec &rc, bool marked,
+                                             const float2 (&acc)[NPG]) {
   const double norm = rs[rc.ou] * rs[rc.ov];
-  const int64_t row_i = rc.row & ~REC_DEGRID_EXC;
-  if (rc.row & REC_DEGRID_EXC) {
+  const int64_t row_i = rc.row;
+  if (marked) {
     // a shared plan's sample whose degridder convention differs: zeros in
     // store mode (k_degrid_exceptions then writes the ones the degridder
     // keeps), nothing when accumulating
@@ -340,6 +333,44 @@ __device__ __forceinline__ void degrid_write(const TiledDegridArgs &a, const Deg
   }
 }
 
+// Stages a tile's sub-grid (W x W cells from tile (tu, tv) of `plane`, the
+// NPG grid polarisations interleaved per cell, zero outside the grid) into
+// shared memory as float2.  SUB_UNROLL loads per thread are issued before
+// their stores, so a thread has several grid reads in flight.  The loop trip
+// count is the same for the whole block.
+constexpr int SUB_UNROLL = 4;
+
+template <int W, int NPG, int THREADS>
+__device__ __forceinline__ void stage_subgrid(const DegridArgs &d, float2 *sub, int64_t plane,
+                                              int tu, int tv, int64_t gplane) {
+  constexpr int N = W * W * NPG;
+  for (int i0 = 0; i0 < N; i0 += THREADS * SUB_UNROLL) {
+    float2 v[SUB_UNROLL];
+#pragma unroll
+    for (int k = 0; k < SUB_UNROLL; ++k) {
+      const int i = i0 + k * THREADS + (int)threadIdx.x;
+      v[k] = make_float2(0.f, 0.f);
+      const int cell = i / NPG, gp = i - cell * NPG;
+      const int iu = cell / W, iv = cell - iu * W;
+      const int64_t gu = (int64_t)tu * TILE + iu, gv = (int64_t)tv * TILE + iv;
+      if (i < N && gp < d.g_npol && gu < d.g_n2 && gv < d.g_n3) {
+        const int64_t gi = (plane * d.g_npol + gp) * gplane + gu * d.g_n3 + gv;
+        if (d.grid_c128) {
+          const double2 x = ((const double2 *)d.grid)[gi];
+          v[k] = make_float2((float)x.x, (float)x.y);
+        } else {
+          v[k] = ((const float2 *)d.grid)[gi];
+        }
+      }
+    }
+#pragma unroll
+    for (int k = 0; k < SUB_UNROLL; ++k) {
+      const int i = i0 + k * THREADS + (int)threadIdx.x;
+      if (i < N) sub[i] = v[k];
+    }
+  }
+}
+
 template <int S, int NPG>
 __global__ void __launch_bounds__(DT_THREADS) k_degrid_tiled(TiledDegridArgs a) {
   using M = DSmem<S, NPG>;
@@ -385,7 +416,7 @@ __global__ void __launch_bounds__(DT_THREADS) k_degrid_tiled(TiledDegridArgs a) 
   const uint32_t v1 = min(r1, n_rec);
   if (r0 >= v1) continue;
 
-  int t = find_tile_d(a.tile_start, a.n_tiles, r0);
+  int t = find_tile_warp(a.tile_start, a.n_tiles, r0);
   uint32_t seg_lo = r0;
   while (seg_lo < v1) {
     uint32_t t_end = a.tile_start[t + 1];
@@ -398,44 +429,42 @@ __global__ void __launch_bounds__(DT_THREADS) k_degrid_tiled(TiledDegridArgs a) 
     const int64_t trem = t - plane * a.ntu * a.ntv;
     const int tu = (int)(trem / a.ntv), tv = (int)(trem - (int64_t)tu * a.ntv);
     __syncthreads();  // previous segment's readers are done with sub
-    // stage the sub-grid, polarisations interleaved per cell (zero outside)
-    for (int i0 = 0; i0 < W * W * NPG; i0 += DT_THREADS) {
-      const int i = i0 + threadIdx.x;
-      if (i >= W * W * NPG) continue;
-      int cell = i / NPG, gp = i - cell * NPG;
-      int iu = cell / W, iv = cell - iu * W;
-      int64_t gu = (int64_t)tu * TILE + iu, gv = (int64_t)tv * TILE + iv;
-      float2 v = make_float2(0.f, 0.f);
-      if (gp < d.g_npol && gu < d.g_n2 && gv < d.g_n3) {
-        int64_t gi = (plane * d.g_npol + gp) * gplane + gu * d.g_n3 + gv;
-        if (d.grid_c128) {
-          double2 x = ((const double2 *)d.grid)[gi];
-          v = make_float2((float)x.x, (float)x.y);
-        } else {
-          v = ((const float2 *)d.grid)[gi];
-        }
-      }
-      sub[i] = v;
-    }
+    stage_subgrid<W, NPG, DT_THREADS>(d, sub, plane, tu, tv, gplane);
     __syncthreads();
     // each thread takes a pair of consecutive records: cell-sorted records
     // usually share the cell, and then one read of the footprint serves
     // both samples; a pair that straddles two cells reads the second
     // footprint with loads predicated on the lanes that need it
+    // records (and whether a shared plan marks them for the degridder's FP64
+    // pass) are loaded one step ahead
     Rec nxa, nxb;
+    bool nma = false, nmb = false;
     {
       const uint32_t r = seg_lo + 2 * threadIdx.x;
-      if (r < seg_hi) nxa = a.recs[r];
-      if (r + 1 < seg_hi) nxb = a.recs[r + 1];
+      if (r < seg_hi) {
+        nxa = a.recs[r];
+        nma = degrid_marked(a.exc_mark, r);
+      }
+      if (r + 1 < seg_hi) {
+        nxb = a.recs[r + 1];
+        nmb = degrid_marked(a.exc_mark, r + 1);
+      }
     }
     // one trip count per block, so every warp reaches the next barrier converged
     for (uint32_t rb = seg_lo; rb < seg_hi; rb += 2 * DT_THREADS) {
       const uint32_t r = rb + 2 * threadIdx.x;
       const Rec ra = nxa, rbx = nxb;
+      const bool ma = nma, mb = nmb;
       {
         const uint32_t rn = r + 2 * DT_THREADS;
-        if (rn < seg_hi) nxa = a.recs[rn];
-        if (rn + 1 < seg_hi) nxb = a.recs[rn + 1];
+        if (rn < seg_hi) {
+          nxa = a.recs[rn];
+          nma = degrid_marked(a.exc_mark, rn);
+        }
+        if (rn + 1 < seg_hi) {
+          nxb = a.recs[rn + 1];
+          nmb = degrid_marked(a.exc_mark, rn + 1);
+        }
       }
       if (r >= seg_hi) continue;
       const bool has_b = r + 1 < seg_hi;
@@ -500,8 +529,8 @@ __global__ void __launch_bounds__(DT_THREADS) k_degrid_tiled(TiledDegridArgs a) 
           accb[gp] = __ffma2_rn(make_float2(cub[i], cub[i]), rowb[gp], accb[gp]);
         }
       }
-      degrid_write<NPG>(a, d, rs, pmv, ra, acca);
-      if (has_b) degrid_write<NPG>(a, d, rs, pmv, rcb, accb);
+      degrid_write<NPG>(a, d, rs, pmv, ra, ma, acca);
+      if (has_b) degrid_write<NPG>(a, d, rs, pmv, rcb, mb, accb);
     }
     seg_lo = seg_hi;
     if (seg_hi == t_end) ++t;
@@ -636,7 +665,7 @@ __global__ void __launch_bounds__(TC_THREADS, 2) k_degrid_tc(TiledDegridArgs a) 
     const uint32_t v1 = min(r1, n_rec);
     if (r0 >= v1) continue;
 
-    int tt = find_tile_d(a.tile_start, a.n_tiles, r0);
+    int tt = find_tile_warp(a.tile_start, a.n_tiles, r0);
     uint32_t seg_lo = r0;
     while (seg_lo < v1) {
       const uint32_t t_end = a.tile_start[tt + 1];
@@ -649,24 +678,7 @@ __global__ void __launch_bounds__(TC_THREADS, 2) k_degrid_tc(TiledDegridArgs a) 
       const int64_t trem = tt - plane * a.ntu * a.ntv;
       const int tu = (int)(trem / a.ntv), tv = (int)(trem - (int64_t)tu * a.ntv);
       __syncthreads();  // previous segment's readers are done with sub
-      for (int i0 = 0; i0 < W * W * 4; i0 += TC_THREADS) {
-        const int i = i0 + threadIdx.x;
-        if (i >= W * W * 4) continue;
-        const int cell = i >> 2, gp = i & 3;
-        const int iu = cell / W, iv = cell - iu * W;
-        const int64_t gu = (int64_t)tu * TILE + iu, gv = (int64_t)tv * TILE + iv;
-        float2 v = make_float2(0.f, 0.f);
-        if (gp < d.g_npol && gu < d.g_n2 && gv < d.g_n3) {
-          const int64_t gi = (plane * d.g_npol + gp) * gplane + gu * d.g_n3 + gv;
-          if (d.grid_c128) {
-            const double2 x = ((const double2 *)d.grid)[gi];
-            v = make_float2((float)x.x, (float)x.y);
-          } else {
-            v = ((const float2 *)d.grid)[gi];
-          }
-        }
-        sub[i] = v;
-      }
+      stage_subgrid<W, 4, TC_THREADS>(d, sub, plane, tu, tv, gplane);
       __syncthreads();
 
       // this warp's slice of the segment, in rounds of 64 records (two per
@@ -684,27 +696,49 @@ __global__ void __launch_bounds__(TC_THREADS, 2) k_degrid_tc(TiledDegridArgs a) 
       uint32_t bh[8][2], bl[8][2];
 #pragma unroll
       for (int q = 0; q < 8; ++q) bh[q][0] = bh[q][1] = bl[q][0] = bl[q][1] = 0u;
+      // records and their mark words (a shared plan's samples marked for
+      // the degridder's FP64 pass) are loaded one round ahead
       Rec na, nb;
-      if (w_lo + lane < w_hi) na = a.recs[w_lo + lane];
-      if (w_lo + 32 + lane < w_hi) nb = a.recs[w_lo + 32 + lane];
+      uint32_t nma = 0u, nmb = 0u;
+      if (w_lo + lane < w_hi) {
+        na = a.recs[w_lo + lane];
+        nma = __ldg(a.exc_mark + ((w_lo + lane) >> 5));
+      }
+      if (w_lo + 32 + lane < w_hi) {
+        nb = a.recs[w_lo + 32 + lane];
+        nmb = __ldg(a.exc_mark + ((w_lo + 32 + lane) >> 5));
+      }
       for (int rd = 0; rd < n_rounds; ++rd) {
         const uint32_t r = w_lo + (uint32_t)rd * TC_ROUND + lane;
         const bool va = r < w_hi, vb = r + 32 < w_hi;
         const Rec ra = na, rb = nb;
-        if (r + TC_ROUND < w_hi) na = a.recs[r + TC_ROUND];
-        if (r + TC_ROUND + 32 < w_hi) nb = a.recs[r + TC_ROUND + 32];
+        const uint32_t ma = nma, mb = nmb;
+        if (r + TC_ROUND < w_hi) {
+          na = a.recs[r + TC_ROUND];
+          nma = __ldg(a.exc_mark + ((r + TC_ROUND) >> 5));
+        }
+        if (r + TC_ROUND + 32 < w_hi) {
+          nb = a.recs[r + TC_ROUND + 32];
+          nmb = __ldg(a.exc_mark + ((r + TC_ROUND + 32) >> 5));
+        }
         const int ka = va ? ((int)ra.du | ((int)ra.dv << 8)) : -1;
         const int kb = vb ? ((int)rb.du | ((int)rb.dv << 8)) : -1;
         __syncwarp();  // the previous round's groups are done with the staging area
+        // staged records carry a shared plan's mark in the row's top bit (the
+        // host runs this kernel only for fewer than 2^31 rows)
         if (va) {
           const double norm = rs[ra.ou] * rs[ra.ov];
           // 1 / norm in FP64, the scaling in FP32; zero-norm samples get 0
-          wrec[lane] = ra;
+          Rec x = ra;
+          if ((ma >> (r & 31u)) & 1u) x.row |= REC_DEGRID_EXC;
+          wrec[lane] = x;
           winv[lane] = norm != 0.0 ? (float)(1.0 / norm) : 0.f;
         }
         if (vb) {
           const double norm = rs[rb.ou] * rs[rb.ov];
-          wrec[lane + 32] = rb;
+          Rec x = rb;
+          if ((mb >> ((r + 32) & 31u)) & 1u) x.row |= REC_DEGRID_EXC;
+          wrec[lane + 32] = x;
           winv[lane + 32] = norm != 0.0 ? (float)(1.0 / norm) : 0.f;
         }
         int pa = __shfl_up_sync(FULL, ka, 1);
@@ -792,15 +826,15 @@ __global__ void __launch_bounds__(TC_THREADS, 2) k_degrid_tc(TiledDegridArgs a) 
             // a shared plan's marked sample gets 0 here (k_degrid_exceptions
             // writes the ones the degridder keeps)
             float2 *out = (float2 *)d.values;
-            const bool mg = (recg.row & REC_DEGRID_EXC) == 0u;
-            const bool mh = (rech.row & REC_DEGRID_EXC) == 0u;
+            const bool ug = (recg.row & REC_DEGRID_EXC) == 0u;
+            const bool uh = (rech.row & REC_DEGRID_EXC) == 0u;
             if (vg)
               out[(int64_t)(recg.row & ~REC_DEGRID_EXC) * 4 + t] =
-                  (src >= 0 && mg) ? make_float2(__fmul_rn(xgre, invg), __fmul_rn(xgim, invg))
+                  (src >= 0 && ug) ? make_float2(__fmul_rn(xgre, invg), __fmul_rn(xgim, invg))
                                    : make_float2(0.f, 0.f);
             if (vh)
               out[(int64_t)(rech.row & ~REC_DEGRID_EXC) * 4 + t] =
-                  (src >= 0 && mh) ? make_float2(__fmul_rn(xhre, invh), __fmul_rn(xhim, invh))
+                  (src >= 0 && uh) ? make_float2(__fmul_rn(xhre, invh), __fmul_rn(xhim, invh))
                                    : make_float2(0.f, 0.f);
           }
           j = j1;
@@ -975,7 +1009,9 @@ static int degrid_dispatch_npg(const TiledDegridArgs &a, int npg, int64_t nb, cu
     const int64_t lanes = tune_value(AV_TUNE_DEGRID_LANES);
     const bool tf32 =
         lanes == AV_DEGRID_LANES_TF32 || (lanes == AV_DEGRID_LANES_AUTO && S >= 7);
-    if (a.fast_out && a.d.g_npol == 4 && tf32) return launch_degrid_tc<S>(a, nb, st);
+    // the TF32 kernel keeps a shared plan's marks in the staged rows' top bit
+    if (a.fast_out && a.d.g_npol == 4 && tf32 && a.n_rows < (int64_t)REC_DEGRID_EXC)
+      return launch_degrid_tc<S>(a, nb, st);
   }
   return launch_degrid_tiled<S, 4>(a, nb, st);
 }
@@ -1167,6 +1203,7 @@ int av_degrid_tiled_execute(const double *dphase, void *values, int values_dtype
   a.recs = p.recs;
   a.tile_start = p.tile_start;
   a.n_rec = p.offs + g.n_keys();
+  a.exc_mark = p.exc_mark;
   a.n_tiles = g.n_tiles();
   a.ntu = g.ntu;
   a.ntv = g.ntv;

@@ -324,16 +324,6 @@ __device__ void build_tap_tables64(double *tab, double *rs, const double *cgk, i
   }
 }
 
-__device__ __forceinline__ int find_tile(const uint32_t *ts, int64_t n_tiles, uint32_t r) {
-  // largest t in [0, n_tiles) with ts[t] <= r (ts[n_tiles] = total > r)
-  int64_t lo = 0, hi = n_tiles;
-  while (hi - lo > 1) {
-    int64_t mid = (lo + hi) >> 1;
-    if (ts[mid] <= r) lo = mid; else hi = mid;
-  }
-  return (int)lo;
-}
-
 // One staged sample in registers (loads in flight until used).
 template <int NPOL>
 struct Pref {
@@ -655,7 +645,7 @@ __global__ void __launch_bounds__(GCfg<S, NPOL>::THREADS, 1) k_grid_tiled(TiledG
     if (ch >= n_chunks) break;
     const uint32_t r0 = (uint32_t)(ch * a.chunk);
     const uint32_t r1 = (uint32_t)min((int64_t)n_rec, (int64_t)r0 + a.chunk);
-    int t = find_tile(a.tile_start, a.n_tiles, r0);
+    int t = find_tile_warp(a.tile_start, a.n_tiles, r0);
     uint32_t seg_lo = r0;
     while (seg_lo < r1) {
       const uint32_t t_end = a.tile_start[t + 1];
@@ -684,11 +674,11 @@ __global__ void __launch_bounds__(GCfg<S, NPOL>::THREADS, 1) k_grid_tiled(TiledG
       {
         const uint32_t r = w_lo + lane;
         Rec r0;
-        if (r < w_hi) r0 = grid_rec(a.recs, r);
+        if (r < w_hi) r0 = a.recs[r];
         prefetch<NPOL>(pf, a, r0, r < w_hi);
       }
       bool rnext_ok = w_lo + GT_STAGE + lane < w_hi;
-      if (rnext_ok) rnext = grid_rec(a.recs, w_lo + GT_STAGE + lane);
+      if (rnext_ok) rnext = a.recs[w_lo + GT_STAGE + lane];
       for (int rd = 0; rd < n_rounds; ++rd) {
         // ---- stage this round's samples, one per lane: FP64 weighted
         // values, the cell key and the offsets of the two tap-table rows
@@ -725,7 +715,7 @@ __global__ void __launch_bounds__(GCfg<S, NPOL>::THREADS, 1) k_grid_tiled(TiledG
           prefetch<NPOL>(pf, a, rnext, rnext_ok);
           const uint32_t r = w_lo + (uint32_t)(rd + 2) * GT_STAGE + lane;
           rnext_ok = r < w_hi;
-          if (rnext_ok) rnext = grid_rec(a.recs, r);
+          if (rnext_ok) rnext = a.recs[r];
         }
         // ---- compute the round's samples in runs of one cell
         const int jn = (int)min((uint32_t)GT_STAGE, w_hi - (w_lo + (uint32_t)rd * GT_STAGE));
@@ -907,7 +897,7 @@ __global__ void __launch_bounds__(MCfg<S, NPOL>::THREADS, 1) k_grid_mma(TiledGri
     if (ch >= n_chunks) break;
     const uint32_t r0 = (uint32_t)(ch * a.chunk);
     const uint32_t r1 = (uint32_t)min((int64_t)n_rec, (int64_t)r0 + a.chunk);
-    int t = find_tile(a.tile_start, a.n_tiles, r0);
+    int t = find_tile_warp(a.tile_start, a.n_tiles, r0);
     uint32_t seg_lo = r0;
     while (seg_lo < r1) {
       const uint32_t t_end = a.tile_start[t + 1];
@@ -934,7 +924,7 @@ __global__ void __launch_bounds__(MCfg<S, NPOL>::THREADS, 1) k_grid_mma(TiledGri
       auto load_rec = [&](int rd) {
         const uint32_t r = w_lo + (uint32_t)rd * GT_STAGE + lane;
         Rec x;
-        if (rd < n_rounds && r < w_hi) x = grid_rec(a.recs, r);
+        if (rd < n_rounds && r < w_hi) x = a.recs[r];
         else x.row = 0xffffffffu;
         return x;
       };

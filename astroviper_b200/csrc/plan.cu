@@ -68,8 +68,9 @@ __device__ __forceinline__ uint32_t sample_key(const PlanGeom &g, double um, dou
 // offsets, so only its bounds tests (against the reference's swapped
 // extents, standard_degrid.py:457-462) are evaluated, in integers.
 // Otherwise the degridder's position is computed exactly.  A record the
-// degridder cannot use as it stands gets REC_DEGRID_EXC; `exc` says the
-// degridder keeps the sample, so it goes to the exception list.
+// degridder cannot use as it stands gets REC_DEGRID_EXC in its walk-order
+// row (k_plan_scatter moves it to exc_mark); `exc` says the degridder keeps
+// the sample, so it goes to the exception list.
 __device__ __forceinline__ uint32_t sample_key_shared(const PlanGeom &g, double um, double vm,
                                                       double us0, double us1, double f,
                                                       int plane, uint32_t row, uint2 &rec,
@@ -183,7 +184,8 @@ constexpr int SC = 4;
 __global__ void __launch_bounds__(256) k_plan_scatter(PlanGeom g,
                                                       const uint32_t *__restrict__ walk_key,
                                                       const uint2 *__restrict__ walk_rec,
-                                                      uint32_t *cursor, uint2 *recs) {
+                                                      uint32_t *cursor, uint2 *recs,
+                                                      uint32_t *exc_mark) {
   const int lane = threadIdx.x & 31;
   const uint32_t n_warps = (gridDim.x * blockDim.x) >> 5;
   const uint32_t nt = (uint32_t)g.nt, nb = (uint32_t)g.nb, nchan = (uint32_t)g.nchan;
@@ -220,7 +222,14 @@ __global__ void __launch_bounds__(256) k_plan_scatter(PlanGeom g,
         const unsigned leaders = __ballot_sync(0xffffffffu, lead[k]);
         const int ll = 31 - __clz(leaders & below);
         const uint32_t p = __shfl_sync(0xffffffffu, pos[k], ll & 31) + (uint32_t)(lane - ll);
-        if (in[k]) recs[p] = rec[k];
+        if (in[k]) {
+          uint2 r = rec[k];
+          if (g.convention == 2 && (r.x & REC_DEGRID_EXC)) {  // rare
+            r.x &= ~REC_DEGRID_EXC;
+            atomicOr(exc_mark + (p >> 5), 1u << (p & 31u));
+          }
+          recs[p] = r;
+        }
       }
     }
   }
@@ -360,12 +369,14 @@ bool plan_carve(const PlanGeom &g, Workspace &ws, Plan &p) {
   p.walk_rec = ws.take<Rec>(g.n_rows > 0 ? g.n_rows : 1);
   p.exc_count = ws.take<uint32_t>(4);
   p.exc_rows = ws.take<uint32_t>(g.n_rows > 0 ? g.n_rows : 1);
+  p.exc_mark = ws.take<uint32_t>((g.n_rows > 0 ? g.n_rows : 1) / 32 + 2);
   p.uv = ws.take<double2>(g.nt * g.nb > 0 ? g.nt * g.nb : 1);
   p.freq = ws.take<double>(g.nchan > 0 ? g.nchan : 1);
   p.chan_map = ws.take<int32_t>(g.nchan > 0 ? g.nchan : 1);
   p.dpar = ws.take<double>(4);
   return p.offs && p.cursor && p.tile_start && p.recs && p.scale && p.scan_tmp &&
-         p.counters && p.walk_key && p.walk_rec && p.exc_count && p.exc_rows && p.uv &&
+         p.counters && p.walk_key && p.walk_rec && p.exc_count && p.exc_rows && p.exc_mark &&
+         p.uv &&
          p.freq && p.chan_map && p.dpar;
 }
 
@@ -404,6 +415,8 @@ int plan_build(const PlanGeom &g, Plan &p, const double *uvw, const double *freq
   }
   AV_CUDA(cudaMemsetAsync(p.cursor, 0, sizeof(uint32_t) * (nk + 2), st));
   AV_CUDA(cudaMemsetAsync(p.exc_count, 0, sizeof(uint32_t) * 4, st));
+  AV_CUDA(cudaMemsetAsync(p.exc_mark, 0,
+                          sizeof(uint32_t) * ((g.n_rows > 0 ? g.n_rows : 1) / 32 + 2), st));
   if (g.convention == 2) {
     const int64_t n = std::max<int64_t>(g.nt * g.nb, g.nchan);
     if (n > 0) {
@@ -433,7 +446,7 @@ int plan_build(const PlanGeom &g, Plan &p, const double *uvw, const double *freq
   if (rc) return rc;
   if (g.n_rows > 0) {
     k_plan_scatter<<<(unsigned)blocks, 256, 0, st>>>(g, p.walk_key, (const uint2 *)p.walk_rec,
-                                                    p.cursor, (uint2 *)p.recs);
+                                                    p.cursor, (uint2 *)p.recs, p.exc_mark);
     AV_LAUNCH_CHECK();
   }
   int64_t nt = g.n_tiles() + 1;

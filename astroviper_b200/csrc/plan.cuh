@@ -21,11 +21,10 @@
 // records are sorted by the gridder's key (int(x + 0.5) rounding,
 // standard_grid.py:337-352), and the samples whose cell, kernel offsets or
 // bounds verdict differ under the degridder's half-even rounding
-// (standard_degrid.py:435-462) are marked for it: their records carry
-// REC_DEGRID_EXC in the row's top bit (the gridder masks it off; the
-// degridder writes zero there or skips them), and those the degridder keeps
-// are listed in exc_rows, which a small FP64 kernel degrids after the tiled
-// one.  The degridder's position is computed exactly only for samples near a
+// (standard_degrid.py:435-462) are marked for it in a bitmap of record
+// positions, exc_mark (the degridder writes zero there or skips them; the
+// gridder never reads it), and those the degridder keeps are listed in
+// exc_rows, which a small FP64 kernel degrids after the tiled one.  The degridder's position is computed exactly only for samples near a
 // rounding boundary (see sample_key_shared in plan.cu); elsewhere the two
 // conventions provably agree.
 #pragma once
@@ -37,9 +36,15 @@ constexpr int TILE = 32;                       // tile edge in cells
 constexpr int SCAN_MAX_BLOCKS = 65536;                    // scan partials
 constexpr int64_t KEY_BUDGET = (int64_t(1) << 28) - 65536;  // scan capacity: 65536 x 4096 keys
 
-// top bit of Rec::row in a shared plan: the degridder's convention differs
-// for this sample (never set in a plan of one convention)
+// While a shared plan is built, the top bit of a walk-order record's row
+// marks a sample whose degridder convention differs; the scatter pass moves
+// the mark into exc_mark, so sorted records carry plain rows.
 constexpr uint32_t REC_DEGRID_EXC = 0x80000000u;
+
+// Whether sorted record r is marked for the degridder (exc_mark bit r).
+__device__ __forceinline__ bool degrid_marked(const uint32_t *exc_mark, uint32_t r) {
+  return (__ldg(exc_mark + (r >> 5)) >> (r & 31u)) & 1u;
+}
 
 struct __align__(8) Rec {
   uint32_t row;     // (t * nb + b) * nchan + c
@@ -47,11 +52,24 @@ struct __align__(8) Rec {
   uint8_t ou, ov;   // kernel offsets + 128
 };
 
-// A record as the gridder reads it: the degridder's mark cleared.
-__device__ __forceinline__ Rec grid_rec(const Rec *recs, uint32_t r) {
-  Rec x = recs[r];
-  x.row &= ~REC_DEGRID_EXC;
-  return x;
+// Tile of record r: the largest t in [0, n_tiles) with ts[t] <= r (ts[0] =
+// 0 <= r < ts[n_tiles]), searched by the calling warp 32 ways at a time: each
+// step probes 32 positions at once, so a plan of 4096 tiles takes 3
+// dependent loads instead of 12.  Every lane of the warp calls it, converged,
+// with the same r, and every lane gets the result.
+__device__ __forceinline__ int find_tile_warp(const uint32_t *ts, int64_t n_tiles, uint32_t r) {
+  const int lane = threadIdx.x & 31;
+  int64_t lo = 0, hi = n_tiles;  // ts[lo] <= r < ts[hi]
+  while (hi - lo > 1) {
+    const int64_t step = (hi - lo + 31) / 32;
+    const int64_t p = lo + (int64_t)(lane + 1) * step;
+    const bool le = p < hi && ts[p] <= r;
+    // ts does not decrease, so the probes at or below r are a prefix of lanes
+    const int cnt = __popc(__ballot_sync(0xffffffffu, le));
+    lo += (int64_t)cnt * step;
+    hi = min(hi, lo + step);
+  }
+  return (int)lo;
 }
 
 struct PlanGeom {
@@ -125,6 +143,7 @@ inline size_t plan_workspace_bytes(const PlanGeom &g) {
   const size_t nc = g.nchan > 0 ? (size_t)g.nchan : 1;
   b += Workspace::need(sizeof(uint32_t) * 4);
   b += Workspace::need(sizeof(uint32_t) * nr);
+  b += Workspace::need(sizeof(uint32_t) * (nr / 32 + 2));     // exc_mark
   b += Workspace::need(sizeof(double2) * ntb);
   b += Workspace::need(sizeof(double) * nc);
   b += Workspace::need(sizeof(int32_t) * nc);
@@ -145,6 +164,7 @@ struct Plan {
   Rec *walk_rec;       // n_rows: record of each sample in walk order (pass 1)
   uint32_t *exc_count; // [0]: degridder exceptions listed (0 unless shared)
   uint32_t *exc_rows;  // n_rows: their rows
+  uint32_t *exc_mark;  // bit per sorted record: the degridder must not use it
   double2 *uv;         // nt * nb: u, v of each (time, baseline) (shared only)
   double *freq;        // nchan (shared only)
   int32_t *chan_map;   // nchan (shared only)

@@ -213,3 +213,73 @@ def run(name, api):
             res = {"error": type(e).__name__, "msg": str(e).strip("'\"")}
         out.append(_py(res))
     return out
+
+
+# ----------------------------------------------------------------------------
+# Imaging-loop cases (imager.py:108-351): the inputs and parameters of the
+# loops that make_golden_imager.py runs through the oracle's loop with the
+# reference's own IterationController, merge_return_dicts and ReturnDict
+# (imager_loop.json), and that tests/test_imager_gpu.py runs through
+# astroviper_b200's run_imaging_loop.
+LOOP_CASES = ("default", "linear4", "circular2", "initial_model_threshold")
+
+
+def loop_inputs(n_time=16, n_chan=2, pol_scale=(1.0, 0.8)):
+    """64 antennas, n_time steps x 2016 baselines x n_chan channels
+    (1.3-1.5 GHz), point sources at half the small workload's offsets,
+    correlations scaled by pol_scale; a flagged stretch and a NaN uvw row."""
+    from astroviper_b200 import synthetic as S
+    W = S.workload_small(n_time=n_time)
+    uvw = W["uvw"].copy()
+    freq = np.linspace(1.3e9, 1.5e9, n_chan)
+    rng = np.random.default_rng(11)
+    flux, dx, dy = W["sources"]
+    l, m = S.source_lm(dx / 2, dy / 2, W["pixelincr"])
+    vis = S.point_source_vis(uvw, freq, len(pol_scale), flux, l, m, 0.01, rng)
+    # distinct correlations (e.g. YY fainter than XX), so Q (V) is not zero
+    vis = vis * np.asarray(pol_scale)
+    weight = np.ones(vis.shape)
+    flag = np.zeros(vis.shape, dtype=bool)
+    flag[3, 10:20] = True
+    uvw[5, 7, 0] = np.nan
+    return vis, uvw, weight, flag, freq, W["pixelincr"]
+
+
+def loop_params(cell):
+    return {"image_size": (128, 128), "cell_size": (abs(cell[0]), abs(cell[1])), "niter": 300,
+            "nmajor": 4, "cyclefactor": 1.5, "gain": 0.1, "threshold": 0.0,
+            "chan_mode": "cube"}
+
+
+def loop_case(name):
+    """(vis, uvw, weight, flag, freq, pols, params, initial_model) of a case."""
+    if name == "default":
+        vis, uvw, weight, flag, freq, cell = loop_inputs()
+        return vis, uvw, weight, flag, freq, ["XX", "YY"], loop_params(cell), None
+    scale = {"linear4": (1.0, 0.1, 0.05, 0.8), "circular2": (1.0, 0.7),
+             "initial_model_threshold": (1.0, 0.8)}[name]
+    pols = {"linear4": ["XX", "XY", "YX", "YY"], "circular2": ["RR", "LL"],
+            "initial_model_threshold": ["XX", "YY"]}[name]
+    vis, uvw, weight, flag, freq, cell = loop_inputs(n_time=12, pol_scale=scale)
+    params = loop_params(cell)
+    params.update(niter=120, nmajor=3)
+    init = None
+    if name == "circular2":
+        params["corr_type"] = "circular"
+    if name == "initial_model_threshold":
+        params.update(threshold=0.05, nmajor=6, niter=2000)
+        init = np.zeros((2, 2, 128, 128))
+        init[0, 0, 60, 64] = 0.3
+    return vis, uvw, weight, flag, freq, pols, params, init
+
+
+def loop_decisions(out):
+    """What a loop's controller decided (from the oracle loop's output dict):
+    its final state, the cycle niter and threshold of every major cycle, and
+    the merged ReturnDict (per plane, the per-cycle iterations, peaks and
+    fluxes the controller read)."""
+    ctl = out["controller"]
+    return {"state": _py(ctl.get_state()),
+            "cycles": [{"niter": int(c["niter"]), "threshold": float(c["threshold"])}
+                       for c in out["cycles"]],
+            "combined": _dump(out["combined"])}

@@ -9,6 +9,8 @@ Writes
 * imager_control.json: the results of every scenario of imager_ops.py run
   against the reference's ReturnDict, merge_return_dicts, readers and
   IterationController (return_dict.py, iteration_control.py);
+* imager_loop.json: the decisions of the reference's controller in the
+  oracle's imaging loop on each of imager_ops.LOOP_CASES;
 * imager.npz: inputs and outputs of the reference's corr_to_stokes,
   stokes_to_corr, image_corr_to_stokes and image_stokes_to_corr
   (corr_to_stokes.py), and PSF planes with the max_sidelobe of its
@@ -145,15 +147,35 @@ def sidelobe_cases(ns, rng):
     return d
 
 
+def loop(ns):
+    """The oracle's imaging loop (oracle/imager.py, imager.py:108-351 restated)
+    driven by the reference's own IterationController, merge_return_dicts and
+    ReturnDict on every imager_ops.LOOP_CASES case: the decisions the
+    reference's controller takes on the loop's actual peaks and sidelobes."""
+    import oracle.imager as OI
+    out = {}
+    for name in imager_ops.LOOP_CASES:
+        vis, uvw, weight, flag, freq, _pols, params, init = imager_ops.loop_case(name)
+        ctl = ns.ic.IterationController(niter=params["niter"], nmajor=params["nmajor"],
+                                        threshold=params["threshold"], gain=params["gain"],
+                                        cyclefactor=params["cyclefactor"])
+        res = OI.run_imaging_loop(vis, uvw, weight, flag, freq, params, ctl,
+                                  ns.ic.merge_return_dicts, ns.rd.ReturnDict, init)
+        out[name] = imager_ops.loop_decisions(res)
+    with open(os.path.join(HERE, "imager_loop.json"), "w") as f:
+        json.dump(out, f, indent=0, sort_keys=True)
+
+
 def main():
     ns = load_reference()
     control(ns)
+    loop(ns)
     rng = np.random.default_rng(20260110)
     d = {}
     d.update(stokes_cases(ns, rng))
     d.update(sidelobe_cases(ns, rng))
     np.savez_compressed(os.path.join(HERE, "imager.npz"), **d)
-    print("wrote imager_control.json and imager.npz")
+    print("wrote imager_control.json, imager_loop.json and imager.npz")
 
 
 if __name__ == "__main__":

@@ -6,13 +6,20 @@ the oracle's restatement of the loop, bit-for-bit in its integer decisions
 (iterations per cycle, stop codes) and within 1e-9 (FP64 mode) / 1e-4 (FP32
 mode) in its images, with the reference's side effects on the measurement
 set."""
+import json
+import os
+import sys
+
 import numpy as np
 import pytest
 import torch
 
 import oracle as O
 import oracle.imager as OI
-from conftest import golden
+from conftest import GOLDEN, golden
+
+sys.path.insert(0, GOLDEN)
+import imager_ops  # noqa: E402
 
 pytestmark = pytest.mark.gpu
 
@@ -181,28 +188,8 @@ class ImagingMS4:
         return k in self._d
 
 
-def _loop_inputs(n_time=16, n_chan=2, pol_scale=(1.0, 0.8)):
-    from astroviper_b200 import synthetic as S
-    W = S.workload_small(n_time=n_time)
-    uvw = W["uvw"].copy()
-    freq = np.linspace(1.3e9, 1.5e9, n_chan)
-    rng = np.random.default_rng(11)
-    flux, dx, dy = W["sources"]
-    l, m = S.source_lm(dx / 2, dy / 2, W["pixelincr"])
-    vis = S.point_source_vis(uvw, freq, len(pol_scale), flux, l, m, 0.01, rng)
-    # distinct correlations (e.g. YY fainter than XX), so Q (V) is not zero
-    vis = vis * np.asarray(pol_scale)
-    weight = np.ones(vis.shape)
-    flag = np.zeros(vis.shape, dtype=bool)
-    flag[3, 10:20] = True
-    uvw[5, 7, 0] = np.nan
-    return vis, uvw, weight, flag, freq, W["pixelincr"]
-
-
-def _params(cell):
-    return {"image_size": (128, 128), "cell_size": (abs(cell[0]), abs(cell[1])), "niter": 300,
-            "nmajor": 4, "cyclefactor": 1.5, "gain": 0.1, "threshold": 0.0,
-            "chan_mode": "cube"}
+_loop_inputs = imager_ops.loop_inputs
+_params = imager_ops.loop_params
 
 
 def _run_oracle(vis, uvw, weight, flag, freq, params, initial_model=None):
@@ -289,6 +276,47 @@ def test_imaging_loop_variants_match_oracle(case):
                                                       abs=1e-12)
     if ref["vis_model"] is not None:
         assert rel(ms["VISIBILITY_MODEL"].data, ref["vis_model"]) <= 1e-9
+
+
+def _close(a, b, tol):
+    if isinstance(b, list):
+        return isinstance(a, list) and len(a) == len(b) and all(
+            _close(x, y, tol) for x, y in zip(a, b))
+    if isinstance(b, float):
+        return a == pytest.approx(b, rel=tol, abs=tol)
+    return a == b
+
+
+@pytest.mark.parametrize("precision", ["fp64", "fp32"])
+@pytest.mark.parametrize("case", imager_ops.LOOP_CASES)
+def test_imaging_loop_decisions_match_reference_controller(case, precision):
+    """imager_loop.json holds what the reference's own IterationController,
+    merge_return_dicts and ReturnDict decided when they drove the oracle's
+    loop on the same inputs: this package's loop (its controller, on the
+    GPU's peaks and sidelobes) ends in the same controller state, with the
+    same iterations per plane and cycle, and the peaks, fluxes and sidelobes
+    the controller read agree to the precision mode's tolerance."""
+    from astroviper_b200.core.imaging.imager import run_imaging_loop
+    with open(os.path.join(GOLDEN, "imager_loop.json")) as f:
+        fix = json.load(f)[case]
+    vis, uvw, weight, flag, freq, pols, params, init = imager_ops.loop_case(case)
+    ms = ImagingMS4(vis, uvw, weight, flag, freq, pols)
+    _model, _resid, combined, ctl = run_imaging_loop(ms, params, initial_model=init,
+                                                     precision=precision)
+    assert imager_ops._py(ctl.get_state()) == fix["state"]
+    got = imager_ops._dump(combined)
+    assert [k for k, _ in got] == [k for k, _ in fix["combined"]]
+    # CLEAN runs in FP32 in both loops (as the reference's deconvolve selects
+    # it), so peaks and fluxes carry FP32 rounding even in the FP64 mode
+    tol = 1e-6 if precision == "fp64" else 2e-5
+    for (key, a), (_, b) in zip(got, fix["combined"]):
+        assert a["iter_done"] == b["iter_done"], key
+        assert a["niter"] == b["niter"] == fix["cycles"][-1]["niter"], key
+        # the fields the oracle loop records (the package's loop records the
+        # reference deconvolve's others besides)
+        assert set(b) <= set(a), key
+        for field in b:
+            assert _close(a[field], b[field], tol), (key, field, a[field], b[field])
 
 
 def test_imaging_loop_drop_in_steps():
