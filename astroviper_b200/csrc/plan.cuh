@@ -171,41 +171,53 @@ struct Plan {
   double *dpar;        // scale0, scale1, offset0, offset1 (shared only)
 };
 
-// Distance of x from the nearest integer.
-__device__ __forceinline__ double int_dist(double x) { return fabs(__dsub_rn(x, rint(x))); }
-
 // Margins that make the gridder's and the degridder's roundings agree (see
 // sample_key_shared in plan.cu): the two FP64 positions of a sample differ
 // by less than 1e-10 cells, its kernel-offset arguments by less than 3e-8.
 constexpr double CELL_SLACK = 1e-7, OFFSET_SLACK = 1e-5;
 
+// Whether x - k (x in [k, k + 1)) lies more than `slack` from both k and k + 1.
+__device__ __forceinline__ bool clear_of_integers(double frac, double slack) {
+  return frac > slack && frac < 1.0 - slack;
+}
+
 // Position of one sample in the gridder's convention (standard_grid.py:
 // 297-352): returns false when it is skipped.  fu/fv = first footprint cell.
-// With `safe`, also whether all four rounded quantities (the cells' and the
-// offsets' int(x + 0.5) arguments) lie more than CELL_SLACK / OFFSET_SLACK
-// from a rounding boundary.
+// ui = int(u_pos + 0.5) truncates; a kept sample has margin <= ui < n_u -
+// margin, which for margin >= 1 is margin <= u_pos + 0.5 < n_u - margin (for
+// margin 0 the lower bound is -1 < u_pos + 0.5), so the range is tested in
+// FP64 (NaN fails it) and only kept values are converted, to 32 bits.  The
+// offsets floor((ui - u_pos) * os + 0.5) convert once, rounding down.  With
+// `safe`, also whether all four rounded quantities (the cells' and the
+// offsets' arguments) lie more than CELL_SLACK / OFFSET_SLACK from a rounding
+// boundary, read from the fractional parts at hand.
 __device__ __forceinline__ bool sample_pos_grid(double um, double vm, double us0, double us1,
                                                 int64_t n_u, int64_t n_v, int support, int os,
                                                 int margin, int &fu, int &fv, int &offu,
                                                 int &offv, bool *safe = nullptr) {
-  double u = __dmul_rn(um, us0), v = __dmul_rn(vm, us1);
-  if (isnan(u) || isnan(v)) return false;
-  double u_pos = __dadd_rn(u, (double)(n_u / 2));
-  double v_pos = __dadd_rn(v, (double)(n_v / 2));
+  const double u = __dmul_rn(um, us0), v = __dmul_rn(vm, us1);
+  const double u_pos = __dadd_rn(u, (double)(n_u / 2));
+  const double v_pos = __dadd_rn(v, (double)(n_v / 2));
   const double au = __dadd_rn(u_pos, 0.5), av = __dadd_rn(v_pos, 0.5);
-  long long ui = trunc_ll(au), vi = trunc_ll(av);
-  const long long sc = support / 2, mg = margin;
-  if (!((ui + mg < n_u) && (vi + mg < n_v) && (ui - mg >= 0) && (vi - mg >= 0))) return false;
-  double uo = __dsub_rn((double)ui, u_pos), vo = __dsub_rn((double)vi, v_pos);
+  const double lo = margin > 0 ? (double)margin : -1.0;
+  const bool in_u = (margin > 0 ? au >= lo : au > lo) && au < (double)(n_u - margin);
+  const bool in_v = (margin > 0 ? av >= lo : av > lo) && av < (double)(n_v - margin);
+  if (!(in_u && in_v)) return false;
+  const int ui = __double2int_rz(au), vi = __double2int_rz(av);
+  const double dui = (double)ui, dvi = (double)vi;
+  const double uo = __dsub_rn(dui, u_pos), vo = __dsub_rn(dvi, v_pos);
   const double bu = __dadd_rn(__dmul_rn(uo, (double)os), 0.5);
   const double bv = __dadd_rn(__dmul_rn(vo, (double)os), 0.5);
-  offu = (int)floor(bu);
-  offv = (int)floor(bv);
-  fu = (int)(ui - sc);
-  fv = (int)(vi - sc);
+  offu = __double2int_rd(bu);
+  offv = __double2int_rd(bv);
+  const int sc = support / 2;
+  fu = ui - sc;
+  fv = vi - sc;
   if (safe)
-    *safe = int_dist(au) > CELL_SLACK && int_dist(av) > CELL_SLACK &&
-            int_dist(bu) > OFFSET_SLACK && int_dist(bv) > OFFSET_SLACK;
+    *safe = clear_of_integers(__dsub_rn(au, dui), CELL_SLACK) &&
+            clear_of_integers(__dsub_rn(av, dvi), CELL_SLACK) &&
+            clear_of_integers(__dsub_rn(bu, (double)offu), OFFSET_SLACK) &&
+            clear_of_integers(__dsub_rn(bv, (double)offv), OFFSET_SLACK);
   return true;
 }
 

@@ -115,8 +115,8 @@ def test_shared_plan_matches_separate_plans(kind, mode):
     assert n_rec_shared == n_rec_grid
     if kind == "ties":
         assert n_exc > 100  # the conventions part on the ties
-    # gridding: the same records (FP64 sums, flush order aside)
-    assert rel(g1, g0) <= 1e-15 and rel(s1, s0) <= 1e-15
+    # gridding: the same records; FP64 sums whose order the atomics set
+    assert rel(g1, g0) <= 1e-13 and rel(s1, s0) <= 1e-13
     # degridding: separate-plan results (FP32 path) within FP32 rounding, and
     # both against the FP64 oracle on the same grid
     assert rel(vs1, vs0) <= 2e-7
