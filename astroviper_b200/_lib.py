@@ -47,6 +47,10 @@ SIGNATURES = {
     "av_grid_tiled_workspace_size": (_sz, [_i64, _i64, _i64, _i64, _i64, _i64, _i]),
     "av_grid_tiled_plan": (_i, [_vp, _vp, _vp, _i64, _i64, _d, _d, _i, _i, _i64, _i64, _i64,
                                 _i64, _vp, _sz, _vp]),
+    "av_grid_tiled_plan_weighted": (_i, [_vp, _vp, _vp, _vp, _i64, _i64, _i64, _d, _d, _i, _i,
+                                         _i64, _i64, _i64, _i64, _vp, _sz, _vp]),
+    "av_grid_tiled_clear": (_i, [_vp, _i, _i64, _i64, _i64, _i, _i64, _i64, _i64, _i64, _vp,
+                                 _sz, _vp]),
     "av_tiled_plan_shared": (_i, [_vp, _vp, _vp, _i64, _i64, _d, _d, _i, _i, _i64, _i64, _i64,
                                   _i64, _vp, _sz, _vp]),
     "av_tiled_plan_counts": (_i, [_i64, _i64, _i64, _i64, _i64, _i64, _i, _vp, _sz, _vp, _vp]),

@@ -9,9 +9,15 @@ so the grids are uneven.
 The binning plan is built once from uvw / freq.  Every call then runs the
 persistent tiled gridder once over all grids: its CTAs take record chunks from
 one counter, so grids with few samples free their SMs for the others with no
-host involvement.  With ``graph=True`` the call (grid and sum-of-weight
-clearing plus the gridding launch) is captured as a CUDA graph on first use
-and replayed afterwards; inputs are copied into the graph's static buffers.
+host involvement.  With ``drop_flagged=True`` each call also bins its own
+batch's samples from the weights (av_grid_tiled_plan_weighted), leaving out
+those whose every weight is zero or NaN, so heavily flagged grids take less
+work.  Only the cells the plan can touch are cleared between calls
+(av_grid_tiled_clear); the rest of the grids stays zero from construction.
+With ``graph=True`` the call (the weighted plan when it applies, the clears and
+the gridding launch) is captured as a CUDA graph on first use and replayed
+afterwards; a replay takes a fresh batch of visibilities and weights for the
+uv coverage given at construction, copied into the graph's static buffers.
 Launch knobs come from the autotuner (astroviper_b200.autotune) when
 ``tune=True``.
 """
@@ -24,7 +30,12 @@ from ._lib import AV_C64, AV_F32, check, lib
 
 class BatchedGridder:
     def __init__(self, uvw, freq, image_size, cell_size, npol, support=7, oversampling=100,
-                 graph=True, tune=False, grid_dtype=torch.complex128):
+                 graph=True, tune=False, grid_dtype=torch.complex128, drop_flagged=False,
+                 alias_tol=1e-2):
+        """support: the kernel support, or "auto" for the smallest of 7 and 9
+        whose aliasing at the edge of the inner 80 % of the field is at most
+        alias_tol (autotune.choose_support; it changes the result, so it is an
+        explicit choice).  tune: let the autotuner choose the launch knobs."""
         self.dev = K.device()
         self.uvw = K.on_device(uvw, torch.float64)
         self.freq = K.on_device(freq, torch.float64)
@@ -33,9 +44,15 @@ class BatchedGridder:
         self.npol = int(npol)
         self.n_u, self.n_v = int(image_size[0]), int(image_size[1])
         self.cell = (float(cell_size[0]), float(cell_size[1]))
-        self.support, self.os = int(support), int(oversampling)
+        self.os = int(oversampling)
+        self.alias = None
+        if support == "auto":
+            from . import autotune
+            support, self.alias = autotune.choose_support((7, 9), self.os, alias_tol)
+        self.support = int(support)
         self.graph = bool(graph)
         self.tune = bool(tune)
+        self.drop_flagged = bool(drop_flagged)
         if self.npol < 1 or self.npol > 4:
             raise ValueError("npol must be in [1, 4]")
         self.chan_map = torch.arange(self.nchan, dtype=torch.int32, device=self.dev)
@@ -43,12 +60,16 @@ class BatchedGridder:
         self.cgk = K.pswf_table(self.os, self.support)
         need = lib().av_grid_tiled_workspace_size(self.nt, self.nb, self.nchan, self.n_u, self.n_v,
                                                   self.nchan, self.support)
+        # the plan of every sample: its tiles bound what any call can touch
         self._ws = K.workspace(need)
         check(lib().av_grid_tiled_plan(K.p(self.uvw), K.p(self.freq), K.p(self.chan_map),
                                        self.n_u, self.n_v, self.cell[0], self.cell[1],
                                        self.support, self.os, self.nt, self.nb, self.nchan,
                                        self.nchan, self._ws[1], self._ws[2], K.stream_ptr()),
               "av_grid_tiled_plan")
+        # each call's plan without its fully flagged samples
+        self._wws = K.workspace(need) if self.drop_flagged else None
+        self._cleared = True  # the grids are all zero until the first launch
         self.grid = torch.zeros((self.nchan, self.npol, self.n_u, self.n_v), dtype=grid_dtype,
                                 device=self.dev)
         self.sum_weight = torch.zeros((self.nchan, self.npol), dtype=torch.float64,
@@ -67,13 +88,27 @@ class BatchedGridder:
                             npol=self.npol, planes=self.nchan)
 
     def _launch(self, vis, wt):
-        self.grid.zero_()
+        if not self._cleared:
+            # only the cells the full plan can touch were ever written
+            check(lib().av_grid_tiled_clear(
+                K.p(self.grid), K.dcode(self.grid), self.npol, self.n_u, self.n_v, self.support,
+                self.nt, self.nb, self.nchan, self.nchan, self._ws[1], self._ws[2],
+                K.stream_ptr()), "av_grid_tiled_clear")
+        self._cleared = False
         self.sum_weight.zero_()
+        ws = self._ws
+        if self.drop_flagged:
+            ws = self._wws
+            check(lib().av_grid_tiled_plan_weighted(
+                K.p(self.uvw), K.p(self.freq), K.p(self.chan_map), K.p(wt), self.npol, self.n_u,
+                self.n_v, self.cell[0], self.cell[1], self.support, self.os, self.nt, self.nb,
+                self.nchan, self.nchan, ws[1], ws[2], K.stream_ptr()),
+                "av_grid_tiled_plan_weighted")
         check(lib().av_grid_tiled_execute(
             K.p(self.grid), K.dcode(self.grid), K.p(self.sum_weight), 0, K.p(vis), AV_C64,
             K.p(wt), AV_F32, K.p(self.pol_map), K.p(self.cgk), self.n_u, self.n_v, self.support,
             self.os, self.nt, self.nb, self.nchan, self.npol, self.nchan, self.npol,
-            self._ws[1], self._ws[2], K.stream_ptr()), "av_grid_tiled_execute")
+            ws[1], ws[2], K.stream_ptr()), "av_grid_tiled_execute")
 
     def _inputs(self, vis, weight):
         v = K.on_device(vis, torch.complex64).contiguous()

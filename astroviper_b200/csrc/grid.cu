@@ -1179,6 +1179,39 @@ int av_grid_tiled_plan(const double *uvw, const double *freq, const int32_t *cha
   return plan_build(g, p, uvw, freq, chan_map, delta_l, delta_m, as_stream(stream));
 }
 
+int av_grid_tiled_plan_weighted(const double *uvw, const double *freq, const int32_t *chan_map,
+                                const float *weight, int64_t npol, int64_t n_u, int64_t n_v,
+                                double delta_l, double delta_m, int support, int oversampling,
+                                int64_t nt, int64_t nb, int64_t nchan, int64_t n_img_chan,
+                                void *workspace, size_t workspace_bytes, void *stream) {
+  clear_error();
+  AV_CHECK_ARG(uvw && freq && chan_map && weight, "av_grid_tiled_plan_weighted: null pointer");
+  AV_CHECK_ARG(npol >= 1 && npol <= 4, "av_grid_tiled_plan_weighted: npol must be in [1, 4]");
+  PlanGeom g;
+  Plan p;
+  int rc = grid_geom_checked(g, n_u, n_v, support, oversampling, nt, nb, nchan, n_img_chan,
+                             workspace, workspace_bytes, p, "av_grid_tiled_plan_weighted");
+  if (rc) return rc;
+  return plan_build(g, p, uvw, freq, chan_map, delta_l, delta_m, as_stream(stream), weight,
+                    (int)npol);
+}
+
+int av_grid_tiled_clear(void *grid, int grid_dtype, int64_t n_img_pol, int64_t n_u, int64_t n_v,
+                        int support, int64_t nt, int64_t nb, int64_t nchan, int64_t n_img_chan,
+                        const void *workspace, size_t workspace_bytes, void *stream) {
+  clear_error();
+  AV_CHECK_ARG(grid, "av_grid_tiled_clear: null pointer");
+  AV_CHECK_ARG(grid_dtype == AV_C64 || grid_dtype == AV_C128,
+               "av_grid_tiled_clear: grid must be complex64 or complex128");
+  AV_CHECK_ARG(n_img_pol >= 1, "av_grid_tiled_clear: bad shape");
+  PlanGeom g;
+  Plan p;
+  int rc = grid_geom_checked(g, n_u, n_v, support, 100, nt, nb, nchan, n_img_chan,
+                             (void *)workspace, workspace_bytes, p, "av_grid_tiled_clear");
+  if (rc) return rc;
+  return plan_clear_tiles(g, p, grid, grid_dtype == AV_C128, n_img_pol, as_stream(stream));
+}
+
 int av_tiled_plan_shared(const double *uvw, const double *freq, const int32_t *chan_map,
                          int64_t n_u, int64_t n_v, double delta_l, double delta_m, int support,
                          int oversampling, int64_t nt, int64_t nb, int64_t nchan,

@@ -137,7 +137,9 @@ __global__ void __launch_bounds__(256) k_plan_count(PlanGeom g, const double *__
                                                     const int32_t *__restrict__ chan_map,
                                                     uint32_t *hist, uint32_t *walk_key,
                                                     uint2 *walk_rec, uint32_t *exc_count,
-                                                    uint32_t *exc_rows) {
+                                                    uint32_t *exc_rows,
+                                                    const float *__restrict__ drop_wt,
+                                                    int drop_npol) {
   const int lane = threadIdx.x & 31;
   const uint32_t n_warps = (gridDim.x * blockDim.x) >> 5;
   const uint32_t nt = (uint32_t)g.nt, nb = (uint32_t)g.nb, nchan = (uint32_t)g.nchan;
@@ -165,13 +167,35 @@ __global__ void __launch_bounds__(256) k_plan_count(PlanGeom g, const double *__
           if (exc) exc_rows[atomicAdd(exc_count, 1u)] = tb * nchan + c;  // rare
         } else {
           key = sample_key(g, um, vm, us0, us1, f, plane, tb * nchan + c, rec);
+          if (drop_wt != nullptr && key != (uint32_t)g.n_keys()) {
+            // a sample whose every weight is zero or NaN adds nothing: the
+            // reference skips zero and NaN weighted data (standard_grid.py:378)
+            const float *wr = drop_wt + (size_t)(tb * nchan + c) * drop_npol;
+            bool any = false;
+            for (int p = 0; p < drop_npol; ++p) {
+              const float x = wr[p];
+              any |= (x == x) && x != 0.f;
+            }
+            if (!any) {
+              key = (uint32_t)g.n_keys();
+              rec = make_uint2(tb * nchan + c, 0u);
+            }
+          }
         }
         walk_key[widx] = key;
         walk_rec[widx] = rec;
       }
       uint32_t len;
+      const uint32_t skip = (uint32_t)g.n_keys();
       const bool lead = run_leader(key, w.in, lane, len);
-      if (lead) atomicAdd(&hist[key], len);
+      if (lead && key != skip) atomicAdd(&hist[key], len);
+      // skipped samples (any order will do): one count per warp, and none in
+      // a gridder plan, which keeps no list of them - a weighted plan skips
+      // every fully flagged sample, and counting those per run would put
+      // millions of atomics on the one skip key
+      const unsigned sm = __ballot_sync(0xffffffffu, w.in && key == skip);
+      if (g.convention != 0 && sm != 0u && lane == __ffs(sm) - 1)
+        atomicAdd(&hist[skip], (uint32_t)__popc(sm));
     }
   }
 }
@@ -209,20 +233,33 @@ __global__ void __launch_bounds__(256) k_plan_scatter(PlanGeom g,
           rec[k] = walk_rec[widx];
         }
       }
+      const uint32_t skip = (uint32_t)g.n_keys();
+      unsigned smask[SC];
 #pragma unroll
       for (int k = 0; k < SC; ++k) {
         uint32_t len;
         lead[k] = run_leader(key[k], in[k], lane, len);
         pos[k] = 0;
-        if (lead[k]) pos[k] = atomicAdd(&cursor[key[k]], len);
+        if (lead[k] && key[k] != skip) pos[k] = atomicAdd(&cursor[key[k]], len);
+        // skipped samples: one cursor atomic per warp (degridder and shared
+        // plans; a gridder plan lists none)
+        smask[k] = __ballot_sync(0xffffffffu, in[k] && key[k] == skip);
+        if (g.convention != 0 && smask[k] != 0u && lane == __ffs(smask[k]) - 1)
+          pos[k] = atomicAdd(&cursor[skip], (uint32_t)__popc(smask[k]));
       }
 #pragma unroll
       for (int k = 0; k < SC; ++k) {
-        // each lane's run leader: the highest leader at or below it
-        const unsigned leaders = __ballot_sync(0xffffffffu, lead[k]);
+        // each lane's run leader: the highest leader at or below it; a
+        // skipped sample's place follows the warp's first skipped lane
+        const unsigned leaders = __ballot_sync(0xffffffffu, lead[k] && key[k] != skip);
         const int ll = 31 - __clz(leaders & below);
-        const uint32_t p = __shfl_sync(0xffffffffu, pos[k], ll & 31) + (uint32_t)(lane - ll);
-        if (in[k]) {
+        const int sl = smask[k] != 0u ? __ffs(smask[k]) - 1 : 0;
+        const uint32_t pr = __shfl_sync(0xffffffffu, pos[k], ll & 31) + (uint32_t)(lane - ll);
+        const uint32_t ps = __shfl_sync(0xffffffffu, pos[k], sl) +
+                            (uint32_t)__popc(smask[k] & (below >> 1));
+        const bool is_skip = key[k] == skip;
+        const uint32_t p = is_skip ? ps : pr;
+        if (in[k] && (!is_skip || g.convention != 0)) {
           uint2 r = rec[k];
           if (g.convention == 2 && (r.x & REC_DEGRID_EXC)) {  // rare
             r.x &= ~REC_DEGRID_EXC;
@@ -357,6 +394,37 @@ __global__ void k_tile_starts(const uint32_t *offs, int64_t n_tiles, int64_t kpt
   tile_start[t] = offs[t * kpt];
 }
 
+// Zeroes the cells a plan's records can touch: the (TILE + support - 1)^2
+// footprint region of every tile that holds records, all grid polarisations
+// (one CTA per tile; empty tiles return at once).  Neighbouring regions
+// overlap; they all write zero.
+__global__ void __launch_bounds__(256) k_clear_tiles(const uint32_t *tile_start, PlanGeom g,
+                                                     void *grid, int grid_c128, int64_t npg) {
+  const int64_t t = blockIdx.x;
+  if (t >= g.n_tiles() || tile_start[t + 1] == tile_start[t]) return;
+  const int64_t plane = t / (g.ntu * g.ntv);
+  const int64_t trem = t - plane * g.ntu * g.ntv;
+  const int64_t tu = trem / g.ntv, tv = trem - tu * g.ntv;
+  const int W = TILE + g.support - 1;
+  const int64_t n = (int64_t)W * W * npg;
+  for (int64_t i = threadIdx.x; i < n; i += blockDim.x) {
+    const int64_t gp = i / ((int64_t)W * W), cell = i - gp * W * W;
+    const int64_t gu = tu * TILE + cell / W, gv = tv * TILE + cell % W;
+    if (gu >= g.n_u || gv >= g.n_v) continue;
+    const int64_t gi = ((plane * npg + gp) * g.n_u + gu) * g.n_v + gv;
+    if (grid_c128) ((double2 *)grid)[gi] = make_double2(0.0, 0.0);
+    else ((float2 *)grid)[gi] = make_float2(0.f, 0.f);
+  }
+}
+
+int plan_clear_tiles(const PlanGeom &g, const Plan &p, void *grid, int grid_c128, int64_t npg,
+                     cudaStream_t st) {
+  if (g.n_tiles() == 0) return AV_OK;
+  k_clear_tiles<<<(unsigned)g.n_tiles(), 256, 0, st>>>(p.tile_start, g, grid, grid_c128, npg);
+  AV_LAUNCH_CHECK();
+  return AV_OK;
+}
+
 bool plan_carve(const PlanGeom &g, Workspace &ws, Plan &p) {
   p.offs = ws.take<uint32_t>(g.n_keys() + 2);
   p.cursor = ws.take<uint32_t>(g.n_keys() + 2);
@@ -402,7 +470,8 @@ __global__ void k_shared_copy(const double *uvw, int64_t ntb, const double *freq
 }
 
 int plan_build(const PlanGeom &g, Plan &p, const double *uvw, const double *freq,
-               const int32_t *chan_map, double delta_l, double delta_m, cudaStream_t st) {
+               const int32_t *chan_map, double delta_l, double delta_m, cudaStream_t st,
+               const float *drop_wt, int drop_npol) {
   int64_t nk = g.n_keys();
   if (nk >= (int64_t)0xffffffffu || g.n_rows >= (int64_t)0xffffffffu) {
     set_error("plan: %lld keys / %lld samples exceed 32-bit indexing", (long long)nk,
@@ -439,7 +508,7 @@ int plan_build(const PlanGeom &g, Plan &p, const double *uvw, const double *freq
   if (g.n_rows > 0) {
     k_plan_count<<<(unsigned)blocks, 256, 0, st>>>(g, uvw, freq, p.scale, chan_map, p.cursor,
                                                   p.walk_key, (uint2 *)p.walk_rec,
-                                                  p.exc_count, p.exc_rows);
+                                                  p.exc_count, p.exc_rows, drop_wt, drop_npol);
     AV_LAUNCH_CHECK();
   }
   int rc = scan_counts(p.cursor, p.offs, nk + 1, p.scan_tmp, st);

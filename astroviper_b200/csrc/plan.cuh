@@ -255,8 +255,16 @@ __device__ __forceinline__ bool sample_pos_degrid(double um, double vm, double f
 // exception count in exc_count[0]).  A shared plan (g.convention == 2) needs
 // the degridder's scale / offset / bounds extents in g as well as the
 // gridder's cell size (delta_l, delta_m).
+// With drop_wt (float32 weights, drop_npol per sample), samples whose every
+// weight is zero or NaN are left out of the records (gridder convention).
 int plan_build(const PlanGeom &g, Plan &p, const double *uvw, const double *freq,
-               const int32_t *chan_map, double delta_l, double delta_m, cudaStream_t st);
+               const int32_t *chan_map, double delta_l, double delta_m, cudaStream_t st,
+               const float *drop_wt = nullptr, int drop_npol = 0);
+
+// Zeroes the grid cells the plan's records can touch (every non-empty tile's
+// footprint region, all npg grid polarisations).
+int plan_clear_tiles(const PlanGeom &g, const Plan &p, void *grid, int grid_c128, int64_t npg,
+                     cudaStream_t st);
 
 // Carve a Plan out of the workspace.
 bool plan_carve(const PlanGeom &g, Workspace &ws, Plan &p);

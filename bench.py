@@ -539,9 +539,13 @@ def bench_batched(args, dev):
     496 time steps = 256 independent 1024^2 grids (cube mode, 2 arcsec
     cells), each with a flag fraction uniform in [0, 0.6) (zero weights).
     For support 7 and 9: the persistent gridder over all grids in one launch
-    replayed as a CUDA graph (launch knob from the autotuner), the same
-    launch without the graph, one launch per grid (plan per channel), and the
-    plain FP64 gridder; error of the batched grids against the FP64 ones."""
+    replayed as a CUDA graph (lane mapping and chunks per SM from the
+    autotuner; only the cells the plan can touch cleared between calls), the
+    same launch without the graph, the graph that also rebuilds the plan from
+    each batch's weights and leaves fully flagged samples out, one launch per
+    grid (plan per channel), and the plain FP64 gridder; error of the batched
+    grids against the FP64 ones.  Also the support the aliasing criterion
+    picks (support="auto")."""
     import torch
     from astroviper_b200 import _kernels as K
     from astroviper_b200 import autotune
@@ -570,8 +574,8 @@ def bench_batched(args, dev):
         r = {}
         B = BatchedGridder(W["uvw"], W["freq"], W["image_size"], W["pixelincr"], npol,
                            support=support, graph=True, tune=True)
-        B(vis, wt)  # tunes the launch knob, captures the graph
-        r["chunks_per_sm"] = autotune._applied.get(B.tune_key())
+        B(vis, wt)  # tunes the launch knobs, captures the graph
+        r["tuned"] = autotune._applied.get(B.tune_key())
         sv, sw = B.static_inputs()
         r["graph_ms"] = timed(lambda: B(sv, sw), 5)             # replay, inputs in place
         r["graph_with_input_copy_ms"] = timed(lambda: B(vis, wt), 3)
@@ -581,6 +585,17 @@ def bench_batched(args, dev):
         r["Mcorr_unflagged_per_s"] = out["corr_unflagged"] / (r["graph_ms"] / 1e3) / 1e6
         gb = B.grid.clone()
         del B
+        torch.cuda.empty_cache()
+        # the plan rebuilt from every batch's weights, fully flagged samples left out
+        Bd = BatchedGridder(W["uvw"], W["freq"], W["image_size"], W["pixelincr"], npol,
+                            support=support, graph=True, tune=True, drop_flagged=True)
+        Bd(vis, wt)
+        sv, sw = Bd.static_inputs()
+        r["drop_flagged_graph_ms"] = timed(lambda: Bd(sv, sw), 5)
+        r["drop_flagged_rel_diff"] = rel(Bd.grid, gb)
+        r["drop_flagged_Mcorr_unflagged_per_s"] = (out["corr_unflagged"] /
+                                                   (r["drop_flagged_graph_ms"] / 1e3) / 1e6)
+        del Bd
         torch.cuda.empty_cache()
         P = PerGridGridder(W["uvw"], W["freq"], W["image_size"], W["pixelincr"], npol,
                            support=support)
@@ -606,7 +621,12 @@ def bench_batched(args, dev):
         del v64, w64, t64, gb
         torch.cuda.empty_cache()
         out[f"support_{support}"] = r
-    del W, vis, wt
+    Ba = BatchedGridder(W["uvw"], W["freq"], W["image_size"], W["pixelincr"], npol,
+                        support="auto", graph=False)
+    out["support_auto"] = {"support": Ba.support, "alias_ratio": Ba.alias,
+                           "criterion": "aliasing at the edge of the inner 80 % of the field "
+                                        "<= 1e-2"}
+    del Ba, W, vis, wt
     torch.cuda.empty_cache()
     return out
 

@@ -196,6 +196,28 @@ int av_grid_tiled(void *grid, int grid_dtype, double *sum_weight, int do_psf,
                   int64_t nb, int64_t nchan, int64_t npol, int64_t n_img_chan,
                   int64_t n_img_pol, void *workspace, size_t workspace_bytes, void *stream);
 
+/* No counterpart in the reference: av_grid_tiled_plan that also leaves out
+ * the samples whose every weight is zero or NaN (flagged data), which
+ * standard_grid_jit skips (standard_grid.py:378), so that grids with many
+ * flagged samples take less work.  weight (nt, nb, nchan, npol) float32, as
+ * the execute will read it: the plan then holds for those weights only (a
+ * fresh set of flags needs a fresh plan).  Same workspace as
+ * av_grid_tiled_plan; for av_grid_tiled_execute only. */
+int av_grid_tiled_plan_weighted(const double *uvw, const double *freq, const int32_t *chan_map,
+                                const float *weight, int64_t npol, int64_t n_u, int64_t n_v,
+                                double delta_l, double delta_m, int support, int oversampling,
+                                int64_t nt, int64_t nb, int64_t nchan, int64_t n_img_chan,
+                                void *workspace, size_t workspace_bytes, void *stream);
+/* No counterpart in the reference: zeroes the grid cells a plan's records
+ * can touch (the footprint region of every tile holding records, all n_img_pol
+ * polarisations), in place of clearing the whole grid before an execute that
+ * accumulates.  The grid's other cells are left as they are: use it on a grid
+ * whose other cells are zero, such as one that held a result of a plan with
+ * the same or a larger footprint.  Any tiled plan (gridder, degridder,
+ * shared, weighted) with these sizes. */
+int av_grid_tiled_clear(void *grid, int grid_dtype, int64_t n_img_pol, int64_t n_u, int64_t n_v,
+                        int support, int64_t nt, int64_t nb, int64_t nchan, int64_t n_img_chan,
+                        const void *workspace, size_t workspace_bytes, void *stream);
 /* No counterpart in the reference: one plan for both av_grid_tiled_execute
  * and av_degrid_tiled_execute (the gridder's and the degridder's binning
  * differ only in their rounding, standard_grid.py:337-352 against

@@ -7,6 +7,7 @@ import pytest
 import torch
 
 import oracle as O
+from astroviper_b200 import _lib
 
 pytestmark = pytest.mark.gpu
 
@@ -32,14 +33,18 @@ def _oracle(W, vis, wt):
                            support=W["support"], chan_mode="cube")
 
 
+@pytest.mark.parametrize("drop_flagged", [False, True])
 @pytest.mark.parametrize("support", [7, 9])
-def test_batched_graph_matches_oracle_and_replays(support):
+def test_batched_graph_matches_oracle_and_replays(support, drop_flagged):
+    """Three calls in a row (so the touched-tile clears run between them):
+    with drop_flagged the graph rebuilds the plan from each batch's weights
+    and leaves the fully flagged samples out."""
     from astroviper_b200.batched import BatchedGridder
     W = _work(support=support)
     frac = W["flag_fraction"]
     assert frac.min() >= 0.0 and frac.max() < 0.6
     B = BatchedGridder(W["uvw"], W["freq"], W["image_size"], W["pixelincr"], 2, support=support,
-                       graph=True)
+                       graph=True, drop_flagged=drop_flagged)
     g, sw = B(W["vis"], W["weight"])
     rg, rs = _oracle(W, W["vis"], W["weight"])
     assert rel(g.cpu().numpy(), rg) <= 1e-12
@@ -83,4 +88,26 @@ def test_batched_with_autotuner(tmp_path, monkeypatch):
     assert rel(g.cpu().numpy(), rg) <= 1e-12
     entries = autotune.load(str(tmp_path / "tune.json"))
     assert B.tune_key() in entries
-    assert entries[B.tune_key()]["value"] in autotune.CANDIDATES
+    best = entries[B.tune_key()]["value"]
+    assert best["chunks_per_sm"] in autotune.CANDIDATES
+    assert best["lanes"] in (_lib.AV_GRID_LANES_MMA, _lib.AV_GRID_LANES_ROWS)
+    assert len(entries[B.tune_key()]["ms"]) == 2 * len(autotune.CANDIDATES)
+    assert _lib.lib().av_tune_get(_lib.AV_TUNE_GRID_LANES) == best["lanes"]
+    # put the process-wide knobs back for the tests that follow
+    _lib.lib().av_tune_set(_lib.AV_TUNE_GRID_LANES, _lib.AV_GRID_LANES_AUTO)
+    _lib.lib().av_tune_set(_lib.AV_TUNE_GRID_CHUNKS_PER_SM, 16)
+    autotune._applied.pop(B.tune_key(), None)
+
+
+def test_batched_support_auto_picks_the_less_aliasing_kernel():
+    """support="auto" takes the smallest of 7 and 9 whose aliasing in the
+    inner 80 % of the field meets the tolerance: 7, which aliases less than 9
+    with the reference's kernel; the grids are then support 7's."""
+    from astroviper_b200.batched import BatchedGridder
+    W = _work(seed=9)
+    B = BatchedGridder(W["uvw"], W["freq"], W["image_size"], W["pixelincr"], 2, support="auto",
+                       graph=False)
+    assert B.support == 7 and B.alias[7] < 1e-2 < B.alias[9]
+    g, _ = B(W["vis"], W["weight"])
+    rg, _ = _oracle(W, W["vis"], W["weight"])
+    assert rel(g.cpu().numpy(), rg) <= 1e-12
