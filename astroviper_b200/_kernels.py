@@ -225,6 +225,7 @@ def degrid(grid_t, uvw, freq, scale, offset, chanmap, polmap, cgk, support, samp
 # overlap needs page-locked host arrays; pageable ones are copied
 # synchronously, with the same results.
 STREAM_CHUNK_BYTES = 128 << 20
+DEGRID_STREAM_SLOTS = 3
 _streams = {}
 
 
@@ -296,8 +297,10 @@ def degrid_streamed(grid_t, uvw, freq, scale, offset, chanmap, polmap, cgk, supp
                     values, flag=None, dphase=None, chunk_bytes=None):
     """values (host array, updated in place) += degridded model of the device
     grid grid_t (tiled kernel), in time chunks: chunk i+1 is copied in while
-    chunk i is degridded and chunk i-1 copied back.  Returns when values
-    holds the result."""
+    chunk i is degridded and chunk i-1 copied back.  Three device slots, so
+    that copying a chunk in never waits for the copy back of the one before
+    it: the two directions of the host link then run at once.  Returns when
+    values holds the result."""
     nt = int(uvw.shape[0])
     per_t = values[0].nbytes * 2 + uvw[0].nbytes + (0 if flag is None else flag[0].nbytes)
     chunks = time_chunks(nt, per_t, chunk_bytes)
@@ -312,8 +315,9 @@ def degrid_streamed(grid_t, uvw, freq, scale, offset, chanmap, polmap, cgk, supp
     cin = _side_stream("h2d")
     cout = _side_stream("d2h")
     vt = torch.from_numpy(values[:1]).dtype
+    n_slots = DEGRID_STREAM_SLOTS
     slots = []
-    for _ in range(2):
+    for _ in range(n_slots):
         slots.append(dict(
             v=torch.empty((tmax,) + tuple(values.shape[1:]), dtype=vt, device=dev),
             u=torch.empty((tmax,) + tuple(uvw.shape[1:]), dtype=torch.float64, device=dev),
@@ -322,14 +326,14 @@ def degrid_streamed(grid_t, uvw, freq, scale, offset, chanmap, polmap, cgk, supp
             d=None if dphase is None else torch.empty((tmax,) + tuple(np.shape(dphase)[1:]),
                                                       dtype=torch.float64, device=dev)))
     vals_t = torch.from_numpy(values)
-    free = [None, None]
+    free = [None] * n_slots
     cin.wait_stream(cur)
     for i, (t0, t1) in enumerate(chunks):
-        sl = slots[i % 2]
+        sl = slots[i % n_slots]
         n = t1 - t0
         with torch.cuda.stream(cin):
-            if free[i % 2] is not None:
-                cin.wait_event(free[i % 2])
+            if free[i % n_slots] is not None:
+                cin.wait_event(free[i % n_slots])
             _h2d(sl["v"][:n], values[t0:t1])
             _h2d(sl["u"][:n], np.asarray(uvw[t0:t1], dtype=np.float64))
             if flag is not None:
@@ -350,7 +354,7 @@ def degrid_streamed(grid_t, uvw, freq, scale, offset, chanmap, polmap, cgk, supp
             vals_t[t0:t1].copy_(sl["v"][:n], non_blocking=True)
             back = torch.cuda.Event()
             back.record(cout)
-        free[i % 2] = back
+        free[i % n_slots] = back
     cur.wait_stream(cout)
     cout.synchronize()
     return values

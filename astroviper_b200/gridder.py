@@ -65,6 +65,18 @@ class Gridder:
             self._gplan = ws
         return self._gplan
 
+    def clear_grid(self, grid):
+        """Zeroes the cells this Gridder's gridding plan can touch (the
+        footprint regions of its tiles): enough before gridding into a grid
+        whose other cells are zero, such as one that held this Gridder's
+        previous result (av_grid_tiled_clear)."""
+        ws = self._grid_plan()
+        check(lib().av_grid_tiled_clear(K.p(grid), K.dcode(grid), int(grid.shape[1]), self.nx,
+                                        self.ny, self.support, self.nt, self.nb, self.nchan,
+                                        self.n_img_chan, ws[1], ws[2], K.stream_ptr()),
+              "av_grid_tiled_clear")
+        return grid
+
     def new_grid(self, dtype=torch.complex128):
         return torch.zeros((self.n_img_chan, self.n_img_pol, self.nx, self.ny), dtype=dtype,
                            device=self.dev)

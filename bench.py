@@ -166,7 +166,8 @@ def bench_config(world, n_time=None):
     n_vis = (n_time or N_TIME) * 2016 * 64
     return {"workload": WORKLOAD, "n_vis": n_vis, "n_corr": 4 * n_vis,
             "l2": "inputs larger than L2 (1.06 GB visibilities per step)",
-            "step": "plan+grid+plan+degrid; grid zeroed, model visibilities written each step",
+            "step": "plan (one for both directions)+grid+degrid; grid cleared, model "
+                    "visibilities written each step",
             "parallelism": f"replicas x{world}"}
 
 
@@ -338,8 +339,8 @@ def main():
     def step(ev=None):
         G._gplan = None  # the binning plans are rebuilt every step (counted in the time)
         G._dplan = None
-        G.plan()         # both plans, concurrently on two streams
-        grid.zero_()
+        G.plan()         # one plan for both directions
+        G.clear_grid(grid)  # the cells the plan can touch (the rest stays zero)
         sumw.zero_()
         if ev is not None:
             ev[0].record()

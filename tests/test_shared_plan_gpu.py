@@ -163,3 +163,22 @@ def test_shared_plan_exception_samples_are_the_degridders():
     err = (v - ref).abs().cpu().numpy()
     scale = float(ref.abs().max())
     assert err.max() <= 1e-5 * scale
+
+
+def test_clear_grid_zeroes_the_cells_a_plan_can_touch():
+    """av_grid_tiled_clear (Gridder.clear_grid) zeroes every cell a plan's
+    samples can reach and leaves cells beyond its tiles alone."""
+    from astroviper_b200.gridder import Gridder
+    c = _case("ordinary")
+    nt, nb, nchan, npol = c["vis"].shape
+    img = np.array([c["n"], c["n"]])
+    G = Gridder(c["uvw"], c["freq"], img, c["cell"], npol, support=c["sup"],
+                oversampling=c["os"])
+    g, _ = G.grid(torch.as_tensor(c["vis"], device="cuda"),
+                  torch.as_tensor(c["wt"], device="cuda"))
+    touched = (g != 0)
+    assert int(touched.sum()) > 0
+    assert bool((G.clear_grid(g.clone()) == 0).all())
+    ones = G.clear_grid(torch.ones_like(g))
+    assert bool((ones[touched] == 0).all())
+    assert ones[0, 0, 0, 0] == 1 and ones[0, 0, -1, -1] == 1  # far from the uv coverage
