@@ -457,6 +457,42 @@ def briggs_apply(density, factors, uvw, freq, weight, flag, n_uv, delta_lm,
     return out, err
 
 
+def imaging_weight_degrid(imaging_weight, grid_imaging_weight, briggs_factors, uvw, freq,
+                          chan_map, pol_map, natural_weight, n_uv, delta_lm):
+    """av_imaging_weight_degrid into the float64 device tensor imaging_weight
+    (nt, nb, nchan, npol), in place; returns it."""
+    w = on_device(natural_weight)
+    if w.dtype not in (torch.float32, torch.float64):
+        w = w.to(torch.float64)
+    G = on_device(grid_imaging_weight)
+    if G.dtype not in (torch.float32, torch.float64):
+        G = G.to(torch.float64)
+    G = G.contiguous()
+    nt, nb, nchan, npol = (int(s) for s in w.shape)
+    g_chan, g_pol = int(G.shape[0]), int(G.shape[1])
+    cm = np.asarray(chan_map).astype(np.int64).ravel()
+    pm = np.asarray(pol_map).astype(np.int64).ravel()
+    if cm.size != nchan or pm.size != npol:
+        raise ValueError("chan_map / pol_map must have one entry per channel / polarisation")
+    if cm.size and (cm.min() < 0 or cm.max() >= g_chan):
+        raise ValueError("chan_map entries must index grid_imaging_weight's channels")
+    if pm.size and (pm.min() < 0 or pm.max() >= g_pol):
+        raise ValueError("pol_map entries must index grid_imaging_weight's polarisations")
+    bf = on_device(briggs_factors, torch.float64).contiguous()
+    if bf.numel() != 2 * g_chan * g_pol:
+        raise ValueError("briggs_factors must have shape (2, n_chan, n_pol) of the grid")
+    uvw_d = on_device(uvw, torch.float64)
+    freq_d = on_device(freq, torch.float64)
+    cm_d = torch.as_tensor(cm.astype(np.int32), device=w.device)
+    pm_d = torch.as_tensor(pm.astype(np.int32), device=w.device)
+    check(lib().av_imaging_weight_degrid(p(imaging_weight), p(G), dcode(G), g_chan, g_pol, p(bf),
+                                         p(uvw_d), p(freq_d), p(cm_d), p(pm_d), p(w), dcode(w),
+                                         int(n_uv[0]), int(n_uv[1]), float(delta_lm[0]),
+                                         float(delta_lm[1]), nt, nb, nchan, npol, stream_ptr()),
+          "av_imaging_weight_degrid")
+    return imaging_weight
+
+
 # ------------------------------------------------------------------- Hogbom --
 def maximg(image, mask=None):
     im = on_device(image)

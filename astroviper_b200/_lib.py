@@ -85,6 +85,8 @@ SIGNATURES = {
     "av_briggs_factors_workspace_size": (_sz, [_i64]),
     "av_briggs_factors": (_i, [_vp, _vp, _vp, _i64, _i64, _i64, _d, _vp, _sz, _vp]),
     "av_briggs_factors_noalloc": (_i, [_vp, _vp, _vp, _i64, _i64, _i64, _d, _vp]),
+    "av_imaging_weight_degrid": (_i, [_vp, _vp, _i, _i64, _i64, _vp, _vp, _vp, _vp, _vp, _vp,
+                                      _i, _i64, _i64, _d, _d, _i64, _i64, _i64, _i64, _vp]),
     "av_briggs_apply": (_i, [_vp, _i, _vp, _vp, _vp, _vp, _vp, _i, _vp, _i64, _i64, _d, _d,
                              _i64, _i64, _i64, _i64, _vp, _vp]),
     "av_maximg": (_i, [_vp, _vp, _i, _i64, _i64, _vp, _vp]),

@@ -157,6 +157,43 @@ def standard_grid_jit(grid, sum_weight, do_psf, do_imaging_weight, vis_data, uvw
                pol_map, weight, cgk_1D, n_uv, delta_lm, support, oversampling, precision)
 
 
+def standard_imaging_weight_degrid_numpy_wrap(grid_imaging_weight, uvw, natural_imaging_weight,
+                                              briggs_factors, freq_chan, grid_params):
+    """standard_grid.py:441-484: per-sample, per-polarisation imaging weights
+    (float64, the shape of natural_imaging_weight) read from a cube of
+    imaging-weight grids (n_chan, n_pol, n_u, n_v) with the Briggs factors
+    (2, n_chan, n_pol); zero for samples off the grid.  Channel c and
+    polarisation p read grid (c, p), as the reference's identity maps."""
+    n_chan = natural_imaging_weight.shape[2]
+    n_imag_pol = natural_imaging_weight.shape[3]
+    out = torch.zeros(tuple(int(s) for s in natural_imaging_weight.shape), dtype=torch.float64,
+                      device=K.device())
+    K.imaging_weight_degrid(out, grid_imaging_weight, briggs_factors, uvw, freq_chan,
+                            np.arange(0, n_chan), np.arange(0, n_imag_pol),
+                            natural_imaging_weight, grid_params["image_size_padded"],
+                            grid_params["cell_size"])
+    if H.is_torch(natural_imaging_weight) or H.is_torch(grid_imaging_weight):
+        return out
+    return H.host(out)
+
+
+def standard_imaging_weight_degrid_jit(imaging_weight, grid_imaging_weight, briggs_factors, uvw,
+                                       freq_chan, chan_map, pol_map, natural_imaging_weight,
+                                       n_uv, delta_lm):
+    """standard_grid.py:487-604: writes the imaging weights of the samples on
+    the grid into imaging_weight in place (entries of samples off the grid
+    keep their values).  chan_map / pol_map entries index the grid's
+    channels / polarisations (ValueError otherwise)."""
+    iw = H.dev(imaging_weight, torch.float64)
+    K.imaging_weight_degrid(iw, grid_imaging_weight, briggs_factors, uvw, freq_chan, chan_map,
+                            pol_map, natural_imaging_weight, n_uv, delta_lm)
+    if H.is_torch(imaging_weight):
+        if imaging_weight.data_ptr() != iw.data_ptr():
+            imaging_weight.copy_(iw)
+    else:
+        H.write_back(imaging_weight, iw)
+
+
 def _is_datatree(x):
     try:
         import xarray  # noqa: F401

@@ -160,6 +160,49 @@ __global__ void __launch_bounds__(256) k_briggs_apply(void *out, int out_dt, con
   }
 }
 
+// standard_imaging_weight_degrid_jit (standard_grid.py:487-604), one thread
+// per (time, baseline, channel): for a sample whose nearest cell (gridder
+// convention) is on the grid, every polarisation's weight becomes its
+// natural weight (the mean of polarisations 0 and 1 when there are two),
+// divided by f0 * G + f1 where both the polarisation's own natural weight
+// and G, the imaging-weight grid of (chan_map[c], pol_map[p]) at that cell,
+// are neither NaN nor zero.  Samples off the grid (or with NaN uv) are left
+// as the caller's array holds them.
+__global__ void __launch_bounds__(256) k_imaging_weight_degrid(
+    double *out, const void *G, int g_dt, int64_t g_chan, int64_t g_pol, const double *factors,
+    const double *uvw, const double *freq, const int32_t *chan_map, const int32_t *pol_map,
+    const void *wt, int dt, int64_t n_u, int64_t n_v, double dl0, double dl1, int64_t nrows,
+    int64_t nchan, int64_t npol) {
+  const int64_t row = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (row >= nrows) return;
+  const int64_t tb = row / nchan, c = row - tb * nchan;
+  long long ui, vi, uic, vic;
+  if (!nearest_cell(uvw[3 * tb], uvw[3 * tb + 1], freq[c], dl0, dl1, n_u, n_v, ui, vi, uic,
+                    vic))
+    return;
+  auto w = [&](int64_t p) {
+    const int64_t i = row * npol + p;
+    return dt == AV_F32 ? (double)((const float *)wt)[i] : ((const double *)wt)[i];
+  };
+  const int64_t ac = chan_map[c];
+  for (int64_t p = 0; p < npol; ++p) {
+    const int64_t ap = pol_map[p];
+    double iw = npol == 2 ? __ddiv_rn(__dadd_rn(w(0), w(1)), 2.0) : w(p);
+    const double nat = w(p);
+    if (!isnan(nat) && nat != 0.0) {
+      const int64_t gi = ((ac * g_pol + ap) * n_u + ui) * n_v + vi;
+      const double g =
+          g_dt == AV_F32 ? (double)((const float *)G)[gi] : ((const double *)G)[gi];
+      if (!isnan(g) && g != 0.0) {
+        const int64_t fi = ac * g_pol + ap;
+        const double den = __dadd_rn(__dmul_rn(factors[fi], g), factors[g_chan * g_pol + fi]);
+        iw = __ddiv_rn(iw, den);
+      }
+    }
+    out[row * npol + p] = iw;
+  }
+}
+
 }  // namespace av
 
 using namespace av;
@@ -229,6 +272,34 @@ int av_briggs_apply(void *out, int out_dtype, const double *density, const doubl
   k_briggs_apply<<<(unsigned)((rows + 255) / 256), 256, 0, st>>>(
       out, out_dtype, density, factors, nchan, uvw, freq, wt, wt_dtype, flag, n_u, n_v, delta_l,
       delta_m, rows, nchan, npol, err_flag);
+  AV_LAUNCH_CHECK();
+  return AV_OK;
+}
+
+int av_imaging_weight_degrid(double *imaging_weight, const void *grid_imaging_weight,
+                             int grid_dtype, int64_t g_chan, int64_t g_pol,
+                             const double *briggs_factors, const double *uvw, const double *freq,
+                             const int32_t *chan_map, const int32_t *pol_map,
+                             const void *natural_weight, int wt_dtype, int64_t n_u, int64_t n_v,
+                             double delta_l, double delta_m, int64_t nt, int64_t nb,
+                             int64_t nchan, int64_t npol, void *stream) {
+  clear_error();
+  AV_CHECK_ARG(imaging_weight && grid_imaging_weight && briggs_factors && uvw && freq &&
+                   chan_map && pol_map && natural_weight,
+               "av_imaging_weight_degrid: null pointer");
+  AV_CHECK_ARG(grid_dtype == AV_F32 || grid_dtype == AV_F64,
+               "av_imaging_weight_degrid: grid dtype");
+  AV_CHECK_ARG(wt_dtype == AV_F32 || wt_dtype == AV_F64,
+               "av_imaging_weight_degrid: weight dtype");
+  AV_CHECK_ARG(n_u > 0 && n_v > 0 && g_chan > 0 && g_pol > 0 && nt >= 0 && nb >= 0 &&
+                   nchan >= 0 && npol >= 1,
+               "av_imaging_weight_degrid: bad shape");
+  const int64_t rows = nt * nb * nchan;
+  if (rows == 0) return AV_OK;
+  k_imaging_weight_degrid<<<(unsigned)((rows + 255) / 256), 256, 0, as_stream(stream)>>>(
+      imaging_weight, grid_imaging_weight, grid_dtype, g_chan, g_pol, briggs_factors, uvw, freq,
+      chan_map, pol_map, natural_weight, wt_dtype, n_u, n_v, delta_l, delta_m, rows, nchan,
+      npol);
   AV_LAUNCH_CHECK();
   return AV_OK;
 }

@@ -408,6 +408,26 @@ int av_briggs_apply(void *out, int out_dtype, const double *density, const doubl
                     double delta_m, int64_t nt, int64_t nb, int64_t nchan, int64_t npol,
                     int32_t *err_flag, void *stream);
 
+/* standard_imaging_weight_degrid_jit, standard_grid.py:487-604 (called by
+ * standard_imaging_weight_degrid_numpy_wrap, :441-484): imaging_weight (nt,
+ * nb, nchan, npol, float64) gets, for every sample whose nearest cell
+ * (int(x + 0.5), bounds [0, n)) is on the grid, each polarisation's natural
+ * weight (the mean of polarisations 0 and 1 when npol == 2) divided by
+ * briggs_factors[0][a] * G[a][cell] + briggs_factors[1][a], a = (chan_map[c],
+ * pol_map[p]), where that polarisation's natural weight and G[a][cell] are
+ * neither NaN nor zero.  Entries of samples off the grid or with NaN uv are
+ * left unchanged (the wrapper passes zeros).  grid_imaging_weight is
+ * (g_chan, g_pol, n_u, n_v) of grid_dtype, briggs_factors (2, g_chan, g_pol);
+ * chan_map (nchan) and pol_map (npol) are device int32 arrays whose entries
+ * the caller keeps in [0, g_chan) and [0, g_pol). */
+int av_imaging_weight_degrid(double *imaging_weight, const void *grid_imaging_weight,
+                             int grid_dtype, int64_t g_chan, int64_t g_pol,
+                             const double *briggs_factors, const double *uvw, const double *freq,
+                             const int32_t *chan_map, const int32_t *pol_map,
+                             const void *natural_weight, int wt_dtype, int64_t n_u, int64_t n_v,
+                             double delta_l, double delta_m, int64_t nt, int64_t nb,
+                             int64_t nchan, int64_t npol, void *stream);
+
 /* ------------------------------------------------------------ Hogbom CLEAN -- */
 /* hclean::maximg, hclean.cpp:51-81: out[0] = min, out[1] = max over pixels
  * with mask > 0.5 (mask may be NULL).  dtype AV_F32 / AV_F64; out of dtype. */

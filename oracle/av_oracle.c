@@ -660,6 +660,46 @@ int orc_degrid_imaging_weights(double *imaging_weight, const double *grid, int64
   return 0;
 }
 
+/* standard_imaging_weight_degrid_jit, standard_grid.py:487-604.  Per
+ * polarisation: the natural weight (pols 0 and 1 averaged when n_pol == 2),
+ * divided by f0 * G + f1 where the polarisation's own natural weight and G
+ * are neither NaN nor zero; samples off the grid are not written. */
+void orc_imaging_weight_degrid(double *imaging_weight, const double *grid, int64_t n_gchan,
+                               int64_t n_gpol, const double *briggs_factors, const double *uvw,
+                               const double *freq, const int64_t *chan_map,
+                               const int64_t *pol_map, const double *natural, int64_t n_u,
+                               int64_t n_v, double dl0, double dl1, int64_t nt, int64_t nb,
+                               int64_t nchan, int64_t npol) {
+  const double c = 299792458.0;
+  const int64_t uc0 = n_u / 2, uc1 = n_v / 2;
+  for (int64_t tb = 0; tb < nt * nb; ++tb) {
+    for (int64_t ic = 0; ic < nchan; ++ic) {
+      const int64_t a_chan = chan_map[ic];
+      const double us0 = -(freq[ic] * dl0 * (double)n_u) / c;
+      const double us1 = -(freq[ic] * dl1 * (double)n_v) / c;
+      const double u = uvw[tb * 3 + 0] * us0, v = uvw[tb * 3 + 1] * us1;
+      if (isnan(u) || isnan(v)) continue;
+      const double u_pos = u + (double)uc0, v_pos = v + (double)uc1;
+      const int64_t ui = trunc_i64(u_pos + 0.5), vi = trunc_i64(v_pos + 0.5);
+      if (!((ui < n_u) && (vi < n_v) && (ui >= 0) && (vi >= 0))) continue;
+      const double *nw = natural + (tb * nchan + ic) * npol;
+      for (int64_t ip = 0; ip < npol; ++ip) {
+        const int64_t a_pol = pol_map[ip];
+        double *out = imaging_weight + (tb * nchan + ic) * npol + ip;
+        *out = npol == 2 ? (nw[0] + nw[1]) / 2.0 : nw[ip];
+        if (!isnan(nw[ip]) && nw[ip] != 0.0) {
+          const double g = grid[((a_chan * n_gpol + a_pol) * n_u + ui) * n_v + vi];
+          if (!isnan(g) && g != 0.0) {
+            const double f0 = briggs_factors[(0 * n_gchan + a_chan) * n_gpol + a_pol];
+            const double f1 = briggs_factors[(1 * n_gchan + a_chan) * n_gpol + a_pol];
+            *out = *out / (f0 * g + f1);
+          }
+        }
+      }
+    }
+  }
+}
+
 /* ---------------------------------------------------------------------------
  * Hogbom CLEAN, hclean.cpp:51-81 (maximg) and :106-210 (clean).
  * Generalised to a PSF of size (pny, pnx) >= (ny, nx) with centre

@@ -56,6 +56,9 @@ def lib():
                                              _i64p, _i64, _dp, _i64, _i64, _d, _d, _i64, _i64,
                                              _i64, _i64]
     L.orc_degrid_imaging_weights.restype = _i
+    L.orc_imaging_weight_degrid.argtypes = [_dp, _dp, _i64, _i64, _dp, _dp, _dp, _i64p, _i64p,
+                                            _dp, _i64, _i64, _d, _d, _i64, _i64, _i64, _i64]
+    L.orc_imaging_weight_degrid.restype = None
     L.orc_hogbom_f32.argtypes = [_fp, _fp, _fp, _i, _i, _i, _fp, _i, _i, _i, _i, _i, _i, _i,
                                  _i, _f, _f, _f, _dp, _i32p, _dp]
     L.orc_hogbom_f32.restype = _i
@@ -304,6 +307,39 @@ def degrid_imaging_weights_jit(imaging_weight, grid_imaging_weight, briggs_facto
                                           float(delta_lm[1]), nt, nb, nchan, npol)
     if rc != 0:
         raise ValueError("NaN in briggs_factors")
+
+
+def standard_imaging_weight_degrid_jit(imaging_weight, grid_imaging_weight, briggs_factors, uvw,
+                                       freq_chan, chan_map, pol_map, natural_imaging_weight,
+                                       n_uv, delta_lm):
+    """Restates standard_imaging_weight_degrid_jit (standard_grid.py:487-604),
+    in place into the float64 array imaging_weight."""
+    assert imaging_weight.flags.c_contiguous and imaging_weight.dtype == np.float64
+    nt, nb = uvw.shape[:2]
+    nchan, npol = natural_imaging_weight.shape[2], natural_imaging_weight.shape[3]
+    g = _c(grid_imaging_weight, np.float64)
+    bf = _c(briggs_factors, np.float64).reshape(2, g.shape[0], g.shape[1])
+    uvw = _c(uvw, np.float64)
+    fr = _c(freq_chan, np.float64)
+    cm = _c(chan_map, np.int64)
+    pm = _c(pol_map, np.int64)
+    nw = _c(natural_imaging_weight, np.float64)
+    lib().orc_imaging_weight_degrid(_p(imaging_weight, _dp), _p(g, _dp), g.shape[0], g.shape[1],
+                                    _p(bf, _dp), _p(uvw, _dp), _p(fr, _dp), _p(cm, _i64p),
+                                    _p(pm, _i64p), _p(nw, _dp), int(n_uv[0]), int(n_uv[1]),
+                                    float(delta_lm[0]), float(delta_lm[1]), nt, nb, nchan, npol)
+
+
+def standard_imaging_weight_degrid_numpy_wrap(grid_imaging_weight, uvw, natural_imaging_weight,
+                                              briggs_factors, freq_chan, grid_params):
+    """Restates standard_imaging_weight_degrid_numpy_wrap (standard_grid.py:441-484)."""
+    n_chan, n_pol = natural_imaging_weight.shape[2], natural_imaging_weight.shape[3]
+    out = np.zeros(natural_imaging_weight.shape, dtype=np.double)
+    standard_imaging_weight_degrid_jit(out, grid_imaging_weight, briggs_factors, uvw, freq_chan,
+                                       np.arange(n_chan), np.arange(n_pol),
+                                       natural_imaging_weight, grid_params["image_size_padded"],
+                                       grid_params["cell_size"])
+    return out
 
 
 def calculate_briggs_params(grid, sum_weight, params):

@@ -351,6 +351,50 @@ def make_weights(R):
     np.savez_compressed(os.path.join(HERE, "weights.npz"), **out)
 
 
+def make_iw_degrid(R):
+    """standard_imaging_weight_degrid_numpy_wrap (standard_grid.py:441-484) and
+    standard_imaging_weight_degrid_jit (:487-604) with permuted maps into a
+    prefilled array: NaN / zero natural weights, NaN / zero grid cells, NaN
+    uv, samples off the grid and one just below index 0 (int() truncation)."""
+    rng = np.random.default_rng(6006)
+    from astroviper_b200 import synthetic as S
+    out = {}
+    c = 299792458.0
+    for npol in (1, 2, 4):
+        uvw, _ = S.array_uvw(9, 6, radius_m=700.0, seed=20 + npol)
+        nt, nb = uvw.shape[:2]
+        uvw[:, -1, :2] *= 50.0
+        uvw[3, 2, 0] = np.nan
+        freq = np.array([1.2e9, 1.35e9, 1.5e9])
+        nchan = len(freq)
+        cell = np.array([-15.0, 15.0]) * np.pi / (180 * 3600)
+        n = np.array([40, 32])
+        # sample (4, 1) at channel 0 lands at u_pos = -0.7: int(-0.2) = 0 is kept
+        us0 = -(freq[0] * cell[0] * n[0]) / c
+        uvw[4, 1, 0] = (-0.7 - n[0] // 2) / us0
+        nat = rng.uniform(0.2, 3.0, size=(nt, nb, nchan, npol))
+        nat[rng.uniform(size=nat.shape) < 0.08] = 0.0
+        nat[rng.uniform(size=nat.shape) < 0.05] = np.nan
+        G = 0.5 * rng.integers(1, 9, size=(nchan, npol, n[0], n[1]))  # compresses
+        G[rng.uniform(size=G.shape) < 0.15] = 0.0
+        G[rng.uniform(size=G.shape) < 0.05] = np.nan
+        bf = np.stack([rng.uniform(0.1, 2.0, size=(nchan, npol)),
+                       rng.uniform(0.5, 1.5, size=(nchan, npol))])
+        params = {"image_size_padded": n, "cell_size": cell}
+        iw = R.sg.standard_imaging_weight_degrid_numpy_wrap(G, uvw, nat, bf, freq, params)
+        Gf = G.astype(np.float32)
+        iw32 = R.sg.standard_imaging_weight_degrid_numpy_wrap(Gf, uvw, nat, bf, freq, params)
+        cm = np.array([2, 0, 1])
+        pm = np.arange(npol)[::-1].copy()
+        jit = np.full(nat.shape, -7.0)
+        R.sg.standard_imaging_weight_degrid_jit(jit, G, bf, uvw, freq, cm, pm, nat, n, cell)
+        d = dict(uvw=uvw, freq=freq, nat=nat, G=G, bf=bf, cell=cell, n=n, iw=iw, iw32=iw32,
+                 cm=cm, pm=pm, jit=jit)
+        for k, v in d.items():
+            out[f"p{npol}_{k}"] = v
+    np.savez_compressed(os.path.join(HERE, "iw_degrid.npz"), **out)
+
+
 def make_hogbom(R):
     from astroviper_b200 import synthetic as S
     cw = S.clean_workload(nx=64, psf_factor=2, n_src=12, n_time=12, seed=5005)
@@ -384,7 +428,7 @@ def make_hogbom(R):
 
 MAKERS = {"pswf": make_pswf, "grid": make_grid, "image": make_image,
           "psf_dropin": make_psf_planes, "degrid": make_degrid, "weights": make_weights,
-          "hogbom": make_hogbom}
+          "hogbom": make_hogbom, "iw_degrid": make_iw_degrid}
 
 
 def main(names=None):

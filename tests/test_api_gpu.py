@@ -261,6 +261,42 @@ def test_weights_dropin_against_golden():
             q("bf_abs"))
 
 
+def test_imaging_weight_degrid_dropin_against_golden():
+    """standard_imaging_weight_degrid_numpy_wrap / _jit (standard_grid.py:441-604)
+    on the GPU: bit-exact to the reference's outputs for numpy and torch
+    inputs, float64 and float32 grids, permuted maps into a prefilled array
+    (entries of samples off the grid untouched); maps outside the grid raise."""
+    import torch
+    from astroviper_b200.core.imaging.imaging_utils import standard_grid as SG
+    g = golden("iw_degrid.npz")
+    for npol in (1, 2, 4):
+        q = lambda k: g[f"p{npol}_{k}"]
+        params = {"image_size_padded": q("n"), "cell_size": q("cell")}
+        iw = SG.standard_imaging_weight_degrid_numpy_wrap(q("G"), q("uvw"), q("nat"), q("bf"),
+                                                          q("freq"), params)
+        assert isinstance(iw, np.ndarray) and iw.dtype == np.float64
+        assert np.array_equal(iw, q("iw"), equal_nan=True)
+        iw32 = SG.standard_imaging_weight_degrid_numpy_wrap(q("G").astype(np.float32), q("uvw"),
+                                                            q("nat"), q("bf"), q("freq"), params)
+        assert np.array_equal(iw32, q("iw32"), equal_nan=True)
+        t = SG.standard_imaging_weight_degrid_numpy_wrap(
+            torch.as_tensor(q("G"), device="cuda"), q("uvw"),
+            torch.as_tensor(q("nat").astype(np.float32), device="cuda"), q("bf"), q("freq"),
+            params)
+        nat32 = q("nat").astype(np.float32).astype(np.float64)
+        ref32 = O.standard_imaging_weight_degrid_numpy_wrap(q("G"), q("uvw"), nat32, q("bf"),
+                                                            q("freq"), params)
+        assert t.is_cuda and np.array_equal(t.cpu().numpy(), ref32, equal_nan=True)
+        jit = np.full(q("nat").shape, -7.0)
+        SG.standard_imaging_weight_degrid_jit(jit, q("G"), q("bf"), q("uvw"), q("freq"), q("cm"),
+                                              q("pm"), q("nat"), q("n"), q("cell"))
+        assert np.array_equal(jit, q("jit"), equal_nan=True)
+        with pytest.raises(ValueError):
+            SG.standard_imaging_weight_degrid_jit(jit, q("G"), q("bf"), q("uvw"), q("freq"),
+                                                  q("cm") + 1, q("pm"), q("nat"), q("n"),
+                                                  q("cell"))
+
+
 def test_calculate_imaging_weights_processing_set():
     from astroviper_b200.core.imaging.calculate_imaging_weights import calculate_imaging_weights
     g = golden("weights.npz")

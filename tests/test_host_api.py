@@ -118,7 +118,8 @@ def test_module_layout_mirrors_reference():
     for mod, names in {
         "astroviper_b200.core.imaging.imaging_utils.standard_grid": [
             "standard_grid_numpy_wrap_input_checked", "standard_grid_numpy_wrap",
-            "standard_grid_psf_numpy_wrap", "standard_grid_jit", "grid2image_spheroid_ms4"],
+            "standard_grid_psf_numpy_wrap", "standard_grid_jit", "grid2image_spheroid_ms4",
+            "standard_imaging_weight_degrid_numpy_wrap", "standard_imaging_weight_degrid_jit"],
         "astroviper_b200.core.imaging.imaging_utils.standard_degrid": [
             "sgrid", "sgrid_numba", "dgrid", "dgrid_optimized", "dgrid2", "dgrid_numba",
             "degrid_spheroid_ms4"],

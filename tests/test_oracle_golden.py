@@ -128,6 +128,27 @@ def test_weights_golden():
                                                         {"weighting": "natural"}), p("bf_nat"))
 
 
+def test_imaging_weight_degrid_golden():
+    """standard_imaging_weight_degrid_numpy_wrap / _jit (standard_grid.py:441-604)
+    restated: bit-exact to the reference's outputs, float32 grid, permuted maps
+    and the entries of samples off the grid left as the caller's array held."""
+    g = golden("iw_degrid.npz")
+    for npol in (1, 2, 4):
+        q = lambda k: g[f"p{npol}_{k}"]
+        params = {"image_size_padded": q("n"), "cell_size": q("cell")}
+        iw = O.standard_imaging_weight_degrid_numpy_wrap(q("G"), q("uvw"), q("nat"), q("bf"),
+                                                         q("freq"), params)
+        assert np.array_equal(iw, q("iw"), equal_nan=True)
+        iw32 = O.standard_imaging_weight_degrid_numpy_wrap(q("G").astype(np.float32), q("uvw"),
+                                                           q("nat"), q("bf"), q("freq"), params)
+        assert np.array_equal(iw32, q("iw32"), equal_nan=True)
+        jit = np.full(q("nat").shape, -7.0)
+        O.standard_imaging_weight_degrid_jit(jit, q("G"), q("bf"), q("uvw"), q("freq"), q("cm"),
+                                             q("pm"), q("nat"), q("n"), q("cell"))
+        assert np.array_equal(jit, q("jit"), equal_nan=True)
+        assert (q("jit") == -7.0).any() and np.isnan(q("iw")).any() and (q("iw") == 0).any()
+
+
 RUNS = {
     "default": dict(max_iter=100),
     "box_thr": dict(max_iter=400, gain=0.2, threshold=0.02, clean_box=(5, 50, 10, 60)),
