@@ -56,6 +56,11 @@ SIGNATURES = {
     "av_tiled_plan_counts": (_i, [_i64, _i64, _i64, _i64, _i64, _i64, _i, _vp, _sz, _vp, _vp]),
     "av_grid_tiled_execute": (_i, [_vp, _i, _vp, _i, _vp, _i, _vp, _i, _vp, _vp, _i64, _i64, _i,
                                    _i, _i64, _i64, _i64, _i64, _i64, _i64, _vp, _sz, _vp]),
+    "av_grid_tiled_execute_det": (_i, [_vp, _i, _vp, _i, _vp, _i, _vp, _i, _vp, _vp, _i64, _i64,
+                                       _i, _i, _i64, _i64, _i64, _i64, _i64, _i64, _vp, _sz, _vp,
+                                       _sz, _vp]),
+    "av_grid_tiled_det_workspace_size": (_sz, [_i64, _i64, _i64, _i64]),
+    "av_tiled_plan_order_rows": (_i, [_i64, _i64, _i64, _i64, _i64, _i64, _i, _vp, _sz, _vp]),
     "av_grid_tiled": (_i, [_vp, _i, _vp, _i, _vp, _i, _vp, _i, _vp, _vp, _vp, _vp, _vp, _i64,
                            _i64, _d, _d, _i, _i, _i64, _i64, _i64, _i64, _i64, _i64, _vp, _sz,
                            _vp]),

@@ -181,6 +181,11 @@ struct TiledGridArgs {
   // adjoint of the degridder: weight 1 / sum_k w_k per sample, flags honoured
   int inv_norm;
   const uint8_t *flag;      // may be NULL
+  // deterministic mode (k_grid_mma<.., true>): fixed-point sums, scales 2^F
+  // of the grid and of the sums of weights in det_scale[0..1]
+  unsigned long long *det_grid;  // (plane, npg, n_u, n_v, re | im)
+  unsigned long long *det_sumw;  // (plane, npg)
+  const double *det_scale;
 };
 
 // Lane mappings.  Each warp streams its own contiguous slice of a tile
@@ -500,7 +505,10 @@ struct MmaLanes {
   }
 
   // Rows and columns past the support hold zeros (zero taps) and are skipped.
-  __device__ __forceinline__ void flush(double *sre, double *sim, int key) {
+  // DET: the sub-grid holds fixed-point integers (value x scale, rounded to
+  // nearest), whose sums do not depend on the order of the additions.
+  template <bool DET = false>
+  __device__ __forceinline__ void flush(double *sre, double *sim, int key, double scale = 0.0) {
     const int du = key & 255, dv = (key >> 8) & 255;
     const int base = (du + g) * C::RS + dv + 2 * t;
 #pragma unroll
@@ -510,8 +518,15 @@ struct MmaLanes {
         const double re = acc[p][q], im = acc[p][2 + q];
         if (ipm[p] >= 0 && g < S && 2 * t + q < S && (re != 0.0 || im != 0.0)) {
           const int e = ipm[p] * C::PS + base + q;
-          atomicAdd(sre + e, re);
-          atomicAdd(sim + e, im);
+          if (DET) {
+            atomicAdd((unsigned long long *)(sre + e),
+                      (unsigned long long)__double2ll_rn(re * scale));
+            atomicAdd((unsigned long long *)(sim + e),
+                      (unsigned long long)__double2ll_rn(im * scale));
+          } else {
+            atomicAdd(sre + e, re);
+            atomicAdd(sim + e, im);
+          }
         }
       }
     }
@@ -578,6 +593,49 @@ __device__ __forceinline__ void flush_subgrid(const TiledGridArgs &a, double *sr
       }
       sre[e] = 0.0;
       sim[e] = 0.0;
+    }
+  }
+}
+
+// Deterministic mode: a warp's sums of weights (summed over its lanes in a
+// fixed order) as fixed-point integers.
+template <int NPOL>
+__device__ __forceinline__ void add_sum_weight_det(const TiledGridArgs &a, double (&sw)[NPOL],
+                                                   const int (&pm)[NPOL], int64_t plane,
+                                                   int lane, double scale) {
+#pragma unroll
+  for (int p = 0; p < NPOL; ++p) {
+    double v = sw[p];
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    if (lane == 0 && pm[p] >= 0 && v != 0.0)
+      atomicAdd(&a.det_sumw[plane * a.npg + pm[p]],
+                (unsigned long long)__double2ll_rn(v * scale));
+  }
+}
+
+// Deterministic mode: the fixed-point sub-grid added to the fixed-point grid
+// (integer additions: exact, in any order) and cleared.
+template <int W, int RS, int PS, int THREADS>
+__device__ __forceinline__ void flush_subgrid_det(const TiledGridArgs &a, double *sre,
+                                                  double *sim, int64_t plane, int tu, int tv) {
+  unsigned long long *qre = (unsigned long long *)sre, *qim = (unsigned long long *)sim;
+  const int sub_n = a.npg * W * W;
+  for (int i0 = 0; i0 < sub_n; i0 += THREADS) {
+    const int i = i0 + threadIdx.x;
+    if (i >= sub_n) continue;
+    const int gp = i / (W * W);
+    const int cell = i - gp * W * W;
+    const int iu = cell / W, iv = cell - iu * W;
+    const int e = gp * PS + iu * RS + iv;
+    const unsigned long long x = qre[e], y = qim[e];
+    if (x != 0ull || y != 0ull) {
+      const int64_t gu = (int64_t)tu * TILE + iu, gv = (int64_t)tv * TILE + iv;
+      const int64_t gi = ((plane * a.npg + gp) * a.n_u + gu) * a.n_v + gv;
+      if (x) atomicAdd(a.det_grid + 2 * gi, x);
+      if (y) atomicAdd(a.det_grid + 2 * gi + 1, y);
+      qre[e] = 0ull;
+      qim[e] = 0ull;
     }
   }
 }
@@ -847,9 +905,11 @@ __device__ __forceinline__ void read_raw(const TiledGridArgs &a, const double2 *
 // the raw values of round rd + 2 are copied while round rd is computed, and
 // records are loaded one round before their copies are issued.  Only for
 // weighted gridding (a.wt != NULL, no 1 / norm scaling).
-template <int S, int NPOL>
+template <int S, int NPOL, bool DET = false>
 __global__ void __launch_bounds__(MCfg<S, NPOL>::THREADS, 1) k_grid_mma(TiledGridArgs a) {
   using C = MCfg<S, NPOL>;
+  const double dscale = DET ? a.det_scale[0] : 0.0;
+  const double wscale = DET ? a.det_scale[1] : 0.0;
   constexpr int W = C::W, RWP = C::RWP;
   extern __shared__ __align__(16) unsigned char smem[];
   double *tab = (double *)smem;
@@ -976,7 +1036,7 @@ __global__ void __launch_bounds__(MCfg<S, NPOL>::THREADS, 1) k_grid_mma(TiledGri
         int j = 0;
         while (j < jn) {
           if ((starts >> j) & 1u) {
-            if (cur >= 0) lanes.flush(sre, sim, cur);
+            if (cur >= 0) lanes.template flush<DET>(sre, sim, cur, dscale);
             cur = __shfl_sync(0xffffffffu, my_key, j);
           }
           const unsigned later = j < 31 ? (starts & (0xfffffffeu << j)) : 0u;
@@ -990,10 +1050,12 @@ __global__ void __launch_bounds__(MCfg<S, NPOL>::THREADS, 1) k_grid_mma(TiledGri
         rc2 = rc3;
       }
       cp_async_wait<0>();
-      if (cur >= 0) lanes.flush(sre, sim, cur);
-      add_sum_weight<NPOL>(a, sw, pm, plane, lane);
+      if (cur >= 0) lanes.template flush<DET>(sre, sim, cur, dscale);
+      if (DET) add_sum_weight_det<NPOL>(a, sw, pm, plane, lane, wscale);
+      else add_sum_weight<NPOL>(a, sw, pm, plane, lane);
       __syncthreads();
-      flush_subgrid<W, C::RS, C::PS, C::THREADS>(a, sre, sim, plane, tu, tv);
+      if (DET) flush_subgrid_det<W, C::RS, C::PS, C::THREADS>(a, sre, sim, plane, tu, tv);
+      else flush_subgrid<W, C::RS, C::PS, C::THREADS>(a, sre, sim, plane, tu, tv);
       __syncthreads();
       seg_lo = seg_hi;
       if (seg_hi == t_end) ++t;
@@ -1019,7 +1081,7 @@ static int launch_grid_rows(const TiledGridArgs &a, int64_t nblocks, cudaStream_
   return AV_OK;
 }
 
-template <int S, int NPOL>
+template <int S, int NPOL, bool DET = false>
 static int launch_grid_mma(const TiledGridArgs &a, int64_t nblocks, cudaStream_t st) {
   using C = MCfg<S, NPOL>;
   size_t smem = C::total(a.npg);
@@ -1027,11 +1089,11 @@ static int launch_grid_mma(const TiledGridArgs &a, int64_t nblocks, cudaStream_t
   int dev = 0;
   AV_CUDA(cudaGetDevice(&dev));
   if (dev >= 0 && dev < 64 && !configured[dev]) {
-    AV_CUDA(cudaFuncSetAttribute(k_grid_mma<S, NPOL>,
+    AV_CUDA(cudaFuncSetAttribute(k_grid_mma<S, NPOL, DET>,
                                  cudaFuncAttributeMaxDynamicSharedMemorySize, (int)C::total(4)));
     configured[dev] = true;
   }
-  k_grid_mma<S, NPOL><<<(unsigned)nblocks, C::THREADS, smem, st>>>(a);
+  k_grid_mma<S, NPOL, DET><<<(unsigned)nblocks, C::THREADS, smem, st>>>(a);
   AV_LAUNCH_CHECK();
   return AV_OK;
 }
@@ -1085,6 +1147,117 @@ static int dispatch_support(const TiledGridArgs &a, int support, int npol, int64
   }
   set_error("av_grid_tiled: support %d not in [3, 9]", support);
   return AV_ERR_UNSUPPORTED;
+}
+
+// ---------------------------------------------------- deterministic mode ----
+// av_grid_tiled_execute_det: k_grid_mma over a row-ordered plan with the
+// run, sub-grid and grid sums in 64-bit fixed point.  A run's FP64 sum is
+// fixed by the order of its records (rows) and by where the chunk and warp
+// slices cut it (fixed by the plan and the launch settings); every sum after
+// that is an integer addition, exact in any order.  The scale 2^F is chosen
+// from a bound of any cell's sum of magnitudes, n_rec * max|value| *
+// max|tap|^2, so that F leaves that bound below 2^61 (no overflow; the
+// rounding of each run sum is at most 2^-F-1).  The sums of weights use
+// their own bound, n_rec * max|weight| * (S max|tap|)^2.
+template <int NPOL>
+static int dispatch_det_npol(const TiledGridArgs &a, int support, int64_t nb, cudaStream_t st) {
+  switch (support) {
+    case 3: return launch_grid_mma<3, NPOL, true>(a, nb, st);
+    case 4: return launch_grid_mma<4, NPOL, true>(a, nb, st);
+    case 5: return launch_grid_mma<5, NPOL, true>(a, nb, st);
+    case 6: return launch_grid_mma<6, NPOL, true>(a, nb, st);
+    case 7: return launch_grid_mma<7, NPOL, true>(a, nb, st);
+    case 8: return launch_grid_mma<8, NPOL, true>(a, nb, st);
+  }
+  set_error("av_grid_tiled_execute_det: support %d not in [3, 8]", support);
+  return AV_ERR_UNSUPPORTED;
+}
+
+// Largest |re|, |im| of the weighted values and |weight| of the planned
+// samples that the gridder adds (NaN skipped), as bit patterns of
+// non-negative doubles (whose integer order is their numeric order).
+__global__ void __launch_bounds__(256) k_det_bound(TiledGridArgs a, unsigned long long *mx) {
+  const uint32_t n_rec = *a.n_rec;
+  double md = 0.0, mw = 0.0;
+  for (uint32_t r = blockIdx.x * blockDim.x + threadIdx.x; r < n_rec;
+       r += gridDim.x * blockDim.x) {
+    const int64_t vb = (int64_t)a.recs[r].row * a.npol;
+    for (int p = 0; p < a.npol; ++p) {
+      const double w = (double)a.wt[vb + p];
+      double dx = w, dy = 0.0;
+      if (!a.do_psf) {
+        const float2 v = a.vis[vb + p];
+        dx = (double)v.x * w;
+        dy = (double)v.y * w;
+      }
+      if (isnan(dx) || isnan(dy) || (dx == 0.0 && dy == 0.0)) continue;
+      md = fmax(md, fmax(fabs(dx), fabs(dy)));
+      mw = fmax(mw, fabs(w));
+    }
+  }
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    md = fmax(md, __shfl_xor_sync(0xffffffffu, md, o));
+    mw = fmax(mw, __shfl_xor_sync(0xffffffffu, mw, o));
+  }
+  if ((threadIdx.x & 31) == 0) {
+    atomicMax(mx, (unsigned long long)__double_as_longlong(md));
+    atomicMax(mx + 1, (unsigned long long)__double_as_longlong(mw));
+  }
+}
+
+// 2^F with bound * 2^F < 2^61 (2^0 for a zero bound); err = 1 for a bound
+// that is not finite (an infinite value has no fixed-point sum).
+__device__ __forceinline__ double det_scale_of(double bound, int *err) {
+  if (!(bound <= 1.7e308)) {
+    *err = 1;
+    return 0.0;
+  }
+  if (bound == 0.0) return 1.0;
+  int e = 0;
+  frexp(bound, &e);  // bound < 2^e
+  int f = 61 - e;
+  if (f > 1000) f = 1000;
+  return ldexp(1.0, f);
+}
+
+__global__ void k_det_scale(const uint32_t *n_rec, const unsigned long long *mx,
+                            const double *cgk, int cgk_len, int support, double *scale,
+                            int *err) {
+  double mt = 0.0;
+  for (int i = 0; i < cgk_len; ++i) mt = fmax(mt, fabs(cgk[i]));
+  const double n = (double)*n_rec;
+  const double md = __longlong_as_double((long long)mx[0]);
+  const double mw = __longlong_as_double((long long)mx[1]);
+  *err = 0;
+  scale[0] = det_scale_of(n * md * mt * mt, err);
+  scale[1] = det_scale_of(n * mw * (support * mt) * (support * mt), err);
+}
+
+// grid += fixed-point sums / 2^F (one FP64 or FP32 addition per value);
+// sum_weight likewise.
+__global__ void __launch_bounds__(256) k_det_finish(void *grid, int grid_c128,
+                                                    const unsigned long long *q, int64_t n,
+                                                    double *sumw, const unsigned long long *qw,
+                                                    int64_t nw, const double *scale) {
+  const double inv = 1.0 / scale[0], invw = 1.0 / scale[1];
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
+       i += (int64_t)gridDim.x * blockDim.x) {
+    const long long x = (long long)q[2 * i], y = (long long)q[2 * i + 1];
+    if (x == 0 && y == 0) continue;
+    const double re = (double)x * inv, im = (double)y * inv;
+    if (grid_c128) {
+      double2 *g = (double2 *)grid + i;
+      g->x += re;
+      g->y += im;
+    } else {
+      float2 *g = (float2 *)grid + i;
+      g->x = (float)((double)g->x + re);
+      g->y = (float)((double)g->y + im);
+    }
+  }
+  const int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (t < nw) sumw[t] += (double)(long long)qw[t] * invw;
 }
 
 }  // namespace av
@@ -1312,6 +1485,145 @@ int av_grid_tiled_execute(void *grid, int grid_dtype, double *sum_weight, int do
     a.a16 = v16 && ((npol == 4 && wp % 16 == 0) || (npol == 2 && wp % 8 == 0));
   }
   return dispatch_support(a, support, npol_t, nblocks, as_stream(stream));
+}
+
+int av_tiled_plan_order_rows(int64_t nt, int64_t nb, int64_t nchan, int64_t n_u, int64_t n_v,
+                             int64_t n_img_chan, int support, void *workspace,
+                             size_t workspace_bytes, void *stream) {
+  clear_error();
+  PlanGeom g;
+  Plan p;
+  int rc = grid_geom_checked(g, n_u, n_v, support, 100, nt, nb, nchan, n_img_chan, workspace,
+                             workspace_bytes, p, "av_tiled_plan_order_rows");
+  if (rc) return rc;
+  return plan_order_rows(g, p, as_stream(stream));
+}
+
+size_t av_grid_tiled_det_workspace_size(int64_t n_img_chan, int64_t n_img_pol, int64_t n_u,
+                                        int64_t n_v) {
+  const size_t cells = (size_t)(n_img_chan > 0 ? n_img_chan : 1) *
+                       (size_t)(n_img_pol > 0 ? n_img_pol : 1) * (size_t)(n_u > 0 ? n_u : 1) *
+                       (size_t)(n_v > 0 ? n_v : 1);
+  const size_t planes = (size_t)(n_img_chan > 0 ? n_img_chan : 1) *
+                        (size_t)(n_img_pol > 0 ? n_img_pol : 1);
+  return Workspace::need(sizeof(unsigned long long) * 2 * cells) +
+         Workspace::need(sizeof(unsigned long long) * planes) +
+         Workspace::need(sizeof(unsigned long long) * 2) + Workspace::need(sizeof(double) * 2) +
+         Workspace::need(sizeof(int) * 4);
+}
+
+int av_grid_tiled_execute_det(void *grid, int grid_dtype, double *sum_weight, int do_psf,
+                              const void *vis, int vis_dtype, const void *weight,
+                              int weight_dtype, const int32_t *pol_map, const double *cgk,
+                              int64_t n_u, int64_t n_v, int support, int oversampling, int64_t nt,
+                              int64_t nb, int64_t nchan, int64_t npol, int64_t n_img_chan,
+                              int64_t n_img_pol, void *workspace, size_t workspace_bytes,
+                              void *det_workspace, size_t det_workspace_bytes, void *stream) {
+  clear_error();
+  AV_CHECK_ARG(grid && sum_weight && weight && pol_map && cgk && det_workspace,
+               "av_grid_tiled_execute_det: null pointer");
+  AV_CHECK_ARG(do_psf || vis, "av_grid_tiled_execute_det: vis is required unless do_psf");
+  AV_CHECK_ARG(grid_dtype == AV_C64 || grid_dtype == AV_C128,
+               "av_grid_tiled_execute_det: grid must be complex64 or complex128");
+  AV_CHECK_ARG(do_psf || vis_dtype == AV_C64, "av_grid_tiled_execute_det: vis must be complex64");
+  AV_CHECK_ARG(weight_dtype == AV_F32, "av_grid_tiled_execute_det: weight must be float32");
+  AV_CHECK_ARG(npol >= 0 && npol <= 4 && n_img_pol >= 1 && n_img_pol <= 4,
+               "av_grid_tiled_execute_det: npol and n_img_pol must be in [1, 4]");
+  AV_CHECK_ARG(support >= 3 && support <= 8,
+               "av_grid_tiled_execute_det: deterministic gridding covers supports 3-8");
+  AV_CHECK_ARG((((uintptr_t)det_workspace) & 255) == 0,
+               "av_grid_tiled_execute_det: det_workspace must be 256-byte aligned");
+  const size_t need = av_grid_tiled_det_workspace_size(n_img_chan, n_img_pol, n_u, n_v);
+  if (det_workspace_bytes < need) {
+    set_error("av_grid_tiled_execute_det: det_workspace %zu bytes < %zu needed",
+              det_workspace_bytes, need);
+    return AV_ERR_WORKSPACE;
+  }
+  PlanGeom g;
+  Plan p;
+  int rc = grid_geom_checked(g, n_u, n_v, support, oversampling, nt, nb, nchan, n_img_chan,
+                             workspace, workspace_bytes, p, "av_grid_tiled_execute_det");
+  if (rc) return rc;
+  int64_t rows = nt * nb * nchan;
+  if (rows == 0 || npol == 0) return AV_OK;
+  const int64_t cells = n_img_chan * n_img_pol * n_u * n_v, planes = n_img_chan * n_img_pol;
+  Workspace dw(det_workspace, det_workspace_bytes);
+  unsigned long long *qg = dw.take<unsigned long long>(2 * cells);
+  unsigned long long *qw = dw.take<unsigned long long>(planes);
+  unsigned long long *mx = dw.take<unsigned long long>(2);
+  double *scale = dw.take<double>(2);
+  int *err = dw.take<int>(4);
+  cudaStream_t st = as_stream(stream);
+  int npol_t = npol <= 1 ? 1 : (npol <= 2 ? 2 : 4);
+  TiledGridArgs a;
+  a.recs = p.recs;
+  a.tile_start = p.tile_start;
+  a.n_rec = p.offs + g.n_keys();
+  a.n_tiles = g.n_tiles();
+  a.ntu = g.ntu;
+  a.ntv = g.ntv;
+  int64_t nblocks = 0;
+  a.chunk = grid_chunking(rows, nblocks);
+  a.sched = p.counters;
+  a.vis = (const float2 *)vis;
+  a.wt = (const float *)weight;
+  a.do_psf = do_psf;
+  a.cgk = cgk;
+  a.cgk_len = oversampling * (support / 2 + 1);
+  a.os = oversampling;
+  a.pol_map = pol_map;
+  a.npol = (int)npol;
+  a.npg = (int)n_img_pol;
+  a.grid = grid;
+  a.grid_c128 = grid_dtype == AV_C128;
+  a.sumw = sum_weight;
+  a.n_u = n_u;
+  a.n_v = n_v;
+  a.inv_norm = 0;
+  a.flag = nullptr;
+  a.det_grid = qg;
+  a.det_sumw = qw;
+  a.det_scale = scale;
+  {
+    const uintptr_t vp = (uintptr_t)vis, wp = (uintptr_t)weight;
+    const bool v16 = do_psf || vp % 16 == 0;
+    a.a16 = v16 && ((npol == 4 && wp % 16 == 0) || (npol == 2 && wp % 8 == 0));
+  }
+  AV_CUDA(cudaMemsetAsync(qg, 0, sizeof(unsigned long long) * (size_t)(2 * cells), st));
+  AV_CUDA(cudaMemsetAsync(qw, 0, sizeof(unsigned long long) * (size_t)planes, st));
+  AV_CUDA(cudaMemsetAsync(mx, 0, sizeof(unsigned long long) * 2, st));
+  const int sms = sm_count();
+  k_det_bound<<<(unsigned)(sms * 4), 256, 0, st>>>(a, mx);
+  AV_LAUNCH_CHECK();
+  k_det_scale<<<1, 1, 0, st>>>(a.n_rec, mx, cgk, a.cgk_len, support, scale, err);
+  AV_LAUNCH_CHECK();
+  int host[2] = {0, 0};
+  uint32_t ordered = 0;
+  AV_CUDA(cudaMemcpyAsync(&host[0], err, sizeof(int), cudaMemcpyDeviceToHost, st));
+  AV_CUDA(cudaMemcpyAsync(&ordered, p.counters + PLAN_ROWS_ORDERED, sizeof(uint32_t),
+                          cudaMemcpyDeviceToHost, st));
+  AV_CUDA(cudaStreamSynchronize(st));
+  if (ordered != 1u) {
+    set_error("av_grid_tiled_execute_det: the plan's records are not ordered by row "
+              "(av_tiled_plan_order_rows)");
+    return AV_ERR_ARG;
+  }
+  if (host[0]) {
+    set_error("av_grid_tiled_execute_det: an infinite weighted value or weight has no "
+              "fixed-point sum");
+    return AV_ERR_ARG;
+  }
+  if (npol_t == 1) rc = dispatch_det_npol<1>(a, support, nblocks, st);
+  else if (npol_t == 2) rc = dispatch_det_npol<2>(a, support, nblocks, st);
+  else rc = dispatch_det_npol<4>(a, support, nblocks, st);
+  if (rc) return rc;
+  int64_t fb = (cells + 255) / 256;
+  if (fb > (int64_t)sms * 8) fb = (int64_t)sms * 8;
+  if (fb < 1) fb = 1;
+  k_det_finish<<<(unsigned)fb, 256, 0, st>>>(grid, a.grid_c128, qg, cells, sum_weight, qw, planes,
+                                            scale);
+  AV_LAUNCH_CHECK();
+  return AV_OK;
 }
 
 // Adjoint of the tiled degridder on a degrid plan (av_degrid_tiled_plan):

@@ -384,6 +384,175 @@ static int scan_counts(uint32_t *counts_then_cursor, uint32_t *offs, int64_t n,
   return AV_OK;
 }
 
+// ------------------------------------------------------------- row order ---
+// For deterministic gridding (av_grid_tiled_execute_det): each key's records
+// ordered by row, so the order in which a cell's samples are summed is a
+// property of the data, not of the scatter pass's atomics.  Keys of up to
+// ORD_WCAP records are sorted by one warp in shared memory, keys of up to
+// ROW_BCAP (224 KiB of records) by one CTA in shared memory
+// (k_plan_order_rows_big, from a list), longer ones by one CTA in place in
+// global memory.  The sort is the bitonic
+// network with every comparator ascending (each size-k merge first compares
+// mirrored pairs), which sorts any n: a pair reaching past n would compare
+// with a virtual +inf and is left alone.  A shared plan's degridder marks
+// (exc_mark) follow their records: during the sort they ride in the top bit
+// of du (a footprint start inside a tile, below TILE).
+constexpr int ROW_WARPS = 8, ROW_BCAP = 28672, ROW_BTHREADS = 1024;
+constexpr size_t ROW_SMEM = (size_t)ROW_WARPS * ORD_WCAP * sizeof(Rec);
+constexpr size_t ROW_BSMEM = (size_t)ROW_BCAP * sizeof(Rec);
+constexpr uint8_t ROW_MARK = 0x80;
+
+__device__ __forceinline__ void row_cmpswap(Rec *x, uint32_t lo, uint32_t hi) {
+  const Rec a = x[lo], b = x[hi];
+  if (b.row < a.row) {
+    x[lo] = b;
+    x[hi] = a;
+  }
+}
+
+// Sorts x[0, n) by row; threads tid = 0 .. nthr - 1 of a warp or CTA, `sync`
+// between the network's stages.
+template <typename Sync>
+__device__ void bitonic_rows(Rec *x, uint32_t n, uint32_t tid, uint32_t nthr, Sync sync) {
+  int lg = 0;  // N = 2^lg >= n
+  while ((1u << lg) < n) ++lg;
+  const uint32_t half = (1u << lg) >> 1;
+  for (int lk = 1; lk <= lg; ++lk) {  // blocks of k = 2^lk
+    const int lh = lk - 1;
+    const uint32_t hm = (1u << lh) - 1u, k = 1u << lk;
+    for (uint32_t i = tid; i < half; i += nthr) {  // mirrored pairs within blocks of k
+      const uint32_t b = (i >> lh) << lk, o = i & hm;
+      if (b + k - 1 - o < n) row_cmpswap(x, b + o, b + k - 1 - o);
+    }
+    sync();
+    for (int lj = lk - 2; lj >= 0; --lj) {  // pairs at distance j = 2^lj
+      const uint32_t jm = (1u << lj) - 1u, j = 1u << lj;
+      for (uint32_t i = tid; i < half; i += nthr) {
+        const uint32_t lo = ((i >> lj) << (lj + 1)) | (i & jm);
+        if (lo + j < n) row_cmpswap(x, lo, lo + j);
+      }
+      sync();
+    }
+  }
+}
+
+// Record base + i with its degridder mark moved into du (the bitmap bit
+// cleared), and back.
+__device__ __forceinline__ Rec take_rec(const Rec *recs, uint32_t *exc_mark, uint32_t pos) {
+  Rec r = recs[pos];
+  const uint32_t bit = 1u << (pos & 31u);
+  if (exc_mark[pos >> 5] & bit) {
+    atomicAnd(exc_mark + (pos >> 5), ~bit);
+    r.du |= ROW_MARK;
+  }
+  return r;
+}
+
+__device__ __forceinline__ void put_rec(Rec *recs, uint32_t *exc_mark, uint32_t pos, Rec r) {
+  if (r.du & ROW_MARK) {
+    r.du &= (uint8_t)~ROW_MARK;
+    atomicOr(exc_mark + (pos >> 5), 1u << (pos & 31u));
+  }
+  recs[pos] = r;
+}
+
+__global__ void __launch_bounds__(ROW_WARPS * 32) k_plan_order_rows(const uint32_t *offs,
+                                                                    int64_t n_keys, Rec *recs,
+                                                                    uint32_t *exc_mark,
+                                                                    uint32_t *big,
+                                                                    uint32_t *n_big) {
+  extern __shared__ __align__(16) unsigned char rsm[];
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  Rec *buf = (Rec *)rsm + (size_t)wid * ORD_WCAP;
+  const int64_t stride = (int64_t)gridDim.x * ROW_WARPS * 32;
+  for (int64_t k0 = ((int64_t)blockIdx.x * ROW_WARPS + wid) * 32; k0 < n_keys; k0 += stride) {
+    const int64_t k = k0 + lane;
+    uint32_t lo = 0, n = 0;
+    if (k < n_keys) {
+      lo = offs[k];
+      n = offs[k + 1] - lo;
+    }
+    if (n > (uint32_t)ORD_WCAP) big[atomicAdd(n_big, 1u)] = (uint32_t)k;
+    unsigned todo = __ballot_sync(0xffffffffu, n >= 2 && n <= (uint32_t)ORD_WCAP);
+    while (todo) {
+      const int src = __ffs(todo) - 1;
+      todo &= todo - 1;
+      const uint32_t klo = __shfl_sync(0xffffffffu, lo, src);
+      const uint32_t kn = __shfl_sync(0xffffffffu, n, src);
+      for (uint32_t i = lane; i < kn; i += 32) buf[i] = take_rec(recs, exc_mark, klo + i);
+      __syncwarp();
+      bitonic_rows(buf, kn, (uint32_t)lane, 32u, []() { __syncwarp(); });
+      for (uint32_t i = lane; i < kn; i += 32) put_rec(recs, exc_mark, klo + i, buf[i]);
+      __syncwarp();
+    }
+  }
+}
+
+__global__ void __launch_bounds__(ROW_BTHREADS) k_plan_order_rows_big(const uint32_t *offs,
+                                                                      Rec *recs,
+                                                                      uint32_t *exc_mark,
+                                                                      const uint32_t *big,
+                                                                      const uint32_t *n_big,
+                                                                      uint32_t *plan_counters) {
+  extern __shared__ __align__(16) unsigned char rsm[];
+  Rec *buf = (Rec *)rsm;
+  const uint32_t nb = *n_big;
+  // the plan's counters[PLAN_ROWS_ORDERED] records that its records are
+  // ordered by row (the plan build zeroes it); read once this launch is done
+  if (blockIdx.x == 0 && threadIdx.x == 0) plan_counters[PLAN_ROWS_ORDERED] = 1u;
+  for (uint32_t it = blockIdx.x; it < nb; it += gridDim.x) {
+    const uint32_t k = big[it];
+    const uint32_t lo = offs[k], n = offs[k + 1] - lo;
+    const bool in_smem = n <= (uint32_t)ROW_BCAP;  // uniform over the CTA
+    if (in_smem) {
+      for (uint32_t i = threadIdx.x; i < n; i += blockDim.x)
+        buf[i] = take_rec(recs, exc_mark, lo + i);
+      __syncthreads();
+      bitonic_rows(buf, n, threadIdx.x, blockDim.x, []() { __syncthreads(); });
+      for (uint32_t i = threadIdx.x; i < n; i += blockDim.x)
+        put_rec(recs, exc_mark, lo + i, buf[i]);
+    } else {
+      for (uint32_t i = threadIdx.x; i < n; i += blockDim.x)
+        recs[lo + i] = take_rec(recs, exc_mark, lo + i);
+      __syncthreads();
+      bitonic_rows(recs + lo, n, threadIdx.x, blockDim.x, []() {
+        __threadfence_block();
+        __syncthreads();
+      });
+      for (uint32_t i = threadIdx.x; i < n; i += blockDim.x)
+        put_rec(recs, exc_mark, lo + i, recs[lo + i]);
+    }
+    __syncthreads();
+  }
+}
+
+int plan_order_rows(const PlanGeom &g, const Plan &p, cudaStream_t st) {
+  static bool configured[64] = {false};
+  int dev = 0;
+  AV_CUDA(cudaGetDevice(&dev));
+  if (dev >= 0 && dev < 64 && !configured[dev]) {
+    AV_CUDA(cudaFuncSetAttribute(k_plan_order_rows, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)ROW_SMEM));
+    AV_CUDA(cudaFuncSetAttribute(k_plan_order_rows_big,
+                                 cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ROW_BSMEM));
+    configured[dev] = true;
+  }
+  const int64_t nk = g.n_keys();
+  const int sms = sm_count();
+  AV_CUDA(cudaMemsetAsync(p.n_big, 0, sizeof(uint32_t), st));
+  int64_t blocks = (nk + ROW_WARPS * 32 - 1) / (ROW_WARPS * 32);
+  if (blocks > (int64_t)sms * 3) blocks = (int64_t)sms * 3;
+  k_plan_order_rows<<<(unsigned)blocks, ROW_WARPS * 32, ROW_SMEM, st>>>(p.offs, nk, p.recs,
+                                                                       p.exc_mark, p.big,
+                                                                       p.n_big);
+  AV_LAUNCH_CHECK();
+  k_plan_order_rows_big<<<(unsigned)sms, ROW_BTHREADS, ROW_BSMEM, st>>>(p.offs, p.recs,
+                                                                        p.exc_mark, p.big,
+                                                                        p.n_big, p.counters);
+  AV_LAUNCH_CHECK();
+  return AV_OK;
+}
+
 // Tile starts, and the plan's scheduling counters set to zero (the tiled
 // kernels take chunks from them and leave them at zero when they finish).
 __global__ void k_tile_starts(const uint32_t *offs, int64_t n_tiles, int64_t kpt,
@@ -438,13 +607,15 @@ bool plan_carve(const PlanGeom &g, Workspace &ws, Plan &p) {
   p.exc_count = ws.take<uint32_t>(4);
   p.exc_rows = ws.take<uint32_t>(g.n_rows > 0 ? g.n_rows : 1);
   p.exc_mark = ws.take<uint32_t>((g.n_rows > 0 ? g.n_rows : 1) / 32 + 2);
+  p.n_big = ws.take<uint32_t>(4);
+  p.big = ws.take<uint32_t>((g.n_rows > 0 ? g.n_rows : 1) / (ORD_WCAP + 1) + 2);
   p.uv = ws.take<double2>(g.nt * g.nb > 0 ? g.nt * g.nb : 1);
   p.freq = ws.take<double>(g.nchan > 0 ? g.nchan : 1);
   p.chan_map = ws.take<int32_t>(g.nchan > 0 ? g.nchan : 1);
   p.dpar = ws.take<double>(4);
   return p.offs && p.cursor && p.tile_start && p.recs && p.scale && p.scan_tmp &&
          p.counters && p.walk_key && p.walk_rec && p.exc_count && p.exc_rows && p.exc_mark &&
-         p.uv &&
+         p.n_big && p.big && p.uv &&
          p.freq && p.chan_map && p.dpar;
 }
 

@@ -33,6 +33,8 @@
 namespace av {
 
 constexpr int TILE = 32;                       // tile edge in cells
+constexpr int PLAN_ROWS_ORDERED = 8;           // Plan::counters entry set by plan_order_rows
+constexpr int ORD_WCAP = 1024;                 // records a warp orders by row (plan_order_rows)
 constexpr int SCAN_MAX_BLOCKS = 65536;                    // scan partials
 constexpr int64_t KEY_BUDGET = (int64_t(1) << 28) - 65536;  // scan capacity: 65536 x 4096 keys
 
@@ -144,6 +146,8 @@ inline size_t plan_workspace_bytes(const PlanGeom &g) {
   b += Workspace::need(sizeof(uint32_t) * 4);
   b += Workspace::need(sizeof(uint32_t) * nr);
   b += Workspace::need(sizeof(uint32_t) * (nr / 32 + 2));     // exc_mark
+  b += Workspace::need(sizeof(uint32_t) * 4);                 // keys too long for a warp
+  b += Workspace::need(sizeof(uint32_t) * (nr / (ORD_WCAP + 1) + 2));  // their list
   b += Workspace::need(sizeof(double2) * ntb);
   b += Workspace::need(sizeof(double) * nc);
   b += Workspace::need(sizeof(int32_t) * nc);
@@ -159,12 +163,15 @@ struct Plan {
   Rec *recs;           // n_rows (only the first n_rec are used)
   double *scale;       // 2 * nchan: per-channel uv scale (gridder convention)
   uint32_t *scan_tmp;
-  uint32_t *counters;
+  uint32_t *counters;  // 16, zero after a build: [0..1] the gridders' chunk schedule,
+                       // [2..3] the degridder's, [PLAN_ROWS_ORDERED] plan_order_rows ran
   uint32_t *walk_key;  // n_rows: key of each sample in walk order (pass 1)
   Rec *walk_rec;       // n_rows: record of each sample in walk order (pass 1)
   uint32_t *exc_count; // [0]: degridder exceptions listed (0 unless shared)
   uint32_t *exc_rows;  // n_rows: their rows
   uint32_t *exc_mark;  // bit per sorted record: the degridder must not use it
+  uint32_t *n_big;     // [0]: keys listed in big (row-order pass)
+  uint32_t *big;       // keys too long for one warp to order by row
   double2 *uv;         // nt * nb: u, v of each (time, baseline) (shared only)
   double *freq;        // nchan (shared only)
   int32_t *chan_map;   // nchan (shared only)
@@ -260,6 +267,10 @@ __device__ __forceinline__ bool sample_pos_degrid(double um, double vm, double f
 int plan_build(const PlanGeom &g, Plan &p, const double *uvw, const double *freq,
                const int32_t *chan_map, double delta_l, double delta_m, cudaStream_t st,
                const float *drop_wt = nullptr, int drop_npol = 0);
+
+// Orders each key's records by row (deterministic gridding); the degridder
+// marks of a shared plan move with their records.
+int plan_order_rows(const PlanGeom &g, const Plan &p, cudaStream_t st);
 
 // Zeroes the grid cells the plan's records can touch (every non-empty tile's
 // footprint region, all npg grid polarisations).

@@ -24,7 +24,10 @@ class Gridder:
     passed to the reference: pixelincr)."""
 
     def __init__(self, uvw, freq, image_size, cell_size, npol, support=7, oversampling=100,
-                 chan_mode="continuum", n_img_pol=None):
+                 chan_mode="continuum", n_img_pol=None, deterministic=False):
+        """deterministic: grid() adds bit-identical results from call to call
+        (plans ordered by row, fixed-point sums: av_grid_tiled_execute_det;
+        supports 3-8, about twice the gridding time)."""
         self.dev = K.device()
         self.uvw = K.on_device(uvw, torch.float64)
         self.freq = K.on_device(freq, torch.float64)
@@ -50,6 +53,10 @@ class Gridder:
         # plan() builds one plan for both directions where it can; False
         # builds the two separately
         self.shared_plan = True
+        self.deterministic = bool(deterministic)
+        if self.deterministic and not 3 <= self.support <= 8:
+            raise ValueError("deterministic gridding covers supports 3-8")
+        self._det_ws = None
 
     # ------------------------------------------------------------- gridding
     def _grid_plan(self):
@@ -62,8 +69,15 @@ class Gridder:
                                            self.support, self.os, self.nt, self.nb, self.nchan,
                                            self.n_img_chan, ws[1], ws[2], K.stream_ptr()),
                   "av_grid_tiled_plan")
+            self._order_rows(ws)
             self._gplan = ws
         return self._gplan
+
+    def _order_rows(self, ws):
+        if self.deterministic:
+            check(lib().av_tiled_plan_order_rows(self.nt, self.nb, self.nchan, self.nx, self.ny,
+                                                 self.n_img_chan, self.support, ws[1], ws[2],
+                                                 K.stream_ptr()), "av_tiled_plan_order_rows")
 
     def clear_grid(self, grid):
         """Zeroes the cells this Gridder's gridding plan can touch (the
@@ -94,6 +108,19 @@ class Gridder:
                                      device=self.dev)
         w = K.on_device(weight, torch.float32)
         v = None if do_psf else K.on_device(vis, torch.complex64)
+        if self.deterministic:
+            need = lib().av_grid_tiled_det_workspace_size(self.n_img_chan, self.n_img_pol,
+                                                          self.nx, self.ny)
+            if self._det_ws is None or self._det_ws[2] < need:
+                self._det_ws = K.workspace(need)
+            dws = self._det_ws
+            check(lib().av_grid_tiled_execute_det(
+                K.p(grid), K.dcode(grid), K.p(sum_weight), int(bool(do_psf)), K.p(v), AV_C64,
+                K.p(w), AV_F32, K.p(self.pol_map), K.p(self.cgk), self.nx, self.ny,
+                self.support, self.os, self.nt, self.nb, self.nchan, self.npol, self.n_img_chan,
+                self.n_img_pol, ws[1], ws[2], dws[1], dws[2], K.stream_ptr()),
+                "av_grid_tiled_execute_det")
+            return grid, sum_weight
         check(lib().av_grid_tiled_execute(K.p(grid), K.dcode(grid), K.p(sum_weight),
                                           int(bool(do_psf)), K.p(v), AV_C64, K.p(w), AV_F32,
                                           K.p(self.pol_map), K.p(self.cgk), self.nx, self.ny,
@@ -124,6 +151,7 @@ class Gridder:
                                              self.support, self.os, self.nt, self.nb,
                                              self.nchan, self.n_img_chan, ws[1], ws[2],
                                              K.stream_ptr()), "av_tiled_plan_shared")
+            self._order_rows(ws)
             self._gplan = ws
             self._dplan = (key, ws)
             return

@@ -246,6 +246,33 @@ int av_tiled_plan_counts(int64_t nt, int64_t nb, int64_t nchan, int64_t n_u, int
                          int64_t n_img_chan, int support, const void *workspace,
                          size_t workspace_bytes, uint32_t *out, void *stream);
 
+/* No counterpart in the reference: bitwise-reproducible gridding.
+ * av_tiled_plan_order_rows orders each cell key's records of a built tiled
+ * plan (gridder or shared; a shared plan's degridder marks move with them)
+ * by row, so the order of a cell's samples no longer depends on the plan
+ * build's atomics.  av_grid_tiled_execute_det then grids like
+ * av_grid_tiled_execute (same arguments; supports 3-8, the FP64 tensor-core
+ * kernel) with every sum past a run's FP64 sum in 64-bit fixed point: the
+ * grid and sum_weight it adds are bit-identical from call to call for the
+ * same plan, inputs and launch settings (AV_TUNE_GRID_CHUNKS_PER_SM), and
+ * within 1e-15 (relative, norm-wise) of the FP64 sums.  It needs
+ * det_workspace (256-byte aligned) of av_grid_tiled_det_workspace_size
+ * bytes, synchronises the stream once (to report an unordered plan or an
+ * infinite value, AV_ERR_ARG) and runs about twice as long as
+ * av_grid_tiled_execute. */
+int av_tiled_plan_order_rows(int64_t nt, int64_t nb, int64_t nchan, int64_t n_u, int64_t n_v,
+                             int64_t n_img_chan, int support, void *workspace,
+                             size_t workspace_bytes, void *stream);
+size_t av_grid_tiled_det_workspace_size(int64_t n_img_chan, int64_t n_img_pol, int64_t n_u,
+                                        int64_t n_v);
+int av_grid_tiled_execute_det(void *grid, int grid_dtype, double *sum_weight, int do_psf,
+                              const void *vis, int vis_dtype, const void *weight,
+                              int weight_dtype, const int32_t *pol_map, const double *cgk,
+                              int64_t n_u, int64_t n_v, int support, int oversampling, int64_t nt,
+                              int64_t nb, int64_t nchan, int64_t npol, int64_t n_img_chan,
+                              int64_t n_img_pol, void *workspace, size_t workspace_bytes,
+                              void *det_workspace, size_t det_workspace_bytes, void *stream);
+
 /* ----------------------------------------------------------- degridding -- */
 /* dgrid_numba, standard_degrid.py:388-485: values (nt, nb, nvchan, nvpol) of
  * values_dtype (AV_C64 / AV_C128) += sum_k w_k grid_k conj(phasor) / sum_k w_k
