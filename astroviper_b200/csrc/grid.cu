@@ -226,8 +226,8 @@ struct TiledGridArgs {
 // cell key, tap-table row offsets) into the warp's shared staging area.
 // k_grid_tiled (RowLanes) keeps the next round's values and the record of
 // the round after in registers while a round is computed; k_grid_mma
-// (MmaLanes) copies raw values two rounds ahead into a per-warp ring in
-// shared memory with cp.async, which holds more loads in flight per SM.
+// (MmaLanes) copies the next round's raw values into a per-warp ring in
+// shared memory with cp.async while a round is computed.
 template <int S, int NPOL>
 struct GCfg {
   // one CTA per SM; as many warps as the registers allow without spilling
@@ -284,7 +284,7 @@ template <int S, int NPOL>
 struct MCfg {
   static constexpr int THREADS = 512;
   static constexpr int WARPS = THREADS / 32;
-  static constexpr int SLOTS = 3;                                  // rounds per ring
+  static constexpr int SLOTS = 2;                                  // rounds per ring
   static constexpr int W = TILE + S - 1;
   static constexpr int RWP = 10;
   static constexpr int SDS = GT_STAGE + 1;
@@ -901,10 +901,12 @@ __device__ __forceinline__ void read_raw(const TiledGridArgs &a, const double2 *
   }
 }
 
-// k_grid_tiled's schedule and segments with MmaLanes and a cp.async ring:
-// the raw values of round rd + 2 are copied while round rd is computed, and
-// records are loaded one round before their copies are issued.  Only for
-// weighted gridding (a.wt != NULL, no 1 / norm scaling).
+// k_grid_tiled's schedule and segments with MmaLanes and a cp.async ring of
+// two slots: the raw values of round rd + 1 are copied while round rd is
+// computed (a round of 32 samples takes several microseconds, well beyond
+// the copies' latency; a third slot, two rounds ahead, measured 3 % slower),
+// and records are loaded one round before their copies are issued.  Only
+// for weighted gridding (a.wt != NULL, no 1 / norm scaling).
 template <int S, int NPOL, bool DET = false>
 __global__ void __launch_bounds__(MCfg<S, NPOL>::THREADS, 1) k_grid_mma(TiledGridArgs a) {
   using C = MCfg<S, NPOL>;
@@ -979,8 +981,8 @@ __global__ void __launch_bounds__(MCfg<S, NPOL>::THREADS, 1) k_grid_mma(TiledGri
 #pragma unroll
       for (int p = 0; p < NPOL; ++p) sw[p] = 0.0;
 
-      // records of rounds rd .. rd + 2 (row 0xffffffff: none)
-      Rec rc0, rc1, rc2;
+      // records of rounds rd and rd + 1 (row 0xffffffff: none)
+      Rec rc0, rc1;
       auto load_rec = [&](int rd) {
         const uint32_t r = w_lo + (uint32_t)rd * GT_STAGE + lane;
         Rec x;
@@ -990,14 +992,11 @@ __global__ void __launch_bounds__(MCfg<S, NPOL>::THREADS, 1) k_grid_mma(TiledGri
       };
       rc0 = load_rec(0);
       rc1 = load_rec(1);
-      rc2 = load_rec(2);
       if (rc0.row != 0xffffffffu) issue_raw<NPOL>(a, wring, lane, rc0.row);
-      cp_async_commit();
-      if (rc1.row != 0xffffffffu) issue_raw<NPOL>(a, wring + C::SLOT, lane, rc1.row);
       cp_async_commit();
       for (int rd = 0; rd < n_rounds; ++rd) {
         double2 *slot = wring + (rd % C::SLOTS) * C::SLOT;
-        cp_async_wait<1>();  // this lane's copies of round rd are complete
+        cp_async_wait<0>();  // this lane's copies of round rd are complete
         // ---- stage: FP64 weighted values in place of the raw ones, the
         // cell key and the offsets of the two tap-table rows
         int my_key = -1;
@@ -1024,12 +1023,12 @@ __global__ void __launch_bounds__(MCfg<S, NPOL>::THREADS, 1) k_grid_mma(TiledGri
         int prev = __shfl_up_sync(0xffffffffu, my_key, 1);
         if (lane == 0) prev = cur;
         const unsigned starts = __ballot_sync(0xffffffffu, my_key >= 0 && my_key != prev);
-        // ---- copies of round rd + 2 (into the slot round rd - 1 used) and
-        // the record of round rd + 3
-        if (rc2.row != 0xffffffffu)
-          issue_raw<NPOL>(a, wring + ((rd + 2) % C::SLOTS) * C::SLOT, lane, rc2.row);
+        // ---- copies of round rd + 1 (into the slot round rd - 1 used) and
+        // the record of round rd + 2
+        if (rc1.row != 0xffffffffu)
+          issue_raw<NPOL>(a, wring + ((rd + 1) % C::SLOTS) * C::SLOT, lane, rc1.row);
         cp_async_commit();
-        const Rec rc3 = load_rec(rd + 3);
+        const Rec rc2 = load_rec(rd + 2);
         __syncwarp();
         // ---- compute the round's samples in runs of one cell
         const int jn = (int)min((uint32_t)GT_STAGE, w_hi - (w_lo + (uint32_t)rd * GT_STAGE));
@@ -1047,7 +1046,6 @@ __global__ void __launch_bounds__(MCfg<S, NPOL>::THREADS, 1) k_grid_mma(TiledGri
         __syncwarp();
         rc0 = rc1;
         rc1 = rc2;
-        rc2 = rc3;
       }
       cp_async_wait<0>();
       if (cur >= 0) lanes.template flush<DET>(sre, sim, cur, dscale);
