@@ -551,6 +551,24 @@ struct MmaLanes {
       }
     }
   }
+
+  // A whole round of one cell (32 samples, eight full groups), unrolled so
+  // the next groups' operand loads overlap the current group's MMAs.
+  __device__ __forceinline__ void run_full(const double2 *wd, const int *wm,
+                                           const double *tab) {
+#pragma unroll
+    for (int j = 0; j < GT_STAGE; j += 4) {
+      const int s = j + t;
+      const int ro = wm[s];
+      const double cu = tab[(ro & 0xffff) + g];
+      const double cv = tab[(ro >> 16) + g];
+#pragma unroll
+      for (int p = 0; p < NPOL; ++p) {
+        const double2 d = wd[p * C::SDS + s];
+        mma_f64_m16n8k4(acc[p], cu * d.x, cu * d.y, cv);
+      }
+    }
+  }
 };
 
 // Sum of weights of a warp's slice: one atomic per warp and polarisation.
@@ -1008,12 +1026,21 @@ __global__ void __launch_bounds__(MCfg<S, NPOL>::THREADS, 1) k_grid_mma(TiledGri
 #pragma unroll
           for (int p = 0; p < NPOL; ++p) {
             double2 d;
-            if (a.do_psf) d = make_double2((double)w[p], 0.0);
-            else d = make_double2((double)v[p].x * (double)w[p], (double)v[p].y * (double)w[p]);
             // the reference skips NaN and exact-zero weighted data
-            // (standard_grid.py:378)
-            const bool ok = p < a.npol && !isnan(d.x) && !isnan(d.y) &&
-                            (d.x != 0.0 || d.y != 0.0);
+            // (standard_grid.py:378); tested on the FP32 factors: their FP64
+            // product is exact, NaN exactly when their FP32 product is, and
+            // zero exactly when a factor is (the FP32 pipe, not the FP64 one
+            // the MMAs use)
+            bool ok;
+            if (a.do_psf) {
+              d = make_double2((double)w[p], 0.0);
+              ok = !isnan(w[p]) && w[p] != 0.f;
+            } else {
+              d = make_double2((double)v[p].x * (double)w[p], (double)v[p].y * (double)w[p]);
+              ok = !isnan(__fmul_rn(v[p].x, w[p])) && !isnan(__fmul_rn(v[p].y, w[p])) &&
+                   w[p] != 0.f && (v[p].x != 0.f || v[p].y != 0.f);
+            }
+            ok = ok && p < a.npol;
             slot[p * C::SDS + lane] = ok ? d : make_double2(0.0, 0.0);
             if (ok) sw[p] += (double)w[p] * nrm;
           }
@@ -1033,6 +1060,14 @@ __global__ void __launch_bounds__(MCfg<S, NPOL>::THREADS, 1) k_grid_mma(TiledGri
         // ---- compute the round's samples in runs of one cell
         const int jn = (int)min((uint32_t)GT_STAGE, w_hi - (w_lo + (uint32_t)rd * GT_STAGE));
         int j = 0;
+        if (starts <= 1u && jn == GT_STAGE) {  // one run over the whole round
+          if (starts) {
+            if (cur >= 0) lanes.template flush<DET>(sre, sim, cur, dscale);
+            cur = __shfl_sync(0xffffffffu, my_key, 0);
+          }
+          lanes.run_full(slot, wm, tab);
+          j = jn;
+        }
         while (j < jn) {
           if ((starts >> j) & 1u) {
             if (cur >= 0) lanes.template flush<DET>(sre, sim, cur, dscale);
