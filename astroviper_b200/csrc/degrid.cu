@@ -751,92 +751,104 @@ __global__ void __launch_bounds__(TC_THREADS, 2) k_degrid_tc(TiledDegridArgs a) 
             ((unsigned long long)__ballot_sync(FULL, kb >= 0 && kb != pb) << 32);
         __syncwarp();
         const int jn = (int)min((uint32_t)TC_ROUND, w_hi - (w_lo + (uint32_t)rd * TC_ROUND));
-        int j = 0;
-        while (j < jn) {
-          if ((starts >> j) & 1ull) {
-            const Rec rj = wrec[j];
-            cur = (int)rj.du | ((int)rj.dv << 8);
-            const int du = rj.du, dv = rj.dv;
-            const bool rok = g < S;
+        // a run starts at sample j: its cell's patch, split, into bh / bl
+        auto load_patch = [&](const int j) {
+          const Rec rj = wrec[j];
+          cur = (int)rj.du | ((int)rj.dv << 8);
+          const int du = rj.du, dv = rj.dv;
+          const bool rok = g < S;
 #pragma unroll
-            for (int pol = 0; pol < 4; ++pol) {
-              float2 v0 = make_float2(0.f, 0.f), v1 = make_float2(0.f, 0.f);
-              if (rok && t < S) v0 = sub[((du + g) * W + dv + t) * 4 + pol];
-              if (rok && t + 4 < S) v1 = sub[((du + g) * W + dv + t + 4) * 4 + pol];
-              tf32_split(v0.x, bh[2 * pol][0], bl[2 * pol][0]);
-              tf32_split(v1.x, bh[2 * pol][1], bl[2 * pol][1]);
-              tf32_split(v0.y, bh[2 * pol + 1][0], bl[2 * pol + 1][0]);
-              tf32_split(v1.y, bh[2 * pol + 1][1], bl[2 * pol + 1][1]);
-            }
+          for (int pol = 0; pol < 4; ++pol) {
+            float2 v0 = make_float2(0.f, 0.f), v1 = make_float2(0.f, 0.f);
+            if (rok && t < S) v0 = sub[((du + g) * W + dv + t) * 4 + pol];
+            if (rok && t + 4 < S) v1 = sub[((du + g) * W + dv + t + 4) * 4 + pol];
+            tf32_split(v0.x, bh[2 * pol][0], bl[2 * pol][0]);
+            tf32_split(v1.x, bh[2 * pol][1], bl[2 * pol][1]);
+            tf32_split(v0.y, bh[2 * pol + 1][0], bl[2 * pol + 1][0]);
+            tf32_split(v1.y, bh[2 * pol + 1][1], bl[2 * pol + 1][1]);
           }
+        };
+        // one group of 16 samples [j0, j0 + 16) of a run ending at j1
+        auto group = [&](const int j0, const int j1) {
+          // samples j0 + g and j0 + g + 8 of the round (an empty slot reads
+          // sample j0 and contributes a zero row of W)
+          const int sg = j0 + g, sh = j0 + g + 8;
+          const bool vg = sg < j1, vh = sh < j1;
+          const Rec recg = wrec[vg ? sg : j0], rech = wrec[vh ? sh : j0];
+          const float invg = winv[vg ? sg : j0], invh = winv[vh ? sh : j0];
+          const int oug = recg.ou, ovg = recg.ov, ouh = rech.ou, ovh = rech.ov;
+          // A = the column taps of samples g and g + 8 (columns t, t + 4),
+          // split in the table; an empty slot is a zero row
+          const uint2 z = make_uint2(0u, 0u);
+          const uint2 ag0 = vg ? tabs[ovg * RW + t] : z, ag1 = vg ? tabs[ovg * RW + t + 4] : z;
+          const uint2 ah0 = vh ? tabs[ovh * RW + t] : z, ah1 = vh ? tabs[ovh * RW + t + 4] : z;
+          // row taps r = 2t, 2t + 1 for the final sum over rows
+          const float2 cg = *(const float2 *)&tab[oug * RW + 2 * t];
+          const float2 ch = *(const float2 *)&tab[ouh * RW + 2 * t];
+          // D[m][(q, r)] = sum_c cv_m[c] P[q][r][c]: the row sums, one
+          // n-tile (8 rows) per output q, three TF32 products each
+          float dq[8][4];
+  #pragma unroll
+          for (int q = 0; q < 8; ++q) {
+            dq[q][0] = dq[q][1] = dq[q][2] = dq[q][3] = 0.f;
+            mma_tf32(dq[q], ag0.y, ah0.y, ag1.y, ah1.y, bh[q][0], bh[q][1]);
+            mma_tf32(dq[q], ag0.x, ah0.x, ag1.x, ah1.x, bl[q][0], bl[q][1]);
+            mma_tf32(dq[q], ag0.x, ah0.x, ag1.x, ah1.x, bh[q][0], bh[q][1]);
+          }
+          // V[m][q] = sum_r cu_m[r] D[m][(q, r)]: rows 2t, 2t + 1 here, the
+          // other rows in the quad's other lanes
+          float vgq[8], vhq[8];
+  #pragma unroll
+          for (int q = 0; q < 8; ++q) {
+            float pg = __fmul_rn(cg.x, dq[q][0]);
+            pg = __fmaf_rn(cg.y, dq[q][1], pg);
+            float ph = __fmul_rn(ch.x, dq[q][2]);
+            ph = __fmaf_rn(ch.y, dq[q][3], ph);
+            pg = __fadd_rn(pg, __shfl_xor_sync(FULL, pg, 1));
+            ph = __fadd_rn(ph, __shfl_xor_sync(FULL, ph, 1));
+            pg = __fadd_rn(pg, __shfl_xor_sync(FULL, pg, 2));
+            ph = __fadd_rn(ph, __shfl_xor_sync(FULL, ph, 2));
+            vgq[q] = pg;
+            vhq[q] = ph;
+          }
+          // this lane writes polarisation t, from grid polarisation src
+          float xgre = 0.f, xgim = 0.f, xhre = 0.f, xhim = 0.f;
+  #pragma unroll
+          for (int pol = 0; pol < 4; ++pol)
+            if (pol == src) {
+              xgre = vgq[2 * pol];
+              xgim = vgq[2 * pol + 1];
+              xhre = vhq[2 * pol];
+              xhim = vhq[2 * pol + 1];
+            }
+          // a shared plan's marked sample gets 0 here (k_degrid_exceptions
+          // writes the ones the degridder keeps)
+          float2 *out = (float2 *)d.values;
+          const bool ug = (recg.row & REC_DEGRID_EXC) == 0u;
+          const bool uh = (rech.row & REC_DEGRID_EXC) == 0u;
+          if (vg)
+            out[(int64_t)(recg.row & ~REC_DEGRID_EXC) * 4 + t] =
+                (src >= 0 && ug) ? make_float2(__fmul_rn(xgre, invg), __fmul_rn(xgim, invg))
+                                 : make_float2(0.f, 0.f);
+          if (vh)
+            out[(int64_t)(rech.row & ~REC_DEGRID_EXC) * 4 + t] =
+                (src >= 0 && uh) ? make_float2(__fmul_rn(xhre, invh), __fmul_rn(xhim, invh))
+                                 : make_float2(0.f, 0.f);
+        };
+        int j = 0;
+        // a round of one run: its four groups with the run's end known (no
+        // empty-slot selects)
+        if (starts <= 1ull && jn == TC_ROUND) {
+          if (starts) load_patch(0);
+#pragma unroll 1
+          for (int j0 = 0; j0 < TC_ROUND; j0 += 16) group(j0, TC_ROUND);
+          j = jn;
+        }
+        while (j < jn) {
+          if ((starts >> j) & 1ull) load_patch(j);
           const unsigned long long later = j < 63 ? (starts & (~1ull << j)) : 0ull;
           const int j1 = later ? min(jn, __ffsll((long long)later) - 1) : jn;
-          for (int j0 = j; j0 < j1; j0 += 16) {
-            // samples j0 + g and j0 + g + 8 of the round (an empty slot reads
-            // sample j0 and contributes a zero row of W)
-            const int sg = j0 + g, sh = j0 + g + 8;
-            const bool vg = sg < j1, vh = sh < j1;
-            const Rec recg = wrec[vg ? sg : j0], rech = wrec[vh ? sh : j0];
-            const float invg = winv[vg ? sg : j0], invh = winv[vh ? sh : j0];
-            const int oug = recg.ou, ovg = recg.ov, ouh = rech.ou, ovh = rech.ov;
-            // A = the column taps of samples g and g + 8 (columns t, t + 4),
-            // split in the table; an empty slot is a zero row
-            const uint2 z = make_uint2(0u, 0u);
-            const uint2 ag0 = vg ? tabs[ovg * RW + t] : z, ag1 = vg ? tabs[ovg * RW + t + 4] : z;
-            const uint2 ah0 = vh ? tabs[ovh * RW + t] : z, ah1 = vh ? tabs[ovh * RW + t + 4] : z;
-            // row taps r = 2t, 2t + 1 for the final sum over rows
-            const float2 cg = *(const float2 *)&tab[oug * RW + 2 * t];
-            const float2 ch = *(const float2 *)&tab[ouh * RW + 2 * t];
-            // D[m][(q, r)] = sum_c cv_m[c] P[q][r][c]: the row sums, one
-            // n-tile (8 rows) per output q, three TF32 products each
-            float dq[8][4];
-#pragma unroll
-            for (int q = 0; q < 8; ++q) {
-              dq[q][0] = dq[q][1] = dq[q][2] = dq[q][3] = 0.f;
-              mma_tf32(dq[q], ag0.y, ah0.y, ag1.y, ah1.y, bh[q][0], bh[q][1]);
-              mma_tf32(dq[q], ag0.x, ah0.x, ag1.x, ah1.x, bl[q][0], bl[q][1]);
-              mma_tf32(dq[q], ag0.x, ah0.x, ag1.x, ah1.x, bh[q][0], bh[q][1]);
-            }
-            // V[m][q] = sum_r cu_m[r] D[m][(q, r)]: rows 2t, 2t + 1 here, the
-            // other rows in the quad's other lanes
-            float vgq[8], vhq[8];
-#pragma unroll
-            for (int q = 0; q < 8; ++q) {
-              float pg = __fmul_rn(cg.x, dq[q][0]);
-              pg = __fmaf_rn(cg.y, dq[q][1], pg);
-              float ph = __fmul_rn(ch.x, dq[q][2]);
-              ph = __fmaf_rn(ch.y, dq[q][3], ph);
-              pg = __fadd_rn(pg, __shfl_xor_sync(FULL, pg, 1));
-              ph = __fadd_rn(ph, __shfl_xor_sync(FULL, ph, 1));
-              pg = __fadd_rn(pg, __shfl_xor_sync(FULL, pg, 2));
-              ph = __fadd_rn(ph, __shfl_xor_sync(FULL, ph, 2));
-              vgq[q] = pg;
-              vhq[q] = ph;
-            }
-            // this lane writes polarisation t, from grid polarisation src
-            float xgre = 0.f, xgim = 0.f, xhre = 0.f, xhim = 0.f;
-#pragma unroll
-            for (int pol = 0; pol < 4; ++pol)
-              if (pol == src) {
-                xgre = vgq[2 * pol];
-                xgim = vgq[2 * pol + 1];
-                xhre = vhq[2 * pol];
-                xhim = vhq[2 * pol + 1];
-              }
-            // a shared plan's marked sample gets 0 here (k_degrid_exceptions
-            // writes the ones the degridder keeps)
-            float2 *out = (float2 *)d.values;
-            const bool ug = (recg.row & REC_DEGRID_EXC) == 0u;
-            const bool uh = (rech.row & REC_DEGRID_EXC) == 0u;
-            if (vg)
-              out[(int64_t)(recg.row & ~REC_DEGRID_EXC) * 4 + t] =
-                  (src >= 0 && ug) ? make_float2(__fmul_rn(xgre, invg), __fmul_rn(xgim, invg))
-                                   : make_float2(0.f, 0.f);
-            if (vh)
-              out[(int64_t)(rech.row & ~REC_DEGRID_EXC) * 4 + t] =
-                  (src >= 0 && uh) ? make_float2(__fmul_rn(xhre, invh), __fmul_rn(xhim, invh))
-                                   : make_float2(0.f, 0.f);
-          }
+          for (int j0 = j; j0 < j1; j0 += 16) group(j0, j1);
           j = j1;
         }
       }
