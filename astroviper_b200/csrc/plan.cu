@@ -154,6 +154,8 @@ __global__ void __launch_bounds__(256) k_plan_count(PlanGeom g, const double *__
       vm = uvw[3 * (size_t)tb + 1];
     }
     uint32_t widx = w.b * nchan * nt + w.t;
+    // unrolled so the position arithmetic of several channels overlaps
+#pragma unroll 4
     for (uint32_t c = 0; c < nchan; ++c, widx += nt) {
       const int plane = __ldg(chan_map + c);
       const double us0 = __ldg(scale + 2 * c), us1 = __ldg(scale + 2 * c + 1);

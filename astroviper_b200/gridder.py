@@ -57,6 +57,7 @@ class Gridder:
         if self.deterministic and not 3 <= self.support <= 8:
             raise ValueError("deterministic gridding covers supports 3-8")
         self._det_ws = None
+        self._dpolmaps = {}
 
     # ------------------------------------------------------------- gridding
     def _grid_plan(self):
@@ -167,6 +168,15 @@ class Gridder:
         cur.wait_stream(self._side)
 
     # ----------------------------------------------------------- degridding
+    def _degrid_polmap(self, g_npol):
+        """Device polarisation map i % g_npol, made once per grid: an upload
+        from pageable memory on every call would wait for the stream."""
+        pm = self._dpolmaps.get(g_npol)
+        if pm is None:
+            pm = K.on_device(np.arange(self.npol) % g_npol, torch.int32)
+            self._dpolmaps[g_npol] = pm
+        return pm
+
     def _degrid_plan(self, g_nchan):
         key = int(g_nchan)
         if self._dplan is None or self._dplan[0] != key:
@@ -197,7 +207,7 @@ class Gridder:
             values = torch.empty((self.nt, self.nb, self.nchan, self.npol),
                                  dtype=torch.complex64, device=self.dev)
             accumulate = False
-        pm = K.on_device(np.round(np.arange(self.npol) % g_npol).astype(int), torch.int32)
+        pm = self._degrid_polmap(g_npol)
         fl = None if flag is None else K.on_device(flag).to(torch.uint8).contiguous()
         dph = None if dphase is None else K.on_device(dphase, torch.float64)
         check(lib().av_degrid_tiled_execute(K.p(dph), K.p(values), K.dcode(values),
