@@ -11,19 +11,104 @@ maps and the support search are small host logic.  conv_kernels computes the
 two Fourier transforms the reference's driver takes of the baseline patterns
 (:111-127) with cuFFT.
 
-The driver make_gridding_convolution_function itself (:24-193) reads the
-measurement set through xradio's accessors and returns an xarray Dataset;
-neither library is a dependency here, so it is not mirrored: its steps are
-the functions of this module, in the order conv_kernels documents.
+The driver make_gridding_convolution_function (:24-193) reads the
+measurement set through the accessors xradio gives an MSv4 dataset (any
+object with the same attributes works) and returns an xarray Dataset when
+xarray is installed, else the minimal dataset.Dataset.
 make_phase_gradient uses the SIN projection directly, where the reference
 asks astropy.wcs for it.
 """
+import copy
 import itertools
 
 import numpy as np
 import torch
 
 from ... import _kernels as K
+from ...utils.check_params import check_sel_params
+from .check_imaging_parameters import check_gcf_params, check_grid_params
+from .dataset import new_dataset
+
+
+def _values(x):
+    return np.asarray(getattr(x, "values", x))
+
+
+def make_gridding_convolution_function(gcf_xds, ms_xds, gcf_params, grid_params, sel_params):
+    """The A-projection convolution functions of one measurement set
+    (make_gridding_convolution_function.py:24-193).  gcf_params gives the
+    beam function (airy / casa_airy), the dish and blockage diameters per
+    antenna type, each antenna's type (unique_ant_indx), the phase direction
+    and the kernel oversampling / support limits; the frequencies,
+    polarisations, baselines' antennas and field phase centre come from
+    ms_xds.  When gcf_xds holds no variables, or another number of baselines,
+    the kernels are built anew: per pair of antenna types and beam frequency
+    the products of the two beams (and of their squares), Fourier transformed
+    on the device, cropped to (max_support + 1) x oversampling and normalised
+    (SUPPORT, CONV_KERNEL, CONV_KERNEL_CONVOLVED, PS_CORR_IMAGE, the
+    baseline / channel / polarisation maps and the attributes cell_uv and
+    oversampling).  PHASE_GRADIENT is always (re)made.  Returns the dataset;
+    the caller's parameter dicts are left as they were."""
+    _gcf_params = copy.deepcopy(gcf_params)
+    _grid_params = copy.deepcopy(grid_params)
+    _sel_params = copy.deepcopy(sel_params)
+    data_group_in, _ = check_sel_params(ms_xds, _sel_params, default_data_group_in_name="base")
+    _gcf_params["field_phase_dir"] = ms_xds.xr_ms.get_field_and_source_xds(
+        data_group_in["data_group_in_name"]).FIELD_PHASE_CENTER_DIRECTION.isel(field_name=0)
+    # each baseline's antennas as the reference finds them: the entries of
+    # antenna x baseline name matches in row-major order
+    names = _values(ms_xds.antenna_xds.antenna_name).ravel()
+    ids = [np.where(names[:, None] == _values(b).ravel()[None, :])[0]
+           for b in (ms_xds.baseline_antenna1_name, ms_xds.baseline_antenna2_name)]
+    _gcf_params["basline_ant"] = np.array(ids).T
+    _gcf_params["freq_chan"] = _values(ms_xds.frequency)
+    _gcf_params["pol"] = _values(ms_xds.polarization)
+    assert check_gcf_params(_gcf_params), "######### ERROR: gcf_params checking failed"
+    assert check_grid_params(_grid_params), "######### ERROR: grid_params checking failed"
+    _gcf_params["resize_conv_size"] = (_gcf_params["max_support"] + 1) * \
+        _gcf_params["oversampling"]
+
+    if len(gcf_xds) < 1 or gcf_xds.baseline.size != len(_gcf_params["basline_ant"]):
+        from .imaging_utils.make_pb_symmetric import airy_disk_rorder, casa_airy_disk_rorder
+        funcs = {"airy": airy_disk_rorder, "casa_airy": casa_airy_disk_rorder}
+        assert _gcf_params["function"] in funcs, \
+            "######### ERROR: Only airy and casa_airy function has been implemented"
+        pb_func = funcs[_gcf_params["function"]]
+        gcf_xds = new_dataset()
+        cf_baseline_map, pb_ant_pairs = create_cf_baseline_map(
+            _gcf_params["unique_ant_indx"], _gcf_params["basline_ant"],
+            len(_gcf_params["list_dish_diameters"]))
+        cf_chan_map, pb_freq = create_cf_chan_map(_gcf_params["freq_chan"],
+                                                  _gcf_params["chan_tolerance_factor"])
+        cf_pol_map = np.zeros((len(_gcf_params["pol"]),), dtype=int)  # one beam for all pols
+        pb_pol = np.array([0])
+        kernels = []
+        for ipower in (1, 2):  # the beams, then their squares
+            _gcf_params["ipower"] = ipower
+            kernels.append(conv_kernels(make_baseline_patterns(
+                pb_freq, pb_pol, pb_ant_pairs, pb_func, _gcf_params, _grid_params)))
+        conv_kernel, conv_kernel_convolved, conv_support = resize_and_calc_support(
+            kernels[0], kernels[1], _gcf_params, _grid_params)
+        lead = ("conv_baseline", "conv_chan", "conv_pol")
+        gcf_xds["SUPPORT"] = (lead + ("xy",), conv_support)
+        gcf_xds["CONV_KERNEL_CONVOLVED"] = (lead + ("u", "v"), conv_kernel_convolved)
+        gcf_xds["CONV_KERNEL"] = (lead + ("u", "v"), conv_kernel)
+        gcf_xds["PS_CORR_IMAGE"] = (("l", "m"), np.ones(_grid_params["image_size"]))
+        gcf_xds["CF_BASELINE_MAP"] = (("baseline",), cf_baseline_map)
+        gcf_xds["CF_CHAN_MAP"] = (("chan",), cf_chan_map)
+        gcf_xds["CF_POL_MAP"] = (("pol",), cf_pol_map)
+        gcf_xds.attrs["cell_uv"] = 1 / (_grid_params["image_size_padded"] *
+                                        _grid_params["cell_size"] * _gcf_params["oversampling"])
+        gcf_xds.attrs["oversampling"] = _gcf_params["oversampling"]
+        # the reference also builds u, v, xy, field_id, l, m coordinates here
+        # but drops the dataset assign_coords returns, so none are attached
+
+    field_phase_dir = np.array(getattr(_gcf_params["field_phase_dir"], "data",
+                                       _gcf_params["field_phase_dir"]))
+    gcf_xds["PHASE_GRADIENT"] = (("field_id", "u", "v"),
+                                 make_phase_gradient(field_phase_dir[None, :], _gcf_params,
+                                                     _grid_params))
+    return gcf_xds
 
 
 def make_baseline_patterns(pb_freq, pb_pol, pb_ant_pairs, pb_func, gcf_params, grid_params):

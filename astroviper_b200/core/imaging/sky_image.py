@@ -36,6 +36,10 @@ class _Var:
     def shape(self):
         return tuple(self.values.shape)
 
+    @property
+    def size(self):
+        return int(np.prod(self.values.shape))
+
     def __len__(self):
         return int(self.values.shape[0]) if len(self.values.shape) else 1
 

@@ -10,9 +10,11 @@ make_pb_symmetric.py beams, the convolution-function helpers of
 make_gridding_convolution_function.py (create_cf_baseline_map,
 create_cf_chan_map, make_baseline_patterns, resize_and_calc_support,
 calc_conv_size) and its Numba kernels mosaic_grid_jit / aperture_grid_jit
-(mosaic_grid.py), run on a convolution function the helpers build.  The
-reference modules are imported unmodified, with stand-in modules for xarray
-and toolviper's logger.
+(mosaic_grid.py), run on a convolution function the helpers build; and
+gcf_driver.npz with the variables the driver make_gridding_convolution_function
+itself builds for a duck-typed measurement set (``... make_golden_mosaic.py
+gcf_driver`` writes only that one).  The reference modules are imported
+unmodified, with stand-in modules for xarray and toolviper's logger.
 """
 import os
 import sys
@@ -75,6 +77,92 @@ def load_reference():
     ns.gcf = _mod("astroviper.core.imaging.make_gridding_convolution_function",
                   SRC + "/core/imaging/make_gridding_convolution_function.py")
     return ns
+
+
+class _DA:
+    """xarray.DataArray stand-in: values and dims."""
+
+    def __init__(self, data, coords=None, dims=None):
+        self.data = self.values = np.asarray(data)
+        self.dims = (dims,) if isinstance(dims, str) else tuple(dims or ())
+
+
+class _DS:
+    """xarray.Dataset stand-in for the driver: item assignment, attrs, len,
+    assign_coords.  Every instance is kept in CREATED, so the dataset the
+    driver fills can be read back after the call."""
+    CREATED = []
+
+    def __init__(self):
+        self.vars = {}
+        self.attrs = {}
+        _DS.CREATED.append(self)
+
+    def __len__(self):
+        return len(self.vars)
+
+    def __setitem__(self, name, value):
+        self.vars[name] = value
+
+    def assign_coords(self, coords):
+        return self
+
+
+def make_gcf_driver(ns):
+    """make_gridding_convolution_function (:24-193) on a duck-typed MSv4
+    dataset of 6 antennas of two types (12 m / 25 m dishes) and 15 baselines
+    whose antenna-2 names are not sorted, 7 channels over 1.0-1.5 GHz, 2
+    polarisations.  Its last step, make_phase_gradient, needs astropy.wcs,
+    which this container lacks: the call stops there with ImportError, after
+    every other variable is in the dataset, which _DS keeps.  Writes
+    gcf_driver.npz."""
+    import xarray
+    xarray.Dataset = _DS
+    xarray.DataArray = _DA
+    ns.gcf.xr = xarray
+    names = [f"ant{i}" for i in range(6)]
+    pairs = [(i, j) for i in range(6) for j in range(i + 1, 6)]
+    freq = np.linspace(1.0e9, 1.5e9, 7)
+    pols = np.array(["XX", "YY"])
+    ra_dec = np.array([0.31, -0.52])
+
+    class _Field:
+        def isel(self, **kw):
+            return types.SimpleNamespace(data=ra_dec)
+
+    ms = types.SimpleNamespace(
+        data_vars=["VISIBILITY", "UVW", "WEIGHT", "FLAG"],
+        attrs={"data_groups": {"base": {"correlated_data": "VISIBILITY", "uvw": "UVW",
+                                        "weight": "WEIGHT", "flag": "FLAG"}}},
+        xr_ms=types.SimpleNamespace(get_field_and_source_xds=lambda name: types.SimpleNamespace(
+            FIELD_PHASE_CENTER_DIRECTION=_Field())),
+        # xarray compares (antenna) with (baseline) names as a 2-D outer test
+        antenna_xds=types.SimpleNamespace(antenna_name=np.array(names)[:, None]),
+        baseline_antenna1_name=np.array([names[i] for i, _ in pairs]),
+        baseline_antenna2_name=np.array([names[j] for _, j in pairs]),
+        frequency=types.SimpleNamespace(values=freq),
+        polarization=types.SimpleNamespace(values=pols))
+    gcf_params = {"function": "casa_airy", "list_dish_diameters": [12.0, 25.0],
+                  "list_blockage_diameters": [0.75, 0.0], "unique_ant_indx": [0, 1, 0, 1, 1, 0],
+                  "oversampling": [4, 4], "max_support": [11, 11], "support_cut_level": 0.025,
+                  "chan_tolerance_factor": 0.05,
+                  "phase_direction": types.SimpleNamespace(values=np.array([0.3, -0.5]))}
+    grid_params = {"image_size": [64, 64], "cell_size": [-1e-4, 1e-4], "fft_padding": 1.5,
+                   "chan_mode": "cube"}
+    _DS.CREATED.clear()
+    try:
+        ns.gcf.make_gridding_convolution_function(_DS(), ms, gcf_params, grid_params, {})
+        raise SystemExit("expected the driver to stop at astropy.wcs")
+    except ImportError:
+        pass
+    ds = _DS.CREATED[-1]
+    d = {f"var_{k}": v.values for k, v in ds.vars.items()}
+    d.update({f"dims_{k}": np.array(v.dims) for k, v in ds.vars.items()})
+    d["attr_cell_uv"] = ds.attrs["cell_uv"]
+    d["attr_oversampling"] = ds.attrs["oversampling"]
+    d.update(names=np.array(names), pairs=np.array(pairs), freq=freq, pols=pols, ra_dec=ra_dec)
+    np.savez_compressed(os.path.join(HERE, "gcf_driver.npz"), **d)
+    print("wrote gcf_driver.npz", sorted(ds.vars))
 
 
 def main():
@@ -185,4 +273,8 @@ def main():
 
 
 if __name__ == "__main__":
-    main()
+    if sys.argv[1:] == ["gcf_driver"]:
+        make_gcf_driver(load_reference())
+    else:
+        main()
+        make_gcf_driver(load_reference())

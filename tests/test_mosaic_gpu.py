@@ -144,3 +144,73 @@ def test_tiled_mosaic_matches_per_sample_kernel(chan_mode):
         assert np.abs(ga).max() > 0
         assert rel(gb, ga) <= 1e-12, i
         assert np.allclose(sb, sa, rtol=1e-12), i
+
+
+def _duck_ms(g, names_2d=False):
+    """An MSv4-like dataset with the attributes the driver reads."""
+    import types
+    names = [str(x) for x in g["names"]]
+    pairs = g["pairs"]
+
+    class _Field:
+        def isel(self, **kw):
+            return types.SimpleNamespace(data=g["ra_dec"])
+
+    return types.SimpleNamespace(
+        data_vars=["VISIBILITY", "UVW", "WEIGHT", "FLAG"],
+        attrs={"data_groups": {"base": {"correlated_data": "VISIBILITY", "uvw": "UVW",
+                                        "weight": "WEIGHT", "flag": "FLAG"}}},
+        xr_ms=types.SimpleNamespace(get_field_and_source_xds=lambda name: types.SimpleNamespace(
+            FIELD_PHASE_CENTER_DIRECTION=_Field())),
+        antenna_xds=types.SimpleNamespace(antenna_name=np.array(names)),
+        baseline_antenna1_name=np.array([names[i] for i, _ in pairs]),
+        baseline_antenna2_name=np.array([names[j] for _, j in pairs]),
+        frequency=types.SimpleNamespace(values=g["freq"]),
+        polarization=types.SimpleNamespace(values=g["pols"]))
+
+
+def test_make_gridding_convolution_function_driver():
+    """The driver (make_gridding_convolution_function.py:24-193) against the
+    variables the reference's own driver built (tests/golden/gcf_driver.npz):
+    maps and supports equal, kernels within cuFFT's rounding of numpy's FFT;
+    PHASE_GRADIENT (the reference's needs astropy.wcs, absent) equal to
+    make_phase_gradient's for the field centre.  A second call on the result
+    keeps its kernels and remakes the phase gradient only."""
+    import types
+    from astroviper_b200.core.imaging import make_gridding_convolution_function as G
+    from astroviper_b200.core.imaging.dataset import Dataset
+    g = golden("gcf_driver.npz")
+    gcf_params = {"function": "casa_airy", "list_dish_diameters": [12.0, 25.0],
+                  "list_blockage_diameters": [0.75, 0.0], "unique_ant_indx": [0, 1, 0, 1, 1, 0],
+                  "oversampling": [4, 4], "max_support": [11, 11], "support_cut_level": 0.025,
+                  "chan_tolerance_factor": 0.05,
+                  "phase_direction": types.SimpleNamespace(values=np.array([0.3, -0.5]))}
+    grid_params = {"image_size": [64, 64], "cell_size": [-1e-4, 1e-4], "fft_padding": 1.5,
+                   "chan_mode": "cube"}
+    before = repr(gcf_params), repr(grid_params)
+    ds = G.make_gridding_convolution_function(Dataset(), _duck_ms(g), gcf_params, grid_params,
+                                              {})
+    assert (repr(gcf_params), repr(grid_params)) == before  # the caller's dicts untouched
+    for name in ("SUPPORT", "CF_BASELINE_MAP", "CF_CHAN_MAP", "CF_POL_MAP", "PS_CORR_IMAGE"):
+        assert np.array_equal(ds[name].values, g[f"var_{name}"]), name
+        assert tuple(ds[name].dims) == tuple(str(x) for x in g[f"dims_{name}"]), name
+    for name in ("CONV_KERNEL", "CONV_KERNEL_CONVOLVED"):
+        assert tuple(ds[name].dims) == tuple(str(x) for x in g[f"dims_{name}"])
+        a, b = ds[name].values, g[f"var_{name}"]
+        assert np.linalg.norm(a - b) <= 1e-12 * np.linalg.norm(b), name
+    assert np.array_equal(ds.attrs["cell_uv"], g["attr_cell_uv"])
+    assert np.array_equal(ds.attrs["oversampling"], g["attr_oversampling"])
+    pg_params = {"phase_direction": gcf_params["phase_direction"],
+                 "oversampling": np.array([4, 4]), "resize_conv_size": np.array([48, 48])}
+    pg = G.make_phase_gradient(g["ra_dec"][None, :], pg_params,
+                               {"image_size_padded": np.array([96, 96]),
+                                "cell_size": np.array([-1e-4, 1e-4])})
+    assert ds["PHASE_GRADIENT"].dims == ("field_id", "u", "v")
+    assert np.array_equal(ds["PHASE_GRADIENT"].values, pg)
+    # reuse: same number of baselines, kernels kept
+    kept = ds["CONV_KERNEL"].values
+    ds2 = G.make_gridding_convolution_function(ds, _duck_ms(g), gcf_params, grid_params, {})
+    assert ds2 is ds and ds2["CONV_KERNEL"].values is kept
+    with pytest.raises(AssertionError, match="gcf_params checking failed"):
+        G.make_gridding_convolution_function(Dataset(), _duck_ms(g), dict(gcf_params,
+                                             function="gauss"), grid_params, {})

@@ -85,3 +85,80 @@ def test_oracle_mosaic_grid_matches_reference():
             want = g[f"mg_{tag}_{int(do_psf)}_grid"]
             assert np.array_equal(grid, want), (tag, do_psf)
             assert np.array_equal(sw, g[f"mg_{tag}_{int(do_psf)}_sw"]), (tag, do_psf)
+
+
+def test_check_params_semantics(capsys):
+    """utils/check_params.py:4-189: defaults written, lists by length and
+    element type, scalars by type / value / range, dict entries filled."""
+    from astroviper_b200.utils.check_params import check_params
+    d = {}
+    assert check_params(d, "x", [int], default=3) and d["x"] == 3
+    assert not check_params(d, "y", [int])
+    assert "must be specified" in capsys.readouterr().out
+    d = {"a": [1, 2], "b": [1, 2.5], "c": [1, 2, 3], "s": "cube", "r": 11.0}
+    assert check_params(d, "a", [list], list_acceptable_data_types=[int], list_len=2)
+    assert not check_params(d, "b", [list], list_acceptable_data_types=[int], list_len=2)
+    assert "Wrong type of" in capsys.readouterr().out
+    assert not check_params(d, "c", [list], list_acceptable_data_types=[int], list_len=2)
+    assert "Wrong length" in capsys.readouterr().out
+    assert check_params(d, "c", [list, np.array], list_acceptable_data_types=[int], list_len=-1)
+    assert not check_params(d, "s", [str], acceptable_data=["continuum"])
+    assert not check_params(d, "r", [float], acceptable_range=[1, 10])
+    assert "within the range" in capsys.readouterr().out
+    assert not check_params(d, "r", [int])
+    # a dict parameter: missing entries from the default; it passes whatever
+    # its entries' checks find, as in the reference
+    d = {"p": {"k1": "wrong type"}}
+    assert check_params(d, "p", [dict], default={"k1": 1, "k2": 2.0})
+    assert d["p"] == {"k1": "wrong type", "k2": 2.0}
+
+
+def test_grid_and_gcf_param_checks():
+    from astroviper_b200.core.imaging.check_imaging_parameters import (check_gcf_params,
+                                                                       check_grid_params)
+    g = {"image_size": [100, 80], "cell_size": [1e-5, 1e-5], "fft_padding": 1.5}
+    assert check_grid_params(g)
+    assert np.array_equal(g["image_size_padded"], [150, 120])
+    assert np.array_equal(g["image_center"], [50, 40]) and g["chan_mode"] == "cube"
+    assert not check_grid_params({"image_size": [100, 80], "cell_size": [1e-5, 1e-5],
+                                  "fft_padding": 20.0})
+    gcf = {"freq_chan": [1e9], "list_dish_diameters": [12.0, 25.0],
+           "list_blockage_diameters": [0.75], "unique_ant_indx": [0, 1], "pol": ["XX"]}
+    assert not check_gcf_params(gcf)  # diameters of different lengths
+    gcf["list_blockage_diameters"] = [0.75, 0.0]
+    assert check_gcf_params(gcf)
+    assert gcf["function"] == "casa_airy" and np.array_equal(gcf["oversampling"], [10, 10])
+    assert gcf["max_support"].dtype.kind == "i" and gcf["a_chan_num_chunk"] == 3
+
+
+def test_check_sel_params_data_groups():
+    import types
+    from astroviper_b200.utils.check_params import check_sel_params
+    xds = types.SimpleNamespace(data_vars=["VISIBILITY", "WEIGHT"],
+                                attrs={"data_groups": {"base": {"correlated_data": "VISIBILITY",
+                                                                "weight": "WEIGHT"}}})
+    gin, gout = check_sel_params(xds, {}, default_data_group_in_name="base",
+                                 default_data_group_out_name="imaging",
+                                 default_data_group_out_modified={"weight_imaging":
+                                                                  "WEIGHT_IMAGING"})
+    assert gin["data_group_in_name"] == "base" and gout["data_group_out_name"] == "imaging"
+    assert gout["weight_imaging"] == "WEIGHT_IMAGING" and gout["weight"] == "WEIGHT"
+    with pytest.raises(AssertionError, match="not found in xds data_groups"):
+        check_sel_params(xds, {"data_group_in_name": "other"})
+    with pytest.raises(AssertionError, match="already exists in xds"):
+        check_sel_params(xds, {"data_group_out": {"weight": "WEIGHT"}},
+                         default_data_group_in_name="base")
+
+
+def test_minimal_dataset():
+    from astroviper_b200.core.imaging.dataset import Dataset
+    ds = Dataset()
+    assert len(ds) == 0
+    ds["A"] = (("baseline", "u"), np.zeros((5, 3)))
+    ds["B"] = (("baseline",), np.arange(5))
+    assert len(ds) == 2 and ds.baseline.size == 5 and ds.sizes == {"baseline": 5, "u": 3}
+    assert ds["B"].dims == ("baseline",) and "A" in ds
+    with pytest.raises(ValueError):
+        ds["C"] = (("baseline",), np.arange(4))
+    ds2 = ds.assign_coords({"u": np.arange(3)})
+    assert "u" in ds2.coords and "u" not in ds.coords
