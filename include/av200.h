@@ -255,7 +255,8 @@ int av_tiled_plan_counts(int64_t nt, int64_t nb, int64_t nchan, int64_t n_u, int
  * kernel) with every sum past a run's FP64 sum in 64-bit fixed point: the
  * grid and sum_weight it adds are bit-identical from call to call for the
  * same plan, inputs and launch settings (AV_TUNE_GRID_CHUNKS_PER_SM), and
- * within 1e-15 (relative, norm-wise) of the FP64 sums.  It needs
+ * agree with av_grid_tiled_execute's to within the FP64 summation order
+ * (the tests hold both to 1e-13, norm-wise, of the FP64 oracle).  It needs
  * det_workspace (256-byte aligned) of av_grid_tiled_det_workspace_size
  * bytes, synchronises the stream once (to report an unordered plan or an
  * infinite value, AV_ERR_ARG) and runs about twice as long as
