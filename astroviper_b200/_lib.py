@@ -17,7 +17,7 @@ AV_TUNE_GRID_CHUNKS_PER_SM, AV_TUNE_DEGRID_CHUNKS_PER_SM, AV_TUNE_GRID_LANES, \
     AV_TUNE_DEGRID_LANES, AV_TUNE_HOGBOM_BARRIER_TIMEOUT_US = range(5)
 AV_HOGBOM_BARRIER_TIMEOUT_US_DEFAULT = 2000000
 AV_GRID_LANES_MMA, AV_GRID_LANES_ROWS, AV_GRID_LANES_AUTO = 1, 2, 3
-AV_DEGRID_LANES_TF32, AV_DEGRID_LANES_FP32, AV_DEGRID_LANES_AUTO = 1, 2, 3
+AV_DEGRID_LANES_TF32, AV_DEGRID_LANES_FP32, AV_DEGRID_LANES_AUTO, AV_DEGRID_LANES_TC05 = 1, 2, 3, 4
 
 _vp = ctypes.c_void_p
 _i = ctypes.c_int
@@ -54,6 +54,7 @@ SIGNATURES = {
     "av_tiled_plan_shared": (_i, [_vp, _vp, _vp, _i64, _i64, _d, _d, _i, _i, _i64, _i64, _i64,
                                   _i64, _vp, _sz, _vp]),
     "av_tiled_plan_counts": (_i, [_i64, _i64, _i64, _i64, _i64, _i64, _i, _vp, _sz, _vp, _vp]),
+    "av_degrid_fault_read": (_i, [_vp, _i, _vp]),
     "av_grid_tiled_execute": (_i, [_vp, _i, _vp, _i, _vp, _i, _vp, _i, _vp, _vp, _i64, _i64, _i,
                                    _i, _i64, _i64, _i64, _i64, _i64, _i64, _vp, _sz, _vp]),
     "av_grid_tiled_execute_det": (_i, [_vp, _i, _vp, _i, _vp, _i, _vp, _i, _vp, _vp, _i64, _i64,

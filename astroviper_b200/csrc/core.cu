@@ -204,9 +204,9 @@ int av_tune_set(int knob, int64_t value) {
   AV_CHECK_ARG(knob != AV_TUNE_GRID_LANES || value <= 3,
                "av_tune_set: AV_TUNE_GRID_LANES takes 1 (mma), 2 (rows) or 3 (auto), not %lld",
                (long long)value);
-  AV_CHECK_ARG(knob != AV_TUNE_DEGRID_LANES || value <= 3,
-               "av_tune_set: AV_TUNE_DEGRID_LANES takes 1 (tf32), 2 (fp32) or 3 (auto), "
-               "not %lld",
+  AV_CHECK_ARG(knob != AV_TUNE_DEGRID_LANES || value <= 4,
+               "av_tune_set: AV_TUNE_DEGRID_LANES takes 1 (tf32), 2 (fp32), 3 (auto) or 4 "
+               "(tc05), not %lld",
                (long long)value);
   g_tune[knob].store(value);
   return AV_OK;

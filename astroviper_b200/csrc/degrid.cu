@@ -10,6 +10,7 @@
 //   FP32 FMAs; the normalisation sum_k w_k is (sum_i cu_i)(sum_j cv_j) from
 //   FP64 per-offset row sums.
 #include "plan.cuh"
+#include "umma.cuh"
 
 namespace av {
 
@@ -590,10 +591,17 @@ struct TCSmem {
   static_assert(S <= 8, "an 8 x 8 footprint");
 };
 
+// x rounded to TF32 (10 stored mantissa bits), to nearest with ties away
+// from zero, as a float bit pattern whose low 13 bits are zero: the same
+// result as cvt.rna.tf32.f32, computed on the integer pipe (the conversion
+// unit's throughput is far lower).  Adding half a TF32 unit to the magnitude
+// bits and truncating rounds the magnitude up at a tie; a carry into the
+// exponent gives the next binade, or infinity past the largest value.  NaN
+// becomes the canonical NaN (its payload could otherwise carry into the sign).
 __device__ __forceinline__ uint32_t tf32_rna(float x) {
-  uint32_t r;
-  asm("cvt.rna.tf32.f32 %0, %1;\n" : "=r"(r) : "f"(x));
-  return r;
+  const uint32_t b = __float_as_uint(x);
+  const uint32_t r = (b + 0x1000u) & 0xFFFFE000u;
+  return (b & 0x7FFFFFFFu) > 0x7F800000u ? 0x7FFFFFFFu : r;
 }
 
 // x = hi + lo, both TF32 (lo: the remainder rounded to TF32)
@@ -867,6 +875,385 @@ __global__ void __launch_bounds__(TC_THREADS, 2) k_degrid_tc(TiledDegridArgs a) 
   }
 }
 
+// ------------------------------------------- fifth-generation tensor cores --
+// k_degrid_umma: the same fast store path as k_degrid_tc on tcgen05.  A
+// warpgroup (128 threads) takes tiles of up to 128 consecutive records of one
+// cell and computes the row sums
+//   D[m][(p, re|im, r)] = sum over c of cv_m[c] P[(p, re|im, r)][c]
+// for the tile's samples in one MMA chain: M = 128 samples, N = 64, K = 8
+// columns, TF32 operands from shared memory, FP32 accumulators in tensor
+// memory.  Operands are split into TF32 high parts and TF32-rounded
+// remainders as in k_degrid_tc; the products lo.hi, hi.lo and hi.hi
+// accumulate into the same columns.  Sample m (tensor-memory lane m, thread m
+// of the warpgroup) then reads its row of D and forms
+//   V[m][p] = sum over r of cu_m[r] D[m][(p, re|im, r)]
+// with its row taps: no shuffles, one 32-byte store per sample.  Row and
+// column taps come divided by their offsets' tap sums, so V carries the
+// sample's 1 / norm (the reference's norm, the sum of the 2-D taps,
+// standard_degrid.py:464-485, is the product of the two sums).  Row n of the
+// B operand (output polarisation p, real or imaginary part, footprint row r)
+// is n = 16 p + 8 (re|im) + r and reads grid polarisation polmap[p].  A is
+// stored K-major in 8-row x 16-byte core matrices: element (m, c) at byte
+// (m % 8) 16 + (m / 8) 256 + (c / 4) 128 + (c % 4) 4; B the same with n for m.
+// Two stages of operands and accumulators per warpgroup: the MMA of tile i
+// runs while the warpgroup finishes tile i - 1 and loads tile i + 1's
+// records; the pipeline runs on across segments and chunks (the epilogue
+// reads no sub-grid).  One CTA of four warpgroups per SM holds all 512
+// tensor-memory columns (4 x 2 stages x 64).  Every wait for an MMA is
+// bounded: a wait that gives up sets g_degrid_fault, and the warpgroup stops
+// issuing, waits once more (bounded) before the CTA frees its tensor memory,
+// and leaves its remaining samples unwritten.
+constexpr int UM_THREADS = 512;
+constexpr int UM_WG = UM_THREADS / 128;
+constexpr int UM_SPIN = 1 << 22;     // mbarrier probes before a wait gives up
+constexpr uint32_t UM_STAGE = 12288; // per stage: A hi | A lo | B hi | B lo
+// set (sticky) when a wait of k_degrid_umma for its MMAs gave up;
+// av_degrid_fault_read reads and clears it
+__device__ uint32_t g_degrid_fault = 0u;
+
+template <int S>
+struct UMSmem {
+  static constexpr int W = TILE + S - 1;
+  // 256 x 8 FP32 taps, each divided by its offset's tap sum (so that the
+  // products of a row's and a column's taps carry 1 / norm), their TF32 high
+  // parts and remainders
+  static constexpr size_t off_tab = 0;
+  static constexpr size_t off_tabh = off_tab + 256 * 8 * 4;
+  static constexpr size_t off_tabl = off_tabh + 256 * 8 * 4;
+  static constexpr size_t off_ops = off_tabl + 256 * 8 * 4;
+  static constexpr size_t off_sub = off_ops + (size_t)UM_WG * 2 * UM_STAGE;
+  static constexpr size_t sub_bytes = (size_t)W * W * 4 * sizeof(float2);  // [cell][pol]
+  static constexpr size_t total = off_sub + sub_bytes;
+  static_assert(off_ops % 1024 == 0 && off_sub % 16 == 0, "alignment");
+  // more than half of an SM's shared memory: one CTA (and its 512 tensor-
+  // memory columns) per SM
+  static_assert(total > 116 * 1024 && total <= 227 * 1024, "one CTA per SM");
+  static_assert(S <= 8, "an 8 x 8 footprint");
+};
+
+__device__ __forceinline__ uint32_t um_kmaj(int n, int c) {
+  return (uint32_t)((n & 7) * 16 + (n >> 3) * 256 + (c >> 2) * 128 + (c & 3) * 4);
+}
+
+// The bounded wait of one thread for an MMA commit; false: it gave up.
+__device__ __forceinline__ bool um_wait(uint64_t *mbar, uint32_t parity) {
+  for (int it = 0; it < UM_SPIN; ++it)
+    if (umma::mbar_try_wait(mbar, parity)) return true;
+  return false;
+}
+
+template <int S>
+__global__ void __launch_bounds__(UM_THREADS, 1) k_degrid_umma(TiledDegridArgs a) {
+  using M = UMSmem<S>;
+  constexpr int W = M::W;
+  constexpr unsigned FULL = 0xffffffffu;
+  extern __shared__ __align__(16) unsigned char smem[];
+  float *tab = (float *)(smem + M::off_tab);
+  uint32_t *tabh = (uint32_t *)(smem + M::off_tabh);
+  uint32_t *tabl = (uint32_t *)(smem + M::off_tabl);
+  float2 *sub = (float2 *)(smem + M::off_sub);
+  __shared__ __align__(8) uint64_t s_mbar[UM_WG][2];
+  __shared__ uint32_t s_mask[UM_WG][4];
+  __shared__ int s_key[UM_WG];
+  __shared__ int s_fault[UM_WG];
+  __shared__ uint32_t s_taddr;
+  __shared__ int s_chunk;
+  const DegridArgs &d = a.d;
+  const int tid = threadIdx.x, wg = tid >> 7, t = tid & 127, j = t >> 5, lane = tid & 31;
+
+  // taps of offset o - 128 (the reference's kernel indices |sampling ix +
+  // off|, standard_degrid.py:466-469), over their FP64 sum; a zero sum gives
+  // zero taps (and a zero value, as norm == 0 does in the reference)
+  for (int o = tid; o < 256; o += UM_THREADS) {
+    const int off = o - 128;
+    double v[8], s = 0.0;
+#pragma unroll
+    for (int i = 0; i < 8; ++i) {
+      v[i] = 0.0;
+      if (i < S) {
+        int k = d.sampling * (i - S / 2) + off;
+        k = k < 0 ? -k : k;
+        v[i] = (k < a.cgk_len) ? d.cf[k] : 0.0;
+        s += v[i];
+      }
+    }
+#pragma unroll
+    for (int i = 0; i < 8; ++i) {
+      const float x = s != 0.0 ? (float)(v[i] / s) : 0.f;
+      tab[o * 8 + i] = x;
+      tf32_split(x, tabh[o * 8 + i], tabl[o * 8 + i]);
+    }
+  }
+  if (tid < 32) {
+    umma::tmem_alloc(&s_taddr, 512);
+    umma::tmem_relinquish();
+  }
+  if (tid < UM_WG) {
+    umma::mbar_init(&s_mbar[tid][0], 1);
+    umma::mbar_init(&s_mbar[tid][1], 1);
+    s_fault[tid] = 0;
+  }
+  umma::mbar_init_fence();
+  umma::fence_before_sync();
+  __syncthreads();
+  umma::fence_after_sync();
+  const uint32_t tmem = s_taddr + (uint32_t)(wg * 128);  // two stages of 64 columns
+  unsigned char *ops = smem + M::off_ops + (size_t)wg * 2 * UM_STAGE;
+  const uint32_t ops_s = umma::smem_addr(ops);
+  // the B rows this thread builds: output polarisation bp, footprint row br,
+  // columns 2 bc and 2 bc + 1; grid polarisation bsrc (-1: zeros)
+  const int bp = t >> 5, br = (t >> 2) & 7, bc = t & 3;
+  int bsrc = -1;
+  {
+    const int v = d.polmap[bp];
+    if (v >= 0 && v < 4 && v < d.g_npol) bsrc = v;
+  }
+  const uint32_t boff = 8192 + um_kmaj(16 * bp + br, 2 * bc);  // real part; imaginary 8 rows on
+  const uint32_t aoff = (uint32_t)((t & 7) * 16 + (t >> 3) * 256);
+  const int64_t gplane = d.g_n2 * d.g_n3;
+  const uint32_t n_rec = *a.n_rec;
+  const uint32_t n_all = (uint32_t)a.n_rows;
+  const int64_t n_chunks = ((int64_t)n_all + a.chunk - 1) / a.chunk;
+  const uint32_t idesc = umma::idesc_tf32(128, 64);
+  uint32_t tiles = 0;       // this warpgroup's tiles so far: stage = tiles & 1
+  uint32_t ph = 0u;         // bit s: the parity stage s's next commit completes
+  int bkey0 = -1, bkey1 = -1;  // the cell whose footprint each stage's B holds
+  bool fault = false;
+  int stuck = -1;           // the stage whose commit this thread gave up on
+  // the tile whose MMA is in flight: its samples, stage and length
+  bool pend = false;
+  int pL = 0, ps = 0;
+  uint32_t prow = 0u, pmk = 0u;
+  int pou = 0;
+
+  // waits for the pending tile's MMA, then each sample of it reads its row of
+  // D, weights it with its row taps and writes its 4 values
+  auto finish = [&]() {
+    if (um_wait(&s_mbar[wg][ps], (ph >> ps) & 1u)) {
+      ph ^= 1u << ps;
+    } else {
+      stuck = ps;
+      s_fault[wg] = 1;
+      atomicExch(&g_degrid_fault, 1u);
+    }
+    umma::fence_after_sync();
+    if (32 * j < pL) {
+      uint32_t d0[32], d1[32];
+      const uint32_t ta = tmem + (uint32_t)(ps * 64) + ((uint32_t)(32 * j) << 16);
+      umma::ld_32x32b_x32(ta, d0);
+      umma::ld_32x32b_x32(ta + 32, d1);
+      umma::wait_ld(d0);
+      umma::wait_ld(d1);
+      if (t < pL) {
+        const float4 c0 = *(const float4 *)(tab + pou * 8);
+        const float4 c1 = *(const float4 *)(tab + pou * 8 + 4);
+        const float cu[8] = {c0.x, c0.y, c0.z, c0.w, c1.x, c1.y, c1.z, c1.w};
+        float v[8];
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+          float s = __fmul_rn(cu[0], __uint_as_float(d0[q * 8]));
+#pragma unroll
+          for (int r = 1; r < S; ++r) s = __fmaf_rn(cu[r], __uint_as_float(d0[q * 8 + r]), s);
+          v[q] = s;
+          float s1 = __fmul_rn(cu[0], __uint_as_float(d1[q * 8]));
+#pragma unroll
+          for (int r = 1; r < S; ++r) s1 = __fmaf_rn(cu[r], __uint_as_float(d1[q * 8 + r]), s1);
+          v[4 + q] = s1;
+        }
+        float4 o0 = make_float4(0.f, 0.f, 0.f, 0.f), o1 = o0;
+        if (!pmk) {
+          o0 = make_float4(v[0], v[1], v[2], v[3]);
+          o1 = make_float4(v[4], v[5], v[6], v[7]);
+        }
+        float4 *out = (float4 *)d.values + (int64_t)prow * 2;
+        out[0] = o0;
+        out[1] = o1;
+      }
+    }
+    umma::fence_before_sync();
+    pend = false;
+  };
+
+  for (;;) {
+    __syncthreads();
+    if (tid == 0) s_chunk = (int)atomicAdd(&a.sched[0], 1u);
+    __syncthreads();
+    const int64_t ch = s_chunk;
+    if (ch >= n_chunks) break;
+    const uint32_t r0 = (uint32_t)(ch * a.chunk);
+    const uint32_t r1 = (uint32_t)min((int64_t)n_all, (int64_t)r0 + a.chunk);
+    if (r1 > n_rec) {  // skipped samples (after the usable records) get zeros
+      const uint32_t z0 = max(r0, n_rec);
+      for (uint32_t rb = z0; rb < r1; rb += UM_THREADS) {
+        const uint32_t r = rb + tid;
+        if (r >= r1) continue;
+        const int64_t row = a.recs[r].row;
+        for (int p = 0; p < 4; ++p) put_value(d, 0, row * 4 + p, 0.0, 0.0);
+      }
+    }
+    const uint32_t v1 = min(r1, n_rec);
+    if (r0 >= v1) continue;
+
+    int tt = find_tile_warp(a.tile_start, a.n_tiles, r0);
+    uint32_t seg_lo = r0;
+    while (seg_lo < v1) {
+      const uint32_t t_end = a.tile_start[tt + 1];
+      const uint32_t seg_hi = min(v1, t_end);
+      if (seg_hi <= seg_lo) {
+        ++tt;
+        continue;
+      }
+      const int64_t plane = tt / (a.ntu * a.ntv);
+      const int64_t trem = tt - plane * a.ntu * a.ntv;
+      const int tu = (int)(trem / a.ntv), tv = (int)(trem - (int64_t)tu * a.ntv);
+      __syncthreads();  // every warpgroup has built its B operands from the previous sub
+      stage_subgrid<W, 4, UM_THREADS>(d, sub, plane, tu, tv, gplane);
+      __syncthreads();
+      bkey0 = bkey1 = -1;  // a new sub-grid: no footprint is current
+
+      // this warpgroup's slice of the segment, in tiles of one cell
+      const uint32_t seg_n = seg_hi - seg_lo;
+      const uint32_t w_lo = seg_lo + (uint32_t)(((uint64_t)seg_n * wg) / UM_WG);
+      const uint32_t w_hi = seg_lo + (uint32_t)(((uint64_t)seg_n * (wg + 1)) / UM_WG);
+      // the first tile's records as loaded (later tiles' are loaded one
+      // tile ahead and decoded when used)
+      uint2 raw = make_uint2(0u, 0u);
+      uint32_t mword = 0u, praw = 0u;
+      {
+        const uint32_t r = w_lo + (uint32_t)t;
+        if (r < w_hi) {
+          raw = *(const uint2 *)(a.recs + r);
+          mword = __ldg(a.exc_mark + (r >> 5));
+          if (lane == 0 && t > 0) praw = ((const uint2 *)(a.recs + r - 1))->y;
+        }
+      }
+      uint32_t base = w_lo;
+      while (!fault && base < w_hi) {
+        const uint32_t r = base + (uint32_t)t;
+        const bool valid = r < w_hi;
+        // Rec = {row, du | dv << 8 | ou << 16 | ov << 24}
+        const int key = valid ? (int)(raw.y & 0xFFFFu) : -1;
+        int prev = __shfl_up_sync(FULL, key, 1);
+        if (lane == 0) prev = t == 0 ? -2 : (int)(praw & 0xFFFFu);
+        const uint32_t starts = __ballot_sync(FULL, valid && key != prev);
+        if (lane == 0) s_mask[wg][j] = starts;
+        if (t == 0) s_key[wg] = key;
+        umma::bar_sync(1 + wg, 128);
+        if (s_fault[wg]) {
+          fault = true;
+          break;
+        }
+        // the tile ends where the second cell starts
+        int p2 = 128;
+#pragma unroll
+        for (int w = 3; w >= 0; --w) {
+          uint32_t m = s_mask[wg][w];
+          if (w == 0) m &= ~1u;  // the tile's own start
+          if (m) p2 = 32 * w + __ffs((int)m) - 1;
+        }
+        const int L = min((int)min(128u, w_hi - base), p2);
+        const int kx = s_key[wg];
+        const uint32_t row = raw.x;
+        const int ou = (int)((raw.y >> 16) & 0xFFu), ov = (int)(raw.y >> 24);
+        const uint32_t mk = (mword >> (r & 31u)) & 1u;
+        // the next tile's records
+        {
+          const uint32_t rn = base + (uint32_t)L + (uint32_t)t;
+          if (rn < w_hi) {
+            raw = *(const uint2 *)(a.recs + rn);
+            mword = __ldg(a.exc_mark + (rn >> 5));
+            if (lane == 0 && t > 0) praw = ((const uint2 *)(a.recs + rn - 1))->y;
+          }
+        }
+        const int s = (int)(tiles & 1u);
+        unsigned char *st = ops + s * UM_STAGE;
+        // A: this sample's column taps (row t), high parts and remainders
+        if (t < L) {
+          const uint4 *th = (const uint4 *)(tabh + ov * 8);
+          const uint4 *tl = (const uint4 *)(tabl + ov * 8);
+          *(uint4 *)(st + aoff) = th[0];
+          *(uint4 *)(st + aoff + 128) = th[1];
+          *(uint4 *)(st + 4096 + aoff) = tl[0];
+          *(uint4 *)(st + 4096 + aoff + 128) = tl[1];
+        }
+        // B: the cell's footprint, split (kept from two tiles back when the
+        // cell is the same)
+        if ((s ? bkey1 : bkey0) != kx) {
+          if (s)
+            bkey1 = kx;
+          else
+            bkey0 = kx;
+          const int du = kx & 255, dv = kx >> 8;
+          float2 c0 = make_float2(0.f, 0.f), c1 = make_float2(0.f, 0.f);
+          if (bsrc >= 0 && br < S) {
+            const float2 *srow = sub + ((du + br) * W + dv + 2 * bc) * 4 + bsrc;
+            if (2 * bc < S) c0 = srow[0];
+            if (2 * bc + 1 < S) c1 = srow[4];
+          }
+          uint2 rh, rl, ih, il;
+          tf32_split(c0.x, rh.x, rl.x);
+          tf32_split(c1.x, rh.y, rl.y);
+          tf32_split(c0.y, ih.x, il.x);
+          tf32_split(c1.y, ih.y, il.y);
+          *(uint2 *)(st + boff) = rh;
+          *(uint2 *)(st + 2048 + boff) = rl;
+          *(uint2 *)(st + boff + 256) = ih;  // row + 8: the next 8-row group
+          *(uint2 *)(st + 2048 + boff + 256) = il;
+        }
+        umma::fence_proxy_async();
+        umma::bar_sync(1 + wg, 128);
+        if (t == 0) {
+          umma::fence_after_sync();
+          const uint32_t sa = ops_s + (uint32_t)(s * UM_STAGE);
+          const uint64_t ah = umma::desc_kmajor(sa, 128, 256);
+          const uint64_t al = umma::desc_kmajor(sa + 4096, 128, 256);
+          const uint64_t bh = umma::desc_kmajor(sa + 8192, 128, 256);
+          const uint64_t bl = umma::desc_kmajor(sa + 10240, 128, 256);
+          const uint32_t td = tmem + (uint32_t)(s * 64);
+          umma::mma_tf32(td, al, bh, idesc, false);
+          umma::mma_tf32(td, ah, bl, idesc, true);
+          umma::mma_tf32(td, ah, bh, idesc, true);
+          umma::commit(&s_mbar[wg][s]);
+        }
+        // the previous tile, while this one's MMA runs
+        if (pend) finish();
+        pend = true;
+        pL = L;
+        ps = s;
+        prow = row;
+        pmk = mk;
+        pou = ou;
+        ++tiles;
+        base += (uint32_t)L;
+      }
+      seg_lo = seg_hi;
+      if (seg_hi == t_end) ++tt;
+    }
+  }
+  // the last tile; after a wait that gave up, one more bounded wait for each
+  // commit still outstanding before the columns are freed
+  if (pend && !fault) finish();
+  if (fault && t == 0) {
+    if (stuck >= 0) um_wait(&s_mbar[wg][stuck], (ph >> stuck) & 1u);
+    if (pend) um_wait(&s_mbar[wg][ps], (ph >> ps) & 1u);
+  }
+  umma::fence_before_sync();
+  __syncthreads();
+  if (tid < 32) {
+    umma::fence_after_sync();
+    umma::tmem_dealloc(s_taddr, 512);
+  }
+  // every CTA has taken its last chunk: the last one to get here re-arms
+  if (tid == 0) {
+    __threadfence();
+    if (atomicAdd(&a.sched[1], 1u) == gridDim.x - 1) {
+      a.sched[0] = 0u;
+      a.sched[1] = 0u;
+      __threadfence();
+    }
+  }
+}
+
 // ------------------------------------------------- shared-plan exceptions --
 // The samples a shared plan lists for the degridder (plan.cuh): each in the
 // degridder's own convention (sample_pos_degrid, standard_degrid.py:435-462)
@@ -984,6 +1371,30 @@ static int launch_degrid_tc(const TiledDegridArgs &a, int64_t nblocks, cudaStrea
   return AV_OK;
 }
 
+template <int S>
+static int launch_degrid_umma(const TiledDegridArgs &a, int64_t nblocks, cudaStream_t st) {
+  const size_t smem = UMSmem<S>::total;
+  static bool attr[64] = {false};
+  int dev = 0;
+  AV_CUDA(cudaGetDevice(&dev));
+  if (dev < 0 || dev >= 64) {
+    set_error("av_degrid_tiled: device %d beyond the 64 this library tracks", dev);
+    return AV_ERR_UNSUPPORTED;
+  }
+  if (!attr[dev]) {
+    AV_CUDA(cudaFuncSetAttribute(k_degrid_umma<S>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)smem));
+    attr[dev] = true;
+  }
+  // one CTA per SM (its shared memory rules out a second, and it holds all
+  // 512 tensor-memory columns)
+  const int64_t sms = sm_count();
+  if (nblocks > sms) nblocks = sms;
+  k_degrid_umma<S><<<(unsigned)nblocks, UM_THREADS, smem, st>>>(a);
+  AV_LAUNCH_CHECK();
+  return AV_OK;
+}
+
 template <int S, int NPG>
 static int launch_degrid_tiled(const TiledDegridArgs &a, int64_t nblocks, cudaStream_t st) {
   // persistent CTAs: at most as many as are resident at once
@@ -1019,6 +1430,8 @@ static int degrid_dispatch_npg(const TiledDegridArgs &a, int npg, int64_t nb, cu
   if (npg == 2) return launch_degrid_tiled<S, 2>(a, nb, st);
   if constexpr (S <= 8) {
     const int64_t lanes = tune_value(AV_TUNE_DEGRID_LANES);
+    if (a.fast_out && a.d.g_npol == 4 && lanes == AV_DEGRID_LANES_TC05)
+      return launch_degrid_umma<S>(a, nb, st);
     const bool tf32 =
         lanes == AV_DEGRID_LANES_TF32 || (lanes == AV_DEGRID_LANES_AUTO && S >= 7);
     // the TF32 kernel keeps a shared plan's marks in the staged rows' top bit
@@ -1250,6 +1663,22 @@ int av_degrid_tiled_execute(const double *dphase, void *values, int values_dtype
   e.accumulate = a.accumulate;
   k_degrid_exceptions<<<(unsigned)sms, 128, 0, as_stream(stream)>>>(e);
   AV_LAUNCH_CHECK();
+  return AV_OK;
+}
+
+int av_degrid_fault_read(int *out, int clear, void *stream) {
+  clear_error();
+  AV_CHECK_ARG(out, "av_degrid_fault_read: null pointer");
+  cudaStream_t st = as_stream(stream);
+  uint32_t v = 0u;
+  AV_CUDA(cudaMemcpyFromSymbolAsync(&v, g_degrid_fault, sizeof(v), 0, cudaMemcpyDeviceToHost, st));
+  AV_CUDA(cudaStreamSynchronize(st));
+  *out = (int)v;
+  if (clear && v) {
+    const uint32_t z = 0u;
+    AV_CUDA(cudaMemcpyToSymbolAsync(g_degrid_fault, &z, sizeof(z), 0, cudaMemcpyHostToDevice, st));
+    AV_CUDA(cudaStreamSynchronize(st));
+  }
   return AV_OK;
 }
 

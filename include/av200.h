@@ -78,8 +78,12 @@ unsigned long long av_launch_count(void);
  *                                or phase) runs: AV_DEGRID_LANES_TF32 (TF32
  *                                tensor-core tiles with split operands,
  *                                supports up to 8), AV_DEGRID_LANES_FP32 (FP32
- *                                FMA) or AV_DEGRID_LANES_AUTO (default: TF32
- *                                for supports 7 and 8, FP32 otherwise)
+ *                                FMA), AV_DEGRID_LANES_TC05 (TF32 with
+ *                                split operands on the fifth-generation
+ *                                tensor cores, accumulators in tensor memory,
+ *                                supports up to 8) or AV_DEGRID_LANES_AUTO
+ *                                (default: TF32 for supports 7 and 8, FP32
+ *                                otherwise)
  *   AV_TUNE_HOGBOM_BARRIER_TIMEOUT_US  how long (microseconds of wall time,
  *                                default 2000000) a CTA of av_hogbom_run
  *                                waits at the per-iteration grid barrier
@@ -92,8 +96,9 @@ unsigned long long av_launch_count(void);
  *                                barrier, which is how the timeout path is
  *                                tested.  Range [0, 600000000].
  * av_tune_set returns AV_ERR_ARG for an unknown knob or a value outside
- * [1, 1024] ([1, 3] for the two lane knobs, [0, 600000000] for the barrier
- * timeout); av_tune_get returns -1 for an unknown knob. */
+ * [1, 1024] ([1, 3] for AV_TUNE_GRID_LANES, [1, 4] for AV_TUNE_DEGRID_LANES,
+ * [0, 600000000] for the barrier timeout); av_tune_get returns -1 for an
+ * unknown knob. */
 enum av_tune {
   AV_TUNE_GRID_CHUNKS_PER_SM = 0,
   AV_TUNE_DEGRID_CHUNKS_PER_SM = 1,
@@ -105,7 +110,8 @@ enum av_grid_lanes { AV_GRID_LANES_MMA = 1, AV_GRID_LANES_ROWS = 2, AV_GRID_LANE
 enum av_degrid_lanes {
   AV_DEGRID_LANES_TF32 = 1,
   AV_DEGRID_LANES_FP32 = 2,
-  AV_DEGRID_LANES_AUTO = 3
+  AV_DEGRID_LANES_AUTO = 3,
+  AV_DEGRID_LANES_TC05 = 4
 };
 int av_tune_set(int knob, int64_t value);
 int64_t av_tune_get(int knob);
@@ -330,6 +336,13 @@ int av_degrid_tiled_execute(const double *dphase, void *values, int values_dtype
                             const double *convFunc, const int32_t *polmap, int64_t nt,
                             int64_t nb, int64_t nvchan, int64_t nvpol, void *workspace,
                             size_t workspace_bytes, void *stream);
+/* Whether a launch of the tensor-memory degridder (AV_DEGRID_LANES_TC05) on
+ * the current device gave up a bounded wait for its MMAs since the flag was
+ * last cleared: *out = 1 if so (the samples of that launch's warpgroup are
+ * then partly unwritten), 0 otherwise; clear != 0 resets it.  Synchronises
+ * the stream.  No counterpart in the reference (its degridder runs on the
+ * CPU). */
+int av_degrid_fault_read(int *out, int clear, void *stream);
 int av_degrid_tiled(const double *uvw, const double *dphase, void *values, int values_dtype,
                     int accumulate, const uint8_t *flag, double scale_x, double scale_y,
                     double offset_x, double offset_y, const void *grid, int grid_dtype,

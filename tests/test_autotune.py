@@ -30,7 +30,8 @@ def test_tune_knobs_set_get_and_reject():
     assert L.av_tune_get(_lib.AV_TUNE_GRID_LANES) == _lib.AV_GRID_LANES_ROWS
     assert L.av_tune_set(_lib.AV_TUNE_GRID_LANES, _lib.AV_GRID_LANES_AUTO) == _lib.AV_OK
     assert L.av_tune_get(_lib.AV_TUNE_DEGRID_LANES) == _lib.AV_DEGRID_LANES_AUTO
-    assert L.av_tune_set(_lib.AV_TUNE_DEGRID_LANES, 4) == _lib.AV_ERR_ARG
+    assert L.av_tune_set(_lib.AV_TUNE_DEGRID_LANES, 5) == _lib.AV_ERR_ARG
+    assert L.av_tune_set(_lib.AV_TUNE_DEGRID_LANES, _lib.AV_DEGRID_LANES_TC05) == _lib.AV_OK
     assert L.av_tune_set(_lib.AV_TUNE_DEGRID_LANES, _lib.AV_DEGRID_LANES_FP32) == _lib.AV_OK
     assert L.av_tune_set(_lib.AV_TUNE_DEGRID_LANES, _lib.AV_DEGRID_LANES_AUTO) == _lib.AV_OK
     assert L.av_tune_set(_lib.AV_TUNE_GRID_CHUNKS_PER_SM, g) == _lib.AV_OK

@@ -239,15 +239,16 @@ def test_tiled_degrid_every_support(support, os_):
     assert rel(v.cpu().numpy(), ref) <= 1e-6
 
 
-@pytest.fixture(params=["tf32", "fp32"])
+@pytest.fixture(params=["tf32", "fp32", "tc05"])
 def degrid_lanes(request):
     """Runs a test under each setting of the tiled degridder's fast store
-    path: TF32 tensor-core tiles with split operands, and FP32 FMA."""
+    path: TF32 tensor-core tiles with split operands (warp MMAs, or MMAs with
+    tensor-memory accumulators), and FP32 FMA."""
     from astroviper_b200 import _lib
     L = _lib.lib()
     old = L.av_tune_get(_lib.AV_TUNE_DEGRID_LANES)
-    want = (_lib.AV_DEGRID_LANES_TF32 if request.param == "tf32"
-            else _lib.AV_DEGRID_LANES_FP32)
+    want = {"tf32": _lib.AV_DEGRID_LANES_TF32, "fp32": _lib.AV_DEGRID_LANES_FP32,
+            "tc05": _lib.AV_DEGRID_LANES_TC05}[request.param]
     assert L.av_tune_set(_lib.AV_TUNE_DEGRID_LANES, want) == _lib.AV_OK
     yield request.param
     L.av_tune_set(_lib.AV_TUNE_DEGRID_LANES, old)
