@@ -890,30 +890,45 @@ __global__ void __launch_bounds__(TC_THREADS, 2) k_degrid_tc(TiledDegridArgs a) 
 // with its row taps: no shuffles, one 32-byte store per sample.  Row and
 // column taps come divided by their offsets' tap sums, so V carries the
 // sample's 1 / norm (the reference's norm, the sum of the 2-D taps,
-// standard_degrid.py:464-485, is the product of the two sums).  Row n of the
-// B operand (output polarisation p, real or imaginary part, footprint row r)
-// is n = 16 p + 8 (re|im) + r and reads grid polarisation polmap[p].  A is
-// stored K-major in 8-row x 16-byte core matrices: element (m, c) at byte
-// (m % 8) 16 + (m / 8) 256 + (c / 4) 128 + (c % 4) 4; B the same with n for m.
-// Two stages of operands and accumulators per warpgroup: the MMA of tile i
-// runs while the warpgroup finishes tile i - 1 and loads tile i + 1's
-// records; the pipeline runs on across segments and chunks (the epilogue
-// reads no sub-grid).  One CTA of four warpgroups per SM holds all 512
-// tensor-memory columns (4 x 2 stages x 64).  Every wait for an MMA is
-// bounded: a wait that gives up sets g_degrid_fault, and the warpgroup stops
-// issuing, waits once more (bounded) before the CTA frees its tensor memory,
-// and leaves its remaining samples unwritten.
+// standard_degrid.py:464-485, is the product of the two sums).
+//
+// Layouts.  Row n of the B operand (output polarisation p, real or imaginary
+// part, footprint row r) is n = 16 p + 8 (re|im) + r and reads grid
+// polarisation polmap[p].  A and B are stored K-major in 8-row x 16-byte core
+// matrices: element (m, c) at byte (m % 8) 16 + (m / 8) 256 + (c / 4) 128 +
+// (c % 4) 4.  The sub-grid is staged as one plane per grid polarisation,
+// rows RS float2 apart (RS = 8 mod 16: the 16 lanes of a half-warp reading 8
+// columns of 2 rows hit distinct banks).
+//
+// Schedule.  Each window of up to UM_WIN records of a segment (one chunk's
+// records in one grid tile) first gets a bitmap of where cells change, so
+// every thread finds its tiles' ends alone.  Within a tile the four warps
+// work independently: warp j writes its 32 samples' A rows and the B rows of
+// output polarisation j, then arrives on the stage's `full` mbarrier; thread
+// 0 issues the MMAs when all four have arrived and commits them to the
+// stage's `done` mbarrier; each warp then finishes the previous tile from its
+// own quarter of the tensor-memory lanes.  Two stages of operands and
+// accumulators per warpgroup: the MMA of tile i runs while the warps finish
+// tile i - 1 and build tile i + 1.  One CTA of four warpgroups per SM holds
+// all 512 tensor-memory columns (4 x 2 stages x 64).  Every wait is bounded: a
+// wait that gives up sets g_degrid_fault and the warpgroup's fault word,
+// after which its warps stop taking tiles (their remaining samples stay
+// unwritten) and the CTA waits once more, bounded, before it frees the
+// tensor memory.
 constexpr int UM_THREADS = 512;
 constexpr int UM_WG = UM_THREADS / 128;
-constexpr int UM_SPIN = 1 << 22;     // mbarrier probes before a wait gives up
+constexpr int UM_SPIN = 1 << 21;     // mbarrier probes before a wait gives up
+constexpr uint32_t UM_SLEEP_NS = 1000; // each probe sleeps at most this long (~2 s in all)
 constexpr uint32_t UM_STAGE = 12288; // per stage: A hi | A lo | B hi | B lo
-// set (sticky) when a wait of k_degrid_umma for its MMAs gave up;
-// av_degrid_fault_read reads and clears it
+constexpr int UM_WIN = 16384;        // records per bitmap window
+// set (sticky) when a wait of k_degrid_umma gave up; av_degrid_fault_read
+// reads and clears it
 __device__ uint32_t g_degrid_fault = 0u;
 
 template <int S>
 struct UMSmem {
   static constexpr int W = TILE + S - 1;
+  static constexpr int RS = ((W + 7) / 16) * 16 + 8;  // plane row stride, 8 mod 16
   // 256 x 8 FP32 taps, each divided by its offset's tap sum (so that the
   // products of a row's and a column's taps carry 1 / norm), their TF32 high
   // parts and remainders
@@ -922,12 +937,14 @@ struct UMSmem {
   static constexpr size_t off_tabl = off_tabh + 256 * 8 * 4;
   static constexpr size_t off_ops = off_tabl + 256 * 8 * 4;
   static constexpr size_t off_sub = off_ops + (size_t)UM_WG * 2 * UM_STAGE;
-  static constexpr size_t sub_bytes = (size_t)W * W * 4 * sizeof(float2);  // [cell][pol]
+  static constexpr size_t sub_bytes = (size_t)4 * W * RS * sizeof(float2);  // [pol][row][col]
   static constexpr size_t total = off_sub + sub_bytes;
+  static_assert(RS >= W && RS % 16 == 8, "plane rows");
   static_assert(off_ops % 1024 == 0 && off_sub % 16 == 0, "alignment");
   // more than half of an SM's shared memory: one CTA (and its 512 tensor-
   // memory columns) per SM
-  static_assert(total > 116 * 1024 && total <= 227 * 1024, "one CTA per SM");
+  static_assert(total > 116 * 1024 && total + UM_WIN / 8 + 1024 <= 227 * 1024,
+                "one CTA per SM");
   static_assert(S <= 8, "an 8 x 8 footprint");
 };
 
@@ -935,31 +952,73 @@ __device__ __forceinline__ uint32_t um_kmaj(int n, int c) {
   return (uint32_t)((n & 7) * 16 + (n >> 3) * 256 + (c >> 2) * 128 + (c & 3) * 4);
 }
 
-// The bounded wait of one thread for an MMA commit; false: it gave up.
+// The bounded wait of one thread for an mbarrier phase; false: it gave up.
 __device__ __forceinline__ bool um_wait(uint64_t *mbar, uint32_t parity) {
   for (int it = 0; it < UM_SPIN; ++it)
-    if (umma::mbar_try_wait(mbar, parity)) return true;
+    if (umma::mbar_try_wait_sleep(mbar, parity, UM_SLEEP_NS)) return true;
   return false;
+}
+
+__device__ __forceinline__ void um_arrive(uint64_t *mbar) {
+  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(umma::smem_addr(mbar))
+               : "memory");
+}
+
+// The sub-grid of tile (plane, tu, tv) as planes [pol][row][col] of float2,
+// rows RS apart (zeros outside the grid or past g_npol).
+template <int W, int RS, int THREADS>
+__device__ __forceinline__ void stage_subgrid_planes(const DegridArgs &d, float2 *sub,
+                                                     int64_t plane, int tu, int tv,
+                                                     int64_t gplane) {
+  constexpr int N = 4 * W * W;
+  for (int i0 = 0; i0 < N; i0 += THREADS * SUB_UNROLL) {
+    float2 v[SUB_UNROLL];
+    int dst[SUB_UNROLL];
+#pragma unroll
+    for (int k = 0; k < SUB_UNROLL; ++k) {
+      const int i = i0 + k * THREADS + (int)threadIdx.x;
+      v[k] = make_float2(0.f, 0.f);
+      const int gp = i / (W * W), rem = i - gp * (W * W);
+      const int iu = rem / W, iv = rem - iu * W;
+      dst[k] = (gp * W + iu) * RS + iv;
+      const int64_t gu = (int64_t)tu * TILE + iu, gv = (int64_t)tv * TILE + iv;
+      if (i < N && gp < d.g_npol && gu < d.g_n2 && gv < d.g_n3) {
+        const int64_t gi = (plane * d.g_npol + gp) * gplane + gu * d.g_n3 + gv;
+        if (d.grid_c128) {
+          const double2 x = ((const double2 *)d.grid)[gi];
+          v[k] = make_float2((float)x.x, (float)x.y);
+        } else {
+          v[k] = ((const float2 *)d.grid)[gi];
+        }
+      }
+    }
+#pragma unroll
+    for (int k = 0; k < SUB_UNROLL; ++k) {
+      const int i = i0 + k * THREADS + (int)threadIdx.x;
+      if (i < N) sub[dst[k]] = v[k];
+    }
+  }
 }
 
 template <int S>
 __global__ void __launch_bounds__(UM_THREADS, 1) k_degrid_umma(TiledDegridArgs a) {
   using M = UMSmem<S>;
-  constexpr int W = M::W;
+  constexpr int W = M::W, RS = M::RS;
   constexpr unsigned FULL = 0xffffffffu;
   extern __shared__ __align__(16) unsigned char smem[];
   float *tab = (float *)(smem + M::off_tab);
   uint32_t *tabh = (uint32_t *)(smem + M::off_tabh);
   uint32_t *tabl = (uint32_t *)(smem + M::off_tabl);
   float2 *sub = (float2 *)(smem + M::off_sub);
-  __shared__ __align__(8) uint64_t s_mbar[UM_WG][2];
-  __shared__ uint32_t s_mask[UM_WG][4];
-  __shared__ int s_key[UM_WG];
+  __shared__ __align__(8) uint64_t s_full[UM_WG][2];
+  __shared__ __align__(8) uint64_t s_done[UM_WG][2];
+  __shared__ uint32_t s_bits[UM_WIN / 32];
   __shared__ int s_fault[UM_WG];
   __shared__ uint32_t s_taddr;
   __shared__ int s_chunk;
   const DegridArgs &d = a.d;
   const int tid = threadIdx.x, wg = tid >> 7, t = tid & 127, j = t >> 5, lane = tid & 31;
+  const int gwarp = tid >> 5;
 
   // taps of offset o - 128 (the reference's kernel indices |sampling ix +
   // off|, standard_degrid.py:466-469), over their FP64 sum; a zero sum gives
@@ -984,13 +1043,15 @@ __global__ void __launch_bounds__(UM_THREADS, 1) k_degrid_umma(TiledDegridArgs a
       tf32_split(x, tabh[o * 8 + i], tabl[o * 8 + i]);
     }
   }
-  if (tid < 32) {
+  if (gwarp == 0) {
     umma::tmem_alloc(&s_taddr, 512);
     umma::tmem_relinquish();
   }
   if (tid < UM_WG) {
-    umma::mbar_init(&s_mbar[tid][0], 1);
-    umma::mbar_init(&s_mbar[tid][1], 1);
+    for (int x = 0; x < 2; ++x) {
+      umma::mbar_init(&s_full[tid][x], 4);  // one arrival per warp
+      umma::mbar_init(&s_done[tid][x], 1);  // the MMA commit
+    }
     s_fault[tid] = 0;
   }
   umma::mbar_init_fence();
@@ -1000,37 +1061,35 @@ __global__ void __launch_bounds__(UM_THREADS, 1) k_degrid_umma(TiledDegridArgs a
   const uint32_t tmem = s_taddr + (uint32_t)(wg * 128);  // two stages of 64 columns
   unsigned char *ops = smem + M::off_ops + (size_t)wg * 2 * UM_STAGE;
   const uint32_t ops_s = umma::smem_addr(ops);
-  // the B rows this thread builds: output polarisation bp, footprint row br,
-  // columns 2 bc and 2 bc + 1; grid polarisation bsrc (-1: zeros)
-  const int bp = t >> 5, br = (t >> 2) & 7, bc = t & 3;
+  // this warp's B rows: output polarisation j from grid polarisation bsrc
+  // (-1: zeros); lane (br, bc) takes footprint rows br and br + 4, column bc
+  const int br = lane >> 3, bc = lane & 7;
   int bsrc = -1;
   {
-    const int v = d.polmap[bp];
+    const int v = d.polmap[j];
     if (v >= 0 && v < 4 && v < d.g_npol) bsrc = v;
   }
-  const uint32_t boff = 8192 + um_kmaj(16 * bp + br, 2 * bc);  // real part; imaginary 8 rows on
   const uint32_t aoff = (uint32_t)((t & 7) * 16 + (t >> 3) * 256);
   const int64_t gplane = d.g_n2 * d.g_n3;
   const uint32_t n_rec = *a.n_rec;
   const uint32_t n_all = (uint32_t)a.n_rows;
   const int64_t n_chunks = ((int64_t)n_all + a.chunk - 1) / a.chunk;
   const uint32_t idesc = umma::idesc_tf32(128, 64);
-  uint32_t tiles = 0;       // this warpgroup's tiles so far: stage = tiles & 1
-  uint32_t ph = 0u;         // bit s: the parity stage s's next commit completes
-  int bkey0 = -1, bkey1 = -1;  // the cell whose footprint each stage's B holds
-  bool fault = false;
-  int stuck = -1;           // the stage whose commit this thread gave up on
+  uint32_t tiles = 0;           // this warpgroup's tiles so far: stage = tiles & 1
+  uint32_t fph = 0u, dph = 0u;  // bit s: the parity of stage s's next full / done phase
+  int bkey0 = -1, bkey1 = -1;   // the cell whose footprint each stage's B holds
+  int stuck = -1;               // the stage whose done phase this thread gave up on
   // the tile whose MMA is in flight: its samples, stage and length
   bool pend = false;
   int pL = 0, ps = 0;
   uint32_t prow = 0u, pmk = 0u;
   int pou = 0;
 
-  // waits for the pending tile's MMA, then each sample of it reads its row of
-  // D, weights it with its row taps and writes its 4 values
+  // waits for the pending tile's MMA, then each of this warp's samples reads
+  // its row of D, weights it with its row taps and writes its 4 values
   auto finish = [&]() {
-    if (um_wait(&s_mbar[wg][ps], (ph >> ps) & 1u)) {
-      ph ^= 1u << ps;
+    if (um_wait(&s_done[wg][ps], (dph >> ps) & 1u)) {
+      dph ^= 1u << ps;
     } else {
       stuck = ps;
       s_fault[wg] = 1;
@@ -1038,36 +1097,27 @@ __global__ void __launch_bounds__(UM_THREADS, 1) k_degrid_umma(TiledDegridArgs a
     }
     umma::fence_after_sync();
     if (32 * j < pL) {
-      uint32_t d0[32], d1[32];
+      const float4 c0 = *(const float4 *)(tab + pou * 8);
+      const float4 c1 = *(const float4 *)(tab + pou * 8 + 4);
+      const float cu[8] = {c0.x, c0.y, c0.z, c0.w, c1.x, c1.y, c1.z, c1.w};
       const uint32_t ta = tmem + (uint32_t)(ps * 64) + ((uint32_t)(32 * j) << 16);
-      umma::ld_32x32b_x32(ta, d0);
-      umma::ld_32x32b_x32(ta + 32, d1);
-      umma::wait_ld(d0);
-      umma::wait_ld(d1);
-      if (t < pL) {
-        const float4 c0 = *(const float4 *)(tab + pou * 8);
-        const float4 c1 = *(const float4 *)(tab + pou * 8 + 4);
-        const float cu[8] = {c0.x, c0.y, c0.z, c0.w, c1.x, c1.y, c1.z, c1.w};
-        float v[8];
+      float4 *out = (float4 *)d.values + (int64_t)prow * 2;
+      // columns [32 h, 32 h + 32): polarisations 2 h and 2 h + 1
+#pragma unroll
+      for (int h = 0; h < 2; ++h) {
+        uint32_t dr[32];
+        umma::ld_32x32b_x32(ta + (uint32_t)(32 * h), dr);
+        umma::wait_ld(dr);
+        float v[4];
 #pragma unroll
         for (int q = 0; q < 4; ++q) {
-          float s = __fmul_rn(cu[0], __uint_as_float(d0[q * 8]));
+          float s = __fmul_rn(cu[0], __uint_as_float(dr[q * 8]));
 #pragma unroll
-          for (int r = 1; r < S; ++r) s = __fmaf_rn(cu[r], __uint_as_float(d0[q * 8 + r]), s);
+          for (int r = 1; r < S; ++r) s = __fmaf_rn(cu[r], __uint_as_float(dr[q * 8 + r]), s);
           v[q] = s;
-          float s1 = __fmul_rn(cu[0], __uint_as_float(d1[q * 8]));
-#pragma unroll
-          for (int r = 1; r < S; ++r) s1 = __fmaf_rn(cu[r], __uint_as_float(d1[q * 8 + r]), s1);
-          v[4 + q] = s1;
         }
-        float4 o0 = make_float4(0.f, 0.f, 0.f, 0.f), o1 = o0;
-        if (!pmk) {
-          o0 = make_float4(v[0], v[1], v[2], v[3]);
-          o1 = make_float4(v[4], v[5], v[6], v[7]);
-        }
-        float4 *out = (float4 *)d.values + (int64_t)prow * 2;
-        out[0] = o0;
-        out[1] = o1;
+        if (t < pL)
+          out[h] = pmk ? make_float4(0.f, 0.f, 0.f, 0.f) : make_float4(v[0], v[1], v[2], v[3]);
       }
     }
     umma::fence_before_sync();
@@ -1106,125 +1156,164 @@ __global__ void __launch_bounds__(UM_THREADS, 1) k_degrid_umma(TiledDegridArgs a
       const int64_t plane = tt / (a.ntu * a.ntv);
       const int64_t trem = tt - plane * a.ntu * a.ntv;
       const int tu = (int)(trem / a.ntv), tv = (int)(trem - (int64_t)tu * a.ntv);
-      __syncthreads();  // every warpgroup has built its B operands from the previous sub
-      stage_subgrid<W, 4, UM_THREADS>(d, sub, plane, tu, tv, gplane);
-      __syncthreads();
+      __syncthreads();  // every warp has built its B rows from the previous sub
+      stage_subgrid_planes<W, RS, UM_THREADS>(d, sub, plane, tu, tv, gplane);
       bkey0 = bkey1 = -1;  // a new sub-grid: no footprint is current
 
-      // this warpgroup's slice of the segment, in tiles of one cell
-      const uint32_t seg_n = seg_hi - seg_lo;
-      const uint32_t w_lo = seg_lo + (uint32_t)(((uint64_t)seg_n * wg) / UM_WG);
-      const uint32_t w_hi = seg_lo + (uint32_t)(((uint64_t)seg_n * (wg + 1)) / UM_WG);
-      // the first tile's records as loaded (later tiles' are loaded one
-      // tile ahead and decoded when used)
-      uint2 raw = make_uint2(0u, 0u);
-      uint32_t mword = 0u, praw = 0u;
-      {
-        const uint32_t r = w_lo + (uint32_t)t;
-        if (r < w_hi) {
-          raw = *(const uint2 *)(a.recs + r);
-          mword = __ldg(a.exc_mark + (r >> 5));
-          if (lane == 0 && t > 0) praw = ((const uint2 *)(a.recs + r - 1))->y;
-        }
-      }
-      uint32_t base = w_lo;
-      while (!fault && base < w_hi) {
-        const uint32_t r = base + (uint32_t)t;
-        const bool valid = r < w_hi;
-        // Rec = {row, du | dv << 8 | ou << 16 | ov << 24}
-        const int key = valid ? (int)(raw.y & 0xFFFFu) : -1;
-        int prev = __shfl_up_sync(FULL, key, 1);
-        if (lane == 0) prev = t == 0 ? -2 : (int)(praw & 0xFFFFu);
-        const uint32_t starts = __ballot_sync(FULL, valid && key != prev);
-        if (lane == 0) s_mask[wg][j] = starts;
-        if (t == 0) s_key[wg] = key;
-        umma::bar_sync(1 + wg, 128);
-        if (s_fault[wg]) {
-          fault = true;
-          break;
-        }
-        // the tile ends where the second cell starts
-        int p2 = 128;
-#pragma unroll
-        for (int w = 3; w >= 0; --w) {
-          uint32_t m = s_mask[wg][w];
-          if (w == 0) m &= ~1u;  // the tile's own start
-          if (m) p2 = 32 * w + __ffs((int)m) - 1;
-        }
-        const int L = min((int)min(128u, w_hi - base), p2);
-        const int kx = s_key[wg];
-        const uint32_t row = raw.x;
-        const int ou = (int)((raw.y >> 16) & 0xFFu), ov = (int)(raw.y >> 24);
-        const uint32_t mk = (mword >> (r & 31u)) & 1u;
-        // the next tile's records
+      for (uint32_t x0 = seg_lo; x0 < seg_hi; x0 += UM_WIN) {
+        const uint32_t x1 = min(seg_hi, x0 + (uint32_t)UM_WIN);
+        if (x0 != seg_lo) __syncthreads();  // every warp is done with the last bitmap
+        // bit i of the window: a cell starts at record x0 + i (each warp
+        // loads 8 words' records before it compares them)
         {
-          const uint32_t rn = base + (uint32_t)L + (uint32_t)t;
-          if (rn < w_hi) {
-            raw = *(const uint2 *)(a.recs + rn);
-            mword = __ldg(a.exc_mark + (rn >> 5));
-            if (lane == 0 && t > 0) praw = ((const uint2 *)(a.recs + rn - 1))->y;
+          constexpr int NW = UM_THREADS / 32, BATCH = 8;
+          const uint32_t nwords = (x1 - x0 + 31u) >> 5;
+          for (uint32_t w0 = (uint32_t)gwarp; w0 < nwords; w0 += NW * BATCH) {
+            uint32_t ky[BATCH], pk[BATCH];
+#pragma unroll
+            for (int b = 0; b < BATCH; ++b) {
+              const uint32_t wi = w0 + (uint32_t)(b * NW);
+              const uint32_t r = x0 + wi * 32u + (uint32_t)lane;
+              ky[b] = r < x1 ? ((const uint2 *)(a.recs + r))->y : 0xFFFFFFFFu;
+              pk[b] = (lane == 0 && wi > 0 && wi < nwords) ? ((const uint2 *)(a.recs + r - 1))->y
+                                                          : 0xFFFFFFFEu;
+            }
+#pragma unroll
+            for (int b = 0; b < BATCH; ++b) {
+              const uint32_t wi = w0 + (uint32_t)(b * NW);
+              if (wi >= nwords) break;  // uniform across the warp
+              const int key = ky[b] == 0xFFFFFFFFu ? -1 : (int)(ky[b] & 0xFFFFu);
+              int prev = __shfl_up_sync(FULL, key, 1);
+              if (lane == 0) prev = wi == 0 ? -2 : (int)(pk[b] & 0xFFFFu);
+              const uint32_t m = __ballot_sync(FULL, key >= 0 && key != prev);
+              if (lane == 0) s_bits[wi] = m;
+            }
           }
         }
-        const int s = (int)(tiles & 1u);
-        unsigned char *st = ops + s * UM_STAGE;
-        // A: this sample's column taps (row t), high parts and remainders
-        if (t < L) {
-          const uint4 *th = (const uint4 *)(tabh + ov * 8);
-          const uint4 *tl = (const uint4 *)(tabl + ov * 8);
-          *(uint4 *)(st + aoff) = th[0];
-          *(uint4 *)(st + aoff + 128) = th[1];
-          *(uint4 *)(st + 4096 + aoff) = tl[0];
-          *(uint4 *)(st + 4096 + aoff + 128) = tl[1];
-        }
-        // B: the cell's footprint, split (kept from two tiles back when the
-        // cell is the same)
-        if ((s ? bkey1 : bkey0) != kx) {
-          if (s)
-            bkey1 = kx;
-          else
-            bkey0 = kx;
-          const int du = kx & 255, dv = kx >> 8;
-          float2 c0 = make_float2(0.f, 0.f), c1 = make_float2(0.f, 0.f);
-          if (bsrc >= 0 && br < S) {
-            const float2 *srow = sub + ((du + br) * W + dv + 2 * bc) * 4 + bsrc;
-            if (2 * bc < S) c0 = srow[0];
-            if (2 * bc + 1 < S) c1 = srow[4];
+        __syncthreads();  // the bitmap (and, in the first window, the sub-grid)
+
+        // this warpgroup's slice of the window, in tiles of one cell
+        const uint32_t n = x1 - x0;
+        const uint32_t w_lo = x0 + (uint32_t)(((uint64_t)n * wg) / UM_WG);
+        const uint32_t w_hi = x0 + (uint32_t)(((uint64_t)n * (wg + 1)) / UM_WG);
+        // the tile from base: up to 128 records, ending before the next cell
+        auto tile_len = [&](uint32_t base) -> int {
+          int L = (int)min(128u, w_hi - base);
+          uint32_t i = base - x0 + 1u;                    // first bit to look at
+          const uint32_t iend = base - x0 + (uint32_t)L;  // one past the last
+          while (i < iend) {
+            const uint32_t m = s_bits[i >> 5] >> (i & 31u);
+            if (m) {
+              const uint32_t pos = i + (uint32_t)(__ffs((int)m) - 1);
+              if (pos < iend) L = (int)(pos - (base - x0));
+              break;
+            }
+            i = (i | 31u) + 1u;
           }
-          uint2 rh, rl, ih, il;
-          tf32_split(c0.x, rh.x, rl.x);
-          tf32_split(c1.x, rh.y, rl.y);
-          tf32_split(c0.y, ih.x, il.x);
-          tf32_split(c1.y, ih.y, il.y);
-          *(uint2 *)(st + boff) = rh;
-          *(uint2 *)(st + 2048 + boff) = rl;
-          *(uint2 *)(st + boff + 256) = ih;  // row + 8: the next 8-row group
-          *(uint2 *)(st + 2048 + boff + 256) = il;
+          return L;
+        };
+        uint32_t base = w_lo;
+        uint2 raw = make_uint2(0u, 0u);
+        uint32_t mword = 0u, kraw = 0u;
+        if (base < w_hi) {
+          const uint32_t r = base + (uint32_t)t;
+          if (r < w_hi) {
+            raw = *(const uint2 *)(a.recs + r);
+            mword = __ldg(a.exc_mark + (r >> 5));
+          }
+          kraw = ((const uint2 *)(a.recs + base))->y;
         }
-        umma::fence_proxy_async();
-        umma::bar_sync(1 + wg, 128);
-        if (t == 0) {
-          umma::fence_after_sync();
-          const uint32_t sa = ops_s + (uint32_t)(s * UM_STAGE);
-          const uint64_t ah = umma::desc_kmajor(sa, 128, 256);
-          const uint64_t al = umma::desc_kmajor(sa + 4096, 128, 256);
-          const uint64_t bh = umma::desc_kmajor(sa + 8192, 128, 256);
-          const uint64_t bl = umma::desc_kmajor(sa + 10240, 128, 256);
-          const uint32_t td = tmem + (uint32_t)(s * 64);
-          umma::mma_tf32(td, al, bh, idesc, false);
-          umma::mma_tf32(td, ah, bl, idesc, true);
-          umma::mma_tf32(td, ah, bh, idesc, true);
-          umma::commit(&s_mbar[wg][s]);
+        int L = base < w_hi ? tile_len(base) : 0;
+        while (base < w_hi) {
+          if (*(volatile int *)&s_fault[wg]) break;
+          const uint32_t r = base + (uint32_t)t;
+          const uint32_t row = raw.x;
+          const int ou = (int)((raw.y >> 16) & 0xFFu), ov = (int)(raw.y >> 24);
+          const uint32_t mk = (mword >> (r & 31u)) & 1u;
+          const int kx = (int)(kraw & 0xFFFFu);
+          // the next tile and its records
+          const uint32_t nbase = base + (uint32_t)L;
+          int nL = 0;
+          if (nbase < w_hi) {
+            const uint32_t rn = nbase + (uint32_t)t;
+            if (rn < w_hi) {
+              raw = *(const uint2 *)(a.recs + rn);
+              mword = __ldg(a.exc_mark + (rn >> 5));
+            }
+            kraw = ((const uint2 *)(a.recs + nbase))->y;
+            nL = tile_len(nbase);
+          }
+          const int s = (int)(tiles & 1u);
+          unsigned char *st = ops + s * UM_STAGE;
+          // A: this sample's column taps (row t), high parts and remainders
+          if (t < L) {
+            const uint4 *th = (const uint4 *)(tabh + ov * 8);
+            const uint4 *tl = (const uint4 *)(tabl + ov * 8);
+            *(uint4 *)(st + aoff) = th[0];
+            *(uint4 *)(st + aoff + 128) = th[1];
+            *(uint4 *)(st + 4096 + aoff) = tl[0];
+            *(uint4 *)(st + 4096 + aoff + 128) = tl[1];
+          }
+          // B: output polarisation j's rows of the cell's footprint, split
+          // (kept from two tiles back when the cell is the same)
+          if ((s ? bkey1 : bkey0) != kx) {
+            if (s)
+              bkey1 = kx;
+            else
+              bkey0 = kx;
+            const int du = kx & 255, dv = kx >> 8;
+#pragma unroll
+            for (int h = 0; h < 2; ++h) {
+              const int rr = br + 4 * h;
+              float2 v = make_float2(0.f, 0.f);
+              if (bsrc >= 0 && rr < S && bc < S) v = sub[(bsrc * W + du + rr) * RS + dv + bc];
+              uint32_t rh, rl, ih, il;
+              tf32_split(v.x, rh, rl);
+              tf32_split(v.y, ih, il);
+              const uint32_t o_re = 8192 + um_kmaj(16 * j + rr, bc);
+              *(uint32_t *)(st + o_re) = rh;
+              *(uint32_t *)(st + 2048 + o_re) = rl;
+              *(uint32_t *)(st + o_re + 256) = ih;  // row + 8: the next 8-row group
+              *(uint32_t *)(st + 2048 + o_re + 256) = il;
+            }
+          }
+          // this warp's operands are written: tell the MMA thread
+          umma::fence_proxy_async();
+          umma::fence_before_sync();
+          __syncwarp();
+          if (lane == 0) um_arrive(&s_full[wg][s]);
+          if (t == 0) {
+            if (um_wait(&s_full[wg][s], (fph >> s) & 1u)) {
+              fph ^= 1u << s;
+              umma::fence_after_sync();
+              const uint32_t sa = ops_s + (uint32_t)(s * UM_STAGE);
+              const uint64_t ah = umma::desc_kmajor(sa, 128, 256);
+              const uint64_t al = umma::desc_kmajor(sa + 4096, 128, 256);
+              const uint64_t bh = umma::desc_kmajor(sa + 8192, 128, 256);
+              const uint64_t bl = umma::desc_kmajor(sa + 10240, 128, 256);
+              const uint32_t td = tmem + (uint32_t)(s * 64);
+              umma::mma_tf32(td, al, bh, idesc, false);
+              umma::mma_tf32(td, ah, bl, idesc, true);
+              umma::mma_tf32(td, ah, bh, idesc, true);
+              umma::commit(&s_done[wg][s]);
+            } else {
+              s_fault[wg] = 1;
+              atomicExch(&g_degrid_fault, 1u);
+            }
+          }
+          __syncwarp();
+          // the previous tile, while this one's MMA runs
+          if (pend) finish();
+          pend = true;
+          pL = L;
+          ps = s;
+          prow = row;
+          pmk = mk;
+          pou = ou;
+          ++tiles;
+          base = nbase;
+          L = nL;
         }
-        // the previous tile, while this one's MMA runs
-        if (pend) finish();
-        pend = true;
-        pL = L;
-        ps = s;
-        prow = row;
-        pmk = mk;
-        pou = ou;
-        ++tiles;
-        base += (uint32_t)L;
       }
       seg_lo = seg_hi;
       if (seg_hi == t_end) ++tt;
@@ -1232,14 +1321,15 @@ __global__ void __launch_bounds__(UM_THREADS, 1) k_degrid_umma(TiledDegridArgs a
   }
   // the last tile; after a wait that gave up, one more bounded wait for each
   // commit still outstanding before the columns are freed
-  if (pend && !fault) finish();
-  if (fault && t == 0) {
-    if (stuck >= 0) um_wait(&s_mbar[wg][stuck], (ph >> stuck) & 1u);
-    if (pend) um_wait(&s_mbar[wg][ps], (ph >> ps) & 1u);
+  const bool faulted = *(volatile int *)&s_fault[wg] != 0;
+  if (pend && !faulted) finish();
+  if (faulted && lane == 0) {
+    if (stuck >= 0) um_wait(&s_done[wg][stuck], (dph >> stuck) & 1u);
+    if (pend) um_wait(&s_done[wg][ps], (dph >> ps) & 1u);
   }
   umma::fence_before_sync();
   __syncthreads();
-  if (tid < 32) {
+  if (gwarp == 0) {
     umma::fence_after_sync();
     umma::tmem_dealloc(s_taddr, 512);
   }

@@ -104,6 +104,19 @@ __device__ __forceinline__ bool mbar_try_wait(uint64_t *mbar, uint32_t parity) {
       : "memory");
   return ok != 0;
 }
+// The same probe with a suspend-time hint: the thread sleeps until the phase
+// completes or about `ns` nanoseconds have passed, instead of spinning.
+__device__ __forceinline__ bool mbar_try_wait_sleep(uint64_t *mbar, uint32_t parity, uint32_t ns) {
+  uint32_t ok;
+  asm volatile(
+      "{\n\t.reg .pred P1;\n\t"
+      "mbarrier.try_wait.parity.shared::cta.b64 P1, [%1], %2, %3;\n\t"
+      "selp.b32 %0, 1, 0, P1;\n\t}\n"
+      : "=r"(ok)
+      : "r"(smem_addr(mbar)), "r"(parity), "r"(ns)
+      : "memory");
+  return ok != 0;
+}
 
 // 32 consecutive FP32 columns of the 32 tensor-memory lanes of this warp's
 // quarter: lane i of the warp gets row (taddr lane + i), columns [c, c + 32).
