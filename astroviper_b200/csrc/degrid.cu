@@ -232,6 +232,32 @@ __device__ void build_tap_tables_d(float *tab, double *rs, const double *cgk, in
   }
 }
 
+// Taps of offset o - 128 (the reference's kernel indices |sampling ix + off|,
+// standard_degrid.py:466-469) divided by their FP64 sum, so that the product
+// of a sample's row and column taps carries its 1 / norm (the reference's
+// norm, the sum of the 2-D taps, standard_degrid.py:464-485, is the product
+// of the two sums); a zero sum gives zero taps (and a zero value, as norm ==
+// 0 does in the reference).  tab[o * RW + i], zero past the support.
+template <int S, int RW>
+__device__ void build_norm_tap_tables(float *tab, const double *cgk, int cgk_len, int os) {
+  for (int o = threadIdx.x; o < 256; o += blockDim.x) {
+    const int off = o - 128;
+    double v[RW], s = 0.0;
+#pragma unroll
+    for (int i = 0; i < RW; ++i) {
+      v[i] = 0.0;
+      if (i < S) {
+        int k = os * (i - S / 2) + off;
+        k = k < 0 ? -k : k;
+        v[i] = (k < cgk_len) ? cgk[k] : 0.0;
+        s += v[i];
+      }
+    }
+#pragma unroll
+    for (int i = 0; i < RW; ++i) tab[o * RW + i] = s != 0.0 ? (float)(v[i] / s) : 0.f;
+  }
+}
+
 __device__ __forceinline__ void put_value(const DegridArgs &d, int accumulate, int64_t k,
                                           double vr, double vi) {
   if (d.values_c128) {
@@ -556,7 +582,8 @@ __global__ void __launch_bounds__(DT_THREADS) k_degrid_tiled(TiledDegridArgs a) 
 // with cv_m the sample's column taps and P[q][r][c] the cell's footprint value
 // at row r, column c for output q = (grid polarisation, real | imaginary):
 // one mma.sync.m16n8k8.tf32 per output (8 rows, k = 8 columns), and then
-// V[m][q] = sum over r of cu_m[r] D[m][(q, r)] on the FP32 pipe.  TF32 keeps
+// V[m][q] = sum over r of cu_m[r] D[m][(q, r)] on the FP32 pipe (row and
+// column taps come divided by their tap sums, so V carries 1 / norm).  TF32 keeps
 // 11 significant bits, so both operands are split into a TF32 high part and
 // the TF32-rounded remainder (the taps once, in a table; the patch once per
 // cell) and the products hi.hi, hi.lo and lo.hi are accumulated in FP32: what
@@ -577,14 +604,10 @@ struct TCSmem {
   static constexpr size_t tab_bytes = 256 * RW * sizeof(float);
   // the same taps split into TF32 (high, remainder) pairs
   static constexpr size_t tabs_bytes = 256 * RW * sizeof(uint2);
-  static constexpr size_t rs_bytes = 256 * sizeof(double);
   static constexpr size_t rec_bytes = (size_t)(TC_THREADS / 32) * TC_ROUND * sizeof(Rec);
-  static constexpr size_t inv_bytes = (size_t)(TC_THREADS / 32) * TC_ROUND * sizeof(float);
   static constexpr size_t off_tabs = tab_bytes;
-  static constexpr size_t off_rs = off_tabs + tabs_bytes;
-  static constexpr size_t off_rec = off_rs + rs_bytes;
-  static constexpr size_t off_inv = off_rec + rec_bytes;
-  static constexpr size_t off_sub = off_inv + inv_bytes;
+  static constexpr size_t off_rec = off_tabs + tabs_bytes;
+  static constexpr size_t off_sub = off_rec + rec_bytes;
   static constexpr size_t sub_bytes = (size_t)W * W * 4 * sizeof(float2);  // [cell][pol]
   static constexpr size_t total = off_sub + sub_bytes;
   static_assert(off_sub % 16 == 0, "alignment");
@@ -626,9 +649,7 @@ __global__ void __launch_bounds__(TC_THREADS, 2) k_degrid_tc(TiledDegridArgs a) 
   extern __shared__ __align__(16) unsigned char smem[];
   float *tab = (float *)smem;
   uint2 *tabs = (uint2 *)(smem + M::off_tabs);
-  double *rs = (double *)(smem + M::off_rs);
   Rec *st_rec = (Rec *)(smem + M::off_rec);
-  float *st_inv = (float *)(smem + M::off_inv);
   float2 *sub = (float2 *)(smem + M::off_sub);
   const DegridArgs &d = a.d;
 
@@ -636,7 +657,8 @@ __global__ void __launch_bounds__(TC_THREADS, 2) k_degrid_tc(TiledDegridArgs a) 
   const uint32_t n_rec = *a.n_rec;
   const uint32_t n_all = (uint32_t)a.n_rows;  // store mode: every sample is written
   const int64_t n_chunks = ((int64_t)n_all + a.chunk - 1) / a.chunk;
-  build_tap_tables_d<S, RW>(tab, rs, d.cf, a.cgk_len, d.sampling);
+  // row and column taps over their sums: the products carry 1 / norm
+  build_norm_tap_tables<S, RW>(tab, d.cf, a.cgk_len, d.sampling);
   __syncthreads();
   for (int i = threadIdx.x; i < 256 * RW; i += TC_THREADS) {
     uint2 hl;
@@ -690,14 +712,13 @@ __global__ void __launch_bounds__(TC_THREADS, 2) k_degrid_tc(TiledDegridArgs a) 
       __syncthreads();
 
       // this warp's slice of the segment, in rounds of 64 records (two per
-      // lane): records and 1 / norm go to the warp's staging area, from which
-      // the lanes of a group read the samples they need
+      // lane): records go to the warp's staging area, from which the lanes of
+      // a group read the samples they need
       const uint32_t seg_n = seg_hi - seg_lo;
       const uint32_t w_lo = seg_lo + (uint32_t)(((uint64_t)seg_n * warp) / WARPS);
       const uint32_t w_hi = seg_lo + (uint32_t)(((uint64_t)seg_n * (warp + 1)) / WARPS);
       const int n_rounds = (int)((w_hi - w_lo + TC_ROUND - 1) / TC_ROUND);
       Rec *wrec = st_rec + warp * TC_ROUND;
-      float *winv = st_inv + warp * TC_ROUND;
       int cur = -1;
       // patch fragments of the current cell, one n-tile per output q =
       // (polarisation q / 2, real | imaginary): b = P[q][r = g][c = t, t + 4]
@@ -735,19 +756,14 @@ __global__ void __launch_bounds__(TC_THREADS, 2) k_degrid_tc(TiledDegridArgs a) 
         // staged records carry a shared plan's mark in the row's top bit (the
         // host runs this kernel only for fewer than 2^31 rows)
         if (va) {
-          const double norm = rs[ra.ou] * rs[ra.ov];
-          // 1 / norm in FP64, the scaling in FP32; zero-norm samples get 0
           Rec x = ra;
           if ((ma >> (r & 31u)) & 1u) x.row |= REC_DEGRID_EXC;
           wrec[lane] = x;
-          winv[lane] = norm != 0.0 ? (float)(1.0 / norm) : 0.f;
         }
         if (vb) {
-          const double norm = rs[rb.ou] * rs[rb.ov];
           Rec x = rb;
           if ((mb >> ((r + 32) & 31u)) & 1u) x.row |= REC_DEGRID_EXC;
           wrec[lane + 32] = x;
-          winv[lane + 32] = norm != 0.0 ? (float)(1.0 / norm) : 0.f;
         }
         int pa = __shfl_up_sync(FULL, ka, 1);
         if (lane == 0) pa = cur;
@@ -783,7 +799,6 @@ __global__ void __launch_bounds__(TC_THREADS, 2) k_degrid_tc(TiledDegridArgs a) 
           const int sg = j0 + g, sh = j0 + g + 8;
           const bool vg = sg < j1, vh = sh < j1;
           const Rec recg = wrec[vg ? sg : j0], rech = wrec[vh ? sh : j0];
-          const float invg = winv[vg ? sg : j0], invh = winv[vh ? sh : j0];
           const int oug = recg.ou, ovg = recg.ov, ouh = rech.ou, ovh = rech.ov;
           // A = the column taps of samples g and g + 8 (columns t, t + 4),
           // split in the table; an empty slot is a zero row
@@ -836,11 +851,11 @@ __global__ void __launch_bounds__(TC_THREADS, 2) k_degrid_tc(TiledDegridArgs a) 
           const bool uh = (rech.row & REC_DEGRID_EXC) == 0u;
           if (vg)
             out[(int64_t)(recg.row & ~REC_DEGRID_EXC) * 4 + t] =
-                (src >= 0 && ug) ? make_float2(__fmul_rn(xgre, invg), __fmul_rn(xgim, invg))
+                (src >= 0 && ug) ? make_float2(xgre, xgim)
                                  : make_float2(0.f, 0.f);
           if (vh)
             out[(int64_t)(rech.row & ~REC_DEGRID_EXC) * 4 + t] =
-                (src >= 0 && uh) ? make_float2(__fmul_rn(xhre, invh), __fmul_rn(xhim, invh))
+                (src >= 0 && uh) ? make_float2(xhre, xhim)
                                  : make_float2(0.f, 0.f);
         };
         int j = 0;
@@ -1020,29 +1035,11 @@ __global__ void __launch_bounds__(UM_THREADS, 1) k_degrid_umma(TiledDegridArgs a
   const int tid = threadIdx.x, wg = tid >> 7, t = tid & 127, j = t >> 5, lane = tid & 31;
   const int gwarp = tid >> 5;
 
-  // taps of offset o - 128 (the reference's kernel indices |sampling ix +
-  // off|, standard_degrid.py:466-469), over their FP64 sum; a zero sum gives
-  // zero taps (and a zero value, as norm == 0 does in the reference)
-  for (int o = tid; o < 256; o += UM_THREADS) {
-    const int off = o - 128;
-    double v[8], s = 0.0;
-#pragma unroll
-    for (int i = 0; i < 8; ++i) {
-      v[i] = 0.0;
-      if (i < S) {
-        int k = d.sampling * (i - S / 2) + off;
-        k = k < 0 ? -k : k;
-        v[i] = (k < a.cgk_len) ? d.cf[k] : 0.0;
-        s += v[i];
-      }
-    }
-#pragma unroll
-    for (int i = 0; i < 8; ++i) {
-      const float x = s != 0.0 ? (float)(v[i] / s) : 0.f;
-      tab[o * 8 + i] = x;
-      tf32_split(x, tabh[o * 8 + i], tabl[o * 8 + i]);
-    }
-  }
+  // row and column taps over their sums (the products carry 1 / norm), and
+  // their TF32 splits
+  build_norm_tap_tables<S, 8>(tab, d.cf, a.cgk_len, d.sampling);
+  __syncthreads();
+  for (int i = tid; i < 256 * 8; i += UM_THREADS) tf32_split(tab[i], tabh[i], tabl[i]);
   if (gwarp == 0) {
     umma::tmem_alloc(&s_taddr, 512);
     umma::tmem_relinquish();
