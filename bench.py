@@ -54,6 +54,9 @@ def parse():
     ap.add_argument("--no-imager", action="store_true")
     ap.add_argument("--no-mosaic", action="store_true")
     ap.add_argument("--clean-iters", type=int, default=20000)
+    ap.add_argument("--degrid-lanes", default="auto", choices=["auto", "tf32", "fp32", "tc05"],
+                    help="the degridder's fast store path: the library's choice (auto), warp "
+                         "TF32 MMAs, FP32 FMA, or tcgen05 MMAs with tensor-memory accumulators")
     return ap.parse_args()
 
 
@@ -312,6 +315,10 @@ def main():
     from astroviper_b200 import _lib
     from astroviper_b200 import synthetic as S
     from astroviper_b200.gridder import Gridder
+    if args.degrid_lanes != "auto":
+        lanes = {"tf32": _lib.AV_DEGRID_LANES_TF32, "fp32": _lib.AV_DEGRID_LANES_FP32,
+                 "tc05": _lib.AV_DEGRID_LANES_TC05}[args.degrid_lanes]
+        _lib.check(_lib.lib().av_tune_set(_lib.AV_TUNE_DEGRID_LANES, lanes), "av_tune_set")
     dev = torch.device("cuda", local)
     n_time = args.n_time
 
@@ -378,8 +385,9 @@ def main():
     # (read now: later legs may tune the knobs)
     grid_kernel = ("k_grid_tiled" if _lib.lib().av_tune_get(_lib.AV_TUNE_GRID_LANES) ==
                    _lib.AV_GRID_LANES_ROWS else "k_grid_mma")
-    degrid_kernel = ("k_degrid_tiled" if _lib.lib().av_tune_get(_lib.AV_TUNE_DEGRID_LANES) ==
-                     _lib.AV_DEGRID_LANES_FP32 else "k_degrid_tc")
+    degrid_kernel = {_lib.AV_DEGRID_LANES_FP32: "k_degrid_tiled",
+                     _lib.AV_DEGRID_LANES_TC05: "k_degrid_umma"}.get(
+        _lib.lib().av_tune_get(_lib.AV_TUNE_DEGRID_LANES), "k_degrid_tc")
 
     if world > 1:
         dist.barrier()
@@ -395,6 +403,13 @@ def main():
     e1.record()
     torch.cuda.synchronize()
     launches = int(_lib.lib().av_launch_count() - launches0)
+    if degrid_kernel == "k_degrid_umma":  # its bounded waits must all have held
+        import ctypes
+        fault = ctypes.c_int(-1)
+        _lib.check(_lib.lib().av_degrid_fault_read(ctypes.byref(fault), 1, K.stream_ptr()),
+                   "av_degrid_fault_read")
+        if fault.value:
+            raise RuntimeError("k_degrid_umma: a wait for its MMAs gave up")
     if world > 1:
         dist.barrier()
     clk = clocks.stop()
@@ -517,7 +532,8 @@ def main():
                      "kernel_ms": dom[2]},
         "fp64_tensor": fp64_tensor,
         "kernels_ms": {"grid_tiled": t_grid_k, "degrid_tiled": t_degrid_k,
-                       "plan_and_rest": ms - t_grid_k - t_degrid_k},
+                       "plan_and_rest": ms - t_grid_k - t_degrid_k,
+                       "degrid_kernel": degrid_kernel},
         "fp64_plain_gridder": {"value": plain_mvis, "unit": "Mvis/s",
                                "sample": f"{ts} of {nt} time steps"},
         "speedup_vs_fp64_plain": (n_vis / (t_grid_k / 1e3) / 1e6) / plain_mvis,
