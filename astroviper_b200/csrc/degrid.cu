@@ -577,23 +577,26 @@ __global__ void __launch_bounds__(DT_THREADS) k_degrid_tiled(TiledDegridArgs a) 
 // ------------------------------------------------------- tensor cores ----
 // k_degrid_tc: the tiled degridder's fast store path (complex64 values, 4
 // visibility and 4 grid polarisations, no flags, no phase) on the TF32 tensor
-// path.  For one cell and 16 samples the row sums are a matrix product,
-//   D[m][(q, r)] = sum over c of cv_m[c] P[q][r][c],
+// path.  For one cell, 16 samples and each footprint row r, the column sums
+// are a matrix product,
+//   D_r[m][q] = sum over c of cv_m[c] P[q][r][c],
 // with cv_m the sample's column taps and P[q][r][c] the cell's footprint value
-// at row r, column c for output q = (grid polarisation, real | imaginary):
-// one mma.sync.m16n8k8.tf32 per output (8 rows, k = 8 columns), and then
-// V[m][q] = sum over r of cu_m[r] D[m][(q, r)] on the FP32 pipe (row and
-// column taps come divided by their tap sums, so V carries 1 / norm).  TF32 keeps
-// 11 significant bits, so both operands are split into a TF32 high part and
-// the TF32-rounded remainder (the taps once, in a table; the patch once per
-// cell) and the products hi.hi, hi.lo and lo.hi are accumulated in FP32: what
-// is left out is below 2^-22 of each product.  Fragment layout (lane = 4 g +
-// t): a = cv[g][t], cv[g + 8][t], cv[g][t + 4], cv[g + 8][t + 4] (samples g
-// and g + 8); b = P[q][g][t], P[q][g][t + 4]; d = D[g][(q, 2t)],
-// D[g][(q, 2t + 1)], D[g + 8][(q, 2t)], D[g + 8][(q, 2t + 1)].  Lane (g, t)
-// thus weights rows 2t and 2t + 1 with its row taps; two shuffles within the
-// quad complete the sum over rows, and the lane writes polarisation t of
-// samples g and g + 8.
+// at row r, column c for output q = (output polarisation, real | imaginary):
+// one mma.sync.m16n8k8.tf32 per row (n = 8 outputs, k = 8 columns), rows at
+// or past the support skipped.  Then V[m][q] = sum over r of cu_m[r]
+// D_r[m][q] accumulates on the FP32 pipe in the lane that holds D_r[m][q]
+// (row and column taps come divided by their tap sums, so V carries
+// 1 / norm).  TF32 keeps 11 significant bits, so both operands are split into
+// a TF32 high part and the TF32-rounded remainder (the taps once, in a table;
+// the patch once per cell) and the products hi.hi, hi.lo and lo.hi are
+// accumulated in FP32: what is left out is below 2^-22 of each product.
+// Fragment layout (lane = 4 g + t): a = cv[g][t], cv[g + 8][t], cv[g][t + 4],
+// cv[g + 8][t + 4] (samples g and g + 8); b = P[q = g][r][t], P[g][r][t + 4]
+// (output g, read from grid polarisation polmap[g / 2]); d = D_r[g][2t],
+// D_r[g][2t + 1], D_r[g + 8][2t], D_r[g + 8][2t + 1].  Lane (g, t) thus owns
+// the real and imaginary parts of output polarisation t of samples g and
+// g + 8, sums them over the rows with its row taps, and writes them: no
+// shuffles.
 constexpr int TC_THREADS = 256;
 constexpr int TC_ROUND = 64;  // records a warp stages per round (two per lane)
 
@@ -667,11 +670,15 @@ __global__ void __launch_bounds__(TC_THREADS, 2) k_degrid_tc(TiledDegridArgs a) 
   }
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const int g = lane >> 2, t = lane & 3;
-  // output polarisation t takes grid polarisation polmap[t]
-  int src = -1;
+  // this lane writes output polarisation t (from grid polarisation polmap[t]);
+  // its B column is output q = g: polarisation g / 2 (from grid polarisation
+  // bsrc), real or imaginary part g % 2
+  int src = -1, bsrc = -1;
   {
     const int v = d.polmap[t];
     if (v >= 0 && v < 4 && v < d.g_npol) src = v;
+    const int u = d.polmap[g >> 1];
+    if (u >= 0 && u < 4 && u < d.g_npol) bsrc = u;
   }
   const int64_t gplane = d.g_n2 * d.g_n3;
 
@@ -720,8 +727,8 @@ __global__ void __launch_bounds__(TC_THREADS, 2) k_degrid_tc(TiledDegridArgs a) 
       const int n_rounds = (int)((w_hi - w_lo + TC_ROUND - 1) / TC_ROUND);
       Rec *wrec = st_rec + warp * TC_ROUND;
       int cur = -1;
-      // patch fragments of the current cell, one n-tile per output q =
-      // (polarisation q / 2, real | imaginary): b = P[q][r = g][c = t, t + 4]
+      // patch fragments of the current cell, one k x n tile per footprint
+      // row r: b = P[q = g][r][c = t, t + 4]
       uint32_t bh[8][2], bl[8][2];
 #pragma unroll
       for (int q = 0; q < 8; ++q) bh[q][0] = bh[q][1] = bl[q][0] = bl[q][1] = 0u;
@@ -776,20 +783,23 @@ __global__ void __launch_bounds__(TC_THREADS, 2) k_degrid_tc(TiledDegridArgs a) 
         __syncwarp();
         const int jn = (int)min((uint32_t)TC_ROUND, w_hi - (w_lo + (uint32_t)rd * TC_ROUND));
         // a run starts at sample j: its cell's patch, split, into bh / bl
+        // (this lane: output q = g, footprint rows 0 .. S - 1, columns t and
+        // t + 4; the real or imaginary part of grid polarisation bsrc)
         auto load_patch = [&](const int j) {
           const Rec rj = wrec[j];
           cur = (int)rj.du | ((int)rj.dv << 8);
           const int du = rj.du, dv = rj.dv;
-          const bool rok = g < S;
+          const float *sf = (const float *)sub + (g & 1);
 #pragma unroll
-          for (int pol = 0; pol < 4; ++pol) {
-            float2 v0 = make_float2(0.f, 0.f), v1 = make_float2(0.f, 0.f);
-            if (rok && t < S) v0 = sub[((du + g) * W + dv + t) * 4 + pol];
-            if (rok && t + 4 < S) v1 = sub[((du + g) * W + dv + t + 4) * 4 + pol];
-            tf32_split(v0.x, bh[2 * pol][0], bl[2 * pol][0]);
-            tf32_split(v1.x, bh[2 * pol][1], bl[2 * pol][1]);
-            tf32_split(v0.y, bh[2 * pol + 1][0], bl[2 * pol + 1][0]);
-            tf32_split(v1.y, bh[2 * pol + 1][1], bl[2 * pol + 1][1]);
+          for (int r = 0; r < S; ++r) {
+            float x0 = 0.f, x1 = 0.f;
+            if (bsrc >= 0) {
+              const int e = ((du + r) * W + dv + t) * 4 + bsrc;
+              if (t < S) x0 = sf[2 * e];
+              if (t + 4 < S) x1 = sf[2 * (e + 16)];  // 4 columns on
+            }
+            tf32_split(x0, bh[r][0], bl[r][0]);
+            tf32_split(x1, bh[r][1], bl[r][1]);
           }
         };
         // one group of 16 samples [j0, j0 + 16) of a run ending at j1
@@ -805,45 +815,29 @@ __global__ void __launch_bounds__(TC_THREADS, 2) k_degrid_tc(TiledDegridArgs a) 
           const uint2 z = make_uint2(0u, 0u);
           const uint2 ag0 = vg ? tabs[ovg * RW + t] : z, ag1 = vg ? tabs[ovg * RW + t + 4] : z;
           const uint2 ah0 = vh ? tabs[ovh * RW + t] : z, ah1 = vh ? tabs[ovh * RW + t + 4] : z;
-          // row taps r = 2t, 2t + 1 for the final sum over rows
-          const float2 cg = *(const float2 *)&tab[oug * RW + 2 * t];
-          const float2 ch = *(const float2 *)&tab[ouh * RW + 2 * t];
-          // D[m][(q, r)] = sum_c cv_m[c] P[q][r][c]: the row sums, one
-          // n-tile (8 rows) per output q, three TF32 products each
-          float dq[8][4];
-  #pragma unroll
-          for (int q = 0; q < 8; ++q) {
-            dq[q][0] = dq[q][1] = dq[q][2] = dq[q][3] = 0.f;
-            mma_tf32(dq[q], ag0.y, ah0.y, ag1.y, ah1.y, bh[q][0], bh[q][1]);
-            mma_tf32(dq[q], ag0.x, ah0.x, ag1.x, ah1.x, bl[q][0], bl[q][1]);
-            mma_tf32(dq[q], ag0.x, ah0.x, ag1.x, ah1.x, bh[q][0], bh[q][1]);
-          }
-          // V[m][q] = sum_r cu_m[r] D[m][(q, r)]: rows 2t, 2t + 1 here, the
-          // other rows in the quad's other lanes
-          float vgq[8], vhq[8];
-  #pragma unroll
-          for (int q = 0; q < 8; ++q) {
-            float pg = __fmul_rn(cg.x, dq[q][0]);
-            pg = __fmaf_rn(cg.y, dq[q][1], pg);
-            float ph = __fmul_rn(ch.x, dq[q][2]);
-            ph = __fmaf_rn(ch.y, dq[q][3], ph);
-            pg = __fadd_rn(pg, __shfl_xor_sync(FULL, pg, 1));
-            ph = __fadd_rn(ph, __shfl_xor_sync(FULL, ph, 1));
-            pg = __fadd_rn(pg, __shfl_xor_sync(FULL, pg, 2));
-            ph = __fadd_rn(ph, __shfl_xor_sync(FULL, ph, 2));
-            vgq[q] = pg;
-            vhq[q] = ph;
-          }
-          // this lane writes polarisation t, from grid polarisation src
+          // row taps of samples g and g + 8
+          const float4 cg0 = *(const float4 *)&tab[oug * RW];
+          const float4 cg1 = *(const float4 *)&tab[oug * RW + 4];
+          const float4 ch0 = *(const float4 *)&tab[ouh * RW];
+          const float4 ch1 = *(const float4 *)&tab[ouh * RW + 4];
+          const float cug[8] = {cg0.x, cg0.y, cg0.z, cg0.w, cg1.x, cg1.y, cg1.z, cg1.w};
+          const float cuh[8] = {ch0.x, ch0.y, ch0.z, ch0.w, ch1.x, ch1.y, ch1.z, ch1.w};
+          // per footprint row r: D_r[m][q] = sum_c cv_m[c] P[q][r][c] (three
+          // TF32 products), of which this lane holds outputs q = 2t, 2t + 1
+          // (polarisation t, real and imaginary) of samples g and g + 8, and
+          // V[m][q] = sum_r cu_m[r] D_r[m][q] accumulates in the lane
           float xgre = 0.f, xgim = 0.f, xhre = 0.f, xhim = 0.f;
   #pragma unroll
-          for (int pol = 0; pol < 4; ++pol)
-            if (pol == src) {
-              xgre = vgq[2 * pol];
-              xgim = vgq[2 * pol + 1];
-              xhre = vhq[2 * pol];
-              xhim = vhq[2 * pol + 1];
-            }
+          for (int r = 0; r < S; ++r) {
+            float dr[4] = {0.f, 0.f, 0.f, 0.f};
+            mma_tf32(dr, ag0.y, ah0.y, ag1.y, ah1.y, bh[r][0], bh[r][1]);
+            mma_tf32(dr, ag0.x, ah0.x, ag1.x, ah1.x, bl[r][0], bl[r][1]);
+            mma_tf32(dr, ag0.x, ah0.x, ag1.x, ah1.x, bh[r][0], bh[r][1]);
+            xgre = __fmaf_rn(cug[r], dr[0], xgre);
+            xgim = __fmaf_rn(cug[r], dr[1], xgim);
+            xhre = __fmaf_rn(cuh[r], dr[2], xhre);
+            xhim = __fmaf_rn(cuh[r], dr[3], xhim);
+          }
           // a shared plan's marked sample gets 0 here (k_degrid_exceptions
           // writes the ones the degridder keeps)
           float2 *out = (float2 *)d.values;
