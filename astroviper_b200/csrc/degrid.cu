@@ -1503,8 +1503,8 @@ static int launch_degrid_tiled(const TiledDegridArgs &a, int64_t nblocks, cudaSt
 }
 
 // The TF32 tensor-core kernel for the fast store path with 4 grid
-// polarisations as AV_TUNE_DEGRID_LANES says (automatically for supports 7
-// and 8, where it is the faster), the FP32 kernel otherwise.
+// polarisations as AV_TUNE_DEGRID_LANES says (automatically for every support
+// it covers, 3-8, where it is the faster), the FP32 kernel otherwise.
 template <int S>
 static int degrid_dispatch_npg(const TiledDegridArgs &a, int npg, int64_t nb, cudaStream_t st) {
   if (npg == 1) return launch_degrid_tiled<S, 1>(a, nb, st);
@@ -1513,8 +1513,7 @@ static int degrid_dispatch_npg(const TiledDegridArgs &a, int npg, int64_t nb, cu
     const int64_t lanes = tune_value(AV_TUNE_DEGRID_LANES);
     if (a.fast_out && a.d.g_npol == 4 && lanes == AV_DEGRID_LANES_TC05)
       return launch_degrid_umma<S>(a, nb, st);
-    const bool tf32 =
-        lanes == AV_DEGRID_LANES_TF32 || (lanes == AV_DEGRID_LANES_AUTO && S >= 7);
+    const bool tf32 = lanes == AV_DEGRID_LANES_TF32 || lanes == AV_DEGRID_LANES_AUTO;
     // the TF32 kernel keeps a shared plan's marks in the staged rows' top bit
     if (a.fast_out && a.d.g_npol == 4 && tf32 && a.n_rows < (int64_t)REC_DEGRID_EXC)
       return launch_degrid_tc<S>(a, nb, st);

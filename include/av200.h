@@ -82,8 +82,8 @@ unsigned long long av_launch_count(void);
  *                                split operands on the fifth-generation
  *                                tensor cores, accumulators in tensor memory,
  *                                supports up to 8) or AV_DEGRID_LANES_AUTO
- *                                (default: TF32 for supports 7 and 8, FP32
- *                                otherwise)
+ *                                (default: TF32 for supports up to 8, FP32
+ *                                for 9)
  *   AV_TUNE_HOGBOM_BARRIER_TIMEOUT_US  how long (microseconds of wall time,
  *                                default 2000000) a CTA of av_hogbom_run
  *                                waits at the per-iteration grid barrier
