@@ -279,6 +279,34 @@ def test_degrid_fast_store_every_support(support, polmap, degrid_lanes):
     assert rel(v.cpu().numpy(), ref) <= 1e-6
 
 
+@pytest.mark.parametrize("polmap", [(0, -1, 2, 7), (1, 1, 0, 0)])
+def test_degrid_fast_store_unmapped_and_repeated_polarisations(polmap, degrid_lanes):
+    """The fast store path with a polarisation map that leaves outputs
+    unmapped (-1, or past the grid's polarisations: zeros) or reads one grid
+    polarisation twice: the mapped outputs match the FP64 degridder on the
+    same grid polarisation, the unmapped ones are exactly zero."""
+    g = golden("degrid.npz")
+    rng = np.random.default_rng(7)
+    nt, nb = g["uvw"].shape[:2]
+    n2, n3 = g["grid"].shape[2:]
+    grid = rng.normal(size=(2, 4, n2, n3)) + 1j * rng.normal(size=(2, 4, n2, n3))
+    cf = O.create_prolate_spheroidal_kernel_1D(100, 7)
+    pm = np.array(polmap, dtype=np.int32)
+    v = K().degrid(torch.as_tensor(grid), g["uvw"], g["freq"], g["scale"][:2], g["offset"][:2],
+                   g["chanmap"], pm, cf, 7, 100, nvchan=3, nvpol=4, precision="fp32",
+                   accumulate=False).cpu().numpy()
+    ident = np.arange(4, dtype=np.int32)
+    ref = np.zeros((nt, nb, 3, 4), complex)
+    O.dgrid_numba(g["uvw"], np.zeros((nt, nb)), ref, np.zeros((nt, nb, 3, 4), bool),
+                  g["scale"], g["offset"], grid, g["freq"], 299792458.0, 7, 100, cf,
+                  g["chanmap"], ident)
+    for p, src in enumerate(polmap):
+        if 0 <= src < 4:
+            assert rel(v[..., p], ref[..., src]) <= 1e-6
+        else:
+            assert np.all(v[..., p] == 0)
+
+
 @pytest.fixture(params=["mma", "rows"])
 def grid_lanes(request):
     """Runs a test under each of the tiled gridder's lane mappings: FP64
