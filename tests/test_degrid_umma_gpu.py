@@ -1,9 +1,9 @@
 """The tensor-memory degridder (AV_DEGRID_LANES_TC05, k_degrid_umma).
 
-Tiles of up to 128 records spanning at most two cells go through one
-tcgen05 MMA chain each; these tests run it on long runs (the 33M-sample
-workload's continuum grid), on short runs and runs that end at every
-position of a tile (a dense uv distribution), on small chunks (many
+Tiles of up to 128 records of one cell go through one tcgen05 MMA chain
+each, with accumulators in tensor memory; these tests run it on long runs
+(the 33M-sample workload's continuum grid), on short runs and runs that end
+at every position of a tile (a dense uv distribution), on small chunks (many
 segments per warpgroup), on a shared plan with exception samples, and check
 it against the FP64 plain degridder (the reference's arithmetic,
 standard_degrid.py:388-485) and against the warp-MMA kernel k_degrid_tc.
