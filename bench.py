@@ -152,6 +152,17 @@ def max_over_ranks(ms, world, device=None):
     return float(t.item())
 
 
+def max_elem_err(a, b):
+    """max |a - b| / max(|b|, 1e-7 max |b|) over the elements: the per-element
+    error with an absolute floor of 1e-7 of the largest reference value."""
+    import torch
+    a = a.to(torch.complex128) if a.is_complex() else a.double()
+    b = b.to(torch.complex128) if b.is_complex() else b.double()
+    mag = b.abs()
+    floor = 1e-7 * float(mag.max())
+    return float(((a - b).abs() / torch.clamp(mag, min=floor)).max()) if floor > 0 else 0.0
+
+
 def rel(a, b):
     import torch
     if isinstance(a, torch.Tensor):
@@ -436,22 +447,27 @@ def main():
     t_plain = pa.elapsed_time(pb)
     plain_mvis = ts * nb * nchan / (t_plain / 1e3) / 1e6
     err_grid = rel(g32, g64)
+    mx_grid = max_elem_err(g32, g64)
     im32 = Gs.image(g32, s32)
     im64 = Gs.image(g64, s64)
     err_img = rel(im32, im64)
+    mx_img = max_elem_err(im32, im64)
     # PSF: the weights gridded (do_psf) and imaged, FP32-input tiled path
     # against the FP64 plain gridder
     p32, ps32 = Gs.grid(None, iw[:ts], do_psf=True)
     p64, ps64 = K.grid(None, iw_s, uvw_s, W["freq"], np.zeros(nchan, int), np.arange(npol),
                        G.cgk, img, cell, 7, 100, 1, npol, do_psf=True, precision="fp64")
-    err_psf = rel(Gs.image(p32, ps32), Gs.image(p64, ps64))
-    del p32, p64
+    pi32, pi64 = Gs.image(p32, ps32), Gs.image(p64, ps64)
+    err_psf = rel(pi32, pi64)
+    mx_psf = max_elem_err(pi32, pi64)
+    del p32, p64, pi32, pi64
     v32 = Gs.degrid(g64)
     nx, ny = int(img[0]), int(img[1])
     v64 = K.degrid(g64, uvw_s, W["freq"], (-cell[0] * nx, -cell[1] * ny), (nx / 2, ny / 2),
                    (np.arange(nchan) / nchan * 1).astype(int), np.arange(npol) % npol, G.cgk, 7,
                    100, nvchan=nchan, nvpol=npol, precision="fp64")
     err_vis = rel(v32, v64)
+    mx_vis = max_elem_err(v32, v64)
     del g64, v64, v32, vis_s
     torch.cuda.empty_cache()
 
@@ -539,6 +555,9 @@ def main():
         "speedup_vs_fp64_plain": (n_vis / (t_grid_k / 1e3) / 1e6) / plain_mvis,
         "rel_err_vs_fp64": {"grid": err_grid, "dirty_image": err_img, "psf": err_psf,
                             "degrid_vis": err_vis, "sample": f"{ts} of {nt} time steps"},
+        "max_elem_err_vs_fp64": {"grid": mx_grid, "dirty_image": mx_img, "psf": mx_psf,
+                                 "degrid_vis": mx_vis,
+                                 "definition": "max |x - x64| / max(|x64|, 1e-7 max |x64|)"},
         "clocks": clk,
         "gpu_launches": launches,
         "cpu_baseline": cpu,
