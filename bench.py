@@ -536,6 +536,7 @@ def main():
                        "peak_source": "av_probe_fp64_mma (mma.sync.m16n8k4.f64) on this GPU"}
     line = {
         "metric": METRIC, "value": value, "unit": "Mvis/s", "n_gpus": world,
+        "Mcorr_per_s": value * npol,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
         "data": "synthetic",
